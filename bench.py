@@ -1,0 +1,337 @@
+"""Benchmark of the RTM propagation hot path (Gpts/s per time step).
+
+Workload (default `vti_cfd`): the VTI pseudo-acoustic single-shot RTM forward
+pass on a 512 x 512 x 400 grid (10 m, 32-cell PML, compact FD, seeded smooth
+layered velocity 1500-4500 m/s, eps 0-0.25, delta 0-0.1, 20 Hz Ricker), with
+the reference's default COMPRESS_16 snapshot store every 8 steps.  One bench
+step = one time step of the forward migration loop (operator with PML,
+update, source injection, snapshot when due), inputs resident in HBM.
+Every volume is 419 MB > the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+N > 1 runs N independent replicas (one shot per GPU, no collective; shots are
+independent in RTM), launched by torch.distributed.run.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic HBM bytes per cell-step (each array read / written once per step)
+#   VTI core: R w1, w0, vel, eps, del; W w0 = 24 B; PML memory 48 B x fraction
+#   of cells in PML slabs (3 first derivatives x 2 rounds x q r/w).
+ALG_BYTES = {"vti_cfd": None, "iso128": None, "tti_q": None}
+
+
+def pml_fraction(spec):
+    f = 0.0
+    for n, a, b in ((spec.nx, spec.nbnd[0], spec.nbnd[1]), (spec.ny, spec.nbnd[2], spec.nbnd[3]),
+                    (spec.nz, spec.nbnd[4], spec.nbnd[5])):
+        f += (a + b) / n
+    return f
+
+
+def alg_bytes_per_cell(spec, snap_fmt, interval):
+    from konglong_b200.spec import ISO, TTI, VTI
+    m = pml_fraction(spec)
+    if spec.model_type == ISO and spec.engine == 0:
+        core, pml = 16.0, 16.0 * m
+    elif spec.model_type == VTI:
+        core, pml = 24.0, 48.0 * m
+    else:
+        core, pml = 32.0, 48.0 * m
+    if spec.use_q:
+        core += 4.0 + 3 * 4.0 * spec.q_order
+    snap = {0: 4.0, 1: 2.0, 2: 2.0}[snap_fmt] / interval
+    return core + pml + snap, core, pml
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4)
+                          if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_workload(name, steps_total):
+    from konglong_b200 import workloads as W
+    if name == "vti_cfd":
+        return W.vti_cfd(scale=1.0, nt=steps_total)
+    if name == "iso128":
+        return W.iso128(scale=1.0, nt=steps_total)
+    if name == "tti_q":
+        return W.tti_q(scale=1.0, nt=steps_total)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def config_of(shot, snap_fmt, steps):
+    s = shot.spec
+    return {"workload": f"{shot.name}: {s.nx}x{s.ny}x{s.nz} {'CFD' if s.engine else 'FD8'} "
+                        f"{['', 'ISO', 'VTI', 'TTI'][s.model_type]}{'+Q' if s.use_q else ''}, PML {s.nbnd[0]}, "
+                        f"dt {s.dt * 1e3:.4f} ms, forward RTM step, snapshots every {shot.interval} steps",
+            "grid": [s.nx, s.ny, s.nz], "cells": s.n, "snapshot_format": ["fp32", "c16", "fp16s"][snap_fmt],
+            "l2": "inputs larger than L2 (419 MB per volume), no flush", "dt_s": s.dt}
+
+
+def run_cuda(args, rank, world):
+    import ctypes as C
+    from konglong_b200 import workloads as W
+    from konglong_b200.propagator import Propagator, spread_coeffs
+    from konglong_b200.spec import FORWARD, SNAP_C16
+
+    K, Wm = args.steps, args.warmup
+    shot = build_workload(args.workload, K + Wm + 8)
+    s = shot.spec
+    snap_fmt = SNAP_C16
+    k1, k2 = W.spread_band(s)
+    src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    rcv = W.make_traceset(shot.rcv_pos, s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    p = Propagator(s)
+    if s.use_q:
+        p.set_q_coeffs(*W.q_coefficients(s.dt, shot.fpeak))
+    p.set_model(**shot.model_arrays())
+    nslots = (K + Wm + shot.interval - 1) // shot.interval + 1
+    p.snapshot_setup(snap_fmt, nslots)
+    p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
+    p.reset()
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    # warm-up steps (untimed), then K timed steps continuing the same shot
+    p.migration(FORWARD, 0, Wm, -1, shot.interval)
+    if dist:
+        tdist.barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        p.migration(FORWARD, Wm, Wm + K, -1, shot.interval)
+    ms = p.last_loop_ms
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+        tdist.barrier()
+    cells = s.n
+    value = world * cells * K / (ms * 1e-3) / 1e9
+    ms_step = ms / K
+
+    # per-kernel device times of one step (CUDA events between launches)
+    prof = p.profile_step() if hasattr(p, "profile_step") else None
+    alg, core, pml = alg_bytes_per_cell(s, snap_fmt, shot.interval)
+    step_bytes = alg * cells
+    peak = 6550.7
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        peak_src = "measured"
+    except Exception:
+        peak_src = "fallback"
+    roof = {"bound": "hbm", "kernel": "time step (all kernels of one step)", "achieved": step_bytes / (ms_step * 1e-3) / 1e9,
+            "peak": peak, "unit": "GB/s", "frac": None, "traffic": None, "alg_bytes_per_cell": round(alg, 2),
+            "peak_source": peak_src}
+    roof["frac"] = roof["achieved"] / peak
+    if prof:
+        roof.update(prof)
+
+    # end to end through the public API with host buffers: modelling run of K
+    # steps with the receiver samples read back (set_injection H2D of the
+    # source trace, modelling, D2H of every extracted sample)
+    e2e = None
+    if not args.no_e2e:
+        q = Propagator(s)
+        if s.use_q:
+            q.set_q_coeffs(*W.q_coefficients(s.dt, shot.fpeak))
+        q.set_model(**shot.model_arrays())
+        q.set_extraction(rcv, K)
+        q.reset()
+        q.set_injection(src, shot.wavelet[None, :K + 1].copy(), s.dt_dxyz)
+        q.modelling(2, -1, 1)  # warm the graph path
+        q.reset()
+        wav = np.ascontiguousarray(shot.wavelet[None, :K + 1])
+        if dist:
+            tdist.barrier()
+        t0 = time.perf_counter()
+        q.set_injection(src, wav, s.dt_dxyz)
+        q.modelling(K, -1, 1)
+        tr = q.traces()
+        t1 = time.perf_counter()
+        wall = t1 - t0
+        if dist:
+            import torch
+            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": world * cells * K / wall / 1e9, "unit": "Gpts/s",
+               "h2d_bytes_per_step": int(wav.nbytes // K), "d2h_bytes_per_step": int(tr.nbytes // K),
+               "what": "Propagator.modelling via the C ABI: traces H2D, K steps with receiver extraction, "
+                       "receiver samples D2H; wall clock"}
+        q.close()
+    launches = p.launch_count() if hasattr(p, "launch_count") else None
+    p.close()
+    return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
+                config=config_of(shot, snap_fmt, K), shot=shot, launches=launches)
+
+
+def cpu_baseline(shot, max_seconds=20.0):
+    """The reference's own CPU kernels (oracle/_ref) on the full grid, all host
+    threads, a bounded number of time steps."""
+    from oracle import pyoracle as O
+    if not O.ref_available():
+        return None, "port"
+    s = shot.spec
+    if s.use_q:
+        return None, "reference"
+    threads = os.cpu_count() or 1
+    r = O.Reference(s, nthreads=threads)
+    r.set_model(shot.vel, shot.eps, shot.dl, shot.pjx, shot.pjy)
+    r.reset()
+    first = r.run(1, 1)
+    n = max(1, min(50, int(max_seconds / max(first, 1e-3))))
+    t = r.run(2, n)
+    r.close()
+    return {"value": s.n * n / t / 1e9, "unit": "Gpts/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} full time steps ({s.nx}x{s.ny}x{s.nz}) of bgprtm KernelCPU "
+                      f"({'CFD' if s.engine else 'FD8'}) + update2nd + source injection, "
+                      f"OMP {threads} threads, {t:.1f} s"}, "reference"
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (oracle/_ref, else the oracle
+    port) timed on this host's cores on the same workload."""
+    from oracle import pyoracle as O
+    shot = build_workload(args.workload, args.steps + args.warmup + 8)
+    s = shot.spec
+    threads = os.cpu_count() or 1
+    if O.ref_available() and not s.use_q:
+        r = O.Reference(s, nthreads=threads)
+        r.set_model(shot.vel, shot.eps, shot.dl, shot.pjx, shot.pjy)
+        kind = "reference"
+    else:
+        r = O.Oracle(s)
+        r.set_model(**shot.model_arrays())
+        kind = "port"
+    r.reset()
+    # warm-up (bounded)
+    t_first = None
+    for w in range(min(args.warmup, 1)):
+        t0 = time.perf_counter()
+        r.kernel(), r.update2nd(), r.swap()
+        t_first = time.perf_counter() - t0
+    budget = 150.0
+    k = args.steps
+    if t_first and t_first * k > budget:
+        k = max(1, int(budget / t_first))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        r.kernel(), r.update2nd(), r.swap()
+    t = time.perf_counter() - t0
+    val = s.n * k / t / 1e9
+    return {"value": val, "k": k, "kind": kind, "threads": threads, "t": t, "shot": shot}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = run_reference(args, rank, world)
+        shot = r["shot"]
+        line = {"metric": "Gpts/s per step", "value": r["value"], "unit": "Gpts/s", "n_gpus": args.gpus,
+                "steps": r["k"], "warmup": min(args.warmup, 1), "ms_per_step": r["t"] / r["k"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded model)", "impl": "reference",
+                "config": config_of(shot, 1, r["k"]),
+                "cpu_baseline": {"value": r["value"], "unit": "Gpts/s", "cores": r["threads"], "kind": r["kind"],
+                                 "sample": f"{r['k']} full time steps on the full grid, {r['t']:.1f} s"},
+                "e2e": {"value": r["value"], "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        try:
+            import torch
+            torch.cuda.set_device(0)
+        except Exception:
+            pass
+    r = run_cuda(args, rank, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = cpu_baseline(r["shot"])
+    if rank == 0:
+        line = {"metric": "Gpts/s per step", "value": r["value"], "unit": "Gpts/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded model)", "config": r["config"], "roofline": r["roofline"],
+                "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"],
+                "gpu_launches": r["launches"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

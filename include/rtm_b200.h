@@ -1,0 +1,214 @@
+/*
+ * rtm_b200.h - C ABI of the B200 reverse-time-migration propagation engine.
+ *
+ * This is the drop-in boundary for bgprtm's propagation path.  Every entry
+ * point takes plain pointers and sizes, returns an int status (0 = ok,
+ * negative = rtm_status), never aborts and never throws.  Host arrays are
+ * copied; device state is owned by the handle.  A handle is bound to the
+ * CUDA device that was current at rtm_create and to one internal stream; it
+ * is not thread-safe, but several handles (shots) may live side by side.
+ *
+ * Volume layout everywhere is the reference's: z fastest, then x, then y,
+ * element (ix, iy, iz) at ((iy * nx + ix) * nz + iz)
+ * (bgprtm/FdEngine.h:41-43, bgprtm/Propagator.cpp:528).
+ *
+ * Reference seams replaced (bgprtm, C++ objects, no C ABI of their own):
+ *   KernelCPU::KernelCPU/setModel/setBoundary   -> rtm_create, rtm_set_model
+ *       (bgprtm/KernelCPU.h:19-27)
+ *   KernelCPU::ISO / VTI / TTI                  -> rtm_kernel
+ *       (bgprtm/KernelCPU.h:29-33, bgprtm/KernelCPU.cpp:93-174)
+ *   KernelCPU::cleanPMLMemory, Wavefield::cleanMemory -> rtm_reset
+ *       (bgprtm/KernelCPU.h:35, bgprtm/Wavefield.cpp:144-170)
+ *   Propagator::update2nd (+ Q branch)          -> rtm_update2nd
+ *       (bgprtm/Propagator.cpp:1764-1818)
+ *   Propagator::Vel2                            -> inside rtm_set_model
+ *       (bgprtm/Propagator.cpp:711-742)
+ *   Q::updateCq                                 -> rtm_set_q_coeffs
+ *       (bgprtm/Q.cpp:310-318)
+ *   Receiver::apply / apply_src                 -> rtm_inject
+ *       (bgprtm/Receiver.cpp:1204-1279, 477-507)
+ *   ExtractReceiverData::extract / extract_value -> rtm_extract
+ *       (bgprtm/ExtractReceiverData.cpp:199-262, bgprtm/Receiver.cpp:394-426)
+ *   Util::CompactOrmsbySpreadCoeff              -> rtm_spread_coeffs
+ *       (bgprtm/Util.cpp:317-397, bgprtm/Receiver.cpp:291-363)
+ *   Wavefield::swapPointers                     -> rtm_swap
+ *       (bgprtm/Wavefield.cpp:175-178)
+ *   WaveFieldCompress::compress / uncompress    -> rtm_c16_compress / rtm_c16_uncompress
+ *       and snapshot store                     -> rtm_snapshot_store
+ *       (bgprtm/WaveFieldCompress.cpp:107-236)
+ *   ImagingCorrelator::crossone + ImagingCondition::applyTape -> rtm_image_accumulate
+ *       (bgprtm/ImagingCorrelator.cpp:180-194, bgprtm/ImagingCondition.cpp:180-226)
+ *   Propagator::modelling / migration time loops -> rtm_modelling / rtm_migration
+ *       (bgprtm/Propagator.cpp:1054-1155, 1157-1260)
+ */
+#ifndef RTM_B200_H
+#define RTM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rtm_status {
+  RTM_OK = 0,
+  RTM_ERR_ARG = -1,         /* bad argument (null pointer, size out of range) */
+  RTM_ERR_STATE = -2,       /* call out of order (e.g. no model set) */
+  RTM_ERR_CUDA = -3,        /* CUDA runtime error (message via rtm_last_error) */
+  RTM_ERR_NOMEM = -4,       /* device allocation failed */
+  RTM_ERR_UNSUPPORTED = -5, /* configuration not built */
+  RTM_ERR_NONFINITE = -6,   /* NaN/Inf detected in an input or the state */
+  RTM_ERR_TIMEOUT = -7      /* a bounded device wait gave up */
+} rtm_status;
+
+enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1 };      /* FD::FD, FD::CFD */
+enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
+enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
+enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2 };
+enum {
+  RTM_FIELD_W0 = 0,  /* current/next wavefield (written by the step) */
+  RTM_FIELD_W1 = 1,  /* previous wavefield (read by the stencil) */
+  RTM_FIELD_VEL = 2, /* (v*dt)^2 after Vel2 */
+  RTM_FIELD_IMAGE = 3,
+  RTM_FIELD_INVQ = 4 /* invQ after the Vel2 correction */
+};
+
+typedef struct rtm_dims {
+  int nx, ny, nz;   /* grid incl. PML; nx, nz >= 9 */
+  float dx, dy, dz; /* spacing (m) */
+  float dt;         /* time step (s) */
+} rtm_dims;
+
+typedef struct rtm_config {
+  int engine;         /* RTM_ENGINE_FD8 or RTM_ENGINE_CFD */
+  int model_type;     /* RTM_ISO, RTM_VTI, RTM_TTI */
+  int use_q;          /* visco-acoustic memory variables (Q::order terms) */
+  int q_order;        /* number of memory variables, default 4 */
+  int nbnd[6];        /* PML widths: x1, x2, y1, y2, z1, z2 (0 = none) */
+  float vmax;         /* PML profile velocity (m/s) */
+  float pml_eps;      /* PML reflection target, default 1e-3 */
+  int pml3d;          /* default 1: PML on the summed operator / cross terms */
+  float pml3d_scaler; /* cross-term damping scale, default 0.3 */
+  int top_pml;        /* default 1; 0 = free surface top (no z1 PML) */
+  int state_fp16;     /* 0: FP32 wavefield state (default) */
+} rtm_config;
+
+typedef struct rtm_handle rtm_handle;
+
+/* Fills the reference's defaults (pml_eps 1e-3, pml3d 1, scaler 0.3, q_order 4). */
+void rtm_config_default(rtm_config *cfg);
+
+/* Reference seam: KernelCPU(nx,ny,nz,dx,dy,dz,engine,nThreads) + setBoundary(...)
+ * (bgprtm/KernelCPU.h:19,27; bgprtm/FdEngine.cpp:108-182).  Allocates all device
+ * state (wavefields, PML memory, Q memory) and builds the FD / CFD tables and
+ * the PML profile in FP64. */
+int rtm_create(const rtm_dims *dims, const rtm_config *cfg, rtm_handle **out);
+int rtm_destroy(rtm_handle *h);
+
+/* Text of the last error on this handle (or of the last failed create when h is NULL). */
+const char *rtm_last_error(const rtm_handle *h);
+
+/* Q::updateCq (bgprtm/Q.cpp:310-318): cq0, cq[q_order], wq[q_order].  Must
+ * precede rtm_set_model when use_q. */
+int rtm_set_q_coeffs(rtm_handle *h, float cq0, const float *cq, const float *wq);
+
+/* KernelCPU::setModel + Propagator::Vel2 (bgprtm/KernelCPU.cpp:76-83,
+ * bgprtm/Propagator.cpp:711-742).  vel is velocity in m/s; it is converted to
+ * (v*dt)^2 on the device (Q-corrected when use_q).  eps/del are needed for
+ * VTI/TTI, pjx/pjy for TTI, invq (1/Q) for use_q; others may be NULL. */
+int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float *del,
+                  const float *pjx, const float *pjy, const float *invq);
+
+/* Zero wavefields, PML memory, Q memory and the extracted traces
+ * (Wavefield::cleanMemory + KernelCPU::cleanPMLMemory). */
+int rtm_reset(rtm_handle *h);
+
+/* One application of the spatial operator: w0 -= (v dt)^2 * L[w1]
+ * (KernelCPU::ISO/VTI/TTI with PML, bgprtm/KernelCPU.cpp:93-174). */
+int rtm_kernel(rtm_handle *h);
+
+/* Leapfrog w0 = 2 w1 - w0, or the Q form (bgprtm/Propagator.cpp:1767-1818). */
+int rtm_update2nd(rtm_handle *h);
+
+/* Swap w0/w1 and the Q memory halves (Wavefield::swapPointers). */
+int rtm_swap(rtm_handle *h);
+
+/* Separable spread kernel of one trace along one axis
+ * (Util::CompactOrmsbySpreadCoeff with nlimit, bgprtm/Util.cpp:317-397, then
+ * the edge taper of Receiver::spreadCoeffs, bgprtm/Receiver.cpp:291-303).
+ * n: grid size on the axis; x: fractional grid index; k1, k2: pass/cut
+ * wavenumbers (fraction of Nyquist*0.5, 0 < k1 <= k2 <= 0.5); *nlimit: in =
+ * kernel capacity (2*spread), out = used length; coeff[nlimit]; ntaper: edge
+ * taper length (0 = none).  Returns the first grid index in *off. */
+int rtm_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper,
+                      float *coeff, int *off);
+
+/* Traces injected into w0 each step (Receiver::apply, no FK/true-amp path):
+ * w0[c] += traces[r][it] * scaler * kx[r][ix] * ky[r][iy] * kz[r][iz] * (v dt)^2[c]
+ * Kernels are packed with fixed strides lx, ly, lz per trace; off3/len3 are
+ * [ntr][3] (x, y, z) first index and used length.  scaler is the reference's
+ * dt_dxyz = 1/(dx*dy*dz) times Receiver::apply's scaler0.  Copies everything. */
+int rtm_set_injection(rtm_handle *h, int ntr, int lx, int ly, int lz, const int *off3,
+                      const int *len3, const float *kx, const float *ky, const float *kz,
+                      const float *traces, int nt, float scaler);
+
+/* Receivers read from w0 (ExtractReceiverData::extract with template receivers):
+ * out[r][jt] = sum kx*ky*kz*w0 over the trace's kernel box. */
+int rtm_set_extraction(rtm_handle *h, int ntr, int lx, int ly, int lz, const int *off3,
+                       const int *len3, const float *kx, const float *ky, const float *kz,
+                       int nt_out);
+
+/* Apply injection sample it (no-op outside [0, nt)). */
+int rtm_inject(rtm_handle *h, int it);
+/* Extract receivers into sample jt (no-op outside [0, nt_out)). */
+int rtm_extract(rtm_handle *h, int jt);
+/* Copy extracted traces [ntr][nt_out] to host. */
+int rtm_get_traces(rtm_handle *h, float *dst);
+
+/* Snapshot store for the source wavefield: nslots slots of format fmt
+ * (RTM_SNAP_FP32 uncompressed, RTM_SNAP_C16 = the reference's COMPRESS_16
+ * codec, bit-exact, RTM_SNAP_FP16S = FP16 with a per-y-slab scale). */
+int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots);
+/* Store w0 into slot (WaveFieldCompress::compress + CacheFile write). */
+int rtm_snapshot_store(rtm_handle *h, int slot);
+/* Decode slot into dst (host, N floats) with the reference's decode tapers. */
+int rtm_snapshot_load(rtm_handle *h, int slot, float *dst);
+
+/* Imaging condition set-up: ntaper_t source time-taper snapshots, ntaper_z
+ * depth-taper cells (ImagingCondition::calTapes), edge_taper=1 applies the
+ * snapshot decode tapers (20 cells x/y, 10 z) to both fields
+ * (WaveFieldCompress::uncompress16).  Clears the image. */
+int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge_taper);
+/* image += T(src[slot]) * T(w0), zero lag, Kahan-compensated FP32. */
+int rtm_image_accumulate(rtm_handle *h, int slot);
+
+/* Propagator::modelling loop (bgprtm/Propagator.cpp:1099-1153): for it in
+ * [0, nts): kernel, update2nd, inject(it + it_shift), extract(it / ntratio)
+ * when it % ntratio == 0, swap.  Fused kernels; time loop in a CUDA graph. */
+int rtm_modelling(rtm_handle *h, int nts, int it_shift, int ntratio);
+
+/* Propagator::migration loop (bgprtm/Propagator.cpp:1210-1255).
+ * dir = RTM_FORWARD: it = 0 .. it_end-1, inject(it + it_shift), store slot
+ *   it/interval when it % interval == 0 and the slot exists.
+ * dir = RTM_BACKWARD: it = it_begin down to it_end+1, inject(it - it_shift),
+ *   image += src[it/interval] * w0 when it % interval == 0 and that slot was
+ *   stored (the zero-lag correlation fused into the backward step). */
+int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift, int interval);
+
+/* Copy a field (RTM_FIELD_*) of N floats to / from host memory. */
+int rtm_get(rtm_handle *h, int field, float *dst);
+int rtm_put(rtm_handle *h, int field, const float *src);
+
+/* The reference's COMPRESS_16 codec on host buffers, run on the device
+ * (bit-exact with WaveFieldCompress::compress16/uncompress16).  out holds
+ * (nx*nz + 2) * ny uint16 values.  uncompress applies the decode tapers. */
+int rtm_c16_compress(const float *in, unsigned short *out, int nx, int ny, int nz);
+int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int nz);
+
+/* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
+int rtm_last_loop_ms(rtm_handle *h, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTM_B200_H */

@@ -1,0 +1,105 @@
+"""ctypes binding of the in-tree CUDA library konglong_b200/_rtm_b200.so.
+
+The C ABI is declared in include/rtm_b200.h.  There is no CPU fallback: if the
+library is missing or fails to load, import-time use raises RuntimeError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_rtm_b200.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+
+RTM_OK = 0
+STATUS = {0: "RTM_OK", -1: "RTM_ERR_ARG", -2: "RTM_ERR_STATE", -3: "RTM_ERR_CUDA",
+          -4: "RTM_ERR_NOMEM", -5: "RTM_ERR_UNSUPPORTED", -6: "RTM_ERR_NONFINITE",
+          -7: "RTM_ERR_TIMEOUT"}
+
+# every entry point of include/rtm_b200.h
+EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", "rtm_set_q_coeffs",
+           "rtm_set_model", "rtm_reset", "rtm_kernel", "rtm_update2nd", "rtm_swap",
+           "rtm_spread_coeffs", "rtm_set_injection", "rtm_set_extraction", "rtm_inject",
+           "rtm_extract", "rtm_get_traces", "rtm_snapshot_setup", "rtm_snapshot_store",
+           "rtm_snapshot_load", "rtm_image_setup", "rtm_image_accumulate", "rtm_modelling",
+           "rtm_migration", "rtm_get", "rtm_put", "rtm_c16_compress", "rtm_c16_uncompress",
+           "rtm_last_loop_ms"]
+
+
+class RtmDims(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_float),
+                ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float)]
+
+
+class RtmConfig(C.Structure):
+    _fields_ = [("engine", C.c_int), ("model_type", C.c_int), ("use_q", C.c_int),
+                ("q_order", C.c_int), ("nbnd", C.c_int * 6), ("vmax", C.c_float),
+                ("pml_eps", C.c_float), ("pml3d", C.c_int), ("pml3d_scaler", C.c_float),
+                ("top_pml", C.c_int), ("state_fp16", C.c_int)]
+
+
+class RtmError(RuntimeError):
+    def __init__(self, code, what, detail=""):
+        self.code = code
+        super().__init__(f"{what} failed: {STATUS.get(code, code)}" + (f" ({detail})" if detail else ""))
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (built by konglong_b200.build / __graft_entry__.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m konglong_b200.build` "
+                           "(the CUDA path has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    i = C.c_int
+    f = C.c_float
+    L.rtm_config_default.argtypes = [C.POINTER(RtmConfig)]
+    L.rtm_config_default.restype = None
+    L.rtm_create.argtypes = [C.POINTER(RtmDims), C.POINTER(RtmConfig), C.POINTER(vp)]
+    L.rtm_destroy.argtypes = [vp]
+    L.rtm_last_error.argtypes = [vp]
+    L.rtm_last_error.restype = C.c_char_p
+    L.rtm_set_q_coeffs.argtypes = [vp, f, _f32p, _f32p]
+    L.rtm_set_model.argtypes = [vp] + [vp] * 6
+    for name in ("rtm_reset", "rtm_kernel", "rtm_update2nd", "rtm_swap"):
+        getattr(L, name).argtypes = [vp]
+    L.rtm_spread_coeffs.argtypes = [i, f, f, f, C.POINTER(i), i, i, _f32p, C.POINTER(i)]
+    L.rtm_set_injection.argtypes = [vp, i, i, i, i, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, i, f]
+    L.rtm_set_extraction.argtypes = [vp, i, i, i, i, _i32p, _i32p, _f32p, _f32p, _f32p, i]
+    L.rtm_inject.argtypes = [vp, i]
+    L.rtm_extract.argtypes = [vp, i]
+    L.rtm_get_traces.argtypes = [vp, _f32p]
+    L.rtm_snapshot_setup.argtypes = [vp, i, i]
+    L.rtm_snapshot_store.argtypes = [vp, i]
+    L.rtm_snapshot_load.argtypes = [vp, i, _f32p]
+    L.rtm_image_setup.argtypes = [vp, i, i, i]
+    L.rtm_image_accumulate.argtypes = [vp, i]
+    L.rtm_modelling.argtypes = [vp, i, i, i]
+    L.rtm_migration.argtypes = [vp, i, i, i, i, i]
+    L.rtm_get.argtypes = [vp, i, vp]
+    L.rtm_put.argtypes = [vp, i, vp]
+    L.rtm_c16_compress.argtypes = [_f32p, _u16p, i, i, i]
+    L.rtm_c16_uncompress.argtypes = [_u16p, _f32p, i, i, i]
+    L.rtm_last_loop_ms.argtypes = [vp, C.POINTER(f)]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if name not in ("rtm_config_default", "rtm_last_error"):
+            fn.restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(code, what, handle=None):
+    if code != RTM_OK:
+        detail = lib().rtm_last_error(handle)
+        raise RtmError(code, what, detail.decode() if detail else "")

@@ -1,0 +1,105 @@
+// kernel_api.h - argument blocks and launchers of the B200 RTM kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "rtm_internal.cuh"
+
+namespace rtm {
+
+struct IsoArgs {
+  int nx, ny, nz, yseg;
+  const float *w1;
+  float *w0;
+  const float *vel;
+  float c2x[5], c2y[5], c2z[5];
+  PmlDev pml;
+  FusedIo io;
+  QDev q;
+};
+
+struct GradArgs {
+  int nx, ny, nz, yseg, pml3d;
+  const float *w1;
+  float *px, *py, *pz;
+  const float *eps, *del, *pjx, *pjy;
+  float c1x[5], c1y[5], c1z[5];
+  PmlDev pml;
+  FusedIo io;
+};
+
+struct DivArgs {
+  int nx, ny, nz, yseg, pml3d;
+  const float *px, *py, *pz;
+  const float *w1;
+  float *w0;
+  const float *vel;
+  float c1x[5], c1y[5], c1z[5];
+  PmlDev pml;
+  QDev q;
+};
+
+// mode: 0 = operator only (w0 -= vel*L), 1 = + leapfrog update, 2 = + Q update
+void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
+void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st);
+void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
+
+// ---- compact FD (kernels_cfd.cu) -------------------------------------------
+struct CfdPlanDev {
+  int n;
+  const float *bm, *bl, *am;  // [n][5], [n][4], [60]
+};
+// one-time attribute set-up of the compact-FD kernels (outside any capture)
+int cfd_init();
+// raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML)
+void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, float *scratch, int nx, int ny,
+                      int nz, cudaStream_t st);
+
+struct CfdGradEpiArgs {  // PML round 1 + scaling on raw gradients, in place
+  int nx, ny, nz, pml3d, model;
+  float *gx, *gy, *gz;
+  const float *eps, *del, *pjx, *pjy;
+  PmlDev pml;
+  FusedIo io;
+  const float *w1;
+};
+void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st);
+
+struct CfdDivEpiArgs {  // PML round 2 on raw divergence parts + update
+  int nx, ny, nz, pml3d, mode;
+  const float *dx, *dy, *dz;
+  const float *w1;
+  float *w0;
+  const float *vel;
+  PmlDev pml;
+  QDev q;
+};
+void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st);
+
+// ---- wavefield I/O, sources, receivers, snapshots (kernels_io.cu) -----------
+void launch_update2nd(float *w0, const float *w1, const QDev *q, long long n, cudaStream_t st);
+// atomic scatter of every trace of `t` (Receiver::apply_src)
+void launch_inject_scatter(const TraceDev &t, int it, float *w0, const float *vel, int nx, int ny, int nz,
+                           cudaStream_t st);
+// grouped injection: xy plane gather then z expansion
+void launch_inject_group(const GroupDev &gr, const TraceDev &t, int it, float *plane, float *w0, const float *vel,
+                         int nx, int ny, int nz, cudaStream_t st);
+void launch_extract_direct(const TraceDev &t, const float *w0, float *out, int jt, int nt_out, int nx, int ny, int nz,
+                           cudaStream_t st);
+void launch_extract_group(const GroupDev &gr, const TraceDev &t, const float *w0, float *plane, float *out, int jt,
+                          int nt_out, int nx, int ny, int nz, cudaStream_t st);
+// per-y-slab max |w| -> slab[iy]; c16 header written into hdr (may be null)
+void launch_slab_max(const float *w, float *slab, uint16_t *c16_base, int fmt, int nx, int ny, int nz, cudaStream_t st);
+// standalone snapshot store / IC (same arithmetic as the fused path)
+void launch_fused_io(const FusedIo &io, const float *u, int nx, int ny, int nz, cudaStream_t st);
+// decode a snapshot slot (with decode tapers when ex/ey/ez given)
+void launch_snap_decode(const SnapDev &s, float *out, const float *ex, const float *ey, const float *ez, int nx, int ny,
+                        int nz, cudaStream_t st);
+// COMPRESS_16 on device buffers
+void launch_c16_compress(const float *in, uint16_t *out, float *slab, int nx, int ny, int nz, cudaStream_t st);
+void launch_c16_uncompress(const uint16_t *in, float *out, float *slab, const float *ex, const float *ey,
+                           const float *ez, int nx, int ny, int nz, cudaStream_t st);
+void launch_vel2(float *vel, float *invq, long long n, float dt2, float cq0, int use_q, cudaStream_t st);
+// NaN/Inf scan: sets *flag = 1 when any value is not finite
+void launch_nonfinite_scan(const float *w, long long n, int *flag, cudaStream_t st);
+
+}  // namespace rtm

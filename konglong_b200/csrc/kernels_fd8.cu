@@ -1,0 +1,318 @@
+// kernels_fd8.cu - 8th-order finite-difference time-step kernels for sm_100a.
+//
+// Tiling: a CTA owns a 32 (z) x TX (x) column tile and marches along y, the
+// slowest axis.  Each thread keeps its column's +-4 y neighbours in a
+// register queue; the current y plane of the tile plus a 4-cell x/z halo is
+// staged in shared memory, so every wavefield value is fetched from L2 about
+// once per plane and from HBM about once per step.  Warps run along z, the
+// contiguous axis: all global accesses are 128-byte coalesced rows.
+//
+//  iso_fd8_step   KernelCPU::ISO + FdEngine_fd::laplacian_irreg + pml2_bnd
+//                 (bgprtm/KernelCPU.cpp:125-140, bgprtm/FdEngine_fd.cpp:204-325)
+//                 fused with update2nd (bgprtm/Propagator.cpp:1767-1818), the
+//                 snapshot store / imaging condition of the previous step.
+//  grad_fd8       first pass of KernelCPU::TTI (bgprtm/KernelCPU.cpp:93-119):
+//                 gradient with PML round 1 and the VTI/TTI scaling
+//                 (bgprtm/KernelCPU.cpp:176-297).
+//  div_fd8        second pass: divergence with PML round 2, accumulated into
+//                 w0, fused with update2nd.
+#include "kernel_api.h"
+#include "rtm_device.cuh"
+
+namespace rtm {
+
+namespace {
+
+constexpr int TZ = 32;
+constexpr int R = 4;  // stencil radius (order 8)
+
+__device__ __forceinline__ float ld_or0(const float *__restrict__ p, long long i, bool ok) {
+  return ok ? __ldg(p + i) : 0.0f;
+}
+
+template <int TX, int MODE, bool PML3D>
+__global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int iz = blockIdx.x * TZ + tz;
+  const int ix = blockIdx.y * TX + tx;
+  const int y0 = blockIdx.z * a.yseg;
+  const int y1 = min(a.ny, y0 + a.yseg);
+  const bool act = iz < a.nz && ix < a.nx;
+  const long long col = (long long)ix * a.nz + iz;
+  const float *__restrict__ w1 = a.w1;
+  const bool do_y = a.ny > 2;
+
+  float q[2 * R + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * R; k++) {
+    const int y = y0 - R + k;
+    q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
+  }
+  for (int iy = y0; iy < y1; iy++) {
+    q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
+    const long long plane = (long long)iy * g.nxz;
+    tile[tx + R][tz + R] = q[R];
+    if (tz < R) {
+      const int izl = iz - R, izh = iz + TZ;
+      tile[tx + R][tz] = ld_or0(w1, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
+      tile[tx + R][tz + TZ + R] = ld_or0(w1, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
+    }
+    if (tx < R) {
+      const int ixl = ix - R, ixh = ix + TX;
+      tile[tx][tz + R] = ld_or0(w1, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
+      tile[tx + TX + R][tz + R] = ld_or0(w1, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+    }
+    __syncthreads();
+    if (act) {
+      const float u = q[R];
+      float lz = a.c2z[0] * u, lx = a.c2x[0] * u, ly = 0.0f;
+#pragma unroll
+      for (int m = 1; m <= R; m++) {
+        lz += a.c2z[m] * (tile[tx + R][tz + R - m] + tile[tx + R][tz + R + m]);
+        lx += a.c2x[m] * (tile[tx + R - m][tz + R] + tile[tx + R + m][tz + R]);
+      }
+      if (do_y) {
+        ly = a.c2y[0] * u;
+#pragma unroll
+        for (int m = 1; m <= R; m++) ly += a.c2y[m] * (q[R - m] + q[R + m]);
+      }
+      float v;
+      if (PML3D) {
+        v = lz + lx + ly;
+        pml2_dim(a.pml, g, DZ, v, ix, iy, iz);
+        pml2_dim(a.pml, g, DX, v, ix, iy, iz);
+        pml2_dim(a.pml, g, DY, v, ix, iy, iz);
+      } else {
+        pml2_dim(a.pml, g, DZ, lz, ix, iy, iz);
+        pml2_dim(a.pml, g, DX, lx, ix, iy, iz);
+        if (do_y) pml2_dim(a.pml, g, DY, ly, ix, iy, iz);
+        v = lz + lx + ly;
+      }
+      const long long i = plane + col;
+      if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, u);
+      const float t = a.w0[i] - v * __ldg(a.vel + i);
+      float out;
+      if (MODE == 0) out = t;                         // KernelCPU seam: w0 -= vel * L[w1]
+      else if (MODE == 1) out = (u + u) - t;          // + update2nd (leapfrog)
+      else out = q_update(a.q, i, (long long)a.ny * g.nxz, t, u);  // + Q
+      a.w0[i] = out;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) q[k] = q[k + 1];
+  }
+}
+
+// ---- anisotropic two-pass ----------------------------------------------------
+template <int TX, int MODEL>
+__global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int iz = blockIdx.x * TZ + tz;
+  const int ix = blockIdx.y * TX + tx;
+  const int y0 = blockIdx.z * a.yseg;
+  const int y1 = min(a.ny, y0 + a.yseg);
+  const bool act = iz < a.nz && ix < a.nx;
+  const long long col = (long long)ix * a.nz + iz;
+  const float *__restrict__ w1 = a.w1;
+  const bool do_y = a.ny > 1;
+
+  float q[2 * R + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * R; k++) {
+    const int y = y0 - R + k;
+    q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
+  }
+  for (int iy = y0; iy < y1; iy++) {
+    q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
+    const long long plane = (long long)iy * g.nxz;
+    tile[tx + R][tz + R] = q[R];
+    if (tz < R) {
+      const int izl = iz - R, izh = iz + TZ;
+      tile[tx + R][tz] = ld_or0(w1, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
+      tile[tx + R][tz + TZ + R] = ld_or0(w1, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
+    }
+    if (tx < R) {
+      const int ixl = ix - R, ixh = ix + TX;
+      tile[tx][tz + R] = ld_or0(w1, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
+      tile[tx + TX + R][tz + R] = ld_or0(w1, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+    }
+    __syncthreads();
+    if (act) {
+      const long long i = plane + col;
+      float gz = 0.f, gx = 0.f, gy = 0.f;
+#pragma unroll
+      for (int m = 1; m <= R; m++) {
+        gz += a.c1z[m] * (tile[tx + R][tz + R + m] - tile[tx + R][tz + R - m]);
+        gx += a.c1x[m] * (tile[tx + R + m][tz + R] - tile[tx + R - m][tz + R]);
+        if (do_y) gy += a.c1y[m] * (q[R + m] - q[R - m]);
+      }
+      if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
+      pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
+      pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
+      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
+      if (MODEL == 2 || MODEL == 3) {
+        // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
+        float e = __ldg(a.eps + i);
+        const float dl = e - __ldg(a.del + i);
+        e = 1.0f + 2.0f * e;
+        if (MODEL == 3) {
+          const float ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
+          const float az = sqrtf(1.0f - (ax * ax + ay * ay));
+          const float v2 = gx * gx + gy * gy + gz * gz;
+          const float vzz = gx * ax + gy * ay + gz * az;
+          const float vz2 = vzz * vzz;
+          const float vh2 = v2 - vz2;
+          const float ecl = e * vh2 + vz2;
+          const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) / (ecl * ecl + 1e-32f));
+          const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
+          const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
+          gx = (bx + (gx - bx) * e) * sc;
+          gy = (by + (gy - by) * e) * sc;
+          gz = (bz + (gz - bz) * e) * sc;
+        } else {
+          const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
+          const float ecl = e * vx2 + vz2;
+          const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) / (ecl * ecl + 1e-32f));
+          const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
+          gx *= sc2;
+          gy *= sc2;
+        }
+      }
+      a.px[i] = gx;
+      a.pz[i] = gz;
+      if (do_y) a.py[i] = gy;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) q[k] = q[k + 1];
+  }
+}
+
+template <int TX, int MODE>
+__global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
+  __shared__ float tpx[TX + 2 * R][TZ];
+  __shared__ float tpz[TX][TZ + 2 * R];
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int iz = blockIdx.x * TZ + tz;
+  const int ix = blockIdx.y * TX + tx;
+  const int y0 = blockIdx.z * a.yseg;
+  const int y1 = min(a.ny, y0 + a.yseg);
+  const bool act = iz < a.nz && ix < a.nx;
+  const long long col = (long long)ix * a.nz + iz;
+  const bool do_y = a.ny > 1;
+
+  float q[2 * R + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * R; k++) {
+    const int y = y0 - R + k;
+    q[k] = do_y ? ld_or0(a.py, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny) : 0.f;
+  }
+  for (int iy = y0; iy < y1; iy++) {
+    if (do_y) q[2 * R] = ld_or0(a.py, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
+    const long long plane = (long long)iy * g.nxz;
+    tpx[tx + R][tz] = ld_or0(a.px, plane + col, act);
+    tpz[tx][tz + R] = ld_or0(a.pz, plane + col, act);
+    if (tz < R) {
+      const int izl = iz - R, izh = iz + TZ;
+      tpz[tx][tz] = ld_or0(a.pz, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
+      tpz[tx][tz + TZ + R] = ld_or0(a.pz, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
+    }
+    if (tx < R) {
+      const int ixl = ix - R, ixh = ix + TX;
+      tpx[tx][tz] = ld_or0(a.px, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
+      tpx[tx + TX + R][tz] = ld_or0(a.px, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+    }
+    __syncthreads();
+    if (act) {
+      const long long i = plane + col;
+      float dxv = 0.f, dzv = 0.f, dyv = 0.f;
+#pragma unroll
+      for (int m = 1; m <= R; m++) {
+        dxv += a.c1x[m] * (tpx[tx + R + m][tz] - tpx[tx + R - m][tz]);
+        dzv += a.c1z[m] * (tpz[tx][tz + R + m] - tpz[tx][tz + R - m]);
+        if (do_y) dyv += a.c1y[m] * (q[R + m] - q[R - m]);
+      }
+      pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
+      pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
+      if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+      const float vel = __ldg(a.vel + i);
+      // accumulation order of KernelCPU::TTI: x, then z, then y
+      float t = a.w0[i] - dxv * vel;
+      t = t - dzv * vel;
+      t = t - dyv * vel;
+      float out;
+      if (MODE == 0) out = t;
+      else {
+        const float u = __ldg(a.w1 + i);
+        out = MODE == 1 ? (u + u) - t : q_update(a.q, i, (long long)a.ny * g.nxz, t, u);
+      }
+      a.w0[i] = out;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) q[k] = q[k + 1];
+  }
+}
+
+}  // namespace
+
+static dim3 fd_grid(int nx, int ny, int nz, int tx, int yseg) {
+  return dim3((nz + TZ - 1) / TZ, (nx + tx - 1) / tx, (ny + yseg - 1) / yseg);
+}
+
+template <int TX>
+static void iso_launch_tx(const IsoArgs &a, int mode, int pml3d, cudaStream_t st) {
+  dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
+#define ISO_L(M, P) iso_fd8_step<TX, M, P><<<grid, block, 0, st>>>(a)
+  if (pml3d) {
+    if (mode == 0) ISO_L(0, true);
+    else if (mode == 1) ISO_L(1, true);
+    else ISO_L(2, true);
+  } else {
+    if (mode == 0) ISO_L(0, false);
+    else if (mode == 1) ISO_L(1, false);
+    else ISO_L(2, false);
+  }
+#undef ISO_L
+}
+
+void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st) {
+  if (tx == 4) iso_launch_tx<4>(a, mode, pml3d, st);
+  else if (tx == 16) iso_launch_tx<16>(a, mode, pml3d, st);
+  else iso_launch_tx<8>(a, mode, pml3d, st);
+}
+
+template <int TX>
+static void grad_launch_tx(const GradArgs &a, int model, cudaStream_t st) {
+  dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
+  if (model == 3) grad_fd8<TX, 3><<<grid, block, 0, st>>>(a);
+  else if (model == 2) grad_fd8<TX, 2><<<grid, block, 0, st>>>(a);
+  else grad_fd8<TX, 1><<<grid, block, 0, st>>>(a);
+}
+
+void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st) {
+  if (tx == 4) grad_launch_tx<4>(a, model, st);
+  else if (tx == 16) grad_launch_tx<16>(a, model, st);
+  else grad_launch_tx<8>(a, model, st);
+}
+
+template <int TX>
+static void div_launch_tx(const DivArgs &a, int mode, cudaStream_t st) {
+  dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
+  if (mode == 0) div_fd8<TX, 0><<<grid, block, 0, st>>>(a);
+  else if (mode == 1) div_fd8<TX, 1><<<grid, block, 0, st>>>(a);
+  else div_fd8<TX, 2><<<grid, block, 0, st>>>(a);
+}
+
+void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st) {
+  if (tx == 4) div_launch_tx<4>(a, mode, st);
+  else if (tx == 16) div_launch_tx<16>(a, mode, st);
+  else div_launch_tx<8>(a, mode, st);
+}
+
+}  // namespace rtm

@@ -1,0 +1,318 @@
+// kernels_io.cu - the non-stencil kernels of a time step: leapfrog update,
+// source / receiver injection (Receiver::apply), receiver extraction
+// (ExtractReceiverData::extract), snapshot codecs (WaveFieldCompress) and the
+// standalone imaging condition.  All are HBM- or latency-bound elementwise /
+// gather work: no tensor cores, coalesced along z.
+#include <cuda_fp16.h>
+
+#include "kernel_api.h"
+#include "rtm_device.cuh"
+
+namespace rtm {
+
+namespace {
+
+__global__ void update2nd_k(float *__restrict__ w0, const float *__restrict__ w1, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float u = w1[i];
+    w0[i] = (u + u) - w0[i];
+  }
+}
+
+__global__ void update2nd_q_k(float *__restrict__ w0, const float *__restrict__ w1, QDev q, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    w0[i] = q_update(q, i, n, w0[i], w1[i]);
+}
+
+// one CTA per trace, threads over the kernel box (iz fastest)
+__global__ void inject_scatter_k(TraceDev t, int it, float *__restrict__ w0, const float *__restrict__ vel, int nx,
+                                 int nz) {
+  const int r = t.ids ? t.ids[blockIdx.x] : blockIdx.x;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], ly = l[1], lz = l[2];
+  const float val = t.traces[(long long)r * t.nt + it] * t.scaler;
+  const int ntap = lx * ly * lz;
+  for (int k = threadIdx.x; k < ntap; k += blockDim.x) {
+    const int iz = k % lz, ix = (k / lz) % lx, iy = k / (lz * lx);
+    const float cy = val * t.ky[(long long)r * t.ly + iy];
+    const float cx = cy * t.kx[(long long)r * t.lx + ix];
+    const long long c = ((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz;
+    atomicAdd(w0 + c, cx * t.kz[(long long)r * t.lz + iz] * vel[c]);
+  }
+}
+
+// Grouped injection: one CTA per xy tile; every cell of the tile sums the xy
+// weight of the group members whose kernel box covers it, then the tile's
+// columns receive that sum times the common z kernel.
+__global__ void inject_group_k(GroupDev g, TraceDev t, int it, float *__restrict__ w0, const float *__restrict__ vel,
+                               int nx, int ny, int nz) {
+  extern __shared__ float s_xy[];
+  const int T = g.tile;
+  const int tile = blockIdx.x;
+  const int x0 = g.tile_xy[2 * tile], y0 = g.tile_xy[2 * tile + 1];
+  const int b = g.tile_ptr[tile], e = g.tile_ptr[tile + 1];
+  for (int c = threadIdx.x; c < T * T; c += blockDim.x) {
+    const int ix = x0 + c % T, iy = y0 + c / T;
+    float acc = 0.f;
+    for (int k = b; k < e; k++) {
+      const int r = g.tile_list[k];
+      const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+      const int jx = ix - o[0], jy = iy - o[1];
+      if (jx < 0 || jx >= l[0] || jy < 0 || jy >= l[1]) continue;
+      const float val = t.traces[(long long)r * t.nt + it] * t.scaler;
+      acc += val * t.ky[(long long)r * t.ly + jy] * t.kx[(long long)r * t.lx + jx];
+    }
+    s_xy[c] = acc;
+  }
+  __syncthreads();
+  const int lz = g.lz;
+  for (int k = threadIdx.x; k < T * T * lz; k += blockDim.x) {
+    const int iz = k % lz, c = k / lz;
+    const int ix = x0 + c % T, iy = y0 + c / T;
+    const float s = s_xy[c];
+    if (ix >= nx || iy >= ny || s == 0.f) continue;
+    const long long i = ((long long)iy * nx + ix) * nz + g.offz + iz;
+    w0[i] += s * g.kz[iz] * vel[i];
+  }
+}
+
+// one warp per receiver over its kernel box
+__global__ void extract_direct_k(TraceDev t, const float *__restrict__ w0, float *__restrict__ out, int jt, int nt_out,
+                                 int nx, int nz) {
+  const int k0 = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (k0 >= (t.ids ? t.nids : t.ntr)) return;
+  const int r = t.ids ? t.ids[k0] : k0;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], ly = l[1], lz = l[2];
+  float acc = 0.f;
+  for (int k = lane; k < lx * ly * lz; k += 32) {
+    const int iz = k % lz, ix = (k / lz) % lx, iy = k / (lz * lx);
+    const float cx = t.ky[(long long)r * t.ly + iy] * t.kx[(long long)r * t.lx + ix];
+    acc += cx * t.kz[(long long)r * t.lz + iz] * w0[((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz];
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+  if (lane == 0) out[(long long)r * nt_out + jt] = acc;
+}
+
+// z reduction of a group's band on its tiles: plane[iy*nx+ix] = sum kz * w0
+__global__ void extract_zplane_k(GroupDev g, const float *__restrict__ w0, float *__restrict__ plane, int nx, int ny,
+                                 int nz) {
+  const int T = g.tile;
+  const int tile = blockIdx.x;
+  const int x0 = g.tile_xy[2 * tile], y0 = g.tile_xy[2 * tile + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+  for (int c = warp; c < T * T; c += nw) {
+    const int ix = x0 + c % T, iy = y0 + c / T;
+    if (ix >= nx || iy >= ny) continue;
+    const long long base = ((long long)iy * nx + ix) * nz + g.offz;
+    float acc = 0.f;
+    for (int iz = lane; iz < g.lz; iz += 32) acc += g.kz[iz] * w0[base + iz];
+#pragma unroll
+    for (int s = 16; s; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+    if (lane == 0) plane[(long long)iy * nx + ix] = acc;
+  }
+}
+
+__global__ void extract_xy_k(GroupDev g, TraceDev t, const float *__restrict__ plane, float *__restrict__ out, int jt,
+                             int nt_out, int nx) {
+  const int m = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (m >= g.ntr) return;
+  const int r = g.members[m];
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  float acc = 0.f;
+  for (int k = lane; k < l[0] * l[1]; k += 32) {
+    const int ix = k % l[0], iy = k / l[0];
+    acc += t.ky[(long long)r * t.ly + iy] * t.kx[(long long)r * t.lx + ix] *
+           plane[(long long)(iy + o[1]) * nx + ix + o[0]];
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+  if (lane == 0) out[(long long)r * nt_out + jt] = acc;
+}
+
+// per-slab max |w| (one CTA per y slab)
+__global__ void slab_max_k(const float *__restrict__ w, float *__restrict__ slab, uint16_t *c16, int fmt, long long nxz) {
+  const int iy = blockIdx.x;
+  const float *p = w + (long long)iy * nxz;
+  float m = 0.f;
+  for (long long i = threadIdx.x; i < nxz; i += blockDim.x) m = fmaxf(m, fabsf(p[i]));
+#pragma unroll
+  for (int s = 16; s; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
+  __shared__ float red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.f;
+#pragma unroll
+    for (int s = 16; s; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
+    if (threadIdx.x == 0) {
+      if (fmt == 1) {
+        const float hdr = m > 1e-25f ? m : 0.f;  // compress16 zeroes silent slabs
+        slab[iy] = hdr;
+        if (c16) {
+          const unsigned bits = __float_as_uint(hdr);
+          uint16_t *h = c16 + (long long)iy * (nxz + 2);
+          h[0] = (uint16_t)(bits & 0xffffu);
+          h[1] = (uint16_t)(bits >> 16);
+        }
+      } else {
+        slab[iy] = m * 6.103515625e-05f;  // fp16 slab scale: max maps to 2^14
+      }
+    }
+  }
+}
+
+__global__ void fused_io_k(FusedIo io, const float *__restrict__ u, int nx, int ny, int nz) {
+  const Grid3 g{nx, ny, nz, (long long)nx * nz};
+  const long long n = g.nxz * ny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(i / g.nxz);
+    const long long in = i - (long long)iy * g.nxz;
+    const int ix = (int)(in / nz), iz = (int)(in - (long long)ix * nz);
+    fused_io(io, g, i, ix, iy, iz, in, u[i]);
+  }
+}
+
+__global__ void snap_decode_k(SnapDev s, float *__restrict__ out, const float *ex, const float *ey, const float *ez,
+                              int nx, int ny, int nz) {
+  const Grid3 g{nx, ny, nz, (long long)nx * nz};
+  const long long n = g.nxz * ny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(i / g.nxz);
+    const long long in = i - (long long)iy * g.nxz;
+    float v = snap_read(s, g, i, iy, in);
+    if (ex) {
+      const int ix = (int)(in / nz), iz = (int)(in - (long long)ix * nz);
+      v = v * ey[iy];
+      v = v * ex[ix];
+      v = v * ez[iz];
+    }
+    out[i] = v;
+  }
+}
+
+__global__ void c16_encode_k(const float *__restrict__ in, uint16_t *__restrict__ out, const float *__restrict__ slab,
+                             int ny, long long nxz) {
+  const long long n = nxz * ny;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(i / nxz);
+    const long long in_ = i - (long long)iy * nxz;
+    const float vmax = slab[iy];
+    out[(long long)iy * (nxz + 2) + 2 + in_] = vmax > 1e-25f ? c16_encode(in[i] * __frcp_rn(vmax)) : (uint16_t)0;
+  }
+}
+
+__global__ void c16_slab_hdr_k(const uint16_t *__restrict__ c, float *__restrict__ slab, int ny, long long nxz) {
+  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iy >= ny) return;
+  const uint16_t *h = c + (long long)iy * (nxz + 2);
+  slab[iy] = __uint_as_float((unsigned)h[0] | ((unsigned)h[1] << 16));
+}
+
+__global__ void nonfinite_k(const float *__restrict__ w, long long n, int *flag) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (!isfinite(w[i])) {
+      *flag = 1;
+      return;
+    }
+}
+
+// Propagator::Vel2 (bgprtm/Propagator.cpp:711-742): v -> (v dt)^2, Q-corrected
+__global__ void vel2_k(float *__restrict__ vel, float *__restrict__ invq, long long n, float dt2, float cq0, int use_q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v = vel[i];
+    if (!use_q) {
+      vel[i] = (v * v) * dt2;
+    } else {
+      const float q = invq[i], q2 = q * q;
+      const float corr = 1.0f / (1.0f - cq0 * q);
+      vel[i] = v * v * dt2 * (1.0f - 0.25f * q2 + q2 * q2 / 48.0f) * corr;
+      invq[i] = q * corr;
+    }
+  }
+}
+
+int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  return (int)(b < 148LL * 16 ? b : 148LL * 16);
+}
+
+}  // namespace
+
+void launch_update2nd(float *w0, const float *w1, const QDev *q, long long n, cudaStream_t st) {
+  if (q) update2nd_q_k<<<grid_for(n, 256), 256, 0, st>>>(w0, w1, *q, n);
+  else update2nd_k<<<grid_for(n, 256), 256, 0, st>>>(w0, w1, n);
+}
+
+void launch_inject_scatter(const TraceDev &t, int it, float *w0, const float *vel, int nx, int ny, int nz,
+                           cudaStream_t st) {
+  (void)ny;
+  const int cnt = t.ids ? t.nids : t.ntr;
+  if (cnt <= 0 || it < 0 || it >= t.nt) return;
+  inject_scatter_k<<<cnt, 256, 0, st>>>(t, it, w0, vel, nx, nz);
+}
+
+void launch_inject_group(const GroupDev &gr, const TraceDev &t, int it, float *plane, float *w0, const float *vel,
+                         int nx, int ny, int nz, cudaStream_t st) {
+  (void)plane;
+  if (gr.ntiles <= 0 || it < 0 || it >= t.nt) return;
+  inject_group_k<<<gr.ntiles, 256, gr.tile * gr.tile * sizeof(float), st>>>(gr, t, it, w0, vel, nx, ny, nz);
+}
+
+void launch_extract_direct(const TraceDev &t, const float *w0, float *out, int jt, int nt_out, int nx, int ny, int nz,
+                           cudaStream_t st) {
+  (void)ny;
+  const int cnt = t.ids ? t.nids : t.ntr;
+  if (cnt <= 0 || jt < 0 || jt >= nt_out) return;
+  extract_direct_k<<<(cnt + 7) / 8, 256, 0, st>>>(t, w0, out, jt, nt_out, nx, nz);
+}
+
+void launch_extract_group(const GroupDev &gr, const TraceDev &t, const float *w0, float *plane, float *out, int jt,
+                          int nt_out, int nx, int ny, int nz, cudaStream_t st) {
+  if (gr.ntiles <= 0 || jt < 0 || jt >= nt_out) return;
+  extract_zplane_k<<<gr.ntiles, 256, 0, st>>>(gr, w0, plane, nx, ny, nz);
+  extract_xy_k<<<(gr.ntr + 7) / 8, 256, 0, st>>>(gr, t, plane, out, jt, nt_out, nx);
+}
+
+void launch_slab_max(const float *w, float *slab, uint16_t *c16_base, int fmt, int nx, int ny, int nz, cudaStream_t st) {
+  slab_max_k<<<ny, 1024, 0, st>>>(w, slab, c16_base, fmt, (long long)nx * nz);
+}
+
+void launch_fused_io(const FusedIo &io, const float *u, int nx, int ny, int nz, cudaStream_t st) {
+  long long n = (long long)nx * ny * nz;
+  fused_io_k<<<grid_for(n, 256), 256, 0, st>>>(io, u, nx, ny, nz);
+}
+
+void launch_snap_decode(const SnapDev &s, float *out, const float *ex, const float *ey, const float *ez, int nx, int ny,
+                        int nz, cudaStream_t st) {
+  long long n = (long long)nx * ny * nz;
+  snap_decode_k<<<grid_for(n, 256), 256, 0, st>>>(s, out, ex, ey, ez, nx, ny, nz);
+}
+
+void launch_c16_compress(const float *in, uint16_t *out, float *slab, int nx, int ny, int nz, cudaStream_t st) {
+  const long long nxz = (long long)nx * nz;
+  slab_max_k<<<ny, 1024, 0, st>>>(in, slab, out, 1, nxz);
+  c16_encode_k<<<grid_for(nxz * ny, 256), 256, 0, st>>>(in, out, slab, ny, nxz);
+}
+
+void launch_c16_uncompress(const uint16_t *in, float *out, float *slab, const float *ex, const float *ey,
+                           const float *ez, int nx, int ny, int nz, cudaStream_t st) {
+  // the header of each slab is its scale; then the generic decode path
+  const long long nxz = (long long)nx * nz;
+  c16_slab_hdr_k<<<(ny + 255) / 256, 256, 0, st>>>(in, slab, ny, nxz);
+  SnapDev s{1, (void *)in, slab};
+  launch_snap_decode(s, out, ex, ey, ez, nx, ny, nz, st);
+}
+
+void launch_vel2(float *vel, float *invq, long long n, float dt2, float cq0, int use_q, cudaStream_t st) {
+  vel2_k<<<grid_for(n, 256), 256, 0, st>>>(vel, invq, n, dt2, cq0, use_q);
+}
+
+void launch_nonfinite_scan(const float *w, long long n, int *flag, cudaStream_t st) {
+  nonfinite_k<<<grid_for(n, 256), 256, 0, st>>>(w, n, flag);
+}
+
+}  // namespace rtm

@@ -1,0 +1,991 @@
+// rtm_capi.cu - the engine behind include/rtm_b200.h: device state of one shot,
+// the time-loop drivers (Propagator::modelling / migration) captured as CUDA
+// graphs, and every extern "C" entry point.  No entry point throws or aborts;
+// CUDA failures become RTM_ERR_CUDA with the message kept on the handle.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/rtm_b200.h"
+#include "host_setup.h"
+#include "kernel_api.h"
+
+namespace rtm {
+
+static std::string g_create_error;
+
+struct TraceSetDev {
+  int ntr = 0, lx = 0, ly = 0, lz = 0, nt = 0;
+  float scaler = 1.f;
+  int *off = nullptr, *len = nullptr;
+  float *kx = nullptr, *ky = nullptr, *kz = nullptr, *traces = nullptr;
+  float *out = nullptr;  // extraction results [ntr][nt]
+  int *ungrouped = nullptr;
+  int n_ungrouped = 0;
+  std::vector<GroupDev> groups;
+  std::vector<void *> group_allocs;
+  TraceDev dev() const {
+    TraceDev t{};
+    t.ntr = ntr, t.lx = lx, t.ly = ly, t.lz = lz, t.nt = nt;
+    t.off = off, t.len = len, t.kx = kx, t.ky = ky, t.kz = kz, t.traces = traces, t.scaler = scaler;
+    return t;
+  }
+};
+
+struct Engine {
+  rtm_dims d{};
+  rtm_config c{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  long long n = 0, nxz = 0;
+  std::string err;
+  std::vector<void *> allocs;
+  // state
+  float *w0 = nullptr, *w1 = nullptr, *vel = nullptr;
+  float *eps = nullptr, *del = nullptr, *pjx = nullptr, *pjy = nullptr, *invq = nullptr;
+  float *wq[2] = {nullptr, nullptr};
+  int iq0 = 0;
+  float *px = nullptr, *py = nullptr, *pz = nullptr;  // gradient scratch (anisotropic / CFD)
+  float *scr = nullptr, *scr2 = nullptr;              // CFD raw-derivative scratch
+  float c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
+  CfdPlanDev cfd[3][2] = {};
+  PmlDev pml{};
+  int model_set = 0;
+  // Q
+  float cq0 = 0.f, cqsum = 0.f, cq[8] = {}, cwq[8] = {};
+  int q_set = 0;
+  // traces
+  TraceSetDev inj, ext;
+  float *plane = nullptr;
+  // snapshots
+  int snap_fmt = 0, nslots = 0;
+  size_t slot_bytes = 0;
+  char *snaps = nullptr;
+  float *slabs = nullptr;  // [nslots][ny]
+  std::vector<char> stored;
+  // imaging
+  float *image = nullptr, *comp = nullptr;
+  float *ex = nullptr, *ey = nullptr, *ez = nullptr, *one_x = nullptr, *one_y = nullptr, *one_z = nullptr;
+  float *taper_z = nullptr;
+  std::vector<float> taper_t;
+  int ic_edge = 1;
+  // launch shape and timing
+  int tx = 8, yseg = 16;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  int *dflag = nullptr;
+
+  template <typename T> int alloc(T *&p, size_t count) {
+    void *v = nullptr;
+    cudaError_t e = cudaMalloc(&v, count * sizeof(T));
+    if (e != cudaSuccess) {
+      err = std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) + " bytes): " + cudaGetErrorString(e);
+      cudaGetLastError();
+      return RTM_ERR_NOMEM;
+    }
+    allocs.push_back(v);
+    p = (T *)v;
+    return RTM_OK;
+  }
+  void release(void *p) {
+    if (!p) return;
+    auto it = std::find(allocs.begin(), allocs.end(), p);
+    if (it != allocs.end()) allocs.erase(it);
+    cudaFree(p);
+  }
+};
+
+int cuda_fail(cudaError_t e, const char *what, Engine *h) {
+  if (h) h->err = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return e == cudaErrorMemoryAllocation ? RTM_ERR_NOMEM : RTM_ERR_CUDA;
+}
+
+#define CK(call) RTM_CUDA_OK(call)
+#define TRY(expr)                 \
+  do {                            \
+    int r__ = (expr);             \
+    if (r__ != RTM_OK) return r__; \
+  } while (0)
+
+static int check_launch(Engine *h, const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what, h);
+  return RTM_OK;
+}
+
+// launch shape: 32 x tx column tiles, y split so the grid covers the 148 SMs
+static void choose_shape(Engine *h) {
+  const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
+  int tx = nx >= 256 ? 8 : 8;
+  long long bxz = (long long)((nz + 31) / 32) * ((nx + tx - 1) / tx);
+  long long want = 148LL * 8;
+  int nseg = (int)std::max(1LL, std::min<long long>((want + bxz - 1) / bxz, std::max(1, ny / 16)));
+  h->tx = tx;
+  h->yseg = (ny + nseg - 1) / nseg;
+}
+
+static PmlDev pml_dev(Engine *h) { return h->pml; }
+
+static int setup_pml(Engine *h) {
+  const rtm_config &c = h->c;
+  const int nn[3] = {h->d.nx, h->d.ny, h->d.nz};
+  const double dd[3] = {h->d.dx, h->d.dy, h->d.dz};
+  const bool second = c.engine == RTM_ENGINE_FD8 && c.model_type == RTM_ISO;
+  const int ncomp = (!c.pml3d || second) ? 1 : 3;
+  for (int dim = 0; dim < 3; dim++)
+    for (int s = 0; s < 2; s++) {
+      PmlFace &F = h->pml.f[dim][s];
+      F = PmlFace{};
+      int w = c.nbnd[2 * dim + s];
+      bool on = w > 1 && !(dim == DZ && s == SIDE_LO && !c.top_pml);
+      if (!on) continue;
+      if (w * 2 > nn[dim] && !(nn[dim] == 1)) {
+        h->err = "PML wider than half the grid";
+        return RTM_ERR_ARG;
+      }
+      std::vector<float> co;
+      pml_profile(w, dd[dim], h->d.dt, c.vmax, c.pml_eps, c.pml3d_scaler, co);
+      float *dco;
+      TRY(h->alloc(dco, co.size()));
+      CK(cudaMemcpy(dco, co.data(), co.size() * 4, cudaMemcpyHostToDevice));
+      F.w = w;
+      F.co = dco;
+      long long plane = dim == DX ? (long long)h->d.ny * h->d.nz
+                                  : dim == DY ? (long long)h->d.nx * h->d.nz : (long long)h->d.nx * h->d.ny;
+      for (int r = 0; r < 2; r++)
+        for (int k = 0; k < ncomp; k++) TRY(h->alloc(F.q[r][k], (size_t)plane * w));
+    }
+  return RTM_OK;
+}
+
+static int zero_state(Engine *h) {
+  CK(cudaMemsetAsync(h->w0, 0, h->n * 4, h->st));
+  CK(cudaMemsetAsync(h->w1, 0, h->n * 4, h->st));
+  for (int dim = 0; dim < 3; dim++)
+    for (int s = 0; s < 2; s++) {
+      PmlFace &F = h->pml.f[dim][s];
+      if (!F.w) continue;
+      long long plane = dim == DX ? (long long)h->d.ny * h->d.nz
+                                  : dim == DY ? (long long)h->d.nx * h->d.nz : (long long)h->d.nx * h->d.ny;
+      for (int r = 0; r < 2; r++)
+        for (int k = 0; k < 3; k++)
+          if (F.q[r][k]) CK(cudaMemsetAsync(F.q[r][k], 0, plane * F.w * 4, h->st));
+    }
+  if (h->c.use_q && h->wq[0]) {
+    CK(cudaMemsetAsync(h->wq[0], 0, (size_t)h->c.q_order * h->n * 4, h->st));
+    CK(cudaMemsetAsync(h->wq[1], 0, (size_t)h->c.q_order * h->n * 4, h->st));
+  }
+  if (h->ext.out) CK(cudaMemsetAsync(h->ext.out, 0, (size_t)h->ext.ntr * h->ext.nt * 4, h->st));
+  h->iq0 = 0;
+  return RTM_OK;
+}
+
+static QDev q_dev(Engine *h) {
+  QDev q{};
+  q.order = h->c.q_order;
+  q.cqsum = h->cqsum;
+  for (int l = 0; l < q.order && l < 8; l++) q.cq[l] = h->cq[l], q.wq[l] = h->cwq[l];
+  q.invq = h->invq;
+  q.d0 = h->wq[h->iq0];
+  q.d1 = h->wq[1 - h->iq0];
+  return q;
+}
+
+// One application of the spatial operator, optionally fused with update2nd
+// (mode 1 leapfrog, 2 Q) and with the snapshot / imaging access of the
+// previous step's wavefield (io).
+static int step_kernel(Engine *h, int mode, const FusedIo &io) {
+  const rtm_dims &d = h->d;
+  QDev q = q_dev(h);
+  if (h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO) {
+    IsoArgs a{};
+    a.nx = d.nx, a.ny = d.ny, a.nz = d.nz, a.yseg = h->yseg;
+    a.w1 = h->w1, a.w0 = h->w0, a.vel = h->vel;
+    memcpy(a.c2x, h->c2x, sizeof a.c2x), memcpy(a.c2y, h->c2y, sizeof a.c2y), memcpy(a.c2z, h->c2z, sizeof a.c2z);
+    a.pml = pml_dev(h);
+    a.io = io;
+    a.q = q;
+    launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
+    return check_launch(h, "iso_fd8_step");
+  }
+  if (h->c.engine == RTM_ENGINE_FD8) {
+    GradArgs g{};
+    g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = h->yseg, g.pml3d = h->c.pml3d;
+    g.w1 = h->w1, g.px = h->px, g.py = h->py, g.pz = h->pz;
+    g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy;
+    memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
+    g.pml = pml_dev(h);
+    g.io = io;
+    launch_grad_fd8(g, h->c.model_type, h->tx, h->st);
+    TRY(check_launch(h, "grad_fd8"));
+    DivArgs v{};
+    v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = h->yseg, v.pml3d = h->c.pml3d;
+    v.px = h->px, v.py = h->py, v.pz = h->pz, v.w1 = h->w1, v.w0 = h->w0, v.vel = h->vel;
+    memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
+    v.pml = pml_dev(h);
+    v.q = q;
+    launch_div_fd8(v, mode, h->tx, h->st);
+    return check_launch(h, "div_fd8");
+  }
+  // compact FD: raw line-solve derivatives, then pointwise PML / scaling /
+  // accumulation epilogues (FdEngine_cfd + KernelCPU::TTI structure)
+  if (io.store || io.ic) {
+    launch_fused_io(io, h->w1, d.nx, d.ny, d.nz, h->st);
+    TRY(check_launch(h, "fused_io"));
+  }
+  launch_cfd_deriv(DZ, h->cfd[DZ][0], h->w1, h->pz, h->scr, d.nx, d.ny, d.nz, h->st);
+  launch_cfd_deriv(DX, h->cfd[DX][0], h->w1, h->px, h->scr, d.nx, d.ny, d.nz, h->st);
+  if (d.ny > 1) launch_cfd_deriv(DY, h->cfd[DY][0], h->w1, h->py, h->scr, d.nx, d.ny, d.nz, h->st);
+  TRY(check_launch(h, "cfd_deriv(grad)"));
+  CfdGradEpiArgs ge{};
+  ge.nx = d.nx, ge.ny = d.ny, ge.nz = d.nz, ge.pml3d = h->c.pml3d, ge.model = h->c.model_type;
+  ge.gx = h->px, ge.gy = h->py, ge.gz = h->pz;
+  ge.eps = h->eps, ge.del = h->del, ge.pjx = h->pjx, ge.pjy = h->pjy;
+  ge.pml = pml_dev(h);
+  launch_cfd_grad_epilogue(ge, h->st);
+  TRY(check_launch(h, "cfd_grad_epilogue"));
+  // divergence parts: d/dx px -> scr, d/dz pz -> scr2, d/dy py -> px (px is free now)
+  launch_cfd_deriv(DX, h->cfd[DX][1], h->px, h->scr2, h->scr, d.nx, d.ny, d.nz, h->st);
+  float *dzp = h->scr;
+  launch_cfd_deriv(DZ, h->cfd[DZ][1], h->pz, dzp, nullptr, d.nx, d.ny, d.nz, h->st);
+  float *dyp = nullptr;
+  if (d.ny > 1) {
+    launch_cfd_deriv(DY, h->cfd[DY][1], h->py, h->px, h->pz, d.nx, d.ny, d.nz, h->st);
+    dyp = h->px;
+  }
+  TRY(check_launch(h, "cfd_deriv(div)"));
+  CfdDivEpiArgs de{};
+  de.nx = d.nx, de.ny = d.ny, de.nz = d.nz, de.pml3d = h->c.pml3d, de.mode = mode;
+  de.dx = h->scr2, de.dz = dzp, de.dy = dyp;
+  de.w1 = h->w1, de.w0 = h->w0, de.vel = h->vel;
+  de.pml = pml_dev(h);
+  de.q = q;
+  launch_cfd_div_epilogue(de, h->st);
+  return check_launch(h, "cfd_div_epilogue");
+}
+
+static int do_inject(Engine *h, int it) {
+  TraceSetDev &t = h->inj;
+  if (!t.ntr || it < 0 || it >= t.nt) return RTM_OK;
+  TraceDev td = t.dev();
+  for (const GroupDev &g : t.groups)
+    launch_inject_group(g, td, it, h->plane, h->w0, h->vel, h->d.nx, h->d.ny, h->d.nz, h->st);
+  if (t.n_ungrouped) {
+    td.ids = t.ungrouped, td.nids = t.n_ungrouped;
+    launch_inject_scatter(td, it, h->w0, h->vel, h->d.nx, h->d.ny, h->d.nz, h->st);
+  }
+  return check_launch(h, "inject");
+}
+
+static int do_extract(Engine *h, int jt) {
+  TraceSetDev &t = h->ext;
+  if (!t.ntr || jt < 0 || jt >= t.nt) return RTM_OK;
+  TraceDev td = t.dev();
+  for (const GroupDev &g : t.groups)
+    launch_extract_group(g, td, h->w0, h->plane, t.out, jt, t.nt, h->d.nx, h->d.ny, h->d.nz, h->st);
+  if (t.n_ungrouped) {
+    td.ids = t.ungrouped, td.nids = t.n_ungrouped;
+    launch_extract_direct(td, h->w0, t.out, jt, t.nt, h->d.nx, h->d.ny, h->d.nz, h->st);
+  }
+  return check_launch(h, "extract");
+}
+
+static void do_swap(Engine *h) {
+  std::swap(h->w0, h->w1);
+  h->iq0 = 1 - h->iq0;
+}
+
+static SnapDev slot_dev(Engine *h, int slot) {
+  SnapDev s{};
+  s.fmt = h->snap_fmt;
+  s.base = h->snaps + (size_t)slot * h->slot_bytes;
+  s.slab = h->slabs ? h->slabs + (size_t)slot * h->d.ny : nullptr;
+  return s;
+}
+
+static FusedIo io_none() { return FusedIo{}; }
+
+static FusedIo io_store(Engine *h, int slot) {
+  FusedIo io{};
+  io.store = 1;
+  io.st = slot_dev(h, slot);
+  return io;
+}
+
+static FusedIo io_image(Engine *h, int slot) {
+  FusedIo io{};
+  io.ic = 1;
+  io.src = slot_dev(h, slot);
+  io.image = h->image, io.comp = h->comp;
+  io.use_t = slot < (int)h->taper_t.size();
+  io.tscale = io.use_t ? h->taper_t[slot] : 1.f;
+  io.taper_z = h->taper_z;
+  io.ex = h->ic_edge ? h->ex : h->one_x;
+  io.ey = h->ic_edge ? h->ey : h->one_y;
+  io.ez = h->ic_edge ? h->ez : h->one_z;
+  return io;
+}
+
+// per-slot slab statistics for the 16-bit formats, taken on w0 after injection
+static int snap_prepare(Engine *h, int slot) {
+  if (h->snap_fmt == RTM_SNAP_FP32) return RTM_OK;
+  SnapDev s = slot_dev(h, slot);
+  launch_slab_max(h->w0, (float *)s.slab, h->snap_fmt == RTM_SNAP_C16 ? (uint16_t *)s.base : nullptr, h->snap_fmt,
+                  h->d.nx, h->d.ny, h->d.nz, h->st);
+  return check_launch(h, "slab_max");
+}
+
+// Runs fn(step index) for `count` steps inside CUDA graphs of up to `chunk`
+// steps each, timed with events on the engine's stream.
+template <typename F> static int run_graphs(Engine *h, int count, F fn) {
+  const int chunk = 256;
+  CK(cudaEventRecord(h->ev0, h->st));
+  for (int s0 = 0; s0 < count; s0 += chunk) {
+    const int s1 = std::min(count, s0 + chunk);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int rc = RTM_OK;
+    for (int s = s0; s < s1 && rc == RTM_OK; s++) rc = fn(s);
+    cudaError_t ec = cudaStreamEndCapture(h->st, &g);
+    if (rc != RTM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture", h);
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate", h);
+    cudaError_t el = cudaGraphLaunch(ge, h->st);
+    cudaGraphExecDestroy(ge);
+    if (el != cudaSuccess) return cuda_fail(el, "cudaGraphLaunch", h);
+  }
+  CK(cudaEventRecord(h->ev1, h->st));
+  CK(cudaEventSynchronize(h->ev1));
+  CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  return RTM_OK;
+}
+
+static int ready(Engine *h) {
+  if (!h) return RTM_ERR_ARG;
+  if (!h->model_set) {
+    h->err = "rtm_set_model has not been called";
+    return RTM_ERR_STATE;
+  }
+  cudaSetDevice(h->device);
+  return RTM_OK;
+}
+
+// Host staging of the traces of a TraceSet and its grouping by z kernel.
+static int upload_traces(Engine *h, TraceSetDev &t, int ntr, int lx, int ly, int lz, const int *off3, const int *len3,
+                         const float *kx, const float *ky, const float *kz, const float *traces, int nt, float scaler,
+                         bool extraction) {
+  for (void *p : {(void *)t.off, (void *)t.len, (void *)t.kx, (void *)t.ky, (void *)t.kz, (void *)t.traces,
+                  (void *)t.out, (void *)t.ungrouped})
+    h->release(p);
+  for (void *p : t.group_allocs) h->release(p);
+  t = TraceSetDev{};
+  if (ntr <= 0) return RTM_OK;
+  // validate every kernel box against the grid
+  for (int r = 0; r < ntr; r++) {
+    const int *o = off3 + 3 * r, *l = len3 + 3 * r;
+    const int nn[3] = {h->d.nx, h->d.ny, h->d.nz}, cap[3] = {lx, ly, lz};
+    for (int a = 0; a < 3; a++)
+      if (l[a] < 0 || l[a] > cap[a] || o[a] < 0 || o[a] + l[a] > nn[a]) {
+        h->err = "trace " + std::to_string(r) + " kernel box outside the grid or its stride";
+        return RTM_ERR_ARG;
+      }
+  }
+  t.ntr = ntr, t.lx = lx, t.ly = ly, t.lz = lz, t.nt = nt, t.scaler = scaler;
+  TRY(h->alloc(t.off, 3 * (size_t)ntr));
+  TRY(h->alloc(t.len, 3 * (size_t)ntr));
+  TRY(h->alloc(t.kx, (size_t)ntr * lx));
+  TRY(h->alloc(t.ky, (size_t)ntr * ly));
+  TRY(h->alloc(t.kz, (size_t)ntr * lz));
+  CK(cudaMemcpy(t.off, off3, 12 * (size_t)ntr, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(t.len, len3, 12 * (size_t)ntr, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(t.kx, kx, 4 * (size_t)ntr * lx, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(t.ky, ky, 4 * (size_t)ntr * ly, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(t.kz, kz, 4 * (size_t)ntr * lz, cudaMemcpyHostToDevice));
+  if (!extraction) {
+    TRY(h->alloc(t.traces, (size_t)ntr * nt));
+    CK(cudaMemcpy(t.traces, traces, 4 * (size_t)ntr * nt, cudaMemcpyHostToDevice));
+  } else {
+    TRY(h->alloc(t.out, (size_t)ntr * nt));
+    CK(cudaMemset(t.out, 0, 4 * (size_t)ntr * nt));
+  }
+  // group traces whose z kernels are identical (first index, length, values)
+  std::map<std::vector<uint32_t>, std::vector<int>> by_z;
+  for (int r = 0; r < ntr; r++) {
+    std::vector<uint32_t> key;
+    key.push_back((uint32_t)off3[3 * r + 2]);
+    key.push_back((uint32_t)len3[3 * r + 2]);
+    for (int k = 0; k < len3[3 * r + 2]; k++) {
+      uint32_t b;
+      memcpy(&b, kz + (size_t)r * lz + k, 4);
+      key.push_back(b);
+    }
+    by_z[key].push_back(r);
+  }
+  std::vector<int> loose;
+  const int T = 16;
+  for (auto &kv : by_z) {
+    const std::vector<int> &mem = kv.second;
+    if (mem.size() < 16) {
+      loose.insert(loose.end(), mem.begin(), mem.end());
+      continue;
+    }
+    const int r0 = mem[0];
+    GroupDev g{};
+    g.ntr = (int)mem.size();
+    g.offz = off3[3 * r0 + 2];
+    g.lz = len3[3 * r0 + 2];
+    g.tile = T;
+    const int ntx = (h->d.nx + T - 1) / T, nty = (h->d.ny + T - 1) / T;
+    std::vector<std::vector<int>> lists((size_t)ntx * nty);
+    for (int r : mem) {
+      const int *o = off3 + 3 * r, *l = len3 + 3 * r;
+      if (!l[0] || !l[1]) continue;
+      for (int ty = o[1] / T; ty <= (o[1] + l[1] - 1) / T; ty++)
+        for (int tx = o[0] / T; tx <= (o[0] + l[0] - 1) / T; tx++) lists[(size_t)ty * ntx + tx].push_back(r);
+    }
+    std::vector<int> txy, ptr{0}, lst;
+    for (int ty = 0; ty < nty; ty++)
+      for (int tx = 0; tx < ntx; tx++) {
+        auto &L = lists[(size_t)ty * ntx + tx];
+        if (L.empty()) continue;
+        txy.push_back(tx * T), txy.push_back(ty * T);
+        lst.insert(lst.end(), L.begin(), L.end());
+        ptr.push_back((int)lst.size());
+      }
+    g.ntiles = (int)txy.size() / 2;
+    int *dm, *dxy, *dp, *dl;
+    float *dkz;
+    TRY(h->alloc(dm, mem.size()));
+    TRY(h->alloc(dkz, std::max(1, g.lz)));
+    TRY(h->alloc(dxy, std::max<size_t>(2, txy.size())));
+    TRY(h->alloc(dp, ptr.size()));
+    TRY(h->alloc(dl, std::max<size_t>(1, lst.size())));
+    t.group_allocs.insert(t.group_allocs.end(), {dm, dkz, dxy, dp, dl});
+    CK(cudaMemcpy(dm, mem.data(), 4 * mem.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dkz, kz + (size_t)r0 * lz, 4 * g.lz, cudaMemcpyHostToDevice));
+    if (!txy.empty()) CK(cudaMemcpy(dxy, txy.data(), 4 * txy.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dp, ptr.data(), 4 * ptr.size(), cudaMemcpyHostToDevice));
+    if (!lst.empty()) CK(cudaMemcpy(dl, lst.data(), 4 * lst.size(), cudaMemcpyHostToDevice));
+    g.members = dm, g.kz = dkz, g.tile_xy = dxy, g.tile_ptr = dp, g.tile_list = dl;
+    t.groups.push_back(g);
+  }
+  if (!loose.empty()) {
+    TRY(h->alloc(t.ungrouped, loose.size()));
+    CK(cudaMemcpy(t.ungrouped, loose.data(), 4 * loose.size(), cudaMemcpyHostToDevice));
+    t.n_ungrouped = (int)loose.size();
+  }
+  if (!t.groups.empty() && !h->plane) TRY(h->alloc(h->plane, (size_t)h->d.nx * h->d.ny));
+  return RTM_OK;
+}
+
+static void edge_taper(int n, int nt, std::vector<float> &w) {
+  // decode tapers of bgprtm/WaveFieldCompress.cpp:88-98 and 189-200
+  w.assign(n, 1.0f);
+  if (n <= 2 * nt) return;
+  for (int i = 0; i < nt; i++) {
+    float v = 0.5f * (1.0f - cosf((float)M_PI * float(i) / float(nt)));
+    w[i] = v;
+    w[n - 1 - i] = v;
+  }
+}
+
+}  // namespace rtm
+
+using rtm::Engine;
+
+struct rtm_handle : Engine {};
+
+extern "C" {
+
+void rtm_config_default(rtm_config *c) {
+  if (!c) return;
+  memset(c, 0, sizeof *c);
+  c->engine = RTM_ENGINE_FD8;
+  c->model_type = RTM_ISO;
+  c->q_order = 4;
+  c->vmax = 4500.f;
+  c->pml_eps = 1e-3f;
+  c->pml3d = 1;
+  c->pml3d_scaler = 0.3f;
+  c->top_pml = 1;
+}
+
+const char *rtm_last_error(const rtm_handle *h) { return h ? h->err.c_str() : rtm::g_create_error.c_str(); }
+
+int rtm_destroy(rtm_handle *h) {
+  if (!h) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->st);
+  for (void *p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return RTM_OK;
+}
+
+int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
+  using namespace rtm;
+  if (!d || !c || !out) return RTM_ERR_ARG;
+  *out = nullptr;
+  if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
+      c->engine < 0 || c->engine > 1 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
+      c->pml_eps <= 0 || c->pml_eps >= 1) {
+    g_create_error = "rtm_create: dimensions or configuration out of range";
+    return RTM_ERR_ARG;
+  }
+  if (c->state_fp16) {
+    g_create_error = "rtm_create: FP16 wavefield state is not built";
+    return RTM_ERR_UNSUPPORTED;
+  }
+  rtm_handle *h = new rtm_handle();
+  h->d = *d;
+  h->c = *c;
+  h->n = (long long)d->nx * d->ny * d->nz;
+  h->nxz = (long long)d->nx * d->nz;
+  int rc = RTM_OK;
+  auto fail = [&](int code) {
+    g_create_error = "rtm_create: " + h->err;
+    rtm_destroy(h);
+    return code;
+  };
+  if (cudaGetDevice(&h->device) != cudaSuccess) {
+    h->err = "no CUDA device";
+    cudaGetLastError();
+    return fail(RTM_ERR_CUDA);
+  }
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    h->err = "stream/event creation failed";
+    cudaGetLastError();
+    return fail(RTM_ERR_CUDA);
+  }
+  if ((rc = h->alloc(h->w0, h->n)) || (rc = h->alloc(h->w1, h->n)) || (rc = h->alloc(h->vel, h->n)) ||
+      (rc = h->alloc(h->dflag, 1)))
+    return fail(rc);
+  const bool first_deriv = !(c->engine == RTM_ENGINE_FD8 && c->model_type == RTM_ISO);
+  if (first_deriv) {
+    if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
+      return fail(rc);
+  }
+  if (c->engine == RTM_ENGINE_CFD) {
+    if (cfd_init() != 0) {
+      h->err = "compact-FD kernel set-up failed";
+      cudaGetLastError();
+      return fail(RTM_ERR_CUDA);
+    }
+    if ((rc = h->alloc(h->scr, h->n)) || (rc = h->alloc(h->scr2, h->n))) return fail(rc);
+    const int nn[3] = {d->nx, d->ny, d->nz};
+    const float dd[3] = {d->dx, d->dy, d->dz};
+    for (int a = 0; a < 3; a++) {
+      if (nn[a] < 16) {
+        if (a == DY && nn[a] == 1) continue;
+        h->err = "compact FD needs at least 16 cells per axis";
+        return fail(RTM_ERR_ARG);
+      }
+      for (int s = 0; s < 2; s++) {
+        std::vector<float> bm, bl, am;
+        cfd_plan(nn[a], dd[a], s + 1, bm, bl, am);
+        float *dbm, *dbl, *dam;
+        if ((rc = h->alloc(dbm, bm.size())) || (rc = h->alloc(dbl, bl.size())) || (rc = h->alloc(dam, am.size())))
+          return fail(rc);
+        cudaMemcpy(dbm, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dbl, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dam, am.data(), am.size() * 4, cudaMemcpyHostToDevice);
+        h->cfd[a][s] = CfdPlanDev{nn[a], dbm, dbl, dam};
+      }
+    }
+  }
+  if (c->model_type >= RTM_VTI) {
+    if ((rc = h->alloc(h->eps, h->n)) || (rc = h->alloc(h->del, h->n))) return fail(rc);
+  }
+  if (c->model_type == RTM_TTI) {
+    if ((rc = h->alloc(h->pjx, h->n)) || (d->ny > 1 && (rc = h->alloc(h->pjy, h->n)))) return fail(rc);
+  }
+  if (c->use_q) {
+    if ((rc = h->alloc(h->invq, h->n)) || (rc = h->alloc(h->wq[0], (size_t)c->q_order * h->n)) ||
+        (rc = h->alloc(h->wq[1], (size_t)c->q_order * h->n)))
+      return fail(rc);
+  }
+  // FD tables (FdEngine_fd constructor + setJacob, rectangular grid, const order)
+  double t1[5], t2[5];
+  fd_weights(4, t1, t2);
+  const float zpi = 1.0f / d->dz, zpi2 = zpi * zpi;
+  const float dx2i = (float)(1.0 / (double)(d->dx * d->dx)), dy2i = (float)(1.0 / (double)(d->dy * d->dy));
+  const float dxi = 1.0f / d->dx, dyi = 1.0f / d->dy;
+  for (int m = 0; m < 5; m++) {
+    const float c2 = (float)t2[m], c1 = m ? (float)t1[m] : 0.f;
+    h->c2z[m] = zpi2 * c2, h->c2x[m] = c2 * dx2i, h->c2y[m] = c2 * dy2i;
+    h->c1z[m] = zpi * c1, h->c1x[m] = c1 * dxi, h->c1y[m] = c1 * dyi;
+  }
+  if ((rc = setup_pml(h))) return fail(rc);
+  // imaging-condition tapers (edge tapers of the decode, depth taper default off)
+  std::vector<float> tx, ty, tz, one;
+  edge_taper(d->nx, 20, tx), edge_taper(d->ny, 20, ty), edge_taper(d->nz, 10, tz);
+  if ((rc = h->alloc(h->ex, d->nx)) || (rc = h->alloc(h->ey, d->ny)) || (rc = h->alloc(h->ez, d->nz)) ||
+      (rc = h->alloc(h->one_x, d->nx)) || (rc = h->alloc(h->one_y, d->ny)) || (rc = h->alloc(h->one_z, d->nz)) ||
+      (rc = h->alloc(h->taper_z, d->nz)))
+    return fail(rc);
+  cudaMemcpy(h->ex, tx.data(), 4 * d->nx, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->ey, ty.data(), 4 * d->ny, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->ez, tz.data(), 4 * d->nz, cudaMemcpyHostToDevice);
+  one.assign(std::max(std::max(d->nx, d->ny), d->nz), 1.0f);
+  cudaMemcpy(h->one_x, one.data(), 4 * d->nx, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->one_y, one.data(), 4 * d->ny, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->one_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
+  choose_shape(h);
+  if ((rc = zero_state(h))) return fail(rc);
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h->err = "initialisation failed";
+    cudaGetLastError();
+    return fail(RTM_ERR_CUDA);
+  }
+  *out = h;
+  return RTM_OK;
+}
+
+int rtm_set_q_coeffs(rtm_handle *h, float cq0, const float *cq, const float *wq) {
+  if (!h || !cq || !wq) return RTM_ERR_ARG;
+  if (!h->c.use_q) {
+    h->err = "use_q is off";
+    return RTM_ERR_STATE;
+  }
+  h->cq0 = cq0;
+  h->cqsum = 0.f;
+  for (int l = 0; l < h->c.q_order; l++) h->cq[l] = cq[l], h->cwq[l] = wq[l], h->cqsum += cq[l];
+  h->q_set = 1;
+  return RTM_OK;
+}
+
+int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float *del, const float *pjx,
+                  const float *pjy, const float *invq) {
+  using namespace rtm;
+  if (!h || !vel) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  const int mt = h->c.model_type;
+  if ((mt >= RTM_VTI && (!eps || !del)) || (mt == RTM_TTI && (!pjx || (h->d.ny > 1 && !pjy))) ||
+      (h->c.use_q && !invq)) {
+    h->err = "model arrays required by the model type are missing";
+    return RTM_ERR_ARG;
+  }
+  if (h->c.use_q && !h->q_set) {
+    h->err = "rtm_set_q_coeffs must precede rtm_set_model when use_q";
+    return RTM_ERR_STATE;
+  }
+  for (long long i = 0; i < h->n; i++)
+    if (!std::isfinite(vel[i]) || vel[i] <= 0.f) {
+      h->err = "velocity not finite or not positive at cell " + std::to_string(i);
+      return RTM_ERR_NONFINITE;
+    }
+  const size_t bytes = (size_t)h->n * 4;
+  CK(cudaMemcpyAsync(h->vel, vel, bytes, cudaMemcpyHostToDevice, h->st));
+  if (mt >= RTM_VTI) {
+    CK(cudaMemcpyAsync(h->eps, eps, bytes, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->del, del, bytes, cudaMemcpyHostToDevice, h->st));
+  }
+  if (mt == RTM_TTI) {
+    CK(cudaMemcpyAsync(h->pjx, pjx, bytes, cudaMemcpyHostToDevice, h->st));
+    if (h->d.ny > 1) CK(cudaMemcpyAsync(h->pjy, pjy, bytes, cudaMemcpyHostToDevice, h->st));
+  }
+  if (h->c.use_q) CK(cudaMemcpyAsync(h->invq, invq, bytes, cudaMemcpyHostToDevice, h->st));
+  launch_vel2(h->vel, h->invq, h->n, h->d.dt * h->d.dt, h->cq0, h->c.use_q, h->st);
+  TRY(check_launch(h, "vel2"));
+  CK(cudaStreamSynchronize(h->st));
+  h->model_set = 1;
+  return RTM_OK;
+}
+
+int rtm_reset(rtm_handle *h) {
+  if (!h) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  TRY(rtm::zero_state(h));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_kernel(rtm_handle *h) {
+  TRY(rtm::ready(h));
+  TRY(rtm::step_kernel(h, 0, rtm::io_none()));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_update2nd(rtm_handle *h) {
+  TRY(rtm::ready(h));
+  rtm::QDev q = rtm::q_dev(h);
+  rtm::launch_update2nd(h->w0, h->w1, h->c.use_q ? &q : nullptr, h->n, h->st);
+  TRY(rtm::check_launch(h, "update2nd"));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_swap(rtm_handle *h) {
+  if (!h) return RTM_ERR_ARG;
+  rtm::do_swap(h);
+  return RTM_OK;
+}
+
+int rtm_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper, float *coeff, int *off) {
+  if (!nlimit || !coeff || !off || n < 1 || !(k1 > 0.f) || k1 > k2 || k2 > 0.5f || !std::isfinite(x)) return RTM_ERR_ARG;
+  if (n > 1 && (x < 0.f || x > (float)(n - 1))) return RTM_ERR_ARG;
+  *off = rtm::spread_coeffs(n, x, k1, k2, nlimit, dipole, ntaper, coeff);
+  return RTM_OK;
+}
+
+int rtm_set_injection(rtm_handle *h, int ntr, int lx, int ly, int lz, const int *off3, const int *len3, const float *kx,
+                      const float *ky, const float *kz, const float *traces, int nt, float scaler) {
+  if (!h || ntr < 0 || (ntr > 0 && (!off3 || !len3 || !kx || !ky || !kz || !traces || nt <= 0 || lx < 1 || ly < 1 ||
+                                   lz < 1)))
+    return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  return rtm::upload_traces(h, h->inj, ntr, lx, ly, lz, off3, len3, kx, ky, kz, traces, nt, scaler, false);
+}
+
+int rtm_set_extraction(rtm_handle *h, int ntr, int lx, int ly, int lz, const int *off3, const int *len3, const float *kx,
+                       const float *ky, const float *kz, int nt_out) {
+  if (!h || ntr < 0 ||
+      (ntr > 0 && (!off3 || !len3 || !kx || !ky || !kz || nt_out <= 0 || lx < 1 || ly < 1 || lz < 1)))
+    return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  return rtm::upload_traces(h, h->ext, ntr, lx, ly, lz, off3, len3, kx, ky, kz, nullptr, nt_out, 1.f, true);
+}
+
+int rtm_inject(rtm_handle *h, int it) {
+  TRY(rtm::ready(h));
+  TRY(rtm::do_inject(h, it));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_extract(rtm_handle *h, int jt) {
+  TRY(rtm::ready(h));
+  TRY(rtm::do_extract(h, jt));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_get_traces(rtm_handle *h, float *dst) {
+  if (!h || !dst) return RTM_ERR_ARG;
+  if (!h->ext.out) {
+    h->err = "no extraction set";
+    return RTM_ERR_STATE;
+  }
+  cudaSetDevice(h->device);
+  CK(cudaMemcpyAsync(dst, h->ext.out, 4 * (size_t)h->ext.ntr * h->ext.nt, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots) {
+  if (!h || nslots < 0 || fmt < RTM_SNAP_FP32 || fmt > RTM_SNAP_FP16S) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  h->release(h->snaps), h->release(h->slabs);
+  h->snaps = nullptr, h->slabs = nullptr;
+  h->snap_fmt = fmt, h->nslots = nslots;
+  h->slot_bytes = fmt == RTM_SNAP_FP32 ? (size_t)h->n * 4
+                                       : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2 : (size_t)h->n * 2;
+  h->slot_bytes = (h->slot_bytes + 255) / 256 * 256;
+  h->stored.assign(nslots, 0);
+  if (!nslots) return RTM_OK;
+  TRY(h->alloc(h->snaps, h->slot_bytes * nslots));
+  if (fmt != RTM_SNAP_FP32) TRY(h->alloc(h->slabs, (size_t)nslots * h->d.ny));
+  return RTM_OK;
+}
+
+int rtm_snapshot_store(rtm_handle *h, int slot) {
+  TRY(rtm::ready(h));
+  if (slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
+  TRY(rtm::snap_prepare(h, slot));
+  rtm::launch_fused_io(rtm::io_store(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
+  TRY(rtm::check_launch(h, "snapshot_store"));
+  h->stored[slot] = 1;
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_snapshot_load(rtm_handle *h, int slot, float *dst) {
+  if (!h || !dst || slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  float *tmp = nullptr;
+  TRY(h->alloc(tmp, h->n));
+  rtm::launch_snap_decode(rtm::slot_dev(h, slot), tmp, h->ex, h->ey, h->ez, h->d.nx, h->d.ny, h->d.nz, h->st);
+  int rc = rtm::check_launch(h, "snapshot_load");
+  if (rc == RTM_OK) {
+    cudaError_t e = cudaMemcpyAsync(dst, tmp, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) rc = rtm::cuda_fail(e, "snapshot_load copy", h);
+  }
+  h->release(tmp);
+  return rc;
+}
+
+int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
+  if (!h || ntaper_t < 0 || ntaper_z < 0 || ntaper_z > h->d.nz) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->image) {
+    TRY(h->alloc(h->image, h->n));
+    TRY(h->alloc(h->comp, h->n));
+  }
+  CK(cudaMemsetAsync(h->image, 0, 4 * (size_t)h->n, h->st));
+  CK(cudaMemsetAsync(h->comp, 0, 4 * (size_t)h->n, h->st));
+  // ImagingCondition::calTapes (bgprtm/ImagingCondition.cpp:180-198)
+  h->taper_t.resize(ntaper_t);
+  for (int i = 0; i < ntaper_t; i++) h->taper_t[i] = 0.5f * (1.0f - cosf((float)M_PI * float(i) / float(ntaper_t)));
+  std::vector<float> tz(h->d.nz, 1.0f);
+  for (int i = 0; i < ntaper_z; i++) tz[i] = 0.5f * (1.0f - cosf((float)M_PI * float(i) / float(ntaper_z)));
+  CK(cudaMemcpyAsync(h->taper_z, tz.data(), 4 * h->d.nz, cudaMemcpyHostToDevice, h->st));
+  h->ic_edge = edge ? 1 : 0;
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_image_accumulate(rtm_handle *h, int slot) {
+  TRY(rtm::ready(h));
+  if (slot < 0 || slot >= h->nslots || !h->image) return RTM_ERR_ARG;
+  if (!h->stored[slot]) return RTM_OK;
+  rtm::launch_fused_io(rtm::io_image(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
+  TRY(rtm::check_launch(h, "image_accumulate"));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_modelling(rtm_handle *h, int nts, int it_shift, int ntratio) {
+  TRY(rtm::ready(h));
+  if (nts < 0 || ntratio < 1) return RTM_ERR_ARG;
+  const int mode = h->c.use_q ? 2 : 1;
+  return rtm::run_graphs(h, nts, [&](int it) {
+    TRY(rtm::step_kernel(h, mode, rtm::io_none()));
+    TRY(rtm::do_inject(h, it + it_shift));
+    if (it % ntratio == 0) TRY(rtm::do_extract(h, it / ntratio));
+    rtm::do_swap(h);
+    return (int)RTM_OK;
+  });
+}
+
+int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift, int interval) {
+  TRY(rtm::ready(h));
+  if ((dir != RTM_FORWARD && dir != RTM_BACKWARD) || interval < 1) return RTM_ERR_ARG;
+  if (dir == RTM_BACKWARD && !h->image) {
+    h->err = "rtm_image_setup must precede a backward migration";
+    return RTM_ERR_STATE;
+  }
+  const int inc = dir == RTM_FORWARD ? 1 : -1;
+  const int count = dir == RTM_FORWARD ? it_end - it_begin : it_begin - it_end;
+  if (count < 0) return RTM_ERR_ARG;
+  const int mode = h->c.use_q ? 2 : 1;
+  rtm::FusedIo pending = rtm::io_none();
+  int rc = rtm::run_graphs(h, count, [&](int s) {
+    const int it = it_begin + s * inc;
+    TRY(rtm::step_kernel(h, mode, pending));
+    pending = rtm::io_none();
+    TRY(rtm::do_inject(h, it + it_shift * inc));
+    if (it % interval == 0) {
+      const int slot = it / interval;
+      if (slot >= 0 && slot < h->nslots) {
+        if (dir == RTM_FORWARD) {
+          TRY(rtm::snap_prepare(h, slot));
+          pending = rtm::io_store(h, slot);
+          h->stored[slot] = 1;
+        } else if (h->stored[slot]) {
+          pending = rtm::io_image(h, slot);
+        }
+      }
+    }
+    rtm::do_swap(h);
+    return (int)RTM_OK;
+  });
+  if (rc != RTM_OK) return rc;
+  if (pending.store || pending.ic) {  // the last step's snapshot / image term
+    rtm::launch_fused_io(pending, h->w1, h->d.nx, h->d.ny, h->d.nz, h->st);
+    TRY(rtm::check_launch(h, "fused_io(last)"));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  return RTM_OK;
+}
+
+int rtm_get(rtm_handle *h, int field, float *dst) {
+  if (!h || !dst) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  const float *src = field == RTM_FIELD_W0 ? h->w0
+                     : field == RTM_FIELD_W1 ? h->w1
+                     : field == RTM_FIELD_VEL ? h->vel
+                     : field == RTM_FIELD_IMAGE ? h->image
+                     : field == RTM_FIELD_INVQ ? h->invq : nullptr;
+  if (!src) return RTM_ERR_ARG;
+  CK(cudaMemcpyAsync(dst, src, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_put(rtm_handle *h, int field, const float *src) {
+  if (!h || !src || (field != RTM_FIELD_W0 && field != RTM_FIELD_W1)) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaMemcpyAsync(field == RTM_FIELD_W0 ? h->w0 : h->w1, src, 4 * (size_t)h->n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_c16_compress(const float *in, unsigned short *out, int nx, int ny, int nz) {
+  if (!in || !out || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  const size_t n = (size_t)nx * ny * nz, nc = ((size_t)nx * nz + 2) * ny;
+  float *din = nullptr, *slab = nullptr;
+  uint16_t *dout = nullptr;
+  cudaStream_t st = 0;
+  int rc = RTM_OK;
+  if (cudaMalloc(&din, n * 4) || cudaMalloc(&dout, nc * 2) || cudaMalloc(&slab, ny * 4)) rc = RTM_ERR_NOMEM;
+  if (rc == RTM_OK && cudaMemcpy(din, in, n * 4, cudaMemcpyHostToDevice)) rc = RTM_ERR_CUDA;
+  if (rc == RTM_OK) {
+    rtm::launch_c16_compress(din, dout, slab, nx, ny, nz, st);
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, dout, nc * 2, cudaMemcpyDeviceToHost)) rc = RTM_ERR_CUDA;
+  }
+  cudaFree(din), cudaFree(dout), cudaFree(slab);
+  cudaGetLastError();
+  return rc;
+}
+
+int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int nz) {
+  if (!in || !out || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  const size_t n = (size_t)nx * ny * nz, nc = ((size_t)nx * nz + 2) * ny;
+  float *dout = nullptr, *slab = nullptr, *ex = nullptr, *ey = nullptr, *ez = nullptr;
+  uint16_t *din = nullptr;
+  int rc = RTM_OK;
+  if (cudaMalloc(&din, nc * 2) || cudaMalloc(&dout, n * 4) || cudaMalloc(&slab, ny * 4) || cudaMalloc(&ex, nx * 4) ||
+      cudaMalloc(&ey, ny * 4) || cudaMalloc(&ez, nz * 4))
+    rc = RTM_ERR_NOMEM;
+  std::vector<float> tx, ty, tz;
+  rtm::edge_taper(nx, 20, tx), rtm::edge_taper(ny, 20, ty), rtm::edge_taper(nz, 10, tz);
+  if (rc == RTM_OK && (cudaMemcpy(din, in, nc * 2, cudaMemcpyHostToDevice) ||
+                       cudaMemcpy(ex, tx.data(), nx * 4, cudaMemcpyHostToDevice) ||
+                       cudaMemcpy(ey, ty.data(), ny * 4, cudaMemcpyHostToDevice) ||
+                       cudaMemcpy(ez, tz.data(), nz * 4, cudaMemcpyHostToDevice)))
+    rc = RTM_ERR_CUDA;
+  if (rc == RTM_OK) {
+    rtm::launch_c16_uncompress(din, dout, slab, ex, ey, ez, nx, ny, nz, 0);
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost)) rc = RTM_ERR_CUDA;
+  }
+  cudaFree(din), cudaFree(dout), cudaFree(slab), cudaFree(ex), cudaFree(ey), cudaFree(ez);
+  cudaGetLastError();
+  return rc;
+}
+
+int rtm_last_loop_ms(rtm_handle *h, float *ms) {
+  if (!h || !ms) return RTM_ERR_ARG;
+  *ms = h->last_ms;
+  return RTM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+// rtm_device.cuh - inline device helpers shared by the kernel files: PML
+// recursion, fused snapshot / imaging-condition access, the COMPRESS_16 code,
+// the FP16 slab codec and the visco-acoustic update.
+#pragma once
+#include <cuda_fp16.h>
+
+#include "rtm_internal.cuh"
+
+namespace rtm {
+
+struct Grid3 {
+  int nx, ny, nz;
+  long long nxz;
+};
+
+// One recursion round of the split-field PML on value p with memory q
+// (bgprtm/PML.cpp:126-134): q' = (1-g)/(1+g) q - 2g/(1-g^2) p ; p' = q' + p/(1-g).
+__device__ __forceinline__ void pml_round(const float *co, float &p, float *q) {
+  float qn = co[0] * (*q) - co[1] * p;
+  *q = qn;
+  p = qn + co[2] * p;
+}
+
+// Memory cell and constants of face (d, s) for grid cell (ix,iy,iz), or null
+// outside the face's layers.  Indexing follows bgprtm/FdEngine.cpp:324-389.
+__device__ __forceinline__ float *pml_at(const PmlDev &P, const Grid3 &g, int d, int s, int r, int c, int ix, int iy,
+                                         int iz, const float *&co) {
+  const PmlFace &F = P.f[d][s];
+  const int w = F.w;
+  if (!w) return nullptr;
+  long long idx;
+  int L;
+  if (d == DZ) {
+    if (s == SIDE_LO) {
+      if (iz >= w) return nullptr;
+      L = iz;
+      idx = ((long long)iy * g.nx + ix) * w + iz;
+    } else {
+      if (iz < g.nz - w) return nullptr;
+      L = g.nz - 1 - iz;
+      idx = ((long long)iy * g.nx + ix) * w + (iz - (g.nz - w));
+    }
+  } else if (d == DX) {
+    if (s == SIDE_LO) {
+      if (ix >= w) return nullptr;
+      L = ix;
+      idx = ((long long)iy * w + ix) * g.nz + iz;
+    } else {
+      if (ix < g.nx - w) return nullptr;
+      L = g.nx - 1 - ix;
+      idx = ((long long)iy * w + ix - (g.nx - w)) * g.nz + iz;
+    }
+  } else {
+    if (s == SIDE_LO) {
+      if (iy >= w) return nullptr;
+      L = iy;
+      idx = ((long long)iy * g.nx + ix) * g.nz + iz;
+    } else {
+      if (iy < g.ny - w) return nullptr;
+      L = g.ny - 1 - iy;
+      idx = ((long long)(iy - (g.ny - w)) * g.nx + ix) * g.nz + iz;
+    }
+  }
+  co = F.co + L * 6;
+  return F.q[r][c] + idx;
+}
+
+// Two rounds along dim d on the summed 2nd-derivative operator
+// (pml2_{z,x,y}bnd, bgprtm/FdEngine.cpp:352-389).
+__device__ __forceinline__ void pml2_dim(const PmlDev &P, const Grid3 &g, int d, float &p, int ix, int iy, int iz) {
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const float *co;
+    float *q1 = pml_at(P, g, d, s, 0, 0, ix, iy, iz, co);
+    if (!q1) continue;
+    const float *co2;
+    float *q2 = pml_at(P, g, d, s, 1, 0, ix, iy, iz, co2);
+    pml_round(co, p, q1);
+    pml_round(co, p, q2);
+  }
+}
+
+// One round (round r) on a first derivative along `axis`, own direction
+// unscaled then the other two scaled (pml1_{z,x,y}bnd, bgprtm/FdEngine.cpp:301-350).
+__device__ __forceinline__ void pml1_dim(const PmlDev &P, const Grid3 &g, int d, int c, int scaled, int r, float &p,
+                                         int ix, int iy, int iz) {
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const float *co;
+    float *q = pml_at(P, g, d, s, r, c, ix, iy, iz, co);
+    if (!q) continue;
+    pml_round(co + 3 * scaled, p, q);
+  }
+}
+__device__ __forceinline__ void pml1(const PmlDev &P, const Grid3 &g, int pml3d, int axis, int r, float &p, int ix,
+                                     int iy, int iz) {
+  if (axis == DZ) {
+    pml1_dim(P, g, DZ, 0, 0, r, p, ix, iy, iz);
+    if (pml3d) pml1_dim(P, g, DX, 1, 1, r, p, ix, iy, iz), pml1_dim(P, g, DY, 1, 1, r, p, ix, iy, iz);
+  } else if (axis == DX) {
+    pml1_dim(P, g, DX, 0, 0, r, p, ix, iy, iz);
+    if (pml3d) pml1_dim(P, g, DZ, 1, 1, r, p, ix, iy, iz), pml1_dim(P, g, DY, 2, 1, r, p, ix, iy, iz);
+  } else {
+    pml1_dim(P, g, DY, 0, 0, r, p, ix, iy, iz);
+    if (pml3d && g.ny > 1) pml1_dim(P, g, DZ, 2, 1, r, p, ix, iy, iz), pml1_dim(P, g, DX, 2, 1, r, p, ix, iy, iz);
+  }
+}
+
+// --- COMPRESS_16 code (bgprtm/WaveFieldCompress.cpp:107-133) ----------------
+__device__ __forceinline__ uint16_t c16_encode(float v) {
+  const int idat = __float_as_int(v);
+  const uint16_t sgn = (uint16_t)(((unsigned)idat & 0x80000000u) >> 16);
+  int e = ((idat & 0x7f800000) >> 23) - 127;
+  if (e > 0) return 0x8000;
+  if (e == 0) return sgn | 0x1;
+  if (e > -5) return sgn | (uint16_t)((((idat & 0x7fffff) | 0x800000)) >> (9 - e));
+  if (e > -21) return sgn | 0x4000 | (uint16_t)((e + 20) << 10) | (uint16_t)((idat & 0x7fffff) >> 13);
+  if (e > -30) return sgn | (uint16_t)((((idat & 0x7fffff) | 0x800000)) >> (-7 - e));
+  return 0;
+}
+// Value of the decode table entry (bgprtm/WaveFieldCompress.cpp:52-86),
+// rebuilt arithmetically: every entry is an exact power-of-two multiple.
+__device__ __forceinline__ float c16_table(uint16_t c) {
+  const int m = c & 0x7fff;
+  float v;
+  if (m == 0) return (c & 0x8000) ? __int_as_float(0x7fffffff) : 0.0f;
+  if (m == 1) v = 1.0f;
+  else if (m < 1024) v = (float)m * 9.31322574615478515625e-10f;  // 2^-30
+  else if (m < 16384) v = (float)m * 6.103515625e-05f;          // 2^-14
+  else {
+    const int j = (m - 16384) >> 10, i = m & 1023;
+    v = __int_as_float((127 - 20 + j) << 23) * (1.0f + (float)i * 9.765625e-4f);
+  }
+  return (c & 0x8000) ? -v : v;
+}
+
+// FP16 with a per-y-slab scale: stored h = fp16(v * (1/s)), value = h * s
+__device__ __forceinline__ float slab16_decode(__half h, float s) { return __half2float(h) * s; }
+__device__ __forceinline__ __half slab16_encode(float v, float s) { return __float2half_rn(s > 0.f ? v / s : 0.f); }
+
+// Raw decoded value of a snapshot cell (no tapers).
+__device__ __forceinline__ float snap_read(const SnapDev &S, const Grid3 &g, long long i, int iy, long long inslab) {
+  if (S.fmt == 0) return ((const float *)S.base)[i];
+  if (S.fmt == 1) {
+    const uint16_t c = ((const uint16_t *)S.base)[(long long)iy * (g.nxz + 2) + 2 + inslab];
+    return S.slab[iy] * c16_table(c);
+  }
+  return slab16_decode(((const __half *)S.base)[i], S.slab[iy]);
+}
+__device__ __forceinline__ void snap_write(const SnapDev &S, const Grid3 &g, long long i, int iy, long long inslab,
+                                           float v) {
+  if (S.fmt == 0) {
+    ((float *)S.base)[i] = v;
+  } else if (S.fmt == 1) {
+    const float vmax = S.slab[iy];
+    uint16_t c = 0;
+    if (vmax > 1e-25f) c = c16_encode(v * __frcp_rn(vmax));
+    ((uint16_t *)S.base)[(long long)iy * (g.nxz + 2) + 2 + inslab] = c;
+  } else {
+    ((__half *)S.base)[i] = slab16_encode(v, S.slab[iy]);
+  }
+}
+
+// Fused snapshot store / zero-lag imaging of the centre value u (the final
+// wavefield of the previous step) at cell (ix,iy,iz).
+__device__ __forceinline__ void fused_io(const FusedIo &io, const Grid3 &g, long long i, int ix, int iy, int iz,
+                                         long long inslab, float u) {
+  if (io.store) snap_write(io.st, g, i, iy, inslab, u);
+  if (io.ic) {
+    float s = snap_read(io.src, g, i, iy, inslab);
+    // decode tapers (y, x, z order as bgprtm/WaveFieldCompress.cpp:189-200),
+    // then the source time / depth taper (bgprtm/ImagingCondition.cpp:207-225)
+    s = s * io.ey[iy];
+    s = s * io.ex[ix];
+    s = s * io.ez[iz];
+    if (io.use_t) s = s * io.tscale;
+    else s = s * io.taper_z[iz];
+    float r = u * io.ey[iy];
+    r = r * io.ex[ix];
+    r = r * io.ez[iz];
+    // Kahan-compensated accumulation (image, comp)
+    const float prod = s * r;
+    const float img = io.image[i];
+    const float y = prod - io.comp[i];
+    const float t = img + y;
+    io.comp[i] = (t - img) - y;
+    io.image[i] = t;
+  }
+}
+
+// Visco-acoustic update (bgprtm/Propagator.cpp:1789-1816) for one cell:
+// t = w0 - vel*L[w1] on entry, u = w1.
+__device__ __forceinline__ float q_update(const QDev &Q, long long i, long long n, float t, float u) {
+  const float iq = Q.invq[i];
+  float v = u * (2.0f + iq * Q.cqsum) - t;
+  for (int l = 0; l < Q.order; l++) {
+    float *d0p = Q.d0 + (long long)l * n + i;
+    const float d0 = *d0p, d1 = Q.d1[(long long)l * n + i];
+    const float el = Q.wq[l];
+    v += iq * ((1.0f + el) * d0 - d1 * 2.0f);
+    *d0p = Q.cq[l] * u + el * d0;
+  }
+  return v;
+}
+
+}  // namespace rtm

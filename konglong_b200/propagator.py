@@ -1,0 +1,205 @@
+"""Host-side mirror of bgprtm's propagation interface over the CUDA engine.
+
+`Propagator` exposes, on one GPU-resident shot, the operations the reference
+splits across KernelCPU (bgprtm/KernelCPU.h:16-64), Propagator
+(bgprtm/Propagator.h:100-148), Receiver / ExtractReceiverData and
+WaveFieldCompress / ImagingCondition, with the reference's names and argument
+meaning.  Every call goes through the C ABI of include/rtm_b200.h; errors
+raise `RtmError` with the engine's message.  There is no CPU code path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .spec import (FIELD_IMAGE, FIELD_W0, FORWARD, PropSpec, TraceSet)
+
+
+def _arr(a, dtype=np.float32):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype).ravel()
+
+
+class Propagator:
+    """One shot's wavefield state on the current CUDA device."""
+
+    def __init__(self, spec: PropSpec):
+        L = _lib.lib()
+        self.L = L
+        self.spec = spec
+        d = _lib.RtmDims(spec.nx, spec.ny, spec.nz, spec.dx, spec.dy, spec.dz, spec.dt)
+        c = _lib.RtmConfig()
+        L.rtm_config_default(C.byref(c))
+        c.engine, c.model_type = spec.engine, spec.model_type
+        c.use_q, c.q_order = int(spec.use_q), spec.q_order
+        for k in range(6):
+            c.nbnd[k] = int(spec.nbnd[k])
+        c.vmax, c.pml_eps = spec.vmax, spec.pml_eps
+        c.pml3d, c.pml3d_scaler, c.top_pml = int(spec.pml3d), spec.pml3d_scaler, int(spec.top_pml)
+        c.state_fp16 = int(spec.state_fp16)
+        h = C.c_void_p()
+        _lib.check(L.rtm_create(C.byref(d), C.byref(c), C.byref(h)), "rtm_create")
+        self.h = h
+        self.n = spec.n
+        self._ext = None
+
+    # -- lifetime -----------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rtm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, code, what):
+        _lib.check(code, what, self.h)
+
+    # -- model (KernelCPU::setModel + Propagator::Vel2, Q::updateCq) ----------------
+    def set_q_coeffs(self, cq0, cq, wq):
+        self._ck(self.L.rtm_set_q_coeffs(self.h, float(cq0), _arr(cq), _arr(wq)), "rtm_set_q_coeffs")
+
+    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None):
+        arrs = [_arr(a) for a in (vel, eps, dl, pjx, pjy, invq)]
+        for a in arrs:
+            if a is not None and a.size != self.n:
+                raise ValueError("model volume size does not match the grid")
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        self._ck(self.L.rtm_set_model(self.h, *ptrs), "rtm_set_model")
+
+    # -- one step's pieces ----------------------------------------------------------
+    def reset(self):
+        self._ck(self.L.rtm_reset(self.h), "rtm_reset")
+
+    def kernel(self):
+        """KernelCPU::ISO / VTI / TTI: w0 -= (v dt)^2 L[w1] with PML."""
+        self._ck(self.L.rtm_kernel(self.h), "rtm_kernel")
+
+    def update2nd(self):
+        self._ck(self.L.rtm_update2nd(self.h), "rtm_update2nd")
+
+    def swap(self):
+        self._ck(self.L.rtm_swap(self.h), "rtm_swap")
+
+    # -- sources / receivers (Receiver::apply, ExtractReceiverData::extract) ---------
+    def set_injection(self, ts: TraceSet, traces, scaler):
+        tr = np.ascontiguousarray(traces, np.float32)
+        self._ck(self.L.rtm_set_injection(self.h, ts.ntr, ts.lx, ts.ly, ts.lz, _arr(ts.off, np.int32),
+                                          _arr(ts.len, np.int32), _arr(ts.kx), _arr(ts.ky), _arr(ts.kz),
+                                          tr.ravel(), tr.shape[1], float(scaler)), "rtm_set_injection")
+
+    def set_extraction(self, ts: TraceSet, nt_out):
+        self._ext = (ts.ntr, nt_out)
+        self._ck(self.L.rtm_set_extraction(self.h, ts.ntr, ts.lx, ts.ly, ts.lz, _arr(ts.off, np.int32),
+                                           _arr(ts.len, np.int32), _arr(ts.kx), _arr(ts.ky), _arr(ts.kz),
+                                           nt_out), "rtm_set_extraction")
+
+    def inject(self, it):
+        self._ck(self.L.rtm_inject(self.h, it), "rtm_inject")
+
+    def extract(self, jt):
+        self._ck(self.L.rtm_extract(self.h, jt), "rtm_extract")
+
+    def traces(self):
+        ntr, nt = self._ext
+        out = np.zeros((ntr, nt), np.float32)
+        self._ck(self.L.rtm_get_traces(self.h, out.ravel()), "rtm_get_traces")
+        return out
+
+    # -- snapshots and imaging --------------------------------------------------------
+    def snapshot_setup(self, fmt, nslots):
+        self._ck(self.L.rtm_snapshot_setup(self.h, fmt, nslots), "rtm_snapshot_setup")
+
+    def snapshot_store(self, slot):
+        self._ck(self.L.rtm_snapshot_store(self.h, slot), "rtm_snapshot_store")
+
+    def snapshot_load(self, slot):
+        out = np.zeros(self.n, np.float32)
+        self._ck(self.L.rtm_snapshot_load(self.h, slot, out), "rtm_snapshot_load")
+        return out
+
+    def image_setup(self, ntaper_t=0, ntaper_z=0, edge=1):
+        self._ck(self.L.rtm_image_setup(self.h, ntaper_t, ntaper_z, edge), "rtm_image_setup")
+
+    def image_accumulate(self, slot):
+        self._ck(self.L.rtm_image_accumulate(self.h, slot), "rtm_image_accumulate")
+
+    # -- time loops (Propagator::modelling / migration) -------------------------------
+    def modelling(self, nts, it_shift=-1, ntratio=1):
+        self._ck(self.L.rtm_modelling(self.h, nts, it_shift, ntratio), "rtm_modelling")
+
+    def migration(self, direction, it_begin, it_end, it_shift=-1, interval=1):
+        self._ck(self.L.rtm_migration(self.h, direction, it_begin, it_end, it_shift, interval),
+                 "rtm_migration")
+
+    @property
+    def last_loop_ms(self):
+        v = C.c_float()
+        self._ck(self.L.rtm_last_loop_ms(self.h, C.byref(v)), "rtm_last_loop_ms")
+        return v.value
+
+    # -- field access -------------------------------------------------------------------
+    def get(self, field):
+        out = np.zeros(self.n, np.float32)
+        self._ck(self.L.rtm_get(self.h, field, out.ctypes.data), "rtm_get")
+        return out
+
+    def put(self, field, a):
+        a = _arr(a)
+        self._ck(self.L.rtm_put(self.h, field, a.ctypes.data), "rtm_put")
+
+    # -- whole-shot drivers ----------------------------------------------------------
+    def rtm_shot(self, src: TraceSet, src_traces, rcv: TraceSet, rcv_traces, nt, nts_fwd, interval,
+                 snap_fmt=0, ntaper_t=0, ntaper_z=0, edge=1, it_shift=-1):
+        """Propagator::rtm for one shot (bgprtm/Propagator.cpp:2157-2280): forward
+        pass storing snapshots, backward pass with the zero-lag imaging condition
+        fused into the step, image returned."""
+        nslots = (nts_fwd - 1) // interval + 1
+        self.snapshot_setup(snap_fmt, nslots)
+        self.reset()
+        self.set_injection(src, src_traces, self.spec.dt_dxyz)
+        self.migration(FORWARD, 0, nts_fwd, it_shift, interval)
+        fwd_ms = self.last_loop_ms
+        self.reset()
+        self.image_setup(ntaper_t, ntaper_z, edge)
+        self.set_injection(rcv, rcv_traces, self.spec.dt_dxyz)
+        self.migration(1, nt - 1, -1, it_shift, interval)
+        bwd_ms = self.last_loop_ms
+        return self.get(FIELD_IMAGE), fwd_ms, bwd_ms
+
+
+def spread_coeffs(n, x, k1, k2, nlimit, dipole=False, ntaper=0):
+    """Util::CompactOrmsbySpreadCoeff + Receiver's edge taper through the C ABI;
+    returns (first grid index, coefficients)."""
+    L = _lib.lib()
+    nl = C.c_int(nlimit)
+    off = C.c_int(0)
+    buf = np.zeros(max(nlimit, 1), np.float32)
+    _lib.check(L.rtm_spread_coeffs(n, float(x), float(k1), float(k2), C.byref(nl), int(dipole), ntaper,
+                                   buf, C.byref(off)), "rtm_spread_coeffs")
+    return off.value, buf[:nl.value].copy()
+
+
+def c16_compress(a, nx, ny, nz):
+    out = np.zeros((nx * nz + 2) * ny, np.uint16)
+    _lib.check(_lib.lib().rtm_c16_compress(_arr(a), out, nx, ny, nz), "rtm_c16_compress")
+    return out
+
+
+def c16_uncompress(c, nx, ny, nz):
+    out = np.zeros(nx * ny * nz, np.float32)
+    _lib.check(_lib.lib().rtm_c16_uncompress(np.ascontiguousarray(c, np.uint16), out, nx, ny, nz),
+               "rtm_c16_uncompress")
+    return out
+
+
+def w0(p: Propagator):
+    return p.get(FIELD_W0)

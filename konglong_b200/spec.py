@@ -1,0 +1,68 @@
+"""Propagation set-up shared by the host driver, the tests and the bench.
+
+`PropSpec` carries what bgprtm's KernelCPU/FdEngine constructor and
+setBoundary take (bgprtm/KernelCPU.h:19-27, bgprtm/FdEngine.cpp:24-53,
+108-182) and maps one-to-one onto the C ABI's rtm_dims + rtm_config.
+`TraceSet` is the packed form of Receiver::spreadCoeffs' per-trace separable
+kernels (kernels_x/y/z, offxs/offys/offzs, lxs/lys/lzs,
+bgprtm/Receiver.h:154-156).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+ENGINE_FD8, ENGINE_CFD = 0, 1
+ISO, VTI, TTI = 1, 2, 3
+FORWARD, BACKWARD = 0, 1
+SNAP_FP32, SNAP_C16, SNAP_FP16S = 0, 1, 2
+FIELD_W0, FIELD_W1, FIELD_VEL, FIELD_IMAGE, FIELD_INVQ = 0, 1, 2, 3, 4
+
+
+@dataclass
+class PropSpec:
+    nx: int
+    ny: int
+    nz: int
+    dx: float = 10.0
+    dy: float = 10.0
+    dz: float = 10.0
+    dt: float = 0.001
+    engine: int = ENGINE_FD8
+    model_type: int = ISO
+    use_q: bool = False
+    q_order: int = 4
+    nbnd: tuple = (20, 20, 20, 20, 20, 20)   # x1, x2, y1, y2, z1, z2
+    vmax: float = 4500.0
+    pml_eps: float = 1e-3
+    pml3d: bool = True
+    pml3d_scaler: float = 0.3
+    top_pml: bool = True
+    state_fp16: bool = False
+
+    @property
+    def n(self):
+        return self.nx * self.ny * self.nz
+
+    @property
+    def shape(self):
+        """numpy shape of a volume in the reference layout (z fastest)."""
+        return (self.ny, self.nx, self.nz)
+
+    @property
+    def dt_dxyz(self):
+        """Receiver::dt_dxyz for a 3-D grid (bgprtm/Receiver.cpp:55-57)."""
+        return np.float32(1.0) / np.float32(self.dz) / np.float32(self.dx) / np.float32(self.dy)
+
+
+@dataclass
+class TraceSet:
+    """Separable spread kernels of ntr traces, padded to fixed strides."""
+    ntr: int
+    lx: int
+    ly: int
+    lz: int
+    off: np.ndarray = field(repr=False)   # int32 [ntr, 3] first index x, y, z
+    len: np.ndarray = field(repr=False)   # int32 [ntr, 3] used length x, y, z
+    kx: np.ndarray = field(repr=False)    # float32 [ntr, lx]
+    ky: np.ndarray = field(repr=False)    # float32 [ntr, ly]
+    kz: np.ndarray = field(repr=False)    # float32 [ntr, lz]

@@ -1,0 +1,266 @@
+"""Seeded synthetic shots for the propagation path (no public data set is used).
+
+Each builder returns a `Shot`: the PropSpec, the model volumes in the
+reference layout ([ny][nx][nz], z fastest), the source wavelet and the
+source / receiver spread kernels.  `scale` shrinks the grid for tests while
+keeping the structure.  Sizes, spacings, frequencies and value ranges follow
+the five workloads the project is measured on:
+  iso128   : 128^3 ISO, FD8, 1000 steps, PML 20, 4 layers + 5 % smooth noise
+  vti_cfd  : 512x512x400 VTI, compact FD, 4000 steps, PML 32, 256x256 receivers
+  tti_q    : 640x640x512 TTI + Q, 5000 steps, PML 32 (assumed)
+  batch    : 64 small ISO/VTI shots of uneven aperture (96-256 cells per axis)
+CFL: the time step is min(stated dt, the stability rule of
+ModelPrepare::calcDeltaTime, bgprtm/ModelPrepare.cpp:647-914), as the
+reference itself only accepts a user dt below its stability bound
+(bgprtm/ModelPrepare.cpp:901-910).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .spec import ENGINE_CFD, ENGINE_FD8, ISO, TTI, VTI, PropSpec, TraceSet
+
+
+@dataclass
+class Shot:
+    spec: PropSpec
+    nt: int                      # recorded time samples (steps)
+    vel: np.ndarray
+    eps: np.ndarray = None
+    dl: np.ndarray = None
+    pjx: np.ndarray = None
+    pjy: np.ndarray = None
+    invq: np.ndarray = None
+    wavelet: np.ndarray = None   # [nt]
+    src_pos: tuple = None        # fractional grid index (x, y, z)
+    rcv_pos: np.ndarray = None   # [nr, 3]
+    interval: int = 4            # snapshot interval (steps)
+    fpeak: float = 15.0
+    name: str = ""
+    extra: dict = field(default_factory=dict)
+
+    def model_arrays(self):
+        return dict(vel=self.vel, eps=self.eps, dl=self.dl, pjx=self.pjx, pjy=self.pjy, invq=self.invq)
+
+
+# ---------------------------------------------------------------------------
+def smooth_field(shape, sigma, rng):
+    """N(0,1) noise Gaussian-smoothed with `sigma` cells, scaled to max|g| = 1."""
+    from scipy.ndimage import gaussian_filter, zoom
+    n = int(np.prod(shape))
+    if n <= 8_000_000 or sigma < 4:
+        g = gaussian_filter(rng.standard_normal(shape).astype(np.float32), sigma, mode="reflect")
+    else:
+        f = 4
+        small = tuple(max(4, s // f) for s in shape)
+        g = gaussian_filter(rng.standard_normal(small).astype(np.float32), sigma / f, mode="reflect")
+        g = zoom(g, [s / c for s, c in zip(shape, small)], order=1)[:shape[0], :shape[1], :shape[2]]
+        g = np.ascontiguousarray(g, dtype=np.float32)
+    m = np.abs(g).max()
+    return (g / m if m > 0 else g).astype(np.float32)
+
+
+def minmax(g, lo, hi):
+    a, b = float(g.min()), float(g.max())
+    return (lo + (g - a) * ((hi - lo) / (b - a if b > a else 1.0))).astype(np.float32)
+
+
+def ricker(f, dt, nt, delay=None):
+    """Ricker wavelet, peak frequency f, delayed by 1/f, amplitude x 1e5 as
+    Wavelet.cpp scales its wavelets (bgprtm/Wavelet.cpp:74-78)."""
+    t0 = 1.0 / f if delay is None else delay
+    t = np.arange(nt) * dt - t0
+    a = (np.pi * f * t) ** 2
+    return ((1.0 - 2.0 * a) * np.exp(-a) * 1e5).astype(np.float32)
+
+
+def fd8_k1max():
+    """FdEngine_fd::get_k1max with Taylor weights (bgprtm/FdEngine_fd.cpp:69-81)."""
+    c2 = [-205 / 72, 8 / 5, -1 / 5, 8 / 315, -1 / 560]
+    s = -c2[0]
+    sg = 2
+    for j in range(1, 5):
+        s += sg * c2[j]
+        sg = -sg
+    return float(np.sqrt(np.float32(s)) * np.float32(1.01))
+
+
+def cfl_dt(spec: PropSpec, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None, maxfreq=None):
+    """ModelPrepare::calcDeltaTime restated (bgprtm/ModelPrepare.cpp:647-881),
+    rectangular grid, no density: FD engines use k1max of the Taylor table, the
+    others pi; VTI/TTI take the largest phase velocity over the grid-axis
+    combinations and divide by sqrt(1+2 eps) again; Q rescales."""
+    k1 = fd8_k1max() if spec.engine == ENGINE_FD8 else np.pi
+    rd = np.array([1 / spec.dx ** 2, 1 / spec.dy ** 2 if spec.ny > 1 else 0.0, 1 / spec.dz ** 2])
+    if spec.model_type == ISO or eps is None:
+        lam = float(vel.max()) * np.sqrt(rd.sum())
+        dt = 2.0 / k1 / lam
+    else:
+        # VTI (axis along z): the reference loops every cell; the bound is
+        # monotone in v and eps, so the per-cell maximum is taken directly
+        v = vel.ravel().astype(np.float64)
+        e = eps.ravel().astype(np.float64)
+        d = dl.ravel().astype(np.float64)
+        lam = np.zeros_like(v)
+        for ic in range(1, 8):
+            icz, icx, icy = ic & 1, (ic >> 1) & 1, (ic >> 2) & 1
+            h2 = rd[0] * icx + rd[1] * icy
+            z2 = rd[2] * icz
+            t1 = (1 + 2 * e) * h2 + z2
+            lam = np.maximum(lam, v * np.sqrt((t1 + np.sqrt(np.maximum(t1 * t1 - 8 * (e - d) * h2 * z2, 0))) / 2))
+        dt = float(np.min(2.0 / k1 / lam / np.sqrt(1 + 2 * e)))
+    if spec.use_q and invq is not None and maxfreq:
+        qref = maxfreq / 3
+        dt *= 1 - float(invq.max()) * (3 + 2 / np.pi * np.log(maxfreq / qref))
+    return dt
+
+
+def update_zlimit(iz_min, iz_max, nz, spread):
+    """Receiver::update_zrange's limit on the z spread (bgprtm/Receiver.cpp:129-161)."""
+    lim = min(iz_min + 1, nz - 1 - iz_max)
+    if lim < spread:
+        spread = max(5, lim)
+    iz0 = iz_min - spread + 1
+    iz1 = iz_max + spread
+    return iz1 - iz0 + 1
+
+
+def make_traceset(points, nx, ny, nz, spread, k1, k2, coeff_fn, ntaper_xy=10):
+    """Receiver::spreadCoeffs (bgprtm/Receiver.cpp:306-363): separable kernels
+    per point.  points: [n, 3] fractional grid indices (x, y, z)."""
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    n = len(pts)
+    izs = np.floor(pts[:, 2]).astype(int)
+    lz_cap = update_zlimit(int(izs.min()), int(izs.max()), nz, spread)
+    lx_cap = 1 if nx == 1 else max(1, 2 * spread)
+    ly_cap = 1 if ny == 1 else max(1, 2 * spread)
+    off = np.zeros((n, 3), np.int32)
+    ln = np.zeros((n, 3), np.int32)
+    kx = np.zeros((n, lx_cap), np.float32)
+    ky = np.zeros((n, ly_cap), np.float32)
+    kz = np.zeros((n, lz_cap), np.float32)
+    for r, (x, y, z) in enumerate(pts):
+        o, c = coeff_fn(nx, np.float32(x), k1, k2, lx_cap, False, ntaper_xy)
+        off[r, 0], ln[r, 0], kx[r, :len(c)] = o, len(c), c
+        o, c = coeff_fn(ny, np.float32(y), k1, k2, ly_cap, False, ntaper_xy)
+        off[r, 1], ln[r, 1], ky[r, :len(c)] = o, len(c), c
+        o, c = coeff_fn(nz, np.float32(z), k1, k2, lz_cap, False, 0)
+        off[r, 2], ln[r, 2], kz[r, :len(c)] = o, len(c), c
+    return TraceSet(n, lx_cap, ly_cap, lz_cap, off, ln, kx, ky, kz)
+
+
+def spread_band(spec: PropSpec):
+    """src_apply_khpass / khcut defaults (bgprtm/ModelRegrid.cpp:86-87) from the
+    engine's dispersion factor (bgprtm/FdEngine.cpp:241-256)."""
+    if spec.engine == ENGINE_CFD:
+        disp = 0.9
+    else:
+        disp = 0.46 if spec.model_type >= VTI else 0.6
+    k = disp * 0.5 if disp <= 0.8 else None
+    return (k, k) if k is not None else (0.40, 0.48)
+
+
+# ---------------------------------------------------------------------------
+def iso128(scale=1.0, seed=1, nt=1000):
+    rng = np.random.default_rng(seed)
+    n = max(32, int(round(128 * scale)))
+    pml = max(6, int(round(20 * scale)))
+    spec = PropSpec(nx=n, ny=n, nz=n, dx=10.0, dy=10.0, dz=10.0, dt=0.001, engine=ENGINE_FD8, model_type=ISO,
+                    nbnd=(pml,) * 6, vmax=4500.0)
+    iz = np.arange(n)
+    layer_v = np.array([1500, 2200, 3000, 4500], np.float32)
+    prof = layer_v[np.minimum(iz * 4 // n, 3)]
+    vel = np.broadcast_to(prof, spec.shape).astype(np.float32)
+    g = smooth_field(spec.shape, 5.0, rng)
+    # 5 % perturbation, clipped to the layer range so dt = 1 ms meets the FD8 CFL bound
+    vel = np.clip(vel * (1.0 + 0.05 * g), 1500.0, 4500.0).astype(np.float32)
+    # dt = 1 ms as stated: v dt / dx = 0.45 is inside the FD8 leapfrog bound 0.4529
+    # (the reference's rule adds a 1 % margin on k1max, which would give 0.996 ms)
+    src = (n / 2, n / 2, pml + 1)
+    nr = max(4, int(round(64 * scale)))
+    step = max(1, (n - 2) // nr)
+    rx = 1 + step * np.arange(nr)
+    rxx, ryy = np.meshgrid(rx, rx, indexing="xy")
+    rcv = np.stack([rxx.ravel(), ryy.ravel(), np.full(rxx.size, pml + 2.0)], 1).astype(np.float32)
+    return Shot(spec, nt, vel, wavelet=ricker(15.0, spec.dt, nt), src_pos=src, rcv_pos=rcv, interval=4,
+                fpeak=15.0, name="iso128")
+
+
+def vti_cfd(scale=1.0, seed=2, nt=4000):
+    rng = np.random.default_rng(seed)
+    nx = max(32, int(round(512 * scale)))
+    nz = max(32, int(round(400 * scale)))
+    pml = max(6, int(round(32 * scale)))
+    spec = PropSpec(nx=nx, ny=nx, nz=nz, dx=10.0, dy=10.0, dz=10.0, dt=0.0008, engine=ENGINE_CFD,
+                    model_type=VTI, nbnd=(pml,) * 6, vmax=4500.0)
+    # smooth layered velocity: 6 seeded interfaces, 1500 -> 4500 m/s, smoothed
+    cuts = np.sort(rng.uniform(0.1, 0.9, 5)) * nz
+    vals = np.linspace(1500, 4500, 6).astype(np.float32)
+    iz = np.arange(nz)
+    prof = vals[np.searchsorted(cuts, iz)]
+    from scipy.ndimage import gaussian_filter1d
+    prof = gaussian_filter1d(prof.astype(np.float32), 3.0)
+    lat = smooth_field(spec.shape, 8.0, rng)
+    vel = np.clip(prof[None, None, :] * (1.0 + 0.03 * lat), 1500.0, 4500.0).astype(np.float32)
+    eps = minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 0.25)
+    dl = minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 0.10)
+    spec.dt = float(min(spec.dt, cfl_dt(spec, vel, eps, dl)))
+    src = (nx / 2, nx / 2, pml + 1)
+    nr = max(4, int(round(256 * scale)))
+    step = max(1, (nx - 2) // nr)
+    rx = 1 + step * np.arange(nr)
+    rxx, ryy = np.meshgrid(rx, rx, indexing="xy")
+    rcv = np.stack([rxx.ravel(), ryy.ravel(), np.full(rxx.size, pml + 2.0)], 1).astype(np.float32)
+    return Shot(spec, nt, vel, eps=eps, dl=dl, wavelet=ricker(20.0, spec.dt, nt), src_pos=src, rcv_pos=rcv,
+                interval=8, fpeak=20.0, name="vti_cfd")
+
+
+def tti_q(scale=1.0, seed=3, nt=5000, engine=ENGINE_FD8):
+    rng = np.random.default_rng(seed)
+    nx = max(32, int(round(640 * scale)))
+    nz = max(32, int(round(512 * scale)))
+    pml = max(6, int(round(32 * scale)))
+    spec = PropSpec(nx=nx, ny=nx, nz=nz, dx=10.0, dy=10.0, dz=10.0, dt=0.001, engine=engine, model_type=TTI,
+                    use_q=True, q_order=4, nbnd=(pml,) * 6, vmax=4500.0)
+    iz = np.arange(nz)
+    prof = (1500.0 + 3000.0 * iz / max(1, nz - 1)).astype(np.float32)
+    lat = smooth_field(spec.shape, 8.0, rng)
+    vel = np.clip(prof[None, None, :] * (1.0 + 0.03 * lat), 1500.0, 4500.0).astype(np.float32)
+    eps = minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 0.25)
+    dl = minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 0.10)
+    theta = np.deg2rad(minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 45.0))
+    phi = np.deg2rad(minmax(smooth_field(spec.shape, 8.0, rng), 0.0, 360.0))
+    pjx = (-np.sin(theta) * np.cos(phi)).astype(np.float32)   # bgprtm/ModelLoader.cpp:303-325
+    pjy = (-np.sin(theta) * np.sin(phi)).astype(np.float32)
+    q = minmax(smooth_field(spec.shape, 8.0, rng), 30.0, 200.0)
+    invq = (1.0 / q).astype(np.float32)
+    spec.dt = float(min(spec.dt, cfl_dt(spec, vel, eps, dl, pjx, pjy, invq, maxfreq=60.0)))
+    src = (nx / 2, nx / 2, pml + 1)
+    nr = max(4, int(round(128 * scale)))
+    step = max(1, (nx - 2) // nr)
+    rx = 1 + step * np.arange(nr)
+    rxx, ryy = np.meshgrid(rx, rx, indexing="xy")
+    rcv = np.stack([rxx.ravel(), ryy.ravel(), np.full(rxx.size, pml + 2.0)], 1).astype(np.float32)
+    return Shot(spec, nt, vel, eps=eps, dl=dl, pjx=pjx, pjy=pjy, invq=invq,
+                wavelet=ricker(20.0, spec.dt, nt), src_pos=src, rcv_pos=rcv, interval=8, fpeak=20.0,
+                name="tti_q")
+
+
+# Order-4 seed of Q::fitQCoeff for q_amp == 1 (bgprtm/Q.cpp:176-177) pushed
+# through the wave-equation transform of bgprtm/Q.cpp:275-290 (the levmar fit
+# itself is bypassed: fixed coefficients).
+Q_SEED4 = [2.0832741, -0.040106162, -0.21464862, -1.0239593, -9.7581205, 0.024538578, 0.18895587,
+           1.0043846, 6.2038145]
+
+
+def q_coefficients(dt, fdom, order=4):
+    c = np.array(Q_SEED4, np.float32)
+    w0_dt = np.float32(2 * np.pi) * np.float32(fdom) * np.float32(dt)
+    # the seed is taken as the fitted result (absolute w_l, as after postFitAdjust)
+    cq = c[1:order + 1].copy()
+    wq = c[order + 1:2 * order + 1].copy()
+    for i in range(order):
+        wn = wq[i] * w0_dt
+        cq[i] = cq[i] * np.float32(np.exp(-wn)) * 2 * w0_dt
+        wq[i] = np.float32(np.exp(-2 * wn))
+    return float(c[0]), cq.astype(np.float32), wq.astype(np.float32)

@@ -1,0 +1,874 @@
+// rtm_oracle.cpp - CPU restatement of bgprtm's propagation/imaging hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+// against; nothing in the product links, loads or calls it.  It restates the
+// reference's algorithm (citations are bgprtm file:line) in C++, templated on
+// the arithmetic type: Prop<float> follows the reference's FP32 expression
+// order, Prop<double> is the FP64 oracle the error of every result is stated
+// against.  Its entry points mirror include/rtm_b200.h with an "orc_" prefix
+// and a precision argument at creation.
+//
+// Parity of this restatement is pinned against the reference's own compiled
+// KernelCPU / FdEngine_fd / FdEngine_cfd / Cfd_plan / PML / WaveFieldCompress
+// (oracle/_ref, built by oracle/Makefile from the reference's sources) through
+// the golden fixtures in tests/golden.  The loop glue (update2nd, Vel2, Q,
+// Receiver::apply/extract_value, crossone) is restated from reference files
+// that do not compile and is pinned only through the same arithmetic.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "oracle_common.hpp"
+
+namespace orc {
+
+using std::max;
+using std::min;
+using std::vector;
+
+enum { ISO = 1, VTI = 2, TTI = 3 };
+enum { FD8 = 0, CFD = 1 };
+enum { X = 0, Y = 1, Z = 2 };
+enum { TOP = 0, BOT = 1 };
+
+struct Config {
+  int engine, model_type, use_q, q_order;
+  int nbnd[6];
+  float vmax, pml_eps;
+  int pml3d;
+  float pml3d_scaler;
+  int top_pml;
+};
+
+// Compact FD plan (bgprtm/Cfd_plan.cpp:54-290): B (9-band) LU factors bm
+// [n][5] (diag + 4 upper), bl [n][4] (multipliers), A boundary rows am[12][5].
+template <typename R> struct CfdPlan {
+  int n = 0;
+  vector<R> bm[2], bl[2], am[2];
+  void build(int n_, R d) {
+    n = n_;
+    for (int s = 0; s < 2; s++) {
+      bm[s].assign(5 * n, 0);
+      bl[s].assign(4 * n, 0);
+      am[s].assign(60, 0);
+      if (n > 1) plan(s + 1, d, bm[s], bl[s], am[s]);
+    }
+  }
+  // init_cfddev1 (bgprtm/Cfd_plan.cpp:127-290) + bandec (98-126) +
+  // reducematrix/cfd_transpose (72-96), restated.
+  void plan(int isgn, R dd, vector<R> &bmo, vector<R> &blo, vector<R> &am) {
+    const R ca5[5] = {(R)0.861085998189822, (R)0.753782983214427, (R)0.257072513289755,
+                      (R)0.031326722562826, (R)0.000410456919800};
+    const R cb5[5] = {(R)1.0, (R)0.753205475977546, (R)0.312203852849021,
+                      (R)0.063580085296350, (R)0.004597763362256};
+    R cb[9] = {cb5[4], cb5[3], cb5[2], cb5[1], cb5[0], cb5[1], cb5[2], cb5[3], cb5[4]};
+    R ca[11] = {-ca5[4], -ca5[3], -ca5[2], -ca5[1], -ca5[0], 0, ca5[0], ca5[1], ca5[2], ca5[3], ca5[4]};
+    vector<R> b(9 * n, 0), al(4 * n, 0);
+    const R refl = isgn == 1 ? R(-1) : R(1);  // boundary reflection sign of B
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 9; j++) {
+        int j1 = i - 4 + j;
+        if (j1 < 0) b[(4 - i - j1) * n + i] += refl * cb[j];
+        else b[j * n + i] += cb[j];
+      }
+    for (int i = 4; i < n - 4; i++)
+      for (int j = 0; j < 9; j++) b[j * n + i] = cb[j];
+    for (int i = n - 4; i < n; i++)
+      for (int j = 0; j < 9; j++) {
+        int j1 = i - 4 + j;
+        if (j1 > n - 1) b[((n + 3 - i) - (j1 - n + 1)) * n + i] += refl * cb[j];
+        else b[j * n + i] += cb[j];
+      }
+    const R arefl = isgn == 1 ? R(1) : R(-1);  // boundary reflection sign of A
+    for (int i = 0; i < 5; i++)
+      for (int j = 0; j < 11; j++) {
+        int j1 = i - 5 + j;
+        if (j1 < 0) am[(5 - i - j1) * 5 + i] += arefl * ca[j];
+        else am[j * 5 + i] += ca[j];
+      }
+    for (int i = 0; i < 5; i++) am[55 + i] = ca5[i];
+    for (int i = 0; i < 60; i++) am[i] = am[i] / dd * (R)0.5;
+    // band LU without pivoting, m1 = 4 sub-diagonals, storage a[band][n]
+    const int m1 = 4, mm = 9;
+    int l = m1;
+    for (int i = 0; i < m1; i++) {
+      for (int j = m1 - i; j < mm; j++) b[(j - l) * n + i] = b[j * n + i];
+      l--;
+      for (int j = mm - l - 1; j < mm; j++) b[j * n + i] = 0;
+    }
+    l = m1;
+    for (int k = 1; k <= n; k++) {
+      R dum = b[k - 1];
+      if (l < n) l++;
+      if (dum == 0) b[k - 1] = (R)1e-20;
+      for (int i = k + 1; i <= l; i++) {
+        dum = b[i - 1] / b[k - 1];
+        al[(i - k - 1) * n + k - 1] = dum;
+        for (int j = 2; j <= mm; j++) b[(j - 2) * n + i - 1] = b[(j - 1) * n + i - 1] - dum * b[(j - 1) * n + k - 1];
+        b[(mm - 1) * n + i - 1] = 0;
+      }
+    }
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < 5; j++) bmo[i * 5 + j] = b[j * n + i];
+      for (int j = 0; j < 4; j++) blo[i * 4 + j] = al[j * n + i];
+    }
+  }
+};
+
+// One strided line: RHS = A x (banmul_dev_z_c, bgprtm/FdEngine_cfd.cpp:304-327)
+// then the LU solve (banbks_dev_z_c, 328-356).  x[i*ld], out[i*ld].
+template <typename R>
+static void cfd_line(const CfdPlan<R> &p, int s, const R *x, R *b, size_t ld) {
+  const int n = p.n;
+  const R *a = p.am[s].data(), *bm = p.bm[s].data(), *al = p.bl[s].data();
+  for (int i = 0; i < 5; i++) {
+    R v = 0;
+    int k = i - 5;
+    for (int j = max(0, -k); j < 11; j++) v = v + a[j * 5 + i] * x[(j + k) * ld];
+    b[i * ld] = v;
+  }
+  for (int i = 5; i < n - 5; i++)
+    b[i * ld] = a[55] * (x[(i + 1) * ld] - x[(i - 1) * ld]) + a[56] * (x[(i + 2) * ld] - x[(i - 2) * ld]) +
+                a[57] * (x[(i + 3) * ld] - x[(i - 3) * ld]) + a[58] * (x[(i + 4) * ld] - x[(i - 4) * ld]) +
+                a[59] * (x[(i + 5) * ld] - x[(i - 5) * ld]);
+  for (int i = n - 5; i < n; i++) {
+    R v = 0;
+    int k = i - 5;
+    for (int j = 0; j < min(11, n - k); j++) v = v - a[n - i + 49 - 5 * j] * x[(j + k) * ld];
+    b[i * ld] = v;
+  }
+  for (int k = 0; k < n - 4; k++)
+    for (int j = 0; j < 4; j++) b[(j + k + 1) * ld] = b[(j + k + 1) * ld] - al[j + k * 4] * b[k * ld];
+  for (int k = n - 4; k < n; k++)
+    for (int j = 0; j < n - k - 1; j++) b[(j + k + 1) * ld] = b[(j + k + 1) * ld] - al[j + k * 4] * b[k * ld];
+  int l = 1;
+  for (int i = n - 1; i >= n - 4; i--) {
+    for (int k = 1; k < l; k++) b[i * ld] += -bm[i * 5 + k] * b[(k + i) * ld];
+    b[i * ld] = b[i * ld] / bm[i * 5];
+    if (l < 5) l++;
+  }
+  for (int i = n - 5; i >= 0; i--)
+    b[i * ld] = (b[i * ld] - bm[i * 5 + 1] * b[(i + 1) * ld] - bm[i * 5 + 2] * b[(i + 2) * ld] -
+                 bm[i * 5 + 3] * b[(i + 3) * ld] - bm[i * 5 + 4] * b[(i + 4) * ld]) /
+                bm[i * 5];
+}
+
+template <typename R> struct TraceSet {
+  int ntr = 0, lx = 0, ly = 0, lz = 0, nt = 0;
+  vector<int> off, len;
+  vector<R> kx, ky, kz, traces;
+  R scaler = 1;
+};
+
+template <typename R> class Prop {
+public:
+  int nx, ny, nz;
+  R dx, dy, dz, dt;
+  size_t nxz, nxyz;
+  Config cfg;
+  vector<R> w0, w1, vel, eps, del, pjx, pjy, invq, px, py, pz;
+  vector<R> wq[2];  // [order][nxyz] each
+  int iq0 = 0, iq1 = 1;
+  // FD tables: c1*[m], c2*[m] for m = 0..4 (m = 0 is the centre of c2)
+  R c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
+  CfdPlan<R> cfdx, cfdy, cfdz;
+  // PML: profile per dim/side (coef, distance from the outer edge) and memory
+  // pml[dim][side][round][comp] (bgprtm/FdEngine.h:178)
+  bool has_pml[3][2] = {};
+  int nb[3][2] = {};
+  vector<R> prof[3][2];
+  vector<R> pbuf[3][2][2][3];
+  int dimPML = 1;
+  // Q
+  R cq0 = 0, cqsum = 0;
+  vector<R> cq, cwq;
+  TraceSet<R> inj, ext;
+  vector<R> ext_out;
+  // snapshots and image
+  int snap_fmt = 0;
+  vector<vector<R>> snaps;
+  vector<vector<uint16_t>> snaps16;
+  vector<char> snap_valid;
+  vector<double> image;
+  int ic_ntaper_t = 0, ic_ntaper_z = 0, ic_edge = 1;
+  vector<R> taperT, taperZ;
+  vector<float> codec_table, wtaper20, wtaper10;
+
+  Prop(int nx_, int ny_, int nz_, R dx_, R dy_, R dz_, R dt_, const Config &c)
+      : nx(nx_), ny(ny_), nz(nz_), dx(dx_), dy(dy_), dz(dz_), dt(dt_), cfg(c) {
+    nxz = (size_t)nx * nz;
+    nxyz = nxz * ny;
+    w0.assign(nxyz, 0);
+    w1.assign(nxyz, 0);
+    vel.assign(nxyz, 0);
+    px.assign(nxyz, 0);
+    py.assign(nxyz, 0);
+    pz.assign(nxyz, 0);
+    build_fd();
+    if (cfg.engine == CFD) {
+      cfdx.build(nx, dx);
+      cfdy.build(ny, dy);
+      cfdz.build(nz, dz);
+    }
+    build_pml();
+    c16_tables(codec_table, wtaper20, wtaper10);
+  }
+
+  // FdEngine_fd constructor + setJacob (bgprtm/FdEngine_fd.cpp:30-54, 106-131),
+  // Taylor weights, const_ne, rectangular grid.  Float rounding as there.
+  void build_fd() {
+    double t1[5], t2[5];
+    taylor_weights(4, t1, t2);
+    R zpi = (R)1 / dz, zpi2 = zpi * zpi;
+    R dx2i = (R)(1. / (double)(dx * dx)), dy2i = (R)(1. / (double)(dy * dy));
+    R dxi = (R)1 / dx, dyi = (R)1 / dy;
+    for (int m = 0; m < 5; m++) {
+      R c2 = (R)t2[m];
+      c2z[m] = zpi2 * c2;
+      c2x[m] = c2 * dx2i;
+      c2y[m] = c2 * dy2i;
+      R c1 = m ? (R)t1[m] : (R)0;
+      c1z[m] = zpi * c1;
+      c1x[m] = c1 * dxi;
+      c1y[m] = c1 * dyi;
+    }
+  }
+
+  // FdEngine::setBoundary + PML::init (bgprtm/FdEngine.cpp:108-182,
+  // bgprtm/PML.cpp:87-124, limit_slope = false).
+  void build_pml() {
+    bool is2nd = (cfg.engine == FD8 && cfg.model_type == ISO);
+    dimPML = (!cfg.pml3d || is2nd) ? 1 : (ny == 1 ? 2 : 3);
+    const int nn[3] = {nx, ny, nz};
+    const R dd[3] = {dx, dy, dz};
+    for (int d = 0; d < 3; d++)
+      for (int s = 0; s < 2; s++) {
+        int w = cfg.nbnd[2 * d + s];
+        nb[d][s] = w;
+        has_pml[d][s] = w > 1 && !(d == Z && s == TOP && !cfg.top_pml);
+        if (has_pml[d][s]) {
+          prof[d][s].resize(w);
+          R beta = dd[d] / (dt * (R)cfg.vmax);
+          R dg1 = std::log((R)1 / (R)cfg.pml_eps) / ((R)w * beta);
+          for (int i = 0; i < w; i++) {
+            R temp = (R)(w - i) / (R)w;
+            prof[d][s][i] = (R)1.5 / 2 * temp * temp * dg1;
+          }
+        }
+        size_t plane = d == X ? (size_t)ny * nz : d == Y ? nxz : (size_t)nx * ny;
+        for (int r = 0; r < 2; r++)
+          for (int c = 0; c < 3; c++) pbuf[d][s][r][c].assign(w > 0 && c < dimPML ? (size_t)w * plane : 0, 0);
+      }
+    (void)nn;
+  }
+
+  void clean() {
+    std::fill(w0.begin(), w0.end(), 0);
+    std::fill(w1.begin(), w1.end(), 0);
+    for (int q = 0; q < 2; q++) std::fill(wq[q].begin(), wq[q].end(), 0);
+    for (auto &a : pbuf)
+      for (auto &b : a)
+        for (auto &c : b)
+          for (auto &v : c) std::fill(v.begin(), v.end(), 0);
+    std::fill(ext_out.begin(), ext_out.end(), 0);
+    iq0 = 0, iq1 = 1;
+  }
+
+  // PML::apply_single / apply_single_trans round (bgprtm/PML.cpp:126-134, 185-192)
+  static inline void pml_round(R g, R &p, R &q) {
+    R qi = ((R)1 - g) / ((R)1 + g) * q - g * (R)2 / ((R)1 - g * g) * p;
+    q = qi;
+    p = qi + p / ((R)1 - g);
+  }
+
+  // PML memory cell of (dim d, side s, round r, comp c) for grid cell (ix,iy,iz),
+  // and the damping g there (zero outside the layer).  Layouts follow
+  // bgprtm/FdEngine.cpp:324-350.
+  inline R *pml_cell(int d, int s, int r, int c, int ix, int iy, int iz, R &g) {
+    if (!has_pml[d][s]) return nullptr;
+    int w = nb[d][s];
+    if (d == Z) {
+      size_t ixy = (size_t)iy * nx + ix;
+      if (s == TOP) {
+        if (iz >= w) return nullptr;
+        g = prof[d][s][iz];
+        return &pbuf[d][s][r][c][ixy * w + iz];
+      }
+      if (iz < nz - w) return nullptr;
+      int i = iz - (nz - w);
+      g = prof[d][s][w - 1 - i];  // feoc
+      return &pbuf[d][s][r][c][ixy * w + i];
+    }
+    if (d == X) {
+      if (s == TOP) {
+        if (ix >= w) return nullptr;
+        g = prof[d][s][ix];
+        return &pbuf[d][s][r][c][((size_t)iy * w + ix) * nz + iz];
+      }
+      if (ix < nx - w) return nullptr;
+      g = prof[d][s][nx - 1 - ix];
+      return &pbuf[d][s][r][c][((size_t)iy * w + ix - nx + w) * nz + iz];
+    }
+    if (s == TOP) {
+      if (iy >= w) return nullptr;
+      g = prof[d][s][iy];
+      return &pbuf[d][s][r][c][((size_t)iy * nx + ix) * nz + iz];
+    }
+    if (iy < ny - w) return nullptr;
+    g = prof[d][s][ny - 1 - iy];
+    return &pbuf[d][s][r][c][((size_t)(iy - ny + w) * nx + ix) * nz + iz];
+  }
+
+  // two rounds along dim d (pml2_{z,x,y}bnd, bgprtm/FdEngine.cpp:352-389)
+  inline void pml2_dim(int d, R &p, int ix, int iy, int iz) {
+    for (int s = 0; s < 2; s++) {
+      R g;
+      R *q1 = pml_cell(d, s, 0, 0, ix, iy, iz, g);
+      if (!q1) continue;
+      R *q2 = pml_cell(d, s, 1, 0, ix, iy, iz, g);
+      pml_round(g, p, *q1);
+      pml_round(g, p, *q2);
+    }
+  }
+  // one round along dim d with component c and scaler (pml1_*bnd private,
+  // bgprtm/FdEngine.cpp:324-350)
+  inline void pml1_dim(int d, int c, R scaler, int round, R &p, int ix, int iy, int iz) {
+    for (int s = 0; s < 2; s++) {
+      R g;
+      R *q = pml_cell(d, s, round, c, ix, iy, iz, g);
+      if (!q) continue;
+      pml_round(g * scaler, p, *q);
+    }
+  }
+  // pml1_zbnd/xbnd/ybnd public (bgprtm/FdEngine.cpp:301-323): derivative along
+  // `axis`, own direction with scaler 1, the other two with pml3d_scaler.
+  inline void pml1(int axis, int round, R &p, int ix, int iy, int iz) {
+    R sc = (R)cfg.pml3d_scaler;
+    if (axis == Z) {
+      pml1_dim(Z, 0, 1, round, p, ix, iy, iz);
+      if (cfg.pml3d) pml1_dim(X, 1, sc, round, p, ix, iy, iz), pml1_dim(Y, 1, sc, round, p, ix, iy, iz);
+    } else if (axis == X) {
+      pml1_dim(X, 0, 1, round, p, ix, iy, iz);
+      if (cfg.pml3d) pml1_dim(Z, 1, sc, round, p, ix, iy, iz), pml1_dim(Y, 2, sc, round, p, ix, iy, iz);
+    } else {
+      pml1_dim(Y, 0, 1, round, p, ix, iy, iz);
+      if (cfg.pml3d && ny > 1) pml1_dim(Z, 2, sc, round, p, ix, iy, iz), pml1_dim(X, 2, sc, round, p, ix, iy, iz);
+    }
+  }
+
+  // FdEngine_fd::laplacian_irreg (bgprtm/FdEngine_fd.cpp:204-325) with the PML
+  // of KernelCPU's path, then applyVel_minus (bgprtm/KernelCPU.cpp:328-338):
+  // w0 -= vel * L[w1].
+  void iso_fd8_kernel() {
+    const R *u0 = w1.data();
+    bool skip_y = !(ny > 2);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        const R *u = u0 + iy * nxz + (size_t)ix * nz;
+        int nev0x = min(4, ix), nev1x = min(4, nx - 1 - ix);
+        int nev0y = min(4, iy), nev1y = min(4, ny - 1 - iy);
+        for (int iz = 0; iz < nz; iz++) {
+          R v = c2z[0] * u[iz];
+          for (int m = -4; m <= 4; m++) {
+            if (!m || iz + m < 0 || iz + m >= nz) continue;
+            v += c2z[m < 0 ? -m : m] * u[iz + m];
+          }
+          if (!cfg.pml3d) pml2_dim(Z, v, ix, iy, iz);
+          R bx = c2x[0] * u[iz];
+          for (int m = 1; m <= 4; m++) {
+            if (m <= nev0x) bx += c2x[m] * u[iz - m * nz];
+            if (m <= nev1x) bx += c2x[m] * u[iz + m * nz];
+          }
+          if (!cfg.pml3d) pml2_dim(X, bx, ix, iy, iz);
+          v += bx;
+          if (!skip_y) {
+            R by = c2y[0] * u[iz];
+            for (int m = 1; m <= 4; m++) {
+              if (m <= nev0y) by += c2y[m] * u[iz - m * nxz];
+              if (m <= nev1y) by += c2y[m] * u[iz + m * nxz];
+            }
+            if (!cfg.pml3d) pml2_dim(Y, by, ix, iy, iz);
+            v += by;
+          }
+          if (cfg.pml3d) {
+            pml2_dim(Z, v, ix, iy, iz);
+            pml2_dim(X, v, ix, iy, iz);
+            pml2_dim(Y, v, ix, iy, iz);
+          }
+          size_t i = iy * nxz + (size_t)ix * nz + iz;
+          w0[i] = w0[i] - v * vel[i];
+        }
+      }
+  }
+
+  // FD8 first derivative of `in` along `axis` at (ix,iy,iz), taps outside the
+  // grid dropped (dxyz1_nz, bgprtm/FdEngine_fd.cpp:394-469).
+  inline R d1_fd(const R *in, int axis, int ix, int iy, int iz) const {
+    size_t i = (size_t)iy * nxz + (size_t)ix * nz + iz;
+    R v = 0;
+    if (axis == Z) {
+      for (int m = -4; m <= 4; m++) {
+        if (!m || iz + m < 0 || iz + m >= nz) continue;
+        v += (m < 0 ? -c1z[-m] : c1z[m]) * in[i + m];
+      }
+    } else {
+      int p = axis == X ? ix : iy, n = axis == X ? nx : ny;
+      size_t st = axis == X ? (size_t)nz : nxz;
+      const R *c = axis == X ? c1x : c1y;
+      int nev0 = min(4, p), nev1 = min(4, n - 1 - p);
+      for (int m = 1; m <= 4; m++) {
+        if (m <= nev0) v -= c[m] * in[i - m * st];
+        if (m <= nev1) v += c[m] * in[i + m * st];
+      }
+    }
+    return v;
+  }
+
+  // derivative of a whole volume along axis, PML round `round`, then either
+  // store (iacc = 0) or out -= deriv * vel (iacc = 1).
+  void deriv_volume(const R *in, R *out, int axis, int round, int iacc) {
+    if (cfg.engine == FD8) {
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx; ix++)
+          for (int iz = 0; iz < nz; iz++) {
+            R v = d1_fd(in, axis, ix, iy, iz);
+            pml1(axis, round, v, ix, iy, iz);
+            size_t i = iy * nxz + (size_t)ix * nz + iz;
+            if (iacc) out[i] = out[i] - v * vel[i];
+            else out[i] = v;
+          }
+      return;
+    }
+    // CFD: solve along lines, then PML and accumulate (FdEngine_cfd.cpp:83-153)
+    vector<R> d(nxyz);
+    const CfdPlan<R> &p = axis == X ? cfdx : axis == Y ? cfdy : cfdz;
+    int s = round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
+    if (axis == Z) {
+#pragma omp parallel for schedule(static)
+      for (long c = 0; c < (long)nx * ny; c++) cfd_line(p, s, in + c * nz, d.data() + c * nz, 1);
+    } else if (axis == X) {
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int iy = 0; iy < ny; iy++)
+        for (int iz = 0; iz < nz; iz++) cfd_line(p, s, in + iy * nxz + iz, d.data() + iy * nxz + iz, nz);
+    } else {
+#pragma omp parallel for collapse(2) schedule(static)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++)
+          cfd_line(p, s, in + (size_t)ix * nz + iz, d.data() + (size_t)ix * nz + iz, nxz);
+    }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+          size_t i = iy * nxz + (size_t)ix * nz + iz;
+          R v = d[i];
+          pml1(axis, round, v, ix, iy, iz);
+          if (iacc) out[i] = out[i] - v * vel[i];
+          else out[i] = v;
+        }
+  }
+
+  // ScalarTTI / ScalarVTI (bgprtm/KernelCPU.cpp:176-297), 3-D forms.
+  void scale_gradient() {
+    const R one = 1, two = 2, eight = 8, half = 0.5, small = (R)1e-32;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nxyz; i++) {
+      R e = eps[i];
+      R dl = e - del[i];
+      e = one + two * e;
+      R vx = px[i], vy = ny > 1 ? py[i] : 0, vz = pz[i];
+      if (cfg.model_type == TTI) {
+        R ax = pjx[i], ay = ny > 1 ? pjy[i] : 0;
+        R az = std::sqrt(one - (ax * ax + ay * ay));
+        R v2 = vx * vx + vy * vy + vz * vz;
+        R vzz = vx * ax + vy * ay + vz * az;
+        R vz2 = vzz * vzz;
+        R vh2 = v2 - vz2;
+        R ecl = e * vh2 + vz2;
+        R parts = std::sqrt(one - eight * (dl * (vh2 * vz2)) / (ecl * ecl + small));
+        R sc = min(half * (one + parts), one);
+        ax = vzz * ax, ay = vzz * ay, az = vzz * az;
+        px[i] = (ax + (vx - ax) * e) * sc;
+        if (ny > 1) py[i] = (ay + (vy - ay) * e) * sc;
+        pz[i] = (az + (vz - az) * e) * sc;
+      } else {
+        R vx2 = vx * vx + vy * vy;
+        R vz2 = vz * vz;
+        R ecl = e * vx2 + vz2;
+        R parts = std::sqrt(one - eight * (dl * (vx2 * vz2)) / (ecl * ecl + small));
+        R sc2 = e * min(half * (one + parts), one);
+        px[i] = vx * sc2;
+        if (ny > 1) py[i] = vy * sc2;
+      }
+    }
+  }
+
+  // KernelCPU::TTI (bgprtm/KernelCPU.cpp:93-119): gradient with PML round 1,
+  // pseudo-acoustic scaling, divergence accumulated into w0 with PML round 2.
+  void aniso_kernel() {
+    if (ny > 1) deriv_volume(w1.data(), py.data(), Y, 0, 0);
+    deriv_volume(w1.data(), pz.data(), Z, 0, 0);
+    deriv_volume(w1.data(), px.data(), X, 0, 0);
+    if (cfg.model_type == TTI || cfg.model_type == VTI) scale_gradient();
+    deriv_volume(px.data(), w0.data(), X, 1, 1);
+    deriv_volume(pz.data(), w0.data(), Z, 1, 1);
+    if (ny > 1) deriv_volume(py.data(), w0.data(), Y, 1, 1);
+  }
+
+  void kernel() {
+    if (cfg.engine == FD8 && cfg.model_type == ISO) iso_fd8_kernel();
+    else aniso_kernel();
+  }
+
+  // Propagator::update2nd (bgprtm/Propagator.cpp:1767-1818)
+  void update2nd() {
+    if (!cfg.use_q) {
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < (long)nxyz; i++) w0[i] = (w1[i] + w1[i]) - w0[i];
+      return;
+    }
+    int L = cfg.q_order;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nxyz; i++) {
+      R v = w1[i] * ((R)2 + invq[i] * cqsum) - w0[i];
+      for (int l = 0; l < L; l++) {
+        R &d0 = wq[iq0][(size_t)l * nxyz + i];
+        R d1 = wq[iq1][(size_t)l * nxyz + i];
+        R el = cwq[l];
+        v += invq[i] * (((R)1 + el) * d0 - d1 * (R)2);
+        d0 = cq[l] * w1[i] + el * d0;
+      }
+      w0[i] = v;
+    }
+  }
+
+  void swap() {
+    std::swap(w0, w1);
+    std::swap(iq0, iq1);
+  }
+
+  // Propagator::Vel2 (bgprtm/Propagator.cpp:711-742)
+  void set_model(const float *v, const float *e, const float *d, const float *ax, const float *ay, const float *iq) {
+    R dt2 = dt * dt;
+    if (cfg.model_type >= VTI) {
+      eps.assign(e, e + nxyz);
+      del.assign(d, d + nxyz);
+    }
+    if (cfg.model_type == TTI) {
+      pjx.assign(ax, ax + nxyz);
+      if (ny > 1) pjy.assign(ay, ay + nxyz);
+    }
+    if (cfg.use_q) {
+      invq.resize(nxyz);
+      for (int q = 0; q < 2; q++) wq[q].assign((size_t)cfg.q_order * nxyz, 0);
+    }
+    for (size_t i = 0; i < nxyz; i++) {
+      R vv = v[i];
+      if (!cfg.use_q) {
+        vel[i] = vv * vv * dt2;
+      } else {
+        R q = iq[i], q2 = q * q;
+        R corr = (R)1 / ((R)1 - cq0 * q);
+        vel[i] = vv * vv * dt2 * ((R)1 - (R)0.25 * q2 + q2 * q2 / (R)48) * corr;
+        invq[i] = q * corr;
+      }
+    }
+  }
+
+  void set_traces(TraceSet<R> &t, int ntr, int lx, int ly, int lz, const int *off, const int *len, const float *kx,
+                  const float *ky, const float *kz, const float *tr, int nt, float scaler) {
+    t.ntr = ntr, t.lx = lx, t.ly = ly, t.lz = lz, t.nt = nt;
+    t.off.assign(off, off + 3 * ntr);
+    t.len.assign(len, len + 3 * ntr);
+    t.kx.assign(kx, kx + (size_t)ntr * lx);
+    t.ky.assign(ky, ky + (size_t)ntr * ly);
+    t.kz.assign(kz, kz + (size_t)ntr * lz);
+    if (tr) t.traces.assign(tr, tr + (size_t)ntr * nt);
+    t.scaler = scaler;
+  }
+
+  // Receiver::apply_src (bgprtm/Receiver.cpp:477-507), traces in order.
+  void inject(int it) {
+    if (it < 0 || it >= inj.nt) return;
+    for (int r = 0; r < inj.ntr; r++) {
+      R val = inj.traces[(size_t)r * inj.nt + it] * inj.scaler;
+      const int *o = &inj.off[3 * r], *l = &inj.len[3 * r];
+      for (int iy = 0; iy < l[1]; iy++) {
+        R cy = val * inj.ky[(size_t)r * inj.ly + iy];
+        for (int ix = 0; ix < l[0]; ix++) {
+          R cx = cy * inj.kx[(size_t)r * inj.lx + ix];
+          size_t off = ((size_t)(iy + o[1]) * nx + ix + o[0]) * nz + o[2];
+          for (int iz = 0; iz < l[2]; iz++) w0[off + iz] += cx * inj.kz[(size_t)r * inj.lz + iz] * vel[off + iz];
+        }
+      }
+    }
+  }
+
+  // Receiver::extract_value (bgprtm/Receiver.cpp:394-426), no mirror ghost.
+  void extract(int jt) {
+    if (jt < 0 || jt >= ext.nt) return;
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < ext.ntr; r++) {
+      R val = 0;
+      const int *o = &ext.off[3 * r], *l = &ext.len[3 * r];
+      for (int iy = 0; iy < l[1]; iy++) {
+        R cy = ext.ky[(size_t)r * ext.ly + iy];
+        for (int ix = 0; ix < l[0]; ix++) {
+          R cx = cy * ext.kx[(size_t)r * ext.lx + ix];
+          size_t off = ((size_t)(iy + o[1]) * nx + ix + o[0]) * nz + o[2];
+          for (int iz = 0; iz < l[2]; iz++) val += cx * ext.kz[(size_t)r * ext.lz + iz] * w0[off + iz];
+        }
+      }
+      ext_out[(size_t)r * ext.nt + jt] = val;
+    }
+  }
+
+  // decode taper factor (WaveFieldCompress::uncompress16, bgprtm/WaveFieldCompress.cpp:185-201)
+  inline R edge(R v, int ix, int iy, int iz) const {
+    if (ny > 40) {
+      if (iy < 20) v *= (R)wtaper20[iy];
+      if (iy > ny - 21) v *= (R)wtaper20[ny - iy - 1];
+    }
+    if (nx > 40) {
+      if (ix < 20) v *= (R)wtaper20[ix];
+      if (ix > nx - 21) v *= (R)wtaper20[nx - ix - 1];
+    }
+    if (nz > 20) {
+      if (iz < 10) v *= (R)wtaper10[iz];
+      if (iz > nz - 11) v *= (R)wtaper10[nz - iz - 1];
+    }
+    return v;
+  }
+
+  void snapshot_setup(int fmt, int n) {
+    snap_fmt = fmt;
+    snaps.assign(fmt == 0 ? n : 0, vector<R>());
+    snaps16.assign(fmt == 1 ? n : 0, vector<uint16_t>());
+    snap_valid.assign(n, 0);
+  }
+  void snapshot_store(int slot) {
+    if (slot < 0 || slot >= (int)snap_valid.size()) return;
+    if (snap_fmt == 0) snaps[slot] = w0;
+    else {
+      vector<float> f(w0.begin(), w0.end());
+      snaps16[slot].resize((nxz + 2) * ny);
+      c16_compress(f.data(), snaps16[slot].data(), nx, ny, nz);
+    }
+    snap_valid[slot] = 1;
+  }
+  // decoded snapshot with the decode tapers (edge) applied
+  void snapshot_decode(int slot, vector<R> &out) {
+    out.resize(nxyz);
+    if (snap_fmt == 0) {
+      for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx; ix++)
+          for (int iz = 0; iz < nz; iz++) {
+            size_t i = iy * nxz + (size_t)ix * nz + iz;
+            out[i] = ic_edge ? edge(snaps[slot][i], ix, iy, iz) : snaps[slot][i];
+          }
+    } else {
+      vector<float> f(nxyz);
+      c16_uncompress(snaps16[slot].data(), f.data(), nx, ny, nz, codec_table.data(), wtaper20.data(),
+                     wtaper10.data(), ic_edge);
+      out.assign(f.begin(), f.end());
+    }
+  }
+
+  // ImagingCondition::calTapes (bgprtm/ImagingCondition.cpp:180-198)
+  void image_setup(int ntt, int ntz, int edge_) {
+    ic_ntaper_t = ntt, ic_ntaper_z = ntz, ic_edge = edge_;
+    taperT.resize(ntt), taperZ.resize(ntz);
+    for (int i = 0; i < ntt; i++) taperT[i] = (R)0.5 * ((R)1 - std::cos((R)M_PI * (R)i / (R)ntt));
+    for (int i = 0; i < ntz; i++) taperZ[i] = (R)0.5 * ((R)1 - std::cos((R)M_PI * (R)i / (R)ntz));
+    image.assign(nxyz, 0);
+  }
+  // applyTape (ImagingCondition.cpp:200-226) on the source snapshot, decode
+  // tapers on the receiver field, then crossone (ImagingCorrelator.cpp:180-194).
+  void image_accumulate(int slot) {
+    if (slot < 0 || slot >= (int)snap_valid.size() || !snap_valid[slot]) return;
+    vector<R> s;
+    snapshot_decode(slot, s);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+          size_t i = iy * nxz + (size_t)ix * nz + iz;
+          R sv = s[i];
+          if (slot < ic_ntaper_t) sv *= taperT[slot];
+          else if (iz < ic_ntaper_z) sv *= taperZ[iz];
+          R rv = ic_edge ? edge(w0[i], ix, iy, iz) : w0[i];
+          image[i] += (double)(sv * rv);
+        }
+  }
+
+  void modelling(int nts, int it_shift, int ntratio) {
+    for (int it = 0; it < nts; it++) {
+      kernel();
+      update2nd();
+      inject(it + it_shift);
+      if (it % ntratio == 0) extract(it / ntratio);
+      swap();
+    }
+  }
+  void migration(int dir, int it_begin, int it_end, int it_shift, int interval) {
+    int inc = dir == 0 ? 1 : -1;
+    for (int it = it_begin; it != it_end; it += inc) {
+      kernel();
+      update2nd();
+      inject(it + it_shift * inc);
+      if (it % interval == 0) {
+        int slot = it / interval;
+        if (dir == 0) snapshot_store(slot);
+        else image_accumulate(slot);
+      }
+      swap();
+    }
+  }
+};
+
+struct Handle {
+  int prec;  // 0 float, 1 double
+  std::unique_ptr<Prop<float>> f;
+  std::unique_ptr<Prop<double>> d;
+};
+
+}  // namespace orc
+
+using orc::Handle;
+
+#define DISPATCH(h, call) ((h)->prec ? (h)->d->call : (h)->f->call)
+
+extern "C" {
+
+void *orc_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt, int engine, int model_type,
+                 int use_q, int q_order, const int *nbnd, float vmax, float pml_eps, int pml3d, float pml3d_scaler,
+                 int top_pml, int prec) {
+  orc::Config c{engine, model_type, use_q, q_order, {0}, vmax, pml_eps, pml3d, pml3d_scaler, top_pml};
+  for (int i = 0; i < 6; i++) c.nbnd[i] = nbnd[i];
+  Handle *h = new Handle();
+  h->prec = prec;
+  if (prec) h->d.reset(new orc::Prop<double>(nx, ny, nz, dx, dy, dz, dt, c));
+  else h->f.reset(new orc::Prop<float>(nx, ny, nz, dx, dy, dz, dt, c));
+  return h;
+}
+void orc_destroy(void *p) { delete (Handle *)p; }
+
+void orc_set_q_coeffs(void *p, float cq0, const float *cq, const float *wq) {
+  Handle *h = (Handle *)p;
+  auto set = [&](auto &pr) {
+    int L = pr.cfg.q_order;
+    pr.cq0 = cq0;
+    pr.cq.assign(cq, cq + L);
+    pr.cwq.assign(wq, wq + L);
+    pr.cqsum = 0;
+    for (int i = 0; i < L; i++) pr.cqsum += pr.cq[i];
+  };
+  if (h->prec) set(*h->d);
+  else set(*h->f);
+}
+void orc_set_model(void *p, const float *v, const float *e, const float *d, const float *ax, const float *ay,
+                   const float *iq) {
+  DISPATCH((Handle *)p, set_model(v, e, d, ax, ay, iq));
+}
+void orc_reset(void *p) { DISPATCH((Handle *)p, clean()); }
+void orc_kernel(void *p) { DISPATCH((Handle *)p, kernel()); }
+void orc_update2nd(void *p) { DISPATCH((Handle *)p, update2nd()); }
+void orc_swap(void *p) { DISPATCH((Handle *)p, swap()); }
+void orc_set_injection(void *p, int ntr, int lx, int ly, int lz, const int *off, const int *len, const float *kx,
+                       const float *ky, const float *kz, const float *tr, int nt, float scaler) {
+  Handle *h = (Handle *)p;
+  if (h->prec) h->d->set_traces(h->d->inj, ntr, lx, ly, lz, off, len, kx, ky, kz, tr, nt, scaler);
+  else h->f->set_traces(h->f->inj, ntr, lx, ly, lz, off, len, kx, ky, kz, tr, nt, scaler);
+}
+void orc_set_extraction(void *p, int ntr, int lx, int ly, int lz, const int *off, const int *len, const float *kx,
+                        const float *ky, const float *kz, int nt_out) {
+  Handle *h = (Handle *)p;
+  auto set = [&](auto &pr) {
+    pr.set_traces(pr.ext, ntr, lx, ly, lz, off, len, kx, ky, kz, nullptr, nt_out, 1.0f);
+    pr.ext_out.assign((size_t)ntr * nt_out, 0);
+  };
+  if (h->prec) set(*h->d);
+  else set(*h->f);
+}
+void orc_inject(void *p, int it) { DISPATCH((Handle *)p, inject(it)); }
+void orc_extract(void *p, int jt) { DISPATCH((Handle *)p, extract(jt)); }
+void orc_get_traces(void *p, float *dst) {
+  Handle *h = (Handle *)p;
+  if (h->prec) std::copy(h->d->ext_out.begin(), h->d->ext_out.end(), dst);
+  else std::copy(h->f->ext_out.begin(), h->f->ext_out.end(), dst);
+}
+void orc_snapshot_setup(void *p, int fmt, int n) { DISPATCH((Handle *)p, snapshot_setup(fmt, n)); }
+void orc_snapshot_store(void *p, int slot) { DISPATCH((Handle *)p, snapshot_store(slot)); }
+void orc_image_setup(void *p, int ntt, int ntz, int edge) { DISPATCH((Handle *)p, image_setup(ntt, ntz, edge)); }
+void orc_image_accumulate(void *p, int slot) { DISPATCH((Handle *)p, image_accumulate(slot)); }
+void orc_modelling(void *p, int nts, int it_shift, int ntratio) {
+  DISPATCH((Handle *)p, modelling(nts, it_shift, ntratio));
+}
+void orc_migration(void *p, int dir, int it_begin, int it_end, int it_shift, int interval) {
+  DISPATCH((Handle *)p, migration(dir, it_begin, it_end, it_shift, interval));
+}
+// field: 0 w0, 1 w1, 2 vel, 3 image, 4 invq; writes double precision values
+void orc_get(void *p, int field, double *dst) {
+  Handle *h = (Handle *)p;
+  auto get = [&](auto &pr) {
+    switch (field) {
+    case 0: std::copy(pr.w0.begin(), pr.w0.end(), dst); break;
+    case 1: std::copy(pr.w1.begin(), pr.w1.end(), dst); break;
+    case 2: std::copy(pr.vel.begin(), pr.vel.end(), dst); break;
+    case 3: std::copy(pr.image.begin(), pr.image.end(), dst); break;
+    case 4: std::copy(pr.invq.begin(), pr.invq.end(), dst); break;
+    }
+  };
+  if (h->prec) get(*h->d);
+  else get(*h->f);
+}
+void orc_put(void *p, int field, const float *src) {
+  Handle *h = (Handle *)p;
+  auto put = [&](auto &pr) {
+    auto &v = field == 0 ? pr.w0 : pr.w1;
+    std::copy(src, src + pr.nxyz, v.begin());
+  };
+  if (h->prec) put(*h->d);
+  else put(*h->f);
+}
+void orc_snapshot_load(void *p, int slot, double *dst) {
+  Handle *h = (Handle *)p;
+  auto ld = [&](auto &pr) {
+    using R = typename std::remove_reference<decltype(pr.w0[0])>::type;
+    std::vector<R> out;
+    pr.snapshot_decode(slot, out);
+    std::copy(out.begin(), out.end(), dst);
+  };
+  if (h->prec) ld(*h->d);
+  else ld(*h->f);
+}
+
+// Standalone restated helpers (bgprtm/Util.cpp:317-397, Receiver.cpp:291-303,
+// WaveFieldCompress.cpp:52-207).
+int orc_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper, float *coeff) {
+  return orc::spread_coeffs(n, x, k1, k2, nlimit, dipole, ntaper, coeff);
+}
+void orc_c16_compress(const float *in, unsigned short *out, int nx, int ny, int nz) {
+  orc::c16_compress(in, out, nx, ny, nz);
+}
+void orc_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int nz) {
+  std::vector<float> t, a, b;
+  orc::c16_tables(t, a, b);
+  orc::c16_uncompress(in, out, nx, ny, nz, t.data(), a.data(), b.data(), 1);
+}
+void orc_taylor_weights(int ne, double *c1, double *c2) { orc::taylor_weights(ne, c1, c2); }
+// The CFD plan factors of one axis (plan s = 0 for isign 1, 1 for isign -1).
+void orc_cfd_plan(int n, float d, int s, float *bm, float *bl, float *am) {
+  orc::CfdPlan<float> p;
+  p.build(n, d);
+  std::copy(p.bm[s].begin(), p.bm[s].end(), bm);
+  std::copy(p.bl[s].begin(), p.bl[s].end(), bl);
+  std::copy(p.am[s].begin(), p.am[s].end(), am);
+}
+}

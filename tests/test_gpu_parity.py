@@ -1,0 +1,198 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference's own kernels (golden fixtures), on seeded inputs.
+
+Tolerances (relative L2):
+  * FD8 operator steps vs the FP32 oracle / reference: 2e-6 (FP32 rounding);
+  * compact FD: the FP32 band-LU solve amplifies rounding; the GPU builds its
+    plan in FP64, so its bound is 2x the reference's own FP32-vs-FP64 spread;
+  * receiver traces and images after hundreds of steps: 1e-4 vs the FP32
+    oracle, and the error against the FP64 oracle is asserted below 1e-4 too.
+"""
+import numpy as np
+import pytest
+
+from konglong_b200 import workloads as W
+from konglong_b200.propagator import Propagator, c16_compress, c16_uncompress, spread_coeffs
+from konglong_b200.spec import (BACKWARD, ENGINE_CFD, ENGINE_FD8, FIELD_IMAGE, FIELD_W1, FORWARD, ISO,
+                                SNAP_C16, SNAP_FP16S, SNAP_FP32, TTI, VTI, PropSpec)
+from oracle import pyoracle as O
+from tests.conftest import rel_l2
+from tests.golden_inputs import CASES, case_inputs, codec_input
+
+pytestmark = pytest.mark.gpu
+
+
+def _steps(x, n):
+    for _ in range(n):
+        x.kernel()
+        x.update2nd()
+        x.swap()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_operator_steps_match_oracle_and_reference(golden, name):
+    c = CASES[name]
+    spec, model, w0, w1 = case_inputs(c)
+    g = Propagator(spec)
+    g.set_model(**model)
+    g.put(0, w0)
+    g.put(1, w1)
+    _steps(g, c["steps"])
+    got = g.get(FIELD_W1)
+    o = O.Oracle(spec)
+    o.set_model(**model)
+    o.put(0, w0)
+    o.put(1, w1)
+    _steps(o, c["steps"])
+    want = o.get(1)
+    ref = golden[f"{name}__w1"]
+    if spec.engine == ENGINE_FD8:
+        assert rel_l2(got, want) < 2e-6
+        assert rel_l2(got, ref) < 2e-6
+    else:
+        d = O.Oracle(spec, double=True)
+        d.set_model(**model)
+        d.put(0, w0)
+        d.put(1, w1)
+        _steps(d, c["steps"])
+        exact = d.get(1)
+        spread = rel_l2(ref, exact)
+        assert rel_l2(got, exact) < 2 * spread + 1e-6
+        assert rel_l2(got, ref) < 3 * spread + 1e-6
+
+
+def _shot_setup(shot, x, coeff_fn):
+    s = shot.spec
+    x.set_model(**shot.model_arrays())
+    k1, k2 = W.spread_band(s)
+    src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, coeff_fn)
+    rcv = W.make_traceset(shot.rcv_pos, s.nx, s.ny, s.nz, 10, k1, k2, coeff_fn)
+    return src, rcv
+
+
+def _modelling(shot, x, coeff_fn, nts):
+    src, rcv = _shot_setup(shot, x, coeff_fn)
+    x.set_injection(src, shot.wavelet[None, :], shot.spec.dt_dxyz)
+    x.set_extraction(rcv, nts)
+    x.reset()
+    x.modelling(nts, -1, 1)
+    return x.traces()
+
+
+@pytest.mark.parametrize("builder,scale,nts", [(W.iso128, 0.375, 300), (W.vti_cfd, 0.1, 200),
+                                               (W.tti_q, 0.08, 150)])
+def test_modelling_traces(builder, scale, nts):
+    shot = builder(scale=scale, nt=nts)
+    if shot.spec.use_q:
+        cq0, cq, wq = W.q_coefficients(shot.spec.dt, shot.fpeak)
+    g = Propagator(shot.spec)
+    if shot.spec.use_q:
+        g.set_q_coeffs(cq0, cq, wq)
+    got = _modelling(shot, g, spread_coeffs, nts)
+    o = O.Oracle(shot.spec)
+    d = O.Oracle(shot.spec, double=True)
+    if shot.spec.use_q:
+        o.set_q_coeffs(cq0, cq, wq)
+        d.set_q_coeffs(cq0, cq, wq)
+    want = _modelling(shot, o, spread_coeffs, nts)
+    exact = _modelling(shot, d, spread_coeffs, nts)
+    assert np.abs(want).max() > 0
+    if shot.spec.engine == ENGINE_FD8:
+        assert rel_l2(got, want) < 1e-4
+        assert rel_l2(got, exact) < 1e-4
+    else:
+        spread = rel_l2(want, exact)
+        assert rel_l2(got, exact) < 2 * spread + 1e-5
+
+
+def _rtm(shot, x, coeff_fn, fmt, nt, nts_fwd, interval):
+    src, rcv = _shot_setup(shot, x, coeff_fn)
+    rng = np.random.default_rng(7)
+    data = (rng.standard_normal((rcv.ntr, nt)) * 1e3).astype(np.float32)
+    nslots = (nts_fwd - 1) // interval + 1
+    x.snapshot_setup(fmt, nslots)
+    x.reset()
+    x.set_injection(src, shot.wavelet[None, :], shot.spec.dt_dxyz)
+    x.migration(FORWARD, 0, nts_fwd, -1, interval)
+    x.reset()
+    x.image_setup(3, 4, 1)
+    x.set_injection(rcv, data, shot.spec.dt_dxyz)
+    x.migration(BACKWARD, nt - 1, -1, -1, interval)
+    return x.get(FIELD_IMAGE if isinstance(x, Propagator) else 3)
+
+
+@pytest.mark.parametrize("fmt,tol", [(SNAP_FP32, 1e-4), (SNAP_C16, 2e-3)])
+def test_rtm_image_iso(fmt, tol):
+    shot = W.iso128(scale=0.375, nt=240)
+    nt, nts, k = 240, 168, 4
+    g = Propagator(shot.spec)
+    got = _rtm(shot, g, spread_coeffs, fmt, nt, nts, k)
+    o = O.Oracle(shot.spec)
+    want = _rtm(shot, o, spread_coeffs, fmt, nt, nts, k)
+    assert np.abs(want).max() > 0
+    assert rel_l2(got, want) < tol
+    if fmt == SNAP_FP32:
+        d = O.Oracle(shot.spec, double=True)
+        exact = _rtm(shot, d, spread_coeffs, fmt, nt, nts, k)
+        assert rel_l2(got, exact) < 1e-4
+
+
+def test_rtm_image_fp16_snapshots_close_to_fp32():
+    shot = W.iso128(scale=0.375, nt=160)
+    a = _rtm(shot, Propagator(shot.spec), spread_coeffs, SNAP_FP32, 160, 112, 4)
+    b = _rtm(shot, Propagator(shot.spec), spread_coeffs, SNAP_FP16S, 160, 112, 4)
+    assert rel_l2(b, a) < 2e-3
+
+
+def test_codec_on_device_bit_exact(golden):
+    for cname, (a, nx, ny, nz) in codec_input().items():
+        codes = c16_compress(a, nx, ny, nz)
+        np.testing.assert_array_equal(codes, golden[f"c16_{cname}__codes"])
+        dec = c16_uncompress(codes, nx, ny, nz)
+        np.testing.assert_array_equal(dec.view(np.uint32), O.c16_uncompress(codes, nx, ny, nz).view(np.uint32))
+
+
+def test_grouped_injection_and_extraction_match_per_trace():
+    """Many receivers on one depth take the grouped (xy gather) path; the
+    oracle applies Receiver::apply_src trace by trace."""
+    spec = PropSpec(nx=64, ny=48, nz=40, nbnd=(8,) * 6)
+    rng = np.random.default_rng(4)
+    vel = (2000 + 1000 * rng.random(spec.shape)).astype(np.float32)
+    xs, ys = np.meshgrid(1.5 + 2 * np.arange(30), 1.5 + 2 * np.arange(22))
+    pts = np.stack([xs.ravel(), ys.ravel(), np.full(xs.size, 10.0)], 1)
+    k1, k2 = W.spread_band(spec)
+    ts = W.make_traceset(pts, spec.nx, spec.ny, spec.nz, 10, k1, k2, spread_coeffs)
+    traces = rng.standard_normal((ts.ntr, 5)).astype(np.float32)
+    out = []
+    for x in (Propagator(spec), O.Oracle(spec)):
+        x.set_model(vel=vel)
+        x.set_injection(ts, traces, 1.0)
+        x.set_extraction(ts, 5)
+        x.reset()
+        for it in range(5):
+            x.inject(it)
+            x.extract(it)
+        out.append((x.get(0), x.traces()))
+    assert rel_l2(out[0][0], out[1][0]) < 1e-6
+    assert rel_l2(out[0][1], out[1][1]) < 1e-6
+
+
+def test_fused_loop_equals_stepwise_calls():
+    shot = W.iso128(scale=0.25, nt=40)
+    s = shot.spec
+    k1, k2 = W.spread_band(s)
+    src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    a = Propagator(s)
+    b = Propagator(s)
+    for x in (a, b):
+        x.set_model(vel=shot.vel)
+        x.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
+        x.reset()
+    a.set_extraction(src, 40)
+    a.modelling(40, -1, 1)
+    for it in range(40):
+        b.kernel()
+        b.update2nd()
+        b.inject(it - 1)
+        b.swap()
+    assert rel_l2(a.get(FIELD_W1), b.get(FIELD_W1)) < 1e-6

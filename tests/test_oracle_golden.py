@@ -1,0 +1,109 @@
+"""The oracle (CPU restatement) against the reference's own compiled kernels.
+
+Fixtures come from oracle/_ref (bgprtm's KernelCPU / FdEngine_fd /
+FdEngine_cfd / Cfd_plan / PML / WaveFieldCompress built from source), see
+tests/golden/make_golden.py.  FD8 must agree to FP32 rounding; the compact-FD
+line solve (band LU without pivoting, pivots down to ~0.016) amplifies FP32
+rounding, so its bound is the reference's own FP32-vs-FP64 spread.
+"""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as O
+from tests.conftest import rel_l2
+from tests.golden_inputs import CASES, case_inputs, codec_input
+
+FD8_TOL = 2e-6
+
+
+def run_oracle(c, double=False):
+    spec, model, w0, w1 = case_inputs(c)
+    o = O.Oracle(spec, double=double)
+    o.set_model(**model)
+    o.put(0, w0)
+    o.put(1, w1)
+    for _ in range(c["steps"]):
+        o.kernel()
+        o.update2nd()
+        o.swap()
+    return o.get(1)
+
+
+@pytest.mark.parametrize("name", [k for k in CASES if "fd8" in k])
+def test_fd8_matches_reference(golden, name):
+    got = run_oracle(CASES[name])
+    ref = golden[f"{name}__w1"]
+    assert rel_l2(got, ref) < FD8_TOL
+
+
+@pytest.mark.parametrize("name", [k for k in CASES if "cfd" in k])
+def test_cfd_matches_reference_within_fp32_conditioning(golden, name):
+    got = run_oracle(CASES[name])
+    exact = run_oracle(CASES[name], double=True)
+    ref = golden[f"{name}__w1"]
+    spread = rel_l2(ref, exact)           # the reference's own FP32 error
+    assert spread < 5e-3
+    assert rel_l2(got, ref) < 2.0 * spread + 1e-6
+    assert rel_l2(got, exact) < 2.0 * spread + 1e-6
+
+
+def test_codec_bit_exact(golden):
+    for cname, (a, nx, ny, nz) in codec_input().items():
+        codes = O.c16_compress(a, nx, ny, nz)
+        np.testing.assert_array_equal(codes, golden[f"c16_{cname}__codes"])
+        dec = O.c16_uncompress(codes, nx, ny, nz).reshape(ny, nx, nz)
+        ref = golden[f"c16_{cname}__decoded"].reshape(ny, nx, nz)
+        # untapered cells decode bit-exactly; in the 20/10-cell edge tapers the
+        # reference build (-ffast-math) may reassociate the taper products
+        inner = (slice(20, -20) if ny > 40 else slice(None), slice(20, -20) if nx > 40 else slice(None),
+                 slice(10, -10) if nz > 20 else slice(None))
+        np.testing.assert_array_equal(dec[inner].view(np.uint32), ref[inner].view(np.uint32))
+        np.testing.assert_allclose(dec, ref, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("n", [40, 57])
+@pytest.mark.parametrize("s", [0, 1])
+def test_cfd_plan(golden, n, s):
+    bm, bl, am = O.cfd_plan(n, 10.0, s)
+    np.testing.assert_array_equal(bm, golden[f"cfd_plan_{n}_{s}__bm"])
+    np.testing.assert_array_equal(bl, golden[f"cfd_plan_{n}_{s}__bl"])
+    np.testing.assert_allclose(am, golden[f"cfd_plan_{n}_{s}__am"], rtol=1e-6, atol=0)
+
+
+def test_taylor_weights_order8():
+    c1, c2 = O.taylor_weights(4)
+    np.testing.assert_allclose(c1[1:], [4 / 5, -1 / 5, 4 / 105, -1 / 280], rtol=1e-13)
+    np.testing.assert_allclose(c2, [-205 / 72, 8 / 5, -1 / 5, 8 / 315, -1 / 560], rtol=1e-13)
+
+
+def test_fd8_known_answer_sine():
+    """FdEngine::init_sine-style field (bgprtm/FdEngine.cpp:404-421): the FD8
+    Laplacian of sin(kx x) sin(kz z) sin(ky y) is -(kx^2+ky^2+kz^2) times the
+    field, up to the FD8 dispersion at these wavenumbers."""
+    from konglong_b200.spec import PropSpec
+    nx, ny, nz = 40, 36, 44
+    spec = PropSpec(nx=nx, ny=ny, nz=nz, dx=10, dy=10, dz=10, dt=0.001, nbnd=(0,) * 6)
+    kx, ky, kz = 2 * np.pi / 20, 2 * np.pi / 18, 2 * np.pi / 22   # per cell
+    iy, ix, iz = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz), indexing="ij")
+    f = (np.sin(kx * ix) * np.sin(ky * iy) * np.sin(kz * iz)).astype(np.float32)
+    o = O.Oracle(spec, double=True)
+    vel = np.full(spec.shape, 1.0 / spec.dt, np.float32)   # (v dt)^2 = 1
+    o.set_model(vel=vel)
+    o.put(1, f)
+    o.put(0, np.zeros_like(f))
+    o.kernel()
+    lap = -o.get(0).reshape(spec.shape)
+    interior = (slice(4, -4),) * 3
+    want = -(kx ** 2 + ky ** 2 + kz ** 2) / 100.0 * f
+    assert rel_l2(lap[interior], want[interior]) < 2e-4
+
+
+def test_pml_profile(golden):
+    # restated profile (float) against the reference's PML object
+    from konglong_b200.spec import PropSpec
+    w, d, dt, vmax = 20, 10.0, 0.001, 4500.0
+    beta = np.float32(d) / (np.float32(dt) * np.float32(vmax))
+    dg1 = np.float32(np.log(np.float32(1) / np.float32(1e-3))) / (np.float32(w) * beta)
+    t = (np.float32(w) - np.arange(w, dtype=np.float32)) / np.float32(w)
+    coef = np.float32(0.75) * t * t * dg1
+    np.testing.assert_allclose(coef, golden["pml_coef_20"], rtol=1e-6)
