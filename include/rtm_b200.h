@@ -207,6 +207,30 @@ int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
+/* Kernels launched by the last rtm_modelling / rtm_migration call. */
+int rtm_last_loop_launches(rtm_handle *h, long long *n);
+
+/* Kernel kinds of the per-kernel profile. */
+enum {
+  RTM_K_ISO = 0,       /* ISO FD8 fused step */
+  RTM_K_GRAD = 1,      /* FD8 gradient pass (VTI/TTI) */
+  RTM_K_DIV = 2,       /* FD8 divergence pass */
+  RTM_K_CFD_Z = 3,     /* compact-FD z-line solves */
+  RTM_K_CFD_X = 4,     /* compact-FD x-line solves */
+  RTM_K_CFD_Y = 5,     /* compact-FD y-line solves */
+  RTM_K_CFD_GEPI = 6,  /* compact-FD gradient epilogue (PML, scaling) */
+  RTM_K_CFD_DEPI = 7,  /* compact-FD divergence epilogue (PML, update) */
+  RTM_K_INJECT = 8,
+  RTM_K_EXTRACT = 9,
+  RTM_K_SLAB = 10,     /* per-slab max of the 16-bit snapshot formats */
+  RTM_K_IO = 11,       /* standalone snapshot store / imaging condition */
+  RTM_NKINDS = 12
+};
+/* on = 1: the time loops run eagerly (no CUDA graph) with CUDA events around
+ * every launch, and the per-kind device time accumulates; on = 0 resets. */
+int rtm_profile(rtm_handle *h, int on);
+/* ms[RTM_NKINDS], count[RTM_NKINDS]: accumulated device time and launches. */
+int rtm_profile_read(rtm_handle *h, double *ms, long long *count);
 
 #ifdef __cplusplus
 }

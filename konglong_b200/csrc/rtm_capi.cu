@@ -79,6 +79,16 @@ struct Engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int *dflag = nullptr;
+  // launch accounting and the optional per-kernel event profile
+  long long launches = 0;
+  int prof_on = 0;
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof_recs;
+  double prof_ms[RTM_NKINDS] = {};
+  long long prof_cnt[RTM_NKINDS] = {};
 
   template <typename T> int alloc(T *&p, size_t count) {
     void *v = nullptr;
@@ -117,6 +127,41 @@ static int check_launch(Engine *h, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what, h);
   return RTM_OK;
+}
+
+// Counts one kernel launch of `kind`; when profiling, brackets it with events.
+struct KScope {
+  Engine *h;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KScope(Engine *h_, int k, int n = 1) : h(h_), kind(k) {
+    h->launches += n;
+    if (h->prof_on) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, h->st);
+    }
+  }
+  ~KScope() {
+    if (h->prof_on) {
+      cudaEventRecord(b, h->st);
+      h->prof_recs.push_back({kind, a, b});
+    }
+  }
+};
+
+static void prof_collect(Engine *h) {
+  for (auto &r : h->prof_recs) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      h->prof_ms[r.kind] += ms;
+      h->prof_cnt[r.kind] += 1;
+    }
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  h->prof_recs.clear();
+  cudaGetLastError();
 }
 
 // launch shape: 32 x tx column tiles, y split so the grid covers the 148 SMs
@@ -211,7 +256,10 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     a.pml = pml_dev(h);
     a.io = io;
     a.q = q;
-    launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
+    {
+      KScope k(h, RTM_K_ISO);
+      launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
+    }
     return check_launch(h, "iso_fd8_step");
   }
   if (h->c.engine == RTM_ENGINE_FD8) {
@@ -222,7 +270,10 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
     g.pml = pml_dev(h);
     g.io = io;
-    launch_grad_fd8(g, h->c.model_type, h->tx, h->st);
+    {
+      KScope k(h, RTM_K_GRAD);
+      launch_grad_fd8(g, h->c.model_type, h->tx, h->st);
+    }
     TRY(check_launch(h, "grad_fd8"));
     DivArgs v{};
     v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = h->yseg, v.pml3d = h->c.pml3d;
@@ -230,32 +281,55 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
     v.pml = pml_dev(h);
     v.q = q;
-    launch_div_fd8(v, mode, h->tx, h->st);
+    {
+      KScope k(h, RTM_K_DIV);
+      launch_div_fd8(v, mode, h->tx, h->st);
+    }
     return check_launch(h, "div_fd8");
   }
   // compact FD: raw line-solve derivatives, then pointwise PML / scaling /
   // accumulation epilogues (FdEngine_cfd + KernelCPU::TTI structure)
   if (io.store || io.ic) {
+    KScope k(h, RTM_K_IO);
     launch_fused_io(io, h->w1, d.nx, d.ny, d.nz, h->st);
-    TRY(check_launch(h, "fused_io"));
   }
-  launch_cfd_deriv(DZ, h->cfd[DZ][0], h->w1, h->pz, h->scr, d.nx, d.ny, d.nz, h->st);
-  launch_cfd_deriv(DX, h->cfd[DX][0], h->w1, h->px, h->scr, d.nx, d.ny, d.nz, h->st);
-  if (d.ny > 1) launch_cfd_deriv(DY, h->cfd[DY][0], h->w1, h->py, h->scr, d.nx, d.ny, d.nz, h->st);
+  TRY(check_launch(h, "fused_io"));
+  {
+    KScope k(h, RTM_K_CFD_Z);
+    launch_cfd_deriv(DZ, h->cfd[DZ][0], h->w1, h->pz, h->scr, d.nx, d.ny, d.nz, h->st);
+  }
+  {
+    KScope k(h, RTM_K_CFD_X);
+    launch_cfd_deriv(DX, h->cfd[DX][0], h->w1, h->px, h->scr, d.nx, d.ny, d.nz, h->st);
+  }
+  if (d.ny > 1) {
+    KScope k(h, RTM_K_CFD_Y);
+    launch_cfd_deriv(DY, h->cfd[DY][0], h->w1, h->py, h->scr, d.nx, d.ny, d.nz, h->st);
+  }
   TRY(check_launch(h, "cfd_deriv(grad)"));
   CfdGradEpiArgs ge{};
   ge.nx = d.nx, ge.ny = d.ny, ge.nz = d.nz, ge.pml3d = h->c.pml3d, ge.model = h->c.model_type;
   ge.gx = h->px, ge.gy = h->py, ge.gz = h->pz;
   ge.eps = h->eps, ge.del = h->del, ge.pjx = h->pjx, ge.pjy = h->pjy;
   ge.pml = pml_dev(h);
-  launch_cfd_grad_epilogue(ge, h->st);
+  {
+    KScope k(h, RTM_K_CFD_GEPI);
+    launch_cfd_grad_epilogue(ge, h->st);
+  }
   TRY(check_launch(h, "cfd_grad_epilogue"));
   // divergence parts: d/dx px -> scr, d/dz pz -> scr2, d/dy py -> px (px is free now)
-  launch_cfd_deriv(DX, h->cfd[DX][1], h->px, h->scr2, h->scr, d.nx, d.ny, d.nz, h->st);
+  {
+    KScope k(h, RTM_K_CFD_X);
+    launch_cfd_deriv(DX, h->cfd[DX][1], h->px, h->scr2, h->scr, d.nx, d.ny, d.nz, h->st);
+  }
   float *dzp = h->scr;
-  launch_cfd_deriv(DZ, h->cfd[DZ][1], h->pz, dzp, nullptr, d.nx, d.ny, d.nz, h->st);
+  {
+    KScope k(h, RTM_K_CFD_Z);
+    launch_cfd_deriv(DZ, h->cfd[DZ][1], h->pz, dzp, nullptr, d.nx, d.ny, d.nz, h->st);
+  }
   float *dyp = nullptr;
   if (d.ny > 1) {
+    KScope k(h, RTM_K_CFD_Y);
     launch_cfd_deriv(DY, h->cfd[DY][1], h->py, h->px, h->pz, d.nx, d.ny, d.nz, h->st);
     dyp = h->px;
   }
@@ -266,7 +340,10 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   de.w1 = h->w1, de.w0 = h->w0, de.vel = h->vel;
   de.pml = pml_dev(h);
   de.q = q;
-  launch_cfd_div_epilogue(de, h->st);
+  {
+    KScope k(h, RTM_K_CFD_DEPI);
+    launch_cfd_div_epilogue(de, h->st);
+  }
   return check_launch(h, "cfd_div_epilogue");
 }
 
@@ -274,6 +351,7 @@ static int do_inject(Engine *h, int it) {
   TraceSetDev &t = h->inj;
   if (!t.ntr || it < 0 || it >= t.nt) return RTM_OK;
   TraceDev td = t.dev();
+  KScope k(h, RTM_K_INJECT, (int)t.groups.size() + (t.n_ungrouped ? 1 : 0));
   for (const GroupDev &g : t.groups)
     launch_inject_group(g, td, it, h->plane, h->w0, h->vel, h->d.nx, h->d.ny, h->d.nz, h->st);
   if (t.n_ungrouped) {
@@ -287,6 +365,7 @@ static int do_extract(Engine *h, int jt) {
   TraceSetDev &t = h->ext;
   if (!t.ntr || jt < 0 || jt >= t.nt) return RTM_OK;
   TraceDev td = t.dev();
+  KScope k(h, RTM_K_EXTRACT, 2 * (int)t.groups.size() + (t.n_ungrouped ? 1 : 0));
   for (const GroupDev &g : t.groups)
     launch_extract_group(g, td, h->w0, h->plane, t.out, jt, t.nt, h->d.nx, h->d.ny, h->d.nz, h->st);
   if (t.n_ungrouped) {
@@ -336,6 +415,7 @@ static FusedIo io_image(Engine *h, int slot) {
 static int snap_prepare(Engine *h, int slot) {
   if (h->snap_fmt == RTM_SNAP_FP32) return RTM_OK;
   SnapDev s = slot_dev(h, slot);
+  KScope k(h, RTM_K_SLAB);
   launch_slab_max(h->w0, (float *)s.slab, h->snap_fmt == RTM_SNAP_C16 ? (uint16_t *)s.base : nullptr, h->snap_fmt,
                   h->d.nx, h->d.ny, h->d.nz, h->st);
   return check_launch(h, "slab_max");
@@ -345,7 +425,16 @@ static int snap_prepare(Engine *h, int slot) {
 // steps each, timed with events on the engine's stream.
 template <typename F> static int run_graphs(Engine *h, int count, F fn) {
   const int chunk = 256;
+  h->launches = 0;
   CK(cudaEventRecord(h->ev0, h->st));
+  if (h->prof_on) {  // eager launches bracketed by events (no graph)
+    for (int s = 0; s < count; s++) TRY(fn(s));
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaEventSynchronize(h->ev1));
+    CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+    prof_collect(h);
+    return RTM_OK;
+  }
   for (int s0 = 0; s0 < count; s0 += chunk) {
     const int s1 = std::min(count, s0 + chunk);
     cudaGraph_t g = nullptr;
@@ -910,6 +999,7 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
   });
   if (rc != RTM_OK) return rc;
   if (pending.store || pending.ic) {  // the last step's snapshot / image term
+    rtm::KScope k(h, RTM_K_IO);
     rtm::launch_fused_io(pending, h->w1, h->d.nx, h->d.ny, h->d.nz, h->st);
     TRY(rtm::check_launch(h, "fused_io(last)"));
     CK(cudaStreamSynchronize(h->st));
@@ -980,6 +1070,25 @@ int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int
   cudaFree(din), cudaFree(dout), cudaFree(slab), cudaFree(ex), cudaFree(ey), cudaFree(ez);
   cudaGetLastError();
   return rc;
+}
+
+int rtm_profile(rtm_handle *h, int on) {
+  if (!h) return RTM_ERR_ARG;
+  h->prof_on = on ? 1 : 0;
+  for (int k = 0; k < RTM_NKINDS; k++) h->prof_ms[k] = 0.0, h->prof_cnt[k] = 0;
+  return RTM_OK;
+}
+
+int rtm_profile_read(rtm_handle *h, double *ms, long long *count) {
+  if (!h || !ms || !count) return RTM_ERR_ARG;
+  for (int k = 0; k < RTM_NKINDS; k++) ms[k] = h->prof_ms[k], count[k] = h->prof_cnt[k];
+  return RTM_OK;
+}
+
+int rtm_last_loop_launches(rtm_handle *h, long long *n) {
+  if (!h || !n) return RTM_ERR_ARG;
+  *n = h->launches;
+  return RTM_OK;
 }
 
 int rtm_last_loop_ms(rtm_handle *h, float *ms) {

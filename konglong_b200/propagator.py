@@ -146,6 +146,21 @@ class Propagator:
         self._ck(self.L.rtm_last_loop_ms(self.h, C.byref(v)), "rtm_last_loop_ms")
         return v.value
 
+    def launch_count(self):
+        v = C.c_longlong()
+        self._ck(self.L.rtm_last_loop_launches(self.h, C.byref(v)), "rtm_last_loop_launches")
+        return v.value
+
+    def profile(self, on=True):
+        self._ck(self.L.rtm_profile(self.h, int(on)), "rtm_profile")
+
+    def profile_read(self):
+        """{kernel kind: (total device ms, launches)} of the profiled loops."""
+        ms = np.zeros(len(_lib.KERNEL_KINDS), np.float64)
+        cnt = np.zeros(len(_lib.KERNEL_KINDS), np.int64)
+        self._ck(self.L.rtm_profile_read(self.h, ms, cnt), "rtm_profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KERNEL_KINDS) if cnt[i]}
+
     # -- field access -------------------------------------------------------------------
     def get(self, field):
         out = np.zeros(self.n, np.float32)

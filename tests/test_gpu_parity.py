@@ -174,7 +174,7 @@ def test_grouped_injection_and_extraction_match_per_trace():
             x.extract(it)
         out.append((x.get(0), x.traces()))
     assert rel_l2(out[0][0], out[1][0]) < 1e-6
-    assert rel_l2(out[0][1], out[1][1]) < 1e-6
+    assert rel_l2(out[0][1], out[1][1]) < 1e-5   # z-plane then xy reduction order
 
 
 def test_fused_loop_equals_stepwise_calls():
