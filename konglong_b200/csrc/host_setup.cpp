@@ -58,7 +58,8 @@ void fd_weights(int ne, double *c1, double *c2) {
   c2[0] = (double)(-2.0L * s);
 }
 
-void cfd_plan(int n, double d, int isgn, std::vector<float> &bm, std::vector<float> &bl, std::vector<float> &am) {
+void cfd_plan(int n, double d, int isgn, std::vector<float> &bm, std::vector<float> &bl, std::vector<float> &am,
+              std::vector<float> *rdiag) {
   // Compact scheme B f' = A f, B 9-banded symmetric, A 11-point antisymmetric
   // (10th-order coefficient set of bgprtm/Cfd_plan.cpp:139-149).  Boundary
   // rows fold the stencil back onto the grid with sign -1 for B / +1 for A
@@ -119,6 +120,10 @@ void cfd_plan(int n, double d, int isgn, std::vector<float> &bm, std::vector<flo
     for (int j = 0; j < 4; j++) bl[(size_t)i * 4 + j] = (float)L[(size_t)j * n + i];
   }
   for (int i = 0; i < 60; i++) am[i] = (float)A[i];
+  if (rdiag) {
+    rdiag->resize(n);
+    for (int i = 0; i < n; i++) (*rdiag)[i] = (float)(1.0 / b(0, i));
+  }
 }
 
 void pml_profile(int w, double d, double dt, double vmax, double eps, double scaler, std::vector<float> &co) {

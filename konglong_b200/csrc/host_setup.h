@@ -5,8 +5,10 @@
 namespace rtm {
 // order-2*ne central-difference weights: c1[0..ne] (c1[0] = 0), c2[0..ne]
 void fd_weights(int ne, double *c1, double *c2);
-// compact FD factors of one axis: bm [n][5], bl [n][4], am [12][5]; isgn 1 or 2
-void cfd_plan(int n, double d, int isgn, std::vector<float> &bm, std::vector<float> &bl, std::vector<float> &am);
+// compact FD factors of one axis: bm [n][5], bl [n][4], am [12][5]; isgn 1 or 2;
+// rdiag [n] = 1 / pivot (FP64 division, then rounded)
+void cfd_plan(int n, double d, int isgn, std::vector<float> &bm, std::vector<float> &bl, std::vector<float> &am,
+              std::vector<float> *rdiag = nullptr);
 // per-layer PML recursion constants [w][6] (scale 1, then scale `scaler`)
 void pml_profile(int w, double d, double dt, double vmax, double eps, double scaler, std::vector<float> &co);
 // Util::CompactOrmsbySpreadCoeff + edge taper; returns the first grid index

@@ -46,7 +46,8 @@ void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {
   int n;
-  const float *bm, *bl, *am;  // [n][5], [n][4], [60]
+  const float *bu, *bl, *am;  // [n][4] upper factor (super-diagonals 1..4), [n][4] multipliers, [60] A
+  const float *rdiag;         // [n] 1 / pivot, from the FP64 factorisation
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();

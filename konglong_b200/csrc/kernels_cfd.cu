@@ -20,116 +20,161 @@ namespace rtm {
 
 namespace {
 
-// Line solve on an abstract accessor: X(i) reads the input, Y(i) / SET(i, v)
-// read / write the in-place result.  in and out may be the same storage.
-template <typename Ld, typename St, typename LdOut>
-__device__ __forceinline__ void cfd_solve_line(const CfdPlanDev &p, Ld X, St SET, LdOut Y) {
+// Line solve on an accessor A(i) -> float& into shared memory, in place.
+// Forward: rhs_i = (A x)_i, then y_i = rhs_i - sum_j al[(i-j)*4+j-1] y_{i-j};
+// backward: f_i = (y_i - sum_k bm[i*5+k] f_{i+k}) * (1 / bm[i*5]).  The
+// newest recurrence term is applied last, so one FMA sits on the dependency
+// chain per point; the pivots' reciprocals come from the FP64 plan set-up.
+template <typename Acc>
+__device__ __forceinline__ void cfd_solve_line(const CfdPlanDev &p, Acc A) {
   const int n = p.n;
   const float *__restrict__ a = p.am;
-  const float *__restrict__ bm = p.bm;
+  const float *__restrict__ bu = p.bu;
   const float *__restrict__ al = p.bl;
-  // --- forward: rhs_i then y_i = rhs_i - sum_j al[(i-j)*4 + j-1] * y_{i-j}
+  const float *__restrict__ rd = p.rdiag;
+  const float a55 = a[55], a56 = a[56], a57 = a[57], a58 = a[58], a59 = a[59];
   float xw[11];  // x[i-5 .. i+5]
 #pragma unroll
-  for (int k = 0; k < 11; k++) xw[k] = (k >= 5 && k - 5 < n) ? X(k - 5) : 0.f;
-  float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;  // y_{i-1} .. y_{i-4}
-  for (int i = 0; i < n; i++) {
-    float r;
-    if (i < 5) {
-      r = 0.f;
-      for (int j = 5 - i; j < 11; j++) r = r + a[j * 5 + i] * xw[j];
-    } else if (i < n - 5) {
-      r = a[55] * (xw[6] - xw[4]) + a[56] * (xw[7] - xw[3]) + a[57] * (xw[8] - xw[2]) + a[58] * (xw[9] - xw[1]) +
-          a[59] * (xw[10] - xw[0]);
-    } else {
-      r = 0.f;
-      const int jmax = min(11, n - (i - 5));
-      for (int j = 0; j < jmax; j++) r = r - a[n - i + 49 - 5 * j] * xw[j];
-    }
-    // subtract the elimination terms in the reference's order (oldest pivot first)
+  for (int k = 0; k < 11; k++) xw[k] = (k >= 5 && k - 5 < n) ? A(k - 5) : 0.f;
+  float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
+  // rows 0..4: one-sided boundary rows of A
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 5 - i; j < 11; j++) r = r + a[j * 5 + i] * xw[j];
     if (i >= 4) r = r - al[(i - 4) * 4 + 3] * y4;
     if (i >= 3) r = r - al[(i - 3) * 4 + 2] * y3;
     if (i >= 2) r = r - al[(i - 2) * 4 + 1] * y2;
     if (i >= 1) r = r - al[(i - 1) * 4 + 0] * y1;
-    // slide the input window before the in-place store overwrites x_i
 #pragma unroll
     for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
-    xw[10] = (i + 6 < n) ? X(i + 6) : 0.f;
-    SET(i, r);
+    xw[10] = (i + 6 < n) ? A(i + 6) : 0.f;
+    A(i) = r;
     y4 = y3, y3 = y2, y2 = y1, y1 = r;
   }
-  // --- backward substitution with the 5-band upper factor
-  float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;  // f_{i+1} .. f_{i+4}
-  for (int i = n - 1; i >= 0; i--) {
-    const float *u = bm + i * 5;
-    float v = Y(i);
-    if (i >= n - 4) {
-      const int l = n - 1 - i;  // terms available
-      if (l >= 1) v += -u[1] * z1;
-      if (l >= 2) v += -u[2] * z2;
-      if (l >= 3) v += -u[3] * z3;
-      v = v / u[0];
-    } else {
-      v = (v - u[1] * z1 - u[2] * z2 - u[3] * z3 - u[4] * z4) / u[0];
-    }
-    SET(i, v);
+  // interior rows: antisymmetric 11-point stencil
+#pragma unroll 4
+  for (int i = 5; i < n - 5; i++) {
+    float r = a55 * (xw[6] - xw[4]) + a56 * (xw[7] - xw[3]) + a57 * (xw[8] - xw[2]) + a58 * (xw[9] - xw[1]) +
+              a59 * (xw[10] - xw[0]);
+    const float4 l4 = *reinterpret_cast<const float4 *>(al + (i - 4) * 4);  // row i-4's multipliers
+    r = r - l4.w * y4;
+    r = r - al[(i - 3) * 4 + 2] * y3;
+    r = r - al[(i - 2) * 4 + 1] * y2;
+    r = r - al[(i - 1) * 4 + 0] * y1;
+#pragma unroll
+    for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
+    xw[10] = (i + 6 < n) ? A(i + 6) : 0.f;
+    A(i) = r;
+    y4 = y3, y3 = y2, y2 = y1, y1 = r;
+  }
+  // rows n-5 .. n-1: the mirrored boundary rows
+#pragma unroll
+  for (int t = 5; t >= 1; t--) {
+    const int i = n - t;
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < 11; j++)
+      if (j < t + 5) r = r - a[t + 49 - 5 * j] * xw[j];
+    r = r - al[(i - 4) * 4 + 3] * y4;
+    r = r - al[(i - 3) * 4 + 2] * y3;
+    r = r - al[(i - 2) * 4 + 1] * y2;
+    r = r - al[(i - 1) * 4 + 0] * y1;
+#pragma unroll
+    for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
+    xw[10] = 0.f;
+    A(i) = r;
+    y4 = y3, y3 = y2, y2 = y1, y1 = r;
+  }
+  // backward substitution
+  float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
+#pragma unroll
+  for (int t = 1; t <= 4; t++) {
+    const int i = n - t;
+    const float *u = bu + i * 4;  // u[k-1] = B's k-th super-diagonal factor of row i
+    float v = A(i);
+    if (t >= 4) v = v - u[2] * z3;
+    if (t >= 3) v = v - u[1] * z2;
+    if (t >= 2) v = v - u[0] * z1;
+    v = v * rd[i];
+    A(i) = v;
+    z4 = z3, z3 = z2, z2 = z1, z1 = v;
+  }
+#pragma unroll 4
+  for (int i = n - 5; i >= 0; i--) {
+    const float4 u = *reinterpret_cast<const float4 *>(bu + i * 4);
+    float v = A(i);
+    v = v - u.w * z4;
+    v = v - u.z * z3;
+    v = v - u.y * z2;
+    v = v - u.x * z1;
+    v = v * rd[i];
+    A(i) = v;
     z4 = z3, z3 = z2, z2 = z1, z1 = v;
   }
 }
 
-// x or y lines: thread per (iz, other index); stride between line points.
-__global__ void cfd_strided_k(CfdPlanDev p, const float *__restrict__ in, float *out, int nz, long long stride,
-                              long long other_stride, int n_other) {
-  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  const int o = blockIdx.y;
-  if (iz >= nz || o >= n_other) return;
-  const long long base = (long long)o * other_stride + iz;
-  const float *src = in + base;
-  float *dst = out + base;
-  cfd_solve_line(
-      p, [&](int i) { return __ldg(src + (long long)i * stride); }, [&](int i, float v) { dst[(long long)i * stride] = v; },
-      [&](int i) { return dst[(long long)i * stride]; });
-}
-
-// z lines: 32 lines per CTA through shared memory
-__global__ void cfd_z_k(CfdPlanDev p, const float *__restrict__ in, float *out, long long nlines) {
+// 32 lines per CTA staged through shared memory; warp 0 walks the lines
+// (lane = line), all warps move data.  x / y lines (STRIDED): element i of
+// line l at base + l + i*es, smem [i][32]; z lines: line l at base + l*n + i,
+// smem [l][n+1].  One HBM read and one write per cell.
+template <bool STRIDED>
+__global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__restrict__ in, float *__restrict__ out,
+                                                   int nz, long long es, long long other_stride, int n_other,
+                                                   long long nlines) {
   extern __shared__ float sm[];
-  const int n = p.n, ld = n + 1;
-  const long long l0 = (long long)blockIdx.x * 32;
-  const int nl = (int)min(32LL, nlines - l0);
-  // coalesced stage-in: warp w copies lines w, w+nw, ...
+  const int n = p.n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int l = warp; l < nl; l += nw)
-    for (int i = lane; i < n; i += 32) sm[l * ld + i] = __ldg(in + (l0 + l) * n + i);
-  __syncthreads();
-  if (threadIdx.x < nl) {
-    float *line = sm + threadIdx.x * ld;
-    cfd_solve_line(
-        p, [&](int i) { return line[i]; }, [&](int i, float v) { line[i] = v; }, [&](int i) { return line[i]; });
+  long long base;
+  int nl;
+  if (STRIDED) {
+    const int izc = blockIdx.x, o = blockIdx.y;
+    const int iz0 = izc * 32;
+    nl = min(32, nz - iz0);
+    base = (long long)o * other_stride + iz0;
+    for (int i = warp; i < n; i += nw)
+      if (lane < nl) sm[i * 32 + lane] = __ldg(in + base + lane + (long long)i * es);
+  } else {
+    const long long l0 = (long long)blockIdx.x * 32;
+    nl = (int)min(32LL, nlines - l0);
+    base = l0 * n;
+    for (int l = warp; l < nl; l += nw)
+      for (int i = lane; i < n; i += 32) sm[l * (n + 1) + i] = __ldg(in + base + (long long)l * n + i);
   }
   __syncthreads();
-  for (int l = warp; l < nl; l += nw)
-    for (int i = lane; i < n; i += 32) out[(l0 + l) * n + i] = sm[l * ld + i];
+  if (warp == 0 && lane < nl) {
+    if (STRIDED) cfd_solve_line(p, [&](int i) -> float & { return sm[i * 32 + lane]; });
+    else cfd_solve_line(p, [&](int i) -> float & { return sm[lane * (n + 1) + i]; });
+  }
+  __syncthreads();
+  if (STRIDED) {
+    for (int i = warp; i < n; i += nw)
+      if (lane < nl) out[base + lane + (long long)i * es] = sm[i * 32 + lane];
+  } else {
+    for (int l = warp; l < nl; l += nw)
+      for (int i = lane; i < n; i += 32) out[base + (long long)l * n + i] = sm[l * (n + 1) + i];
+  }
 }
 
-__global__ void cfd_grad_epi_k(CfdGradEpiArgs a) {
+// pointwise epilogues: block (32 z, 8 x), grid (z tiles, x tiles, ny)
+__global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const long long n = g.nxz * a.ny;
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz >= a.nz || ix >= a.nx) return;
   const bool do_y = a.ny > 1;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / g.nxz);
-    const long long in = i - (long long)iy * g.nxz;
-    const int ix = (int)(in / a.nz), iz = (int)(in - (long long)ix * a.nz);
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
+  {
     float gz = a.gz[i], gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f;
     pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
     pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
     if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
     if (a.model >= 2) {
-      float e = a.eps[i];
-      const float dl = e - a.del[i];
+      float e = __ldg(a.eps + i);
+      const float dl = e - __ldg(a.del + i);
       e = 1.0f + 2.0f * e;
       if (a.model == 3) {
-        const float ax = a.pjx[i], ay = do_y ? a.pjy[i] : 0.f;
+        const float ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
         const float az = sqrtf(1.0f - (ax * ax + ay * ay));
         const float v2 = gx * gx + gy * gy + gz * gz;
         const float vzz = gx * ax + gy * ay + gz * az;
@@ -156,35 +201,27 @@ __global__ void cfd_grad_epi_k(CfdGradEpiArgs a) {
   }
 }
 
-__global__ void cfd_div_epi_k(CfdDivEpiArgs a) {
+__global__ void __launch_bounds__(256) cfd_div_epi_k(CfdDivEpiArgs a) {
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const long long n = g.nxz * a.ny;
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz >= a.nz || ix >= a.nx) return;
   const bool do_y = a.ny > 1 && a.dy;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / g.nxz);
-    const long long in = i - (long long)iy * g.nxz;
-    const int ix = (int)(in / a.nz), iz = (int)(in - (long long)ix * a.nz);
-    float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
-    pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
-    pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
-    if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
-    const float vel = a.vel[i];
-    float t = a.w0[i] - dxv * vel;
-    t = t - dzv * vel;
-    t = t - dyv * vel;
-    float out;
-    if (a.mode == 0) out = t;
-    else {
-      const float u = a.w1[i];
-      out = a.mode == 1 ? (u + u) - t : q_update(a.q, i, n, t, u);
-    }
-    a.w0[i] = out;
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
+  float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
+  pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
+  pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
+  if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+  const float vel = __ldg(a.vel + i);
+  float t = a.w0[i] - dxv * vel;
+  t = t - dzv * vel;
+  t = t - dyv * vel;
+  float out;
+  if (a.mode == 0) out = t;
+  else {
+    const float u = __ldg(a.w1 + i);
+    out = a.mode == 1 ? (u + u) - t : q_update(a.q, i, g.nxz * a.ny, t, u);
   }
-}
-
-int grid_for(long long n, int threads) {
-  long long b = (n + threads - 1) / threads;
-  return (int)(b < 148LL * 16 ? b : 148LL * 16);
+  a.w0[i] = out;
 }
 
 }  // namespace
@@ -196,26 +233,29 @@ void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out
   if (axis == DZ) {
     const long long nlines = (long long)nx * ny;
     const size_t smem = (size_t)32 * (nz + 1) * sizeof(float);
-    cfd_z_k<<<(unsigned)((nlines + 31) / 32), 128, smem, st>>>(p, in, out, nlines);
-  } else if (axis == DX) {
-    dim3 grid((nz + 127) / 128, ny);
-    cfd_strided_k<<<grid, 128, 0, st>>>(p, in, out, nz, nz, nxz, ny);
+    cfd_lines_k<false><<<(unsigned)((nlines + 31) / 32), 128, smem, st>>>(p, in, out, nz, 1, 0, 0, nlines);
   } else {
-    dim3 grid((nz + 127) / 128, nx);
-    cfd_strided_k<<<grid, 128, 0, st>>>(p, in, out, nz, nxz, nz, nx);
+    const int n = axis == DX ? nx : ny;
+    const size_t smem = (size_t)32 * n * sizeof(float);
+    dim3 grid((nz + 31) / 32, axis == DX ? ny : nx);
+    if (axis == DX) cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nz, nxz, ny, 0);
+    else cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nxz, nz, nx, 0);
   }
 }
 
 int cfd_init() {
-  return cudaFuncSetAttribute(cfd_z_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) == cudaSuccess ? 0 : -1;
+  const int mx = 227 * 1024;
+  bool ok = cudaFuncSetAttribute(cfd_lines_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_lines_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  return ok ? 0 : -1;
 }
 
 void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st) {
-  cfd_grad_epi_k<<<grid_for((long long)a.nx * a.ny * a.nz, 256), 256, 0, st>>>(a);
+  cfd_grad_epi_k<<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
 }
 
 void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
-  cfd_div_epi_k<<<grid_for((long long)a.nx * a.ny * a.nz, 256), 256, 0, st>>>(a);
+  cfd_div_epi_k<<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
 }
 
 }  // namespace rtm

@@ -5,6 +5,8 @@
 // gather work: no tensor cores, coalesced along z.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "kernel_api.h"
 #include "rtm_device.cuh"
 
@@ -24,16 +26,18 @@ __global__ void update2nd_q_k(float *__restrict__ w0, const float *__restrict__ 
     w0[i] = q_update(q, i, n, w0[i], w1[i]);
 }
 
-// one CTA per trace, threads over the kernel box (iz fastest)
+// one CTA per (trace, y tap), threads over the x-z taps (z fastest)
 __global__ void inject_scatter_k(TraceDev t, int it, float *__restrict__ w0, const float *__restrict__ vel, int nx,
                                  int nz) {
   const int r = t.ids ? t.ids[blockIdx.x] : blockIdx.x;
   const int *o = t.off + 3 * r, *l = t.len + 3 * r;
-  const int lx = l[0], ly = l[1], lz = l[2];
+  const int lx = l[0], lz = l[2];
+  const int iy = blockIdx.y;
+  if (iy >= l[1]) return;
   const float val = t.traces[(long long)r * t.nt + it] * t.scaler;
-  const int ntap = lx * ly * lz;
+  const int ntap = lx * lz;
   for (int k = threadIdx.x; k < ntap; k += blockDim.x) {
-    const int iz = k % lz, ix = (k / lz) % lx, iy = k / (lz * lx);
+    const int iz = k % lz, ix = k / lz;
     const float cy = val * t.ky[(long long)r * t.ly + iy];
     const float cx = cy * t.kx[(long long)r * t.lx + ix];
     const long long c = ((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz;
@@ -165,43 +169,37 @@ __global__ void slab_max_k(const float *__restrict__ w, float *__restrict__ slab
   }
 }
 
-__global__ void fused_io_k(FusedIo io, const float *__restrict__ u, int nx, int ny, int nz) {
+// elementwise kernels: block (32 z, 8 x), grid (z tiles, x tiles, ny)
+__global__ void __launch_bounds__(256) fused_io_k(FusedIo io, const float *__restrict__ u, int nx, int ny, int nz) {
   const Grid3 g{nx, ny, nz, (long long)nx * nz};
-  const long long n = g.nxz * ny;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / g.nxz);
-    const long long in = i - (long long)iy * g.nxz;
-    const int ix = (int)(in / nz), iz = (int)(in - (long long)ix * nz);
-    fused_io(io, g, i, ix, iy, iz, in, u[i]);
-  }
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz >= nz || ix >= nx) return;
+  const long long in = (long long)ix * nz + iz, i = (long long)iy * g.nxz + in;
+  fused_io(io, g, i, ix, iy, iz, in, u[i]);
 }
 
-__global__ void snap_decode_k(SnapDev s, float *__restrict__ out, const float *ex, const float *ey, const float *ez,
-                              int nx, int ny, int nz) {
+__global__ void __launch_bounds__(256) snap_decode_k(SnapDev s, float *__restrict__ out, const float *ex,
+                                                     const float *ey, const float *ez, int nx, int ny, int nz) {
   const Grid3 g{nx, ny, nz, (long long)nx * nz};
-  const long long n = g.nxz * ny;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / g.nxz);
-    const long long in = i - (long long)iy * g.nxz;
-    float v = snap_read(s, g, i, iy, in);
-    if (ex) {
-      const int ix = (int)(in / nz), iz = (int)(in - (long long)ix * nz);
-      v = v * ey[iy];
-      v = v * ex[ix];
-      v = v * ez[iz];
-    }
-    out[i] = v;
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz >= nz || ix >= nx) return;
+  const long long in = (long long)ix * nz + iz, i = (long long)iy * g.nxz + in;
+  float v = snap_read(s, g, i, iy, in);
+  if (ex) {
+    v = v * ey[iy];
+    v = v * ex[ix];
+    v = v * ez[iz];
   }
+  out[i] = v;
 }
 
 __global__ void c16_encode_k(const float *__restrict__ in, uint16_t *__restrict__ out, const float *__restrict__ slab,
-                             int ny, long long nxz) {
-  const long long n = nxz * ny;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / nxz);
-    const long long in_ = i - (long long)iy * nxz;
+                             long long nxz) {
+  const int iy = blockIdx.y;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nxz; k += (long long)gridDim.x * blockDim.x) {
     const float vmax = slab[iy];
-    out[(long long)iy * (nxz + 2) + 2 + in_] = vmax > 1e-25f ? c16_encode(in[i] * __frcp_rn(vmax)) : (uint16_t)0;
+    out[(long long)iy * (nxz + 2) + 2 + k] =
+        vmax > 1e-25f ? c16_encode(in[(long long)iy * nxz + k] * __frcp_rn(vmax)) : (uint16_t)0;
   }
 }
 
@@ -252,7 +250,7 @@ void launch_inject_scatter(const TraceDev &t, int it, float *w0, const float *ve
   (void)ny;
   const int cnt = t.ids ? t.nids : t.ntr;
   if (cnt <= 0 || it < 0 || it >= t.nt) return;
-  inject_scatter_k<<<cnt, 256, 0, st>>>(t, it, w0, vel, nx, nz);
+  inject_scatter_k<<<dim3(cnt, t.ly), 256, 0, st>>>(t, it, w0, vel, nx, nz);
 }
 
 void launch_inject_group(const GroupDev &gr, const TraceDev &t, int it, float *plane, float *w0, const float *vel,
@@ -282,20 +280,18 @@ void launch_slab_max(const float *w, float *slab, uint16_t *c16_base, int fmt, i
 }
 
 void launch_fused_io(const FusedIo &io, const float *u, int nx, int ny, int nz, cudaStream_t st) {
-  long long n = (long long)nx * ny * nz;
-  fused_io_k<<<grid_for(n, 256), 256, 0, st>>>(io, u, nx, ny, nz);
+  fused_io_k<<<dim3((nz + 31) / 32, (nx + 7) / 8, ny), dim3(32, 8), 0, st>>>(io, u, nx, ny, nz);
 }
 
 void launch_snap_decode(const SnapDev &s, float *out, const float *ex, const float *ey, const float *ez, int nx, int ny,
                         int nz, cudaStream_t st) {
-  long long n = (long long)nx * ny * nz;
-  snap_decode_k<<<grid_for(n, 256), 256, 0, st>>>(s, out, ex, ey, ez, nx, ny, nz);
+  snap_decode_k<<<dim3((nz + 31) / 32, (nx + 7) / 8, ny), dim3(32, 8), 0, st>>>(s, out, ex, ey, ez, nx, ny, nz);
 }
 
 void launch_c16_compress(const float *in, uint16_t *out, float *slab, int nx, int ny, int nz, cudaStream_t st) {
   const long long nxz = (long long)nx * nz;
   slab_max_k<<<ny, 1024, 0, st>>>(in, slab, out, 1, nxz);
-  c16_encode_k<<<grid_for(nxz * ny, 256), 256, 0, st>>>(in, out, slab, ny, nxz);
+  c16_encode_k<<<dim3((unsigned)std::min<long long>((nxz + 255) / 256, 64), ny), 256, 0, st>>>(in, out, slab, nxz);
 }
 
 void launch_c16_uncompress(const uint16_t *in, float *out, float *slab, const float *ex, const float *ey,
