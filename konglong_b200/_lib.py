@@ -19,6 +19,7 @@ RTM_OK = 0
 STATUS = {0: "RTM_OK", -1: "RTM_ERR_ARG", -2: "RTM_ERR_STATE", -3: "RTM_ERR_CUDA",
           -4: "RTM_ERR_NOMEM", -5: "RTM_ERR_UNSUPPORTED", -6: "RTM_ERR_NONFINITE",
           -7: "RTM_ERR_TIMEOUT"}
+STATUS_CODE = {v: k for k, v in STATUS.items()}
 
 # every entry point of include/rtm_b200.h
 EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", "rtm_set_q_coeffs",
@@ -27,7 +28,8 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_extract", "rtm_get_traces", "rtm_snapshot_setup", "rtm_snapshot_store",
            "rtm_snapshot_load", "rtm_image_setup", "rtm_image_accumulate", "rtm_modelling",
            "rtm_migration", "rtm_get", "rtm_put", "rtm_c16_compress", "rtm_c16_uncompress",
-           "rtm_last_loop_ms", "rtm_last_loop_launches", "rtm_profile", "rtm_profile_read"]
+           "rtm_last_loop_ms", "rtm_last_loop_launches", "rtm_profile", "rtm_profile_read",
+           "rtm_c16_compress_noalloc"]
 
 KERNEL_KINDS = ["iso_fd8_step", "grad_fd8", "div_fd8", "cfd_z", "cfd_x", "cfd_y", "cfd_grad_epilogue",
                 "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io"]
@@ -94,6 +96,7 @@ def lib():
     L.rtm_c16_compress.argtypes = [_f32p, _u16p, i, i, i]
     L.rtm_c16_uncompress.argtypes = [_u16p, _f32p, i, i, i]
     L.rtm_last_loop_ms.argtypes = [vp, C.POINTER(f)]
+    L.rtm_c16_compress_noalloc.argtypes = [vp, vp, i, i, i, vp]
     L.rtm_last_loop_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.rtm_profile.argtypes = [vp, i]
     L.rtm_profile_read.argtypes = [vp, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),

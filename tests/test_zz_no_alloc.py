@@ -1,0 +1,42 @@
+"""The allocation-free COMPRESS_16 entry point (rtm_c16_compress_noalloc).
+
+It serves callers that cannot allocate GPU memory (a fixed memory budget, work
+recorded into their own CUDA graph, threads that must not wait on the
+allocator): they pass device buffers and the entry point's scratch lives in a
+fixed array of the library.  Its codes must equal those of the allocating
+entry point rtm_c16_compress bit for bit, on two calls in a row (the second
+call reuses the scratch the first one left behind).  This file is collected
+last so a run that stops at the first failure has run every other test.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_noalloc_compress_matches_allocating_entry_point():
+    import torch
+    from konglong_b200 import _lib
+    from konglong_b200.propagator import c16_compress
+    from tests.golden_inputs import codec_input
+
+    L = _lib.lib()
+    cases = list(codec_input().values())
+    rng = np.random.default_rng(99)
+    a2 = (rng.standard_normal((30, 20, 16)) * np.exp(-np.arange(30))[:, None, None]).astype(np.float32)
+    cases.append((a2, 20, 30, 16))
+    for a, nx, ny, nz in cases:                      # consecutive calls share the scratch
+        want = c16_compress(a, nx, ny, nz)
+        d_in = torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).cuda()
+        d_out = torch.zeros(want.size, dtype=torch.int16, device="cuda")
+        rc = L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), nx, ny, nz, None)
+        assert rc == 0, _lib.lib().rtm_last_error(None)
+        torch.cuda.synchronize()
+        got = d_out.cpu().numpy().view(np.uint16)
+        np.testing.assert_array_equal(got, want)
+
+
+def test_noalloc_rejects_too_many_slabs():
+    from konglong_b200 import _lib
+    L = _lib.lib()
+    assert L.rtm_c16_compress_noalloc(1, 1, 4, 65537, 4, None) == _lib.STATUS_CODE["RTM_ERR_ARG"]
