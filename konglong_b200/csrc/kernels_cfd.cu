@@ -29,45 +29,53 @@ template <typename Acc>
 __device__ __forceinline__ void cfd_solve_line(const CfdPlanDev &p, Acc A) {
   const int n = p.n;
   const float *__restrict__ a = p.am;
-  const float *__restrict__ bu = p.bu;
-  const float *__restrict__ al = p.bl;
+  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
+  const float4 *__restrict__ al4 = reinterpret_cast<const float4 *>(p.bl);
   const float *__restrict__ rd = p.rdiag;
-  const float a55 = a[55], a56 = a[56], a57 = a[57], a58 = a[58], a59 = a[59];
+  const float a55 = __ldg(a + 55), a56 = __ldg(a + 56), a57 = __ldg(a + 57), a58 = __ldg(a + 58),
+              a59 = __ldg(a + 59);
   float xw[11];  // x[i-5 .. i+5]
 #pragma unroll
   for (int k = 0; k < 11; k++) xw[k] = (k >= 5 && k - 5 < n) ? A(k - 5) : 0.f;
   float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
+  // multipliers applied to row i: al[i-1].x, al[i-2].y, al[i-3].z, al[i-4].w
+  float4 m1 = make_float4(0.f, 0.f, 0.f, 0.f), m2 = m1, m3 = m1, m4 = m1;  // rows i-1 .. i-4
   // rows 0..4: one-sided boundary rows of A
 #pragma unroll
   for (int i = 0; i < 5; i++) {
     float r = 0.f;
 #pragma unroll
-    for (int j = 5 - i; j < 11; j++) r = r + a[j * 5 + i] * xw[j];
-    if (i >= 4) r = r - al[(i - 4) * 4 + 3] * y4;
-    if (i >= 3) r = r - al[(i - 3) * 4 + 2] * y3;
-    if (i >= 2) r = r - al[(i - 2) * 4 + 1] * y2;
-    if (i >= 1) r = r - al[(i - 1) * 4 + 0] * y1;
+    for (int j = 5 - i; j < 11; j++) r = r + __ldg(a + j * 5 + i) * xw[j];
+    r = r - m4.w * y4;
+    r = r - m3.z * y3;
+    r = r - m2.y * y2;
+    r = r - m1.x * y1;
 #pragma unroll
     for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
     xw[10] = (i + 6 < n) ? A(i + 6) : 0.f;
     A(i) = r;
     y4 = y3, y3 = y2, y2 = y1, y1 = r;
+    m4 = m3, m3 = m2, m2 = m1, m1 = __ldg(al4 + i);
   }
-  // interior rows: antisymmetric 11-point stencil
-#pragma unroll 4
+  // interior rows: antisymmetric 11-point stencil; the next row's multipliers
+  // are fetched one step ahead so no load sits on the recurrence
+  float4 nxt = __ldg(al4 + 5);
+#pragma unroll 2
   for (int i = 5; i < n - 5; i++) {
+    const float x_ahead = (i + 6 < n) ? A(i + 6) : 0.f;
     float r = a55 * (xw[6] - xw[4]) + a56 * (xw[7] - xw[3]) + a57 * (xw[8] - xw[2]) + a58 * (xw[9] - xw[1]) +
               a59 * (xw[10] - xw[0]);
-    const float4 l4 = *reinterpret_cast<const float4 *>(al + (i - 4) * 4);  // row i-4's multipliers
-    r = r - l4.w * y4;
-    r = r - al[(i - 3) * 4 + 2] * y3;
-    r = r - al[(i - 2) * 4 + 1] * y2;
-    r = r - al[(i - 1) * 4 + 0] * y1;
+    r = r - m4.w * y4;
+    r = r - m3.z * y3;
+    r = r - m2.y * y2;
+    r = r - m1.x * y1;
 #pragma unroll
     for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
-    xw[10] = (i + 6 < n) ? A(i + 6) : 0.f;
+    xw[10] = x_ahead;
     A(i) = r;
     y4 = y3, y3 = y2, y2 = y1, y1 = r;
+    m4 = m3, m3 = m2, m2 = m1, m1 = nxt;
+    nxt = __ldg(al4 + min(i + 1, n - 1));
   }
   // rows n-5 .. n-1: the mirrored boundary rows
 #pragma unroll
@@ -76,42 +84,50 @@ __device__ __forceinline__ void cfd_solve_line(const CfdPlanDev &p, Acc A) {
     float r = 0.f;
 #pragma unroll
     for (int j = 0; j < 11; j++)
-      if (j < t + 5) r = r - a[t + 49 - 5 * j] * xw[j];
-    r = r - al[(i - 4) * 4 + 3] * y4;
-    r = r - al[(i - 3) * 4 + 2] * y3;
-    r = r - al[(i - 2) * 4 + 1] * y2;
-    r = r - al[(i - 1) * 4 + 0] * y1;
+      if (j < t + 5) r = r - __ldg(a + t + 49 - 5 * j) * xw[j];
+    r = r - m4.w * y4;
+    r = r - m3.z * y3;
+    r = r - m2.y * y2;
+    r = r - m1.x * y1;
 #pragma unroll
     for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
     xw[10] = 0.f;
     A(i) = r;
     y4 = y3, y3 = y2, y2 = y1, y1 = r;
+    m4 = m3, m3 = m2, m2 = m1, m1 = __ldg(al4 + i);
   }
-  // backward substitution
+  // backward substitution: f_i = (y_i - u3 f_{i+4} - u2 f_{i+3} - u1 f_{i+2} - u0 f_{i+1}) / pivot_i
   float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
 #pragma unroll
   for (int t = 1; t <= 4; t++) {
     const int i = n - t;
-    const float *u = bu + i * 4;  // u[k-1] = B's k-th super-diagonal factor of row i
+    const float4 u = __ldg(bu4 + i);
     float v = A(i);
-    if (t >= 4) v = v - u[2] * z3;
-    if (t >= 3) v = v - u[1] * z2;
-    if (t >= 2) v = v - u[0] * z1;
-    v = v * rd[i];
+    if (t >= 4) v = v - u.z * z3;
+    if (t >= 3) v = v - u.y * z2;
+    if (t >= 2) v = v - u.x * z1;
+    v = v * __ldg(rd + i);
     A(i) = v;
     z4 = z3, z3 = z2, z2 = z1, z1 = v;
   }
-#pragma unroll 4
+  float4 u = __ldg(bu4 + n - 5);
+  float rdi = __ldg(rd + n - 5);
+  float yv = A(n - 5);
+#pragma unroll 2
   for (int i = n - 5; i >= 0; i--) {
-    const float4 u = *reinterpret_cast<const float4 *>(bu + i * 4);
-    float v = A(i);
+    const int j = max(i - 1, 0);
+    const float4 un = __ldg(bu4 + j);
+    const float rdn = __ldg(rd + j);
+    const float yn = A(j);
+    float v = yv;
     v = v - u.w * z4;
     v = v - u.z * z3;
     v = v - u.y * z2;
     v = v - u.x * z1;
-    v = v * rd[i];
+    v = v * rdi;
     A(i) = v;
     z4 = z3, z3 = z2, z2 = z1, z1 = v;
+    u = un, rdi = rdn, yv = yn;
   }
 }
 
@@ -134,13 +150,13 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
     nl = min(32, nz - iz0);
     base = (long long)o * other_stride + iz0;
     for (int i = warp; i < n; i += nw)
-      if (lane < nl) sm[i * 32 + lane] = __ldg(in + base + lane + (long long)i * es);
+      if (lane < nl) sm[i * 32 + lane] = __ldcg(in + base + lane + (long long)i * es);
   } else {
     const long long l0 = (long long)blockIdx.x * 32;
     nl = (int)min(32LL, nlines - l0);
     base = l0 * n;
     for (int l = warp; l < nl; l += nw)
-      for (int i = lane; i < n; i += 32) sm[l * (n + 1) + i] = __ldg(in + base + (long long)l * n + i);
+      for (int i = lane; i < n; i += 32) sm[l * (n + 1) + i] = __ldcg(in + base + (long long)l * n + i);
   }
   __syncthreads();
   if (warp == 0 && lane < nl) {
@@ -150,10 +166,10 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
   __syncthreads();
   if (STRIDED) {
     for (int i = warp; i < n; i += nw)
-      if (lane < nl) out[base + lane + (long long)i * es] = sm[i * 32 + lane];
+      if (lane < nl) __stcg(out + base + lane + (long long)i * es, sm[i * 32 + lane]);
   } else {
     for (int l = warp; l < nl; l += nw)
-      for (int i = lane; i < n; i += 32) out[base + (long long)l * n + i] = sm[l * (n + 1) + i];
+      for (int i = lane; i < n; i += 32) __stcg(out + base + (long long)l * n + i, sm[l * (n + 1) + i]);
   }
 }
 
@@ -166,9 +182,11 @@ __global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
   const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
   {
     float gz = a.gz[i], gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f;
-    pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
-    pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
-    if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
+    if (in_pml(a.pml, g, ix, iy, iz)) {
+      pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
+      pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
+      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
+    }
     if (a.model >= 2) {
       float e = __ldg(a.eps + i);
       const float dl = e - __ldg(a.del + i);
@@ -180,7 +198,7 @@ __global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
         const float vzz = gx * ax + gy * ay + gz * az;
         const float vz2 = vzz * vzz, vh2 = v2 - vz2;
         const float ecl = e * vh2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) / (ecl * ecl + 1e-32f));
+        const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
         const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
         const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
         gx = (bx + (gx - bx) * e) * sc;
@@ -189,7 +207,7 @@ __global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
       } else {
         const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
         const float ecl = e * vx2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) / (ecl * ecl + 1e-32f));
+        const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
         const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
         gx *= sc2;
         gy *= sc2;
@@ -208,9 +226,11 @@ __global__ void __launch_bounds__(256) cfd_div_epi_k(CfdDivEpiArgs a) {
   const bool do_y = a.ny > 1 && a.dy;
   const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
   float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
-  pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
-  pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
-  if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+  if (in_pml(a.pml, g, ix, iy, iz)) {
+    pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
+    pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
+    if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+  }
   const float vel = __ldg(a.vel + i);
   float t = a.w0[i] - dxv * vel;
   t = t - dzv * vel;

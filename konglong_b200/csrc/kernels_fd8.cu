@@ -79,15 +79,20 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
         for (int m = 1; m <= R; m++) ly += a.c2y[m] * (q[R - m] + q[R + m]);
       }
       float v;
+      const bool edge = in_pml(a.pml, g, ix, iy, iz);
       if (PML3D) {
         v = lz + lx + ly;
-        pml2_dim(a.pml, g, DZ, v, ix, iy, iz);
-        pml2_dim(a.pml, g, DX, v, ix, iy, iz);
-        pml2_dim(a.pml, g, DY, v, ix, iy, iz);
+        if (edge) {
+          pml2_dim(a.pml, g, DZ, v, ix, iy, iz);
+          pml2_dim(a.pml, g, DX, v, ix, iy, iz);
+          pml2_dim(a.pml, g, DY, v, ix, iy, iz);
+        }
       } else {
-        pml2_dim(a.pml, g, DZ, lz, ix, iy, iz);
-        pml2_dim(a.pml, g, DX, lx, ix, iy, iz);
-        if (do_y) pml2_dim(a.pml, g, DY, ly, ix, iy, iz);
+        if (edge) {
+          pml2_dim(a.pml, g, DZ, lz, ix, iy, iz);
+          pml2_dim(a.pml, g, DX, lx, ix, iy, iz);
+          if (do_y) pml2_dim(a.pml, g, DY, ly, ix, iy, iz);
+        }
         v = lz + lx + ly;
       }
       const long long i = plane + col;
@@ -151,9 +156,11 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
         if (do_y) gy += a.c1y[m] * (q[R + m] - q[R - m]);
       }
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
-      pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
-      pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
-      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
+      if (in_pml(a.pml, g, ix, iy, iz)) {
+        pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
+        pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
+        if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
+      }
       if (MODEL == 2 || MODEL == 3) {
         // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
         float e = __ldg(a.eps + i);
@@ -167,7 +174,7 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
           const float vz2 = vzz * vzz;
           const float vh2 = v2 - vz2;
           const float ecl = e * vh2 + vz2;
-          const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) / (ecl * ecl + 1e-32f));
+          const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
           const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
           const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
           gx = (bx + (gx - bx) * e) * sc;
@@ -176,7 +183,7 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
         } else {
           const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
           const float ecl = e * vx2 + vz2;
-          const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) / (ecl * ecl + 1e-32f));
+          const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
           const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
           gx *= sc2;
           gy *= sc2;
@@ -237,9 +244,11 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
         dzv += a.c1z[m] * (tpz[tx][tz + R + m] - tpz[tx][tz + R - m]);
         if (do_y) dyv += a.c1y[m] * (q[R + m] - q[R - m]);
       }
-      pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
-      pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
-      if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+      if (in_pml(a.pml, g, ix, iy, iz)) {
+        pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
+        pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
+        if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
+      }
       const float vel = __ldg(a.vel + i);
       // accumulation order of KernelCPU::TTI: x, then z, then y
       float t = a.w0[i] - dxv * vel;

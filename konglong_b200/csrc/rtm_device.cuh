@@ -65,6 +65,13 @@ __device__ __forceinline__ float *pml_at(const PmlDev &P, const Grid3 &g, int d,
   return F.q[r][c] + idx;
 }
 
+// True when (ix,iy,iz) lies in any PML layer; interior cells skip the PML code.
+__device__ __forceinline__ bool in_pml(const PmlDev &P, const Grid3 &g, int ix, int iy, int iz) {
+  const int zl = P.f[DZ][0].w, zh = P.f[DZ][1].w, xl = P.f[DX][0].w, xh = P.f[DX][1].w, yl = P.f[DY][0].w,
+            yh = P.f[DY][1].w;
+  return iz < zl || iz >= g.nz - zh || ix < xl || ix >= g.nx - xh || iy < yl || iy >= g.ny - yh;
+}
+
 // Two rounds along dim d on the summed 2nd-derivative operator
 // (pml2_{z,x,y}bnd, bgprtm/FdEngine.cpp:352-389).
 __device__ __forceinline__ void pml2_dim(const PmlDev &P, const Grid3 &g, int d, float &p, int ix, int iy, int iz) {
