@@ -122,6 +122,11 @@ def build_workload(name, steps_total):
         return W.iso128(scale=1.0, nt=steps_total)
     if name == "tti_q":
         return W.tti_q(scale=1.0, nt=steps_total)
+    if name == "vti_fd8":
+        shot = W.vti_cfd(scale=1.0, nt=steps_total)
+        shot.spec.engine = 0
+        shot.name = "vti_fd8"
+        return shot
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -303,7 +308,7 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q"])
+    ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q", "vti_fd8"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

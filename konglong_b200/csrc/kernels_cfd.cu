@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
   extern __shared__ float sm[];
   const int n = p.n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  constexpr int U = 16;  // independent loads in flight per thread during staging
   long long base;
   int nl;
   if (STRIDED) {
@@ -149,14 +150,37 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
     const int iz0 = izc * 32;
     nl = min(32, nz - iz0);
     base = (long long)o * other_stride + iz0;
-    for (int i = warp; i < n; i += nw)
-      if (lane < nl) sm[i * 32 + lane] = __ldcg(in + base + lane + (long long)i * es);
+    // rows i of 32 lines: warp w stages rows w*U .. w*U+U-1, then every nw*U rows
+    for (int i0 = warp * U; i0 < n; i0 += nw * U) {
+      float v[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const int i = i0 + k;
+        v[k] = (i < n && lane < nl) ? __ldcg(in + base + lane + (long long)i * es) : 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < U; k++)
+        if (i0 + k < n) sm[(i0 + k) * 32 + lane] = v[k];
+    }
   } else {
     const long long l0 = (long long)blockIdx.x * 32;
     nl = (int)min(32LL, nlines - l0);
     base = l0 * n;
-    for (int l = warp; l < nl; l += nw)
-      for (int i = lane; i < n; i += 32) sm[l * (n + 1) + i] = __ldcg(in + base + (long long)l * n + i);
+    const int per_line = (n + 31) / 32;  // 32-float chunks per line
+    const int chunks = nl * per_line;
+    for (int c0 = warp * U; c0 < chunks; c0 += nw * U) {
+      float v[U];
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const int c = c0 + k, l = c / per_line, i = (c - l * per_line) * 32 + lane;
+        v[k] = (c < chunks && i < n) ? __ldcg(in + base + (long long)l * n + i) : 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < U; k++) {
+        const int c = c0 + k, l = c / per_line, i = (c - l * per_line) * 32 + lane;
+        if (c < chunks && i < n) sm[l * (n + 1) + i] = v[k];
+      }
+    }
   }
   __syncthreads();
   if (warp == 0 && lane < nl) {
