@@ -30,6 +30,39 @@ __device__ __forceinline__ float ld_or0(const float *__restrict__ p, long long i
   return ok ? __ldg(p + i) : 0.0f;
 }
 
+// Halo values a thread stages into the plane tile: two z-halo cells (threads
+// tz < R) and two x-halo cells (threads tx < R).  Fetched two planes ahead so
+// the loads overlap the compute of the current plane.
+struct Halo {
+  float zl, zh, xl, xh;
+};
+
+template <int TX>
+__device__ __forceinline__ Halo fetch_halo(const float *__restrict__ f, int iy, int ny, int ix, int iz, int nx, int nz,
+                                           long long nxz, int tx, int tz) {
+  Halo h{0.f, 0.f, 0.f, 0.f};
+  if (iy < 0 || iy >= ny) return h;
+  const long long plane = (long long)iy * nxz;
+  if (tz < R) {
+    const int izl = iz - R, izh = iz + TZ;
+    h.zl = ld_or0(f, plane + (long long)ix * nz + izl, ix < nx && izl >= 0);
+    h.zh = ld_or0(f, plane + (long long)ix * nz + izh, ix < nx && izh < nz);
+  }
+  if (tx < R) {
+    const int ixl = ix - R, ixh = ix + TX;
+    h.xl = ld_or0(f, plane + (long long)ixl * nz + iz, iz < nz && ixl >= 0);
+    h.xh = ld_or0(f, plane + (long long)ixh * nz + iz, iz < nz && ixh < nx);
+  }
+  return h;
+}
+
+template <int TX>
+__device__ __forceinline__ void put_tile(float (*tile)[TZ + 2 * R], const Halo &h, float c, int tx, int tz) {
+  tile[tx + R][tz + R] = c;
+  if (tz < R) tile[tx + R][tz] = h.zl, tile[tx + R][tz + TZ + R] = h.zh;
+  if (tx < R) tile[tx][tz + R] = h.xl, tile[tx + TX + R][tz + R] = h.xh;
+}
+
 template <int TX, int MODE, bool PML3D>
 __global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
   __shared__ float tile[TX + 2 * R][TZ + 2 * R];
@@ -50,19 +83,21 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
     const int y = y0 - R + k;
     q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
   }
+  Halo h0 = fetch_halo<TX>(w1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  Halo h1 = fetch_halo<TX>(w1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  // per-cell inputs of the next plane
+  float nw0 = act ? a.w0[(long long)y0 * g.nxz + col] : 0.f;
+  float nvel = act ? __ldg(a.vel + (long long)y0 * g.nxz + col) : 0.f;
   for (int iy = y0; iy < y1; iy++) {
     q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
     const long long plane = (long long)iy * g.nxz;
-    tile[tx + R][tz + R] = q[R];
-    if (tz < R) {
-      const int izl = iz - R, izh = iz + TZ;
-      tile[tx + R][tz] = ld_or0(w1, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
-      tile[tx + R][tz + TZ + R] = ld_or0(w1, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
-    }
-    if (tx < R) {
-      const int ixl = ix - R, ixh = ix + TX;
-      tile[tx][tz + R] = ld_or0(w1, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
-      tile[tx + TX + R][tz + R] = ld_or0(w1, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+    put_tile<TX>(tile, h0, q[R], tx, tz);
+    h0 = h1;
+    h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+    const float cw0 = nw0, cvel = nvel;
+    if (act && iy + 1 < y1) {
+      nw0 = a.w0[plane + g.nxz + col];
+      nvel = __ldg(a.vel + plane + g.nxz + col);
     }
     __syncthreads();
     if (act) {
@@ -97,7 +132,7 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
       }
       const long long i = plane + col;
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, u);
-      const float t = a.w0[i] - v * __ldg(a.vel + i);
+      const float t = cw0 - v * cvel;
       float out;
       if (MODE == 0) out = t;                         // KernelCPU seam: w0 -= vel * L[w1]
       else if (MODE == 1) out = (u + u) - t;          // + update2nd (leapfrog)
@@ -131,20 +166,14 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
     const int y = y0 - R + k;
     q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
   }
+  Halo h0 = fetch_halo<TX>(w1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  Halo h1 = fetch_halo<TX>(w1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
   for (int iy = y0; iy < y1; iy++) {
     q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
     const long long plane = (long long)iy * g.nxz;
-    tile[tx + R][tz + R] = q[R];
-    if (tz < R) {
-      const int izl = iz - R, izh = iz + TZ;
-      tile[tx + R][tz] = ld_or0(w1, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
-      tile[tx + R][tz + TZ + R] = ld_or0(w1, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
-    }
-    if (tx < R) {
-      const int ixl = ix - R, ixh = ix + TX;
-      tile[tx][tz + R] = ld_or0(w1, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
-      tile[tx + TX + R][tz + R] = ld_or0(w1, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
-    }
+    put_tile<TX>(tile, h0, q[R], tx, tz);
+    h0 = h1;
+    h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
     __syncthreads();
     if (act) {
       const long long i = plane + col;
@@ -199,6 +228,31 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
   }
 }
 
+struct DivPlane {
+  float pxc, pzc, zl, zh, xl, xh;
+};
+
+template <int TX>
+__device__ __forceinline__ DivPlane fetch_div(const DivArgs &a, int iy, int ix, int iz, long long nxz, int tx, int tz,
+                                              bool act) {
+  DivPlane d{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (iy < 0 || iy >= a.ny) return d;
+  const long long plane = (long long)iy * nxz, col = (long long)ix * a.nz + iz;
+  d.pxc = ld_or0(a.px, plane + col, act);
+  d.pzc = ld_or0(a.pz, plane + col, act);
+  if (tz < R) {
+    const int izl = iz - R, izh = iz + TZ;
+    d.zl = ld_or0(a.pz, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
+    d.zh = ld_or0(a.pz, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
+  }
+  if (tx < R) {
+    const int ixl = ix - R, ixh = ix + TX;
+    d.xl = ld_or0(a.px, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
+    d.xh = ld_or0(a.px, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+  }
+  return d;
+}
+
 template <int TX, int MODE>
 __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
   __shared__ float tpx[TX + 2 * R][TZ];
@@ -219,20 +273,25 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
     const int y = y0 - R + k;
     q[k] = do_y ? ld_or0(a.py, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny) : 0.f;
   }
+  DivPlane d0 = fetch_div<TX>(a, y0, ix, iz, g.nxz, tx, tz, act);
+  DivPlane d1 = fetch_div<TX>(a, y0 + 1 < y1 ? y0 + 1 : a.ny, ix, iz, g.nxz, tx, tz, act);
+  float nw0 = act ? a.w0[(long long)y0 * g.nxz + col] : 0.f;
+  float nvel = act ? __ldg(a.vel + (long long)y0 * g.nxz + col) : 0.f;
+  float nw1 = act && MODE != 0 ? __ldg(a.w1 + (long long)y0 * g.nxz + col) : 0.f;
   for (int iy = y0; iy < y1; iy++) {
     if (do_y) q[2 * R] = ld_or0(a.py, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
     const long long plane = (long long)iy * g.nxz;
-    tpx[tx + R][tz] = ld_or0(a.px, plane + col, act);
-    tpz[tx][tz + R] = ld_or0(a.pz, plane + col, act);
-    if (tz < R) {
-      const int izl = iz - R, izh = iz + TZ;
-      tpz[tx][tz] = ld_or0(a.pz, plane + (long long)ix * a.nz + izl, ix < a.nx && izl >= 0);
-      tpz[tx][tz + TZ + R] = ld_or0(a.pz, plane + (long long)ix * a.nz + izh, ix < a.nx && izh < a.nz);
-    }
-    if (tx < R) {
-      const int ixl = ix - R, ixh = ix + TX;
-      tpx[tx][tz] = ld_or0(a.px, plane + (long long)ixl * a.nz + iz, iz < a.nz && ixl >= 0);
-      tpx[tx + TX + R][tz] = ld_or0(a.px, plane + (long long)ixh * a.nz + iz, iz < a.nz && ixh < a.nx);
+    tpx[tx + R][tz] = d0.pxc;
+    tpz[tx][tz + R] = d0.pzc;
+    if (tz < R) tpz[tx][tz] = d0.zl, tpz[tx][tz + TZ + R] = d0.zh;
+    if (tx < R) tpx[tx][tz] = d0.xl, tpx[tx + TX + R][tz] = d0.xh;
+    d0 = d1;
+    d1 = fetch_div<TX>(a, iy + 2 < y1 ? iy + 2 : a.ny, ix, iz, g.nxz, tx, tz, act);
+    const float cw0 = nw0, cvel = nvel, cw1 = nw1;
+    if (act && iy + 1 < y1) {
+      nw0 = a.w0[plane + g.nxz + col];
+      nvel = __ldg(a.vel + plane + g.nxz + col);
+      if (MODE != 0) nw1 = __ldg(a.w1 + plane + g.nxz + col);
     }
     __syncthreads();
     if (act) {
@@ -249,17 +308,13 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
         pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
         if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
       }
-      const float vel = __ldg(a.vel + i);
       // accumulation order of KernelCPU::TTI: x, then z, then y
-      float t = a.w0[i] - dxv * vel;
-      t = t - dzv * vel;
-      t = t - dyv * vel;
+      float t = cw0 - dxv * cvel;
+      t = t - dzv * cvel;
+      t = t - dyv * cvel;
       float out;
       if (MODE == 0) out = t;
-      else {
-        const float u = __ldg(a.w1 + i);
-        out = MODE == 1 ? (u + u) - t : q_update(a.q, i, (long long)a.ny * g.nxz, t, u);
-      }
+      else out = MODE == 1 ? (cw1 + cw1) - t : q_update(a.q, i, (long long)a.ny * g.nxz, t, cw1);
       a.w0[i] = out;
     }
     __syncthreads();

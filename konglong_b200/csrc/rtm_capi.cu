@@ -167,9 +167,9 @@ static void prof_collect(Engine *h) {
 // launch shape: 32 x tx column tiles, y split so the grid covers the 148 SMs
 static void choose_shape(Engine *h) {
   const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
-  int tx = nx >= 256 ? 8 : 8;
+  int tx = 8;
   long long bxz = (long long)((nz + 31) / 32) * ((nx + tx - 1) / tx);
-  long long want = 148LL * 8;
+  long long want = 148LL * 2 * 8;  // ~8 waves of 2 CTAs per SM
   int nseg = (int)std::max(1LL, std::min<long long>((want + bxz - 1) / bxz, std::max(1, ny / 16)));
   h->tx = tx;
   h->yseg = (ny + nseg - 1) / nseg;
