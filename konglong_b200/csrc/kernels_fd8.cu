@@ -168,12 +168,23 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
   }
   Halo h0 = fetch_halo<TX>(w1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
   Halo h1 = fetch_halo<TX>(w1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  // anisotropy parameters of the next plane
+  float4 nm = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto fetch_model = [&](long long i) {
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (MODEL >= 2) m.x = __ldg(a.eps + i), m.y = __ldg(a.del + i);
+    if (MODEL == 3) m.z = __ldg(a.pjx + i), m.w = do_y ? __ldg(a.pjy + i) : 0.f;
+    return m;
+  };
+  if (act) nm = fetch_model((long long)y0 * g.nxz + col);
   for (int iy = y0; iy < y1; iy++) {
     q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
     const long long plane = (long long)iy * g.nxz;
     put_tile<TX>(tile, h0, q[R], tx, tz);
     h0 = h1;
     h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+    const float4 cm = nm;
+    if (act && iy + 1 < y1) nm = fetch_model(plane + g.nxz + col);
     __syncthreads();
     if (act) {
       const long long i = plane + col;
@@ -192,11 +203,11 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
       }
       if (MODEL == 2 || MODEL == 3) {
         // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
-        float e = __ldg(a.eps + i);
-        const float dl = e - __ldg(a.del + i);
+        float e = cm.x;
+        const float dl = e - cm.y;
         e = 1.0f + 2.0f * e;
         if (MODEL == 3) {
-          const float ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
+          const float ax = cm.z, ay = cm.w;
           const float az = sqrtf(1.0f - (ax * ax + ay * ay));
           const float v2 = gx * gx + gy * gy + gz * gz;
           const float vzz = gx * ax + gy * ay + gz * az;
