@@ -122,6 +122,12 @@ def build_workload(name, steps_total):
         return W.iso128(scale=1.0, nt=steps_total)
     if name == "tti_q":
         return W.tti_q(scale=1.0, nt=steps_total)
+    if name == "iso512":
+        shot = W.vti_cfd(scale=1.0, nt=steps_total)
+        shot.spec.engine, shot.spec.model_type = 0, 1
+        shot.eps = shot.dl = None
+        shot.name = "iso512"
+        return shot
     if name == "vti_fd8":
         shot = W.vti_cfd(scale=1.0, nt=steps_total)
         shot.spec.engine = 0
@@ -308,7 +314,7 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q", "vti_fd8"])
+    ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -91,6 +91,7 @@ typedef struct rtm_config {
   float pml3d_scaler; /* cross-term damping scale, default 0.3 */
   int top_pml;        /* default 1; 0 = free surface top (no z1 PML) */
   int state_fp16;     /* 0: FP32 wavefield state (default) */
+  int kernel_variant; /* 0: auto (TMA plane pipeline when nz % 4 == 0), 1: register pipeline */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;

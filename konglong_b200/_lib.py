@@ -44,7 +44,7 @@ class RtmConfig(C.Structure):
     _fields_ = [("engine", C.c_int), ("model_type", C.c_int), ("use_q", C.c_int),
                 ("q_order", C.c_int), ("nbnd", C.c_int * 6), ("vmax", C.c_float),
                 ("pml_eps", C.c_float), ("pml3d", C.c_int), ("pml3d_scaler", C.c_float),
-                ("top_pml", C.c_int), ("state_fp16", C.c_int)]
+                ("top_pml", C.c_int), ("state_fp16", C.c_int), ("kernel_variant", C.c_int)]
 
 
 class RtmError(RuntimeError):

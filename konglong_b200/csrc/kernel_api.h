@@ -1,5 +1,6 @@
 // kernel_api.h - argument blocks and launchers of the B200 RTM kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "rtm_internal.cuh"
@@ -42,6 +43,13 @@ struct DivArgs {
 void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
 void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st);
 void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
+
+// ---- TMA plane pipelines (kernels_tma.cu), nz % 4 == 0 ------------------------
+bool tma_supported(int nz);
+// fp32 volume [ny][nx][nz], box (bz, bx, 1)
+bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx);
+void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
+                        int *err, int mode, int pml3d, cudaStream_t st);
 
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {

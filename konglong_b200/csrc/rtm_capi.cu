@@ -11,6 +11,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/rtm_b200.h"
 #include "host_setup.h"
 #include "kernel_api.h"
@@ -81,6 +83,13 @@ struct Engine {
   int *dflag = nullptr;
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
+  int use_tma = 0;
+  struct TMap {
+    const void *p;
+    int bz, bx;
+    CUtensorMap m;
+  };
+  std::vector<TMap> tmaps;
   int prof_on = 0;
   struct ProfRec {
     int kind;
@@ -126,6 +135,18 @@ int cuda_fail(cudaError_t e, const char *what, Engine *h) {
 static int check_launch(Engine *h, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what, h);
+  return RTM_OK;
+}
+
+// a bounded device wait that gave up raises the engine's flag
+static int check_flag(Engine *h) {
+  int f = 0;
+  CK(cudaMemcpy(&f, h->dflag, sizeof f, cudaMemcpyDeviceToHost));
+  if (f) {
+    cudaMemset(h->dflag, 0, sizeof f);
+    h->err = "a pipelined kernel's bounded wait for its tile copies gave up";
+    return RTM_ERR_TIMEOUT;
+  }
   return RTM_OK;
 }
 
@@ -176,6 +197,16 @@ static void choose_shape(Engine *h) {
 }
 
 static PmlDev pml_dev(Engine *h) { return h->pml; }
+
+// tensor map of a device volume with box (bz, bx, 1), built once per buffer
+static const CUtensorMap *tmap(Engine *h, const void *p, int bz, int bx) {
+  for (auto &t : h->tmaps)
+    if (t.p == p && t.bz == bz && t.bx == bx) return &t.m;
+  Engine::TMap t{p, bz, bx, {}};
+  if (!make_tmap(&t.m, p, h->d.nx, h->d.ny, h->d.nz, bz, bx)) return nullptr;
+  h->tmaps.push_back(t);
+  return &h->tmaps.back().m;
+}
 
 static int setup_pml(Engine *h) {
   const rtm_config &c = h->c;
@@ -256,9 +287,15 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     a.pml = pml_dev(h);
     a.io = io;
     a.q = q;
+    const CUtensorMap *m1 = nullptr, *m0 = nullptr, *mv = nullptr;
+    if (h->use_tma) {
+      m1 = tmap(h, h->w1, 40, 16), m0 = tmap(h, h->w0, 32, 8), mv = tmap(h, h->vel, 32, 8);
+      if (!m1 || !m0 || !mv) h->use_tma = 0;
+    }
     {
       KScope k(h, RTM_K_ISO);
-      launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
+      if (h->use_tma) launch_iso_fd8_tma(a, *m1, *m0, *mv, h->dflag, mode, h->c.pml3d, h->st);
+      else launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
     }
     return check_launch(h, "iso_fd8_step");
   }
@@ -433,7 +470,7 @@ template <typename F> static int run_graphs(Engine *h, int count, F fn) {
     CK(cudaEventSynchronize(h->ev1));
     CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
     prof_collect(h);
-    return RTM_OK;
+    return check_flag(h);
   }
   for (int s0 = 0; s0 < count; s0 += chunk) {
     const int s1 = std::min(count, s0 + chunk);
@@ -458,7 +495,7 @@ template <typename F> static int run_graphs(Engine *h, int count, F fn) {
   CK(cudaEventRecord(h->ev1, h->st));
   CK(cudaEventSynchronize(h->ev1));
   CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
-  return RTM_OK;
+  return check_flag(h);
 }
 
 static int ready(Engine *h) {
@@ -742,6 +779,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->one_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
+  h->use_tma = c->kernel_variant == 0 && tma_supported(d->nz);
+  CK(cudaMemset(h->dflag, 0, sizeof(int)));
   if ((rc = zero_state(h))) return fail(rc);
   if (cudaStreamSynchronize(h->st) != cudaSuccess) {
     h->err = "initialisation failed";
@@ -815,7 +854,7 @@ int rtm_kernel(rtm_handle *h) {
   TRY(rtm::ready(h));
   TRY(rtm::step_kernel(h, 0, rtm::io_none()));
   CK(cudaStreamSynchronize(h->st));
-  return RTM_OK;
+  return rtm::check_flag(h);
 }
 
 int rtm_update2nd(rtm_handle *h) {

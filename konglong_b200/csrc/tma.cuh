@@ -1,0 +1,63 @@
+// tma.cuh - Tensor Memory Accelerator and mbarrier helpers (sm_100a inline PTX)
+// for the plane pipelines of the FD8 kernels.  Loads are plain (non-multicast)
+// cp.async.bulk.tensor copies into this CTA's own shared memory; every wait on
+// an mbarrier is bounded.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rtm {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// producer: announce `bytes` of TMA traffic on this phase and arrive
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// plain arrive (count 1, no transaction bytes)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait for the phase of `parity`.  Gives up after 2^20 polls, or as
+// soon as another CTA has raised *err, sets *err and returns false (the caller
+// then skips its compute; the copies it waited for are its own).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+  for (uint32_t it = 0; it < (1u << 20); it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 1023) == 1023 && err && *(volatile int *)err) return false;
+  }
+  if (err) atomicExch(err, 1);
+  return false;
+}
+
+// 3-D tiled load (coordinates innermost first: z, x, y) completing on `bar`.
+// The proxy fence orders earlier generic writes of this stage before the copy.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int cz, int cx, int cy) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)map), "r"(cz), "r"(cx), "r"(cy), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace rtm

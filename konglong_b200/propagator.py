@@ -36,6 +36,7 @@ class Propagator:
         c.vmax, c.pml_eps = spec.vmax, spec.pml_eps
         c.pml3d, c.pml3d_scaler, c.top_pml = int(spec.pml3d), spec.pml3d_scaler, int(spec.top_pml)
         c.state_fp16 = int(spec.state_fp16)
+        c.kernel_variant = int(getattr(spec, "kernel_variant", 0))
         h = C.c_void_p()
         _lib.check(L.rtm_create(C.byref(d), C.byref(c), C.byref(h)), "rtm_create")
         self.h = h

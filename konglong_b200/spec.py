@@ -38,6 +38,7 @@ class PropSpec:
     pml3d_scaler: float = 0.3
     top_pml: bool = True
     state_fp16: bool = False
+    kernel_variant: int = 0       # 0 auto (TMA pipeline), 1 register pipeline
 
     @property
     def n(self):

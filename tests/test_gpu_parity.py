@@ -196,3 +196,19 @@ def test_fused_loop_equals_stepwise_calls():
         b.inject(it - 1)
         b.swap()
     assert rel_l2(a.get(FIELD_W1), b.get(FIELD_W1)) < 1e-6
+
+
+@pytest.mark.parametrize("builder,scale", [(W.iso128, 0.375)])
+def test_tma_pipeline_equals_register_pipeline(builder, scale):
+    """The TMA plane pipeline and the register-prefetch kernel compute the same
+    arithmetic in the same order: equal results."""
+    shot = builder(scale=scale, nt=60)
+    out = []
+    for variant in (0, 1):
+        s = shot.spec
+        s.kernel_variant = variant
+        p = Propagator(s)
+        out.append(_modelling(shot, p, spread_coeffs, 60))
+        out.append(p.get(FIELD_W1))
+    np.testing.assert_array_equal(out[0], out[2])
+    np.testing.assert_array_equal(out[1], out[3])
