@@ -165,6 +165,7 @@ def run_cuda(args, rank, world):
     nslots = (2 * K + Wm) // shot.interval + 2
     p.snapshot_setup(snap_fmt, nslots)
     p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
+    tuned = p.autotune(3)
     p.reset()
     dist = world > 1
     if dist:
@@ -247,8 +248,10 @@ def run_cuda(args, rank, world):
                        "receiver samples D2H; wall clock"}
         q.close()
     p.close()
+    cfg = config_of(shot, snap_fmt, K)
+    cfg["autotuned_shape"] = tuned
     return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
-                config=config_of(shot, snap_fmt, K), shot=shot, launches=launches)
+                config=cfg, shot=shot, launches=launches)
 
 
 def cpu_baseline(shot, max_seconds=20.0):

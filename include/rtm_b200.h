@@ -224,6 +224,12 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
+/* Autotuner: times `steps` fused steps of every launch shape this handle's
+ * kernels offer (TMA tile width / prefetch depth for ISO FD8, tile width of
+ * the FD8 gradient / divergence passes), keeps the fastest, returns its index
+ * in *choice, then zeroes the wavefields and PML memory (as rtm_reset). */
+int rtm_autotune(rtm_handle *h, int steps, int *choice);
+
 /* Kernels launched by the last rtm_modelling / rtm_migration call. */
 int rtm_last_loop_launches(rtm_handle *h, long long *n);
 

@@ -48,8 +48,14 @@ void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
 bool tma_supported(int nz);
 // fp32 volume [ny][nx][nz], box (bz, bx, 1)
 bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx);
+struct TmaShape {
+  int tx, depth;  // tile width (x) and planes prefetched beyond the stencil window
+};
+extern const TmaShape kIsoTmaShapes[];
+extern const int kIsoTmaNShapes;
+bool iso_tma_init();  // shared-memory attributes (call outside any capture)
 void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
-                        int *err, int mode, int pml3d, cudaStream_t st);
+                        int *err, int mode, int pml3d, int shape, cudaStream_t st);
 
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {

@@ -26,25 +26,30 @@ namespace rtm {
 
 namespace {
 
-constexpr int TZ = 32, TX = 8, R = 4;
-constexpr int HZ = TZ + 2 * R, HX = TX + 2 * R;  // haloed tile 40 x 16
-constexpr int P = 3;                              // prefetch depth (planes)
-constexpr int SA = 2 * R + 1 + P;                 // ring A stages
-constexpr int SB = P + 1;                         // ring B stages
+constexpr int TZ = 32, R = 4;
+constexpr int HZ = TZ + 2 * R;  // haloed tile height (z)
 
+// Shared-memory rings of one CTA: TX = tile width (x), P = prefetch depth.
+template <int TX, int P>
 struct __align__(128) IsoSmem {
-  float a[SA][HX][HZ];   // w1 tiles with halo
-  float w0[SB][TX][TZ];  // w0 tiles
-  float vel[SB][TX][TZ]; // (v dt)^2 tiles
+  static constexpr int HX = TX + 2 * R;
+  static constexpr int SA = 2 * R + 1 + P;  // ring A stages (the +-4 window + prefetch)
+  static constexpr int SB = P + 1;          // ring B stages
+  float a[SA][HX][HZ];    // w1 tiles with halo
+  float w0[SB][TX][TZ];   // w0 tiles
+  float vel[SB][TX][TZ];  // (v dt)^2 tiles
   uint64_t bar_a[SA];
   uint64_t bar_b[SB];
 };
 
-template <int MODE, bool PML3D>
+template <int TX, int P, int MODE, bool PML3D>
 __global__ void __launch_bounds__(TZ *TX) iso_fd8_tma(IsoArgs a, const __grid_constant__ CUtensorMap map_w1,
                                                       const __grid_constant__ CUtensorMap map_w0,
                                                       const __grid_constant__ CUtensorMap map_vel, int *err) {
-  __shared__ IsoSmem s;
+  using Smem = IsoSmem<TX, P>;
+  constexpr int HX = Smem::HX, SA = Smem::SA, SB = Smem::SB;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem &s = *reinterpret_cast<Smem *>(smem_raw);
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
   const int tz = threadIdx.x, tx = threadIdx.y;
   const int iz0 = blockIdx.x * TZ, ix0 = blockIdx.y * TX;
@@ -187,10 +192,12 @@ bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz,
   return r == CUDA_SUCCESS;
 }
 
-void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
-                        int *err, int mode, int pml3d, cudaStream_t st) {
+template <int TX, int P>
+static void iso_tma_shape(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
+                          int *err, int mode, int pml3d, cudaStream_t st) {
   dim3 grid((a.nz + TZ - 1) / TZ, (a.nx + TX - 1) / TX, (a.ny + a.yseg - 1) / a.yseg), block(TZ, TX);
-#define L_(M, P3) iso_fd8_tma<M, P3><<<grid, block, 0, st>>>(a, w1, w0, vel, err)
+  const size_t smem = sizeof(IsoSmem<TX, P>);
+#define L_(M, P3) iso_fd8_tma<TX, P, M, P3><<<grid, block, smem, st>>>(a, w1, w0, vel, err)
   if (pml3d) {
     if (mode == 0) L_(0, true);
     else if (mode == 1) L_(1, true);
@@ -201,6 +208,39 @@ void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorM
     else L_(2, false);
   }
 #undef L_
+}
+
+template <int TX, int P>
+static bool iso_tma_attr() {
+  const int smem = (int)sizeof(IsoSmem<TX, P>);
+  bool ok = true;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  ok &= cudaFuncSetAttribute(iso_fd8_tma<TX, P, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0;
+  return ok;
+}
+
+// (tile width, prefetch depth) shapes the autotuner chooses from
+const TmaShape kIsoTmaShapes[] = {{8, 3}, {8, 6}, {8, 10}, {16, 4}, {16, 8}};
+const int kIsoTmaNShapes = sizeof(kIsoTmaShapes) / sizeof(kIsoTmaShapes[0]);
+
+bool iso_tma_init() {
+  return iso_tma_attr<8, 3>() && iso_tma_attr<8, 6>() && iso_tma_attr<8, 10>() && iso_tma_attr<16, 4>() &&
+         iso_tma_attr<16, 8>();
+}
+
+void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
+                        int *err, int mode, int pml3d, int shape, cudaStream_t st) {
+  switch (shape) {
+    case 0: iso_tma_shape<8, 3>(a, w1, w0, vel, err, mode, pml3d, st); break;
+    case 1: iso_tma_shape<8, 6>(a, w1, w0, vel, err, mode, pml3d, st); break;
+    case 2: iso_tma_shape<8, 10>(a, w1, w0, vel, err, mode, pml3d, st); break;
+    case 3: iso_tma_shape<16, 4>(a, w1, w0, vel, err, mode, pml3d, st); break;
+    default: iso_tma_shape<16, 8>(a, w1, w0, vel, err, mode, pml3d, st); break;
+  }
 }
 
 }  // namespace rtm

@@ -84,6 +84,7 @@ struct Engine {
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
+  int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
     int bz, bx;
@@ -196,6 +197,15 @@ static void choose_shape(Engine *h) {
   h->yseg = (ny + nseg - 1) / nseg;
 }
 
+// y segment length for a tile width: enough CTAs for ~8 waves of 2 per SM
+static int yseg_for(Engine *h, int tx) {
+  const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
+  long long bxz = (long long)((nz + 31) / 32) * ((nx + tx - 1) / tx);
+  long long want = 148LL * 2 * 8;
+  int nseg = (int)std::max(1LL, std::min<long long>((want + bxz - 1) / bxz, std::max(1, ny / 16)));
+  return (ny + nseg - 1) / nseg;
+}
+
 static PmlDev pml_dev(Engine *h) { return h->pml; }
 
 // tensor map of a device volume with box (bz, bx, 1), built once per buffer
@@ -289,12 +299,14 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     a.q = q;
     const CUtensorMap *m1 = nullptr, *m0 = nullptr, *mv = nullptr;
     if (h->use_tma) {
-      m1 = tmap(h, h->w1, 40, 16), m0 = tmap(h, h->w0, 32, 8), mv = tmap(h, h->vel, 32, 8);
+      const int tx = kIsoTmaShapes[h->tma_shape].tx;
+      m1 = tmap(h, h->w1, 40, tx + 8), m0 = tmap(h, h->w0, 32, tx), mv = tmap(h, h->vel, 32, tx);
       if (!m1 || !m0 || !mv) h->use_tma = 0;
+      else a.yseg = yseg_for(h, tx);
     }
     {
       KScope k(h, RTM_K_ISO);
-      if (h->use_tma) launch_iso_fd8_tma(a, *m1, *m0, *mv, h->dflag, mode, h->c.pml3d, h->st);
+      if (h->use_tma) launch_iso_fd8_tma(a, *m1, *m0, *mv, h->dflag, mode, h->c.pml3d, h->tma_shape, h->st);
       else launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
     }
     return check_launch(h, "iso_fd8_step");
@@ -779,7 +791,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->one_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
-  h->use_tma = c->kernel_variant == 0 && tma_supported(d->nz);
+  h->use_tma = c->kernel_variant == 0 && tma_supported(d->nz) && iso_tma_init();
+  cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
   if ((rc = zero_state(h))) return fail(rc);
   if (cudaStreamSynchronize(h->st) != cudaSuccess) {
@@ -1114,6 +1127,46 @@ int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int
   cudaFree(din), cudaFree(dout), cudaFree(slab), cudaFree(ex), cudaFree(ey), cudaFree(ez);
   cudaGetLastError();
   return rc;
+}
+
+int rtm_autotune(rtm_handle *h, int steps, int *choice) {
+  TRY(rtm::ready(h));
+  if (steps < 1) return RTM_ERR_ARG;
+  // candidate launch shapes of this handle's step kernels
+  struct Cand {
+    int tma_shape, tx;
+  };
+  std::vector<Cand> cands;
+  const bool iso = h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO;
+  if (iso && h->use_tma)
+    for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({k, h->tx});
+  else if (h->c.engine == RTM_ENGINE_FD8)
+    for (int tx : {4, 8, 16}) cands.push_back({h->tma_shape, tx});
+  if (cands.empty()) {
+    if (choice) *choice = 0;
+    return RTM_OK;
+  }
+  const int yseg0 = h->yseg;
+  float best = 1e30f;
+  int bi = 0;
+  for (size_t c = 0; c < cands.size(); c++) {
+    h->tma_shape = cands[c].tma_shape, h->tx = cands[c].tx, h->yseg = rtm::yseg_for(h, cands[c].tx);
+    TRY(rtm::step_kernel(h, 1, rtm::io_none()));  // warm-up (tensor maps, first launch)
+    CK(cudaEventRecord(h->ev0, h->st));
+    for (int s = 0; s < steps; s++) TRY(rtm::step_kernel(h, 1, rtm::io_none()));
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (ms < best) best = ms, bi = (int)c;
+  }
+  h->tma_shape = cands[bi].tma_shape, h->tx = cands[bi].tx;
+  h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
+  if (choice) *choice = bi;
+  TRY(rtm::check_flag(h));
+  TRY(rtm::zero_state(h));
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
 }
 
 int rtm_profile(rtm_handle *h, int on) {

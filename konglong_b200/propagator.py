@@ -147,6 +147,12 @@ class Propagator:
         self._ck(self.L.rtm_last_loop_ms(self.h, C.byref(v)), "rtm_last_loop_ms")
         return v.value
 
+    def autotune(self, steps=5):
+        """Pick the fastest launch shape for this grid (clobbers the state)."""
+        ch = C.c_int(0)
+        self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
+        return ch.value
+
     def launch_count(self):
         v = C.c_longlong()
         self._ck(self.L.rtm_last_loop_launches(self.h, C.byref(v)), "rtm_last_loop_launches")
