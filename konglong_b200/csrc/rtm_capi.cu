@@ -208,14 +208,19 @@ static int yseg_for(Engine *h, int tx) {
 
 static PmlDev pml_dev(Engine *h) { return h->pml; }
 
-// tensor map of a device volume with box (bz, bx, 1), built once per buffer
-static const CUtensorMap *tmap(Engine *h, const void *p, int bz, int bx) {
-  for (auto &t : h->tmaps)
-    if (t.p == p && t.bz == bz && t.bx == bx) return &t.m;
+// tensor map of a device volume with box (bz, bx, 1), built once per buffer;
+// returned by value (the cache may grow and move its entries)
+static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out) {
+  for (const auto &t : h->tmaps)
+    if (t.p == p && t.bz == bz && t.bx == bx) {
+      *out = t.m;
+      return true;
+    }
   Engine::TMap t{p, bz, bx, {}};
-  if (!make_tmap(&t.m, p, h->d.nx, h->d.ny, h->d.nz, bz, bx)) return nullptr;
+  if (!make_tmap(&t.m, p, h->d.nx, h->d.ny, h->d.nz, bz, bx)) return false;
   h->tmaps.push_back(t);
-  return &h->tmaps.back().m;
+  *out = t.m;
+  return true;
 }
 
 static int setup_pml(Engine *h) {
@@ -297,16 +302,16 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     a.pml = pml_dev(h);
     a.io = io;
     a.q = q;
-    const CUtensorMap *m1 = nullptr, *m0 = nullptr, *mv = nullptr;
+    CUtensorMap m1, m0, mv;
     if (h->use_tma) {
       const int tx = kIsoTmaShapes[h->tma_shape].tx;
-      m1 = tmap(h, h->w1, 40, tx + 8), m0 = tmap(h, h->w0, 32, tx), mv = tmap(h, h->vel, 32, tx);
-      if (!m1 || !m0 || !mv) h->use_tma = 0;
+      if (!tmap(h, h->w1, 40, tx + 8, &m1) || !tmap(h, h->w0, 32, tx, &m0) || !tmap(h, h->vel, 32, tx, &mv))
+        h->use_tma = 0;
       else a.yseg = yseg_for(h, tx);
     }
     {
       KScope k(h, RTM_K_ISO);
-      if (h->use_tma) launch_iso_fd8_tma(a, *m1, *m0, *mv, h->dflag, mode, h->c.pml3d, h->tma_shape, h->st);
+      if (h->use_tma) launch_iso_fd8_tma(a, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->tma_shape, h->st);
       else launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
     }
     return check_launch(h, "iso_fd8_step");
