@@ -96,6 +96,10 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_tma(IsoArgs a, const __grid_co
   }
   bool ok = true;
   for (int p = y0 - R; p < y0 + R && ok; p++) ok = mbar_wait(&s.bar_a[stage_a(p)], par_a(p), err);
+  // ring-A stages of the y window iy-R .. iy+R, rotated once per plane
+  int win[2 * R + 1];
+#pragma unroll
+  for (int k = 0; k <= 2 * R; k++) win[k] = stage_a(y0 - R + k);
 
   for (int iy = y0; iy < y1; iy++) {
     if (producer) {
@@ -105,8 +109,7 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_tma(IsoArgs a, const __grid_co
     ok = ok && mbar_wait(&s.bar_a[stage_a(iy + R)], par_a(iy + R), err);
     ok = ok && mbar_wait(&s.bar_b[stage_b(iy)], par_b(iy), err);
     if (act && ok) {
-      const int sy = stage_a(iy);
-      const float(*T)[HZ] = s.a[sy];
+      const float(*T)[HZ] = s.a[win[R]];
       const float u = T[tx + R][tz + R];
       float lz = a.c2z[0] * u, lx = a.c2x[0] * u, ly = 0.0f;
 #pragma unroll
@@ -117,10 +120,7 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_tma(IsoArgs a, const __grid_co
       if (do_y) {
         ly = a.c2y[0] * u;
 #pragma unroll
-        for (int m = 1; m <= R; m++) {
-          const int sm_ = (sy - m + SA) % SA, sp = (sy + m) % SA;
-          ly += a.c2y[m] * (s.a[sm_][tx + R][tz + R] + s.a[sp][tx + R][tz + R]);
-        }
+        for (int m = 1; m <= R; m++) ly += a.c2y[m] * (s.a[win[R - m]][tx + R][tz + R] + s.a[win[R + m]][tx + R][tz + R]);
       }
       float v;
       const bool edge = in_pml(a.pml, g, ix, iy, iz);
@@ -150,6 +150,9 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_tma(IsoArgs a, const __grid_co
       a.w0[i] = out;
     }
     __syncthreads();  // every thread is done with the stages the producer refills next
+#pragma unroll
+    for (int k = 0; k < 2 * R; k++) win[k] = win[k + 1];
+    win[2 * R] = win[2 * R - 1] + 1 == SA ? 0 : win[2 * R - 1] + 1;
   }
 }
 

@@ -22,12 +22,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// try_wait with a suspend-time hint: a waiting warp sleeps (up to ~1 us)
+// until the phase completes instead of spinning on the issue slots
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
       : "memory");
   return ok != 0;
 }
@@ -37,13 +39,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait for the phase of `parity`.  Gives up after 2^20 polls, or as
+// Bounded wait for the phase of `parity`.  Gives up after 2^16 polls, or as
 // soon as another CTA has raised *err, sets *err and returns false (the caller
 // then skips its compute; the copies it waited for are its own).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
-  for (uint32_t it = 0; it < (1u << 20); it++) {
+  for (uint32_t it = 0; it < (1u << 16); it++) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 1023) == 1023 && err && *(volatile int *)err) return false;
+    if ((it & 63) == 63 && err && *(volatile int *)err) return false;
   }
   if (err) atomicExch(err, 1);
   return false;
