@@ -62,6 +62,7 @@ struct CfdPlanDev {
   int n;
   const float *bu, *bl, *am;  // [n][4] upper factor (super-diagonals 1..4), [n][4] multipliers, [60] A
   const float *rdiag;         // [n] 1 / pivot, from the FP64 factorisation
+  const float *lm;            // [n][4] multipliers acting on row i: l[i-1][0], l[i-2][1], l[i-3][2], l[i-4][3]
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();

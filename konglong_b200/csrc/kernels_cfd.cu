@@ -1,16 +1,16 @@
 // kernels_cfd.cu - compact finite differences (FdEngine_cfd + Cfd_plan) on
 // sm_100a.  A derivative along one axis solves B f' = A f for every grid line:
 // the 11-point right-hand side (banmul_*, bgprtm/FdEngine_cfd.cpp:164-201,
-// 304-327) is fused with the forward elimination of the band LU, then the back
-// substitution (banbks_*, bgprtm/FdEngine_cfd.cpp:203-302, 328-356) runs from
-// the far end.  The recurrences are sequential along a line, so parallelism
-// comes from the batch of lines:
-//   x / y lines: one thread per (z, other) line, the walk along the line is a
-//     z-coalesced sweep; the forward results are parked in the output array
-//     and read back by the backward sweep (same thread, same addresses).
-//   z lines (contiguous): a CTA stages 32 lines in shared memory (stride nz+1,
-//     bank-conflict free), one thread walks one line, the result is written
-//     back through shared memory with coalesced stores.
+// 304-327), the forward elimination of the band LU and the back substitution
+// (banbks_*, bgprtm/FdEngine_cfd.cpp:203-302, 328-356).  A CTA stages 32 lines
+// in shared memory (one HBM read and one write per cell):
+//   phase 1  all four warps form the right-hand sides of a quarter of every
+//            line each, in place (embarrassingly parallel along the line);
+//   phase 2  one warp (lane = line) runs the two sequential recurrences in
+//            register chunks of 8 points: the chunk's operands are loaded
+//            together and the next chunk is prefetched, so the dependency
+//            chain is one FMA per point in elimination, FMA + multiply in
+//            back substitution.
 // The PML / scaling / accumulation steps of FdEngine_cfd::d{x,y,z}1_2D and
 // KernelCPU::TTI run as pointwise epilogues afterwards.
 #include "kernel_api.h"
@@ -20,114 +20,158 @@ namespace rtm {
 
 namespace {
 
-// Line solve on an accessor A(i) -> float& into shared memory, in place.
-// Forward: rhs_i = (A x)_i, then y_i = rhs_i - sum_j al[(i-j)*4+j-1] y_{i-j};
-// backward: f_i = (y_i - sum_k bm[i*5+k] f_{i+k}) * (1 / bm[i*5]).  The
-// newest recurrence term is applied last, so one FMA sits on the dependency
-// chain per point; the pivots' reciprocals come from the FP64 plan set-up.
-template <typename Acc>
-__device__ __forceinline__ void cfd_solve_line(const CfdPlanDev &p, Acc A) {
-  const int n = p.n;
-  const float *__restrict__ a = p.am;
-  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
-  const float4 *__restrict__ al4 = reinterpret_cast<const float4 *>(p.bl);
-  const float *__restrict__ rd = p.rdiag;
+constexpr int kChunk = 8;  // points per register chunk (both phases)
+
+// Phase 1: right-hand sides of positions [p0, p1) of one line (element i at
+// L[i * S]), in place, C outputs per chunk from a window of C + 10 inputs
+// carried in registers.  The first and the last five outputs of the range
+// are parked in head / tail and written after a barrier, because the
+// neighbouring warps read those inputs as their window ends.  Rows within 5
+// of a line end use the one-sided rows of A (banmul_dev_z_c,
+// bgprtm/FdEngine_cfd.cpp:304-327).  Requires p1 - p0 to be a multiple of C
+// unless p1 == n.
+template <int S, int C>
+__device__ __forceinline__ void cfd_rhs_range(const float *__restrict__ a, float *L, int n, int p0, int p1,
+                                              float (&head)[5], float (&tail)[5]) {
   const float a55 = __ldg(a + 55), a56 = __ldg(a + 56), a57 = __ldg(a + 57), a58 = __ldg(a + 58),
               a59 = __ldg(a + 59);
-  float xw[11];  // x[i-5 .. i+5]
+  float w[C + 10];
 #pragma unroll
-  for (int k = 0; k < 11; k++) xw[k] = (k >= 5 && k - 5 < n) ? A(k - 5) : 0.f;
+  for (int k = 0; k < 10; k++) {
+    const int j = p0 - 5 + k;
+    w[k] = (j >= 0 && j < n) ? L[j * S] : 0.f;
+  }
+  for (int i0 = p0; i0 < p1; i0 += C) {
+#pragma unroll
+    for (int k = 10; k < C + 10; k++) {
+      const int j = i0 - 5 + k;
+      w[k] = j < n ? L[j * S] : 0.f;
+    }
+    float r[C];
+    if (i0 >= 5 && i0 + C <= n - 5) {
+#pragma unroll
+      for (int k = 0; k < C; k++)
+        r[k] = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
+               a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        const int i = i0 + k;
+        float v = 0.f;
+        if (i < 5) {
+#pragma unroll
+          for (int j = 0; j < 11; j++)
+            if (j >= 5 - i) v = v + __ldg(a + j * 5 + i) * w[k + j];
+        } else if (i >= n - 5) {
+          const int t = n - i;
+#pragma unroll
+          for (int j = 0; j < 11; j++)
+            if (j < t + 5) v = v - __ldg(a + t + 49 - 5 * j) * w[k + j];
+        } else {
+          v = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
+              a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
+        }
+        r[k] = v;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      const int i = i0 + k;
+      if (i < p1) {
+        const bool h = i0 == p0 && k < 5, t = i0 + C == p1 && k >= C - 5;
+        if (h) head[k < 5 ? k : 0] = r[k];
+        if (t) tail[k >= C - 5 ? k - (C - 5) : 0] = r[k];
+        if (!h && !t) L[i * S] = r[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 10; k++) w[k] = w[k + C];
+  }
+}
+
+// Phase 2, forward: y_i = rhs_i - l[i-4][3] y_{i-4} - l[i-3][2] y_{i-3}
+// - l[i-2][1] y_{i-2} - l[i-1][0] y_{i-1}, oldest pivot first, with the
+// row-packed multipliers lm[i] = (l[i-1][0], l[i-2][1], l[i-3][2], l[i-4][3]).
+template <int S, int C>
+__device__ __forceinline__ void cfd_forward(const float4 *__restrict__ lm, float *L, int n) {
   float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
-  // multipliers applied to row i: al[i-1].x, al[i-2].y, al[i-3].z, al[i-4].w
-  float4 m1 = make_float4(0.f, 0.f, 0.f, 0.f), m2 = m1, m3 = m1, m4 = m1;  // rows i-1 .. i-4
-  // rows 0..4: one-sided boundary rows of A
+  float rv[C];
+  float4 m[C];
 #pragma unroll
-  for (int i = 0; i < 5; i++) {
-    float r = 0.f;
-#pragma unroll
-    for (int j = 5 - i; j < 11; j++) r = r + __ldg(a + j * 5 + i) * xw[j];
-    r = r - m4.w * y4;
-    r = r - m3.z * y3;
-    r = r - m2.y * y2;
-    r = r - m1.x * y1;
-#pragma unroll
-    for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
-    xw[10] = (i + 6 < n) ? A(i + 6) : 0.f;
-    A(i) = r;
-    y4 = y3, y3 = y2, y2 = y1, y1 = r;
-    m4 = m3, m3 = m2, m2 = m1, m1 = __ldg(al4 + i);
+  for (int k = 0; k < C; k++) {
+    const int i = min(k, n - 1);
+    rv[k] = L[i * S];
+    m[k] = __ldg(lm + i);
   }
-  // interior rows: antisymmetric 11-point stencil; the next row's multipliers
-  // are fetched one step ahead so no load sits on the recurrence
-  float4 nxt = __ldg(al4 + 5);
-#pragma unroll 2
-  for (int i = 5; i < n - 5; i++) {
-    const float x_ahead = (i + 6 < n) ? A(i + 6) : 0.f;
-    float r = a55 * (xw[6] - xw[4]) + a56 * (xw[7] - xw[3]) + a57 * (xw[8] - xw[2]) + a58 * (xw[9] - xw[1]) +
-              a59 * (xw[10] - xw[0]);
-    r = r - m4.w * y4;
-    r = r - m3.z * y3;
-    r = r - m2.y * y2;
-    r = r - m1.x * y1;
+  for (int i0 = 0; i0 < n; i0 += C) {
+    float nrv[C];
+    float4 nm[C];
 #pragma unroll
-    for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
-    xw[10] = x_ahead;
-    A(i) = r;
-    y4 = y3, y3 = y2, y2 = y1, y1 = r;
-    m4 = m3, m3 = m2, m2 = m1, m1 = nxt;
-    nxt = __ldg(al4 + min(i + 1, n - 1));
+    for (int k = 0; k < C; k++) {
+      const int i = min(i0 + C + k, n - 1);
+      nrv[k] = L[i * S];
+      nm[k] = __ldg(lm + i);
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      float r = rv[k];
+      r = r - m[k].w * y4;
+      r = r - m[k].z * y3;
+      r = r - m[k].y * y2;
+      r = r - m[k].x * y1;
+      y4 = y3, y3 = y2, y2 = y1, y1 = r;
+      rv[k] = r;
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++)
+      if (i0 + k < n) L[(i0 + k) * S] = rv[k];
+#pragma unroll
+    for (int k = 0; k < C; k++) rv[k] = nrv[k], m[k] = nm[k];
   }
-  // rows n-5 .. n-1: the mirrored boundary rows
-#pragma unroll
-  for (int t = 5; t >= 1; t--) {
-    const int i = n - t;
-    float r = 0.f;
-#pragma unroll
-    for (int j = 0; j < 11; j++)
-      if (j < t + 5) r = r - __ldg(a + t + 49 - 5 * j) * xw[j];
-    r = r - m4.w * y4;
-    r = r - m3.z * y3;
-    r = r - m2.y * y2;
-    r = r - m1.x * y1;
-#pragma unroll
-    for (int k = 0; k < 10; k++) xw[k] = xw[k + 1];
-    xw[10] = 0.f;
-    A(i) = r;
-    y4 = y3, y3 = y2, y2 = y1, y1 = r;
-    m4 = m3, m3 = m2, m2 = m1, m1 = __ldg(al4 + i);
-  }
-  // backward substitution: f_i = (y_i - u3 f_{i+4} - u2 f_{i+3} - u1 f_{i+2} - u0 f_{i+1}) / pivot_i
+}
+
+// Phase 2, backward: f_i = (y_i - u3 f_{i+4} - u2 f_{i+3} - u1 f_{i+2}
+// - u0 f_{i+1}) * (1 / pivot_i), the reciprocal pivots from the FP64 plan
+// set-up.  Upper-factor entries beyond the line end are zero.
+template <int S, int C>
+__device__ __forceinline__ void cfd_backward(const float4 *__restrict__ bu4, const float *__restrict__ rd, float *L,
+                                             int n) {
   float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
+  float yv[C], rv[C];
+  float4 u[C];
 #pragma unroll
-  for (int t = 1; t <= 4; t++) {
-    const int i = n - t;
-    const float4 u = __ldg(bu4 + i);
-    float v = A(i);
-    if (t >= 4) v = v - u.z * z3;
-    if (t >= 3) v = v - u.y * z2;
-    if (t >= 2) v = v - u.x * z1;
-    v = v * __ldg(rd + i);
-    A(i) = v;
-    z4 = z3, z3 = z2, z2 = z1, z1 = v;
+  for (int k = 0; k < C; k++) {
+    const int i = max(n - 1 - k, 0);
+    yv[k] = L[i * S];
+    u[k] = __ldg(bu4 + i);
+    rv[k] = __ldg(rd + i);
   }
-  float4 u = __ldg(bu4 + n - 5);
-  float rdi = __ldg(rd + n - 5);
-  float yv = A(n - 5);
-#pragma unroll 2
-  for (int i = n - 5; i >= 0; i--) {
-    const int j = max(i - 1, 0);
-    const float4 un = __ldg(bu4 + j);
-    const float rdn = __ldg(rd + j);
-    const float yn = A(j);
-    float v = yv;
-    v = v - u.w * z4;
-    v = v - u.z * z3;
-    v = v - u.y * z2;
-    v = v - u.x * z1;
-    v = v * rdi;
-    A(i) = v;
-    z4 = z3, z3 = z2, z2 = z1, z1 = v;
-    u = un, rdi = rdn, yv = yn;
+  for (int i0 = n - 1; i0 >= 0; i0 -= C) {
+    float nyv[C], nrv[C];
+    float4 nu[C];
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      const int i = max(i0 - C - k, 0);
+      nyv[k] = L[i * S];
+      nu[k] = __ldg(bu4 + i);
+      nrv[k] = __ldg(rd + i);
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      float v = yv[k];
+      v = v - u[k].w * z4;
+      v = v - u[k].z * z3;
+      v = v - u[k].y * z2;
+      v = v - u[k].x * z1;
+      v = v * rv[k];
+      z4 = z3, z3 = z2, z2 = z1, z1 = v;
+      yv[k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++)
+      if (i0 - k >= 0) L[(i0 - k) * S] = yv[k];
+#pragma unroll
+    for (int k = 0; k < C; k++) yv[k] = nyv[k], u[k] = nu[k], rv[k] = nrv[k];
   }
 }
 
@@ -182,10 +226,29 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
       }
     }
   }
+  // phase 1: right-hand sides, each warp a run of whole chunks of every line
+  constexpr int S = STRIDED ? 32 : 1;
+  float *L = STRIDED ? sm + lane : sm + lane * (n + 1);
+  const int run = (((n + nw - 1) / nw) + kChunk - 1) / kChunk * kChunk;
+  const int p0 = min(n, warp * run), p1 = min(n, p0 + run);
+  float head[5], tail[5];
   __syncthreads();
+  if (lane < nl && p0 < p1) cfd_rhs_range<S, kChunk>(p.am, L, n, p0, p1, head, tail);
+  __syncthreads();
+  if (lane < nl && p0 < p1) {
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+      if (p0 + k < p1) L[(p0 + k) * S] = head[k];
+    if ((p1 - p0) % kChunk == 0) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) L[(p1 - 5 + k) * S] = tail[k];
+    }
+  }
+  __syncthreads();
+  // phase 2: the two sequential recurrences, one warp
   if (warp == 0 && lane < nl) {
-    if (STRIDED) cfd_solve_line(p, [&](int i) -> float & { return sm[i * 32 + lane]; });
-    else cfd_solve_line(p, [&](int i) -> float & { return sm[lane * (n + 1) + i]; });
+    cfd_forward<S, kChunk>(reinterpret_cast<const float4 *>(p.lm), L, n);
+    cfd_backward<S, kChunk>(reinterpret_cast<const float4 *>(p.bu), p.rdiag, L, n);
   }
   __syncthreads();
   if (STRIDED) {

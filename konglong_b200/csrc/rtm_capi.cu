@@ -742,18 +742,22 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
       for (int s = 0; s < 2; s++) {
         std::vector<float> bm, bl, am, rd;
         cfd_plan(nn[a], dd[a], s + 1, bm, bl, am, &rd);
-        std::vector<float> bu(4 * (size_t)nn[a]);
-        for (int i = 0; i < nn[a]; i++)
+        std::vector<float> bu(4 * (size_t)nn[a]), lm(4 * (size_t)nn[a], 0.f);
+        for (int i = 0; i < nn[a]; i++) {
           for (int k = 0; k < 4; k++) bu[(size_t)i * 4 + k] = bm[(size_t)i * 5 + 1 + k];
-        float *dbu, *dbl, *dam, *drd;
+          for (int k = 0; k < 4; k++)
+            if (i - 1 - k >= 0) lm[(size_t)i * 4 + k] = bl[(size_t)(i - 1 - k) * 4 + k];
+        }
+        float *dbu, *dbl, *dam, *drd, *dlm;
         if ((rc = h->alloc(dbu, bu.size())) || (rc = h->alloc(dbl, bl.size())) || (rc = h->alloc(dam, am.size())) ||
-            (rc = h->alloc(drd, rd.size())))
+            (rc = h->alloc(drd, rd.size())) || (rc = h->alloc(dlm, lm.size())))
           return fail(rc);
+        cudaMemcpy(dlm, lm.data(), lm.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(dbu, bu.data(), bu.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(dbl, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(dam, am.data(), am.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(drd, rd.data(), rd.size() * 4, cudaMemcpyHostToDevice);
-        h->cfd[a][s] = CfdPlanDev{nn[a], dbu, dbl, dam, drd};
+        h->cfd[a][s] = CfdPlanDev{nn[a], dbu, dbl, dam, drd, dlm};
       }
     }
   }
