@@ -47,7 +47,7 @@ void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
 // ---- TMA plane pipelines (kernels_tma.cu), nz % 4 == 0 ------------------------
 bool tma_supported(int nz);
 // fp32 volume [ny][nx][nz], box (bz, bx, 1)
-bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx);
+bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx, int by = 1);
 struct TmaShape {
   int tx, depth;  // tile width (x) and planes prefetched beyond the stencil window
 };
@@ -63,12 +63,20 @@ struct CfdPlanDev {
   const float *bu, *bl, *am;  // [n][4] upper factor (super-diagonals 1..4), [n][4] multipliers, [60] A
   const float *rdiag;         // [n] 1 / pivot, from the FP64 factorisation
   const float *lm;            // [n][4] multipliers acting on row i: l[i-1][0], l[i-2][1], l[i-3][2], l[i-4][3]
+  // rows [c0, c1] hold bitwise-identical (lm, bu, rdiag): the factors of the
+  // Toeplitz interior have converged in FP32; c0 > c1 when there is no such run
+  int c0, c1;
+  float lmc[4], buc[4], rdc;
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();
-// raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML)
-void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, float *scratch, int nx, int ny,
-                      int nz, cudaStream_t st);
+// TMA box of the x / y line kernels: nb boxes of R rows (R <= 256) per tile
+void cfd_tma_box(int n, int *R, int *nb);
+// raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML).  For
+// x / y, tensor maps of in / out with box (32, R, 1) / (32, 1, R) select the
+// TMA tile kernel (null: plain loads and stores); err receives wait timeouts.
+void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
+                      const CUtensorMap *tin, const CUtensorMap *tout, int *err, cudaStream_t st);
 
 struct CfdGradEpiArgs {  // PML round 1 + scaling on raw gradients, in place
   int nx, ny, nz, pml3d, model;

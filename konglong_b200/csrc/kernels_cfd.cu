@@ -15,6 +15,7 @@
 // KernelCPU::TTI run as pointwise epilogues afterwards.
 #include "kernel_api.h"
 #include "rtm_device.cuh"
+#include "tma.cuh"
 
 namespace rtm {
 
@@ -92,93 +93,179 @@ __device__ __forceinline__ void cfd_rhs_range(const float *__restrict__ a, float
 // Phase 2, forward: y_i = rhs_i - l[i-4][3] y_{i-4} - l[i-3][2] y_{i-3}
 // - l[i-2][1] y_{i-2} - l[i-1][0] y_{i-1}, oldest pivot first, with the
 // row-packed multipliers lm[i] = (l[i-1][0], l[i-2][1], l[i-3][2], l[i-4][3]).
-template <int S, int C>
-__device__ __forceinline__ void cfd_forward(const float4 *__restrict__ lm, float *L, int n) {
-  float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
+// Rows [b, e) in chunks of C from b, the next chunk prefetched; CST: the
+// multipliers are the register constant mc; PART: the last chunk may run
+// past e (= n), otherwise e - b is a multiple of C.
+struct Chain {
+  float y1, y2, y3, y4;
+};
+
+template <int S, int C, bool CST, bool PART>
+__device__ __forceinline__ void fwd_region(const float4 *__restrict__ lm, float4 mc, float *L, int b, int e, int n,
+                                           Chain &y) {
+  if (b >= e) return;
   float rv[C];
   float4 m[C];
 #pragma unroll
   for (int k = 0; k < C; k++) {
-    const int i = min(k, n - 1);
+    const int i = PART ? min(b + k, n - 1) : b + k;
     rv[k] = L[i * S];
-    m[k] = __ldg(lm + i);
+    if (!CST) m[k] = __ldg(lm + i);
   }
-  for (int i0 = 0; i0 < n; i0 += C) {
+  for (int i0 = b; i0 < e; i0 += C) {
+    const bool more = i0 + C < e;
     float nrv[C];
     float4 nm[C];
+    if (more) {
 #pragma unroll
-    for (int k = 0; k < C; k++) {
-      const int i = min(i0 + C + k, n - 1);
-      nrv[k] = L[i * S];
-      nm[k] = __ldg(lm + i);
+      for (int k = 0; k < C; k++) {
+        const int i = PART ? min(i0 + C + k, n - 1) : i0 + C + k;
+        nrv[k] = L[i * S];
+        if (!CST) nm[k] = __ldg(lm + i);
+      }
     }
 #pragma unroll
     for (int k = 0; k < C; k++) {
+      const float4 c = CST ? mc : m[k];
       float r = rv[k];
-      r = r - m[k].w * y4;
-      r = r - m[k].z * y3;
-      r = r - m[k].y * y2;
-      r = r - m[k].x * y1;
-      y4 = y3, y3 = y2, y2 = y1, y1 = r;
+      r = r - c.w * y.y4;
+      r = r - c.z * y.y3;
+      r = r - c.y * y.y2;
+      r = r - c.x * y.y1;
+      y.y4 = y.y3, y.y3 = y.y2, y.y2 = y.y1, y.y1 = r;
       rv[k] = r;
     }
+    if (!PART || i0 + C <= e) {
 #pragma unroll
-    for (int k = 0; k < C; k++)
-      if (i0 + k < n) L[(i0 + k) * S] = rv[k];
+      for (int k = 0; k < C; k++) L[(i0 + k) * S] = rv[k];
+    } else {
 #pragma unroll
-    for (int k = 0; k < C; k++) rv[k] = nrv[k], m[k] = nm[k];
+      for (int k = 0; k < C; k++)
+        if (i0 + k < e) L[(i0 + k) * S] = rv[k];
+    }
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        rv[k] = nrv[k];
+        if (!CST) m[k] = nm[k];
+      }
+    }
   }
 }
 
 // Phase 2, backward: f_i = (y_i - u3 f_{i+4} - u2 f_{i+3} - u1 f_{i+2}
 // - u0 f_{i+1}) * (1 / pivot_i), the reciprocal pivots from the FP64 plan
-// set-up.  Upper-factor entries beyond the line end are zero.
-template <int S, int C>
-__device__ __forceinline__ void cfd_backward(const float4 *__restrict__ bu4, const float *__restrict__ rd, float *L,
-                                             int n) {
-  float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
+// set-up; upper-factor entries beyond the line end are zero.  Rows hi down
+// to lo in chunks of C; PART: the last chunk may run below lo (= 0).
+template <int S, int C, bool CST, bool PART>
+__device__ __forceinline__ void bwd_region(const float4 *__restrict__ bu4, const float *__restrict__ rd, float4 uc,
+                                           float rc, float *L, int hi, int lo, Chain &z) {
+  if (hi < lo) return;
   float yv[C], rv[C];
   float4 u[C];
 #pragma unroll
   for (int k = 0; k < C; k++) {
-    const int i = max(n - 1 - k, 0);
+    const int i = PART ? max(hi - k, 0) : hi - k;
     yv[k] = L[i * S];
-    u[k] = __ldg(bu4 + i);
-    rv[k] = __ldg(rd + i);
+    if (!CST) u[k] = __ldg(bu4 + i), rv[k] = __ldg(rd + i);
   }
-  for (int i0 = n - 1; i0 >= 0; i0 -= C) {
+  for (int t = hi; t >= lo; t -= C) {
+    const bool more = t - C >= lo;
     float nyv[C], nrv[C];
     float4 nu[C];
+    if (more) {
 #pragma unroll
-    for (int k = 0; k < C; k++) {
-      const int i = max(i0 - C - k, 0);
-      nyv[k] = L[i * S];
-      nu[k] = __ldg(bu4 + i);
-      nrv[k] = __ldg(rd + i);
+      for (int k = 0; k < C; k++) {
+        const int i = PART ? max(t - C - k, 0) : t - C - k;
+        nyv[k] = L[i * S];
+        if (!CST) nu[k] = __ldg(bu4 + i), nrv[k] = __ldg(rd + i);
+      }
     }
 #pragma unroll
     for (int k = 0; k < C; k++) {
+      const float4 c = CST ? uc : u[k];
       float v = yv[k];
-      v = v - u[k].w * z4;
-      v = v - u[k].z * z3;
-      v = v - u[k].y * z2;
-      v = v - u[k].x * z1;
-      v = v * rv[k];
-      z4 = z3, z3 = z2, z2 = z1, z1 = v;
+      v = v - c.w * z.y4;
+      v = v - c.z * z.y3;
+      v = v - c.y * z.y2;
+      v = v - c.x * z.y1;
+      v = v * (CST ? rc : rv[k]);
+      z.y4 = z.y3, z.y3 = z.y2, z.y2 = z.y1, z.y1 = v;
       yv[k] = v;
     }
+    if (!PART || t - C + 1 >= lo) {
 #pragma unroll
-    for (int k = 0; k < C; k++)
-      if (i0 - k >= 0) L[(i0 - k) * S] = yv[k];
+      for (int k = 0; k < C; k++) L[(t - k) * S] = yv[k];
+    } else {
 #pragma unroll
-    for (int k = 0; k < C; k++) yv[k] = nyv[k], u[k] = nu[k], rv[k] = nrv[k];
+      for (int k = 0; k < C; k++)
+        if (t - k >= lo) L[(t - k) * S] = yv[k];
+    }
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        yv[k] = nyv[k];
+        if (!CST) u[k] = nu[k], rv[k] = nrv[k];
+      }
+    }
   }
+}
+
+// Both recurrences of one line: table rows, the constant interior run
+// [c0, c1] from registers, table rows again.
+template <int S, int C>
+__device__ __forceinline__ void cfd_solve(const CfdPlanDev &p, float *L, int n) {
+  const float4 *__restrict__ lm = reinterpret_cast<const float4 *>(p.lm);
+  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
+  const float4 mc = make_float4(p.lmc[0], p.lmc[1], p.lmc[2], p.lmc[3]);
+  const float4 uc = make_float4(p.buc[0], p.buc[1], p.buc[2], p.buc[3]);
+  // forward chunks j cover [jC, jC + C - 1]; constant for ka <= j < kb
+  int ka = (p.c0 + C - 1) / C, kb = (p.c1 + 1) / C;
+  if (p.c0 > p.c1 || ka >= kb) ka = kb = 0;
+  Chain y{0.f, 0.f, 0.f, 0.f};
+  fwd_region<S, C, false, false>(lm, mc, L, 0, ka * C, n, y);
+  fwd_region<S, C, true, false>(lm, mc, L, ka * C, kb * C, n, y);
+  fwd_region<S, C, false, true>(lm, mc, L, kb * C, n, n, y);
+  // backward chunks j cover [n - (j+1)C, n - 1 - jC]; constant for ja <= j < jb
+  int ja = (n - 1 - p.c1 + C - 1) / C, jb = (n - p.c0) / C;
+  if (p.c0 > p.c1 || ja >= jb) ja = jb = 0;
+  Chain z{0.f, 0.f, 0.f, 0.f};
+  bwd_region<S, C, false, false>(bu4, p.rdiag, uc, p.rdc, L, n - 1, n - ja * C, z);
+  bwd_region<S, C, true, false>(bu4, p.rdiag, uc, p.rdc, L, n - 1 - ja * C, n - jb * C, z);
+  bwd_region<S, C, false, true>(bu4, p.rdiag, uc, p.rdc, L, n - 1 - jb * C, 0, z);
+}
+
+// Phases 1 and 2 on a staged tile (element i of this lane's line at L[i*S]);
+// entered after a barrier that follows the staging, leaves the tile final
+// for this warp only (callers barrier before storing).
+template <int S>
+__device__ __forceinline__ void cfd_tile_compute(const CfdPlanDev &p, float *L, int n, int nl, int lane, int warp,
+                                                 int nw) {
+  // phase 1: right-hand sides, each warp a run of whole chunks of every line
+  const int run = (((n + nw - 1) / nw) + kChunk - 1) / kChunk * kChunk;
+  const int p0 = min(n, warp * run), p1 = min(n, p0 + run);
+  float head[5], tail[5];
+  if (lane < nl && p0 < p1) cfd_rhs_range<S, kChunk>(p.am, L, n, p0, p1, head, tail);
+  __syncthreads();
+  if (lane < nl && p0 < p1) {
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+      if (p0 + k < p1) L[(p0 + k) * S] = head[k];
+    if ((p1 - p0) % kChunk == 0) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) L[(p1 - 5 + k) * S] = tail[k];
+    }
+  }
+  __syncthreads();
+  // phase 2: the two sequential recurrences, one warp
+  if (warp == 0 && lane < nl) cfd_solve<S, kChunk>(p, L, n);
 }
 
 // 32 lines per CTA staged through shared memory; warp 0 walks the lines
 // (lane = line), all warps move data.  x / y lines (STRIDED): element i of
 // line l at base + l + i*es, smem [i][32]; z lines: line l at base + l*n + i,
-// smem [l][n+1].  One HBM read and one write per cell.
+// smem [l][n+1] (bank-conflict free), filled by asynchronous 4-byte copies.
+// One HBM read and one write per cell.
 template <bool STRIDED>
 __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__restrict__ in, float *__restrict__ out,
                                                    int nz, long long es, long long other_stride, int n_other,
@@ -210,46 +297,17 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
     const long long l0 = (long long)blockIdx.x * 32;
     nl = (int)min(32LL, nlines - l0);
     base = l0 * n;
-    const int per_line = (n + 31) / 32;  // 32-float chunks per line
-    const int chunks = nl * per_line;
-    for (int c0 = warp * U; c0 < chunks; c0 += nw * U) {
-      float v[U];
-#pragma unroll
-      for (int k = 0; k < U; k++) {
-        const int c = c0 + k, l = c / per_line, i = (c - l * per_line) * 32 + lane;
-        v[k] = (c < chunks && i < n) ? __ldcg(in + base + (long long)l * n + i) : 0.f;
-      }
-#pragma unroll
-      for (int k = 0; k < U; k++) {
-        const int c = c0 + k, l = c / per_line, i = (c - l * per_line) * 32 + lane;
-        if (c < chunks && i < n) sm[l * (n + 1) + i] = v[k];
-      }
+    for (int l = warp; l < nl; l += nw) {
+      const float *src = in + base + (long long)l * n;
+      float *dst = sm + l * (n + 1);
+#pragma unroll 4
+      for (int i = lane; i < n; i += 32) cp_async4(dst + i, src + i);
     }
+    cp_async_wait_all();
   }
-  // phase 1: right-hand sides, each warp a run of whole chunks of every line
   constexpr int S = STRIDED ? 32 : 1;
-  float *L = STRIDED ? sm + lane : sm + lane * (n + 1);
-  const int run = (((n + nw - 1) / nw) + kChunk - 1) / kChunk * kChunk;
-  const int p0 = min(n, warp * run), p1 = min(n, p0 + run);
-  float head[5], tail[5];
   __syncthreads();
-  if (lane < nl && p0 < p1) cfd_rhs_range<S, kChunk>(p.am, L, n, p0, p1, head, tail);
-  __syncthreads();
-  if (lane < nl && p0 < p1) {
-#pragma unroll
-    for (int k = 0; k < 5; k++)
-      if (p0 + k < p1) L[(p0 + k) * S] = head[k];
-    if ((p1 - p0) % kChunk == 0) {
-#pragma unroll
-      for (int k = 0; k < 5; k++) L[(p1 - 5 + k) * S] = tail[k];
-    }
-  }
-  __syncthreads();
-  // phase 2: the two sequential recurrences, one warp
-  if (warp == 0 && lane < nl) {
-    cfd_forward<S, kChunk>(reinterpret_cast<const float4 *>(p.lm), L, n);
-    cfd_backward<S, kChunk>(reinterpret_cast<const float4 *>(p.bu), p.rdiag, L, n);
-  }
+  cfd_tile_compute<S>(p, STRIDED ? sm + lane : sm + lane * (n + 1), n, nl, lane, warp, nw);
   __syncthreads();
   if (STRIDED) {
     for (int i = warp; i < n; i += nw)
@@ -257,6 +315,48 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
   } else {
     for (int l = warp; l < nl; l += nw)
       for (int i = lane; i < n; i += 32) __stcg(out + base + (long long)l * n + i, sm[l * (n + 1) + i]);
+  }
+}
+
+// x / y lines with TMA tile moves: the 32 (z) x n tile arrives as nb boxes of
+// R rows on one mbarrier and leaves as nb bulk tensor stores.  Rows past n in
+// the last box and z >= nz are zero-filled on load and clipped on store.
+// Shared memory: 128 B for the barrier, then the tile [nb*R][32].
+template <int AXIS>
+__global__ void __launch_bounds__(128) cfd_lines_tma_k(CfdPlanDev p, const __grid_constant__ CUtensorMap tin,
+                                                       const __grid_constant__ CUtensorMap tout, int nz, int R, int nb,
+                                                       int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw);
+  float *sm = reinterpret_cast<float *>(smraw + 128);
+  const int n = p.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int iz0 = blockIdx.x * 32, o = blockIdx.y;
+  const int nl = min(32, nz - iz0);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, (uint32_t)nb * (uint32_t)R * 32u * 4u);
+    for (int b = 0; b < nb; b++) {
+      if (AXIS == DX) tma_load_3d(sm + (size_t)b * R * 32, &tin, bar, iz0, b * R, o);
+      else tma_load_3d(sm + (size_t)b * R * 32, &tin, bar, iz0, o, b * R);
+    }
+  }
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
+  if (!ok) return;
+  cfd_tile_compute<32>(p, sm + lane, n, nl, lane, warp, nw);
+  fence_proxy_async();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < nb; b++) {
+      if (AXIS == DX) tma_store_3d(&tout, sm + (size_t)b * R * 32, iz0, b * R, o);
+      else tma_store_3d(&tout, sm + (size_t)b * R * 32, iz0, o, b * R);
+    }
+    bulk_commit();
+    bulk_wait_read();
   }
 }
 
@@ -333,27 +433,41 @@ __global__ void __launch_bounds__(256) cfd_div_epi_k(CfdDivEpiArgs a) {
 
 }  // namespace
 
-void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, float *scratch, int nx, int ny,
-                      int nz, cudaStream_t st) {
-  (void)scratch;
+void cfd_tma_box(int n, int *R, int *nb) {
+  *nb = (n + 255) / 256;
+  *R = (n + *nb - 1) / *nb;
+}
+
+void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
+                      const CUtensorMap *tin, const CUtensorMap *tout, int *err, cudaStream_t st) {
   const long long nxz = (long long)nx * nz;
   if (axis == DZ) {
     const long long nlines = (long long)nx * ny;
     const size_t smem = (size_t)32 * (nz + 1) * sizeof(float);
     cfd_lines_k<false><<<(unsigned)((nlines + 31) / 32), 128, smem, st>>>(p, in, out, nz, 1, 0, 0, nlines);
-  } else {
-    const int n = axis == DX ? nx : ny;
-    const size_t smem = (size_t)32 * n * sizeof(float);
-    dim3 grid((nz + 31) / 32, axis == DX ? ny : nx);
-    if (axis == DX) cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nz, nxz, ny, 0);
-    else cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nxz, nz, nx, 0);
+    return;
   }
+  const int n = axis == DX ? nx : ny;
+  dim3 grid((nz + 31) / 32, axis == DX ? ny : nx);
+  if (tin && tout) {
+    int R, nb;
+    cfd_tma_box(n, &R, &nb);
+    const size_t smem = 128 + (size_t)nb * R * 32 * sizeof(float);
+    if (axis == DX) cfd_lines_tma_k<DX><<<grid, 128, smem, st>>>(p, *tin, *tout, nz, R, nb, err);
+    else cfd_lines_tma_k<DY><<<grid, 128, smem, st>>>(p, *tin, *tout, nz, R, nb, err);
+    return;
+  }
+  const size_t smem = (size_t)32 * n * sizeof(float);
+  if (axis == DX) cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nz, nxz, ny, 0);
+  else cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nxz, nz, nx, 0);
 }
 
 int cfd_init() {
   const int mx = 227 * 1024;
   bool ok = cudaFuncSetAttribute(cfd_lines_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   return ok ? 0 : -1;
 }
 

@@ -182,12 +182,12 @@ static EncodeTiledFn encode_fn() {
 bool tma_supported(int nz) { return nz % 4 == 0 && encode_fn() != nullptr; }
 
 // fp32 volume [ny][nx][nz] with a box of (bz, bx, 1) cells
-bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx) {
+bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx, int by) {
   EncodeTiledFn fn = encode_fn();
   if (!fn || nz % 4 != 0 || ((uintptr_t)base & 15)) return false;
   cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)nx, (cuuint64_t)ny};
   cuuint64_t strides[2] = {(cuuint64_t)nz * 4, (cuuint64_t)nz * nx * 4};
-  cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)bx, 1};
+  cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)bx, (cuuint32_t)by};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

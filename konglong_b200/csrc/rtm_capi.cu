@@ -84,10 +84,11 @@ struct Engine {
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
+  int cfd_tma = 0;  // compact-FD x / y line kernels with TMA tile moves
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
-    int bz, bx;
+    int bz, bx, by;
     CUtensorMap m;
   };
   std::vector<TMap> tmaps;
@@ -206,21 +207,62 @@ static int yseg_for(Engine *h, int tx) {
   return (ny + nseg - 1) / nseg;
 }
 
+// Longest run of rows whose (lm, bu, rdiag) are bitwise identical: in the
+// interior of a line the LU of the Toeplitz band matrix has converged, and
+// the line kernels hold those factors in registers instead of loading them.
+static void cfd_constant_run(int n, const std::vector<float> &lm, const std::vector<float> &bu,
+                             const std::vector<float> &rd, CfdPlanDev &pd) {
+  auto same = [&](int i, int j) {
+    return !memcmp(&lm[(size_t)i * 4], &lm[(size_t)j * 4], 16) && !memcmp(&bu[(size_t)i * 4], &bu[(size_t)j * 4], 16) &&
+           !memcmp(&rd[i], &rd[j], 4);
+  };
+  int best = 0, blo = 0;
+  for (int lo = 0; lo < n;) {
+    int hi = lo;
+    while (hi + 1 < n && same(lo, hi + 1)) hi++;
+    if (hi - lo + 1 > best) best = hi - lo + 1, blo = lo;
+    lo = hi + 1;
+  }
+  if (best < 16) {
+    pd.c0 = 1, pd.c1 = 0;
+    return;
+  }
+  pd.c0 = blo, pd.c1 = blo + best - 1;
+  for (int k = 0; k < 4; k++) pd.lmc[k] = lm[(size_t)blo * 4 + k], pd.buc[k] = bu[(size_t)blo * 4 + k];
+  pd.rdc = rd[blo];
+}
+
 static PmlDev pml_dev(Engine *h) { return h->pml; }
 
 // tensor map of a device volume with box (bz, bx, 1), built once per buffer;
 // returned by value (the cache may grow and move its entries)
-static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out) {
+static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out, int by = 1) {
   for (const auto &t : h->tmaps)
-    if (t.p == p && t.bz == bz && t.bx == bx) {
+    if (t.p == p && t.bz == bz && t.bx == bx && t.by == by) {
       *out = t.m;
       return true;
     }
-  Engine::TMap t{p, bz, bx, {}};
-  if (!make_tmap(&t.m, p, h->d.nx, h->d.ny, h->d.nz, bz, bx)) return false;
+  Engine::TMap t{p, bz, bx, by, {}};
+  if (!make_tmap(&t.m, p, h->d.nx, h->d.ny, h->d.nz, bz, bx, by)) return false;
   h->tmaps.push_back(t);
   *out = t.m;
   return true;
+}
+
+// one compact-FD line derivative; x / y take the TMA tile kernel when the
+// tensor maps can be made (nz % 4 == 0), else plain loads and stores
+static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out) {
+  const rtm_dims &d = h->d;
+  CUtensorMap mi, mo;
+  bool tma = false;
+  if (axis != DZ && h->cfd_tma) {
+    int R, nb;
+    cfd_tma_box(axis == DX ? d.nx : d.ny, &R, &nb);
+    const int bx = axis == DX ? R : 1, by = axis == DX ? 1 : R;
+    tma = tmap(h, in, 32, bx, &mi, by) && tmap(h, out, 32, bx, &mo, by);
+  }
+  launch_cfd_deriv(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, tma ? &mi : nullptr, tma ? &mo : nullptr,
+                   h->dflag, h->st);
 }
 
 static int setup_pml(Engine *h) {
@@ -350,15 +392,15 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   TRY(check_launch(h, "fused_io"));
   {
     KScope k(h, RTM_K_CFD_Z);
-    launch_cfd_deriv(DZ, h->cfd[DZ][0], h->w1, h->pz, h->scr, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DZ, 0, h->w1, h->pz);
   }
   {
     KScope k(h, RTM_K_CFD_X);
-    launch_cfd_deriv(DX, h->cfd[DX][0], h->w1, h->px, h->scr, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DX, 0, h->w1, h->px);
   }
   if (d.ny > 1) {
     KScope k(h, RTM_K_CFD_Y);
-    launch_cfd_deriv(DY, h->cfd[DY][0], h->w1, h->py, h->scr, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DY, 0, h->w1, h->py);
   }
   TRY(check_launch(h, "cfd_deriv(grad)"));
   CfdGradEpiArgs ge{};
@@ -374,17 +416,17 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   // divergence parts: d/dx px -> scr, d/dz pz -> scr2, d/dy py -> px (px is free now)
   {
     KScope k(h, RTM_K_CFD_X);
-    launch_cfd_deriv(DX, h->cfd[DX][1], h->px, h->scr2, h->scr, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DX, 1, h->px, h->scr2);
   }
   float *dzp = h->scr;
   {
     KScope k(h, RTM_K_CFD_Z);
-    launch_cfd_deriv(DZ, h->cfd[DZ][1], h->pz, dzp, nullptr, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DZ, 1, h->pz, dzp);
   }
   float *dyp = nullptr;
   if (d.ny > 1) {
     KScope k(h, RTM_K_CFD_Y);
-    launch_cfd_deriv(DY, h->cfd[DY][1], h->py, h->px, h->pz, d.nx, d.ny, d.nz, h->st);
+    cfd_deriv(h, DY, 1, h->py, h->px);
     dyp = h->px;
   }
   TRY(check_launch(h, "cfd_deriv(div)"));
@@ -757,7 +799,9 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
         cudaMemcpy(dbl, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(dam, am.data(), am.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(drd, rd.data(), rd.size() * 4, cudaMemcpyHostToDevice);
-        h->cfd[a][s] = CfdPlanDev{nn[a], dbu, dbl, dam, drd, dlm};
+        CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f};
+        cfd_constant_run(nn[a], lm, bu, rd, pd);
+        h->cfd[a][s] = pd;
       }
     }
   }
@@ -801,6 +845,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
   h->use_tma = c->kernel_variant == 0 && tma_supported(d->nz) && iso_tma_init();
+  h->cfd_tma = c->kernel_variant == 0 && c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
   cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
   if ((rc = zero_state(h))) return fail(rc);

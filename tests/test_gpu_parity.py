@@ -198,10 +198,12 @@ def test_fused_loop_equals_stepwise_calls():
     assert rel_l2(a.get(FIELD_W1), b.get(FIELD_W1)) < 1e-6
 
 
-@pytest.mark.parametrize("builder,scale", [(W.iso128, 0.375)])
+@pytest.mark.parametrize("builder,scale", [(W.iso128, 0.375), (W.vti_cfd, 0.2), (W.vti_cfd, 0.55)])
 def test_tma_pipeline_equals_register_pipeline(builder, scale):
-    """The TMA plane pipeline and the register-prefetch kernel compute the same
-    arithmetic in the same order: equal results."""
+    """The TMA pipelines (FD8 plane ring; compact-FD x / y line tiles moved by
+    bulk tensor copies, one and two boxes per tile, ragged last z tile) and the
+    plain-load kernels compute the same arithmetic in the same order: equal
+    results."""
     shot = builder(scale=scale, nt=60)
     out = []
     for variant in (0, 1):
