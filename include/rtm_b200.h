@@ -91,7 +91,9 @@ typedef struct rtm_config {
   float pml3d_scaler; /* cross-term damping scale, default 0.3 */
   int top_pml;        /* default 1; 0 = free surface top (no z1 PML) */
   int state_fp16;     /* 0: FP32 wavefield state (default) */
-  int kernel_variant; /* 0: auto (TMA plane pipeline when nz % 4 == 0), 1: register pipeline */
+  int kernel_variant; /* 0: auto (ISO FD8: TMA plane pipeline when nz % 4 == 0; compact FD: register-
+                         streamed x / y line solves, the autotuner may pick TMA tiles), 1: register
+                         pipeline / plain staged tiles, 2: compact-FD x / y TMA tiles */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;
@@ -226,8 +228,9 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
 /* Autotuner: times `steps` fused steps of every launch shape this handle's
  * kernels offer (TMA tile width / prefetch depth for ISO FD8, tile width of
- * the FD8 gradient / divergence passes), keeps the fastest, returns its index
- * in *choice, then zeroes the wavefields and PML memory (as rtm_reset). */
+ * the FD8 gradient / divergence passes, register-streamed or TMA-tiled x / y
+ * line solves for compact FD), keeps the fastest, returns its index in
+ * *choice, then zeroes the wavefields and PML memory (as rtm_reset). */
 int rtm_autotune(rtm_handle *h, int steps, int *choice);
 
 /* Kernels launched by the last rtm_modelling / rtm_migration call. */

@@ -67,6 +67,7 @@ struct CfdPlanDev {
   // Toeplitz interior have converged in FP32; c0 > c1 when there is no such run
   int c0, c1;
   float lmc[4], buc[4], rdc;
+  float a[60];  // copy of am, read from the kernel-parameter (constant) bank
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();
@@ -77,6 +78,9 @@ void cfd_tma_box(int n, int *R, int *nb);
 // TMA tile kernel (null: plain loads and stores); err receives wait timeouts.
 void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                       const CUtensorMap *tin, const CUtensorMap *tout, int *err, cudaStream_t st);
+// x / y derivative by the register-streamed kernel (no shared memory)
+void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
+                             cudaStream_t st);
 
 struct CfdGradEpiArgs {  // PML round 1 + scaling on raw gradients, in place
   int nx, ny, nz, pml3d, model;

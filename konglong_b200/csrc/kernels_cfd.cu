@@ -22,6 +22,9 @@ namespace rtm {
 namespace {
 
 constexpr int kChunk = 8;  // points per register chunk (both phases)
+// prefetch depth (chunks) of the streamed x / y kernel with 32- / 64-bit line
+// offsets: the deepest that fits 128 registers without spilling
+constexpr int kStreamD = 3, kStreamDWide = 2;
 
 // Phase 1: right-hand sides of positions [p0, p1) of one line (element i at
 // L[i * S]), in place, C outputs per chunk from a window of C + 10 inputs
@@ -29,13 +32,13 @@ constexpr int kChunk = 8;  // points per register chunk (both phases)
 // are parked in head / tail and written after a barrier, because the
 // neighbouring warps read those inputs as their window ends.  Rows within 5
 // of a line end use the one-sided rows of A (banmul_dev_z_c,
-// bgprtm/FdEngine_cfd.cpp:304-327).  Requires p1 - p0 to be a multiple of C
-// unless p1 == n.
+// bgprtm/FdEngine_cfd.cpp:304-327); A is the plan's copy in the
+// kernel-parameter bank (uniform, runtime-indexed reads).  Requires p1 - p0
+// to be a multiple of C unless p1 == n.
 template <int S, int C>
-__device__ __forceinline__ void cfd_rhs_range(const float *__restrict__ a, float *L, int n, int p0, int p1,
-                                              float (&head)[5], float (&tail)[5]) {
-  const float a55 = __ldg(a + 55), a56 = __ldg(a + 56), a57 = __ldg(a + 57), a58 = __ldg(a + 58),
-              a59 = __ldg(a + 59);
+__device__ __forceinline__ void cfd_rhs_range(const float (&a)[60], float *L, int n, int p0, int p1, float (&head)[5],
+                                              float (&tail)[5]) {
+  const float a55 = a[55], a56 = a[56], a57 = a[57], a58 = a[58], a59 = a[59];
   float w[C + 10];
 #pragma unroll
   for (int k = 0; k < 10; k++) {
@@ -62,12 +65,12 @@ __device__ __forceinline__ void cfd_rhs_range(const float *__restrict__ a, float
         if (i < 5) {
 #pragma unroll
           for (int j = 0; j < 11; j++)
-            if (j >= 5 - i) v = v + __ldg(a + j * 5 + i) * w[k + j];
+            if (j >= 5 - i) v = v + a[j * 5 + i] * w[k + j];
         } else if (i >= n - 5) {
           const int t = n - i;
 #pragma unroll
           for (int j = 0; j < 11; j++)
-            if (j < t + 5) v = v - __ldg(a + t + 49 - 5 * j) * w[k + j];
+            if (j < t + 5) v = v - a[t + 49 - 5 * j] * w[k + j];
         } else {
           v = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
               a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
@@ -245,7 +248,7 @@ __device__ __forceinline__ void cfd_tile_compute(const CfdPlanDev &p, float *L, 
   const int run = (((n + nw - 1) / nw) + kChunk - 1) / kChunk * kChunk;
   const int p0 = min(n, warp * run), p1 = min(n, p0 + run);
   float head[5], tail[5];
-  if (lane < nl && p0 < p1) cfd_rhs_range<S, kChunk>(p.am, L, n, p0, p1, head, tail);
+  if (lane < nl && p0 < p1) cfd_rhs_range<S, kChunk>(p.a, L, n, p0, p1, head, tail);
   __syncthreads();
   if (lane < nl && p0 < p1) {
 #pragma unroll
@@ -318,6 +321,208 @@ __global__ void __launch_bounds__(128) cfd_lines_k(CfdPlanDev p, const float *__
   }
 }
 
+// x / y lines streamed through registers, no shared memory: lane = z line,
+// one warp per 32 z of one line set (element i of a line at X[i * es]).
+// Forward: the 11-point right-hand side (one-sided rows at both ends) fused
+// with the elimination.  x arrives in chunks of C rows into a ring of R =
+// D + 2 register slots (chunk c in slot c % R, prefetched D + 1 chunks
+// ahead); the chunk loop is unrolled by R so every window read is a static
+// register.  y is parked in `out` (L2-resident until read back).  Backward:
+// y read back in reverse through a ring of D + 1 slots and overwritten by f'.
+// Lanes past nz read a valid column and store nothing.  Arithmetic and its
+// order are those of the staged kernels: the results are bitwise equal.
+template <int D, typename Off>
+__global__ void __launch_bounds__(128, 4) cfd_stream_k(const CfdPlanDev p, const float *__restrict__ in, float *out,
+                                                       int nz, long long es, long long other_stride, long long ntask) {
+  constexpr int C = kChunk, R = D + 2, RB = D + 1;
+  const int lane = threadIdx.x & 31;
+  const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (task >= ntask) return;
+  const int nzc = (nz + 31) >> 5;
+  const int izc = (int)(task % nzc);
+  const long long o = task / nzc;
+  const int iz = izc * 32 + lane;
+  const bool act = iz < nz;
+  const long long off = o * other_stride + min(iz, nz - 1);
+  const float *X = in + off;
+  float *Y = out + off;
+  const Off e = (Off)es;
+  const int n = p.n;
+  const int nch = (n + C - 1) / C;
+  const float a55 = p.a[55], a56 = p.a[56], a57 = p.a[57], a58 = p.a[58], a59 = p.a[59];
+
+  // ---- right-hand sides of the one-sided end rows
+  float rbf[5], rbb[5];
+  {
+    float xf[11], xb[11];
+#pragma unroll
+    for (int m = 0; m < 11; m++) xf[m] = __ldcs(X + (Off)m * e), xb[m] = __ldcs(X + (Off)(n - 11 + m) * e);
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      float v = 0.f;
+#pragma unroll
+      for (int j = 5 - i; j < 11; j++) v = v + p.a[j * 5 + i] * xf[i - 5 + j];
+      rbf[i] = v;
+    }
+#pragma unroll
+    for (int t = 5; t >= 1; t--) {
+      float v = 0.f;
+#pragma unroll
+      for (int j = 0; j < t + 5; j++) v = v - p.a[t + 49 - 5 * j] * xb[6 - t + j];
+      rbb[5 - t] = v;
+    }
+  }
+
+  // ---- forward: fused right-hand side + elimination
+  const float4 *__restrict__ lm = reinterpret_cast<const float4 *>(p.lm);
+  const float4 mc = make_float4(p.lmc[0], p.lmc[1], p.lmc[2], p.lmc[3]);
+  int ka = (p.c0 + C - 1) / C, kb = (p.c1 + 1) / C;
+  if (p.c0 > p.c1 || ka >= kb) ka = kb = 0;
+  float xr[R][C];
+  auto load_chunk = [&](float(&dst)[C], int c) {
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      const int i = c * C + k;
+      dst[k] = i < n ? __ldcs(X + (Off)i * e) : 0.f;
+    }
+  };
+#pragma unroll
+  for (int k = 0; k < C; k++) xr[R - 1][k] = 0.f;  // chunk -1
+#pragma unroll
+  for (int d = 0; d <= D; d++) load_chunk(xr[d], d);
+  float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
+  for (int c0 = 0; c0 < nch; c0 += R) {
+#pragma unroll
+    for (int s = 0; s < R; s++) {
+      const int c = c0 + s;
+      if (c < nch) {
+        const int sp = (s + R - 1) % R, sn = (s + 1) % R;
+        // x at chunk-relative row q in [-5, C + 5)
+        auto xa = [&](int q) -> float { return q < 0 ? xr[sp][C + q] : q < C ? xr[s][q] : xr[sn][q - C]; };
+        const int i0 = c * C;
+        const bool cst = c >= ka && c < kb;
+        float4 m[C];
+        if (!cst) {
+#pragma unroll
+          for (int k = 0; k < C; k++) m[k] = __ldg(lm + min(i0 + k, n - 1));
+        }
+        float r[C];
+#pragma unroll
+        for (int k = 0; k < C; k++)
+          r[k] = a55 * (xa(k + 1) - xa(k - 1)) + a56 * (xa(k + 2) - xa(k - 2)) + a57 * (xa(k + 3) - xa(k - 3)) +
+                 a58 * (xa(k + 4) - xa(k - 4)) + a59 * (xa(k + 5) - xa(k - 5));
+        if (i0 < 5 || i0 + C > n - 5) {
+#pragma unroll
+          for (int k = 0; k < C; k++) {
+            const int i = i0 + k;
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+              if (i == q) r[k] = rbf[q];
+              if (i == n - 5 + q) r[k] = rbb[q];
+            }
+          }
+        }
+        // slot sp (chunk c - 1) is free now: chunk c + D + 1 goes there
+        load_chunk(xr[sp], c + D + 1);
+        if (cst) {
+#pragma unroll
+          for (int k = 0; k < C; k++) {
+            float v = r[k];
+            v = v - mc.w * y4;
+            v = v - mc.z * y3;
+            v = v - mc.y * y2;
+            v = v - mc.x * y1;
+            y4 = y3, y3 = y2, y2 = y1, y1 = v;
+            r[k] = v;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < C; k++) {
+            float v = r[k];
+            v = v - m[k].w * y4;
+            v = v - m[k].z * y3;
+            v = v - m[k].y * y2;
+            v = v - m[k].x * y1;
+            y4 = y3, y3 = y2, y2 = y1, y1 = v;
+            r[k] = v;
+          }
+        }
+        if (act) {
+#pragma unroll
+          for (int k = 0; k < C; k++)
+            if (i0 + k < n) __stcg(Y + (Off)(i0 + k) * e, r[k]);
+        }
+      }
+    }
+  }
+
+  // ---- backward: chunks j cover rows n-1-jC down to n-(j+1)C
+  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
+  const float *__restrict__ rd = p.rdiag;
+  const float4 uc = make_float4(p.buc[0], p.buc[1], p.buc[2], p.buc[3]);
+  const float rc = p.rdc;
+  int ja = (n - 1 - p.c1 + C - 1) / C, jb = (n - p.c0) / C;
+  if (p.c0 > p.c1 || ja >= jb) ja = jb = 0;
+  float yr[RB][C];
+  auto load_back = [&](float(&dst)[C], int j) {
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      const int i = n - 1 - j * C - k;
+      dst[k] = i >= 0 ? __ldcg(Y + (Off)i * e) : 0.f;
+    }
+  };
+#pragma unroll
+  for (int d = 0; d < RB; d++) load_back(yr[d], d);
+  float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
+  for (int j0 = 0; j0 < nch; j0 += RB) {
+#pragma unroll
+    for (int s = 0; s < RB; s++) {
+      const int j = j0 + s;
+      if (j < nch) {
+        const int t = n - 1 - j * C;
+        const bool cst = j >= ja && j < jb;
+        float v[C];
+#pragma unroll
+        for (int k = 0; k < C; k++) v[k] = yr[s][k];
+        load_back(yr[s], j + RB);
+        if (cst) {
+#pragma unroll
+          for (int k = 0; k < C; k++) {
+            float w = v[k];
+            w = w - uc.w * z4;
+            w = w - uc.z * z3;
+            w = w - uc.y * z2;
+            w = w - uc.x * z1;
+            w = w * rc;
+            z4 = z3, z3 = z2, z2 = z1, z1 = w;
+            v[k] = w;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < C; k++) {
+            const int i = max(t - k, 0);
+            const float4 u = __ldg(bu4 + i);
+            const float rr = __ldg(rd + i);
+            float w = v[k];
+            w = w - u.w * z4;
+            w = w - u.z * z3;
+            w = w - u.y * z2;
+            w = w - u.x * z1;
+            w = w * rr;
+            z4 = z3, z3 = z2, z2 = z1, z1 = w;
+            v[k] = w;
+          }
+        }
+        if (act) {
+#pragma unroll
+          for (int k = 0; k < C; k++)
+            if (t - k >= 0) __stcg(Y + (Off)(t - k) * e, v[k]);
+        }
+      }
+    }
+  }
+}
+
 // x / y lines with TMA tile moves: the 32 (z) x n tile arrives as nb boxes of
 // R rows on one mbarrier and leaves as nb bulk tensor stores.  Rows past n in
 // the last box and z >= nz are zero-filled on load and clipped on store.
@@ -360,75 +565,130 @@ __global__ void __launch_bounds__(128) cfd_lines_tma_k(CfdPlanDev p, const __gri
   }
 }
 
-// pointwise epilogues: block (32 z, 8 x), grid (z tiles, x tiles, ny)
-__global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
-  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
-  if (iz >= a.nz || ix >= a.nx) return;
-  const bool do_y = a.ny > 1;
-  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
-  {
-    float gz = a.gz[i], gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f;
-    if (in_pml(a.pml, g, ix, iy, iz)) {
-      pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
-      pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
-      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
-    }
-    if (a.model >= 2) {
-      float e = __ldg(a.eps + i);
-      const float dl = e - __ldg(a.del + i);
-      e = 1.0f + 2.0f * e;
-      if (a.model == 3) {
-        const float ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
-        const float az = sqrtf(1.0f - (ax * ax + ay * ay));
-        const float v2 = gx * gx + gy * gy + gz * gz;
-        const float vzz = gx * ax + gy * ay + gz * az;
-        const float vz2 = vzz * vzz, vh2 = v2 - vz2;
-        const float ecl = e * vh2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-        const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
-        const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
-        gx = (bx + (gx - bx) * e) * sc;
-        gy = (by + (gy - by) * e) * sc;
-        gz = (bz + (gz - bz) * e) * sc;
-      } else {
-        const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
-        const float ecl = e * vx2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-        const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
-        gx *= sc2;
-        gy *= sc2;
-      }
-    }
-    a.gz[i] = gz;
-    a.gx[i] = gx;
-    if (do_y) a.gy[i] = gy;
+// V consecutive floats at p (V = 4: one 16-byte access; p 16-byte aligned)
+template <int V>
+__device__ __forceinline__ void ldv(float (&v)[V], const float *p) {
+  if constexpr (V == 4) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; k++) v[k] = p[k];
+  }
+}
+template <int V>
+__device__ __forceinline__ void stv(float *p, const float (&v)[V]) {
+  if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else {
+#pragma unroll
+    for (int k = 0; k < V; k++) p[k] = v[k];
   }
 }
 
+// Pointwise epilogues: block (32, 8) threads, each thread V consecutive z
+// cells (V = 4 when nz % 4 == 0); grid (z tiles, x tiles, ny).  Every input
+// of a cell is loaded before the PML branch, so a cell costs one memory
+// round trip; PML cells then run the split-field recursion per cell.
+template <int V>
+__global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int iz0 = (blockIdx.x * 32 + threadIdx.x) * V, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz0 >= a.nz || ix >= a.nx) return;
+  const bool do_y = a.ny > 1;
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz0;
+  float gz[V], gx[V], gy[V], ep[V], dl[V], px[V], py[V];
+  ldv<V>(gz, a.gz + i);
+  ldv<V>(gx, a.gx + i);
+  if (do_y) ldv<V>(gy, a.gy + i);
+  else {
+#pragma unroll
+    for (int k = 0; k < V; k++) gy[k] = 0.f;
+  }
+  if (a.model >= 2) {
+    ldv<V>(ep, a.eps + i);
+    ldv<V>(dl, a.del + i);
+  }
+  if (a.model == 3) {
+    ldv<V>(px, a.pjx + i);
+    if (do_y) ldv<V>(py, a.pjy + i);
+    else {
+#pragma unroll
+      for (int k = 0; k < V; k++) py[k] = 0.f;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    const int iz = iz0 + k;
+    if (in_pml(a.pml, g, ix, iy, iz)) {
+      pml1(a.pml, g, a.pml3d, DZ, 0, gz[k], ix, iy, iz);
+      pml1(a.pml, g, a.pml3d, DX, 0, gx[k], ix, iy, iz);
+      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy[k], ix, iy, iz);
+    }
+    if (a.model >= 2) {
+      float e = ep[k];
+      const float d = e - dl[k];
+      e = 1.0f + 2.0f * e;
+      if (a.model == 3) {
+        const float ax = px[k], ay = py[k];
+        const float az = sqrtf(1.0f - (ax * ax + ay * ay));
+        const float v2 = gx[k] * gx[k] + gy[k] * gy[k] + gz[k] * gz[k];
+        const float vzz = gx[k] * ax + gy[k] * ay + gz[k] * az;
+        const float vz2 = vzz * vzz, vh2 = v2 - vz2;
+        const float ecl = e * vh2 + vz2;
+        const float parts = sqrtf(1.0f - 8.0f * (d * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
+        const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
+        const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
+        gx[k] = (bx + (gx[k] - bx) * e) * sc;
+        gy[k] = (by + (gy[k] - by) * e) * sc;
+        gz[k] = (bz + (gz[k] - bz) * e) * sc;
+      } else {
+        const float vx2 = gx[k] * gx[k] + gy[k] * gy[k], vz2 = gz[k] * gz[k];
+        const float ecl = e * vx2 + vz2;
+        const float parts = sqrtf(1.0f - 8.0f * (d * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
+        const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
+        gx[k] *= sc2;
+        gy[k] *= sc2;
+      }
+    }
+  }
+  stv<V>(a.gz + i, gz);
+  stv<V>(a.gx + i, gx);
+  if (do_y) stv<V>(a.gy + i, gy);
+}
+
+template <int V>
 __global__ void __launch_bounds__(256) cfd_div_epi_k(CfdDivEpiArgs a) {
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
-  if (iz >= a.nz || ix >= a.nx) return;
+  const int iz0 = (blockIdx.x * 32 + threadIdx.x) * V, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
+  if (iz0 >= a.nz || ix >= a.nx) return;
   const bool do_y = a.ny > 1 && a.dy;
-  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
-  float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
-  if (in_pml(a.pml, g, ix, iy, iz)) {
-    pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
-    pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
-    if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
-  }
-  const float vel = __ldg(a.vel + i);
-  float t = a.w0[i] - dxv * vel;
-  t = t - dzv * vel;
-  t = t - dyv * vel;
-  float out;
-  if (a.mode == 0) out = t;
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz0;
+  float dxv[V], dzv[V], dyv[V], vel[V], w0[V], w1[V];
+  ldv<V>(dxv, a.dx + i);
+  ldv<V>(dzv, a.dz + i);
+  if (do_y) ldv<V>(dyv, a.dy + i);
   else {
-    const float u = __ldg(a.w1 + i);
-    out = a.mode == 1 ? (u + u) - t : q_update(a.q, i, g.nxz * a.ny, t, u);
+#pragma unroll
+    for (int k = 0; k < V; k++) dyv[k] = 0.f;
   }
-  a.w0[i] = out;
+  ldv<V>(vel, a.vel + i);
+  ldv<V>(w0, a.w0 + i);
+  if (a.mode != 0) ldv<V>(w1, a.w1 + i);
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    const int iz = iz0 + k;
+    if (in_pml(a.pml, g, ix, iy, iz)) {
+      pml1(a.pml, g, a.pml3d, DX, 1, dxv[k], ix, iy, iz);
+      pml1(a.pml, g, a.pml3d, DZ, 1, dzv[k], ix, iy, iz);
+      if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv[k], ix, iy, iz);
+    }
+    float t = w0[k] - dxv[k] * vel[k];
+    t = t - dzv[k] * vel[k];
+    t = t - dyv[k] * vel[k];
+    if (a.mode == 0) w0[k] = t;
+    else w0[k] = a.mode == 1 ? (w1[k] + w1[k]) - t : q_update(a.q, i + k, g.nxz * a.ny, t, w1[k]);
+  }
+  stv<V>(a.w0 + i, w0);
 }
 
 }  // namespace
@@ -462,6 +722,17 @@ void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out
   else cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nxz, nz, nx, 0);
 }
 
+void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
+                             cudaStream_t st) {
+  const long long nxz = (long long)nx * nz;
+  const long long ntask = (long long)((nz + 31) / 32) * (axis == DX ? ny : nx);
+  const unsigned blocks = (unsigned)((ntask + 3) / 4);
+  const long long es = axis == DX ? nz : nxz, other = axis == DX ? nxz : nz;
+  // 32-bit element offsets along a line when they cannot overflow
+  if ((long long)p.n * es < (1LL << 31)) cfd_stream_k<kStreamD, int><<<blocks, 128, 0, st>>>(p, in, out, nz, es, other, ntask);
+  else cfd_stream_k<kStreamDWide, long long><<<blocks, 128, 0, st>>>(p, in, out, nz, es, other, ntask);
+}
+
 int cfd_init() {
   const int mx = 227 * 1024;
   bool ok = cudaFuncSetAttribute(cfd_lines_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
@@ -472,11 +743,11 @@ int cfd_init() {
 }
 
 void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st) {
-  cfd_grad_epi_k<<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
+  cfd_grad_epi_k<1><<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
 }
 
 void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
-  cfd_div_epi_k<<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
+  cfd_div_epi_k<1><<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
 }
 
 }  // namespace rtm

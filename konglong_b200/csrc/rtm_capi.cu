@@ -84,7 +84,8 @@ struct Engine {
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
-  int cfd_tma = 0;  // compact-FD x / y line kernels with TMA tile moves
+  int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
+  int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -249,13 +250,18 @@ static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out, int
   return true;
 }
 
-// one compact-FD line derivative; x / y take the TMA tile kernel when the
-// tensor maps can be made (nz % 4 == 0), else plain loads and stores
+// one compact-FD line derivative.  x / y: the register-streamed kernel
+// (cfd_xy 0), the TMA tile kernel (1, when the tensor maps can be made:
+// nz % 4 == 0) or the plain staged tile kernel (2)
 static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out) {
   const rtm_dims &d = h->d;
+  if (axis != DZ && h->cfd_xy == 0) {
+    launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
+    return;
+  }
   CUtensorMap mi, mo;
   bool tma = false;
-  if (axis != DZ && h->cfd_tma) {
+  if (axis != DZ && h->cfd_xy == 1 && h->cfd_tma) {
     int R, nb;
     cfd_tma_box(axis == DX ? d.nx : d.ny, &R, &nb);
     const int bx = axis == DX ? R : 1, by = axis == DX ? 1 : R;
@@ -799,7 +805,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
         cudaMemcpy(dbl, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(dam, am.data(), am.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(drd, rd.data(), rd.size() * 4, cudaMemcpyHostToDevice);
-        CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f};
+        CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f, {}};
+        for (int k = 0; k < 60; k++) pd.a[k] = am[k];
         cfd_constant_run(nn[a], lm, bu, rd, pd);
         h->cfd[a][s] = pd;
       }
@@ -844,8 +851,9 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->one_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
-  h->use_tma = c->kernel_variant == 0 && tma_supported(d->nz) && iso_tma_init();
-  h->cfd_tma = c->kernel_variant == 0 && c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
+  h->use_tma = c->kernel_variant != 1 && tma_supported(d->nz) && iso_tma_init();
+  h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
+  h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
   if ((rc = zero_state(h))) return fail(rc);
@@ -1188,14 +1196,18 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
   if (steps < 1) return RTM_ERR_ARG;
   // candidate launch shapes of this handle's step kernels
   struct Cand {
-    int tma_shape, tx;
+    int tma_shape, tx, cfd_xy;
   };
   std::vector<Cand> cands;
   const bool iso = h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO;
   if (iso && h->use_tma)
-    for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({k, h->tx});
+    for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({k, h->tx, h->cfd_xy});
   else if (h->c.engine == RTM_ENGINE_FD8)
-    for (int tx : {4, 8, 16}) cands.push_back({h->tma_shape, tx});
+    for (int tx : {4, 8, 16}) cands.push_back({h->tma_shape, tx, h->cfd_xy});
+  else if (h->c.kernel_variant == 0) {
+    cands.push_back({h->tma_shape, h->tx, 0});
+    if (h->cfd_tma) cands.push_back({h->tma_shape, h->tx, 1});
+  }
   if (cands.empty()) {
     if (choice) *choice = 0;
     return RTM_OK;
@@ -1205,6 +1217,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
   int bi = 0;
   for (size_t c = 0; c < cands.size(); c++) {
     h->tma_shape = cands[c].tma_shape, h->tx = cands[c].tx, h->yseg = rtm::yseg_for(h, cands[c].tx);
+    h->cfd_xy = cands[c].cfd_xy;
     TRY(rtm::step_kernel(h, 1, rtm::io_none()));  // warm-up (tensor maps, first launch)
     CK(cudaEventRecord(h->ev0, h->st));
     for (int s = 0; s < steps; s++) TRY(rtm::step_kernel(h, 1, rtm::io_none()));
@@ -1214,7 +1227,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (ms < best) best = ms, bi = (int)c;
   }
-  h->tma_shape = cands[bi].tma_shape, h->tx = cands[bi].tx;
+  h->tma_shape = cands[bi].tma_shape, h->tx = cands[bi].tx, h->cfd_xy = cands[bi].cfd_xy;
   h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
   if (choice) *choice = bi;
   TRY(rtm::check_flag(h));

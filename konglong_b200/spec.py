@@ -38,7 +38,7 @@ class PropSpec:
     pml3d_scaler: float = 0.3
     top_pml: bool = True
     state_fp16: bool = False
-    kernel_variant: int = 0       # 0 auto (TMA pipeline), 1 register pipeline
+    kernel_variant: int = 0       # 0 auto, 1 register pipeline / plain tiles, 2 CFD x/y TMA tiles
 
     @property
     def n(self):
