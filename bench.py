@@ -68,6 +68,14 @@ def kernel_alg_bytes(spec, m):
             "fused_io": 6.0, "slab_max": 4.0}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
+# launch, from ncu captures of the same kernels on the 0.75-scale grid of the
+# vti_cfd workload (profiles/*_vti_cfd_384x384x300.md).  The PML slabs scale
+# with the grid, so bytes per cell carry over to the full grid.
+MEASURED_DRAM_B_PER_CELL = {"vti_cfd": {"cfd_div_epilogue": 36.98, "cfd_grad_epilogue": 40.64,
+                                        "cfd_x": 6.87, "cfd_y": 6.87}}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -114,22 +122,22 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def build_workload(name, steps_total):
+def build_workload(name, steps_total, scale=1.0):
     from konglong_b200 import workloads as W
     if name == "vti_cfd":
-        return W.vti_cfd(scale=1.0, nt=steps_total)
+        return W.vti_cfd(scale=scale, nt=steps_total)
     if name == "iso128":
-        return W.iso128(scale=1.0, nt=steps_total)
+        return W.iso128(scale=scale, nt=steps_total)
     if name == "tti_q":
-        return W.tti_q(scale=1.0, nt=steps_total)
+        return W.tti_q(scale=scale, nt=steps_total)
     if name == "iso512":
-        shot = W.vti_cfd(scale=1.0, nt=steps_total)
+        shot = W.vti_cfd(scale=scale, nt=steps_total)
         shot.spec.engine, shot.spec.model_type = 0, 1
         shot.eps = shot.dl = None
         shot.name = "iso512"
         return shot
     if name == "vti_fd8":
-        shot = W.vti_cfd(scale=1.0, nt=steps_total)
+        shot = W.vti_cfd(scale=scale, nt=steps_total)
         shot.spec.engine = 0
         shot.name = "vti_fd8"
         return shot
@@ -142,7 +150,7 @@ def config_of(shot, snap_fmt, steps):
                         f"{['', 'ISO', 'VTI', 'TTI'][s.model_type]}{'+Q' if s.use_q else ''}, PML {s.nbnd[0]}, "
                         f"dt {s.dt * 1e3:.4f} ms, forward RTM step, snapshots every {shot.interval} steps",
             "grid": [s.nx, s.ny, s.nz], "cells": s.n, "snapshot_format": ["fp32", "c16", "fp16s"][snap_fmt],
-            "l2": "inputs larger than L2 (419 MB per volume), no flush", "dt_s": s.dt}
+            "l2": f"inputs larger than L2 ({s.n * 4 / 1e6:.0f} MB per volume), no flush", "dt_s": s.dt}
 
 
 def run_cuda(args, rank, world):
@@ -152,7 +160,7 @@ def run_cuda(args, rank, world):
     from konglong_b200.spec import FORWARD, SNAP_C16
 
     K, Wm = args.steps, args.warmup
-    shot = build_workload(args.workload, 2 * K + Wm + 8)
+    shot = build_workload(args.workload, 2 * K + Wm + 8, args.scale)
     s = shot.spec
     snap_fmt = SNAP_C16
     k1, k2 = W.spread_band(s)
@@ -213,6 +221,10 @@ def run_cuda(args, rank, world):
                      "frac": alg * cells / (ms_step * 1e-3) / 1e9 / peak},
             "kernels_ms_per_step": {k: round(v[0] / K, 4) for k, v in prof.items()}}
     roof["frac"] = roof["achieved"] / peak
+    bpc = MEASURED_DRAM_B_PER_CELL.get(args.workload, {}).get(dom)
+    if bpc is not None:
+        roof["traffic"] = bpc * cells
+        roof["traffic_source"] = "ncu DRAM bytes per cell at 0.75 scale x cells of one launch"
 
     # end to end through the public API with host buffers: modelling run of K
     # steps with the receiver samples read back (set_injection H2D of the
@@ -281,7 +293,7 @@ def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path (oracle/_ref, else the oracle
     port) timed on this host's cores on the same workload."""
     from oracle import pyoracle as O
-    shot = build_workload(args.workload, args.steps + args.warmup + 8)
+    shot = build_workload(args.workload, args.steps + args.warmup + 8, args.scale)
     s = shot.spec
     threads = os.cpu_count() or 1
     if O.ref_available() and not s.use_q:
@@ -318,6 +330,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="vti_cfd", choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="grid scale of the workload (1.0 = the configuration the metric is quoted on; "
+                         "smaller values are for profiler captures)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
