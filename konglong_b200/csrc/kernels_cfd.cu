@@ -13,6 +13,8 @@
 //            back substitution.
 // The PML / scaling / accumulation steps of FdEngine_cfd::d{x,y,z}1_2D and
 // KernelCPU::TTI run as pointwise epilogues afterwards.
+#include <type_traits>
+
 #include "kernel_api.h"
 #include "rtm_device.cuh"
 #include "tma.cuh"
@@ -565,131 +567,116 @@ __global__ void __launch_bounds__(128) cfd_lines_tma_k(CfdPlanDev p, const __gri
   }
 }
 
-// V consecutive floats at p (V = 4: one 16-byte access; p 16-byte aligned)
-template <int V>
-__device__ __forceinline__ void ldv(float (&v)[V], const float *p) {
-  if constexpr (V == 4) {
-    const float4 t = *reinterpret_cast<const float4 *>(p);
-    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
-  } else {
-#pragma unroll
-    for (int k = 0; k < V; k++) v[k] = p[k];
-  }
-}
-template <int V>
-__device__ __forceinline__ void stv(float *p, const float (&v)[V]) {
-  if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  else {
-#pragma unroll
-    for (int k = 0; k < V; k++) p[k] = v[k];
-  }
-}
+// Cell regions of the pointwise epilogues.  The PML cells form six disjoint
+// boxes (y bands over the whole xz plane, x bands inside the y interior, z
+// bands inside both); the rest is the interior box.  Each box is one launch
+// of a 3-D grid: interior cells run without PML code, PML cells gather every
+// PML memory value of the cell first (pml1_all).
+struct EpiBox {
+  int z0, z1, x0, x1, y0, y1;
+};
 
-// Pointwise epilogues: block (32, 8) threads, each thread V consecutive z
-// cells (V = 4 when nz % 4 == 0); grid (z tiles, x tiles, ny).  Every input
-// of a cell is loaded before the PML branch, so a cell costs one memory
-// round trip; PML cells then run the split-field recursion per cell.
-template <int V>
-__global__ void __launch_bounds__(256) cfd_grad_epi_k(CfdGradEpiArgs a) {
-  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const int iz0 = (blockIdx.x * 32 + threadIdx.x) * V, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
-  if (iz0 >= a.nz || ix >= a.nx) return;
+// PML round 1 + VTI / TTI scaling of the raw gradients of one cell, in place
+// (pml1 on each component, then KernelCPU::ScalarVTI / ScalarTTI).
+template <bool PML, int MASK>
+__device__ __forceinline__ void grad_cell(const CfdGradEpiArgs &a, const Grid3 &g, int ix, int iy, int iz) {
   const bool do_y = a.ny > 1;
-  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz0;
-  float gz[V], gx[V], gy[V], ep[V], dl[V], px[V], py[V];
-  ldv<V>(gz, a.gz + i);
-  ldv<V>(gx, a.gx + i);
-  if (do_y) ldv<V>(gy, a.gy + i);
-  else {
-#pragma unroll
-    for (int k = 0; k < V; k++) gy[k] = 0.f;
-  }
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
+  float gz = a.gz[i], gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f;
+  float ep = 0.f, dl = 0.f, ax = 0.f, ay = 0.f;
+  if (a.model >= 2) ep = __ldg(a.eps + i), dl = __ldg(a.del + i);
+  if (a.model == 3) ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
+  if (PML) pml1_all<0, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
   if (a.model >= 2) {
-    ldv<V>(ep, a.eps + i);
-    ldv<V>(dl, a.del + i);
-  }
-  if (a.model == 3) {
-    ldv<V>(px, a.pjx + i);
-    if (do_y) ldv<V>(py, a.pjy + i);
-    else {
-#pragma unroll
-      for (int k = 0; k < V; k++) py[k] = 0.f;
+    float e = ep;
+    const float d = e - dl;
+    e = 1.0f + 2.0f * e;
+    if (a.model == 3) {
+      const float az = sqrtf(1.0f - (ax * ax + ay * ay));
+      const float v2 = gx * gx + gy * gy + gz * gz;
+      const float vzz = gx * ax + gy * ay + gz * az;
+      const float vz2 = vzz * vzz, vh2 = v2 - vz2;
+      const float ecl = e * vh2 + vz2;
+      const float parts = sqrtf(1.0f - 8.0f * (d * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
+      const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
+      const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
+      gx = (bx + (gx - bx) * e) * sc;
+      gy = (by + (gy - by) * e) * sc;
+      gz = (bz + (gz - bz) * e) * sc;
+    } else {
+      const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
+      const float ecl = e * vx2 + vz2;
+      const float parts = sqrtf(1.0f - 8.0f * (d * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
+      const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
+      gx *= sc2;
+      gy *= sc2;
     }
   }
-#pragma unroll
-  for (int k = 0; k < V; k++) {
-    const int iz = iz0 + k;
-    if (in_pml(a.pml, g, ix, iy, iz)) {
-      pml1(a.pml, g, a.pml3d, DZ, 0, gz[k], ix, iy, iz);
-      pml1(a.pml, g, a.pml3d, DX, 0, gx[k], ix, iy, iz);
-      if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy[k], ix, iy, iz);
-    }
-    if (a.model >= 2) {
-      float e = ep[k];
-      const float d = e - dl[k];
-      e = 1.0f + 2.0f * e;
-      if (a.model == 3) {
-        const float ax = px[k], ay = py[k];
-        const float az = sqrtf(1.0f - (ax * ax + ay * ay));
-        const float v2 = gx[k] * gx[k] + gy[k] * gy[k] + gz[k] * gz[k];
-        const float vzz = gx[k] * ax + gy[k] * ay + gz[k] * az;
-        const float vz2 = vzz * vzz, vh2 = v2 - vz2;
-        const float ecl = e * vh2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (d * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-        const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
-        const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
-        gx[k] = (bx + (gx[k] - bx) * e) * sc;
-        gy[k] = (by + (gy[k] - by) * e) * sc;
-        gz[k] = (bz + (gz[k] - bz) * e) * sc;
-      } else {
-        const float vx2 = gx[k] * gx[k] + gy[k] * gy[k], vz2 = gz[k] * gz[k];
-        const float ecl = e * vx2 + vz2;
-        const float parts = sqrtf(1.0f - 8.0f * (d * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-        const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
-        gx[k] *= sc2;
-        gy[k] *= sc2;
-      }
-    }
-  }
-  stv<V>(a.gz + i, gz);
-  stv<V>(a.gx + i, gx);
-  if (do_y) stv<V>(a.gy + i, gy);
+  a.gz[i] = gz;
+  a.gx[i] = gx;
+  if (do_y) a.gy[i] = gy;
 }
 
-template <int V>
-__global__ void __launch_bounds__(256) cfd_div_epi_k(CfdDivEpiArgs a) {
-  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
-  const int iz0 = (blockIdx.x * 32 + threadIdx.x) * V, ix = blockIdx.y * 8 + threadIdx.y, iy = blockIdx.z;
-  if (iz0 >= a.nz || ix >= a.nx) return;
+// PML round 2 on the raw divergence parts of one cell, then
+// w0 = w0 - vel (dx + dz + dy) followed by the leapfrog / Q update of MODE
+// (KernelCPU::applyVel_minus + Propagator::update2nd).
+template <bool PML, int MASK, int MODE>
+__device__ __forceinline__ void div_cell(const CfdDivEpiArgs &a, const Grid3 &g, int ix, int iy, int iz) {
   const bool do_y = a.ny > 1 && a.dy;
-  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz0;
-  float dxv[V], dzv[V], dyv[V], vel[V], w0[V], w1[V];
-  ldv<V>(dxv, a.dx + i);
-  ldv<V>(dzv, a.dz + i);
-  if (do_y) ldv<V>(dyv, a.dy + i);
-  else {
-#pragma unroll
-    for (int k = 0; k < V; k++) dyv[k] = 0.f;
-  }
-  ldv<V>(vel, a.vel + i);
-  ldv<V>(w0, a.w0 + i);
-  if (a.mode != 0) ldv<V>(w1, a.w1 + i);
-#pragma unroll
-  for (int k = 0; k < V; k++) {
-    const int iz = iz0 + k;
-    if (in_pml(a.pml, g, ix, iy, iz)) {
-      pml1(a.pml, g, a.pml3d, DX, 1, dxv[k], ix, iy, iz);
-      pml1(a.pml, g, a.pml3d, DZ, 1, dzv[k], ix, iy, iz);
-      if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv[k], ix, iy, iz);
-    }
-    float t = w0[k] - dxv[k] * vel[k];
-    t = t - dzv[k] * vel[k];
-    t = t - dyv[k] * vel[k];
-    if (a.mode == 0) w0[k] = t;
-    else w0[k] = a.mode == 1 ? (w1[k] + w1[k]) - t : q_update(a.q, i + k, g.nxz * a.ny, t, w1[k]);
-  }
-  stv<V>(a.w0 + i, w0);
+  const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
+  float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
+  const float vel = __ldg(a.vel + i);
+  const float w0 = a.w0[i];
+  const float w1 = MODE != 0 ? __ldg(a.w1 + i) : 0.f;
+  if (PML) pml1_all<1, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
+  float t = w0 - dxv * vel;
+  t = t - dzv * vel;
+  t = t - dyv * vel;
+  float out;
+  if (MODE == 0) out = t;
+  else out = MODE == 1 ? (w1 + w1) - t : q_update(a.q, i, g.nxz * a.ny, t, w1);
+  a.w0[i] = out;
 }
+
+// one box: block (32 z, 8 x), grid (z tiles, x tiles, y count) from (z0, x0, y0);
+// MASK (bit 2*d + s) lists the PML faces that can hold the box's cells
+template <bool PML, int MASK>
+__global__ void __launch_bounds__(256) cfd_grad_box_k(CfdGradEpiArgs a, EpiBox b) {
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int iz = b.z0 + blockIdx.x * 32 + threadIdx.x, ix = b.x0 + blockIdx.y * 8 + threadIdx.y, iy = b.y0 + blockIdx.z;
+  if (iz < b.z1 && ix < b.x1) grad_cell<PML, MASK>(a, g, ix, iy, iz);
+}
+template <bool PML, int MASK, int MODE>
+__global__ void __launch_bounds__(256) cfd_div_box_k(CfdDivEpiArgs a, EpiBox b) {
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int iz = b.z0 + blockIdx.x * 32 + threadIdx.x, ix = b.x0 + blockIdx.y * 8 + threadIdx.y, iy = b.y0 + blockIdx.z;
+  if (iz < b.z1 && ix < b.x1) div_cell<PML, MASK, MODE>(a, g, ix, iy, iz);
+}
+
+// face masks of the PML boxes: y band (its y face, any x / z face), x band
+// (its x face, any z face), z band (its z face)
+constexpr int kZL = 1 << (2 * DZ), kZH = 2 << (2 * DZ), kXL = 1 << (2 * DX), kXH = 2 << (2 * DX),
+              kYL = 1 << (2 * DY), kYH = 2 << (2 * DY);
+constexpr int kBoxMask[7] = {0, kYL | kXL | kXH | kZL | kZH, kYH | kXL | kXH | kZL | kZH, kXL | kZL | kZH,
+                             kXH | kZL | kZH, kZL, kZH};
+
+// interior box [0] and the six PML boxes [1..6] (kBoxMask order; empty boxes
+// have z1 <= z0)
+void epi_boxes(const PmlDev &P, int nx, int ny, int nz, EpiBox *out) {
+  const int zl = min(P.f[DZ][0].w, nz), zh = min(P.f[DZ][1].w, nz - zl);
+  const int xl = min(P.f[DX][0].w, nx), xh = min(P.f[DX][1].w, nx - xl);
+  const int yl = min(P.f[DY][0].w, ny), yh = min(P.f[DY][1].w, ny - yl);
+  out[0] = EpiBox{zl, nz - zh, xl, nx - xh, yl, ny - yh};
+  out[1] = EpiBox{0, nz, 0, nx, 0, yl};
+  out[2] = EpiBox{0, nz, 0, nx, ny - yh, ny};
+  out[3] = EpiBox{0, nz, 0, xl, yl, ny - yh};
+  out[4] = EpiBox{0, nz, nx - xh, nx, yl, ny - yh};
+  out[5] = EpiBox{0, zl, xl, nx - xh, yl, ny - yh};
+  out[6] = EpiBox{nz - zh, nz, xl, nx - xh, yl, ny - yh};
+}
+
+dim3 box_grid(const EpiBox &b) { return dim3((b.z1 - b.z0 + 31) / 32, (b.x1 - b.x0 + 7) / 8, b.y1 - b.y0); }
+bool box_empty(const EpiBox &b) { return b.z1 <= b.z0 || b.x1 <= b.x0 || b.y1 <= b.y0; }
 
 }  // namespace
 
@@ -742,12 +729,49 @@ int cfd_init() {
   return ok ? 0 : -1;
 }
 
+template <int K, typename F>
+static void each_box(const EpiBox *bx, F &&f) {
+  if constexpr (K < 7) {
+    if (!box_empty(bx[K])) f(std::integral_constant<int, K>{});
+    each_box<K + 1>(bx, f);
+  }
+}
+
+// lo and hi layers of one dimension overlap (small grids): a cell of a band
+// box can then also lie in the opposite face, so every box takes all faces
+static bool pml_overlap(const PmlDev &P, int nx, int ny, int nz) {
+  return P.f[DZ][0].w + P.f[DZ][1].w > nz || P.f[DX][0].w + P.f[DX][1].w > nx || P.f[DY][0].w + P.f[DY][1].w > ny;
+}
+
 void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st) {
-  cfd_grad_epi_k<1><<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
+  EpiBox bx[7];
+  epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  const bool all = pml_overlap(a.pml, a.nx, a.ny, a.nz);
+  each_box<0>(bx, [&](auto k) {
+    constexpr int K = decltype(k)::value;
+    const dim3 g = box_grid(bx[K]), block(32, 8);
+    if (K > 0 && all) cfd_grad_box_k<true, 63><<<g, block, 0, st>>>(a, bx[K]);
+    else cfd_grad_box_k<(K > 0), kBoxMask[K]><<<g, block, 0, st>>>(a, bx[K]);
+  });
+}
+
+template <int K, int MODE>
+static void div_box(const CfdDivEpiArgs &a, const EpiBox &b, bool all, cudaStream_t st) {
+  const dim3 g = box_grid(b), block(32, 8);
+  if (K > 0 && all) cfd_div_box_k<true, 63, MODE><<<g, block, 0, st>>>(a, b);
+  else cfd_div_box_k<(K > 0), kBoxMask[K], MODE><<<g, block, 0, st>>>(a, b);
 }
 
 void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
-  cfd_div_epi_k<1><<<dim3((a.nz + 31) / 32, (a.nx + 7) / 8, a.ny), dim3(32, 8), 0, st>>>(a);
+  EpiBox bx[7];
+  epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  const bool all = pml_overlap(a.pml, a.nx, a.ny, a.nz);
+  each_box<0>(bx, [&](auto k) {
+    constexpr int K = decltype(k)::value;
+    if (a.mode == 0) div_box<K, 0>(a, bx[K], all, st);
+    else if (a.mode == 1) div_box<K, 1>(a, bx[K], all, st);
+    else div_box<K, 2>(a, bx[K], all, st);
+  });
 }
 
 }  // namespace rtm

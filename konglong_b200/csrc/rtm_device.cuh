@@ -113,6 +113,127 @@ __device__ __forceinline__ void pml1(const PmlDev &P, const Grid3 &g, int pml3d,
   }
 }
 
+// Where a cell sits in the split-field PML faces: for each dimension d and
+// side s (lo, hi) the layer L (-1 outside the face) and the cell's index in
+// the face arrays.  Same indexing as pml_at.
+struct PmlCell {
+  int layer[3][2];
+  long long idx[3][2];
+};
+
+// MASK: faces to consider, bit 2*d + s (the others are known not to hold the cell)
+template <int MASK = 63>
+__device__ __forceinline__ void pml_locate(const PmlDev &P, const Grid3 &g, int ix, int iy, int iz, PmlCell &c) {
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int w = (MASK >> (2 * d + s)) & 1 ? P.f[d][s].w : 0;
+      int L = -1;
+      long long idx = 0;
+      if (d == DZ) {
+        if (s == SIDE_LO && iz < w) L = iz, idx = ((long long)iy * g.nx + ix) * w + iz;
+        if (s == SIDE_HI && w && iz >= g.nz - w)
+          L = g.nz - 1 - iz, idx = ((long long)iy * g.nx + ix) * w + (iz - (g.nz - w));
+      } else if (d == DX) {
+        if (s == SIDE_LO && ix < w) L = ix, idx = ((long long)iy * w + ix) * g.nz + iz;
+        if (s == SIDE_HI && w && ix >= g.nx - w)
+          L = g.nx - 1 - ix, idx = ((long long)iy * w + ix - (g.nx - w)) * g.nz + iz;
+      } else {
+        if (s == SIDE_LO && iy < w) L = iy, idx = ((long long)iy * g.nx + ix) * g.nz + iz;
+        if (s == SIDE_HI && w && iy >= g.ny - w)
+          L = g.ny - 1 - iy, idx = ((long long)(iy - (g.ny - w)) * g.nx + ix) * g.nz + iz;
+      }
+      c.layer[d][s] = L, c.idx[d][s] = idx;
+    }
+}
+
+// Round R of the first-derivative PML on all three components of one cell
+// (pml1 for axes z, x, y in turn: own dimension unscaled, then the two cross
+// dimensions scaled when pml3d; each dimension lo face before hi face;
+// bgprtm/FdEngine.cpp:301-350).  The work is grouped by face (d, s) behind
+// one branch each, so a cell pays only for the faces that hold it; every
+// memory value is loaded before the first recursion (one memory round trip),
+// and the recursion order is that of pml1.
+template <int R, int MASK = 63>
+__device__ __forceinline__ void pml1_all(const PmlDev &P, const Grid3 &g, int pml3d, bool do_y, int ix, int iy, int iz,
+                                         float &pz, float &px, float &py) {
+  PmlCell c;
+  pml_locate<MASK>(P, g, ix, iy, iz, c);
+  // cross terms only when pml3d (for the y component only when ny > 1)
+  const bool cross = pml3d != 0, ycross = pml3d != 0 && g.ny > 1;
+  // q values per face and component (k: 0 z, 1 x, 2 y)
+  float qz[3][2], qx[3][2], qy[3][2];
+  // memory component index of component k in face dim d
+  auto cz = [](int d) { return d == DZ ? 0 : 1; };           // z component: own DZ(0), cross DX(1), DY(1)
+  auto cx = [](int d) { return d == DX ? 0 : d == DZ ? 1 : 2; };  // x component: own DX(0), DZ(1), DY(2)
+  auto cy = [](int d) { return d == DY ? 0 : 2; };           // y component: own DY(0), DZ(2), DX(2)
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[d][s] >= 0) {
+        const long long i = c.idx[d][s];
+        if (d == DZ || cross) qz[d][s] = P.f[d][s].q[R][cz(d)][i];
+        if (d == DX || cross) qx[d][s] = P.f[d][s].q[R][cx(d)][i];
+        if (do_y && (d == DY || ycross)) qy[d][s] = P.f[d][s].q[R][cy(d)][i];
+      }
+  auto round = [&](float &p, float &q, int d, int s, int scaled) {
+    const float *co = P.f[d][s].co + c.layer[d][s] * 6 + 3 * scaled;
+    const float qn = co[0] * q - co[1] * p;
+    q = qn;
+    p = qn + co[2] * p;
+  };
+  // component z: DZ, then DX, DY scaled
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+    if (c.layer[DZ][s] >= 0) round(pz, qz[DZ][s], DZ, s, 0);
+  if (cross) {
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[DX][s] >= 0) round(pz, qz[DX][s], DX, s, 1);
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[DY][s] >= 0) round(pz, qz[DY][s], DY, s, 1);
+  }
+  // component x: DX, then DZ, DY scaled
+#pragma unroll
+  for (int s = 0; s < 2; s++)
+    if (c.layer[DX][s] >= 0) round(px, qx[DX][s], DX, s, 0);
+  if (cross) {
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[DZ][s] >= 0) round(px, qx[DZ][s], DZ, s, 1);
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[DY][s] >= 0) round(px, qx[DY][s], DY, s, 1);
+  }
+  // component y: DY, then DZ, DX scaled
+  if (do_y) {
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[DY][s] >= 0) round(py, qy[DY][s], DY, s, 0);
+    if (ycross) {
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (c.layer[DZ][s] >= 0) round(py, qy[DZ][s], DZ, s, 1);
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (c.layer[DX][s] >= 0) round(py, qy[DX][s], DX, s, 1);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (c.layer[d][s] >= 0) {
+        const long long i = c.idx[d][s];
+        if (d == DZ || cross) P.f[d][s].q[R][cz(d)][i] = qz[d][s];
+        if (d == DX || cross) P.f[d][s].q[R][cx(d)][i] = qx[d][s];
+        if (do_y && (d == DY || ycross)) P.f[d][s].q[R][cy(d)][i] = qy[d][s];
+      }
+}
+
 // --- COMPRESS_16 code (bgprtm/WaveFieldCompress.cpp:107-133) ----------------
 __device__ __forceinline__ uint16_t c16_encode(float v) {
   const int idat = __float_as_int(v);
