@@ -26,6 +26,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from konglong_b200 import replicas as R  # noqa: E402
+
 # algorithmic HBM bytes per cell-step (each array read / written once per step)
 #   VTI core: R w1, w0, vel, eps, del; W w0 = 24 B; PML memory 48 B x fraction
 #   of cells in PML slabs (3 first derivatives x 2 rounds x q r/w).
@@ -175,24 +177,16 @@ def run_cuda(args, rank, world):
     p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
     tuned = p.autotune(3)
     p.reset()
-    dist = world > 1
-    if dist:
-        import torch.distributed as tdist
+    ranks = R.Ranks.from_env()
     # warm-up steps (untimed), then K timed steps continuing the same shot
     p.migration(FORWARD, 0, Wm, -1, shot.interval)
-    if dist:
-        tdist.barrier()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+    R.barrier(ranks)
+    with ClockSampler(ranks.local_rank) as clk:
         p.migration(FORWARD, Wm, Wm + K, -1, shot.interval)
-    ms = p.last_loop_ms
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
-        tdist.barrier()
+    ms = R.max_over_ranks(ranks, p.last_loop_ms, device="cuda")
+    R.barrier(ranks)
     cells = s.n
-    value = world * cells * K / (ms * 1e-3) / 1e9
+    value = R.aggregate_gpts(world, cells, K, ms)
     ms_step = ms / K
 
     launches = p.launch_count()
@@ -241,20 +235,14 @@ def run_cuda(args, rank, world):
         q.modelling(2, -1, 1)  # warm the graph path
         q.reset()
         wav = np.ascontiguousarray(shot.wavelet[None, :K + 1])
-        if dist:
-            tdist.barrier()
+        R.barrier(ranks)
         t0 = time.perf_counter()
         q.set_injection(src, wav, s.dt_dxyz)
         q.modelling(K, -1, 1)
         tr = q.traces()
         t1 = time.perf_counter()
-        wall = t1 - t0
-        if dist:
-            import torch
-            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            wall = float(t.item())
-        e2e = {"value": world * cells * K / wall / 1e9, "unit": "Gpts/s",
+        wall = R.max_over_ranks(ranks, t1 - t0, device="cuda")
+        e2e = {"value": R.aggregate_gpts(world, cells, K, wall * 1e3), "unit": "Gpts/s",
                "h2d_bytes_per_step": int(wav.nbytes // K), "d2h_bytes_per_step": int(tr.nbytes // K),
                "what": "Propagator.modelling via the C ABI: traces H2D, K steps with receiver extraction, "
                        "receiver samples D2H; wall clock"}
@@ -338,10 +326,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    ranks = R.Ranks.from_env()
+    world, rank = ranks.world, ranks.rank
     if args.impl == "reference":
-        if rank != 0:
+        if not R.runs_reference_arm(ranks):
             return
         r = run_reference(args, rank, world)
         shot = r["shot"]
@@ -357,9 +345,8 @@ def main():
         return
     if world > 1:
         import torch
-        import torch.distributed as tdist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        torch.cuda.set_device(ranks.local_rank)
+        R.init(ranks, "nccl", timeout_s=300)
     else:
         try:
             import torch
@@ -378,10 +365,7 @@ def main():
                 "cpu_baseline": cpu, "e2e": r["e2e"], "clocks": r["clocks"],
                 "gpu_launches": r["launches"]}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as tdist
-        tdist.barrier()
-        tdist.destroy_process_group()
+    R.finish(ranks)
 
 
 if __name__ == "__main__":

@@ -226,6 +226,18 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
+/* Failure detection.  rtm_check_finite scans field RTM_FIELD_W0 / W1 / IMAGE on
+ * the device and sets *nonfinite to 1 when it holds a NaN or an infinity (an
+ * unstable model or dt), else 0.  RTM_ERR_ARG for a field the handle does not
+ * hold (the image before rtm_image_setup).  No reference counterpart: bgprtm
+ * never checks its wavefields. */
+int rtm_check_finite(rtm_handle *h, int field, int *nonfinite);
+/* Self-test of the engine's bounded device waits: launches one kernel whose
+ * mbarrier wait can never complete; the wait gives up after its poll limit,
+ * raises the device flag, and the call returns RTM_ERR_TIMEOUT with the
+ * context still usable.  Any other return value is a failure.  No reference
+ * counterpart. */
+int rtm_selftest_bounded_wait(rtm_handle *h);
 /* Autotuner: times `steps` fused steps of every launch shape this handle's
  * kernels offer (TMA tile width / prefetch depth for ISO FD8, tile width of
  * the FD8 gradient / divergence passes, register-streamed or TMA-tiled x / y

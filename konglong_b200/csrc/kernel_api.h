@@ -46,6 +46,8 @@ void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
 
 // ---- TMA plane pipelines (kernels_tma.cu), nz % 4 == 0 ------------------------
 bool tma_supported(int nz);
+// one kernel whose bounded mbarrier wait can never complete (raises *err)
+void launch_selftest_wait(int *err, cudaStream_t st);
 // fp32 volume [ny][nx][nz], box (bz, bx, 1)
 bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx, int by = 1);
 struct TmaShape {

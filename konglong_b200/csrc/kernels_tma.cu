@@ -179,6 +179,21 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// A wait that nothing completes: one thread initialises an mbarrier for one
+// arrival that never comes and waits on it; the bounded wait gives up and
+// raises *err.  Issues no copy, so returning early leaves nothing in flight.
+__global__ void selftest_wait_k(int *err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) (void)mbar_wait(&bar, 0, err);
+}
+
+void launch_selftest_wait(int *err, cudaStream_t st) { selftest_wait_k<<<1, 32, 0, st>>>(err); }
+
 bool tma_supported(int nz) { return nz % 4 == 0 && encode_fn() != nullptr; }
 
 // fp32 volume [ny][nx][nz] with a box of (bz, bx, 1) cells

@@ -81,6 +81,7 @@ struct Engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int *dflag = nullptr;
+  int *nfflag = nullptr;  // result of the non-finite scan (allocated on first use)
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
@@ -1138,6 +1139,31 @@ int rtm_get(rtm_handle *h, int field, float *dst) {
   CK(cudaMemcpyAsync(dst, src, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
+}
+
+int rtm_check_finite(rtm_handle *h, int field, int *nonfinite) {
+  if (!h || !nonfinite) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  const float *src = field == RTM_FIELD_W0 ? h->w0 : field == RTM_FIELD_W1 ? h->w1 : field == RTM_FIELD_IMAGE ? h->image : nullptr;
+  if (!src) return RTM_ERR_ARG;
+  if (!h->nfflag) TRY(h->alloc(h->nfflag, 1));
+  int f = 0;
+  CK(cudaMemsetAsync(h->nfflag, 0, sizeof(int), h->st));
+  rtm::launch_nonfinite_scan(src, h->n, h->nfflag, h->st);
+  TRY(rtm::check_launch(h, "nonfinite_scan"));
+  CK(cudaMemcpyAsync(&f, h->nfflag, sizeof f, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  *nonfinite = f != 0;
+  return RTM_OK;
+}
+
+int rtm_selftest_bounded_wait(rtm_handle *h) {
+  if (!h) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  rtm::launch_selftest_wait(h->dflag, h->st);
+  TRY(rtm::check_launch(h, "selftest_wait"));
+  CK(cudaStreamSynchronize(h->st));
+  return rtm::check_flag(h);
 }
 
 int rtm_put(rtm_handle *h, int field, const float *src) {

@@ -153,6 +153,17 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def check_finite(self, field):
+        """True when `field` (W0 / W1 / IMAGE) holds only finite values."""
+        nf = C.c_int(0)
+        self._ck(self.L.rtm_check_finite(self.h, field, C.byref(nf)), "rtm_check_finite")
+        return nf.value == 0
+
+    def selftest_bounded_wait(self):
+        """Status code of the bounded-wait self-test (RTM_ERR_TIMEOUT when the
+        engine's device waits give up as designed)."""
+        return self.L.rtm_selftest_bounded_wait(self.h)
+
     def launch_count(self):
         v = C.c_longlong()
         self._ck(self.L.rtm_last_loop_launches(self.h, C.byref(v)), "rtm_last_loop_launches")
