@@ -226,6 +226,28 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
+/* ---- Batched small shots (many shots, one persistent launch per step) ----
+ * A batch steps several ISO FD8 handles (no Q) of different grids and step
+ * counts together: each time step is one persistent kernel over the column
+ * tiles of every active shot, one batched injection and one batched
+ * extraction launch, and the time loop runs as CUDA graphs.  Each handle must
+ * have its model, injection (and, optionally, extraction) set and be reset.
+ * No reference counterpart: bgprtm runs one shot per process
+ * (bgprtm/Propagator.cpp:1054-1260 per shot). */
+typedef struct rtm_batch rtm_batch;
+int rtm_batch_create(rtm_handle *const *shots, int nshots, rtm_batch **out);
+int rtm_batch_destroy(rtm_batch *b);
+/* rtm_modelling(shots[s], nts[s], it_shift, ntratio) for every shot at once:
+ * same wavefields and traces (receiver sums may differ in the last bit from a
+ * handle's grouped extraction). */
+int rtm_batch_modelling(rtm_batch *b, const int *nts, int it_shift, int ntratio);
+/* Device time of the last rtm_batch_modelling (ms). */
+int rtm_batch_last_ms(rtm_batch *b, float *ms);
+/* Times `steps` batched steps for each tile width / y-segment length the
+ * batched kernel offers, keeps the fastest and returns its index; zeroes the
+ * shots' wavefields, PML memory and traces (as rtm_reset). */
+int rtm_batch_autotune(rtm_batch *b, int steps, int *choice);
+
 /* Failure detection.  rtm_check_finite scans field RTM_FIELD_W0 / W1 / IMAGE on
  * the device and sets *nonfinite to 1 when it holds a NaN or an infinity (an
  * unstable model or dt), else 0.  RTM_ERR_ARG for a field the handle does not

@@ -29,7 +29,9 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_snapshot_load", "rtm_image_setup", "rtm_image_accumulate", "rtm_modelling",
            "rtm_migration", "rtm_get", "rtm_put", "rtm_c16_compress", "rtm_c16_uncompress",
            "rtm_last_loop_ms", "rtm_last_loop_launches", "rtm_profile", "rtm_profile_read",
-           "rtm_c16_compress_noalloc", "rtm_autotune", "rtm_check_finite", "rtm_selftest_bounded_wait"]
+           "rtm_c16_compress_noalloc", "rtm_autotune", "rtm_check_finite", "rtm_selftest_bounded_wait",
+           "rtm_batch_create", "rtm_batch_destroy", "rtm_batch_modelling", "rtm_batch_last_ms",
+           "rtm_batch_autotune"]
 
 KERNEL_KINDS = ["iso_fd8_step", "grad_fd8", "div_fd8", "cfd_z", "cfd_x", "cfd_y", "cfd_grad_epilogue",
                 "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io"]
@@ -100,6 +102,11 @@ def lib():
     L.rtm_autotune.argtypes = [vp, i, C.POINTER(i)]
     L.rtm_check_finite.argtypes = [vp, i, C.POINTER(i)]
     L.rtm_selftest_bounded_wait.argtypes = [vp]
+    L.rtm_batch_create.argtypes = [C.POINTER(vp), i, C.POINTER(vp)]
+    L.rtm_batch_destroy.argtypes = [vp]
+    L.rtm_batch_modelling.argtypes = [vp, _i32p, i, i]
+    L.rtm_batch_last_ms.argtypes = [vp, C.POINTER(f)]
+    L.rtm_batch_autotune.argtypes = [vp, i, C.POINTER(i)]
     L.rtm_last_loop_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.rtm_profile.argtypes = [vp, i]
     L.rtm_profile_read.argtypes = [vp, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),

@@ -18,6 +18,16 @@ struct IsoArgs {
   QDev q;
 };
 
+// one shot of a batched ISO step (device array): its step arguments, its two
+// wavefield buffers (w1 = wa on even steps) and its tile grid
+struct IsoBatchShot {
+  IsoArgs a;
+  float *wa, *wb;
+  int tiles_z, tiles_x, tiles_y;
+  TraceDev inj, ext;  // source traces (scatter) and receivers (gathered into ext_out)
+  float *ext_out;     // [ext.ntr][ext.nt]
+};
+
 struct GradArgs {
   int nx, ny, nz, yseg, pml3d;
   const float *w1;
@@ -41,6 +51,17 @@ struct DivArgs {
 
 // mode: 0 = operator only (w0 -= vel*L), 1 = + leapfrog update, 2 = + Q update
 void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
+// one step of every active shot of a batch (ISO, leapfrog): shots[0..nactive)
+// device array, start[] their first work items (start[nactive] = total)
+void launch_iso_fd8_batch(const IsoBatchShot *shots, const int *start, int nactive, int total, int it, int pml3d,
+                          int tx, int ctas, cudaStream_t st);
+// the CTAs per SM the batched ISO kernel keeps resident at tile width tx
+int iso_batch_ctas_per_sm(int tx, int pml3d);
+// batched source injection at trace sample it_src and receiver extraction at
+// sample jt, into the step-`it` output buffers of shots[0..nactive)
+void launch_batch_inject(const IsoBatchShot *shots, int nactive, int max_ntr, int max_ly, int it_src, int it,
+                         cudaStream_t st);
+void launch_batch_extract(const IsoBatchShot *shots, int nactive, int max_ntr, int jt, int it, cudaStream_t st);
 void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st);
 void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
 

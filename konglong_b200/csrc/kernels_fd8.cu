@@ -16,6 +16,8 @@
 //                 (bgprtm/KernelCPU.cpp:176-297).
 //  div_fd8        second pass: divergence with PML round 2, accumulated into
 //                 w0, fused with update2nd.
+#include <algorithm>
+
 #include "kernel_api.h"
 #include "rtm_device.cuh"
 
@@ -63,58 +65,69 @@ __device__ __forceinline__ void put_tile(float (*tile)[TZ + 2 * R], const Halo &
   if (tx < R) tile[tx][tz + R] = h.xl, tile[tx + TX + R][tz + R] = h.xh;
 }
 
+// One 32 (z) x TX (x) column tile of an ISO step, marching y over segment
+// bz (planes bz*yseg .. ), tile (bx, by); w1 / w0 are the wavefields of this
+// step (the batched kernel passes a shot's buffers of the current parity).
+// The coefficients and the PML widths are read once into registers.
 template <int TX, int MODE, bool PML3D>
-__global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
-  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
-  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+__device__ __forceinline__ void iso_tile(const IsoArgs &a, const float *__restrict__ w1, float *__restrict__ w0, int bx,
+                                         int by, int bz, float (*tile)[TZ + 2 * R]) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz, yseg = a.yseg;
+  const Grid3 g{nx, ny, nz, (long long)nx * nz};
+  float c2x[R + 1], c2y[R + 1], c2z[R + 1];
+#pragma unroll
+  for (int m = 0; m <= R; m++) c2x[m] = a.c2x[m], c2y[m] = a.c2y[m], c2z[m] = a.c2z[m];
+  const int zl = a.pml.f[DZ][0].w, zh = a.pml.f[DZ][1].w, xl = a.pml.f[DX][0].w, xh = a.pml.f[DX][1].w,
+            yl = a.pml.f[DY][0].w, yh = a.pml.f[DY][1].w;
+  const float *__restrict__ vel = a.vel;
   const int tz = threadIdx.x, tx = threadIdx.y;
-  const int iz = blockIdx.x * TZ + tz;
-  const int ix = blockIdx.y * TX + tx;
-  const int y0 = blockIdx.z * a.yseg;
-  const int y1 = min(a.ny, y0 + a.yseg);
-  const bool act = iz < a.nz && ix < a.nx;
-  const long long col = (long long)ix * a.nz + iz;
-  const float *__restrict__ w1 = a.w1;
-  const bool do_y = a.ny > 2;
+  const int iz = bx * TZ + tz;
+  const int ix = by * TX + tx;
+  const int y0 = bz * yseg;
+  const int y1 = min(ny, y0 + yseg);
+  const bool act = iz < nz && ix < nx;
+  const long long col = (long long)ix * nz + iz;
+  const bool do_y = ny > 2;
+  const bool xz_edge = iz < zl || iz >= nz - zh || ix < xl || ix >= nx - xh;
 
   float q[2 * R + 1];
 #pragma unroll
   for (int k = 0; k < 2 * R; k++) {
     const int y = y0 - R + k;
-    q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
+    q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < ny);
   }
-  Halo h0 = fetch_halo<TX>(w1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
-  Halo h1 = fetch_halo<TX>(w1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  Halo h0 = fetch_halo<TX>(w1, y0, ny, ix, iz, nx, nz, g.nxz, tx, tz);
+  Halo h1 = fetch_halo<TX>(w1, y0 + 1, ny, ix, iz, nx, nz, g.nxz, tx, tz);
   // per-cell inputs of the next plane
-  float nw0 = act ? a.w0[(long long)y0 * g.nxz + col] : 0.f;
-  float nvel = act ? __ldg(a.vel + (long long)y0 * g.nxz + col) : 0.f;
+  float nw0 = act ? w0[(long long)y0 * g.nxz + col] : 0.f;
+  float nvel = act ? __ldg(vel + (long long)y0 * g.nxz + col) : 0.f;
   for (int iy = y0; iy < y1; iy++) {
-    q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
+    q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < ny);
     const long long plane = (long long)iy * g.nxz;
     put_tile<TX>(tile, h0, q[R], tx, tz);
     h0 = h1;
-    h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+    h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : ny, ny, ix, iz, nx, nz, g.nxz, tx, tz);
     const float cw0 = nw0, cvel = nvel;
     if (act && iy + 1 < y1) {
-      nw0 = a.w0[plane + g.nxz + col];
-      nvel = __ldg(a.vel + plane + g.nxz + col);
+      nw0 = w0[plane + g.nxz + col];
+      nvel = __ldg(vel + plane + g.nxz + col);
     }
     __syncthreads();
     if (act) {
       const float u = q[R];
-      float lz = a.c2z[0] * u, lx = a.c2x[0] * u, ly = 0.0f;
+      float lz = c2z[0] * u, lx = c2x[0] * u, ly = 0.0f;
 #pragma unroll
       for (int m = 1; m <= R; m++) {
-        lz += a.c2z[m] * (tile[tx + R][tz + R - m] + tile[tx + R][tz + R + m]);
-        lx += a.c2x[m] * (tile[tx + R - m][tz + R] + tile[tx + R + m][tz + R]);
+        lz += c2z[m] * (tile[tx + R][tz + R - m] + tile[tx + R][tz + R + m]);
+        lx += c2x[m] * (tile[tx + R - m][tz + R] + tile[tx + R + m][tz + R]);
       }
       if (do_y) {
-        ly = a.c2y[0] * u;
+        ly = c2y[0] * u;
 #pragma unroll
-        for (int m = 1; m <= R; m++) ly += a.c2y[m] * (q[R - m] + q[R + m]);
+        for (int m = 1; m <= R; m++) ly += c2y[m] * (q[R - m] + q[R + m]);
       }
       float v;
-      const bool edge = in_pml(a.pml, g, ix, iy, iz);
+      const bool edge = xz_edge || iy < yl || iy >= ny - yh;
       if (PML3D) {
         v = lz + lx + ly;
         if (edge) {
@@ -136,12 +149,43 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
       float out;
       if (MODE == 0) out = t;                         // KernelCPU seam: w0 -= vel * L[w1]
       else if (MODE == 1) out = (u + u) - t;          // + update2nd (leapfrog)
-      else out = q_update(a.q, i, (long long)a.ny * g.nxz, t, u);  // + Q
-      a.w0[i] = out;
+      else out = q_update(a.q, i, (long long)ny * g.nxz, t, u);  // + Q
+      w0[i] = out;
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 2 * R; k++) q[k] = q[k + 1];
+  }
+}
+
+template <int TX, int MODE, bool PML3D>
+__global__ void __launch_bounds__(TZ *TX) iso_fd8_step(IsoArgs a) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  iso_tile<TX, MODE, PML3D>(a, a.w1, a.w0, blockIdx.x, blockIdx.y, blockIdx.z, tile);
+}
+
+// Many shots in one persistent launch: the work items are the column tiles of
+// the active shots (a prefix of the step-count-sorted batch), laid end to end
+// (start[s] = first item of shot s); each CTA strides over them.  Shot s
+// steps its buffers wa / wb in lockstep with the others: at step `it` w1 is wa
+// on even steps and wb on odd ones.  Leapfrog update (MODE 1), no snapshot I/O.
+template <int TX, bool PML3D>
+__global__ void __launch_bounds__(TZ *TX) iso_fd8_batch(const IsoBatchShot *__restrict__ shots,
+                                                         const int *__restrict__ start, int nactive, int total, int it) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int lo = 0, hi = nactive - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const IsoBatchShot &S = shots[lo];
+    const int l = w - __ldg(start + lo);
+    const int bx = l % S.tiles_z, by = (l / S.tiles_z) % S.tiles_x, bz = l / (S.tiles_z * S.tiles_x);
+    const float *w1 = (it & 1) ? S.wb : S.wa;
+    float *w0 = (it & 1) ? S.wa : S.wb;
+    iso_tile<TX, 1, PML3D>(S.a, w1, w0, bx, by, bz, tile);
   }
 }
 
@@ -360,6 +404,33 @@ void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t 
   if (tx == 4) iso_launch_tx<4>(a, mode, pml3d, st);
   else if (tx == 16) iso_launch_tx<16>(a, mode, pml3d, st);
   else iso_launch_tx<8>(a, mode, pml3d, st);
+}
+
+template <int TX>
+static void iso_batch_tx(const IsoBatchShot *shots, const int *start, int nactive, int total, int it, int pml3d,
+                         int ctas, cudaStream_t st) {
+  const unsigned grid = (unsigned)std::max(1, std::min(total, ctas));
+  if (pml3d) iso_fd8_batch<TX, true><<<grid, dim3(TZ, TX), 0, st>>>(shots, start, nactive, total, it);
+  else iso_fd8_batch<TX, false><<<grid, dim3(TZ, TX), 0, st>>>(shots, start, nactive, total, it);
+}
+
+void launch_iso_fd8_batch(const IsoBatchShot *shots, const int *start, int nactive, int total, int it, int pml3d,
+                          int tx, int ctas, cudaStream_t st) {
+  if (total <= 0 || nactive <= 0) return;
+  if (tx == 16) iso_batch_tx<16>(shots, start, nactive, total, it, pml3d, ctas, st);
+  else iso_batch_tx<8>(shots, start, nactive, total, it, pml3d, ctas, st);
+}
+
+int iso_batch_ctas_per_sm(int tx, int pml3d) {
+  int n = 0;
+  if (tx == 16) {
+    if (pml3d) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_batch<16, true>, TZ * 16, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_batch<16, false>, TZ * 16, 0);
+  } else {
+    if (pml3d) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_batch<8, true>, TZ * 8, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_batch<8, false>, TZ * 8, 0);
+  }
+  return std::max(1, n);
 }
 
 template <int TX>

@@ -253,6 +253,64 @@ void launch_inject_scatter(const TraceDev &t, int it, float *w0, const float *ve
   inject_scatter_k<<<dim3(cnt, t.ly), 256, 0, st>>>(t, it, w0, vel, nx, nz);
 }
 
+// Batched injection: block (trace, y row of its kernel, shot); the same
+// scatter as inject_scatter_k into the step output of each shot.
+__global__ void batch_inject_k(const IsoBatchShot *__restrict__ shots, int it_src, int it) {
+  const IsoBatchShot &S = shots[blockIdx.z];
+  const TraceDev &t = S.inj;
+  const int r = blockIdx.x;
+  if (r >= t.ntr || it_src < 0 || it_src >= t.nt) return;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], lz = l[2];
+  const int iy = blockIdx.y;
+  if (iy >= l[1]) return;
+  float *w0 = (it & 1) ? S.wa : S.wb;
+  const float *vel = S.a.vel;
+  const int nx = S.a.nx, nz = S.a.nz;
+  const float val = t.traces[(long long)r * t.nt + it_src] * t.scaler;
+  const int ntap = lx * lz;
+  for (int k = threadIdx.x; k < ntap; k += blockDim.x) {
+    const int iz = k % lz, ix = k / lz;
+    const float cy = val * t.ky[(long long)r * t.ly + iy];
+    const float cx = cy * t.kx[(long long)r * t.lx + ix];
+    const long long c = ((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz;
+    atomicAdd(w0 + c, cx * t.kz[(long long)r * t.lz + iz] * vel[c]);
+  }
+}
+
+// Batched extraction: a warp per receiver (extract_direct_k), blockIdx.y = shot.
+__global__ void batch_extract_k(const IsoBatchShot *__restrict__ shots, int jt, int it) {
+  const IsoBatchShot &S = shots[blockIdx.y];
+  const TraceDev &t = S.ext;
+  const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (r >= t.ntr || jt < 0 || jt >= t.nt) return;
+  const float *w0 = (it & 1) ? S.wa : S.wb;
+  const int nx = S.a.nx, nz = S.a.nz;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], ly = l[1], lz = l[2];
+  float acc = 0.f;
+  for (int k = lane; k < lx * ly * lz; k += 32) {
+    const int iz = k % lz, ix = (k / lz) % lx, iy = k / (lz * lx);
+    const float cx = t.ky[(long long)r * t.ly + iy] * t.kx[(long long)r * t.lx + ix];
+    acc += cx * t.kz[(long long)r * t.lz + iz] * w0[((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz];
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+  if (lane == 0) S.ext_out[(long long)r * t.nt + jt] = acc;
+}
+
+void launch_batch_inject(const IsoBatchShot *shots, int nactive, int max_ntr, int max_ly, int it_src, int it,
+                         cudaStream_t st) {
+  if (nactive <= 0 || max_ntr <= 0 || max_ly <= 0) return;
+  batch_inject_k<<<dim3(max_ntr, max_ly, nactive), 256, 0, st>>>(shots, it_src, it);
+}
+
+void launch_batch_extract(const IsoBatchShot *shots, int nactive, int max_ntr, int jt, int it, cudaStream_t st) {
+  if (nactive <= 0 || max_ntr <= 0) return;
+  batch_extract_k<<<dim3((max_ntr + 7) / 8, nactive), 256, 0, st>>>(shots, jt, it);
+}
+
 void launch_inject_group(const GroupDev &gr, const TraceDev &t, int it, float *plane, float *w0, const float *vel,
                          int nx, int ny, int nz, cudaStream_t st) {
   (void)plane;

@@ -699,6 +699,127 @@ using rtm::Engine;
 
 struct rtm_handle : Engine {};
 
+// ---- batched small shots ----------------------------------------------------
+struct rtm_batch {
+  std::vector<rtm::Engine *> shots;
+  int device = 0, pml3d = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  int tx = 8, yseg = 0;  // tile width, y segment (0: whole y extent)
+  rtm::IsoBatchShot *d_shots = nullptr;
+  int *d_start = nullptr;
+  int cap = 0;
+  std::string err;
+};
+
+namespace rtm {
+// tile-shape candidates of the batched ISO kernel: {tile width, y segment (0 = whole y)}
+static const int kBatchShapes[][2] = {{8, 0}, {8, 32}, {16, 0}, {16, 32}, {8, 16}};
+static const int kBatchNShapes = 5;
+
+// Device table of the shots in `order`, their first work items, and the
+// trace maxima of the batched I/O launches.
+static int batch_upload(rtm_batch *b, const std::vector<int> &order, std::vector<int> &start, int &max_inj,
+                        int &max_ly, int &max_ext) {
+  const int n = (int)order.size();
+  std::vector<IsoBatchShot> hs(n);
+  start.assign(n + 1, 0);
+  max_inj = max_ly = max_ext = 0;
+  for (int k = 0; k < n; k++) {
+    Engine *h = b->shots[order[k]];
+    const rtm_dims &d = h->d;
+    IsoBatchShot &S = hs[k];
+    IsoArgs &a = S.a;
+    a.nx = d.nx, a.ny = d.ny, a.nz = d.nz;
+    a.yseg = b->yseg > 0 ? std::min(b->yseg, d.ny) : d.ny;
+    a.w1 = h->w1, a.w0 = h->w0, a.vel = h->vel;
+    memcpy(a.c2x, h->c2x, sizeof a.c2x), memcpy(a.c2y, h->c2y, sizeof a.c2y), memcpy(a.c2z, h->c2z, sizeof a.c2z);
+    a.pml = pml_dev(h);
+    a.io = FusedIo{};
+    a.q = QDev{};
+    S.wa = h->w1, S.wb = h->w0;
+    S.tiles_z = (d.nz + 31) / 32, S.tiles_x = (d.nx + b->tx - 1) / b->tx, S.tiles_y = (d.ny + a.yseg - 1) / a.yseg;
+    S.inj = h->inj.dev(), S.ext = h->ext.dev(), S.ext_out = h->ext.out;
+    S.inj.ids = nullptr, S.ext.ids = nullptr;
+    start[k + 1] = start[k] + S.tiles_z * S.tiles_x * S.tiles_y;
+    max_inj = std::max(max_inj, h->inj.ntr), max_ly = std::max(max_ly, h->inj.ly);
+    max_ext = std::max(max_ext, h->ext.ntr);
+  }
+  if (n > b->cap) {
+    cudaFree(b->d_shots), cudaFree(b->d_start);
+    b->d_shots = nullptr, b->d_start = nullptr, b->cap = 0;
+    if (cudaMalloc(&b->d_shots, n * sizeof(IsoBatchShot)) != cudaSuccess ||
+        cudaMalloc(&b->d_start, (n + 1) * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      b->err = "batch table allocation failed";
+      return RTM_ERR_NOMEM;
+    }
+    b->cap = n;
+  }
+  if (cudaMemcpyAsync(b->d_shots, hs.data(), n * sizeof(IsoBatchShot), cudaMemcpyHostToDevice, b->st) ||
+      cudaMemcpyAsync(b->d_start, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, b->st)) {
+    b->err = "batch table upload failed";
+    return RTM_ERR_CUDA;
+  }
+  return RTM_OK;
+}
+
+// `count` steps of the shots in `order` (sorted by step count, descending:
+// the active shots of step it are the prefix with nts > it), as CUDA graphs
+// of up to 256 steps.  extract: ntratio > 0 gathers receivers every ntratio steps.
+static int batch_run(rtm_batch *b, const std::vector<int> &order, const std::vector<int> &nts_sorted, int count,
+                     int it_shift, int ntratio) {
+  std::vector<int> start;
+  int max_inj, max_ly, max_ext;
+  TRY(batch_upload(b, order, start, max_inj, max_ly, max_ext));
+  int num_sms = 0;
+  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, b->device);
+  const int grid = iso_batch_ctas_per_sm(b->tx, b->pml3d) * (num_sms > 0 ? num_sms : 148);
+  const int n = (int)order.size();
+  auto step = [&](int it) {
+    int na = 0;
+    while (na < n && nts_sorted[na] > it) na++;
+    launch_iso_fd8_batch(b->d_shots, b->d_start, na, start[na], it, b->pml3d, b->tx, grid, b->st);
+    launch_batch_inject(b->d_shots, na, max_inj, max_ly, it + it_shift, it, b->st);
+    if (ntratio > 0 && it % ntratio == 0) launch_batch_extract(b->d_shots, na, max_ext, it / ntratio, it, b->st);
+  };
+  if (cudaEventRecord(b->ev0, b->st)) return RTM_ERR_CUDA;
+  for (int s0 = 0; s0 < count; s0 += 256) {
+    const int s1 = std::min(count, s0 + 256);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal)) return RTM_ERR_CUDA;
+    for (int it = s0; it < s1; it++) step(it);
+    cudaError_t ec = cudaStreamEndCapture(b->st, &g);
+    if (ec != cudaSuccess) {
+      b->err = std::string("batch graph capture: ") + cudaGetErrorString(ec);
+      cudaGetLastError();
+      return RTM_ERR_CUDA;
+    }
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      b->err = std::string("batch graph instantiate: ") + cudaGetErrorString(ei);
+      cudaGetLastError();
+      return RTM_ERR_CUDA;
+    }
+    cudaError_t el = cudaGraphLaunch(ge, b->st);
+    cudaGraphExecDestroy(ge);
+    if (el != cudaSuccess) {
+      b->err = std::string("batch graph launch: ") + cudaGetErrorString(el);
+      return RTM_ERR_CUDA;
+    }
+  }
+  if (cudaEventRecord(b->ev1, b->st) || cudaEventSynchronize(b->ev1)) {
+    b->err = std::string("batch loop: ") + cudaGetErrorString(cudaGetLastError());
+    return RTM_ERR_CUDA;
+  }
+  cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+  return RTM_OK;
+}
+}  // namespace rtm
+
 extern "C" {
 
 void rtm_config_default(rtm_config *c) {
@@ -1215,6 +1336,96 @@ int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int
   cudaFree(din), cudaFree(dout), cudaFree(slab), cudaFree(ex), cudaFree(ey), cudaFree(ez);
   cudaGetLastError();
   return rc;
+}
+
+int rtm_batch_create(rtm_handle *const *shots, int nshots, rtm_batch **out) {
+  if (!shots || nshots < 1 || !out) return RTM_ERR_ARG;
+  *out = nullptr;
+  rtm_batch *b = new rtm_batch();
+  for (int k = 0; k < nshots; k++) {
+    rtm::Engine *h = shots[k];
+    if (!h || !h->model_set || h->c.engine != RTM_ENGINE_FD8 || h->c.model_type != RTM_ISO || h->c.use_q ||
+        h->device != shots[0]->device || h->c.pml3d != shots[0]->c.pml3d) {
+      delete b;
+      return !h || !h->model_set ? RTM_ERR_STATE : RTM_ERR_UNSUPPORTED;
+    }
+    b->shots.push_back(h);
+  }
+  b->device = shots[0]->device, b->pml3d = shots[0]->c.pml3d;
+  cudaSetDevice(b->device);
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) || cudaEventCreate(&b->ev0) ||
+      cudaEventCreate(&b->ev1)) {
+    cudaGetLastError();
+    rtm_batch_destroy(b);
+    return RTM_ERR_CUDA;
+  }
+  *out = b;
+  return RTM_OK;
+}
+
+int rtm_batch_destroy(rtm_batch *b) {
+  if (!b) return RTM_ERR_ARG;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  cudaFree(b->d_shots), cudaFree(b->d_start);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return RTM_OK;
+}
+
+int rtm_batch_modelling(rtm_batch *b, const int *nts, int it_shift, int ntratio) {
+  if (!b || !nts || ntratio < 1) return RTM_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int n = (int)b->shots.size();
+  for (int k = 0; k < n; k++)
+    if (nts[k] < 0) return RTM_ERR_ARG;
+  // every handle's own stream must be idle before the batch stream touches its buffers
+  for (rtm::Engine *h : b->shots) CK(cudaStreamSynchronize(h->st));
+  std::vector<int> order(n);
+  for (int k = 0; k < n; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nts[x] > nts[y]; });
+  std::vector<int> sorted(n);
+  for (int k = 0; k < n; k++) sorted[k] = nts[order[k]];
+  TRY(rtm::batch_run(b, order, sorted, sorted.empty() ? 0 : sorted[0], it_shift, ntratio));
+  // each shot swapped its wavefields once per step
+  for (int k = 0; k < n; k++)
+    if (nts[k] & 1) {
+      std::swap(b->shots[k]->w0, b->shots[k]->w1);
+      b->shots[k]->iq0 = 1 - b->shots[k]->iq0;
+    }
+  return RTM_OK;
+}
+
+int rtm_batch_last_ms(rtm_batch *b, float *ms) {
+  if (!b || !ms) return RTM_ERR_ARG;
+  *ms = b->last_ms;
+  return RTM_OK;
+}
+
+int rtm_batch_autotune(rtm_batch *b, int steps, int *choice) {
+  if (!b || steps < 1) return RTM_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int n = (int)b->shots.size();
+  for (rtm::Engine *h : b->shots) CK(cudaStreamSynchronize(h->st));
+  std::vector<int> order(n), sorted(n, steps);
+  for (int k = 0; k < n; k++) order[k] = k;
+  float best = 1e30f;
+  int bi = 0;
+  for (int c = 0; c < rtm::kBatchNShapes; c++) {
+    b->tx = rtm::kBatchShapes[c][0], b->yseg = rtm::kBatchShapes[c][1];
+    TRY(rtm::batch_run(b, order, sorted, 1, 0, 0));  // warm-up
+    TRY(rtm::batch_run(b, order, sorted, steps, 0, 0));
+    if (b->last_ms < best) best = b->last_ms, bi = c;
+  }
+  b->tx = rtm::kBatchShapes[bi][0], b->yseg = rtm::kBatchShapes[bi][1];
+  for (rtm::Engine *h : b->shots) {
+    TRY(rtm::zero_state(h));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  if (choice) *choice = bi;
+  return RTM_OK;
 }
 
 int rtm_autotune(rtm_handle *h, int steps, int *choice) {

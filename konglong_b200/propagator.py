@@ -209,6 +209,51 @@ class Propagator:
         return self.get(FIELD_IMAGE), fwd_ms, bwd_ms
 
 
+class Batch:
+    """Several ISO FD8 shots stepped together (rtm_batch_*): one persistent
+    kernel per time step over every active shot's tiles, batched injection and
+    extraction, the time loop as CUDA graphs.  The shots keep their own state:
+    after `modelling`, each Propagator holds what its own `modelling` call
+    would have produced."""
+
+    def __init__(self, shots):
+        self.L = _lib.lib()
+        self.shots = list(shots)
+        arr = (C.c_void_p * len(self.shots))(*[p.h for p in self.shots])
+        b = C.c_void_p()
+        _lib.check(self.L.rtm_batch_create(arr, len(self.shots), C.byref(b)), "rtm_batch_create")
+        self.b = b
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.rtm_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self, steps=5):
+        """Fastest tile shape of the batched kernel (zeroes the shots' state)."""
+        ch = C.c_int(0)
+        _lib.check(self.L.rtm_batch_autotune(self.b, steps, C.byref(ch)), "rtm_batch_autotune")
+        return ch.value
+
+    def modelling(self, nts, it_shift=-1, ntratio=1):
+        nts = np.ascontiguousarray(nts, np.int32)
+        if nts.size != len(self.shots):
+            raise ValueError("one step count per shot")
+        _lib.check(self.L.rtm_batch_modelling(self.b, nts, it_shift, ntratio), "rtm_batch_modelling")
+
+    @property
+    def last_ms(self):
+        v = C.c_float()
+        _lib.check(self.L.rtm_batch_last_ms(self.b, C.byref(v)), "rtm_batch_last_ms")
+        return v.value
+
+
 def spread_coeffs(n, x, k1, k2, nlimit, dipole=False, ntaper=0):
     """Util::CompactOrmsbySpreadCoeff + Receiver's edge taper through the C ABI;
     returns (first grid index, coefficients)."""
