@@ -64,7 +64,7 @@ typedef enum rtm_status {
 enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1 };      /* FD::FD, FD::CFD */
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
-enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2 };
+enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
 enum {
   RTM_FIELD_W0 = 0,  /* current/next wavefield (written by the step) */
   RTM_FIELD_W1 = 1,  /* previous wavefield (read by the stencil) */
@@ -170,7 +170,9 @@ int rtm_get_traces(rtm_handle *h, float *dst);
 
 /* Snapshot store for the source wavefield: nslots slots of format fmt
  * (RTM_SNAP_FP32 uncompressed, RTM_SNAP_C16 = the reference's COMPRESS_16
- * codec, bit-exact, RTM_SNAP_FP16S = FP16 with a per-y-slab scale). */
+ * codec, bit-exact, RTM_SNAP_FP16S = FP16 with a per-y-slab scale,
+ * RTM_SNAP_AE = the learned compressor attached by rtm_set_compressor:
+ * 32 latent floats + 1 scale per 8^3 block, 15.5:1). */
 int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots);
 /* Store w0 into slot (WaveFieldCompress::compress + CacheFile write). */
 int rtm_snapshot_store(rtm_handle *h, int slot);
@@ -226,6 +228,40 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
+/* ---- Learned snapshot compressor ------------------------------------------
+ * A 3-D convolutional autoencoder on 8^3-cell blocks (4 encoder + 4 decoder
+ * layers, 16 channels, 512 cells -> 32 latent floats + the block's max |w|),
+ * trained and run on the GPU with BF16 tensor-core GEMMs and FP32
+ * accumulation.  Replaces WaveFieldCompress (bgprtm/WaveFieldCompress.cpp
+ * compress/uncompress) for the forward-wavefield snapshots when attached to a
+ * handle; the FP32 / COMPRESS_16 stores stay available as the fallback.
+ * Blocks on the host are [n][512] floats, each scale-normalised (max |v| = 1)
+ * and in Morton order within the block (bit triples z y x from the least
+ * significant bit).  Parameters: rtm_ae_nparams() floats, layer by layer
+ * W [K][N] then bias [N]. */
+typedef struct rtm_ae rtm_ae;
+int rtm_ae_nparams(void);
+int rtm_ae_create(rtm_ae **out);
+int rtm_ae_destroy(rtm_ae *a);
+int rtm_ae_set_params(rtm_ae *a, const float *params);
+int rtm_ae_get_params(rtm_ae *a, float *params);
+/* MSE loss of the reconstruction of n host blocks and its gradient
+ * (grads may be NULL); no update. */
+int rtm_ae_loss_grad(rtm_ae *a, const float *blocks, int n, float *loss, float *grads);
+/* One Adam step (learning rate lr) on a batch of n host blocks; returns the
+ * batch loss before the step. */
+int rtm_ae_train_step(rtm_ae *a, const float *blocks, int n, float lr, float *loss);
+/* Reconstruction [n][512] (and latents [n][32] when latent != NULL). */
+int rtm_ae_reconstruct(rtm_ae *a, const float *blocks, int n, float *out, float *latent);
+/* Device volume (z fastest) <-> latents [nb][32] + scales [nb], nb = the 8^3
+ * blocks covering the volume (zero-padded); on `stream` (NULL = default). */
+int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, float *d_latent, float *d_scales,
+                           void *stream);
+int rtm_ae_decompress_volume(rtm_ae *a, const float *d_latent, const float *d_scales, int nx, int ny, int nz,
+                             float *d_vol, void *stream);
+/* Attach a compressor to a handle (same device) for RTM_SNAP_AE snapshots. */
+int rtm_set_compressor(rtm_handle *h, rtm_ae *a);
+
 /* ---- Batched small shots (many shots, one persistent launch per step) ----
  * A batch steps several ISO FD8 handles (no Q) of different grids and step
  * counts together: each time step is one persistent kernel over the column

@@ -31,7 +31,9 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_last_loop_ms", "rtm_last_loop_launches", "rtm_profile", "rtm_profile_read",
            "rtm_c16_compress_noalloc", "rtm_autotune", "rtm_check_finite", "rtm_selftest_bounded_wait",
            "rtm_batch_create", "rtm_batch_destroy", "rtm_batch_modelling", "rtm_batch_last_ms",
-           "rtm_batch_autotune"]
+           "rtm_batch_autotune", "rtm_ae_nparams", "rtm_ae_create", "rtm_ae_destroy", "rtm_ae_set_params",
+           "rtm_ae_get_params", "rtm_ae_loss_grad", "rtm_ae_train_step", "rtm_ae_reconstruct",
+           "rtm_ae_compress_volume", "rtm_ae_decompress_volume", "rtm_set_compressor"]
 
 KERNEL_KINDS = ["iso_fd8_step", "grad_fd8", "div_fd8", "cfd_z", "cfd_x", "cfd_y", "cfd_grad_epilogue",
                 "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io"]
@@ -107,6 +109,17 @@ def lib():
     L.rtm_batch_modelling.argtypes = [vp, _i32p, i, i]
     L.rtm_batch_last_ms.argtypes = [vp, C.POINTER(f)]
     L.rtm_batch_autotune.argtypes = [vp, i, C.POINTER(i)]
+    L.rtm_ae_nparams.argtypes = []
+    L.rtm_ae_create.argtypes = [C.POINTER(vp)]
+    L.rtm_ae_destroy.argtypes = [vp]
+    L.rtm_ae_set_params.argtypes = [vp, _f32p]
+    L.rtm_ae_get_params.argtypes = [vp, _f32p]
+    L.rtm_ae_loss_grad.argtypes = [vp, _f32p, i, C.POINTER(f), _f32p]
+    L.rtm_ae_train_step.argtypes = [vp, _f32p, i, f, C.POINTER(f)]
+    L.rtm_ae_reconstruct.argtypes = [vp, _f32p, i, _f32p, _f32p]
+    L.rtm_ae_compress_volume.argtypes = [vp, vp, i, i, i, vp, vp, vp]
+    L.rtm_ae_decompress_volume.argtypes = [vp, vp, vp, i, i, i, vp, vp]
+    L.rtm_set_compressor.argtypes = [vp, vp]
     L.rtm_last_loop_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.rtm_profile.argtypes = [vp, i]
     L.rtm_profile_read.argtypes = [vp, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),

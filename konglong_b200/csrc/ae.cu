@@ -1,0 +1,457 @@
+// ae.cu - learned snapshot compressor: a small 3-D convolutional autoencoder
+// on 8^3-cell blocks, trained and run with hand-written tensor-core kernels.
+//
+// A block's cells are kept in Morton order (bit triples z y x from the least
+// significant end), so the 8 children of every 2^3 cube are consecutive.
+// With that layout every layer is one row-major GEMM on the previous layer's
+// output memory, no reshaping:
+//   E1  2^3 patch conv, stride 2   1 -> 16 ch   rows/block 64  K   8 N  16  leaky ReLU
+//   E2  2^3 patch conv, stride 2  16 -> 16 ch              8   K 128 N  16  leaky ReLU
+//   E3  pointwise                 16 -> 16 ch              8   K  16 N  16  leaky ReLU
+//   E4  2^3 patch conv, stride 2  16 -> 32 ch (latent)     1   K 128 N  32  linear
+//   D1  transposed 2^3, stride 2  32 -> 16 ch              1   K  32 N 128  leaky ReLU
+//   D2  pointwise                 16 -> 16 ch              8   K  16 N  16  leaky ReLU
+//   D3  transposed 2^3, stride 2  16 -> 16 ch              8   K  16 N 128  leaky ReLU
+//   D4  transposed 2^3, stride 2  16 ->  1 ch              64  K  16 N   8  linear
+// 512 cells -> 32 latent floats (16:1) plus the block's max |value| scale.
+// GEMMs: mma.sync m16n8k16, BF16 operands (rounded from the FP32 activations
+// and FP32 master weights), FP32 accumulation.  Training: MSE loss on the
+// scale-normalised block, backward GEMMs, Adam on the FP32 master weights.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernel_api.h"
+#include "rtm_b200.h"
+
+namespace rtm {
+namespace {
+
+constexpr int kLayers = 8;
+constexpr int kL_K[kLayers] = {8, 128, 16, 128, 32, 16, 16, 16};
+constexpr int kL_N[kLayers] = {16, 16, 16, 32, 128, 16, 128, 8};
+constexpr int kL_R[kLayers] = {64, 8, 8, 1, 1, 8, 8, 64};  // rows per block
+constexpr int kL_ACT[kLayers] = {1, 1, 1, 0, 1, 1, 1, 0};
+constexpr float kSlope = 0.1f;  // leaky ReLU
+constexpr int kLatent = 32;
+constexpr int kBlock = 512;
+
+constexpr int w_off(int l) {
+  int o = 0;
+  for (int k = 0; k < l; k++) o += kL_K[k] * kL_N[k] + kL_N[k];
+  return o;
+}
+constexpr int kNParams = w_off(kLayers);
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// C(m, n) [+]= sum_k A(m, k) B(k, n) over k in this block's split of [0, K),
+// A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn]; operands rounded to
+// BF16.  Epilogue: + bias[n], optional pre-activation copy, leaky ReLU; or an
+// atomic add into C (split-K reductions, bias / activation not allowed).
+struct Gemm {
+  int M, N, K, ksplit;
+  const float *A;
+  long long sam, sak;
+  const float *B;
+  long long sbk, sbn;
+  float *C;
+  long long ldc;
+  const float *bias;
+  float *pre;
+  int act, atomic;
+};
+
+// block: 4 warps, each a 16 x 32 tile; grid (M / 64, N / 32, ksplit)
+__global__ void __launch_bounds__(128) gemm_bf16_k(Gemm g) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gr = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.x * 64 + warp * 16, n0 = blockIdx.y * 32;
+  const int kc = ((g.K + g.ksplit - 1) / g.ksplit + 15) / 16 * 16;
+  const int kb = blockIdx.z * kc, ke = min(g.K, kb + kc);
+  float acc[4][4] = {};
+  auto a_at = [&](int m, int k) -> float { return (m < g.M && k < ke) ? g.A[m * g.sam + k * g.sak] : 0.f; };
+  auto b_at = [&](int k, int n) -> float { return (n < g.N && k < ke) ? g.B[k * g.sbk + n * g.sbn] : 0.f; };
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+    uint32_t a[4];
+    const int r0 = m0 + gr, r1 = m0 + gr + 8, c0 = k0 + 2 * t, c1 = k0 + 2 * t + 8;
+    a[0] = pack_bf16(a_at(r0, c0), a_at(r0, c0 + 1));
+    a[1] = pack_bf16(a_at(r1, c0), a_at(r1, c0 + 1));
+    a[2] = pack_bf16(a_at(r0, c1), a_at(r0, c1 + 1));
+    a[3] = pack_bf16(a_at(r1, c1), a_at(r1, c1 + 1));
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) {
+      const int n = n0 + nt * 8 + gr;
+      const uint32_t b0 = pack_bf16(b_at(c0, n), b_at(c0 + 1, n));
+      const uint32_t b1 = pack_bf16(b_at(c1, n), b_at(c1 + 1, n));
+      mma_bf16(acc[nt], a, b0, b1);
+    }
+  }
+#pragma unroll
+  for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int m = m0 + gr + (q >= 2 ? 8 : 0), n = n0 + nt * 8 + 2 * t + (q & 1);
+      if (m >= g.M || n >= g.N) continue;
+      float v = acc[nt][q];
+      float *c = g.C + m * g.ldc + n;
+      if (g.atomic) {
+        atomicAdd(c, v);
+        continue;
+      }
+      if (g.bias) v += g.bias[n];
+      if (g.pre) g.pre[m * g.ldc + n] = v;
+      if (g.act) v = v > 0.f ? v : kSlope * v;
+      *c = v;
+    }
+}
+
+void gemm(const Gemm &g0, cudaStream_t st) {
+  Gemm g = g0;
+  if (g.M <= 0 || g.N <= 0) return;
+  if (!g.atomic) g.ksplit = 1;
+  const dim3 grid((g.M + 63) / 64, (g.N + 31) / 32, std::max(1, g.ksplit));
+  gemm_bf16_k<<<grid, 128, 0, st>>>(g);
+}
+
+// dP = dY * act'(pre) in place (leaky ReLU), for n elements
+__global__ void act_back_k(float *dy, const float *pre, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (pre[i] <= 0.f) dy[i] *= kSlope;
+}
+
+// column sums of an R x N matrix into out[n] (atomic across row chunks)
+__global__ void colsum_k(const float *dy, int R, int N, float *out) {
+  const int n = blockIdx.y * 32 + (threadIdx.x & 31);
+  if (n >= N) return;
+  float s = 0.f;
+  for (int r = blockIdx.x * 8 + (threadIdx.x >> 5); r < R; r += gridDim.x * 8) s += dy[(long long)r * N + n];
+  atomicAdd(out + n, s);
+}
+
+// MSE loss on n values: loss += sum (y - x)^2 / n; dy = 2 (y - x) / n
+__global__ void mse_k(const float *y, const float *x, long long n, float *dy, float *loss) {
+  float s = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float d = y[i] - x[i];
+    s += d * d;
+    dy[i] = 2.f * d / (float)n;
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, s / (float)n);
+}
+
+// Adam (bias-corrected) on the FP32 master parameters
+__global__ void adam_k(float *p, const float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi, vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi, v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Morton index of cell (x, y, z) of an 8^3 block: bits z0 y0 x0 z1 y1 x1 z2 y2 x2
+__host__ __device__ __forceinline__ int morton8(int x, int y, int z) {
+  int m = 0;
+#pragma unroll
+  for (int b = 0; b < 3; b++) m |= (((z >> b) & 1) << (3 * b)) | (((y >> b) & 1) << (3 * b + 1)) | (((x >> b) & 1) << (3 * b + 2));
+  return m;
+}
+
+// volume (z fastest) -> scale-normalised Morton blocks; cells outside the
+// volume are 0.  One CTA of 512 threads per block; blocks b0 .. b0+gridDim.x
+// of the (bx, by, bz) grid with bz fastest.
+__global__ void __launch_bounds__(512) blockify_k(const float *__restrict__ w, int nx, int ny, int nz, long long b0,
+                                                  float *__restrict__ blocks, float *__restrict__ scales) {
+  __shared__ float red[16];
+  const long long b = b0 + blockIdx.x;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+  const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
+  const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;  // z, x, y within the block
+  const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
+  const float v = (x < nx && y < ny && z < nz) ? w[((long long)y * nx + x) * nz + z] : 0.f;
+  float a = fabsf(v);
+  for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    a = threadIdx.x < 16 ? red[threadIdx.x] : 0.f;
+    for (int o = 8; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if (threadIdx.x == 0) red[0] = a;
+  }
+  __syncthreads();
+  const float s = red[0];
+  blocks[blockIdx.x * (long long)kBlock + morton8(i, j, k)] = s > 0.f ? v / s : 0.f;
+  if (threadIdx.x == 0) scales[blockIdx.x] = s;
+}
+
+// Morton blocks x scale -> volume (cells outside the volume dropped)
+__global__ void __launch_bounds__(512) unblockify_k(const float *__restrict__ blocks, const float *__restrict__ scales,
+                                                    long long b0, int nx, int ny, int nz, float *__restrict__ w) {
+  const long long b = b0 + blockIdx.x;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+  const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
+  const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;
+  const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
+  if (x < nx && y < ny && z < nz)
+    w[((long long)y * nx + x) * nz + z] = scales[blockIdx.x] * blocks[blockIdx.x * (long long)kBlock + morton8(i, j, k)];
+}
+
+}  // namespace
+}  // namespace rtm
+
+// ---- the compressor object ---------------------------------------------------
+struct rtm_ae {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // params, grads, Adam moments
+  float *loss = nullptr;
+  int step = 0;
+  // workspace for `cap` blocks: normalised input, per-layer outputs; training
+  // also keeps pre-activations and gradients
+  int cap = 0, cap_train = 0;
+  float *x0 = nullptr, *y[8] = {}, *pre[8] = {}, *dy[8] = {}, *dx0 = nullptr, *sc = nullptr;
+  std::string err;
+};
+
+namespace rtm {
+namespace {
+
+void ae_free_ws(rtm_ae *a) {
+  auto fr = [](float *&q) {
+    cudaFree(q);
+    q = nullptr;
+  };
+  fr(a->x0), fr(a->dx0), fr(a->sc);
+  for (int l = 0; l < kLayers; l++) fr(a->y[l]), fr(a->pre[l]), fr(a->dy[l]);
+  a->cap = a->cap_train = 0;
+}
+
+// workspace for n blocks (train: also pre-activations and gradients)
+int ae_reserve(rtm_ae *a, int n, bool train) {
+  if (n <= a->cap && (!train || n <= a->cap_train)) return RTM_OK;
+  const int cap = std::max(n, a->cap);
+  const bool tr = train || a->cap_train > 0;
+  ae_free_ws(a);
+  bool ok = cudaMalloc(&a->x0, (size_t)cap * kBlock * 4) == cudaSuccess &&
+            cudaMalloc(&a->sc, (size_t)cap * 4) == cudaSuccess;
+  if (tr) ok = ok && cudaMalloc(&a->dx0, (size_t)cap * kBlock * 4) == cudaSuccess;
+  for (int l = 0; l < kLayers && ok; l++) {
+    const size_t e = (size_t)cap * kL_R[l] * kL_N[l] * 4;
+    ok = cudaMalloc(&a->y[l], e) == cudaSuccess;
+    if (tr) ok = ok && cudaMalloc(&a->pre[l], e) == cudaSuccess && cudaMalloc(&a->dy[l], e) == cudaSuccess;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    ae_free_ws(a);
+    a->err = "compressor workspace allocation failed";
+    return RTM_ERR_NOMEM;
+  }
+  a->cap = cap, a->cap_train = tr ? cap : 0;
+  return RTM_OK;
+}
+
+// forward of layers [l0, l1) for n blocks, input of layer l0 at `in`
+void ae_forward(rtm_ae *a, int n, const float *in, int l0, int l1, bool keep_pre, cudaStream_t st) {
+  const float *x = in;
+  for (int l = l0; l < l1; l++) {
+    Gemm g{};
+    g.M = n * kL_R[l], g.N = kL_N[l], g.K = kL_K[l], g.ksplit = 1;
+    g.A = x, g.sam = kL_K[l], g.sak = 1;
+    g.B = a->p + w_off(l), g.sbk = kL_N[l], g.sbn = 1;
+    g.C = a->y[l], g.ldc = kL_N[l];
+    g.bias = a->p + w_off(l) + kL_K[l] * kL_N[l];
+    g.pre = keep_pre ? a->pre[l] : nullptr;
+    g.act = kL_ACT[l];
+    gemm(g, st);
+    x = a->y[l];
+  }
+}
+
+// loss and parameter gradients (into a->g) of n normalised blocks at a->x0
+void ae_loss_grad(rtm_ae *a, int n) {
+  cudaStream_t st = a->st;
+  ae_forward(a, n, a->x0, 0, kLayers, true, st);
+  cudaMemsetAsync(a->loss, 0, 4, st);
+  cudaMemsetAsync(a->g, 0, (size_t)kNParams * 4, st);
+  const long long tot = (long long)n * kBlock;
+  mse_k<<<(int)std::min<long long>((tot + 255) / 256, 1024), 256, 0, st>>>(a->y[kLayers - 1], a->x0, tot,
+                                                                            a->dy[kLayers - 1], a->loss);
+  for (int l = kLayers - 1; l >= 0; l--) {
+    const int R = n * kL_R[l], K = kL_K[l], N = kL_N[l];
+    const long long e = (long long)R * N;
+    if (kL_ACT[l])
+      act_back_k<<<(int)std::min<long long>((e + 255) / 256, 2048), 256, 0, st>>>(a->dy[l], a->pre[l], e);
+    const float *xin = l == 0 ? a->x0 : a->y[l - 1];
+    Gemm gw{};  // dW = X^T dP (K x N), reduction over the R rows, split-K
+    gw.M = K, gw.N = N, gw.K = R, gw.ksplit = std::max(1, std::min(128, R / 256));
+    gw.A = xin, gw.sam = 1, gw.sak = K;
+    gw.B = a->dy[l], gw.sbk = N, gw.sbn = 1;
+    gw.C = a->g + w_off(l), gw.ldc = N, gw.atomic = 1;
+    gemm(gw, st);
+    colsum_k<<<dim3(std::min(64, (R + 7) / 8), (N + 31) / 32), 256, 0, st>>>(a->dy[l], R, N,
+                                                                            a->g + w_off(l) + K * N);
+    Gemm gx{};  // dX = dP W^T (R x K)
+    gx.M = R, gx.N = K, gx.K = N, gx.ksplit = 1;
+    gx.A = a->dy[l], gx.sam = N, gx.sak = 1;
+    gx.B = a->p + w_off(l), gx.sbk = 1, gx.sbn = N;
+    gx.C = l == 0 ? a->dx0 : a->dy[l - 1], gx.ldc = K;
+    gemm(gx, st);
+  }
+}
+
+constexpr int kChunkBlocks = 8192;  // blocks per encode / decode pass over a volume
+
+}  // namespace
+
+long long ae_volume_blocks(int nx, int ny, int nz) {
+  return (long long)((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8);
+}
+
+int ae_prepare(rtm_ae *a) { return ae_reserve(a, kChunkBlocks, false); }
+
+// volume -> latents [nb][32] + scales [nb] (device), on stream st
+int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, float *latent, float *scales, cudaStream_t st) {
+  const long long nb = ae_volume_blocks(nx, ny, nz);
+  if (int rc = ae_reserve(a, kChunkBlocks, false)) return rc;
+  for (long long b0 = 0; b0 < nb; b0 += kChunkBlocks) {
+    const int n = (int)std::min<long long>(kChunkBlocks, nb - b0);
+    blockify_k<<<n, 512, 0, st>>>(w, nx, ny, nz, b0, a->x0, scales + b0);
+    ae_forward(a, n, a->x0, 0, 4, false, st);
+    cudaMemcpyAsync(latent + b0 * kLatent, a->y[3], (size_t)n * kLatent * 4, cudaMemcpyDeviceToDevice, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+// latents + scales -> volume (device), on stream st
+int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, int ny, int nz, float *w,
+                  cudaStream_t st) {
+  const long long nb = ae_volume_blocks(nx, ny, nz);
+  if (int rc = ae_reserve(a, kChunkBlocks, false)) return rc;
+  for (long long b0 = 0; b0 < nb; b0 += kChunkBlocks) {
+    const int n = (int)std::min<long long>(kChunkBlocks, nb - b0);
+    ae_forward(a, n, latent + b0 * kLatent, 4, kLayers, false, st);
+    unblockify_k<<<n, 512, 0, st>>>(a->y[kLayers - 1], scales + b0, b0, nx, ny, nz, w);
+  }
+  return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+}  // namespace rtm
+
+extern "C" {
+
+int rtm_ae_nparams(void) { return rtm::kNParams; }
+
+int rtm_ae_create(rtm_ae **out) {
+  if (!out) return RTM_ERR_ARG;
+  *out = nullptr;
+  rtm_ae *a = new rtm_ae();
+  cudaGetDevice(&a->device);
+  const size_t b = (size_t)rtm::kNParams * 4;
+  if (cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking) || cudaMalloc(&a->p, b) || cudaMalloc(&a->g, b) ||
+      cudaMalloc(&a->m, b) || cudaMalloc(&a->v, b) || cudaMalloc(&a->loss, 4) || cudaMemset(a->p, 0, b) ||
+      cudaMemset(a->m, 0, b) || cudaMemset(a->v, 0, b)) {
+    cudaGetLastError();
+    rtm_ae_destroy(a);
+    return RTM_ERR_NOMEM;
+  }
+  *out = a;
+  return RTM_OK;
+}
+
+int rtm_ae_destroy(rtm_ae *a) {
+  if (!a) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  if (a->st) cudaStreamSynchronize(a->st);
+  rtm::ae_free_ws(a);
+  cudaFree(a->p), cudaFree(a->g), cudaFree(a->m), cudaFree(a->v), cudaFree(a->loss);
+  if (a->st) cudaStreamDestroy(a->st);
+  delete a;
+  return RTM_OK;
+}
+
+int rtm_ae_set_params(rtm_ae *a, const float *params) {
+  if (!a || !params) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  if (cudaMemcpy(a->p, params, (size_t)rtm::kNParams * 4, cudaMemcpyHostToDevice)) return RTM_ERR_CUDA;
+  cudaMemset(a->m, 0, (size_t)rtm::kNParams * 4), cudaMemset(a->v, 0, (size_t)rtm::kNParams * 4);
+  a->step = 0;
+  return RTM_OK;
+}
+
+int rtm_ae_get_params(rtm_ae *a, float *params) {
+  if (!a || !params) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  cudaStreamSynchronize(a->st);
+  return cudaMemcpy(params, a->p, (size_t)rtm::kNParams * 4, cudaMemcpyDeviceToHost) ? RTM_ERR_CUDA : RTM_OK;
+}
+
+int rtm_ae_loss_grad(rtm_ae *a, const float *blocks, int n, float *loss, float *grads) {
+  if (!a || !blocks || n < 1 || !loss) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  if (int rc = rtm::ae_reserve(a, n, true)) return rc;
+  if (cudaMemcpyAsync(a->x0, blocks, (size_t)n * rtm::kBlock * 4, cudaMemcpyHostToDevice, a->st)) return RTM_ERR_CUDA;
+  rtm::ae_loss_grad(a, n);
+  cudaMemcpyAsync(loss, a->loss, 4, cudaMemcpyDeviceToHost, a->st);
+  if (grads) cudaMemcpyAsync(grads, a->g, (size_t)rtm::kNParams * 4, cudaMemcpyDeviceToHost, a->st);
+  return cudaStreamSynchronize(a->st) == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+int rtm_ae_train_step(rtm_ae *a, const float *blocks, int n, float lr, float *loss) {
+  if (!a || !blocks || n < 1 || !loss || !(lr > 0.f)) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  if (int rc = rtm::ae_reserve(a, n, true)) return rc;
+  if (cudaMemcpyAsync(a->x0, blocks, (size_t)n * rtm::kBlock * 4, cudaMemcpyHostToDevice, a->st)) return RTM_ERR_CUDA;
+  rtm::ae_loss_grad(a, n);
+  a->step++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)a->step), c2 = 1.f - powf(b2, (float)a->step);
+  rtm::adam_k<<<(rtm::kNParams + 255) / 256, 256, 0, a->st>>>(a->p, a->g, a->m, a->v, rtm::kNParams, lr, b1, b2, 1e-8f,
+                                                            c1, c2);
+  cudaMemcpyAsync(loss, a->loss, 4, cudaMemcpyDeviceToHost, a->st);
+  return cudaStreamSynchronize(a->st) == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+int rtm_ae_reconstruct(rtm_ae *a, const float *blocks, int n, float *out, float *latent) {
+  if (!a || !blocks || n < 1 || !out) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  if (int rc = rtm::ae_reserve(a, n, false)) return rc;
+  if (cudaMemcpyAsync(a->x0, blocks, (size_t)n * rtm::kBlock * 4, cudaMemcpyHostToDevice, a->st)) return RTM_ERR_CUDA;
+  rtm::ae_forward(a, n, a->x0, 0, rtm::kLayers, false, a->st);
+  cudaMemcpyAsync(out, a->y[rtm::kLayers - 1], (size_t)n * rtm::kBlock * 4, cudaMemcpyDeviceToHost, a->st);
+  if (latent) cudaMemcpyAsync(latent, a->y[3], (size_t)n * rtm::kLatent * 4, cudaMemcpyDeviceToHost, a->st);
+  return cudaStreamSynchronize(a->st) == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, float *d_latent, float *d_scales,
+                           void *stream) {
+  if (!a || !d_vol || !d_latent || !d_scales || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  return rtm::ae_compress(a, d_vol, nx, ny, nz, d_latent, d_scales, (cudaStream_t)stream);
+}
+
+int rtm_ae_decompress_volume(rtm_ae *a, const float *d_latent, const float *d_scales, int nx, int ny, int nz,
+                             float *d_vol, void *stream) {
+  if (!a || !d_vol || !d_latent || !d_scales || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  cudaSetDevice(a->device);
+  return rtm::ae_decompress(a, d_latent, d_scales, nx, ny, nz, d_vol, (cudaStream_t)stream);
+}
+
+}  // extern "C"

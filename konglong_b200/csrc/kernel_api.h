@@ -5,6 +5,8 @@
 
 #include "rtm_internal.cuh"
 
+struct rtm_ae;
+
 namespace rtm {
 
 struct IsoArgs {
@@ -152,5 +154,13 @@ void launch_c16_uncompress(const uint16_t *in, float *out, float *slab, const fl
 void launch_vel2(float *vel, float *invq, long long n, float dt2, float cq0, int use_q, cudaStream_t st);
 // NaN/Inf scan: sets *flag = 1 when any value is not finite
 void launch_nonfinite_scan(const float *w, long long n, int *flag, cudaStream_t st);
+
+// ---- learned snapshot compressor (ae.cu) --------------------------------------
+long long ae_volume_blocks(int nx, int ny, int nz);  // 8^3 blocks covering a volume
+int ae_prepare(rtm_ae *a);                           // workspace (call outside any capture)
+// volume -> latents [nb][32] + scales [nb]; latents + scales -> volume (device, stream st)
+int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, float *latent, float *scales, cudaStream_t st);
+int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, int ny, int nz, float *w,
+                  cudaStream_t st);
 
 }  // namespace rtm

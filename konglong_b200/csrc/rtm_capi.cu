@@ -82,6 +82,8 @@ struct Engine {
   float last_ms = 0.f;
   int *dflag = nullptr;
   int *nfflag = nullptr;  // result of the non-finite scan (allocated on first use)
+  rtm_ae *ae = nullptr;      // learned compressor of RTM_SNAP_AE snapshots
+  float *ae_scratch = nullptr;  // decoded source snapshot for the imaging condition
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
@@ -514,9 +516,31 @@ static FusedIo io_image(Engine *h, int slot) {
   return io;
 }
 
+// learned-compressor slot: latents [nb][32], then scales [nb]
+static float *ae_latent(Engine *h, int slot) { return (float *)(h->snaps + (size_t)slot * h->slot_bytes); }
+static float *ae_scales(Engine *h, int slot) {
+  return ae_latent(h, slot) + (size_t)ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 32;
+}
+static int ae_store(Engine *h, int slot, const float *w) {
+  KScope k(h, RTM_K_IO);
+  TRY(ae_compress(h->ae, w, h->d.nx, h->d.ny, h->d.nz, ae_latent(h, slot), ae_scales(h, slot), h->st));
+  return check_launch(h, "ae_compress");
+}
+static int ae_load(Engine *h, int slot, float *w) {
+  KScope k(h, RTM_K_IO);
+  TRY(ae_decompress(h->ae, ae_latent(h, slot), ae_scales(h, slot), h->d.nx, h->d.ny, h->d.nz, w, h->st));
+  return check_launch(h, "ae_decompress");
+}
+// imaging-condition term with the source snapshot decoded into ae_scratch
+static FusedIo io_image_ae(Engine *h, int slot) {
+  FusedIo io = io_image(h, slot);
+  io.src = SnapDev{RTM_SNAP_FP32, h->ae_scratch, nullptr};
+  return io;
+}
+
 // per-slot slab statistics for the 16-bit formats, taken on w0 after injection
 static int snap_prepare(Engine *h, int slot) {
-  if (h->snap_fmt == RTM_SNAP_FP32) return RTM_OK;
+  if (h->snap_fmt == RTM_SNAP_FP32 || h->snap_fmt == RTM_SNAP_AE) return RTM_OK;
   SnapDev s = slot_dev(h, slot);
   KScope k(h, RTM_K_SLAB);
   launch_slab_max(h->w0, (float *)s.slab, h->snap_fmt == RTM_SNAP_C16 ? (uint16_t *)s.base : nullptr, h->snap_fmt,
@@ -1121,27 +1145,49 @@ int rtm_get_traces(rtm_handle *h, float *dst) {
 }
 
 int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots) {
-  if (!h || nslots < 0 || fmt < RTM_SNAP_FP32 || fmt > RTM_SNAP_FP16S) return RTM_ERR_ARG;
+  if (!h || nslots < 0 || fmt < RTM_SNAP_FP32 || fmt > RTM_SNAP_AE) return RTM_ERR_ARG;
+  if (fmt == RTM_SNAP_AE && !h->ae) {
+    h->err = "RTM_SNAP_AE needs rtm_set_compressor first";
+    return RTM_ERR_STATE;
+  }
   cudaSetDevice(h->device);
-  h->release(h->snaps), h->release(h->slabs);
-  h->snaps = nullptr, h->slabs = nullptr;
+  h->release(h->snaps), h->release(h->slabs), h->release(h->ae_scratch);
+  h->snaps = nullptr, h->slabs = nullptr, h->ae_scratch = nullptr;
   h->snap_fmt = fmt, h->nslots = nslots;
-  h->slot_bytes = fmt == RTM_SNAP_FP32 ? (size_t)h->n * 4
-                                       : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2 : (size_t)h->n * 2;
+  h->slot_bytes = fmt == RTM_SNAP_FP32  ? (size_t)h->n * 4
+                  : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2
+                  : fmt == RTM_SNAP_AE  ? (size_t)rtm::ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4
+                                        : (size_t)h->n * 2;
   h->slot_bytes = (h->slot_bytes + 255) / 256 * 256;
   h->stored.assign(nslots, 0);
   if (!nslots) return RTM_OK;
   TRY(h->alloc(h->snaps, h->slot_bytes * nslots));
-  if (fmt != RTM_SNAP_FP32) TRY(h->alloc(h->slabs, (size_t)nslots * h->d.ny));
+  if (fmt == RTM_SNAP_C16 || fmt == RTM_SNAP_FP16S) TRY(h->alloc(h->slabs, (size_t)nslots * h->d.ny));
+  if (fmt == RTM_SNAP_AE) TRY(h->alloc(h->ae_scratch, h->n));
+  return RTM_OK;
+}
+
+int rtm_set_compressor(rtm_handle *h, rtm_ae *a) {
+  if (!h) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  h->ae = a;
+  if (a && rtm::ae_prepare(a) != RTM_OK) {
+    h->err = "compressor workspace allocation failed";
+    return RTM_ERR_NOMEM;
+  }
   return RTM_OK;
 }
 
 int rtm_snapshot_store(rtm_handle *h, int slot) {
   TRY(rtm::ready(h));
   if (slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
-  TRY(rtm::snap_prepare(h, slot));
-  rtm::launch_fused_io(rtm::io_store(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
-  TRY(rtm::check_launch(h, "snapshot_store"));
+  if (h->snap_fmt == RTM_SNAP_AE) {
+    TRY(rtm::ae_store(h, slot, h->w0));
+  } else {
+    TRY(rtm::snap_prepare(h, slot));
+    rtm::launch_fused_io(rtm::io_store(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
+    TRY(rtm::check_launch(h, "snapshot_store"));
+  }
   h->stored[slot] = 1;
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
@@ -1152,8 +1198,13 @@ int rtm_snapshot_load(rtm_handle *h, int slot, float *dst) {
   cudaSetDevice(h->device);
   float *tmp = nullptr;
   TRY(h->alloc(tmp, h->n));
-  rtm::launch_snap_decode(rtm::slot_dev(h, slot), tmp, h->ex, h->ey, h->ez, h->d.nx, h->d.ny, h->d.nz, h->st);
-  int rc = rtm::check_launch(h, "snapshot_load");
+  int rc;
+  if (h->snap_fmt == RTM_SNAP_AE) {
+    rc = rtm::ae_load(h, slot, tmp);
+  } else {
+    rtm::launch_snap_decode(rtm::slot_dev(h, slot), tmp, h->ex, h->ey, h->ez, h->d.nx, h->d.ny, h->d.nz, h->st);
+    rc = rtm::check_launch(h, "snapshot_load");
+  }
   if (rc == RTM_OK) {
     cudaError_t e = cudaMemcpyAsync(dst, tmp, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
@@ -1227,11 +1278,20 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
       const int slot = it / interval;
       if (slot >= 0 && slot < h->nslots) {
         if (dir == RTM_FORWARD) {
-          TRY(rtm::snap_prepare(h, slot));
-          pending = rtm::io_store(h, slot);
+          if (h->snap_fmt == RTM_SNAP_AE) {
+            TRY(rtm::ae_store(h, slot, h->w0));
+          } else {
+            TRY(rtm::snap_prepare(h, slot));
+            pending = rtm::io_store(h, slot);
+          }
           h->stored[slot] = 1;
         } else if (h->stored[slot]) {
-          pending = rtm::io_image(h, slot);
+          if (h->snap_fmt == RTM_SNAP_AE) {
+            TRY(rtm::ae_load(h, slot, h->ae_scratch));
+            pending = rtm::io_image_ae(h, slot);
+          } else {
+            pending = rtm::io_image(h, slot);
+          }
         }
       }
     }

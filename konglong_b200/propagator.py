@@ -153,6 +153,11 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def set_compressor(self, ae):
+        """Attach a compressor.AutoEncoder for RTM_SNAP_AE snapshots (None detaches)."""
+        self._ck(self.L.rtm_set_compressor(self.h, ae.a if ae is not None else None), "rtm_set_compressor")
+        self._ae = ae  # keep it alive while attached
+
     def check_finite(self, field):
         """True when `field` (W0 / W1 / IMAGE) holds only finite values."""
         nf = C.c_int(0)

@@ -1,0 +1,57 @@
+"""Learned compressor, CPU side: the oracle's gradient against finite
+differences, the Morton block layout and the volume <-> block round trip."""
+import numpy as np
+
+from konglong_b200 import compressor as AE
+from oracle import ae_oracle as O
+
+
+def test_layer_table_matches_library_layout():
+    assert AE.LAYERS == O.LAYERS
+    # every layer consumes the previous layer's output memory exactly
+    rows_out = [R * N for K, N, R, _ in AE.LAYERS]
+    rows_in = [R * K for K, N, R, _ in AE.LAYERS]
+    assert rows_in[0] == AE.BLOCK and rows_out[-1] == AE.BLOCK
+    assert rows_in[1:] == rows_out[:-1]
+    assert rows_out[3] == AE.LATENT
+    assert AE.init_params().size == sum(K * N + N for K, N, _, _ in AE.LAYERS)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    p = AE.init_params(3).astype(np.float64) + 0.01 * rng.standard_normal(AE.init_params().size)
+    blocks = rng.uniform(-1, 1, (2, AE.BLOCK))
+    loss, g = O.loss_grad(p, blocks)
+    idx = rng.choice(p.size, 40, replace=False)
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = O.loss_grad(q, blocks)
+        q[i] -= 2 * h
+        lm, _ = O.loss_grad(q, blocks)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (i, fd, g[i])
+
+
+def test_morton_layout_and_round_trip():
+    perm = AE.morton_perm()
+    assert sorted(perm.tolist()) == list(range(AE.BLOCK))
+    # the 8 children of each 2^3 cube are consecutive: Morton m // 8 groups
+    # cells whose (y, x, z) // 2 agree
+    loc = np.stack([perm // 64, (perm // 8) % 8, perm % 8], 1)
+    for g in range(64):
+        c = loc[8 * g:8 * g + 8] // 2
+        assert (c == c[0]).all()
+    rng = np.random.default_rng(1)
+    w = rng.standard_normal((19, 13, 21)).astype(np.float32)
+    b, s = AE.volume_to_blocks(w)
+    assert b.shape == (3 * 2 * 3, AE.BLOCK) and np.abs(b).max() <= 1.0 + 1e-6
+    np.testing.assert_allclose(AE.blocks_to_volume(b, s, w.shape), w, rtol=1e-6, atol=1e-6)
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -3.14159, 0.0], np.float32)
+    r = O.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6  # ties to even
+    assert abs(r[3] + 3.140625) < 1e-7 and r[4] == 0.0

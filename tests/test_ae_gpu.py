@@ -1,0 +1,113 @@
+"""Learned snapshot compressor on the GPU: tensor-core forward and gradients
+against the CPU oracle, training on the engine's own forward wavefields, the
+gain of the trained network over the code without learning, and the learned
+snapshots inside an RTM shot next to the plain FP32 store (the fallback that
+judges its image error) and COMPRESS_16."""
+import numpy as np
+import pytest
+
+from konglong_b200 import compressor as AE
+from konglong_b200 import workloads as W
+from konglong_b200.propagator import Propagator, spread_coeffs
+from konglong_b200.spec import FIELD_W0, SNAP_AE, SNAP_C16, SNAP_FP32
+from oracle import ae_oracle as O
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def data():
+    """Blocks of VTI compact-FD forward runs (the 512x512x400 workload's model
+    family at 0.2 scale): training blocks from two models, held-out blocks
+    from a third."""
+    tr = [AE.training_blocks(W.vti_cfd(scale=0.2, seed=sd, nt=400), Propagator, spread_coeffs,
+                             nblocks=6000, every=10)[0] for sd in (2, 3)]
+    held = AE.training_blocks(W.vti_cfd(scale=0.2, seed=9, nt=400), Propagator, spread_coeffs,
+                              nblocks=2000, every=10)[0]
+    return np.concatenate(tr), held
+
+
+def test_forward_matches_oracle(data):
+    ae = AE.AutoEncoder(seed=5)
+    p, b = ae.params(), data[0][:64]
+    out, lat = ae.reconstruct(b)
+    ref, ref_lat = O.reconstruct(p, b, round_bf16=True)
+    # same BF16 operands; the FP32 (GPU) and FP64 (oracle) sums of a layer can
+    # round an activation to neighbouring BF16 values in the next layer
+    assert rel_l2(out, ref) < 2e-3 and rel_l2(lat, ref_lat) < 2e-3
+    exact, _ = O.reconstruct(p, b, round_bf16=False)
+    assert rel_l2(out, exact) < 2e-2  # BF16 operands vs FP64
+
+
+def test_gradients_match_oracle(data):
+    ae = AE.AutoEncoder(seed=5)
+    p, b = ae.params(), data[0][:32]
+    loss, g = ae.loss_grad(b)
+    l_ref, g_ref = O.loss_grad(p, b, round_bf16=True)
+    assert abs(loss - l_ref) <= 1e-4 * l_ref
+    assert rel_l2(g, g_ref) < 2e-3
+    l64, g64 = O.loss_grad(p, b, round_bf16=False)
+    assert abs(loss - l64) <= 1e-3 * l64 and rel_l2(g, g64) < 2e-2
+
+
+def test_training_gain_over_untrained_and_naive_code(data):
+    train, held = data
+    ae = AE.AutoEncoder(seed=5)
+    before = rel_l2(ae.reconstruct(held)[0], held)
+    losses = ae.fit(train, steps=1500, batch=256, lr=3e-3)
+    after = rel_l2(ae.reconstruct(held)[0], held)
+    naive = rel_l2(AE.naive_16to1(held), held)
+    assert losses[-50:].mean() < 0.1 * losses[:10].mean()
+    # held-out blocks of another model, same 16:1 ratio as the averaging code
+    assert after < 0.2 * before
+    assert after < 0.6 * naive, (after, naive)
+
+
+def test_learned_snapshots_in_rtm(data):
+    train, _ = data
+    ae = AE.AutoEncoder(seed=5)
+    ae.fit(train, steps=1500, batch=256, lr=3e-3)
+    sh = W.vti_cfd(scale=0.2, seed=9, nt=300)
+    s = sh.spec
+    k1, k2 = W.spread_band(s)
+    src = W.make_traceset([sh.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    rcv = W.make_traceset(sh.rcv_pos, s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    m = Propagator(s)
+    m.set_model(**sh.model_arrays())
+    m.set_injection(src, sh.wavelet[None, :], s.dt_dxyz)
+    m.set_extraction(rcv, 300)
+    m.reset()
+    m.modelling(300, -1, 1)
+    rec = m.traces()
+    # the device store / load of one snapshot equals the host round trip
+    w = np.ascontiguousarray(m.get(FIELD_W0).reshape(s.shape))
+    m.set_compressor(ae)
+    m.snapshot_setup(SNAP_AE, 1)
+    m.put(FIELD_W0, w)
+    m.snapshot_store(0)
+    dev = m.snapshot_load(0).reshape(s.shape)
+    b, sc = AE.volume_to_blocks(w)
+    host = AE.blocks_to_volume(ae.reconstruct(b)[0], sc, s.shape)
+    assert rel_l2(dev, host) < 1e-6
+    m.close()
+    imgs = {}
+    for fmt in (SNAP_FP32, SNAP_C16, SNAP_AE):
+        q = Propagator(s)
+        q.set_model(**sh.model_arrays())
+        if fmt == SNAP_AE:
+            q.set_compressor(ae)
+        imgs[fmt] = q.rtm_shot(src, sh.wavelet[None, :], rcv, rec, 300, 210, 5, snap_fmt=fmt, ntaper_t=3,
+                               ntaper_z=4)[0].reshape(s.shape)
+        q.close()
+    ref = imgs[SNAP_FP32]
+    assert np.isfinite(imgs[SNAP_AE]).all() and np.abs(ref).max() > 0
+    assert rel_l2(imgs[SNAP_C16], ref) < 2e-3
+    # below the near-surface mute (source and receiver depth + 10 cells)
+    z0 = s.nbnd[4] + 12
+    deep = rel_l2(imgs[SNAP_AE][:, :, z0:], ref[:, :, z0:])
+    full = rel_l2(imgs[SNAP_AE], ref)
+    print(f"learned-snapshot image NRMSE vs FP32 store: full {full:.3f}, below z={z0}: {deep:.3f}")
+    # measured: full 0.96, below the mute 0.51 (the 16:1 code does not hold the
+    # near-source blocks, which carry most of the energy); regression bounds
+    assert full < 1.2 and deep < 0.7
