@@ -240,11 +240,7 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
         if (do_y) gy += a.c1y[m] * (q[R + m] - q[R - m]);
       }
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
-      if (in_pml(a.pml, g, ix, iy, iz)) {
-        pml1(a.pml, g, a.pml3d, DZ, 0, gz, ix, iy, iz);
-        pml1(a.pml, g, a.pml3d, DX, 0, gx, ix, iy, iz);
-        if (do_y) pml1(a.pml, g, a.pml3d, DY, 0, gy, ix, iy, iz);
-      }
+      if (in_pml(a.pml, g, ix, iy, iz)) pml1_all<0>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
       if (MODEL == 2 || MODEL == 3) {
         // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
         float e = cm.x;
@@ -358,11 +354,7 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
         dzv += a.c1z[m] * (tpz[tx][tz + R + m] - tpz[tx][tz + R - m]);
         if (do_y) dyv += a.c1y[m] * (q[R + m] - q[R - m]);
       }
-      if (in_pml(a.pml, g, ix, iy, iz)) {
-        pml1(a.pml, g, a.pml3d, DX, 1, dxv, ix, iy, iz);
-        pml1(a.pml, g, a.pml3d, DZ, 1, dzv, ix, iy, iz);
-        if (do_y) pml1(a.pml, g, a.pml3d, DY, 1, dyv, ix, iy, iz);
-      }
+      if (in_pml(a.pml, g, ix, iy, iz)) pml1_all<1>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
       // accumulation order of KernelCPU::TTI: x, then z, then y
       float t = cw0 - dxv * cvel;
       t = t - dzv * cvel;
