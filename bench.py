@@ -53,7 +53,9 @@ def alg_bytes_per_cell(spec, snap_fmt, interval):
         core, pml = 32.0, 48.0 * m
     if spec.use_q:
         core += 4.0 + 3 * 4.0 * spec.q_order
-    snap = {0: 4.0, 1: 2.0, 2: 2.0}[snap_fmt] / interval
+    if getattr(spec, "state_fp16", False):
+        core -= 3 * 2.0  # w1 read, w0 read and write in 2 bytes (3s with s = 2)
+    snap = {0: 4.0, 1: 2.0, 2: 2.0, 3: 33 * 4.0 / 512}[snap_fmt] / interval
     return core + pml + snap, core, pml
 
 
@@ -164,6 +166,7 @@ def run_cuda(args, rank, world):
     K, Wm = args.steps, args.warmup
     shot = build_workload(args.workload, 2 * K + Wm + 8, args.scale)
     s = shot.spec
+    s.state_fp16 = bool(args.state_fp16)
     snap_fmt = SNAP_C16
     k1, k2 = W.spread_band(s)
     src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
@@ -250,6 +253,7 @@ def run_cuda(args, rank, world):
     p.close()
     cfg = config_of(shot, snap_fmt, K)
     cfg["autotuned_shape"] = tuned
+    cfg["state"] = "fp16 per-slab scale" if s.state_fp16 else "fp32"
     return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
                 config=cfg, shot=shot, launches=launches)
 
@@ -397,6 +401,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="grid scale of the workload (1.0 = the configuration the metric is quoted on; "
                          "smaller values are for profiler captures)")
+    ap.add_argument("--state-fp16", action="store_true",
+                    help="FP16 wavefield state with per-slab scales (FD8 VTI / TTI workloads)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

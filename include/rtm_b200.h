@@ -90,7 +90,9 @@ typedef struct rtm_config {
   int pml3d;          /* default 1: PML on the summed operator / cross terms */
   float pml3d_scaler; /* cross-term damping scale, default 0.3 */
   int top_pml;        /* default 1; 0 = free surface top (no z1 PML) */
-  int state_fp16;     /* 0: FP32 wavefield state (default) */
+  int state_fp16;     /* 0: FP32 wavefield state (default); 1: FP16 w0 / w1 with a per-y-slab scale
+                         (stencils, PML, Q memory and image in FP32), FD8 VTI / TTI (+Q) only, loop
+                         drivers only (the stepwise seam calls return RTM_ERR_UNSUPPORTED) */
   int kernel_variant; /* 0: auto (ISO FD8: TMA plane pipeline when nz % 4 == 0; compact FD: register-
                          streamed x / y line solves, the autotuner may pick TMA tiles), 1: register
                          pipeline / plain staged tiles, 2: compact-FD x / y TMA tiles */

@@ -1,6 +1,7 @@
 // kernel_api.h - argument blocks and launchers of the B200 RTM kernels.
 #pragma once
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "rtm_internal.cuh"
@@ -30,8 +31,18 @@ struct IsoBatchShot {
   float *ext_out;     // [ext.ntr][ext.nt]
 };
 
+// FP16 wavefield state (per-y-slab scale: value = half * scale[iy])
+struct StateF16 {
+  const __half *w1;     // current field, scale s1
+  const float *s1;
+  __half *w0;           // previous field (read, scale s0) overwritten by the new one (scale sn)
+  const float *s0, *sn;
+  unsigned *m0;         // per-slab max |new value| (float bits), atomically raised
+};
+
 struct GradArgs {
   int nx, ny, nz, yseg, pml3d;
+  StateF16 h;           // used by the FP16-state instantiations
   const float *w1;
   float *px, *py, *pz;
   const float *eps, *del, *pjx, *pjy;
@@ -42,6 +53,7 @@ struct GradArgs {
 
 struct DivArgs {
   int nx, ny, nz, yseg, pml3d;
+  StateF16 h;
   const float *px, *py, *pz;
   const float *w1;
   float *w0;
@@ -64,8 +76,24 @@ int iso_batch_ctas_per_sm(int tx, int pml3d);
 void launch_batch_inject(const IsoBatchShot *shots, int nactive, int max_ntr, int max_ly, int it_src, int it,
                          cudaStream_t st);
 void launch_batch_extract(const IsoBatchShot *shots, int nactive, int max_ntr, int jt, int it, cudaStream_t st);
-void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st);
-void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st);
+void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st, bool f16 = false);
+void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st, bool f16 = false);
+// FP16 state: new-field scales sn[y] = max(max over |dy| <= 4 of m0 / m1, floor) * 2^-12
+void launch_f16_scales(const unsigned *m0, const unsigned *m1, float *sn, int ny, float floor, cudaStream_t st);
+// snapshot slab headers of the FP16 state's new field from its slab maxima
+void launch_f16_slab_hdr(const unsigned *m, float *slab, uint16_t *c16, int fmt, int nx, int ny, int nz,
+                         cudaStream_t st);
+// FP16 state <-> FP32 volume; f32_to_f16 takes the slab max, sets the scale
+// (max * 2^-12, at least floor * 2^-12) and records the max
+void launch_f16_to_f32(const __half *h, const float *s, float *out, int ny, long long nxz, cudaStream_t st);
+void launch_f32_to_f16(const float *in, __half *h, float *s, unsigned *m, int ny, long long nxz, float floor,
+                       cudaStream_t st);
+// FP16 state: scatter of every trace into h (scale s), raising the slab max m;
+// gather of every receiver from h
+void launch_inject_scatter_f16(const TraceDev &t, int it, __half *h, const float *s, unsigned *m, const float *vel,
+                               int nx, int ny, int nz, cudaStream_t st);
+void launch_extract_direct_f16(const TraceDev &t, const __half *h, const float *s, float *out, int jt, int nt_out,
+                               int nx, int ny, int nz, cudaStream_t st);
 
 // ---- TMA plane pipelines (kernels_tma.cu), nz % 4 == 0 ------------------------
 bool tma_supported(int nz);

@@ -58,6 +58,31 @@ __device__ __forceinline__ Halo fetch_halo(const float *__restrict__ f, int iy, 
   return h;
 }
 
+// fetch_halo with an accessor v(i, iy) for the wavefield (FP16 state)
+template <int TX, typename V>
+__device__ __forceinline__ Halo fetch_halo_v(V v, int iy, int ny, int ix, int iz, int nx, int nz, long long nxz, int tx,
+                                             int tz) {
+  Halo h{0.f, 0.f, 0.f, 0.f};
+  if (iy < 0 || iy >= ny) return h;
+  const long long plane = (long long)iy * nxz;
+  if (tz < R) {
+    const int izl = iz - R, izh = iz + TZ;
+    if (ix < nx && izl >= 0) h.zl = v(plane + (long long)ix * nz + izl, iy);
+    if (ix < nx && izh < nz) h.zh = v(plane + (long long)ix * nz + izh, iy);
+  }
+  if (tx < R) {
+    const int ixl = ix - R, ixh = ix + TX;
+    if (iz < nz && ixl >= 0) h.xl = v(plane + (long long)ixl * nz + iz, iy);
+    if (iz < nz && ixh < nx) h.xh = v(plane + (long long)ixh * nz + iz, iy);
+  }
+  return h;
+}
+
+// FP16 state value: half * per-slab scale
+__device__ __forceinline__ float f16v(const __half *h, const float *s, long long i, int iy) {
+  return __half2float(h[i]) * __ldg(s + iy);
+}
+
 template <int TX>
 __device__ __forceinline__ void put_tile(float (*tile)[TZ + 2 * R], const Halo &h, float c, int tx, int tz) {
   tile[tx + R][tz + R] = c;
@@ -190,7 +215,7 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_batch(const IsoBatchShot *__re
 }
 
 // ---- anisotropic two-pass ----------------------------------------------------
-template <int TX, int MODEL>
+template <int TX, int MODEL, bool F16>
 __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
   __shared__ float tile[TX + 2 * R][TZ + 2 * R];
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
@@ -203,15 +228,16 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
   const long long col = (long long)ix * a.nz + iz;
   const float *__restrict__ w1 = a.w1;
   const bool do_y = a.ny > 1;
+  auto v1 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w1, a.h.s1, i, iy) : __ldg(w1 + i); };
 
   float q[2 * R + 1];
 #pragma unroll
   for (int k = 0; k < 2 * R; k++) {
     const int y = y0 - R + k;
-    q[k] = ld_or0(w1, (long long)y * g.nxz + col, act && y >= 0 && y < a.ny);
+    q[k] = act && y >= 0 && y < a.ny ? v1((long long)y * g.nxz + col, y) : 0.f;
   }
-  Halo h0 = fetch_halo<TX>(w1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
-  Halo h1 = fetch_halo<TX>(w1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  Halo h0 = fetch_halo_v<TX>(v1, y0, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+  Halo h1 = fetch_halo_v<TX>(v1, y0 + 1, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
   // anisotropy parameters of the next plane
   float4 nm = make_float4(0.f, 0.f, 0.f, 0.f);
   auto fetch_model = [&](long long i) {
@@ -222,11 +248,11 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
   };
   if (act) nm = fetch_model((long long)y0 * g.nxz + col);
   for (int iy = y0; iy < y1; iy++) {
-    q[2 * R] = ld_or0(w1, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
+    q[2 * R] = act && iy + R < a.ny ? v1((long long)(iy + R) * g.nxz + col, iy + R) : 0.f;
     const long long plane = (long long)iy * g.nxz;
     put_tile<TX>(tile, h0, q[R], tx, tz);
     h0 = h1;
-    h1 = fetch_halo<TX>(w1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
+    h1 = fetch_halo_v<TX>(v1, iy + 2 < y1 ? iy + 2 : a.ny, a.ny, ix, iz, a.nx, a.nz, g.nxz, tx, tz);
     const float4 cm = nm;
     if (act && iy + 1 < y1) nm = fetch_model(plane + g.nxz + col);
     __syncthreads();
@@ -304,7 +330,7 @@ __device__ __forceinline__ DivPlane fetch_div(const DivArgs &a, int iy, int ix, 
   return d;
 }
 
-template <int TX, int MODE>
+template <int TX, int MODE, bool F16>
 __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
   __shared__ float tpx[TX + 2 * R][TZ];
   __shared__ float tpz[TX][TZ + 2 * R];
@@ -326,9 +352,12 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
   }
   DivPlane d0 = fetch_div<TX>(a, y0, ix, iz, g.nxz, tx, tz, act);
   DivPlane d1 = fetch_div<TX>(a, y0 + 1 < y1 ? y0 + 1 : a.ny, ix, iz, g.nxz, tx, tz, act);
-  float nw0 = act ? a.w0[(long long)y0 * g.nxz + col] : 0.f;
+  auto v0 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w0, a.h.s0, i, iy) : a.w0[i]; };
+  auto v1 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w1, a.h.s1, i, iy) : __ldg(a.w1 + i); };
+  float nw0 = act ? v0((long long)y0 * g.nxz + col, y0) : 0.f;
   float nvel = act ? __ldg(a.vel + (long long)y0 * g.nxz + col) : 0.f;
-  float nw1 = act && MODE != 0 ? __ldg(a.w1 + (long long)y0 * g.nxz + col) : 0.f;
+  float nw1 = act && MODE != 0 ? v1((long long)y0 * g.nxz + col, y0) : 0.f;
+  float amax = 0.f;
   for (int iy = y0; iy < y1; iy++) {
     if (do_y) q[2 * R] = ld_or0(a.py, (long long)(iy + R) * g.nxz + col, act && iy + R < a.ny);
     const long long plane = (long long)iy * g.nxz;
@@ -340,9 +369,9 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
     d1 = fetch_div<TX>(a, iy + 2 < y1 ? iy + 2 : a.ny, ix, iz, g.nxz, tx, tz, act);
     const float cw0 = nw0, cvel = nvel, cw1 = nw1;
     if (act && iy + 1 < y1) {
-      nw0 = a.w0[plane + g.nxz + col];
+      nw0 = v0(plane + g.nxz + col, iy + 1);
       nvel = __ldg(a.vel + plane + g.nxz + col);
-      if (MODE != 0) nw1 = __ldg(a.w1 + plane + g.nxz + col);
+      if (MODE != 0) nw1 = v1(plane + g.nxz + col, iy + 1);
     }
     __syncthreads();
     if (act) {
@@ -362,7 +391,20 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
       float out;
       if (MODE == 0) out = t;
       else out = MODE == 1 ? (cw1 + cw1) - t : q_update(a.q, i, (long long)a.ny * g.nxz, t, cw1);
-      a.w0[i] = out;
+      if (F16) {
+        const float sc = __ldg(a.h.sn + iy);
+        float hv = out / sc;
+        if (fabsf(hv) > 65504.f) hv = copysignf(65504.f, hv);  // saturate; a NaN stays a NaN
+        a.h.w0[i] = __float2half_rn(hv);
+        amax = fabsf(out);
+      } else {
+        a.w0[i] = out;
+      }
+    }
+    if (F16) {  // slab max of the new field (all lanes of a warp are on plane iy)
+      for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      if ((threadIdx.x & 31) == 0 && amax > 0.f) atomicMax(a.h.m0 + iy, __float_as_uint(amax));
+      amax = 0.f;
     }
     __syncthreads();
 #pragma unroll
@@ -425,32 +467,44 @@ int iso_batch_ctas_per_sm(int tx, int pml3d) {
   return std::max(1, n);
 }
 
-template <int TX>
+template <int TX, bool F16>
 static void grad_launch_tx(const GradArgs &a, int model, cudaStream_t st) {
   dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
-  if (model == 3) grad_fd8<TX, 3><<<grid, block, 0, st>>>(a);
-  else if (model == 2) grad_fd8<TX, 2><<<grid, block, 0, st>>>(a);
-  else grad_fd8<TX, 1><<<grid, block, 0, st>>>(a);
+  if (model == 3) grad_fd8<TX, 3, F16><<<grid, block, 0, st>>>(a);
+  else if (model == 2) grad_fd8<TX, 2, F16><<<grid, block, 0, st>>>(a);
+  else grad_fd8<TX, 1, F16><<<grid, block, 0, st>>>(a);
 }
 
-void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st) {
-  if (tx == 4) grad_launch_tx<4>(a, model, st);
-  else if (tx == 16) grad_launch_tx<16>(a, model, st);
-  else grad_launch_tx<8>(a, model, st);
+void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st, bool f16) {
+  if (f16) {
+    if (tx == 4) grad_launch_tx<4, true>(a, model, st);
+    else if (tx == 16) grad_launch_tx<16, true>(a, model, st);
+    else grad_launch_tx<8, true>(a, model, st);
+    return;
+  }
+  if (tx == 4) grad_launch_tx<4, false>(a, model, st);
+  else if (tx == 16) grad_launch_tx<16, false>(a, model, st);
+  else grad_launch_tx<8, false>(a, model, st);
 }
 
-template <int TX>
+template <int TX, bool F16>
 static void div_launch_tx(const DivArgs &a, int mode, cudaStream_t st) {
   dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
-  if (mode == 0) div_fd8<TX, 0><<<grid, block, 0, st>>>(a);
-  else if (mode == 1) div_fd8<TX, 1><<<grid, block, 0, st>>>(a);
-  else div_fd8<TX, 2><<<grid, block, 0, st>>>(a);
+  if (mode == 0) div_fd8<TX, 0, F16><<<grid, block, 0, st>>>(a);
+  else if (mode == 1) div_fd8<TX, 1, F16><<<grid, block, 0, st>>>(a);
+  else div_fd8<TX, 2, F16><<<grid, block, 0, st>>>(a);
 }
 
-void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st) {
-  if (tx == 4) div_launch_tx<4>(a, mode, st);
-  else if (tx == 16) div_launch_tx<16>(a, mode, st);
-  else div_launch_tx<8>(a, mode, st);
+void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st, bool f16) {
+  if (f16) {
+    if (tx == 4) div_launch_tx<4, true>(a, mode, st);
+    else if (tx == 16) div_launch_tx<16, true>(a, mode, st);
+    else div_launch_tx<8, true>(a, mode, st);
+    return;
+  }
+  if (tx == 4) div_launch_tx<4, false>(a, mode, st);
+  else if (tx == 16) div_launch_tx<16, false>(a, mode, st);
+  else div_launch_tx<8, false>(a, mode, st);
 }
 
 }  // namespace rtm

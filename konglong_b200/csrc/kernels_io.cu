@@ -311,6 +311,143 @@ void launch_batch_extract(const IsoBatchShot *shots, int nactive, int max_ntr, i
   batch_extract_k<<<dim3((max_ntr + 7) / 8, nactive), 256, 0, st>>>(shots, jt, it);
 }
 
+// ---- FP16 wavefield state ----------------------------------------------------
+// new-field scales: the largest slab max within +-4 slabs of either field
+// (the stencil radius bounds how far the wave moves in one step), at least
+// `floor`, with 16x headroom (2^-12 of the FP16 range 65504 ~ 2^16)
+__global__ void f16_scales_k(const unsigned *__restrict__ m0, const unsigned *__restrict__ m1, float *sn, int ny,
+                             float floor) {
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= ny) return;
+  float m = floor;
+  for (int d = -4; d <= 4; d++) {
+    const int k = y + d;
+    if (k < 0 || k >= ny) continue;
+    m = fmaxf(m, fmaxf(__uint_as_float(m0[k]), __uint_as_float(m1[k])));
+  }
+  sn[y] = m * (1.0f / 4096.0f);
+}
+
+// snapshot slab headers (COMPRESS_16 vmax / FP16 slab scale, as slab_max_k
+// writes them) from the tracked slab maxima of the FP16 state
+__global__ void f16_slab_hdr_k(const unsigned *__restrict__ m, float *slab, uint16_t *c16, int fmt, long long nxz,
+                               int ny) {
+  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iy >= ny) return;
+  const float mx = __uint_as_float(m[iy]);
+  if (fmt == 1) {
+    const float hdr = mx > 1e-25f ? mx : 0.f;
+    slab[iy] = hdr;
+    if (c16) {
+      const unsigned bits = __float_as_uint(hdr);
+      uint16_t *h = c16 + (long long)iy * (nxz + 2);
+      h[0] = (uint16_t)(bits & 0xffffu);
+      h[1] = (uint16_t)(bits >> 16);
+    }
+  } else {
+    slab[iy] = mx * 6.103515625e-05f;
+  }
+}
+
+__global__ void f16_to_f32_k(const __half *__restrict__ h, const float *__restrict__ s, float *__restrict__ out,
+                             long long nxz, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = __half2float(h[i]) * s[i / nxz];
+}
+
+// one block per y slab: max, scale, conversion
+__global__ void f32_to_f16_k(const float *__restrict__ in, __half *__restrict__ h, float *s, unsigned *m, long long nxz,
+                             float floor) {
+  __shared__ float red[32];
+  const long long base = (long long)blockIdx.x * nxz;
+  float a = 0.f;
+  for (long long i = threadIdx.x; i < nxz; i += blockDim.x) a = fmaxf(a, fabsf(in[base + i]));
+  for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    a = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if (threadIdx.x == 0) red[0] = a;
+  }
+  __syncthreads();
+  const float mx = red[0], sc = fmaxf(mx, floor) * (1.0f / 4096.0f);
+  if (threadIdx.x == 0) s[blockIdx.x] = sc, m[blockIdx.x] = __float_as_uint(mx);
+  const float r = 1.0f / sc;
+  for (long long i = threadIdx.x; i < nxz; i += blockDim.x) h[base + i] = __float2half_rn(in[base + i] * r);
+}
+
+// Receiver::apply_src into FP16 state: value / scale added with a 16-bit atomic
+__global__ void inject_scatter_f16_k(TraceDev t, int it, __half *__restrict__ h, const float *__restrict__ s,
+                                     unsigned *m, const float *__restrict__ vel, int nx, int nz) {
+  const int r = blockIdx.x;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], lz = l[2];
+  const int iy = blockIdx.y;
+  if (iy >= l[1]) return;
+  const int gy = iy + o[1];
+  const float val = t.traces[(long long)r * t.nt + it] * t.scaler;
+  const float rs = 1.0f / s[gy];
+  float amax = 0.f;
+  for (int k = threadIdx.x; k < lx * lz; k += blockDim.x) {
+    const int iz = k % lz, ix = k / lz;
+    const float cy = val * t.ky[(long long)r * t.ly + iy];
+    const float cx = cy * t.kx[(long long)r * t.lx + ix];
+    const long long c = ((long long)gy * nx + ix + o[0]) * nz + o[2] + iz;
+    const float add = cx * t.kz[(long long)r * t.lz + iz] * vel[c];
+    const __half old = atomicAdd(h + c, __float2half_rn(add * rs));
+    amax = fmaxf(amax, fabsf(__half2float(old) + add * rs) * s[gy]);
+  }
+  for (int o2 = 16; o2; o2 >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o2));
+  if ((threadIdx.x & 31) == 0 && amax > 0.f) atomicMax(m + gy, __float_as_uint(amax));
+}
+
+__global__ void extract_direct_f16_k(TraceDev t, const __half *__restrict__ h, const float *__restrict__ s,
+                                     float *__restrict__ out, int jt, int nt_out, int nx, int nz) {
+  const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (r >= t.ntr) return;
+  const int *o = t.off + 3 * r, *l = t.len + 3 * r;
+  const int lx = l[0], ly = l[1], lz = l[2];
+  float acc = 0.f;
+  for (int k = lane; k < lx * ly * lz; k += 32) {
+    const int iz = k % lz, ix = (k / lz) % lx, iy = k / (lz * lx);
+    const float cx = t.ky[(long long)r * t.ly + iy] * t.kx[(long long)r * t.lx + ix];
+    const long long c = ((long long)(iy + o[1]) * nx + ix + o[0]) * nz + o[2] + iz;
+    acc += cx * t.kz[(long long)r * t.lz + iz] * (__half2float(h[c]) * s[iy + o[1]]);
+  }
+  for (int o2 = 16; o2; o2 >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o2);
+  if (lane == 0) out[(long long)r * nt_out + jt] = acc;
+}
+
+void launch_f16_scales(const unsigned *m0, const unsigned *m1, float *sn, int ny, float floor, cudaStream_t st) {
+  f16_scales_k<<<(ny + 127) / 128, 128, 0, st>>>(m0, m1, sn, ny, floor);
+}
+void launch_f16_slab_hdr(const unsigned *m, float *slab, uint16_t *c16, int fmt, int nx, int ny, int nz,
+                         cudaStream_t st) {
+  f16_slab_hdr_k<<<(ny + 127) / 128, 128, 0, st>>>(m, slab, c16, fmt, (long long)nx * nz, ny);
+}
+void launch_f16_to_f32(const __half *h, const float *s, float *out, int ny, long long nxz, cudaStream_t st) {
+  const long long n = nxz * ny;
+  f16_to_f32_k<<<(int)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(h, s, out, nxz, n);
+}
+void launch_f32_to_f16(const float *in, __half *h, float *s, unsigned *m, int ny, long long nxz, float floor,
+                       cudaStream_t st) {
+  f32_to_f16_k<<<ny, 512, 0, st>>>(in, h, s, m, nxz, floor);
+}
+void launch_inject_scatter_f16(const TraceDev &t, int it, __half *h, const float *s, unsigned *m, const float *vel,
+                               int nx, int ny, int nz, cudaStream_t st) {
+  (void)ny;
+  if (t.ntr <= 0 || it < 0 || it >= t.nt) return;
+  inject_scatter_f16_k<<<dim3(t.ntr, t.ly), 256, 0, st>>>(t, it, h, s, m, vel, nx, nz);
+}
+void launch_extract_direct_f16(const TraceDev &t, const __half *h, const float *s, float *out, int jt, int nt_out,
+                               int nx, int ny, int nz, cudaStream_t st) {
+  (void)ny;
+  if (t.ntr <= 0 || jt < 0 || jt >= nt_out) return;
+  extract_direct_f16_k<<<(t.ntr + 7) / 8, 256, 0, st>>>(t, h, s, out, jt, nt_out, nx, nz);
+}
+
 void launch_inject_group(const GroupDev &gr, const TraceDev &t, int it, float *plane, float *w0, const float *vel,
                          int nx, int ny, int nz, cudaStream_t st) {
   (void)plane;

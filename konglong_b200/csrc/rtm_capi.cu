@@ -83,6 +83,14 @@ struct Engine {
   int *dflag = nullptr;
   int *nfflag = nullptr;  // result of the non-finite scan (allocated on first use)
   rtm_ae *ae = nullptr;      // learned compressor of RTM_SNAP_AE snapshots
+  // FP16 wavefield state (state_fp16): h0 / h1 play w0 / w1, value = half * s[iy];
+  // sn is the scale of the field the current step writes; m0 / m1 slab maxima
+  int f16 = 0;
+  __half *h0 = nullptr, *h1 = nullptr;
+  float *s0 = nullptr, *s1 = nullptr, *sn = nullptr;
+  unsigned *m0 = nullptr, *m1 = nullptr;
+  float f16_floor = 1e-20f;  // smallest slab max a scale is built for (source amplitude)
+  float vel2max = 0.f;       // max (v dt)^2 of the model
   float *ae_scratch = nullptr;  // decoded source snapshot for the imaging condition
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
@@ -307,8 +315,18 @@ static int setup_pml(Engine *h) {
 }
 
 static int zero_state(Engine *h) {
-  CK(cudaMemsetAsync(h->w0, 0, h->n * 4, h->st));
-  CK(cudaMemsetAsync(h->w1, 0, h->n * 4, h->st));
+  if (h->f16) {
+    CK(cudaMemsetAsync(h->h0, 0, h->n * 2, h->st));
+    CK(cudaMemsetAsync(h->h1, 0, h->n * 2, h->st));
+    CK(cudaMemsetAsync(h->m0, 0, h->d.ny * 4, h->st));
+    CK(cudaMemsetAsync(h->m1, 0, h->d.ny * 4, h->st));
+    launch_f16_scales(h->m0, h->m1, h->s0, h->d.ny, h->f16_floor, h->st);
+    launch_f16_scales(h->m0, h->m1, h->s1, h->d.ny, h->f16_floor, h->st);
+    launch_f16_scales(h->m0, h->m1, h->sn, h->d.ny, h->f16_floor, h->st);
+  } else {
+    CK(cudaMemsetAsync(h->w0, 0, h->n * 4, h->st));
+    CK(cudaMemsetAsync(h->w1, 0, h->n * 4, h->st));
+  }
   for (int dim = 0; dim < 3; dim++)
     for (int s = 0; s < 2; s++) {
       PmlFace &F = h->pml.f[dim][s];
@@ -371,24 +389,30 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     GradArgs g{};
     g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = h->yseg, g.pml3d = h->c.pml3d;
     g.w1 = h->w1, g.px = h->px, g.py = h->py, g.pz = h->pz;
+    g.h = StateF16{h->h1, h->s1, h->h0, h->s0, h->sn, h->m0};
     g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy;
     memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
     g.pml = pml_dev(h);
     g.io = io;
     {
       KScope k(h, RTM_K_GRAD);
-      launch_grad_fd8(g, h->c.model_type, h->tx, h->st);
+      launch_grad_fd8(g, h->c.model_type, h->tx, h->st, h->f16);
     }
     TRY(check_launch(h, "grad_fd8"));
+    if (h->f16) {  // scale of the field this step writes, then its fresh slab maxima
+      launch_f16_scales(h->m0, h->m1, h->sn, d.ny, h->f16_floor, h->st);
+      CK(cudaMemsetAsync(h->m0, 0, d.ny * 4, h->st));
+    }
     DivArgs v{};
     v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = h->yseg, v.pml3d = h->c.pml3d;
+    v.h = StateF16{h->h1, h->s1, h->h0, h->s0, h->sn, h->m0};
     v.px = h->px, v.py = h->py, v.pz = h->pz, v.w1 = h->w1, v.w0 = h->w0, v.vel = h->vel;
     memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
     v.pml = pml_dev(h);
     v.q = q;
     {
       KScope k(h, RTM_K_DIV);
-      launch_div_fd8(v, mode, h->tx, h->st);
+      launch_div_fd8(v, mode, h->tx, h->st, h->f16);
     }
     return check_launch(h, "div_fd8");
   }
@@ -456,6 +480,11 @@ static int do_inject(Engine *h, int it) {
   TraceSetDev &t = h->inj;
   if (!t.ntr || it < 0 || it >= t.nt) return RTM_OK;
   TraceDev td = t.dev();
+  if (h->f16) {
+    KScope k(h, RTM_K_INJECT);
+    launch_inject_scatter_f16(td, it, h->h0, h->sn, h->m0, h->vel, h->d.nx, h->d.ny, h->d.nz, h->st);
+    return check_launch(h, "inject");
+  }
   KScope k(h, RTM_K_INJECT, (int)t.groups.size() + (t.n_ungrouped ? 1 : 0));
   for (const GroupDev &g : t.groups)
     launch_inject_group(g, td, it, h->plane, h->w0, h->vel, h->d.nx, h->d.ny, h->d.nz, h->st);
@@ -470,6 +499,11 @@ static int do_extract(Engine *h, int jt) {
   TraceSetDev &t = h->ext;
   if (!t.ntr || jt < 0 || jt >= t.nt) return RTM_OK;
   TraceDev td = t.dev();
+  if (h->f16) {
+    KScope k(h, RTM_K_EXTRACT);
+    launch_extract_direct_f16(td, h->h0, h->sn, t.out, jt, t.nt, h->d.nx, h->d.ny, h->d.nz, h->st);
+    return check_launch(h, "extract");
+  }
   KScope k(h, RTM_K_EXTRACT, 2 * (int)t.groups.size() + (t.n_ungrouped ? 1 : 0));
   for (const GroupDev &g : t.groups)
     launch_extract_group(g, td, h->w0, h->plane, t.out, jt, t.nt, h->d.nx, h->d.ny, h->d.nz, h->st);
@@ -483,6 +517,21 @@ static int do_extract(Engine *h, int jt) {
 static void do_swap(Engine *h) {
   std::swap(h->w0, h->w1);
   h->iq0 = 1 - h->iq0;
+  if (h->f16) {  // the new field (scale sn) becomes w1, the old w1 (scale s1) becomes w0
+    std::swap(h->h0, h->h1);
+    float *t = h->s0;
+    h->s0 = h->s1, h->s1 = h->sn, h->sn = t;
+    std::swap(h->m0, h->m1);
+  }
+}
+
+// FP32 copy of an FP16 state field in the px scratch: which = 0 / 1 the w0 /
+// w1 of a completed step, 2 the field the current step wrote (before the swap)
+static float *f16_view(Engine *h, int which) {
+  const __half *f = which == 1 ? h->h1 : h->h0;
+  const float *sc = which == 0 ? h->s0 : which == 1 ? h->s1 : h->sn;
+  launch_f16_to_f32(f, sc, h->px, h->d.ny, h->nxz, h->st);
+  return h->px;
 }
 
 static SnapDev slot_dev(Engine *h, int slot) {
@@ -543,6 +592,11 @@ static int snap_prepare(Engine *h, int slot) {
   if (h->snap_fmt == RTM_SNAP_FP32 || h->snap_fmt == RTM_SNAP_AE) return RTM_OK;
   SnapDev s = slot_dev(h, slot);
   KScope k(h, RTM_K_SLAB);
+  if (h->f16) {
+    launch_f16_slab_hdr(h->m0, (float *)s.slab, h->snap_fmt == RTM_SNAP_C16 ? (uint16_t *)s.base : nullptr,
+                        h->snap_fmt, h->d.nx, h->d.ny, h->d.nz, h->st);
+    return check_launch(h, "slab_hdr");
+  }
   launch_slab_max(h->w0, (float *)s.slab, h->snap_fmt == RTM_SNAP_C16 ? (uint16_t *)s.base : nullptr, h->snap_fmt,
                   h->d.nx, h->d.ny, h->d.nz, h->st);
   return check_launch(h, "slab_max");
@@ -884,8 +938,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
   }
-  if (c->state_fp16) {
-    g_create_error = "rtm_create: FP16 wavefield state is not built";
+  if (c->state_fp16 && (c->engine != RTM_ENGINE_FD8 || c->model_type < RTM_VTI)) {
+    g_create_error = "rtm_create: FP16 wavefield state is built for the FD8 VTI / TTI (+Q) path";
     return RTM_ERR_UNSUPPORTED;
   }
   rtm_handle *h = new rtm_handle();
@@ -910,9 +964,16 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     cudaGetLastError();
     return fail(RTM_ERR_CUDA);
   }
-  if ((rc = h->alloc(h->w0, h->n)) || (rc = h->alloc(h->w1, h->n)) || (rc = h->alloc(h->vel, h->n)) ||
-      (rc = h->alloc(h->dflag, 1)))
+  h->f16 = c->state_fp16 ? 1 : 0;
+  if (h->f16) {
+    if ((rc = h->alloc(h->h0, h->n)) || (rc = h->alloc(h->h1, h->n)) || (rc = h->alloc(h->s0, d->ny)) ||
+        (rc = h->alloc(h->s1, d->ny)) || (rc = h->alloc(h->sn, d->ny)) || (rc = h->alloc(h->m0, d->ny)) ||
+        (rc = h->alloc(h->m1, d->ny)))
+      return fail(rc);
+  } else if ((rc = h->alloc(h->w0, h->n)) || (rc = h->alloc(h->w1, h->n))) {
     return fail(rc);
+  }
+  if ((rc = h->alloc(h->vel, h->n)) || (rc = h->alloc(h->dflag, 1))) return fail(rc);
   const bool first_deriv = !(c->engine == RTM_ENGINE_FD8 && c->model_type == RTM_ISO);
   if (first_deriv) {
     if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
@@ -1046,6 +1107,11 @@ int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float
       return RTM_ERR_NONFINITE;
     }
   const size_t bytes = (size_t)h->n * 4;
+  {
+    float vmx = 0.f;
+    for (long long i = 0; i < h->n; i++) vmx = std::max(vmx, vel[i]);
+    h->vel2max = (vmx * h->d.dt) * (vmx * h->d.dt);
+  }
   CK(cudaMemcpyAsync(h->vel, vel, bytes, cudaMemcpyHostToDevice, h->st));
   if (mt >= RTM_VTI) {
     CK(cudaMemcpyAsync(h->eps, eps, bytes, cudaMemcpyHostToDevice, h->st));
@@ -1073,6 +1139,10 @@ int rtm_reset(rtm_handle *h) {
 
 int rtm_kernel(rtm_handle *h) {
   TRY(rtm::ready(h));
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   TRY(rtm::step_kernel(h, 0, rtm::io_none()));
   CK(cudaStreamSynchronize(h->st));
   return rtm::check_flag(h);
@@ -1080,6 +1150,10 @@ int rtm_kernel(rtm_handle *h) {
 
 int rtm_update2nd(rtm_handle *h) {
   TRY(rtm::ready(h));
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   rtm::QDev q = rtm::q_dev(h);
   rtm::launch_update2nd(h->w0, h->w1, h->c.use_q ? &q : nullptr, h->n, h->st);
   TRY(rtm::check_launch(h, "update2nd"));
@@ -1089,6 +1163,10 @@ int rtm_update2nd(rtm_handle *h) {
 
 int rtm_swap(rtm_handle *h) {
   if (!h) return RTM_ERR_ARG;
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   rtm::do_swap(h);
   return RTM_OK;
 }
@@ -1106,6 +1184,16 @@ int rtm_set_injection(rtm_handle *h, int ntr, int lx, int ly, int lz, const int 
                                    lz < 1)))
     return RTM_ERR_ARG;
   cudaSetDevice(h->device);
+  if (ntr > 0) {  // the largest value one injection can add: floor of the FP16 state's scales
+    float tm = 0.f, km[3] = {0.f, 0.f, 0.f};
+    for (long long i = 0; i < (long long)ntr * nt; i++) tm = std::max(tm, std::fabs(traces[i]));
+    const float *kk[3] = {kx, ky, kz};
+    const int ll[3] = {lx, ly, lz};
+    for (int a = 0; a < 3; a++)
+      for (long long i = 0; i < (long long)ntr * ll[a]; i++) km[a] = std::max(km[a], std::fabs(kk[a][i]));
+    const float amp = tm * std::fabs(scaler) * km[0] * km[1] * km[2] * (h->vel2max > 0.f ? h->vel2max : 1.f);
+    if (amp > 0.f && std::isfinite(amp)) h->f16_floor = amp;
+  }
   return rtm::upload_traces(h, h->inj, ntr, lx, ly, lz, off3, len3, kx, ky, kz, traces, nt, scaler, false);
 }
 
@@ -1120,6 +1208,10 @@ int rtm_set_extraction(rtm_handle *h, int ntr, int lx, int ly, int lz, const int
 
 int rtm_inject(rtm_handle *h, int it) {
   TRY(rtm::ready(h));
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   TRY(rtm::do_inject(h, it));
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
@@ -1127,6 +1219,10 @@ int rtm_inject(rtm_handle *h, int it) {
 
 int rtm_extract(rtm_handle *h, int jt) {
   TRY(rtm::ready(h));
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   TRY(rtm::do_extract(h, jt));
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
@@ -1180,6 +1276,10 @@ int rtm_set_compressor(rtm_handle *h, rtm_ae *a) {
 
 int rtm_snapshot_store(rtm_handle *h, int slot) {
   TRY(rtm::ready(h));
+  if (h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   if (slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
   if (h->snap_fmt == RTM_SNAP_AE) {
     TRY(rtm::ae_store(h, slot, h->w0));
@@ -1235,6 +1335,10 @@ int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
 }
 
 int rtm_image_accumulate(rtm_handle *h, int slot) {
+  if (h && h->f16) {
+    h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
+    return RTM_ERR_UNSUPPORTED;
+  }
   TRY(rtm::ready(h));
   if (slot < 0 || slot >= h->nslots || !h->image) return RTM_ERR_ARG;
   if (!h->stored[slot]) return RTM_OK;
@@ -1279,7 +1383,7 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
       if (slot >= 0 && slot < h->nslots) {
         if (dir == RTM_FORWARD) {
           if (h->snap_fmt == RTM_SNAP_AE) {
-            TRY(rtm::ae_store(h, slot, h->w0));
+            TRY(rtm::ae_store(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
           } else {
             TRY(rtm::snap_prepare(h, slot));
             pending = rtm::io_store(h, slot);
@@ -1301,7 +1405,7 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
   if (rc != RTM_OK) return rc;
   if (pending.store || pending.ic) {  // the last step's snapshot / image term
     rtm::KScope k(h, RTM_K_IO);
-    rtm::launch_fused_io(pending, h->w1, h->d.nx, h->d.ny, h->d.nz, h->st);
+    rtm::launch_fused_io(pending, h->f16 ? rtm::f16_view(h, 1) : h->w1, h->d.nx, h->d.ny, h->d.nz, h->st);
     TRY(rtm::check_launch(h, "fused_io(last)"));
     CK(cudaStreamSynchronize(h->st));
   }
@@ -1311,8 +1415,8 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
 int rtm_get(rtm_handle *h, int field, float *dst) {
   if (!h || !dst) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
-  const float *src = field == RTM_FIELD_W0 ? h->w0
-                     : field == RTM_FIELD_W1 ? h->w1
+  const float *src = field == RTM_FIELD_W0 ? (h->f16 ? rtm::f16_view(h, 0) : h->w0)
+                     : field == RTM_FIELD_W1 ? (h->f16 ? rtm::f16_view(h, 1) : h->w1)
                      : field == RTM_FIELD_VEL ? h->vel
                      : field == RTM_FIELD_IMAGE ? h->image
                      : field == RTM_FIELD_INVQ ? h->invq : nullptr;
@@ -1325,7 +1429,10 @@ int rtm_get(rtm_handle *h, int field, float *dst) {
 int rtm_check_finite(rtm_handle *h, int field, int *nonfinite) {
   if (!h || !nonfinite) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
-  const float *src = field == RTM_FIELD_W0 ? h->w0 : field == RTM_FIELD_W1 ? h->w1 : field == RTM_FIELD_IMAGE ? h->image : nullptr;
+  const float *src = field == RTM_FIELD_W0   ? (h->f16 ? rtm::f16_view(h, 0) : h->w0)
+                     : field == RTM_FIELD_W1 ? (h->f16 ? rtm::f16_view(h, 1) : h->w1)
+                     : field == RTM_FIELD_IMAGE ? h->image
+                                                : nullptr;
   if (!src) return RTM_ERR_ARG;
   if (!h->nfflag) TRY(h->alloc(h->nfflag, 1));
   int f = 0;
@@ -1350,7 +1457,15 @@ int rtm_selftest_bounded_wait(rtm_handle *h) {
 int rtm_put(rtm_handle *h, int field, const float *src) {
   if (!h || !src || (field != RTM_FIELD_W0 && field != RTM_FIELD_W1)) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
-  CK(cudaMemcpyAsync(field == RTM_FIELD_W0 ? h->w0 : h->w1, src, 4 * (size_t)h->n, cudaMemcpyHostToDevice, h->st));
+  if (h->f16) {  // through the px scratch: slab max, scale, FP16 codes
+    CK(cudaMemcpyAsync(h->px, src, 4 * (size_t)h->n, cudaMemcpyHostToDevice, h->st));
+    const bool w0 = field == RTM_FIELD_W0;
+    rtm::launch_f32_to_f16(h->px, w0 ? h->h0 : h->h1, w0 ? h->s0 : h->s1, w0 ? h->m0 : h->m1, h->d.ny, h->nxz,
+                           h->f16_floor, h->st);
+    TRY(rtm::check_launch(h, "f32_to_f16"));
+  } else {
+    CK(cudaMemcpyAsync(field == RTM_FIELD_W0 ? h->w0 : h->w1, src, 4 * (size_t)h->n, cudaMemcpyHostToDevice, h->st));
+  }
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
 }
