@@ -167,6 +167,7 @@ def run_cuda(args, rank, world):
     shot = build_workload(args.workload, 2 * K + Wm + 8, args.scale)
     s = shot.spec
     s.state_fp16 = bool(args.state_fp16)
+    s.kernel_variant = args.kernel_variant
     snap_fmt = SNAP_C16
     k1, k2 = W.spread_band(s)
     src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
@@ -253,6 +254,7 @@ def run_cuda(args, rank, world):
     p.close()
     cfg = config_of(shot, snap_fmt, K)
     cfg["autotuned_shape"] = tuned
+    cfg["kernel_variant"] = args.kernel_variant
     cfg["state"] = "fp16 per-slab scale" if s.state_fp16 else "fp32"
     return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
                 config=cfg, shot=shot, launches=launches)
@@ -403,6 +405,8 @@ def main():
                          "smaller values are for profiler captures)")
     ap.add_argument("--state-fp16", action="store_true",
                     help="FP16 wavefield state with per-slab scales (FD8 VTI / TTI workloads)")
+    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

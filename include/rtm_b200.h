@@ -93,9 +93,13 @@ typedef struct rtm_config {
   int state_fp16;     /* 0: FP32 wavefield state (default); 1: FP16 w0 / w1 with a per-y-slab scale
                          (stencils, PML, Q memory and image in FP32), FD8 VTI / TTI (+Q) only, loop
                          drivers only (the stepwise seam calls return RTM_ERR_UNSUPPORTED) */
-  int kernel_variant; /* 0: auto (ISO FD8: TMA plane pipeline when nz % 4 == 0; compact FD: register-
-                         streamed x / y line solves, the autotuner may pick TMA tiles), 1: register
-                         pipeline / plain staged tiles, 2: compact-FD x / y TMA tiles */
+  int kernel_variant; /* 0: auto (ISO FD8: 4 z cells per thread with TMA rings when nz % 4 == 0,
+                         the autotuner picks among all ISO kernels; compact FD: register-streamed
+                         x / y line solves, the autotuner may pick TMA tiles), 1: register
+                         pipeline / plain staged tiles, 2: compact-FD x / y TMA tiles, ISO FD8 TMA
+                         plane pipeline, 3: ISO FD8 4 z cells per thread with TMA rings, 4: ISO
+                         FD8 4 z cells per thread with register prefetch (ISO variants fall back
+                         to 1 when nz % 4 != 0) */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;

@@ -65,6 +65,11 @@ struct DivArgs {
 
 // mode: 0 = operator only (w0 -= vel*L), 1 = + leapfrog update, 2 = + Q update
 void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
+// the same step with 4 z cells per thread (float4 rows; nz % 4 == 0), tile
+// 32 (z) x tx (x) with tx in {8, 16, 32}
+void launch_iso_fd8_v4(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
+// the CTAs per SM launch_iso_fd8_v4 keeps resident (leapfrog mode)
+int iso_v4_ctas_per_sm(int tx, int pml3d);
 // one step of every active shot of a batch (ISO, leapfrog): shots[0..nactive)
 // device array, start[] their first work items (start[nactive] = total)
 void launch_iso_fd8_batch(const IsoBatchShot *shots, const int *start, int nactive, int total, int it, int pml3d,
@@ -109,6 +114,14 @@ extern const int kIsoTmaNShapes;
 bool iso_tma_init();  // shared-memory attributes (call outside any capture)
 void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
                         int *err, int mode, int pml3d, int shape, cudaStream_t st);
+// the 4-z-cells-per-thread step with TMA rings (kernels_iso4.cu): tensor maps
+// with boxes (40, tx + 8) for w1 and (32, tx) for w0 / (v dt)^2
+extern const TmaShape kIso4TmaShapes[];
+extern const int kIso4TmaNShapes;
+bool iso_tma4_init();
+int iso_tma4_ctas_per_sm(int shape, int pml3d);
+void launch_iso_fd8_tma4(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
+                         int *err, int mode, int pml3d, int shape, cudaStream_t st);
 
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {

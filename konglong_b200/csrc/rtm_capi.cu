@@ -95,6 +95,10 @@ struct Engine {
   // launch accounting and the optional per-kernel event profile
   long long launches = 0;
   int use_tma = 0;
+  // ISO FD8 with 4 z cells per thread (takes precedence over use_tma): 0 off,
+  // 1 register-prefetch kernel (tile width v4_tx), 2 TMA rings (kIso4TmaShapes[v4_shape])
+  int iso4 = 0;
+  int v4_tx = 16, v4_shape = 0, v4_yseg = 16;
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
   int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile
   int tma_shape = 1;  // index into kIsoTmaShapes
@@ -217,6 +221,31 @@ static int yseg_for(Engine *h, int tx) {
   long long want = 148LL * 2 * 8;
   int nseg = (int)std::max(1LL, std::min<long long>((want + bxz - 1) / bxz, std::max(1, ny / 16)));
   return (ny + nseg - 1) / nseg;
+}
+
+// y segment of the 4-z-cell ISO kernel at tile width tx: the count of
+// segments whose waves of resident CTAs cover the y planes in the fewest
+// plane-steps (a segment re-reads an 8-plane y halo, mostly from L2)
+static int yseg_v4(Engine *h, int tx, int ctas_per_sm) {
+  const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+  const long long bxz = (long long)((nz + 31) / 32) * ((nx + tx - 1) / tx);
+  const long long res = (long long)std::max(1, nsm) * std::max(1, ctas_per_sm);
+  int best_y = ny;
+  double best = 1e300;
+  for (int nseg = 1; nseg <= std::max(1, ny / 8); nseg++) {
+    const int yseg = (ny + nseg - 1) / nseg;
+    const long long ctas = bxz * ((ny + yseg - 1) / yseg);
+    const double cost = (double)((ctas + res - 1) / res) * (yseg + 3);
+    if (cost < best * 0.98) best = cost, best_y = yseg;
+  }
+  return best_y;
+}
+static int yseg_iso4(Engine *h) {
+  if (h->iso4 == 2)
+    return yseg_v4(h, kIso4TmaShapes[h->v4_shape].tx, iso_tma4_ctas_per_sm(h->v4_shape, h->c.pml3d));
+  return yseg_v4(h, h->v4_tx, iso_v4_ctas_per_sm(h->v4_tx, h->c.pml3d));
 }
 
 // Longest run of rows whose (lm, bu, rdiag) are bitwise identical: in the
@@ -372,6 +401,22 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     a.io = io;
     a.q = q;
     CUtensorMap m1, m0, mv;
+    if (h->iso4 == 2) {
+      const int tx = kIso4TmaShapes[h->v4_shape].tx;
+      if (!tmap(h, h->w1, 40, tx + 8, &m1) || !tmap(h, h->w0, 32, tx, &m0) || !tmap(h, h->vel, 32, tx, &mv)) {
+        h->iso4 = 1;
+        h->v4_yseg = yseg_iso4(h);
+      }
+    }
+    if (h->iso4) {
+      a.yseg = h->v4_yseg;
+      {
+        KScope k(h, RTM_K_ISO);
+        if (h->iso4 == 2) launch_iso_fd8_tma4(a, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape, h->st);
+        else launch_iso_fd8_v4(a, mode, h->c.pml3d, h->v4_tx, h->st);
+      }
+      return check_launch(h, "iso_fd8_v4");
+    }
     if (h->use_tma) {
       const int tx = kIsoTmaShapes[h->tma_shape].tx;
       if (!tmap(h, h->w1, 40, tx + 8, &m1) || !tmap(h, h->w0, 32, tx, &m0) || !tmap(h, h->vel, 32, tx, &mv))
@@ -1058,7 +1103,12 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->one_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
-  h->use_tma = c->kernel_variant != 1 && tma_supported(d->nz) && iso_tma_init();
+  h->use_tma = (c->kernel_variant == 0 || c->kernel_variant == 2) && tma_supported(d->nz) && iso_tma_init();
+  if (c->engine == RTM_ENGINE_FD8 && c->model_type == RTM_ISO && d->nz % 4 == 0 &&
+      (c->kernel_variant == 0 || c->kernel_variant == 3 || c->kernel_variant == 4)) {
+    h->iso4 = c->kernel_variant != 4 && tma_supported(d->nz) && iso_tma4_init() ? 2 : 1;
+    h->v4_yseg = yseg_iso4(h);
+  }
   h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
   h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
@@ -1608,28 +1658,54 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
   if (steps < 1) return RTM_ERR_ARG;
   // candidate launch shapes of this handle's step kernels
   struct Cand {
+    int iso4, v4, yseg;  // iso4 kind, its tile width (1) or shape (2), its y segment
     int tma_shape, tx, cfd_xy;
   };
   std::vector<Cand> cands;
   const bool iso = h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO;
+  const bool v4_ok = iso && h->d.nz % 4 == 0 &&
+                     (h->c.kernel_variant == 0 || h->c.kernel_variant == 3 || h->c.kernel_variant == 4);
+  const int iso4_0 = h->iso4, v4_tx0 = h->v4_tx, v4_shape0 = h->v4_shape;
+  // kind 1: tile width v, kind 2: TMA shape v; the modelled y segment and 32 planes
+  auto add_iso4 = [&](int kind, int v) {
+    h->iso4 = kind;
+    if (kind == 1) h->v4_tx = v;
+    else h->v4_shape = v;
+    const int ym = rtm::yseg_iso4(h);
+    cands.push_back({kind, v, ym, h->tma_shape, h->tx, h->cfd_xy});
+    if (ym != 32 && h->d.ny > 32) cands.push_back({kind, v, 32, h->tma_shape, h->tx, h->cfd_xy});
+  };
+  if (v4_ok) {
+    for (int tx : {8, 16, 32}) add_iso4(1, tx);
+    if (iso4_0 == 2)
+      for (int k = 0; k < rtm::kIso4TmaNShapes; k++) add_iso4(2, k);
+    h->iso4 = iso4_0, h->v4_tx = v4_tx0, h->v4_shape = v4_shape0;
+  }
   if (iso && h->use_tma)
-    for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({k, h->tx, h->cfd_xy});
-  else if (h->c.engine == RTM_ENGINE_FD8)
-    for (int tx : {4, 8, 16}) cands.push_back({h->tma_shape, tx, h->cfd_xy});
-  else if (h->c.kernel_variant == 0) {
-    cands.push_back({h->tma_shape, h->tx, 0});
-    if (h->cfd_tma) cands.push_back({h->tma_shape, h->tx, 1});
+    for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({0, 0, 0, k, h->tx, h->cfd_xy});
+  else if (h->c.engine == RTM_ENGINE_FD8 && !v4_ok)
+    for (int tx : {4, 8, 16}) cands.push_back({0, 0, 0, h->tma_shape, tx, h->cfd_xy});
+  else if (h->c.engine == RTM_ENGINE_CFD && h->c.kernel_variant == 0) {
+    cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
+    if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
   }
   if (cands.empty()) {
     if (choice) *choice = 0;
     return RTM_OK;
   }
   const int yseg0 = h->yseg;
+  auto apply = [&](const Cand &c) {
+    h->iso4 = c.iso4;
+    if (c.iso4 == 1) h->v4_tx = c.v4;
+    if (c.iso4 == 2) h->v4_shape = c.v4;
+    if (c.iso4) h->v4_yseg = c.yseg;
+    h->tma_shape = c.tma_shape, h->tx = c.tx, h->cfd_xy = c.cfd_xy;
+    h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
+  };
   float best = 1e30f;
   int bi = 0;
   for (size_t c = 0; c < cands.size(); c++) {
-    h->tma_shape = cands[c].tma_shape, h->tx = cands[c].tx, h->yseg = rtm::yseg_for(h, cands[c].tx);
-    h->cfd_xy = cands[c].cfd_xy;
+    apply(cands[c]);
     TRY(rtm::step_kernel(h, 1, rtm::io_none()));  // warm-up (tensor maps, first launch)
     CK(cudaEventRecord(h->ev0, h->st));
     for (int s = 0; s < steps; s++) TRY(rtm::step_kernel(h, 1, rtm::io_none()));
@@ -1639,8 +1715,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (ms < best) best = ms, bi = (int)c;
   }
-  h->tma_shape = cands[bi].tma_shape, h->tx = cands[bi].tx, h->cfd_xy = cands[bi].cfd_xy;
-  h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
+  apply(cands[bi]);
   if (choice) *choice = bi;
   TRY(rtm::check_flag(h));
   TRY(rtm::zero_state(h));

@@ -51,6 +51,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return false;
 }
 
+// Bounded wait used on an error path before a CTA exits: polls the phase of
+// `parity` up to 2^16 times whatever *err says (its own copies must land
+// before the shared memory is released).
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 16); it++)
+    if (mbar_try_wait(bar, parity)) return;
+}
+
 // 3-D tiled load (coordinates innermost first: z, x, y) completing on `bar`.
 // The proxy fence orders earlier generic writes of this stage before the copy.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int cz, int cx, int cy) {

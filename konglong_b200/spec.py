@@ -38,7 +38,9 @@ class PropSpec:
     pml3d_scaler: float = 0.3
     top_pml: bool = True
     state_fp16: bool = False
-    kernel_variant: int = 0       # 0 auto, 1 register pipeline / plain tiles, 2 CFD x/y TMA tiles
+    kernel_variant: int = 0       # 0 auto, 1 register pipeline / plain tiles, 2 TMA (CFD x/y tiles,
+                                  # ISO plane pipeline), 3 / 4 ISO 4 z cells per thread (TMA rings /
+                                  # register prefetch)
 
     @property
     def n(self):
