@@ -179,7 +179,7 @@ def run_cuda(args, rank, world):
     nslots = (2 * K + Wm) // shot.interval + 2
     p.snapshot_setup(snap_fmt, nslots)
     p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
-    tuned = p.autotune(3)
+    tuned = p.autotune(3) if not args.no_autotune else None
     p.reset()
     ranks = R.Ranks.from_env()
     # warm-up steps (untimed), then K timed steps continuing the same shot
@@ -407,6 +407,8 @@ def main():
                     help="FP16 wavefield state with per-slab scales (FD8 VTI / TTI workloads)")
     ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (profiler runs: timings under a profiler mislead the tuner)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

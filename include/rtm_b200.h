@@ -303,11 +303,20 @@ int rtm_check_finite(rtm_handle *h, int field, int *nonfinite);
  * counterpart. */
 int rtm_selftest_bounded_wait(rtm_handle *h);
 /* Autotuner: times `steps` fused steps of every launch shape this handle's
- * kernels offer (TMA tile width / prefetch depth for ISO FD8, tile width of
- * the FD8 gradient / divergence passes, register-streamed or TMA-tiled x / y
- * line solves for compact FD), keeps the fastest, returns its index in
- * *choice, then zeroes the wavefields and PML memory (as rtm_reset). */
+ * kernels offer (ISO FD8: 4-z-cell kernels with TMA rings or register
+ * prefetch at several tile widths, prefetch depths and y segments, and the
+ * one-cell TMA plane pipeline; tile width of the FD8 gradient / divergence
+ * passes; register-streamed or TMA-tiled x / y line solves for compact FD),
+ * keeps the fastest, returns its index in *choice, then zeroes the wavefields
+ * and PML memory (as rtm_reset). */
 int rtm_autotune(rtm_handle *h, int steps, int *choice);
+/* Candidate `idx` of the last rtm_autotune: desc[0] kernel family (0 one cell
+ * per thread / FD8 two-pass / compact FD, 1 ISO 4 z cells with register
+ * prefetch, 2 ISO 4 z cells with TMA rings, 3 ISO one-cell TMA pipeline),
+ * desc[1] its tile width or shape index, desc[2] its y segment (0: default),
+ * desc[3] the compact-FD x / y kernel; *ms the time of its `steps` steps.
+ * RTM_ERR_ARG when idx is out of range. */
+int rtm_autotune_result(rtm_handle *h, int idx, int desc[4], float *ms);
 
 /* Kernels launched by the last rtm_modelling / rtm_migration call. */
 int rtm_last_loop_launches(rtm_handle *h, long long *n);

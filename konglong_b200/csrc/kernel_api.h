@@ -115,13 +115,19 @@ bool iso_tma_init();  // shared-memory attributes (call outside any capture)
 void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
                         int *err, int mode, int pml3d, int shape, cudaStream_t st);
 // the 4-z-cells-per-thread step with TMA rings (kernels_iso4.cu): tensor maps
-// with boxes (40, tx + 8) for w1 and (32, tx) for w0 / (v dt)^2
+// with boxes (40, tx + 8) for w1 and (32, tx) for w0 / (v dt)^2.  One CTA per
+// entry of a tile table (device array); `edge` tiles may hold PML cells, the
+// others run a kernel compiled without the PML code.
+struct Tile4 {
+  int bz, bx, y0, y1;  // z tile (32 cells), x tile (tx cells), planes [y0, y1)
+};
 extern const TmaShape kIso4TmaShapes[];
 extern const int kIso4TmaNShapes;
 bool iso_tma4_init();
 int iso_tma4_ctas_per_sm(int shape, int pml3d);
-void launch_iso_fd8_tma4(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
-                         int *err, int mode, int pml3d, int shape, cudaStream_t st);
+void launch_iso_fd8_tma4(const IsoArgs &a, const Tile4 *tiles, int ntiles, bool edge, const CUtensorMap &w1,
+                         const CUtensorMap &w0, const CUtensorMap &vel, int *err, int mode, int pml3d, int shape,
+                         cudaStream_t st);
 
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {

@@ -444,8 +444,9 @@ __device__ __forceinline__ void iso4_prefetch(const IsoArgs &a, const Grid3 &g, 
   }
 }
 
-template <int TX, int P, int MODE, bool PML3D>
+template <int TX, int P, int MODE, bool PML3D, bool EDGE>
 __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ IsoArgs a,
+                                                       const Tile4 *__restrict__ tiles,
                                                        const __grid_constant__ CUtensorMap map_w1,
                                                        const __grid_constant__ CUtensorMap map_w0,
                                                        const __grid_constant__ CUtensorMap map_vel, int *err) {
@@ -457,19 +458,71 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const Grid3 g{nx, ny, nz, (long long)nx * nz};
   const int tzq = threadIdx.x, tx = threadIdx.y;
-  const int iz0 = blockIdx.x * 32, ix0 = blockIdx.y * TX;
+  const Tile4 tile = tiles[blockIdx.x];
+  const int iz0 = tile.bz * 32, ix0 = tile.bx * TX;
   const int iz4 = iz0 + 4 * tzq, ix = ix0 + tx;
-  const int y0 = blockIdx.z * a.yseg, y1 = min(ny, y0 + a.yseg);
+  const int y0 = tile.y0, y1 = tile.y1;
   const bool act = iz4 < nz && ix < nx;
   const bool producer = tzq == 0 && tx == 0;
   const long long col = (long long)ix * nz + iz4;
   const bool do_y = ny > 2;
   const int zl = a.pml.f[DZ][0].w, zh = a.pml.f[DZ][1].w, xl = a.pml.f[DX][0].w, xh = a.pml.f[DX][1].w,
             yl = a.pml.f[DY][0].w, yh = a.pml.f[DY][1].w;
-  const bool x_edge = ix < xl || ix >= nx - xh;
-  const bool z_edge = iz4 < zl || iz4 + 3 >= nz - zh;
+  // interior tiles hold no PML cell (the tile table guarantees it)
+  const bool x_edge = EDGE && (ix < xl || ix >= nx - xh);
+  const bool z_edge = EDGE && (iz4 < zl || iz4 + 3 >= nz - zh);
   const bool z4ok = zl % 4 == 0 && zh % 4 == 0;
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto y_edge_at = [&](int y) { return EDGE && (y < yl || y >= ny - yh); };
+  // PML tiles with z faces a multiple of 4 cells wide: the x and z faces of
+  // the thread's 4 cells are fixed over the tile's planes; their round-0 /
+  // round-1 memory (one float4 per array, z fastest) advances by a constant
+  // stride per plane and their recursion constants stay in registers
+  const bool vpml = EDGE && z4ok;
+  float *qx1 = nullptr, *qx2 = nullptr, *qz1 = nullptr, *qz2 = nullptr;
+  long long stx = 0, stz = 0;
+  float cx[3] = {0.f, 0.f, 0.f}, cz[4][3] = {};
+  if (vpml && act && x_edge) {
+    const int sd = ix < xl ? 0 : 1;
+    const PmlFace &F = a.pml.f[DX][sd];
+    const int w = F.w, L = sd ? nx - 1 - ix : ix;
+    const long long idx = ((long long)y0 * w + (sd ? ix - (nx - w) : ix)) * nz + iz4;
+    qx1 = F.q[0][0] + idx, qx2 = F.q[1][0] + idx, stx = (long long)w * nz;
+#pragma unroll
+    for (int k = 0; k < 3; k++) cx[k] = F.co[L * 6 + k];
+  }
+  if (vpml && act && z_edge) {
+    const int sd = iz4 < zl ? 0 : 1;
+    const PmlFace &F = a.pml.f[DZ][sd];
+    const int w = F.w;
+    const long long idx = ((long long)y0 * nx + ix) * w + (sd ? iz4 - (nz - w) : iz4);
+    qz1 = F.q[0][0] + idx, qz2 = F.q[1][0] + idx, stz = (long long)nx * w;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int L = sd ? nz - 1 - (iz4 + c) : iz4 + c;
+#pragma unroll
+      for (int k = 0; k < 3; k++) cz[c][k] = F.co[L * 6 + k];
+    }
+  }
+  // the y face of plane y (memory of the thread's cells, recursion constants)
+  auto yface = [&](int y, float *&q1, float *&q2, const float *&co) {
+    const int sd = y < yl ? 0 : 1;
+    const PmlFace &F = a.pml.f[DY][sd];
+    const long long idx = ((long long)(sd ? y - (ny - F.w) : y) * nx + ix) * nz + iz4;
+    q1 = F.q[0][0] + idx, q2 = F.q[1][0] + idx, co = F.co + (sd ? ny - 1 - y : y) * 6;
+  };
+  // L1 prefetch of the face memory of plane y, k planes beyond the one the
+  // x / z pointers are at
+  auto pml_prefetch = [&](int y, int k) {
+    if (qx1) prefetch_l1(qx1 + k * stx), prefetch_l1(qx2 + k * stx);
+    if (qz1) prefetch_l1(qz1 + k * stz), prefetch_l1(qz2 + k * stz);
+    if ((PML3D || do_y) && y_edge_at(y)) {
+      float *q1, *q2;
+      const float *co;
+      yface(y, q1, q2, co);
+      prefetch_l1(q1), prefetch_l1(q2);
+    }
+  };
 
   // plane p (y0 <= p) lives in stage (p - y0) % S of its ring, phase ((p - y0) / S) & 1
   auto issue_a = [&](int p) {
@@ -508,10 +561,11 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
     const int y = y0 - R4 + k;
     q[k] = act && y >= 0 && y < ny ? __ldg(w1g + y * nxz4 + col4) : zero4;
   }
-  if (act) {
-    if (y0 < y1) iso4_prefetch<MODE>(a, g, x_edge || z_edge || y0 < yl || y0 >= ny - yh, ix, y0, iz4, col);
-    if (y0 + 1 < y1) iso4_prefetch<MODE>(a, g, x_edge || z_edge || y0 + 1 < yl || y0 + 1 >= ny - yh, ix, y0 + 1, iz4, col);
-  }
+  if (act)
+    for (int y = y0; y < min(y0 + 2, y1); y++) {
+      iso4_prefetch<MODE>(a, g, !vpml && (x_edge || z_edge || y_edge_at(y)), ix, y, iz4, col);
+      if (vpml) pml_prefetch(y, y - y0);
+    }
   bool ok = true;
 #pragma unroll 1
   for (int iy = y0; iy < y1; iy++) {
@@ -519,8 +573,10 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
       if (iy + R4 + P < y1 + R4) issue_a(iy + R4 + P), last_a = iy + R4 + P;
       if (iy + P < y1) issue_b(iy + P), last_b = iy + P;
     }
-    if (act && iy + 2 < y1)
-      iso4_prefetch<MODE>(a, g, x_edge || z_edge || iy + 2 < yl || iy + 2 >= ny - yh, ix, iy + 2, iz4, col);
+    if (act && iy + 2 < y1) {
+      iso4_prefetch<MODE>(a, g, !vpml && (x_edge || z_edge || y_edge_at(iy + 2)), ix, iy + 2, iz4, col);
+      if (vpml) pml_prefetch(iy + 2, 2);
+    }
     const int r0 = iy - y0, sa0 = r0 % SA, sa4 = (r0 + R4) % SA, sb = r0 % SB;
     if (r0 < R4) ok = ok && mbar_wait(&s.bar_a[sa0], (uint32_t)((r0 / SA) & 1), err);
     ok = ok && mbar_wait(&s.bar_a[sa4], (uint32_t)(((r0 + R4) / SA) & 1), err);
@@ -553,14 +609,44 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
         lyv[c] = ly;
       }
       float v[4];
-      const bool y_edge = iy < yl || iy >= ny - yh;
-      if (x_edge || y_edge || z_edge) {
-        if (z4ok) {
-          const float4 r = iso4_pml4<PML3D>(a.pml, g, make_float4(lzv[0], lzv[1], lzv[2], lzv[3]),
-                                            make_float4(lxv[0], lxv[1], lxv[2], lxv[3]),
-                                            make_float4(lyv[0], lyv[1], lyv[2], lyv[3]), do_y, ix, iy, iz4);
-          v[0] = r.x, v[1] = r.y, v[2] = r.z, v[3] = r.w;
-        } else {
+      const bool y_edge = y_edge_at(iy);
+      const bool yf = (PML3D || do_y) && y_edge;
+      if (vpml && (qx1 || qz1 || yf)) {
+        // pml2_dim's rounds per cell in the order z, x, y; all loads first
+        float *qy1 = nullptr, *qy2 = nullptr;
+        const float *cyp = nullptr;
+        if (yf) yface(iy, qy1, qy2, cyp);
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 z1 = qz1 ? *reinterpret_cast<const float4 *>(qz1) : z4, z2 = qz1 ? *reinterpret_cast<const float4 *>(qz2) : z4;
+        float4 x1 = qx1 ? *reinterpret_cast<const float4 *>(qx1) : z4, x2 = qx1 ? *reinterpret_cast<const float4 *>(qx2) : z4;
+        float4 y1 = yf ? *reinterpret_cast<const float4 *>(qy1) : z4, y2 = yf ? *reinterpret_cast<const float4 *>(qy2) : z4;
+        float cy[3] = {0.f, 0.f, 0.f};
+        if (yf) cy[0] = cyp[0], cy[1] = cyp[1], cy[2] = cyp[2];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          float pz = PML3D ? lzv[c] + lxv[c] + lyv[c] : lzv[c], px = lxv[c], py = lyv[c];
+          float m;
+          if (qz1) {
+            m = comp(z1, c), pml_round(cz[c], pz, &m), setc(z1, c, m);
+            m = comp(z2, c), pml_round(cz[c], pz, &m), setc(z2, c, m);
+          }
+          float &pxr = PML3D ? pz : px;
+          if (qx1) {
+            m = comp(x1, c), pml_round(cx, pxr, &m), setc(x1, c, m);
+            m = comp(x2, c), pml_round(cx, pxr, &m), setc(x2, c, m);
+          }
+          float &pyr = PML3D ? pz : py;
+          if (yf) {
+            m = comp(y1, c), pml_round(cy, pyr, &m), setc(y1, c, m);
+            m = comp(y2, c), pml_round(cy, pyr, &m), setc(y2, c, m);
+          }
+          v[c] = PML3D ? pz : pz + px + py;
+        }
+        if (qz1) *reinterpret_cast<float4 *>(qz1) = z1, *reinterpret_cast<float4 *>(qz2) = z2;
+        if (qx1) *reinterpret_cast<float4 *>(qx1) = x1, *reinterpret_cast<float4 *>(qx2) = x2;
+        if (yf) *reinterpret_cast<float4 *>(qy1) = y1, *reinterpret_cast<float4 *>(qy2) = y2;
+      } else if (EDGE && !z4ok && (x_edge || y_edge || z_edge)) {
+        {
 #pragma unroll
           for (int c = 0; c < 4; c++) {
             const int iz = iz4 + c;
@@ -585,6 +671,8 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
       else out4 = iso4_q4(a.q, i0, (long long)ny * g.nxz, t4, u4);
       reinterpret_cast<float4 *>(a.w0)[i0 / 4] = out4;
     }
+    if (qx1) qx1 += stx, qx2 += stx;
+    if (qz1) qz1 += stz, qz2 += stz;
     __syncthreads();  // every thread is done with the stages the producer refills next
 #pragma unroll
     for (int k = 0; k < 2 * R4; k++) q[k] = q[k + 1];
@@ -598,12 +686,11 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
   }
 }
 
-template <int TX, int P>
-void tma4_shape(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel, int *err,
-                int mode, int pml3d, cudaStream_t st) {
-  const dim3 grid((a.nz + 31) / 32, (a.nx + TX - 1) / TX, (a.ny + a.yseg - 1) / a.yseg), block(8, TX);
+template <int TX, int P, bool EDGE>
+void tma4_launch(const IsoArgs &a, const Tile4 *tiles, int ntiles, const CUtensorMap &w1, const CUtensorMap &w0,
+                 const CUtensorMap &vel, int *err, int mode, int pml3d, cudaStream_t st) {
   const size_t smem = sizeof(Iso4Smem<TX, P>);
-#define L_(M, P3) iso_fd8_tma4<TX, P, M, P3><<<grid, block, smem, st>>>(a, w1, w0, vel, err)
+#define L_(M, P3) iso_fd8_tma4<TX, P, M, P3, EDGE><<<ntiles, dim3(8, TX), smem, st>>>(a, tiles, w1, w0, vel, err)
   if (pml3d) {
     if (mode == 0) L_(0, true);
     else if (mode == 1) L_(1, true);
@@ -617,11 +704,18 @@ void tma4_shape(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, 
 }
 
 template <int TX, int P>
-bool tma4_attr() {
-  const int smem = (int)sizeof(Iso4Smem<TX, P>);
+void tma4_shape(const IsoArgs &a, const Tile4 *tiles, int ntiles, bool edge, const CUtensorMap &w1,
+                const CUtensorMap &w0, const CUtensorMap &vel, int *err, int mode, int pml3d, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  if (edge) tma4_launch<TX, P, true>(a, tiles, ntiles, w1, w0, vel, err, mode, pml3d, st);
+  else tma4_launch<TX, P, false>(a, tiles, ntiles, w1, w0, vel, err, mode, pml3d, st);
+}
+
+template <int TX, int P, bool EDGE>
+bool tma4_attr_e(int smem) {
   bool ok = true;
 #define A_(M, P3) \
-  ok &= cudaFuncSetAttribute(iso_fd8_tma4<TX, P, M, P3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0
+  ok &= cudaFuncSetAttribute(iso_fd8_tma4<TX, P, M, P3, EDGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == 0
   A_(0, true);
   A_(1, true);
   A_(2, true);
@@ -633,11 +727,18 @@ bool tma4_attr() {
 }
 
 template <int TX, int P>
+bool tma4_attr() {
+  const int smem = (int)sizeof(Iso4Smem<TX, P>);
+  return tma4_attr_e<TX, P, true>(smem) && tma4_attr_e<TX, P, false>(smem);
+}
+
+// resident CTAs per SM of the interior (PML-free) kernel, leapfrog mode
+template <int TX, int P>
 int tma4_occupancy(int pml3d) {
   int n = 0;
   const size_t smem = sizeof(Iso4Smem<TX, P>);
-  if (pml3d) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_tma4<TX, P, 1, true>, 8 * TX, smem);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_tma4<TX, P, 1, false>, 8 * TX, smem);
+  if (pml3d) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_tma4<TX, P, 1, true, false>, 8 * TX, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_tma4<TX, P, 1, false, false>, 8 * TX, smem);
   return n;
 }
 
@@ -682,11 +783,12 @@ int iso_tma4_ctas_per_sm(int shape, int pml3d) {
   return n > 0 ? n : 1;
 }
 
-void launch_iso_fd8_tma4(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
-                         int *err, int mode, int pml3d, int shape, cudaStream_t st) {
-  if (shape == 0) tma4_shape<16, 2>(a, w1, w0, vel, err, mode, pml3d, st);
-  else if (shape == 1) tma4_shape<16, 4>(a, w1, w0, vel, err, mode, pml3d, st);
-  else tma4_shape<32, 2>(a, w1, w0, vel, err, mode, pml3d, st);
+void launch_iso_fd8_tma4(const IsoArgs &a, const Tile4 *tiles, int ntiles, bool edge, const CUtensorMap &w1,
+                         const CUtensorMap &w0, const CUtensorMap &vel, int *err, int mode, int pml3d, int shape,
+                         cudaStream_t st) {
+  if (shape == 0) tma4_shape<16, 2>(a, tiles, ntiles, edge, w1, w0, vel, err, mode, pml3d, st);
+  else if (shape == 1) tma4_shape<16, 4>(a, tiles, ntiles, edge, w1, w0, vel, err, mode, pml3d, st);
+  else tma4_shape<32, 2>(a, tiles, ntiles, edge, w1, w0, vel, err, mode, pml3d, st);
 }
 
 }  // namespace rtm

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <array>
 #include <vector>
 
 #include <cuda.h>
@@ -99,6 +100,11 @@ struct Engine {
   // 1 register-prefetch kernel (tile width v4_tx), 2 TMA rings (kIso4TmaShapes[v4_shape])
   int iso4 = 0;
   int v4_tx = 16, v4_shape = 0, v4_yseg = 16;
+  // tile table of the TMA-ring kernel: interior tiles [0, n_int), then PML tiles
+  Tile4 *tiles = nullptr;
+  int tiles_cap = 0, n_int = 0, n_edge = 0, tiles_tx = 0, tiles_yseg = 0;
+  std::vector<std::array<int, 4>> tune_desc;  // candidates of the last rtm_autotune and their times
+  std::vector<float> tune_ms;
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
   int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile
   int tma_shape = 1;  // index into kIsoTmaShapes
@@ -242,6 +248,53 @@ static int yseg_v4(Engine *h, int tx, int ctas_per_sm) {
   }
   return best_y;
 }
+// Tile table of the TMA-ring ISO kernel for its current (tile width, y
+// segment): columns touching an x or z PML face are PML tiles over all y; the
+// others are PML tiles over the y faces and interior tiles between.  Built on
+// the host and uploaded (never inside a stream capture).
+static int iso4_tiles(Engine *h) {
+  const int tx = kIso4TmaShapes[h->v4_shape].tx, yseg = std::max(1, h->v4_yseg);
+  if (h->tiles && h->tiles_tx == tx && h->tiles_yseg == yseg) return RTM_OK;
+  const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
+  const int zl = h->pml.f[DZ][0].w, zh = h->pml.f[DZ][1].w, xl = h->pml.f[DX][0].w, xh = h->pml.f[DX][1].w,
+            yl = h->pml.f[DY][0].w, yh = h->pml.f[DY][1].w;
+  std::vector<Tile4> in, ed;
+  auto segs = [&](std::vector<Tile4> &v, int bz, int bx, int a, int b) {
+    for (int y = a; y < b; y += yseg) v.push_back({bz, bx, y, std::min(b, y + yseg)});
+  };
+  const int nbz = (nz + 31) / 32, nbx = (nx + tx - 1) / tx;
+  for (int bx = 0; bx < nbx; bx++)
+    for (int bz = 0; bz < nbz; bz++) {
+      const bool exz = bx * tx < xl || std::min(nx, (bx + 1) * tx) > nx - xh || bz * 32 < zl ||
+                       std::min(nz, bz * 32 + 32) > nz - zh;
+      if (exz) {
+        segs(ed, bz, bx, 0, ny);
+      } else {
+        segs(ed, bz, bx, 0, yl);
+        segs(in, bz, bx, yl, ny - yh);
+        segs(ed, bz, bx, ny - yh, ny);
+      }
+    }
+  // launch order: y segment slowest, then x, then z (neighbouring CTAs share halos)
+  auto by_y = [](const Tile4 &a, const Tile4 &b) {
+    return a.y0 != b.y0 ? a.y0 < b.y0 : a.bx != b.bx ? a.bx < b.bx : a.bz < b.bz;
+  };
+  std::stable_sort(in.begin(), in.end(), by_y);
+  std::stable_sort(ed.begin(), ed.end(), by_y);
+  const int n = (int)(in.size() + ed.size());
+  if (n > h->tiles_cap) {
+    h->release(h->tiles);
+    h->tiles = nullptr, h->tiles_cap = 0;
+    TRY(h->alloc(h->tiles, (size_t)n));
+    h->tiles_cap = n;
+  }
+  std::vector<Tile4> all(in);
+  all.insert(all.end(), ed.begin(), ed.end());
+  CK(cudaMemcpy(h->tiles, all.data(), sizeof(Tile4) * n, cudaMemcpyHostToDevice));
+  h->n_int = (int)in.size(), h->n_edge = (int)ed.size(), h->tiles_tx = tx, h->tiles_yseg = yseg;
+  return RTM_OK;
+}
+
 static int yseg_iso4(Engine *h) {
   if (h->iso4 == 2)
     return yseg_v4(h, kIso4TmaShapes[h->v4_shape].tx, iso_tma4_ctas_per_sm(h->v4_shape, h->c.pml3d));
@@ -403,6 +456,10 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     CUtensorMap m1, m0, mv;
     if (h->iso4 == 2) {
       const int tx = kIso4TmaShapes[h->v4_shape].tx;
+      if (!h->tiles || h->tiles_tx != tx || h->tiles_yseg != std::max(1, h->v4_yseg)) {
+        h->err = "iso4 tile table is stale";
+        return RTM_ERR_STATE;
+      }
       if (!tmap(h, h->w1, 40, tx + 8, &m1) || !tmap(h, h->w0, 32, tx, &m0) || !tmap(h, h->vel, 32, tx, &mv)) {
         h->iso4 = 1;
         h->v4_yseg = yseg_iso4(h);
@@ -410,10 +467,19 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     }
     if (h->iso4) {
       a.yseg = h->v4_yseg;
+      if (h->iso4 == 2) {
+        {
+          KScope k(h, RTM_K_ISO, (h->n_int > 0) + (h->n_edge > 0));
+          launch_iso_fd8_tma4(a, h->tiles, h->n_int, false, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape,
+                              h->st);
+          launch_iso_fd8_tma4(a, h->tiles + h->n_int, h->n_edge, true, m1, m0, mv, h->dflag, mode, h->c.pml3d,
+                              h->v4_shape, h->st);
+        }
+        return check_launch(h, "iso_fd8_tma4");
+      }
       {
         KScope k(h, RTM_K_ISO);
-        if (h->iso4 == 2) launch_iso_fd8_tma4(a, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape, h->st);
-        else launch_iso_fd8_v4(a, mode, h->c.pml3d, h->v4_tx, h->st);
+        launch_iso_fd8_v4(a, mode, h->c.pml3d, h->v4_tx, h->st);
       }
       return check_launch(h, "iso_fd8_v4");
     }
@@ -1108,6 +1174,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
       (c->kernel_variant == 0 || c->kernel_variant == 3 || c->kernel_variant == 4)) {
     h->iso4 = c->kernel_variant != 4 && tma_supported(d->nz) && iso_tma4_init() ? 2 : 1;
     h->v4_yseg = yseg_iso4(h);
+    if (h->iso4 == 2 && (rc = iso4_tiles(h))) return fail(rc);
   }
   h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
   h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
@@ -1673,7 +1740,8 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     else h->v4_shape = v;
     const int ym = rtm::yseg_iso4(h);
     cands.push_back({kind, v, ym, h->tma_shape, h->tx, h->cfd_xy});
-    if (ym != 32 && h->d.ny > 32) cands.push_back({kind, v, 32, h->tma_shape, h->tx, h->cfd_xy});
+    for (int y : {32, 64})
+      if (ym != y && h->d.ny > y) cands.push_back({kind, v, y, h->tma_shape, h->tx, h->cfd_xy});
   };
   if (v4_ok) {
     for (int tx : {8, 16, 32}) add_iso4(1, tx);
@@ -1701,11 +1769,13 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     if (c.iso4) h->v4_yseg = c.yseg;
     h->tma_shape = c.tma_shape, h->tx = c.tx, h->cfd_xy = c.cfd_xy;
     h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
+    return h->iso4 == 2 ? rtm::iso4_tiles(h) : (int)RTM_OK;
   };
   float best = 1e30f;
   int bi = 0;
+  h->tune_desc.clear(), h->tune_ms.clear();
   for (size_t c = 0; c < cands.size(); c++) {
-    apply(cands[c]);
+    TRY(apply(cands[c]));
     TRY(rtm::step_kernel(h, 1, rtm::io_none()));  // warm-up (tensor maps, first launch)
     CK(cudaEventRecord(h->ev0, h->st));
     for (int s = 0; s < steps; s++) TRY(rtm::step_kernel(h, 1, rtm::io_none()));
@@ -1714,12 +1784,23 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (ms < best) best = ms, bi = (int)c;
+    const Cand &k = cands[c];
+    const int fam = k.iso4 ? k.iso4 : (iso && h->use_tma ? 3 : 0);
+    h->tune_desc.push_back({fam, k.iso4 ? k.v4 : fam == 3 ? k.tma_shape : k.tx, k.iso4 ? k.yseg : 0, k.cfd_xy});
+    h->tune_ms.push_back(ms);
   }
-  apply(cands[bi]);
+  TRY(apply(cands[bi]));
   if (choice) *choice = bi;
   TRY(rtm::check_flag(h));
   TRY(rtm::zero_state(h));
   CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_autotune_result(rtm_handle *h, int idx, int desc[4], float *ms) {
+  if (!h || !desc || !ms || idx < 0 || idx >= (int)h->tune_ms.size()) return RTM_ERR_ARG;
+  for (int k = 0; k < 4; k++) desc[k] = h->tune_desc[idx][k];
+  *ms = h->tune_ms[idx];
   return RTM_OK;
 }
 

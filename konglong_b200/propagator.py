@@ -153,6 +153,15 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def autotune_results(self):
+        """[(family, shape, yseg, cfd_xy, ms)] of the candidates the last autotune timed."""
+        out, k = [], 0
+        desc, ms = (C.c_int * 4)(), C.c_float(0)
+        while self.L.rtm_autotune_result(self.h, k, desc, C.byref(ms)) == 0:
+            out.append((*desc, ms.value))
+            k += 1
+        return out
+
     def set_compressor(self, ae):
         """Attach a compressor.AutoEncoder for RTM_SNAP_AE snapshots (None detaches)."""
         self._ck(self.L.rtm_set_compressor(self.h, ae.a if ae is not None else None), "rtm_set_compressor")

@@ -78,6 +78,7 @@ GRIDS = [
     (37, 14, 36, True, True),    # Q update, nx odd, ny below one y segment
     (50, 30, 64, False, False),  # per-axis PML rounds
     (33, 12, 42, False, True),   # nz % 4 != 0: every variant runs one cell per thread
+    (70, 30, 100, True, True),   # interior (PML-free) tiles next to PML tiles, Q update
 ]
 
 
@@ -104,7 +105,7 @@ def test_variants_bit_equal(grid):
 
 def test_autotuned_shapes_bit_equal():
     """Every launch shape the autotuner may leave behind gives the same wavefields."""
-    shot = _iso_shot(76, 40, 68)
+    shot = _iso_shot(76, 40, 100)
     p, src, rcv = _engine(shot, 1)
     ref = _modelling(shot, p, src, rcv)
     p.close()
