@@ -444,8 +444,9 @@ __device__ __forceinline__ void iso4_prefetch(const IsoArgs &a, const Grid3 &g, 
   }
 }
 
+// PML tiles without the Q update: at most 128 registers per thread (512 threads per SM)
 template <int TX, int P, int MODE, bool PML3D, bool EDGE>
-__global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ IsoArgs a,
+__global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 512 / (8 * TX) : 0) iso_fd8_tma4(const __grid_constant__ IsoArgs a,
                                                        const Tile4 *__restrict__ tiles,
                                                        const __grid_constant__ CUtensorMap map_w1,
                                                        const __grid_constant__ CUtensorMap map_w0,
@@ -577,6 +578,26 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
       iso4_prefetch<MODE>(a, g, !vpml && (x_edge || z_edge || y_edge_at(iy + 2)), ix, iy + 2, iz4, col);
       if (vpml) pml_prefetch(iy + 2, 2);
     }
+    // PML face memory of this plane, loaded before the waits and the stencil
+    // so that its latency overlaps them (PML tiles only)
+    const bool yf = (PML3D || do_y) && y_edge_at(iy);
+    float4 z1, z2, x1, x2, y1, y2;
+    float *qy1 = nullptr, *qy2 = nullptr;
+    float cy[3] = {0.f, 0.f, 0.f};
+    if constexpr (EDGE) {
+      if (vpml && act) {
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        z1 = z2 = x1 = x2 = y1 = y2 = z4;
+        if (qz1) z1 = *reinterpret_cast<const float4 *>(qz1), z2 = *reinterpret_cast<const float4 *>(qz2);
+        if (qx1) x1 = *reinterpret_cast<const float4 *>(qx1), x2 = *reinterpret_cast<const float4 *>(qx2);
+        if (yf) {
+          const float *cyp;
+          yface(iy, qy1, qy2, cyp);
+          y1 = *reinterpret_cast<const float4 *>(qy1), y2 = *reinterpret_cast<const float4 *>(qy2);
+          cy[0] = cyp[0], cy[1] = cyp[1], cy[2] = cyp[2];
+        }
+      }
+    }
     const int r0 = iy - y0, sa0 = r0 % SA, sa4 = (r0 + R4) % SA, sb = r0 % SB;
     if (r0 < R4) ok = ok && mbar_wait(&s.bar_a[sa0], (uint32_t)((r0 / SA) & 1), err);
     ok = ok && mbar_wait(&s.bar_a[sa4], (uint32_t)(((r0 + R4) / SA) & 1), err);
@@ -610,43 +631,36 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
       }
       float v[4];
       const bool y_edge = y_edge_at(iy);
-      const bool yf = (PML3D || do_y) && y_edge;
-      if (vpml && (qx1 || qz1 || yf)) {
-        // pml2_dim's rounds per cell in the order z, x, y; all loads first
-        float *qy1 = nullptr, *qy2 = nullptr;
-        const float *cyp = nullptr;
-        if (yf) yface(iy, qy1, qy2, cyp);
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 z1 = qz1 ? *reinterpret_cast<const float4 *>(qz1) : z4, z2 = qz1 ? *reinterpret_cast<const float4 *>(qz2) : z4;
-        float4 x1 = qx1 ? *reinterpret_cast<const float4 *>(qx1) : z4, x2 = qx1 ? *reinterpret_cast<const float4 *>(qx2) : z4;
-        float4 y1 = yf ? *reinterpret_cast<const float4 *>(qy1) : z4, y2 = yf ? *reinterpret_cast<const float4 *>(qy2) : z4;
-        float cy[3] = {0.f, 0.f, 0.f};
-        if (yf) cy[0] = cyp[0], cy[1] = cyp[1], cy[2] = cyp[2];
+      bool pml_done = false;
+      if constexpr (EDGE) {
+        if (vpml && (qx1 || qz1 || yf)) {
+          // pml2_dim's rounds per cell in the order z, x, y
+          pml_done = true;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-          float pz = PML3D ? lzv[c] + lxv[c] + lyv[c] : lzv[c], px = lxv[c], py = lyv[c];
-          float m;
-          if (qz1) {
-            m = comp(z1, c), pml_round(cz[c], pz, &m), setc(z1, c, m);
-            m = comp(z2, c), pml_round(cz[c], pz, &m), setc(z2, c, m);
+          for (int c = 0; c < 4; c++) {
+            float pz = PML3D ? lzv[c] + lxv[c] + lyv[c] : lzv[c], px = lxv[c], py = lyv[c];
+            float m;
+            if (qz1) {
+              m = comp(z1, c), pml_round(cz[c], pz, &m), setc(z1, c, m);
+              m = comp(z2, c), pml_round(cz[c], pz, &m), setc(z2, c, m);
+            }
+            float &pxr = PML3D ? pz : px;
+            if (qx1) {
+              m = comp(x1, c), pml_round(cx, pxr, &m), setc(x1, c, m);
+              m = comp(x2, c), pml_round(cx, pxr, &m), setc(x2, c, m);
+            }
+            float &pyr = PML3D ? pz : py;
+            if (yf) {
+              m = comp(y1, c), pml_round(cy, pyr, &m), setc(y1, c, m);
+              m = comp(y2, c), pml_round(cy, pyr, &m), setc(y2, c, m);
+            }
+            v[c] = PML3D ? pz : pz + px + py;
           }
-          float &pxr = PML3D ? pz : px;
-          if (qx1) {
-            m = comp(x1, c), pml_round(cx, pxr, &m), setc(x1, c, m);
-            m = comp(x2, c), pml_round(cx, pxr, &m), setc(x2, c, m);
-          }
-          float &pyr = PML3D ? pz : py;
-          if (yf) {
-            m = comp(y1, c), pml_round(cy, pyr, &m), setc(y1, c, m);
-            m = comp(y2, c), pml_round(cy, pyr, &m), setc(y2, c, m);
-          }
-          v[c] = PML3D ? pz : pz + px + py;
-        }
-        if (qz1) *reinterpret_cast<float4 *>(qz1) = z1, *reinterpret_cast<float4 *>(qz2) = z2;
-        if (qx1) *reinterpret_cast<float4 *>(qx1) = x1, *reinterpret_cast<float4 *>(qx2) = x2;
-        if (yf) *reinterpret_cast<float4 *>(qy1) = y1, *reinterpret_cast<float4 *>(qy2) = y2;
-      } else if (EDGE && !z4ok && (x_edge || y_edge || z_edge)) {
-        {
+          if (qz1) *reinterpret_cast<float4 *>(qz1) = z1, *reinterpret_cast<float4 *>(qz2) = z2;
+          if (qx1) *reinterpret_cast<float4 *>(qx1) = x1, *reinterpret_cast<float4 *>(qx2) = x2;
+          if (yf) *reinterpret_cast<float4 *>(qy1) = y1, *reinterpret_cast<float4 *>(qy2) = y2;
+        } else if (!z4ok && (x_edge || y_edge || z_edge)) {
+          pml_done = true;
 #pragma unroll
           for (int c = 0; c < 4; c++) {
             const int iz = iz4 + c;
@@ -655,10 +669,10 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_tma4(const __grid_constant__ I
             else v[c] = lzv[c] + lxv[c] + lyv[c];
           }
         }
-      } else {
+      }
+      if (!pml_done)
 #pragma unroll
         for (int c = 0; c < 4; c++) v[c] = lzv[c] + lxv[c] + lyv[c];
-      }
       const long long i0 = (long long)iy * g.nxz + col;
       if (a.io.store | a.io.ic) iso4_io4(a.io, g, i0, ix, iy, iz4, col, u4);
       const float4 cw0 = s.w0[sb][tx][tzq], cvel = s.vel[sb][tx][tzq];
