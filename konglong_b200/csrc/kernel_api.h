@@ -10,6 +10,12 @@ struct rtm_ae;
 
 namespace rtm {
 
+// one column tile of the FD8 kernels: z tile bz (32 cells), x tile bx (tx
+// cells), planes [y0, y1)
+struct Tile4 {
+  int bz, bx, y0, y1;  // z tile (32 cells), x tile (tx cells), planes [y0, y1)
+};
+
 struct IsoArgs {
   int nx, ny, nz, yseg;
   const float *w1;
@@ -81,8 +87,12 @@ int iso_batch_ctas_per_sm(int tx, int pml3d);
 void launch_batch_inject(const IsoBatchShot *shots, int nactive, int max_ntr, int max_ly, int it_src, int it,
                          cudaStream_t st);
 void launch_batch_extract(const IsoBatchShot *shots, int nactive, int max_ntr, int jt, int it, cudaStream_t st);
-void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st, bool f16 = false);
-void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st, bool f16 = false);
+// one CTA per entry of tiles[0, ntiles) (column tiles of 32 z x tx x cells);
+// non-edge tiles hold no PML cell and run without the PML code
+void launch_grad_fd8(const GradArgs &a, const Tile4 *tiles, int ntiles, bool edge, int model, int tx,
+                     cudaStream_t st, bool f16 = false);
+void launch_div_fd8(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, int mode, int tx, cudaStream_t st,
+                    bool f16 = false);
 // FP16 state: new-field scales sn[y] = max(max over |dy| <= 4 of m0 / m1, floor) * 2^-12
 void launch_f16_scales(const unsigned *m0, const unsigned *m1, float *sn, int ny, float floor, cudaStream_t st);
 // snapshot slab headers of the FP16 state's new field from its slab maxima
@@ -118,9 +128,6 @@ void launch_iso_fd8_tma(const IsoArgs &a, const CUtensorMap &w1, const CUtensorM
 // with boxes (40, tx + 8) for w1 and (32, tx) for w0 / (v dt)^2.  One CTA per
 // entry of a tile table (device array); `edge` tiles may hold PML cells, the
 // others run a kernel compiled without the PML code.
-struct Tile4 {
-  int bz, bx, y0, y1;  // z tile (32 cells), x tile (tx cells), planes [y0, y1)
-};
 extern const TmaShape kIso4TmaShapes[];
 extern const int kIso4TmaNShapes;
 bool iso_tma4_init();

@@ -215,15 +215,18 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_batch(const IsoBatchShot *__re
 }
 
 // ---- anisotropic two-pass ----------------------------------------------------
-template <int TX, int MODEL, bool F16>
-__global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
+// One CTA per tile of the table; EDGE = false tiles hold no PML cell and are
+// compiled without the PML code (fewer registers, more resident warps).
+template <int TX, int MODEL, bool F16, bool EDGE>
+__global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__restrict__ tiles) {
   __shared__ float tile[TX + 2 * R][TZ + 2 * R];
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
   const int tz = threadIdx.x, tx = threadIdx.y;
-  const int iz = blockIdx.x * TZ + tz;
-  const int ix = blockIdx.y * TX + tx;
-  const int y0 = blockIdx.z * a.yseg;
-  const int y1 = min(a.ny, y0 + a.yseg);
+  const Tile4 tl = tiles[blockIdx.x];
+  const int iz = tl.bz * TZ + tz;
+  const int ix = tl.bx * TX + tx;
+  const int y0 = tl.y0;
+  const int y1 = tl.y1;
   const bool act = iz < a.nz && ix < a.nx;
   const long long col = (long long)ix * a.nz + iz;
   const float *__restrict__ w1 = a.w1;
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a) {
         if (do_y) gy += a.c1y[m] * (q[R + m] - q[R - m]);
       }
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
-      if (in_pml(a.pml, g, ix, iy, iz)) pml1_all<0>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
+      if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<0>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
       if (MODEL == 2 || MODEL == 3) {
         // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
         float e = cm.x;
@@ -330,16 +333,17 @@ __device__ __forceinline__ DivPlane fetch_div(const DivArgs &a, int iy, int ix, 
   return d;
 }
 
-template <int TX, int MODE, bool F16>
-__global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
+template <int TX, int MODE, bool F16, bool EDGE>
+__global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__restrict__ tiles) {
   __shared__ float tpx[TX + 2 * R][TZ];
   __shared__ float tpz[TX][TZ + 2 * R];
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
   const int tz = threadIdx.x, tx = threadIdx.y;
-  const int iz = blockIdx.x * TZ + tz;
-  const int ix = blockIdx.y * TX + tx;
-  const int y0 = blockIdx.z * a.yseg;
-  const int y1 = min(a.ny, y0 + a.yseg);
+  const Tile4 tl = tiles[blockIdx.x];
+  const int iz = tl.bz * TZ + tz;
+  const int ix = tl.bx * TX + tx;
+  const int y0 = tl.y0;
+  const int y1 = tl.y1;
   const bool act = iz < a.nz && ix < a.nx;
   const long long col = (long long)ix * a.nz + iz;
   const bool do_y = a.ny > 1;
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a) {
         dzv += a.c1z[m] * (tpz[tx][tz + R + m] - tpz[tx][tz + R - m]);
         if (do_y) dyv += a.c1y[m] * (q[R + m] - q[R - m]);
       }
-      if (in_pml(a.pml, g, ix, iy, iz)) pml1_all<1>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
+      if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<1>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
       // accumulation order of KernelCPU::TTI: x, then z, then y
       float t = cw0 - dxv * cvel;
       t = t - dzv * cvel;
@@ -467,44 +471,58 @@ int iso_batch_ctas_per_sm(int tx, int pml3d) {
   return std::max(1, n);
 }
 
-template <int TX, bool F16>
-static void grad_launch_tx(const GradArgs &a, int model, cudaStream_t st) {
-  dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
-  if (model == 3) grad_fd8<TX, 3, F16><<<grid, block, 0, st>>>(a);
-  else if (model == 2) grad_fd8<TX, 2, F16><<<grid, block, 0, st>>>(a);
-  else grad_fd8<TX, 1, F16><<<grid, block, 0, st>>>(a);
+template <int TX, bool F16, bool EDGE>
+static void grad_launch_tx(const GradArgs &a, const Tile4 *tiles, int n, int model, cudaStream_t st) {
+  const dim3 block(TZ, TX);
+  if (model == 3) grad_fd8<TX, 3, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
+  else if (model == 2) grad_fd8<TX, 2, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
+  else grad_fd8<TX, 1, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
 }
 
-void launch_grad_fd8(const GradArgs &a, int model, int tx, cudaStream_t st, bool f16) {
+template <bool F16, bool EDGE>
+static void grad_launch(const GradArgs &a, const Tile4 *tiles, int n, int model, int tx, cudaStream_t st) {
+  if (tx == 4) grad_launch_tx<4, F16, EDGE>(a, tiles, n, model, st);
+  else if (tx == 16) grad_launch_tx<16, F16, EDGE>(a, tiles, n, model, st);
+  else grad_launch_tx<8, F16, EDGE>(a, tiles, n, model, st);
+}
+
+void launch_grad_fd8(const GradArgs &a, const Tile4 *tiles, int ntiles, bool edge, int model, int tx,
+                     cudaStream_t st, bool f16) {
+  if (ntiles <= 0) return;
   if (f16) {
-    if (tx == 4) grad_launch_tx<4, true>(a, model, st);
-    else if (tx == 16) grad_launch_tx<16, true>(a, model, st);
-    else grad_launch_tx<8, true>(a, model, st);
-    return;
+    if (edge) grad_launch<true, true>(a, tiles, ntiles, model, tx, st);
+    else grad_launch<true, false>(a, tiles, ntiles, model, tx, st);
+  } else {
+    if (edge) grad_launch<false, true>(a, tiles, ntiles, model, tx, st);
+    else grad_launch<false, false>(a, tiles, ntiles, model, tx, st);
   }
-  if (tx == 4) grad_launch_tx<4, false>(a, model, st);
-  else if (tx == 16) grad_launch_tx<16, false>(a, model, st);
-  else grad_launch_tx<8, false>(a, model, st);
 }
 
-template <int TX, bool F16>
-static void div_launch_tx(const DivArgs &a, int mode, cudaStream_t st) {
-  dim3 grid = fd_grid(a.nx, a.ny, a.nz, TX, a.yseg), block(TZ, TX);
-  if (mode == 0) div_fd8<TX, 0, F16><<<grid, block, 0, st>>>(a);
-  else if (mode == 1) div_fd8<TX, 1, F16><<<grid, block, 0, st>>>(a);
-  else div_fd8<TX, 2, F16><<<grid, block, 0, st>>>(a);
+template <int TX, bool F16, bool EDGE>
+static void div_launch_tx(const DivArgs &a, const Tile4 *tiles, int n, int mode, cudaStream_t st) {
+  const dim3 block(TZ, TX);
+  if (mode == 0) div_fd8<TX, 0, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
+  else if (mode == 1) div_fd8<TX, 1, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
+  else div_fd8<TX, 2, F16, EDGE><<<n, block, 0, st>>>(a, tiles);
 }
 
-void launch_div_fd8(const DivArgs &a, int mode, int tx, cudaStream_t st, bool f16) {
+template <bool F16, bool EDGE>
+static void div_launch(const DivArgs &a, const Tile4 *tiles, int n, int mode, int tx, cudaStream_t st) {
+  if (tx == 4) div_launch_tx<4, F16, EDGE>(a, tiles, n, mode, st);
+  else if (tx == 16) div_launch_tx<16, F16, EDGE>(a, tiles, n, mode, st);
+  else div_launch_tx<8, F16, EDGE>(a, tiles, n, mode, st);
+}
+
+void launch_div_fd8(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, int mode, int tx, cudaStream_t st,
+                    bool f16) {
+  if (ntiles <= 0) return;
   if (f16) {
-    if (tx == 4) div_launch_tx<4, true>(a, mode, st);
-    else if (tx == 16) div_launch_tx<16, true>(a, mode, st);
-    else div_launch_tx<8, true>(a, mode, st);
-    return;
+    if (edge) div_launch<true, true>(a, tiles, ntiles, mode, tx, st);
+    else div_launch<true, false>(a, tiles, ntiles, mode, tx, st);
+  } else {
+    if (edge) div_launch<false, true>(a, tiles, ntiles, mode, tx, st);
+    else div_launch<false, false>(a, tiles, ntiles, mode, tx, st);
   }
-  if (tx == 4) div_launch_tx<4, false>(a, mode, st);
-  else if (tx == 16) div_launch_tx<16, false>(a, mode, st);
-  else div_launch_tx<8, false>(a, mode, st);
 }
 
 }  // namespace rtm

@@ -40,6 +40,14 @@ struct TraceSetDev {
   }
 };
 
+// A device table of 32 (z) x tx (x) column tiles over y segments of yseg
+// planes: n_int tiles free of PML cells, then n_edge tiles that may hold some.
+struct TileSet {
+  Tile4 *d = nullptr;
+  int cap = 0, n_int = 0, n_edge = 0, tx = 0, yseg = 0;
+  bool current(int tx_, int yseg_) const { return d && tx == tx_ && yseg == std::max(1, yseg_); }
+};
+
 struct Engine {
   rtm_dims d{};
   rtm_config c{};
@@ -100,9 +108,9 @@ struct Engine {
   // 1 register-prefetch kernel (tile width v4_tx), 2 TMA rings (kIso4TmaShapes[v4_shape])
   int iso4 = 0;
   int v4_tx = 16, v4_shape = 0, v4_yseg = 16;
-  // tile table of the TMA-ring kernel: interior tiles [0, n_int), then PML tiles
-  Tile4 *tiles = nullptr;
-  int tiles_cap = 0, n_int = 0, n_edge = 0, tiles_tx = 0, tiles_yseg = 0;
+  // column-tile tables (interior tiles [0, n_int), then PML tiles) of the
+  // ISO TMA-ring kernel and of the FD8 gradient / divergence passes
+  TileSet t_iso, t_fd8;
   std::vector<std::array<int, 4>> tune_desc;  // candidates of the last rtm_autotune and their times
   std::vector<float> tune_ms;
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
@@ -248,13 +256,13 @@ static int yseg_v4(Engine *h, int tx, int ctas_per_sm) {
   }
   return best_y;
 }
-// Tile table of the TMA-ring ISO kernel for its current (tile width, y
-// segment): columns touching an x or z PML face are PML tiles over all y; the
-// others are PML tiles over the y faces and interior tiles between.  Built on
-// the host and uploaded (never inside a stream capture).
-static int iso4_tiles(Engine *h) {
-  const int tx = kIso4TmaShapes[h->v4_shape].tx, yseg = std::max(1, h->v4_yseg);
-  if (h->tiles && h->tiles_tx == tx && h->tiles_yseg == yseg) return RTM_OK;
+// Tile table for tile width tx and y segment yseg: columns touching an x or
+// z PML face are PML tiles over all y; the others are PML tiles over the y
+// faces and interior tiles between.  Built on the host and uploaded (never
+// inside a stream capture).
+static int build_tiles(Engine *h, TileSet &t, int tx, int yseg) {
+  yseg = std::max(1, yseg);
+  if (t.current(tx, yseg)) return RTM_OK;
   const int nx = h->d.nx, ny = h->d.ny, nz = h->d.nz;
   const int zl = h->pml.f[DZ][0].w, zh = h->pml.f[DZ][1].w, xl = h->pml.f[DX][0].w, xh = h->pml.f[DX][1].w,
             yl = h->pml.f[DY][0].w, yh = h->pml.f[DY][1].w;
@@ -282,18 +290,23 @@ static int iso4_tiles(Engine *h) {
   std::stable_sort(in.begin(), in.end(), by_y);
   std::stable_sort(ed.begin(), ed.end(), by_y);
   const int n = (int)(in.size() + ed.size());
-  if (n > h->tiles_cap) {
-    h->release(h->tiles);
-    h->tiles = nullptr, h->tiles_cap = 0;
-    TRY(h->alloc(h->tiles, (size_t)n));
-    h->tiles_cap = n;
+  if (n > t.cap) {
+    h->release(t.d);
+    t.d = nullptr, t.cap = 0;
+    TRY(h->alloc(t.d, (size_t)n));
+    t.cap = n;
   }
   std::vector<Tile4> all(in);
   all.insert(all.end(), ed.begin(), ed.end());
-  CK(cudaMemcpy(h->tiles, all.data(), sizeof(Tile4) * n, cudaMemcpyHostToDevice));
-  h->n_int = (int)in.size(), h->n_edge = (int)ed.size(), h->tiles_tx = tx, h->tiles_yseg = yseg;
+  CK(cudaMemcpy(t.d, all.data(), sizeof(Tile4) * n, cudaMemcpyHostToDevice));
+  t.n_int = (int)in.size(), t.n_edge = (int)ed.size(), t.tx = tx, t.yseg = yseg;
   return RTM_OK;
 }
+static int iso4_tiles(Engine *h) {
+  return build_tiles(h, h->t_iso, kIso4TmaShapes[h->v4_shape].tx, h->v4_yseg);
+}
+// tables of the FD8 gradient / divergence passes (tile width tx, y segment yseg)
+static int fd8_tiles(Engine *h) { return build_tiles(h, h->t_fd8, h->tx, h->yseg); }
 
 static int yseg_iso4(Engine *h) {
   if (h->iso4 == 2)
@@ -456,7 +469,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     CUtensorMap m1, m0, mv;
     if (h->iso4 == 2) {
       const int tx = kIso4TmaShapes[h->v4_shape].tx;
-      if (!h->tiles || h->tiles_tx != tx || h->tiles_yseg != std::max(1, h->v4_yseg)) {
+      if (!h->t_iso.current(tx, h->v4_yseg)) {
         h->err = "iso4 tile table is stale";
         return RTM_ERR_STATE;
       }
@@ -469,11 +482,11 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
       a.yseg = h->v4_yseg;
       if (h->iso4 == 2) {
         {
-          KScope k(h, RTM_K_ISO, (h->n_int > 0) + (h->n_edge > 0));
-          launch_iso_fd8_tma4(a, h->tiles, h->n_int, false, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape,
+          const TileSet &t = h->t_iso;
+          KScope k(h, RTM_K_ISO, (t.n_int > 0) + (t.n_edge > 0));
+          launch_iso_fd8_tma4(a, t.d, t.n_int, false, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape, h->st);
+          launch_iso_fd8_tma4(a, t.d + t.n_int, t.n_edge, true, m1, m0, mv, h->dflag, mode, h->c.pml3d, h->v4_shape,
                               h->st);
-          launch_iso_fd8_tma4(a, h->tiles + h->n_int, h->n_edge, true, m1, m0, mv, h->dflag, mode, h->c.pml3d,
-                              h->v4_shape, h->st);
         }
         return check_launch(h, "iso_fd8_tma4");
       }
@@ -497,6 +510,11 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     return check_launch(h, "iso_fd8_step");
   }
   if (h->c.engine == RTM_ENGINE_FD8) {
+    const TileSet &t = h->t_fd8;
+    if (!t.current(h->tx, h->yseg)) {
+      h->err = "FD8 tile table is stale";
+      return RTM_ERR_STATE;
+    }
     GradArgs g{};
     g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = h->yseg, g.pml3d = h->c.pml3d;
     g.w1 = h->w1, g.px = h->px, g.py = h->py, g.pz = h->pz;
@@ -506,8 +524,9 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     g.pml = pml_dev(h);
     g.io = io;
     {
-      KScope k(h, RTM_K_GRAD);
-      launch_grad_fd8(g, h->c.model_type, h->tx, h->st, h->f16);
+      KScope k(h, RTM_K_GRAD, (t.n_int > 0) + (t.n_edge > 0));
+      launch_grad_fd8(g, t.d, t.n_int, false, h->c.model_type, h->tx, h->st, h->f16);
+      launch_grad_fd8(g, t.d + t.n_int, t.n_edge, true, h->c.model_type, h->tx, h->st, h->f16);
     }
     TRY(check_launch(h, "grad_fd8"));
     if (h->f16) {  // scale of the field this step writes, then its fresh slab maxima
@@ -522,8 +541,9 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     v.pml = pml_dev(h);
     v.q = q;
     {
-      KScope k(h, RTM_K_DIV);
-      launch_div_fd8(v, mode, h->tx, h->st, h->f16);
+      KScope k(h, RTM_K_DIV, (t.n_int > 0) + (t.n_edge > 0));
+      launch_div_fd8(v, t.d, t.n_int, false, mode, h->tx, h->st, h->f16);
+      launch_div_fd8(v, t.d + t.n_int, t.n_edge, true, mode, h->tx, h->st, h->f16);
     }
     return check_launch(h, "div_fd8");
   }
@@ -1176,6 +1196,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     h->v4_yseg = yseg_iso4(h);
     if (h->iso4 == 2 && (rc = iso4_tiles(h))) return fail(rc);
   }
+  if (c->engine == RTM_ENGINE_FD8 && c->model_type != RTM_ISO && (rc = fd8_tiles(h))) return fail(rc);
   h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
   h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
@@ -1769,6 +1790,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     if (c.iso4) h->v4_yseg = c.yseg;
     h->tma_shape = c.tma_shape, h->tx = c.tx, h->cfd_xy = c.cfd_xy;
     h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
+    if (h->c.engine == RTM_ENGINE_FD8 && h->c.model_type != RTM_ISO) TRY(rtm::fd8_tiles(h));
     return h->iso4 == 2 ? rtm::iso4_tiles(h) : (int)RTM_OK;
   };
   float best = 1e30f;
