@@ -139,7 +139,7 @@ __device__ __noinline__ float4 iso4_q4(const QDev &Q, long long i, long long n, 
   const float uv[4] = {u.x, u.y, u.z, u.w}, iv[4] = {iq.x, iq.y, iq.z, iq.w};
   float v[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-  for (int c = 0; c < 4; c++) v[c] = uv[c] * (2.0f + iv[c] * Q.cqsum) - v[c];
+  for (int c = 0; c < 4; c++) v[c] = q_init(uv[c], iv[c], Q.cqsum, v[c]);
   for (int l0 = 0; l0 < Q.order; l0 += 4) {
     float4 d0[4], d1[4];
 #pragma unroll
@@ -155,8 +155,8 @@ __device__ __noinline__ float4 iso4_q4(const QDev &Q, long long i, long long n, 
         if (l0 + l < Q.order) {
           const float e0 = comp(d0[l], c), e1 = comp(d1[l], c);
           const float el = Q.wq[l0 + l];
-          v[c] += iv[c] * ((1.0f + el) * e0 - e1 * 2.0f);
-          setc(d0[l], c, Q.cq[l0 + l] * uv[c] + el * e0);
+          v[c] = q_acc(v[c], iv[c], el, e0, e1);
+          setc(d0[l], c, q_next(Q.cq[l0 + l], uv[c], el, e0));
         }
 #pragma unroll
     for (int l = 0; l < 4; l++)

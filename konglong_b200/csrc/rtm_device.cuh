@@ -318,15 +318,41 @@ __device__ __forceinline__ void fused_io(const FusedIo &io, const Grid3 &g, long
 
 // Visco-acoustic update (bgprtm/Propagator.cpp:1789-1816) for one cell:
 // t = w0 - vel*L[w1] on entry, u = w1.
+// Steps of the update with every rounding written out (fused multiply-adds
+// in a fixed form), so that the one-cell and the 4-cell kernels compute
+// identical bits whatever the compiler would otherwise contract:
+//   v   = u (2 + iq cqsum) - t
+//   v  += iq ((1 + w_l) d0_l - 2 d1_l)
+//   d0' = cq_l u + w_l d0_l
+__device__ __forceinline__ float q_init(float u, float iq, float cqsum, float t) {
+  return __fmaf_rn(u, __fmaf_rn(iq, cqsum, 2.0f), -t);
+}
+__device__ __forceinline__ float q_acc(float v, float iq, float el, float d0, float d1) {
+  return __fmaf_rn(iq, __fmaf_rn(__fadd_rn(1.0f, el), d0, -2.0f * d1), v);
+}
+__device__ __forceinline__ float q_next(float cq, float u, float el, float d0) {
+  return __fmaf_rn(el, d0, __fmul_rn(cq, u));
+}
+
+// The memory variables of up to 4 orders are loaded before any is updated, so
+// a cell waits for one load round trip per 4 orders (order <= 8, QDev::cq).
 __device__ __forceinline__ float q_update(const QDev &Q, long long i, long long n, float t, float u) {
   const float iq = Q.invq[i];
-  float v = u * (2.0f + iq * Q.cqsum) - t;
-  for (int l = 0; l < Q.order; l++) {
-    float *d0p = Q.d0 + (long long)l * n + i;
-    const float d0 = *d0p, d1 = Q.d1[(long long)l * n + i];
-    const float el = Q.wq[l];
-    v += iq * ((1.0f + el) * d0 - d1 * 2.0f);
-    *d0p = Q.cq[l] * u + el * d0;
+  float v = q_init(u, iq, Q.cqsum, t);
+#pragma unroll
+  for (int l0 = 0; l0 < 8; l0 += 4) {
+    if (l0 >= Q.order) break;
+    float d0[4], d1[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      if (l0 + l < Q.order) d0[l] = Q.d0[(long long)(l0 + l) * n + i], d1[l] = Q.d1[(long long)(l0 + l) * n + i];
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      if (l0 + l < Q.order) {
+        const float el = Q.wq[l0 + l];
+        v = q_acc(v, iq, el, d0[l], d1[l]);
+        Q.d0[(long long)(l0 + l) * n + i] = q_next(Q.cq[l0 + l], u, el, d0[l]);
+      }
   }
   return v;
 }
