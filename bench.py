@@ -81,14 +81,52 @@ MEASURED_DRAM_B_PER_CELL = {"vti_cfd": {"cfd_div_epilogue": 36.98, "cfd_grad_epi
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: NVML read
+    every 5 ms from a thread (the timed regions here last 0.1-1 s), nvidia-smi
+    every 200 ms when NVML is not importable.  Reads only; changes no setting."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index=0):
         self.index = index
-        self.rows = []
+        self.rows = []   # (sm_mhz, max_mhz, reasons set)
         self.proc = None
+        self.stop = threading.Event()
+        self.th = None
+
+    def _nvml_handle(self, nv):
+        try:  # the CUDA device this process uses, matched by UUID (indices may differ)
+            import torch
+            u = str(torch.cuda.get_device_properties(self.index).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            bits = [getattr(nv, "nvmlClocksEventReason" + k, getattr(nv, "nvmlClocksThrottleReason" + k, 0))
+                    for k in ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                                 getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = reasons_fn(h) if reasons_fn else 0
+                        self.rows.append((sm, mx, {self.NAMES[k] for k in range(4) if bits[k] and r & bits[k]}))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.005)
+            self.th = threading.Thread(target=run, daemon=True)
+            self.th.start()
+            return self
+        except Exception:
+            pass
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -104,26 +142,28 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                self.rows.append((float(r[1]), float(r[2]),
+                                  {self.NAMES[k] for k in range(4) if r[5 + k].lower() == "active"}))
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.th:
+            self.th.join(timeout=5)
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4)
-                          if r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        sm = [r[0] for r in self.rows]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(set().union(*[r[2] for r in self.rows])), "samples": len(self.rows)}
 
 
 def build_workload(name, steps_total, scale=1.0):
