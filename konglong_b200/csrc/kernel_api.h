@@ -136,6 +136,22 @@ void launch_iso_fd8_tma4(const IsoArgs &a, const Tile4 *tiles, int ntiles, bool 
                          const CUtensorMap &w0, const CUtensorMap &vel, int *err, int mode, int pml3d, int shape,
                          cudaStream_t st);
 
+// FD8 VTI / TTI passes with 4 z cells per thread and TMA rings
+// (kernels_aniso4.cu), tile width kAniso4TX, nz % 4 == 0, FP32 state
+constexpr int kAniso4TX = 16;
+struct Grad4Maps {
+  CUtensorMap w1, m[4];  // w1 box (40, tx + 8); eps, del, pjx, pjy boxes (32, tx)
+};
+struct Div4Maps {
+  CUtensorMap py, px, pz, w0, vel, w1;  // py (32, tx); px (32, tx + 8); pz (40, tx); w0 / vel / w1 (32, tx)
+};
+bool aniso4_init();         // shared-memory attributes (call outside any capture)
+int aniso4_ctas_per_sm();   // resident CTAs per SM of the interior divergence kernel
+void launch_grad4(const GradArgs &a, const Tile4 *tiles, int ntiles, bool edge, int model, const Grad4Maps &m,
+                  int *err, cudaStream_t st);
+void launch_div4(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, int mode, const Div4Maps &m, int *err,
+                 cudaStream_t st);
+
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {
   int n;

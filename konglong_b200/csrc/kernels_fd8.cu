@@ -264,40 +264,13 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__re
       float gz = 0.f, gx = 0.f, gy = 0.f;
 #pragma unroll
       for (int m = 1; m <= R; m++) {
-        gz += a.c1z[m] * (tile[tx + R][tz + R + m] - tile[tx + R][tz + R - m]);
-        gx += a.c1x[m] * (tile[tx + R + m][tz + R] - tile[tx + R - m][tz + R]);
-        if (do_y) gy += a.c1y[m] * (q[R + m] - q[R - m]);
+        gz = d1_acc(gz, a.c1z[m], tile[tx + R][tz + R + m], tile[tx + R][tz + R - m]);
+        gx = d1_acc(gx, a.c1x[m], tile[tx + R + m][tz + R], tile[tx + R - m][tz + R]);
+        if (do_y) gy = d1_acc(gy, a.c1y[m], q[R + m], q[R - m]);
       }
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
       if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<0>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
-      if (MODEL == 2 || MODEL == 3) {
-        // pseudo-acoustic scaling (ScalarVTI / ScalarTTI)
-        float e = cm.x;
-        const float dl = e - cm.y;
-        e = 1.0f + 2.0f * e;
-        if (MODEL == 3) {
-          const float ax = cm.z, ay = cm.w;
-          const float az = sqrtf(1.0f - (ax * ax + ay * ay));
-          const float v2 = gx * gx + gy * gy + gz * gz;
-          const float vzz = gx * ax + gy * ay + gz * az;
-          const float vz2 = vzz * vzz;
-          const float vh2 = v2 - vz2;
-          const float ecl = e * vh2 + vz2;
-          const float parts = sqrtf(1.0f - 8.0f * (dl * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-          const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
-          const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
-          gx = (bx + (gx - bx) * e) * sc;
-          gy = (by + (gy - by) * e) * sc;
-          gz = (bz + (gz - bz) * e) * sc;
-        } else {
-          const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
-          const float ecl = e * vx2 + vz2;
-          const float parts = sqrtf(1.0f - 8.0f * (dl * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-          const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
-          gx *= sc2;
-          gy *= sc2;
-        }
-      }
+      if (MODEL == 2 || MODEL == 3) aniso_scale<MODEL>(cm, gx, gy, gz);
       a.px[i] = gx;
       a.pz[i] = gz;
       if (do_y) a.py[i] = gy;
@@ -383,18 +356,15 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__rest
       float dxv = 0.f, dzv = 0.f, dyv = 0.f;
 #pragma unroll
       for (int m = 1; m <= R; m++) {
-        dxv += a.c1x[m] * (tpx[tx + R + m][tz] - tpx[tx + R - m][tz]);
-        dzv += a.c1z[m] * (tpz[tx][tz + R + m] - tpz[tx][tz + R - m]);
-        if (do_y) dyv += a.c1y[m] * (q[R + m] - q[R - m]);
+        dxv = d1_acc(dxv, a.c1x[m], tpx[tx + R + m][tz], tpx[tx + R - m][tz]);
+        dzv = d1_acc(dzv, a.c1z[m], tpz[tx][tz + R + m], tpz[tx][tz + R - m]);
+        if (do_y) dyv = d1_acc(dyv, a.c1y[m], q[R + m], q[R - m]);
       }
       if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<1>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
-      // accumulation order of KernelCPU::TTI: x, then z, then y
-      float t = cw0 - dxv * cvel;
-      t = t - dzv * cvel;
-      t = t - dyv * cvel;
+      const float t = div_accumulate(cw0, cvel, dxv, dzv, dyv);
       float out;
       if (MODE == 0) out = t;
-      else out = MODE == 1 ? (cw1 + cw1) - t : q_update(a.q, i, (long long)a.ny * g.nxz, t, cw1);
+      else out = MODE == 1 ? __fsub_rn(__fadd_rn(cw1, cw1), t) : q_update(a.q, i, (long long)a.ny * g.nxz, t, cw1);
       if (F16) {
         const float sc = __ldg(a.h.sn + iy);
         float hv = out / sc;

@@ -165,77 +165,6 @@ __device__ __noinline__ float4 iso4_q4(const QDev &Q, long long i, long long n, 
   return make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// Fused snapshot store / imaging condition (fused_io) of the thread's 4 cells
-// with one vector access per array: FP32 slots and the image / compensation
-// pair as float4, FP16 slots as 8 bytes, COMPRESS_16 codes as two 4-byte
-// words (a slab's codes start 4 bytes into it).  Same arithmetic per cell.
-__device__ __forceinline__ void iso4_io4(const FusedIo &io, const Grid3 &g, long long i0, int ix, int iy, int iz4,
-                                         long long col, float4 u4) {
-  const float uv[4] = {u4.x, u4.y, u4.z, u4.w};
-  if (io.store) {
-    const SnapDev &S = io.st;
-    if (S.fmt == 0) {
-      *reinterpret_cast<float4 *>((float *)S.base + i0) = u4;
-    } else if (S.fmt == 1) {
-      const float vmax = S.slab[iy];
-      uint16_t c[4] = {0, 0, 0, 0};
-      if (vmax > 1e-25f)
-#pragma unroll
-        for (int k = 0; k < 4; k++) c[k] = c16_encode(uv[k] * __frcp_rn(vmax));
-      uint32_t *w = reinterpret_cast<uint32_t *>((uint16_t *)S.base + (long long)iy * (g.nxz + 2) + 2 + col);
-      w[0] = (uint32_t)c[0] | ((uint32_t)c[1] << 16);
-      w[1] = (uint32_t)c[2] | ((uint32_t)c[3] << 16);
-    } else {
-      const float sc = S.slab[iy];
-      __half2 h[2] = {__halves2half2(slab16_encode(uv[0], sc), slab16_encode(uv[1], sc)),
-                      __halves2half2(slab16_encode(uv[2], sc), slab16_encode(uv[3], sc))};
-      *reinterpret_cast<uint2 *>((__half *)S.base + i0) = *reinterpret_cast<uint2 *>(h);
-    }
-  }
-  if (io.ic) {
-    const SnapDev &S = io.src;
-    float sv[4];
-    if (S.fmt == 0) {
-      const float4 v = *reinterpret_cast<const float4 *>((const float *)S.base + i0);
-      sv[0] = v.x, sv[1] = v.y, sv[2] = v.z, sv[3] = v.w;
-    } else if (S.fmt == 1) {
-      const uint32_t *w = reinterpret_cast<const uint32_t *>((const uint16_t *)S.base + (long long)iy * (g.nxz + 2) + 2 + col);
-      const uint32_t a = w[0], b = w[1];
-      const float sl = S.slab[iy];
-      sv[0] = sl * c16_table((uint16_t)(a & 0xffff)), sv[1] = sl * c16_table((uint16_t)(a >> 16));
-      sv[2] = sl * c16_table((uint16_t)(b & 0xffff)), sv[3] = sl * c16_table((uint16_t)(b >> 16));
-    } else {
-      const uint2 hv = *reinterpret_cast<const uint2 *>((const __half *)S.base + i0);
-      const __half2 h0 = *reinterpret_cast<const __half2 *>(&hv.x), h1 = *reinterpret_cast<const __half2 *>(&hv.y);
-      const float sl = S.slab[iy];
-      sv[0] = slab16_decode(__low2half(h0), sl), sv[1] = slab16_decode(__high2half(h0), sl);
-      sv[2] = slab16_decode(__low2half(h1), sl), sv[3] = slab16_decode(__high2half(h1), sl);
-    }
-    float4 img = *reinterpret_cast<const float4 *>(io.image + i0), cmp = *reinterpret_cast<const float4 *>(io.comp + i0);
-    const float ey = io.ey[iy], ex = io.ex[ix];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const int iz = iz4 + k;
-      float s = sv[k] * ey;
-      s = s * ex;
-      s = s * io.ez[iz];
-      if (io.use_t) s = s * io.tscale;
-      else s = s * io.taper_z[iz];
-      float r = uv[k] * ey;
-      r = r * ex;
-      r = r * io.ez[iz];
-      const float prod = s * r;
-      const float im = comp(img, k);
-      const float y = prod - comp(cmp, k);
-      const float t = im + y;
-      setc(cmp, k, (t - im) - y);
-      setc(img, k, t);
-    }
-    *reinterpret_cast<float4 *>(io.comp + i0) = cmp;
-    *reinterpret_cast<float4 *>(io.image + i0) = img;
-  }
-}
-
 template <int TX, int MODE, bool PML3D>
 __global__ void __launch_bounds__(8 * TX) iso_fd8_v4(const __grid_constant__ IsoArgs a) {
   __shared__ float4 tile[2][TX + 2 * R4][10];  // [buffer][x + halo][z float4 + one halo float4 each side]
@@ -352,7 +281,7 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_v4(const __grid_constant__ Iso
         for (int c = 0; c < 4; c++) v[c] = lzv[c] + lxv[c] + lyv[c];
       }
       const long long i0 = (long long)iy * g.nxz + col;
-      if (a.io.store | a.io.ic) iso4_io4(a.io, g, i0, ix, iy, iz4, col, u4);
+      if (a.io.store | a.io.ic) fused_io4(a.io, g, i0, ix, iy, iz4, col, u4);
       float4 t4, out4;
 #pragma unroll
       for (int c = 0; c < 4; c++) setc(t4, c, comp(cw0, c) - v[c] * comp(cvel, c));
@@ -674,7 +603,7 @@ __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 512 / (8 * TX) : 0
 #pragma unroll
         for (int c = 0; c < 4; c++) v[c] = lzv[c] + lxv[c] + lyv[c];
       const long long i0 = (long long)iy * g.nxz + col;
-      if (a.io.store | a.io.ic) iso4_io4(a.io, g, i0, ix, iy, iz4, col, u4);
+      if (a.io.store | a.io.ic) fused_io4(a.io, g, i0, ix, iy, iz4, col, u4);
       const float4 cw0 = s.w0[sb][tx][tzq], cvel = s.vel[sb][tx][tzq];
       float4 t4, out4;
 #pragma unroll

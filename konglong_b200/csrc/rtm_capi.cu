@@ -111,6 +111,9 @@ struct Engine {
   // column-tile tables (interior tiles [0, n_int), then PML tiles) of the
   // ISO TMA-ring kernel and of the FD8 gradient / divergence passes
   TileSet t_iso, t_fd8;
+  // FD8 VTI / TTI with 4 z cells per thread and TMA rings (kernels_aniso4.cu) and its y segment
+  int aniso4 = 0, an4_yseg = 16;
+  TileSet t_an4;
   std::vector<std::array<int, 4>> tune_desc;  // candidates of the last rtm_autotune and their times
   std::vector<float> tune_ms;
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
@@ -307,6 +310,9 @@ static int iso4_tiles(Engine *h) {
 }
 // tables of the FD8 gradient / divergence passes (tile width tx, y segment yseg)
 static int fd8_tiles(Engine *h) { return build_tiles(h, h->t_fd8, h->tx, h->yseg); }
+static int an4_tiles(Engine *h) { return build_tiles(h, h->t_an4, kAniso4TX, h->an4_yseg); }
+
+static int yseg_an4(Engine *h) { return yseg_v4(h, kAniso4TX, aniso4_ctas_per_sm()); }
 
 static int yseg_iso4(Engine *h) {
   if (h->iso4 == 2)
@@ -508,6 +514,51 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
       else launch_iso_fd8(a, mode, h->c.pml3d, h->tx, h->st);
     }
     return check_launch(h, "iso_fd8_step");
+  }
+  if (h->c.engine == RTM_ENGINE_FD8 && h->aniso4) {
+    const TileSet &t = h->t_an4;
+    if (!t.current(kAniso4TX, h->an4_yseg)) {
+      h->err = "FD8 4-cell tile table is stale";
+      return RTM_ERR_STATE;
+    }
+    GradArgs g{};
+    g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = h->an4_yseg, g.pml3d = h->c.pml3d;
+    g.w1 = h->w1, g.px = h->px, g.py = h->py, g.pz = h->pz;
+    g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy;
+    memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
+    g.pml = pml_dev(h);
+    g.io = io;
+    DivArgs v{};
+    v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = h->an4_yseg, v.pml3d = h->c.pml3d;
+    v.px = h->px, v.py = h->py, v.pz = h->pz, v.w1 = h->w1, v.w0 = h->w0, v.vel = h->vel;
+    memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
+    v.pml = pml_dev(h);
+    v.q = q;
+    const int T = kAniso4TX;
+    Grad4Maps gm;
+    Div4Maps dm;
+    const bool tti = h->c.model_type == RTM_TTI;
+    bool ok = tmap(h, h->w1, 40, T + 8, &gm.w1) && tmap(h, h->eps, 32, T, &gm.m[0]) && tmap(h, h->del, 32, T, &gm.m[1]);
+    gm.m[2] = gm.m[3] = gm.m[0];
+    if (tti) ok = ok && tmap(h, h->pjx, 32, T, &gm.m[2]) && (!h->pjy || tmap(h, h->pjy, 32, T, &gm.m[3]));
+    ok = ok && tmap(h, h->px, 32, T + 8, &dm.px) && tmap(h, h->pz, 40, T, &dm.pz) &&
+         tmap(h, h->py ? h->py : h->px, 32, T, &dm.py) && tmap(h, h->w0, 32, T, &dm.w0) &&
+         tmap(h, h->vel, 32, T, &dm.vel) && tmap(h, h->w1, 32, T, &dm.w1);
+    if (ok) {
+      {
+        KScope k(h, RTM_K_GRAD, (t.n_int > 0) + (t.n_edge > 0));
+        launch_grad4(g, t.d, t.n_int, false, h->c.model_type, gm, h->dflag, h->st);
+        launch_grad4(g, t.d + t.n_int, t.n_edge, true, h->c.model_type, gm, h->dflag, h->st);
+      }
+      TRY(check_launch(h, "grad4"));
+      {
+        KScope k(h, RTM_K_DIV, (t.n_int > 0) + (t.n_edge > 0));
+        launch_div4(v, t.d, t.n_int, false, mode, dm, h->dflag, h->st);
+        launch_div4(v, t.d + t.n_int, t.n_edge, true, mode, dm, h->dflag, h->st);
+      }
+      return check_launch(h, "div4");
+    }
+    h->aniso4 = 0;  // tensor maps unavailable: the one-cell passes below
   }
   if (h->c.engine == RTM_ENGINE_FD8) {
     const TileSet &t = h->t_fd8;
@@ -1197,6 +1248,12 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     if (h->iso4 == 2 && (rc = iso4_tiles(h))) return fail(rc);
   }
   if (c->engine == RTM_ENGINE_FD8 && c->model_type != RTM_ISO && (rc = fd8_tiles(h))) return fail(rc);
+  if (c->engine == RTM_ENGINE_FD8 && c->model_type != RTM_ISO && !c->state_fp16 && d->nz % 4 == 0 &&
+      (c->kernel_variant == 0 || c->kernel_variant == 3) && tma_supported(d->nz) && aniso4_init()) {
+    h->aniso4 = 1;
+    h->an4_yseg = yseg_an4(h);
+    if ((rc = an4_tiles(h))) return fail(rc);
+  }
   h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
   h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
@@ -1748,6 +1805,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
   struct Cand {
     int iso4, v4, yseg;  // iso4 kind, its tile width (1) or shape (2), its y segment
     int tma_shape, tx, cfd_xy;
+    int an4 = 0;  // FD8 VTI / TTI 4-cell kernels (y segment in yseg)
   };
   std::vector<Cand> cands;
   const bool iso = h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO;
@@ -1774,6 +1832,13 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     for (int k = 0; k < rtm::kIsoTmaNShapes; k++) cands.push_back({0, 0, 0, k, h->tx, h->cfd_xy});
   else if (h->c.engine == RTM_ENGINE_FD8 && !v4_ok)
     for (int tx : {4, 8, 16}) cands.push_back({0, 0, 0, h->tma_shape, tx, h->cfd_xy});
+  const int an4_0 = h->aniso4;
+  if (an4_0) {
+    const int ym = rtm::yseg_an4(h);
+    cands.push_back({0, 0, ym, h->tma_shape, h->tx, h->cfd_xy, 1});
+    for (int y : {32, 64})
+      if (ym != y && h->d.ny > y) cands.push_back({0, 0, y, h->tma_shape, h->tx, h->cfd_xy, 1});
+  }
   else if (h->c.engine == RTM_ENGINE_CFD && h->c.kernel_variant == 0) {
     cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
     if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
@@ -1784,6 +1849,13 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
   }
   const int yseg0 = h->yseg;
   auto apply = [&](const Cand &c) {
+    if (an4_0) {
+      h->aniso4 = c.an4;
+      if (c.an4) {
+        h->an4_yseg = c.yseg;
+        TRY(rtm::an4_tiles(h));
+      }
+    }
     h->iso4 = c.iso4;
     if (c.iso4 == 1) h->v4_tx = c.v4;
     if (c.iso4 == 2) h->v4_shape = c.v4;
@@ -1807,8 +1879,9 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (ms < best) best = ms, bi = (int)c;
     const Cand &k = cands[c];
-    const int fam = k.iso4 ? k.iso4 : (iso && h->use_tma ? 3 : 0);
-    h->tune_desc.push_back({fam, k.iso4 ? k.v4 : fam == 3 ? k.tma_shape : k.tx, k.iso4 ? k.yseg : 0, k.cfd_xy});
+    const int fam = k.an4 ? 4 : k.iso4 ? k.iso4 : (iso && h->use_tma ? 3 : 0);
+    h->tune_desc.push_back({fam, k.an4 ? rtm::kAniso4TX : k.iso4 ? k.v4 : fam == 3 ? k.tma_shape : k.tx,
+                            k.iso4 || k.an4 ? k.yseg : 0, k.cfd_xy});
     h->tune_ms.push_back(ms);
   }
   TRY(apply(cands[bi]));

@@ -15,10 +15,12 @@ struct Grid3 {
 
 // One recursion round of the split-field PML on value p with memory q
 // (bgprtm/PML.cpp:126-134): q' = (1-g)/(1+g) q - 2g/(1-g^2) p ; p' = q' + p/(1-g).
+// The roundings are written out (fused multiply-adds in a fixed form) so that
+// every kernel computing this recursion gives the same bits.
 __device__ __forceinline__ void pml_round(const float *co, float &p, float *q) {
-  float qn = co[0] * (*q) - co[1] * p;
+  const float qn = __fmaf_rn(co[0], *q, -__fmul_rn(co[1], p));
   *q = qn;
-  p = qn + co[2] * p;
+  p = __fmaf_rn(co[2], p, qn);
 }
 
 // Memory cell and constants of face (d, s) for grid cell (ix,iy,iz), or null
@@ -179,10 +181,7 @@ __device__ __forceinline__ void pml1_all(const PmlDev &P, const Grid3 &g, int pm
         if (do_y && (d == DY || ycross)) qy[d][s] = P.f[d][s].q[R][cy(d)][i];
       }
   auto round = [&](float &p, float &q, int d, int s, int scaled) {
-    const float *co = P.f[d][s].co + c.layer[d][s] * 6 + 3 * scaled;
-    const float qn = co[0] * q - co[1] * p;
-    q = qn;
-    p = qn + co[2] * p;
+    pml_round(P.f[d][s].co + c.layer[d][s] * 6 + 3 * scaled, p, &q);
   };
   // component z: DZ, then DX, DY scaled
 #pragma unroll
@@ -232,6 +231,56 @@ __device__ __forceinline__ void pml1_all(const PmlDev &P, const Grid3 &g, int pm
         if (d == DX || cross) P.f[d][s].q[R][cx(d)][i] = qx[d][s];
         if (do_y && (d == DY || ycross)) P.f[d][s].q[R][cy(d)][i] = qy[d][s];
       }
+}
+
+// --- FD8 two-pass pieces shared by the one-cell and the 4-cell kernels ---------
+// (roundings written out so that both give the same bits)
+
+// one tap pair of a first derivative: acc + c (a - b)
+__device__ __forceinline__ float d1_acc(float acc, float c, float a, float b) {
+  return __fmaf_rn(c, __fsub_rn(a, b), acc);
+}
+
+// accumulation order of KernelCPU::TTI: w0 - vel dx, then - vel dz, then - vel dy
+__device__ __forceinline__ float div_accumulate(float w0, float vel, float dx, float dz, float dy) {
+  float t = __fmaf_rn(-dx, vel, w0);
+  t = __fmaf_rn(-dz, vel, t);
+  return __fmaf_rn(-dy, vel, t);
+}
+
+// pseudo-acoustic scaling of the gradient (ScalarVTI / ScalarTTI,
+// bgprtm/KernelCPU.cpp:176-297); m = (eps, delta, pjx, pjy)
+template <int MODEL>
+__device__ __forceinline__ void aniso_scale(const float4 &m, float &gx, float &gy, float &gz) {
+  float e = m.x;
+  const float dl = __fsub_rn(e, m.y);
+  e = __fmaf_rn(2.0f, e, 1.0f);
+  if (MODEL == 3) {
+    const float ax = m.z, ay = m.w;
+    const float az = sqrtf(__fsub_rn(1.0f, __fmaf_rn(ax, ax, __fmul_rn(ay, ay))));
+    const float v2 = __fmaf_rn(gz, gz, __fmaf_rn(gy, gy, __fmul_rn(gx, gx)));
+    const float vzz = __fmaf_rn(gz, az, __fmaf_rn(gy, ay, __fmul_rn(gx, ax)));
+    const float vz2 = __fmul_rn(vzz, vzz);
+    const float vh2 = __fsub_rn(v2, vz2);
+    const float ecl = __fmaf_rn(e, vh2, vz2);
+    const float parts =
+        sqrtf(__fsub_rn(1.0f, __fmul_rn(__fmul_rn(8.0f, __fmul_rn(dl, __fmul_rn(vh2, vz2))),
+                                        __frcp_rn(__fmaf_rn(ecl, ecl, 1e-32f)))));
+    const float sc = fminf(__fmul_rn(0.5f, __fadd_rn(1.0f, parts)), 1.0f);
+    const float bx = __fmul_rn(vzz, ax), by = __fmul_rn(vzz, ay), bz = __fmul_rn(vzz, az);
+    gx = __fmul_rn(__fmaf_rn(__fsub_rn(gx, bx), e, bx), sc);
+    gy = __fmul_rn(__fmaf_rn(__fsub_rn(gy, by), e, by), sc);
+    gz = __fmul_rn(__fmaf_rn(__fsub_rn(gz, bz), e, bz), sc);
+  } else {
+    const float vx2 = __fmaf_rn(gy, gy, __fmul_rn(gx, gx)), vz2 = __fmul_rn(gz, gz);
+    const float ecl = __fmaf_rn(e, vx2, vz2);
+    const float parts =
+        sqrtf(__fsub_rn(1.0f, __fmul_rn(__fmul_rn(8.0f, __fmul_rn(dl, __fmul_rn(vx2, vz2))),
+                                        __frcp_rn(__fmaf_rn(ecl, ecl, 1e-32f)))));
+    const float sc2 = __fmul_rn(e, fminf(__fmul_rn(0.5f, __fadd_rn(1.0f, parts)), 1.0f));
+    gx = __fmul_rn(gx, sc2);
+    gy = __fmul_rn(gy, sc2);
+  }
 }
 
 // --- COMPRESS_16 code (bgprtm/WaveFieldCompress.cpp:107-133) ----------------
@@ -313,6 +362,85 @@ __device__ __forceinline__ void fused_io(const FusedIo &io, const Grid3 &g, long
     const float t = img + y;
     io.comp[i] = (t - img) - y;
     io.image[i] = t;
+  }
+}
+
+__device__ __forceinline__ float io4_get(const float4 &v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+__device__ __forceinline__ void io4_set(float4 &v, int c, float x) {
+  if (c == 0) v.x = x;
+  else if (c == 1) v.y = x;
+  else if (c == 2) v.z = x;
+  else v.w = x;
+}
+
+// Fused snapshot store / imaging condition (fused_io) of the thread's 4 cells
+// with one vector access per array: FP32 slots and the image / compensation
+// pair as float4, FP16 slots as 8 bytes, COMPRESS_16 codes as two 4-byte
+// words (a slab's codes start 4 bytes into it).  Same arithmetic per cell.
+__device__ __forceinline__ void fused_io4(const FusedIo &io, const Grid3 &g, long long i0, int ix, int iy, int iz4,
+                                         long long col, float4 u4) {
+  const float uv[4] = {u4.x, u4.y, u4.z, u4.w};
+  if (io.store) {
+    const SnapDev &S = io.st;
+    if (S.fmt == 0) {
+      *reinterpret_cast<float4 *>((float *)S.base + i0) = u4;
+    } else if (S.fmt == 1) {
+      const float vmax = S.slab[iy];
+      uint16_t c[4] = {0, 0, 0, 0};
+      if (vmax > 1e-25f)
+#pragma unroll
+        for (int k = 0; k < 4; k++) c[k] = c16_encode(uv[k] * __frcp_rn(vmax));
+      uint32_t *w = reinterpret_cast<uint32_t *>((uint16_t *)S.base + (long long)iy * (g.nxz + 2) + 2 + col);
+      w[0] = (uint32_t)c[0] | ((uint32_t)c[1] << 16);
+      w[1] = (uint32_t)c[2] | ((uint32_t)c[3] << 16);
+    } else {
+      const float sc = S.slab[iy];
+      __half2 h[2] = {__halves2half2(slab16_encode(uv[0], sc), slab16_encode(uv[1], sc)),
+                      __halves2half2(slab16_encode(uv[2], sc), slab16_encode(uv[3], sc))};
+      *reinterpret_cast<uint2 *>((__half *)S.base + i0) = *reinterpret_cast<uint2 *>(h);
+    }
+  }
+  if (io.ic) {
+    const SnapDev &S = io.src;
+    float sv[4];
+    if (S.fmt == 0) {
+      const float4 v = *reinterpret_cast<const float4 *>((const float *)S.base + i0);
+      sv[0] = v.x, sv[1] = v.y, sv[2] = v.z, sv[3] = v.w;
+    } else if (S.fmt == 1) {
+      const uint32_t *w = reinterpret_cast<const uint32_t *>((const uint16_t *)S.base + (long long)iy * (g.nxz + 2) + 2 + col);
+      const uint32_t a = w[0], b = w[1];
+      const float sl = S.slab[iy];
+      sv[0] = sl * c16_table((uint16_t)(a & 0xffff)), sv[1] = sl * c16_table((uint16_t)(a >> 16));
+      sv[2] = sl * c16_table((uint16_t)(b & 0xffff)), sv[3] = sl * c16_table((uint16_t)(b >> 16));
+    } else {
+      const uint2 hv = *reinterpret_cast<const uint2 *>((const __half *)S.base + i0);
+      const __half2 h0 = *reinterpret_cast<const __half2 *>(&hv.x), h1 = *reinterpret_cast<const __half2 *>(&hv.y);
+      const float sl = S.slab[iy];
+      sv[0] = slab16_decode(__low2half(h0), sl), sv[1] = slab16_decode(__high2half(h0), sl);
+      sv[2] = slab16_decode(__low2half(h1), sl), sv[3] = slab16_decode(__high2half(h1), sl);
+    }
+    float4 img = *reinterpret_cast<const float4 *>(io.image + i0), cmp = *reinterpret_cast<const float4 *>(io.comp + i0);
+    const float ey = io.ey[iy], ex = io.ex[ix];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int iz = iz4 + k;
+      float s = sv[k] * ey;
+      s = s * ex;
+      s = s * io.ez[iz];
+      if (io.use_t) s = s * io.tscale;
+      else s = s * io.taper_z[iz];
+      float r = uv[k] * ey;
+      r = r * ex;
+      r = r * io.ez[iz];
+      const float prod = s * r;
+      const float im = io4_get(img, k);
+      const float y = prod - io4_get(cmp, k);
+      const float t = im + y;
+      io4_set(cmp, k, (t - im) - y);
+      io4_set(img, k, t);
+    }
+    *reinterpret_cast<float4 *>(io.comp + i0) = cmp;
+    *reinterpret_cast<float4 *>(io.image + i0) = img;
   }
 }
 
