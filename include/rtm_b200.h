@@ -93,13 +93,14 @@ typedef struct rtm_config {
   int state_fp16;     /* 0: FP32 wavefield state (default); 1: FP16 w0 / w1 with a per-y-slab scale
                          (stencils, PML, Q memory and image in FP32), FD8 VTI / TTI (+Q) only, loop
                          drivers only (the stepwise seam calls return RTM_ERR_UNSUPPORTED) */
-  int kernel_variant; /* 0: auto (ISO FD8: 4 z cells per thread with TMA rings when nz % 4 == 0,
-                         the autotuner picks among all ISO kernels; compact FD: register-streamed
-                         x / y line solves, the autotuner may pick TMA tiles), 1: register
-                         pipeline / plain staged tiles, 2: compact-FD x / y TMA tiles, ISO FD8 TMA
-                         plane pipeline, 3: ISO FD8 4 z cells per thread with TMA rings, 4: ISO
-                         FD8 4 z cells per thread with register prefetch (ISO variants fall back
-                         to 1 when nz % 4 != 0) */
+  int kernel_variant; /* 0: auto (FD8: 4 z cells per thread with TMA rings when nz % 4 == 0 and,
+                         for VTI / TTI, the state is FP32; the autotuner picks among all FD8
+                         kernels; compact FD: register-streamed x / y line solves, the autotuner
+                         may pick TMA tiles), 1: one cell per thread / plain staged tiles, 2:
+                         compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline, 3: FD8 4 z
+                         cells per thread with TMA rings, 4: ISO FD8 4 z cells per thread with
+                         register prefetch (the 4-cell variants fall back to 1 when they do not
+                         apply) */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;
@@ -312,7 +313,8 @@ int rtm_selftest_bounded_wait(rtm_handle *h);
 int rtm_autotune(rtm_handle *h, int steps, int *choice);
 /* Candidate `idx` of the last rtm_autotune: desc[0] kernel family (0 one cell
  * per thread / FD8 two-pass / compact FD, 1 ISO 4 z cells with register
- * prefetch, 2 ISO 4 z cells with TMA rings, 3 ISO one-cell TMA pipeline),
+ * prefetch, 2 ISO 4 z cells with TMA rings, 3 ISO one-cell TMA pipeline,
+ * 4 FD8 VTI / TTI 4 z cells with TMA rings),
  * desc[1] its tile width or shape index, desc[2] its y segment (0: default),
  * desc[3] the compact-FD x / y kernel; *ms the time of its `steps` steps.
  * RTM_ERR_ARG when idx is out of range. */

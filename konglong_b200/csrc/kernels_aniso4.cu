@@ -467,9 +467,7 @@ __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 384 / (8 * TX) : 0
 #pragma unroll
         for (int c = 0; c < 4; c++) set4(out4, c, __fsub_rn(__fadd_rn(cmp4(cw1, c), cmp4(cw1, c)), cmp4(t4, c)));
       } else {
-#pragma unroll
-        for (int c = 0; c < 4; c++)
-          set4(out4, c, q_update(a.q, i0 + c, (long long)ny * g.nxz, cmp4(t4, c), cmp4(cw1, c)));
+        out4 = q_update4(a.q, i0, (long long)ny * g.nxz, t4, cw1);
       }
       st4(a.w0 + i0, out4);
     }

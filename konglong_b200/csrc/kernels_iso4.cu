@@ -132,38 +132,6 @@ __device__ __noinline__ float4 iso4_pml4(const PmlDev &P, Grid3 g, float4 lz, fl
   return v;
 }
 
-// Visco-acoustic update (q_update) of the thread's 4 cells: the memory
-// variables of up to 4 orders are loaded before any is computed or written.
-__device__ __noinline__ float4 iso4_q4(const QDev &Q, long long i, long long n, float4 t, float4 u) {
-  const float4 iq = *reinterpret_cast<const float4 *>(Q.invq + i);
-  const float uv[4] = {u.x, u.y, u.z, u.w}, iv[4] = {iq.x, iq.y, iq.z, iq.w};
-  float v[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-  for (int c = 0; c < 4; c++) v[c] = q_init(uv[c], iv[c], Q.cqsum, v[c]);
-  for (int l0 = 0; l0 < Q.order; l0 += 4) {
-    float4 d0[4], d1[4];
-#pragma unroll
-    for (int l = 0; l < 4; l++)
-      if (l0 + l < Q.order) {
-        d0[l] = *reinterpret_cast<const float4 *>(Q.d0 + (long long)(l0 + l) * n + i);
-        d1[l] = *reinterpret_cast<const float4 *>(Q.d1 + (long long)(l0 + l) * n + i);
-      }
-#pragma unroll
-    for (int c = 0; c < 4; c++)
-#pragma unroll
-      for (int l = 0; l < 4; l++)
-        if (l0 + l < Q.order) {
-          const float e0 = comp(d0[l], c), e1 = comp(d1[l], c);
-          const float el = Q.wq[l0 + l];
-          v[c] = q_acc(v[c], iv[c], el, e0, e1);
-          setc(d0[l], c, q_next(Q.cq[l0 + l], uv[c], el, e0));
-        }
-#pragma unroll
-    for (int l = 0; l < 4; l++)
-      if (l0 + l < Q.order) *reinterpret_cast<float4 *>(Q.d0 + (long long)(l0 + l) * n + i) = d0[l];
-  }
-  return make_float4(v[0], v[1], v[2], v[3]);
-}
 
 template <int TX, int MODE, bool PML3D>
 __global__ void __launch_bounds__(8 * TX) iso_fd8_v4(const __grid_constant__ IsoArgs a) {
@@ -288,7 +256,7 @@ __global__ void __launch_bounds__(8 * TX) iso_fd8_v4(const __grid_constant__ Iso
       if (MODE == 0) out4 = t4;  // KernelCPU seam: w0 -= vel * L[w1]
       else if (MODE == 1)        // + update2nd (leapfrog)
         out4 = make_float4((u4.x + u4.x) - t4.x, (u4.y + u4.y) - t4.y, (u4.z + u4.z) - t4.z, (u4.w + u4.w) - t4.w);
-      else out4 = iso4_q4(a.q, i0, (long long)ny * g.nxz, t4, u4);  // + Q
+      else out4 = q_update4(a.q, i0, (long long)ny * g.nxz, t4, u4);  // + Q
       w0[plane4 + col4] = out4;
     }
   };
@@ -611,7 +579,7 @@ __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 512 / (8 * TX) : 0
       if (MODE == 0) out4 = t4;
       else if (MODE == 1)
         out4 = make_float4((u4.x + u4.x) - t4.x, (u4.y + u4.y) - t4.y, (u4.z + u4.z) - t4.z, (u4.w + u4.w) - t4.w);
-      else out4 = iso4_q4(a.q, i0, (long long)ny * g.nxz, t4, u4);
+      else out4 = q_update4(a.q, i0, (long long)ny * g.nxz, t4, u4);
       reinterpret_cast<float4 *>(a.w0)[i0 / 4] = out4;
     }
     if (qx1) qx1 += stx, qx2 += stx;

@@ -485,4 +485,37 @@ __device__ __forceinline__ float q_update(const QDev &Q, long long i, long long 
   return v;
 }
 
+// Visco-acoustic update (q_update) of the thread's 4 cells: the memory
+// variables of up to 4 orders are loaded before any is computed or written.
+static __device__ __noinline__ float4 q_update4(const QDev &Q, long long i, long long n, float4 t, float4 u) {
+  const float4 iq = *reinterpret_cast<const float4 *>(Q.invq + i);
+  const float uv[4] = {u.x, u.y, u.z, u.w}, iv[4] = {iq.x, iq.y, iq.z, iq.w};
+  float v[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+  for (int c = 0; c < 4; c++) v[c] = q_init(uv[c], iv[c], Q.cqsum, v[c]);
+  for (int l0 = 0; l0 < Q.order; l0 += 4) {
+    float4 d0[4], d1[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      if (l0 + l < Q.order) {
+        d0[l] = *reinterpret_cast<const float4 *>(Q.d0 + (long long)(l0 + l) * n + i);
+        d1[l] = *reinterpret_cast<const float4 *>(Q.d1 + (long long)(l0 + l) * n + i);
+      }
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+      for (int l = 0; l < 4; l++)
+        if (l0 + l < Q.order) {
+          const float e0 = io4_get(d0[l], c), e1 = io4_get(d1[l], c);
+          const float el = Q.wq[l0 + l];
+          v[c] = q_acc(v[c], iv[c], el, e0, e1);
+          io4_set(d0[l], c, q_next(Q.cq[l0 + l], uv[c], el, e0));
+        }
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      if (l0 + l < Q.order) *reinterpret_cast<float4 *>(Q.d0 + (long long)(l0 + l) * n + i) = d0[l];
+  }
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
 }  // namespace rtm

@@ -38,9 +38,9 @@ class PropSpec:
     pml3d_scaler: float = 0.3
     top_pml: bool = True
     state_fp16: bool = False
-    kernel_variant: int = 0       # 0 auto, 1 register pipeline / plain tiles, 2 TMA (CFD x/y tiles,
-                                  # ISO plane pipeline), 3 / 4 ISO 4 z cells per thread (TMA rings /
-                                  # register prefetch)
+    kernel_variant: int = 0       # 0 auto, 1 one cell per thread / plain tiles, 2 TMA (CFD x/y tiles,
+                                  # ISO one-cell plane pipeline), 3 FD8 4 z cells per thread with TMA
+                                  # rings, 4 ISO 4 z cells with register prefetch
 
     @property
     def n(self):
