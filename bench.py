@@ -218,6 +218,8 @@ def run_cuda(args, rank, world):
     p.set_model(**shot.model_arrays())
     nslots = (2 * K + Wm) // shot.interval + 2
     p.snapshot_setup(snap_fmt, nslots)
+    if args.snap_offload:
+        p.snapshot_offload(args.snap_offload)
     p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
     tuned = p.autotune(3) if not args.no_autotune else None
     p.reset()
@@ -296,6 +298,8 @@ def run_cuda(args, rank, world):
     cfg["autotuned_shape"] = tuned
     cfg["kernel_variant"] = args.kernel_variant
     cfg["state"] = "fp16 per-slab scale" if s.state_fp16 else "fp32"
+    if args.snap_offload:
+        cfg["snapshots"] = f"pinned host memory, {args.snap_offload} device staging slots"
     return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
                 config=cfg, shot=shot, launches=launches)
 
@@ -449,6 +453,8 @@ def main():
                     help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiler runs: timings under a profiler mislead the tuner)")
+    ap.add_argument("--snap-offload", type=int, default=0,
+                    help="keep the snapshots in pinned host memory with this many device staging slots")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

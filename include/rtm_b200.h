@@ -185,6 +185,14 @@ int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots);
 int rtm_snapshot_store(rtm_handle *h, int slot);
 /* Decode slot into dst (host, N floats) with the reference's decode tapers. */
 int rtm_snapshot_load(rtm_handle *h, int slot, float *dst);
+/* Snapshot offload (CacheFile / AsyncIO / WaveFieldHolder spill,
+ * bgprtm/CacheFile.cpp:32-109, bgprtm/WaveFieldHolder.cpp:50-77): after
+ * rtm_snapshot_setup, moves the slots to pinned host memory and keeps nstage
+ * (2..8) device slots that stage them; the forward loop copies each stored
+ * snapshot to the host while the next steps run, the backward loop fetches
+ * slots ahead of the imaging condition.  Clears the slots; nstage = 0 returns
+ * to device slots.  FP32, COMPRESS_16 and FP16 formats. */
+int rtm_snapshot_offload(rtm_handle *h, int nstage);
 
 /* Imaging condition set-up: ntaper_t source time-taper snapshots, ntaper_z
  * depth-taper cells (ImagingCondition::calTapes), edge_taper=1 applies the

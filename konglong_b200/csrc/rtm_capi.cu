@@ -77,6 +77,16 @@ struct Engine {
   int snap_fmt = 0, nslots = 0;
   size_t slot_bytes = 0;
   char *snaps = nullptr;
+  // snapshot offload (rtm_snapshot_offload): the slots live in pinned host memory and
+  // `nstage` device slots (snaps) stage them; slot s uses staging slot s % nstage.
+  // Copies run on st_copy, forked from st by events and joined back before every
+  // graph capture ends; stage_ev[k] marks the last copy into / out of staging slot k.
+  char *host_snaps = nullptr;
+  int nstage = 0;
+  cudaStream_t st_copy = nullptr;
+  cudaEvent_t ev_fork = nullptr, stage_ev[8] = {};
+  int stage_slot[8] = {};  // slot a staging buffer holds (-1: none)
+  bool stage_wait[8] = {};  // st has not yet waited for the last copy into / out of it
   float *slabs = nullptr;  // [nslots][ny]
   std::vector<char> stored;
   // imaging
@@ -719,7 +729,7 @@ static float *f16_view(Engine *h, int which) {
 static SnapDev slot_dev(Engine *h, int slot) {
   SnapDev s{};
   s.fmt = h->snap_fmt;
-  s.base = h->snaps + (size_t)slot * h->slot_bytes;
+  s.base = h->snaps + (size_t)(h->nstage ? slot % h->nstage : slot) * h->slot_bytes;
   s.slab = h->slabs ? h->slabs + (size_t)slot * h->d.ny : nullptr;
   return s;
 }
@@ -784,14 +794,57 @@ static int snap_prepare(Engine *h, int slot) {
   return check_launch(h, "slab_max");
 }
 
+// ---- snapshot offload: copies between host slots and device staging slots ----
+// (all on st_copy; st forks to it with ev_fork and waits for stage_ev[k])
+static int stage_fork(Engine *h) {
+  CK(cudaEventRecord(h->ev_fork, h->st));
+  CK(cudaStreamWaitEvent(h->st_copy, h->ev_fork, 0));
+  return RTM_OK;
+}
+// slot s (just written to its staging slot by work already on st) to the host
+static int offload_d2h(Engine *h, int s) {
+  const int k = s % h->nstage;
+  TRY(stage_fork(h));
+  CK(cudaMemcpyAsync(h->host_snaps + (size_t)s * h->slot_bytes, h->snaps + (size_t)k * h->slot_bytes, h->slot_bytes,
+                     cudaMemcpyDeviceToHost, h->st_copy));
+  CK(cudaEventRecord(h->stage_ev[k], h->st_copy));
+  h->stage_slot[k] = -1, h->stage_wait[k] = true;
+  return RTM_OK;
+}
+// slot s from the host into its staging slot (after every kernel already on st)
+static int offload_h2d(Engine *h, int s) {
+  const int k = s % h->nstage;
+  TRY(stage_fork(h));
+  CK(cudaMemcpyAsync(h->snaps + (size_t)k * h->slot_bytes, h->host_snaps + (size_t)s * h->slot_bytes, h->slot_bytes,
+                     cudaMemcpyHostToDevice, h->st_copy));
+  CK(cudaEventRecord(h->stage_ev[k], h->st_copy));
+  h->stage_slot[k] = s, h->stage_wait[k] = true;
+  return RTM_OK;
+}
+// st waits for the last copy into / out of the staging slot of s
+static int stage_ready(Engine *h, int s) {
+  const int k = s % h->nstage;
+  if (h->stage_wait[k]) CK(cudaStreamWaitEvent(h->st, h->stage_ev[k], 0));
+  h->stage_wait[k] = false;
+  return RTM_OK;
+}
+// join every copy back into st (before a graph capture ends, and after a loop)
+static int stage_join(Engine *h) {
+  if (!h->nstage) return RTM_OK;
+  for (int k = 0; k < h->nstage; k++) TRY(stage_ready(h, k));
+  return RTM_OK;
+}
+
 // Runs fn(step index) for `count` steps inside CUDA graphs of up to `chunk`
-// steps each, timed with events on the engine's stream.
+// steps each, timed with events on the engine's stream; every snapshot copy
+// forked from the engine stream is joined back before a capture ends.
 template <typename F> static int run_graphs(Engine *h, int count, F fn) {
   const int chunk = 256;
   h->launches = 0;
   CK(cudaEventRecord(h->ev0, h->st));
   if (h->prof_on) {  // eager launches bracketed by events (no graph)
     for (int s = 0; s < count; s++) TRY(fn(s));
+    TRY(stage_join(h));
     CK(cudaEventRecord(h->ev1, h->st));
     CK(cudaEventSynchronize(h->ev1));
     CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
@@ -804,6 +857,7 @@ template <typename F> static int run_graphs(Engine *h, int count, F fn) {
     CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     int rc = RTM_OK;
     for (int s = s0; s < s1 && rc == RTM_OK; s++) rc = fn(s);
+    if (rc == RTM_OK) rc = stage_join(h);
     cudaError_t ec = cudaStreamEndCapture(h->st, &g);
     if (rc != RTM_OK) {
       if (g) cudaGraphDestroy(g);
@@ -1103,6 +1157,12 @@ int rtm_destroy(rtm_handle *h) {
   cudaStreamSynchronize(h->st);
   for (void *p : h->allocs) cudaFree(p);
   h->allocs.clear();
+  if (h->st_copy) cudaStreamSynchronize(h->st_copy);
+  if (h->host_snaps) cudaFreeHost(h->host_snaps);
+  for (cudaEvent_t e : h->stage_ev)
+    if (e) cudaEventDestroy(e);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->st_copy) cudaStreamDestroy(h->st_copy);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->st) cudaStreamDestroy(h->st);
@@ -1442,6 +1502,9 @@ int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots) {
     return RTM_ERR_STATE;
   }
   cudaSetDevice(h->device);
+  if (h->st_copy) cudaStreamSynchronize(h->st_copy);
+  if (h->host_snaps) cudaFreeHost(h->host_snaps);
+  h->host_snaps = nullptr, h->nstage = 0;
   h->release(h->snaps), h->release(h->slabs), h->release(h->ae_scratch);
   h->snaps = nullptr, h->slabs = nullptr, h->ae_scratch = nullptr;
   h->snap_fmt = fmt, h->nslots = nslots;
@@ -1469,6 +1532,38 @@ int rtm_set_compressor(rtm_handle *h, rtm_ae *a) {
   return RTM_OK;
 }
 
+int rtm_snapshot_offload(rtm_handle *h, int nstage) {
+  if (!h || nstage < 0 || nstage == 1 || nstage > 8) return RTM_ERR_ARG;
+  if (nstage && h->snap_fmt == RTM_SNAP_AE) {
+    h->err = "snapshot offload stores the FP32 / COMPRESS_16 / FP16 formats";
+    return RTM_ERR_UNSUPPORTED;
+  }
+  cudaSetDevice(h->device);
+  if (!h->st_copy) {
+    if (cudaStreamCreateWithFlags(&h->st_copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+      return rtm::cuda_fail(cudaGetLastError(), "snapshot offload streams", h);
+    for (cudaEvent_t &e : h->stage_ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        return rtm::cuda_fail(cudaGetLastError(), "snapshot offload events", h);
+  }
+  const int fmt = h->snap_fmt, nslots = h->nslots;
+  TRY(rtm_snapshot_setup(h, fmt, nslots));  // drops any previous slots and their contents
+  if (!nstage || !nslots) return RTM_OK;
+  h->release(h->snaps);
+  h->snaps = nullptr;
+  TRY(h->alloc(h->snaps, h->slot_bytes * nstage));
+  if (cudaHostAlloc((void **)&h->host_snaps, h->slot_bytes * nslots, cudaHostAllocDefault) != cudaSuccess) {
+    h->host_snaps = nullptr;
+    h->err = "cudaHostAlloc of " + std::to_string(h->slot_bytes * nslots) + " bytes failed";
+    cudaGetLastError();
+    return RTM_ERR_NOMEM;
+  }
+  h->nstage = nstage;
+  for (int k = 0; k < 8; k++) h->stage_slot[k] = -1, h->stage_wait[k] = false;
+  return RTM_OK;
+}
+
 int rtm_snapshot_store(rtm_handle *h, int slot) {
   TRY(rtm::ready(h));
   if (h->f16) {
@@ -1476,12 +1571,17 @@ int rtm_snapshot_store(rtm_handle *h, int slot) {
     return RTM_ERR_UNSUPPORTED;
   }
   if (slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
+  if (h->nstage) TRY(rtm::stage_ready(h, slot));
   if (h->snap_fmt == RTM_SNAP_AE) {
     TRY(rtm::ae_store(h, slot, h->w0));
   } else {
     TRY(rtm::snap_prepare(h, slot));
     rtm::launch_fused_io(rtm::io_store(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
     TRY(rtm::check_launch(h, "snapshot_store"));
+  }
+  if (h->nstage) {
+    TRY(rtm::offload_d2h(h, slot));
+    TRY(rtm::stage_join(h));
   }
   h->stored[slot] = 1;
   CK(cudaStreamSynchronize(h->st));
@@ -1491,6 +1591,11 @@ int rtm_snapshot_store(rtm_handle *h, int slot) {
 int rtm_snapshot_load(rtm_handle *h, int slot, float *dst) {
   if (!h || !dst || slot < 0 || slot >= h->nslots) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
+  if (h->nstage) {
+    TRY(rtm::stage_join(h));
+    TRY(rtm::offload_h2d(h, slot));
+    TRY(rtm::stage_ready(h, slot));
+  }
   float *tmp = nullptr;
   TRY(h->alloc(tmp, h->n));
   int rc;
@@ -1537,6 +1642,10 @@ int rtm_image_accumulate(rtm_handle *h, int slot) {
   TRY(rtm::ready(h));
   if (slot < 0 || slot >= h->nslots || !h->image) return RTM_ERR_ARG;
   if (!h->stored[slot]) return RTM_OK;
+  if (h->nstage) {
+    TRY(rtm::offload_h2d(h, slot));
+    TRY(rtm::stage_ready(h, slot));
+  }
   rtm::launch_fused_io(rtm::io_image(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
   TRY(rtm::check_launch(h, "image_accumulate"));
   CK(cudaStreamSynchronize(h->st));
@@ -1568,10 +1677,13 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
   if (count < 0) return RTM_ERR_ARG;
   const int mode = h->c.use_q ? 2 : 1;
   rtm::FusedIo pending = rtm::io_none();
+  int pending_slot = -1;  // slot the pending store writes (offload: copied to the host after it)
+  const bool off = h->nstage > 0;
   int rc = rtm::run_graphs(h, count, [&](int s) {
     const int it = it_begin + s * inc;
     TRY(rtm::step_kernel(h, mode, pending));
-    pending = rtm::io_none();
+    if (off && pending.store) TRY(rtm::offload_d2h(h, pending_slot));
+    pending = rtm::io_none(), pending_slot = -1;
     TRY(rtm::do_inject(h, it + it_shift * inc));
     if (it % interval == 0) {
       const int slot = it / interval;
@@ -1580,8 +1692,9 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
           if (h->snap_fmt == RTM_SNAP_AE) {
             TRY(rtm::ae_store(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
           } else {
+            if (off) TRY(rtm::stage_ready(h, slot));  // its staging slot's previous copy is done
             TRY(rtm::snap_prepare(h, slot));
-            pending = rtm::io_store(h, slot);
+            pending = rtm::io_store(h, slot), pending_slot = slot;
           }
           h->stored[slot] = 1;
         } else if (h->stored[slot]) {
@@ -1589,6 +1702,16 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
             TRY(rtm::ae_load(h, slot, h->ae_scratch));
             pending = rtm::io_image_ae(h, slot);
           } else {
+            if (off) {
+              // this slot in its staging slot before the next kernel reads it, then
+              // the next slots (consumed in decreasing order) fetched ahead
+              if (h->stage_slot[slot % h->nstage] != slot) TRY(rtm::offload_h2d(h, slot));
+              TRY(rtm::stage_ready(h, slot));
+              for (int a = 1; a < h->nstage && slot - a >= 0; a++) {
+                const int sn = slot - a;
+                if (h->stored[sn] && h->stage_slot[sn % h->nstage] != sn) TRY(rtm::offload_h2d(h, sn));
+              }
+            }
             pending = rtm::io_image(h, slot);
           }
         }
@@ -1602,6 +1725,8 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
     rtm::KScope k(h, RTM_K_IO);
     rtm::launch_fused_io(pending, h->f16 ? rtm::f16_view(h, 1) : h->w1, h->d.nx, h->d.ny, h->d.nz, h->st);
     TRY(rtm::check_launch(h, "fused_io(last)"));
+    if (off && pending.store) TRY(rtm::offload_d2h(h, pending_slot));
+    TRY(rtm::stage_join(h));
     CK(cudaStreamSynchronize(h->st));
   }
   return RTM_OK;

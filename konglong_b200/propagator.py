@@ -153,6 +153,10 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def snapshot_offload(self, nstage):
+        """Keep the snapshot slots in pinned host memory with `nstage` device staging slots (0: device slots)."""
+        self._ck(self.L.rtm_snapshot_offload(self.h, int(nstage)), "rtm_snapshot_offload")
+
     def autotune_results(self):
         """[(family, shape, yseg, cfd_xy, ms)] of the candidates the last autotune timed."""
         out, k = [], 0
