@@ -70,7 +70,8 @@ enum {
   RTM_FIELD_W1 = 1,  /* previous wavefield (read by the stencil) */
   RTM_FIELD_VEL = 2, /* (v*dt)^2 after Vel2 */
   RTM_FIELD_IMAGE = 3,
-  RTM_FIELD_INVQ = 4 /* invQ after the Vel2 correction */
+  RTM_FIELD_INVQ = 4, /* invQ after the Vel2 correction */
+  RTM_FIELD_ILLUM = 5 /* source illumination, or its damping factor after rtm_illum_compensate */
 };
 
 typedef struct rtm_dims {
@@ -201,6 +202,17 @@ int rtm_snapshot_offload(rtm_handle *h, int nstage);
 int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge_taper);
 /* image += T(src[slot]) * T(w0), zero lag, Kahan-compensated FP32. */
 int rtm_image_accumulate(rtm_handle *h, int slot);
+/* Source illumination (ImagingCondition::calIllum, bgprtm/ImagingCondition.cpp:143-149):
+ * on = 1 allocates and zeroes a volume that every later imaging-condition term adds the
+ * squared source value to (after the time / depth and edge tapers); on = 0 stops. */
+int rtm_illum_setup(rtm_handle *h, int on);
+/* Shot illumination compensation (ShotIllumComp, ImagingCondition::computeDamping +
+ * applyDamping, bgprtm/ImagingCondition.cpp:600-689): box-smooths the illumination
+ * (half widths smooth_xy, smooth_z; avgVolume3D, both 0 = no smoothing), turns it into the
+ * damping factor 1 / (avg (a + damp_weight e^-a)), a = illum / avg, avg = mean^amp_damping,
+ * with 10-cell x / y edge tapers, and multiplies the image by it.  Reference defaults:
+ * 10, 10, 1.0, 0.07. */
+int rtm_illum_compensate(rtm_handle *h, int smooth_xy, int smooth_z, float amp_damping, float damp_weight);
 
 /* Propagator::modelling loop (bgprtm/Propagator.cpp:1099-1153): for it in
  * [0, nts): kernel, update2nd, inject(it + it_shift), extract(it / ntratio)

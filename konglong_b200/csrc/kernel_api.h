@@ -152,6 +152,12 @@ void launch_grad4(const GradArgs &a, const Tile4 *tiles, int ntiles, bool edge, 
 void launch_div4(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, int mode, const Div4Maps &m, int *err,
                  cudaStream_t st);
 
+// shot illumination compensation: optional box smoothing (half widths hxy, hz),
+// damping factor from the mean (dsum: one double of scratch), image *= factor;
+// tmp: one volume of scratch
+void launch_illum_compensate(float *illum, float *tmp, float *image, double *dsum, int nx, int ny, int nz, int smooth,
+                             int hxy, int hz, float amp_damping, float damp_weight, cudaStream_t st);
+
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {
   int n;

@@ -506,4 +506,94 @@ void launch_nonfinite_scan(const float *w, long long n, int *flag, cudaStream_t 
   nonfinite_k<<<grid_for(n, 256), 256, 0, st>>>(w, n, flag);
 }
 
+// ---- shot illumination compensation (ImagingCondition::computeDamping /
+// applyDamping, bgprtm/ImagingCondition.cpp:600-677; avgVolume3D / avgVolume1D,
+// bgprtm/volumefilter.cpp:59-135) --------------------------------------------
+
+namespace {
+
+// Running box average of half width h along one axis of every line (one thread
+// per line, the reference's order: edge value counted h+1 times, then one add
+// and one subtract per step).  Line t: axis 0 = y (lines over x, z), 1 = x
+// (lines over y, z), 2 = z (lines over y, x).
+__global__ void box_avg_k(const float *__restrict__ a, float *__restrict__ b, int axis, int nx, int ny, int nz, int h) {
+  const long long nxz = (long long)nx * nz;
+  const long long nl = axis == 0 ? nxz : axis == 1 ? (long long)ny * nz : (long long)ny * nx;
+  const float scaler = 1.0f / (2.0f * h + 1.0f);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nl; t += (long long)gridDim.x * blockDim.x) {
+    long long base, stride;
+    int n1;
+    if (axis == 0) base = t, stride = nxz, n1 = ny;
+    else if (axis == 1) base = (t / nz) * nxz + t % nz, stride = nz, n1 = nx;
+    else base = t * nz, stride = 1, n1 = nz;
+    float m = __fmul_rn((float)h + 1.0f, a[base]);
+    for (int j = 1; j <= h; j++) m = __fadd_rn(m, a[base + (long long)min(j, n1 - 1) * stride]);
+    b[base] = __fmul_rn(m, scaler);
+    for (int k = 1; k < n1; k++) {
+      const int k1 = max(0, k - h - 1), k2 = min(n1 - 1, k + h);
+      m = __fadd_rn(m, __fsub_rn(a[base + (long long)k2 * stride], a[base + (long long)k1 * stride]));
+      b[base + (long long)k * stride] = __fmul_rn(m, scaler);
+    }
+  }
+}
+
+__global__ void sum_k(const float *__restrict__ a, long long n, double *out) {
+  double v = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v += a[i];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(out, v);
+  }
+}
+
+// damping factor 1 / (avg (a + w e^-a)), a = illum / avg, x / y edge tapers,
+// then image *= factor; the factor stays in illum
+__global__ void damping_k(float *__restrict__ illum, float *__restrict__ image, const double *sum, double count,
+                          float amp_damping, float damp_weight, int nx, int ny, int nz) {
+  const long long nxz = (long long)nx * nz, n = nxz * ny;
+  const double average = pow(*sum / count, (double)amp_damping), o_average = 1.0 / average;
+  const int ntaper = 10;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(i / nxz), ix = (int)((i % nxz) / nz);
+    const float aa = (float)(illum[i] * o_average);
+    const float bb = expf(-aa);
+    float f = (float)(1.0 / (average * (double)__fadd_rn(aa, __fmul_rn(damp_weight, bb))));
+    auto wt = [&](int k) { return 0.5f * (1.0f - cosf((float)M_PI * float(k) / float(ntaper))); };
+    if (iy < ntaper && ny > 1) f *= wt(iy);
+    if (iy > ny - ntaper - 1 && ny > 1) f *= wt(ny - iy - 1);
+    if (ix < ntaper) f *= wt(ix);
+    if (ix > nx - ntaper - 1) f *= wt(nx - ix - 1);
+    illum[i] = f;
+    if (image) image[i] *= f;
+  }
+}
+
+}  // namespace
+
+void launch_illum_compensate(float *illum, float *tmp, float *image, double *dsum, int nx, int ny, int nz, int smooth,
+                             int hxy, int hz, float amp_damping, float damp_weight, cudaStream_t st) {
+  const long long nxz = (long long)nx * nz, n = nxz * ny;
+  auto lines = [&](int axis) { return axis == 0 ? nxz : axis == 1 ? (long long)ny * nz : (long long)ny * nx; };
+  if (smooth) {  // avgVolume3D for ny > 1 (y, x, z), avgVolume2D otherwise (x, z)
+    if (ny > 1) {
+      box_avg_k<<<grid_for(lines(0), 256), 256, 0, st>>>(illum, tmp, 0, nx, ny, nz, hxy);
+      box_avg_k<<<grid_for(lines(1), 256), 256, 0, st>>>(tmp, illum, 1, nx, ny, nz, hxy);
+    } else {
+      box_avg_k<<<grid_for(lines(1), 256), 256, 0, st>>>(illum, tmp, 1, nx, ny, nz, hxy);
+      cudaMemcpyAsync(illum, tmp, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    }
+    box_avg_k<<<grid_for(lines(2), 256), 256, 0, st>>>(illum, tmp, 2, nx, ny, nz, hz);
+    cudaMemcpyAsync(illum, tmp, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
+  }
+  cudaMemsetAsync(dsum, 0, sizeof(double), st);
+  sum_k<<<1184, 256, 0, st>>>(illum, n, dsum);
+  damping_k<<<grid_for(n, 256), 256, 0, st>>>(illum, image, dsum, (double)n, amp_damping, damp_weight, nx, ny, nz);
+}
+
 }  // namespace rtm

@@ -81,6 +81,8 @@ struct Engine {
   // `nstage` device slots (snaps) stage them; slot s uses staging slot s % nstage.
   // Copies run on st_copy, forked from st by events and joined back before every
   // graph capture ends; stage_ev[k] marks the last copy into / out of staging slot k.
+  float *illum = nullptr;  // source illumination (rtm_illum_setup), accumulated by the imaging condition
+  int illum_on = 0;
   char *host_snaps = nullptr;
   int nstage = 0;
   cudaStream_t st_copy = nullptr;
@@ -754,6 +756,7 @@ static FusedIo io_image(Engine *h, int slot) {
   io.ex = h->ic_edge ? h->ex : h->one_x;
   io.ey = h->ic_edge ? h->ey : h->one_y;
   io.ez = h->ic_edge ? h->ez : h->one_z;
+  io.illum = h->illum_on ? h->illum : nullptr;
   return io;
 }
 
@@ -1634,6 +1637,34 @@ int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
   return RTM_OK;
 }
 
+int rtm_illum_setup(rtm_handle *h, int on) {
+  if (!h) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (on && !h->illum) TRY(h->alloc(h->illum, h->n));
+  if (h->illum) CK(cudaMemsetAsync(h->illum, 0, 4 * (size_t)h->n, h->st));
+  h->illum_on = on ? 1 : 0;
+  CK(cudaStreamSynchronize(h->st));
+  return RTM_OK;
+}
+
+int rtm_illum_compensate(rtm_handle *h, int smooth_xy, int smooth_z, float amp_damping, float damp_weight) {
+  if (!h || !h->illum || !h->image || smooth_xy < 0 || smooth_z < 0) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  float *tmp = nullptr;
+  double *dsum = nullptr;
+  int rc = h->alloc(tmp, h->n);
+  if (rc == RTM_OK) rc = h->alloc(dsum, 1);
+  if (rc == RTM_OK) {
+    rtm::launch_illum_compensate(h->illum, tmp, h->image, dsum, h->d.nx, h->d.ny, h->d.nz, smooth_xy > 0 || smooth_z > 0,
+                                 smooth_xy, smooth_z, amp_damping, damp_weight, h->st);
+    rc = rtm::check_launch(h, "illum_compensate");
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    if (rc == RTM_OK && e != cudaSuccess) rc = rtm::cuda_fail(e, "illum_compensate", h);
+  }
+  h->release(tmp), h->release(dsum);
+  return rc;
+}
+
 int rtm_image_accumulate(rtm_handle *h, int slot) {
   if (h && h->f16) {
     h->err = "the stepwise KernelCPU-seam calls do not run on FP16 wavefield state; use the loop drivers";
@@ -1739,7 +1770,8 @@ int rtm_get(rtm_handle *h, int field, float *dst) {
                      : field == RTM_FIELD_W1 ? (h->f16 ? rtm::f16_view(h, 1) : h->w1)
                      : field == RTM_FIELD_VEL ? h->vel
                      : field == RTM_FIELD_IMAGE ? h->image
-                     : field == RTM_FIELD_INVQ ? h->invq : nullptr;
+                     : field == RTM_FIELD_INVQ ? h->invq
+                     : field == RTM_FIELD_ILLUM ? h->illum : nullptr;
   if (!src) return RTM_ERR_ARG;
   CK(cudaMemcpyAsync(dst, src, 4 * (size_t)h->n, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));

@@ -352,6 +352,8 @@ __device__ __forceinline__ void fused_io(const FusedIo &io, const Grid3 &g, long
     s = s * io.ez[iz];
     if (io.use_t) s = s * io.tscale;
     else s = s * io.taper_z[iz];
+    // source illumination (ImagingCondition::calIllum, bgprtm/ImagingCondition.cpp:143-149)
+    if (io.illum) io.illum[i] = __fmaf_rn(s, s, io.illum[i]);
     float r = u * io.ey[iy];
     r = r * io.ex[ix];
     r = r * io.ez[iz];
@@ -420,6 +422,7 @@ __device__ __forceinline__ void fused_io4(const FusedIo &io, const Grid3 &g, lon
       sv[2] = slab16_decode(__low2half(h1), sl), sv[3] = slab16_decode(__high2half(h1), sl);
     }
     float4 img = *reinterpret_cast<const float4 *>(io.image + i0), cmp = *reinterpret_cast<const float4 *>(io.comp + i0);
+    float4 ill = io.illum ? *reinterpret_cast<const float4 *>(io.illum + i0) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float ey = io.ey[iy], ex = io.ex[ix];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -429,6 +432,7 @@ __device__ __forceinline__ void fused_io4(const FusedIo &io, const Grid3 &g, lon
       s = s * io.ez[iz];
       if (io.use_t) s = s * io.tscale;
       else s = s * io.taper_z[iz];
+      io4_set(ill, k, __fmaf_rn(s, s, io4_get(ill, k)));
       float r = uv[k] * ey;
       r = r * ex;
       r = r * io.ez[iz];
@@ -441,6 +445,7 @@ __device__ __forceinline__ void fused_io4(const FusedIo &io, const Grid3 &g, lon
     }
     *reinterpret_cast<float4 *>(io.comp + i0) = cmp;
     *reinterpret_cast<float4 *>(io.image + i0) = img;
+    if (io.illum) *reinterpret_cast<float4 *>(io.illum + i0) = ill;
   }
 }
 

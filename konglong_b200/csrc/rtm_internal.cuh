@@ -76,6 +76,7 @@ struct FusedIo {
   float tscale;
   const float *taper_z;     // [nz] depth taper (1 below), used when tscale == 0
   const float *ex, *ey, *ez;  // decode edge tapers per axis (1 inside)
+  float *illum;               // source illumination sum of s^2 (calIllum), null when off
 };
 
 struct QDev {

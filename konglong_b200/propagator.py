@@ -153,6 +153,15 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def illum_setup(self, on=True):
+        """Accumulate the source illumination (sum of squared source values) in the imaging condition."""
+        self._ck(self.L.rtm_illum_setup(self.h, int(bool(on))), "rtm_illum_setup")
+
+    def illum_compensate(self, smooth_xy=10, smooth_z=10, amp_damping=1.0, damp_weight=0.07):
+        """Shot illumination compensation of the image (reference defaults)."""
+        self._ck(self.L.rtm_illum_compensate(self.h, smooth_xy, smooth_z, amp_damping, damp_weight),
+                 "rtm_illum_compensate")
+
     def snapshot_offload(self, nstage):
         """Keep the snapshot slots in pinned host memory with `nstage` device staging slots (0: device slots)."""
         self._ck(self.L.rtm_snapshot_offload(self.h, int(nstage)), "rtm_snapshot_offload")
