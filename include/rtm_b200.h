@@ -65,6 +65,7 @@ enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1 };      /* FD::FD, FD::CFD */
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
 enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
+enum { RTM_IC_IMAGE1 = 0, RTM_IC_INVERSION = 1 }; /* ImagingCorrelator options IMAGE1, INVERSION */
 enum {
   RTM_FIELD_W0 = 0,  /* current/next wavefield (written by the step) */
   RTM_FIELD_W1 = 1,  /* previous wavefield (read by the stencil) */
@@ -202,6 +203,15 @@ int rtm_snapshot_offload(rtm_handle *h, int nstage);
 int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge_taper);
 /* image += T(src[slot]) * T(w0), zero lag, Kahan-compensated FP32. */
 int rtm_image_accumulate(rtm_handle *h, int slot);
+/* Imaging condition of the backward loop and of rtm_image_accumulate
+ * (ImagingCondition::getImagingOption, bgprtm/ImagingCondition.cpp:151-160):
+ * RTM_IC_IMAGE1 (default) the zero-lag correlation s r fused into the next step;
+ * RTM_IC_INVERSION (the reference's default LowcutFilter) s r - grad^ s . grad^ r with
+ * the normalised k-domain derivatives of both tapered fields
+ * (ImagingCorrelator::inversion1, bgprtm/ImagingCorrelator.cpp:374-424), computed with
+ * cuFFT at each imaging step.  The first INVERSION call creates the FFT plans and 4
+ * volumes + 3 spectra of scratch (call it before any stream capture). */
+int rtm_image_condition(rtm_handle *h, int option);
 /* Source illumination (ImagingCondition::calIllum, bgprtm/ImagingCondition.cpp:143-149):
  * on = 1 allocates and zeroes a volume that every later imaging-condition term adds the
  * squared source value to (after the time / depth and edge tapers); on = 0 stops. */

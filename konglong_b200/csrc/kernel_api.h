@@ -158,6 +158,16 @@ void launch_div4(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, in
 void launch_illum_compensate(float *illum, float *tmp, float *image, double *dsum, int nx, int ny, int nz, int smooth,
                              int hxy, int hz, float amp_damping, float damp_weight, cudaStream_t st);
 
+// INVERSION imaging condition (kernels_ic.cu): cuFFT plans, spectrum size in
+// floats, and one imaging term of source slot io.src against receiver field u
+// (S, Rv, Ds, Dr: volumes; Sh, Rh, Th: spectra); 0 or -1 (cuFFT failure)
+void *ic_plans_create(int nx, int ny, int nz);
+void ic_plans_destroy(void *plans);
+long long ic_spectrum_floats(int nx, int ny, int nz);
+int launch_ic_inversion(void *plans, const FusedIo &io, const float *u, float *S, float *Rv, float *Ds, float *Dr,
+                        float *Sh, float *Rh, float *Th, int nx, int ny, int nz, float dx, float dy, float dz,
+                        cudaStream_t st);
+
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {
   int n;

@@ -83,6 +83,12 @@ struct Engine {
   // graph capture ends; stage_ev[k] marks the last copy into / out of staging slot k.
   float *illum = nullptr;  // source illumination (rtm_illum_setup), accumulated by the imaging condition
   int illum_on = 0;
+  // imaging condition (rtm_image_condition): 0 zero-lag correlation fused into the
+  // step, 1 INVERSION with cuFFT derivatives (plans and scratch volumes / spectra)
+  int ic_opt = 0;
+  void *ic_plans = nullptr;
+  float *icS = nullptr, *icR = nullptr, *icDs = nullptr, *icDr = nullptr, *icSh = nullptr, *icRh = nullptr,
+        *icTh = nullptr;
   char *host_snaps = nullptr;
   int nstage = 0;
   cudaStream_t st_copy = nullptr;
@@ -782,6 +788,18 @@ static FusedIo io_image_ae(Engine *h, int slot) {
   return io;
 }
 
+// INVERSION imaging term of slot `slot` against receiver field u, at once
+static int ic_explicit(Engine *h, int slot, const float *u) {
+  const FusedIo io = h->snap_fmt == RTM_SNAP_AE ? io_image_ae(h, slot) : io_image(h, slot);
+  KScope k(h, RTM_K_IO, 10);
+  if (launch_ic_inversion(h->ic_plans, io, u, h->icS, h->icR, h->icDs, h->icDr, h->icSh, h->icRh, h->icTh, h->d.nx,
+                          h->d.ny, h->d.nz, h->d.dx, h->d.dy, h->d.dz, h->st)) {
+    h->err = "cuFFT execution failed";
+    return RTM_ERR_CUDA;
+  }
+  return check_launch(h, "ic_inversion");
+}
+
 // per-slot slab statistics for the 16-bit formats, taken on w0 after injection
 static int snap_prepare(Engine *h, int slot) {
   if (h->snap_fmt == RTM_SNAP_FP32 || h->snap_fmt == RTM_SNAP_AE) return RTM_OK;
@@ -1161,6 +1179,7 @@ int rtm_destroy(rtm_handle *h) {
   for (void *p : h->allocs) cudaFree(p);
   h->allocs.clear();
   if (h->st_copy) cudaStreamSynchronize(h->st_copy);
+  if (h->ic_plans) rtm::ic_plans_destroy(h->ic_plans);
   if (h->host_snaps) cudaFreeHost(h->host_snaps);
   for (cudaEvent_t e : h->stage_ev)
     if (e) cudaEventDestroy(e);
@@ -1637,6 +1656,28 @@ int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
   return RTM_OK;
 }
 
+int rtm_image_condition(rtm_handle *h, int option) {
+  if (!h || (option != RTM_IC_IMAGE1 && option != RTM_IC_INVERSION)) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (option == RTM_IC_INVERSION && !h->ic_plans) {
+    h->ic_plans = rtm::ic_plans_create(h->d.nx, h->d.ny, h->d.nz);
+    if (!h->ic_plans) {
+      h->err = "cuFFT plan creation failed";
+      return RTM_ERR_CUDA;
+    }
+    const long long nc = rtm::ic_spectrum_floats(h->d.nx, h->d.ny, h->d.nz);
+    TRY(h->alloc(h->icS, h->n));
+    TRY(h->alloc(h->icR, h->n));
+    TRY(h->alloc(h->icDs, h->n));
+    TRY(h->alloc(h->icDr, h->n));
+    TRY(h->alloc(h->icSh, (size_t)nc));
+    TRY(h->alloc(h->icRh, (size_t)nc));
+    TRY(h->alloc(h->icTh, (size_t)nc));
+  }
+  h->ic_opt = option;
+  return RTM_OK;
+}
+
 int rtm_illum_setup(rtm_handle *h, int on) {
   if (!h) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
@@ -1677,8 +1718,13 @@ int rtm_image_accumulate(rtm_handle *h, int slot) {
     TRY(rtm::offload_h2d(h, slot));
     TRY(rtm::stage_ready(h, slot));
   }
-  rtm::launch_fused_io(rtm::io_image(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
-  TRY(rtm::check_launch(h, "image_accumulate"));
+  if (h->ic_opt == RTM_IC_INVERSION) {
+    if (h->snap_fmt == RTM_SNAP_AE) TRY(rtm::ae_load(h, slot, h->ae_scratch));
+    TRY(rtm::ic_explicit(h, slot, h->w0));
+  } else {
+    rtm::launch_fused_io(rtm::io_image(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
+    TRY(rtm::check_launch(h, "image_accumulate"));
+  }
   CK(cudaStreamSynchronize(h->st));
   return RTM_OK;
 }
@@ -1731,7 +1777,10 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
         } else if (h->stored[slot]) {
           if (h->snap_fmt == RTM_SNAP_AE) {
             TRY(rtm::ae_load(h, slot, h->ae_scratch));
-            pending = rtm::io_image_ae(h, slot);
+            if (h->ic_opt == RTM_IC_INVERSION)
+              TRY(rtm::ic_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
+            else
+              pending = rtm::io_image_ae(h, slot);
           } else {
             if (off) {
               // this slot in its staging slot before the next kernel reads it, then
@@ -1743,7 +1792,10 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
                 if (h->stored[sn] && h->stage_slot[sn % h->nstage] != sn) TRY(rtm::offload_h2d(h, sn));
               }
             }
-            pending = rtm::io_image(h, slot);
+            if (h->ic_opt == RTM_IC_INVERSION)  // now, on this step's field (the pending term's)
+              TRY(rtm::ic_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
+            else
+              pending = rtm::io_image(h, slot);
           }
         }
       }

@@ -153,6 +153,10 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def image_condition(self, option):
+        """spec.IC_IMAGE1 (zero-lag, default) or spec.IC_INVERSION (k-domain derivative terms)."""
+        self._ck(self.L.rtm_image_condition(self.h, int(option)), "rtm_image_condition")
+
     def illum_setup(self, on=True):
         """Accumulate the source illumination (sum of squared source values) in the imaging condition."""
         self._ck(self.L.rtm_illum_setup(self.h, int(bool(on))), "rtm_illum_setup")

@@ -16,6 +16,7 @@ ISO, VTI, TTI = 1, 2, 3
 FORWARD, BACKWARD = 0, 1
 SNAP_FP32, SNAP_C16, SNAP_FP16S, SNAP_AE = 0, 1, 2, 3
 FIELD_W0, FIELD_W1, FIELD_VEL, FIELD_IMAGE, FIELD_INVQ, FIELD_ILLUM = 0, 1, 2, 3, 4, 5
+IC_IMAGE1, IC_INVERSION = 0, 1
 
 
 @dataclass
