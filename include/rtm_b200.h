@@ -298,6 +298,14 @@ int rtm_ae_decompress_volume(rtm_ae *a, const float *d_latent, const float *d_sc
                              float *d_vol, void *stream);
 /* Attach a compressor to a handle (same device) for RTM_SNAP_AE snapshots. */
 int rtm_set_compressor(rtm_handle *h, rtm_ae *a);
+/* Fallback of learned snapshots to a plain store for the blocks the code
+ * represents worst, the high-energy ones: each RTM_SNAP_AE slot also keeps, as
+ * FP16 values of v / block scale, the 8^3 blocks whose scale exceeds tau x the
+ * slot's largest, largest first, at most ceil(max_fraction x blocks) of them;
+ * decoding overwrites those blocks.  max_fraction = 0 turns it off (default).
+ * Clears existing RTM_SNAP_AE slots (their size changes).  No counterpart in the
+ * reference (its WaveFieldCompress has no learned code). */
+int rtm_set_compressor_fallback(rtm_handle *h, float tau, float max_fraction);
 
 /* ---- Batched small shots (many shots, one persistent launch per step) ----
  * A batch steps several ISO FD8 handles (no Q) of different grids and step

@@ -58,6 +58,35 @@ def blocks_to_volume(blocks, scales, shape):
     return np.ascontiguousarray(v[:ny, :nx, :nz])
 
 
+def fallback_selection(scales, tau, max_fraction):
+    """Blocks a learned snapshot also keeps as FP16 (rtm_set_compressor_fallback):
+    the candidates (scale > 0 and > tau x the largest) whose scale exceeds the
+    (cap+1)-th largest candidate scale, cap = ceil(max_fraction x blocks); all
+    candidates when there are at most cap.  Returns ascending block indices."""
+    s = np.asarray(scales, np.float32)
+    if max_fraction <= 0 or s.size == 0:
+        return np.zeros(0, np.int64)
+    cap = max(1, int(np.ceil(float(np.float32(max_fraction)) * s.size)))
+    cand = (s > 0) & (s > np.float32(tau) * s.max())
+    if cand.sum() > cap:
+        cand &= s > np.sort(s[cand])[::-1][cap]
+    return np.flatnonzero(cand)
+
+
+def apply_fallback(rec, w, scales, sel):
+    """Overwrite the selected 8^3 blocks of the decoded volume `rec` with the
+    FP16 copy of w / scale, times scale, as the device load does."""
+    rec = np.array(rec, np.float32, copy=True)
+    ny, nx, nz = rec.shape
+    nbz, nbx = -(-nz // 8), -(-nx // 8)
+    for b in np.asarray(sel):
+        bz, bx, by = b % nbz, (b // nbz) % nbx, b // (nbz * nbx)
+        sl = (slice(by * 8, by * 8 + 8), slice(bx * 8, bx * 8 + 8), slice(bz * 8, bz * 8 + 8))
+        sc = np.float32(scales[b])
+        rec[sl] = (np.asarray(w[sl], np.float32) / sc).astype(np.float16).astype(np.float32) * sc
+    return rec
+
+
 def init_params(seed=5):
     """Glorot-uniform weights, zero biases, in the library's parameter layout."""
     rng = np.random.default_rng(seed)

@@ -25,6 +25,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "kernel_api.h"
 #include "rtm_b200.h"
 
@@ -351,6 +353,168 @@ int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, i
     unblockify_k<<<n, 512, 0, st>>>(a->y[kLayers - 1], scales + b0, b0, nx, ny, nz, w);
   }
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+}
+
+
+// ---- FP16 fallback of the high-energy blocks of a learned snapshot ----------
+// Per slot: a header, the indices of the stored blocks, and each stored block
+// as 512 FP16 values of v / scale (natural z, x, y order).  The stored blocks
+// are the candidates (scale > 0 and > tau x the largest) whose scale exceeds
+// the (cap+1)-th largest candidate scale, all of them when there are at most
+// cap: a deterministic choice, found by a radix select over the scales' IEEE
+// bit patterns (positive floats order like their bits) in three levels of
+// 11, 11 and 9 bits; thr ends as the smallest bit pattern stored.
+namespace {
+
+constexpr int kFbBins = 2048;
+__host__ __device__ constexpr int fb_shift(int L) { return L == 0 ? 20 : L == 1 ? 9 : 0; }
+__host__ __device__ constexpr int fb_width(int L) { return L == 2 ? 9 : 11; }
+
+struct FbHdr {
+  unsigned maxbits, prefix, thr;
+  int count, rem, done;
+  int hist[kFbBins];
+};
+
+__global__ void fb_max_k(const float *__restrict__ scales, long long nb, FbHdr *h) {
+  float m = 0.f;
+  for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, scales[b]);
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(&h->maxbits, __float_as_uint(m));
+}
+
+// histogram of the candidates inside the current prefix, by their next bits
+template <int L>
+__global__ void fb_hist_k(const float *__restrict__ scales, long long nb, float tau, FbHdr *h) {
+  if (h->done) return;
+  constexpr int hi = fb_shift(L) + fb_width(L);
+  const float mx = __uint_as_float(h->maxbits);
+  const unsigned pre = h->prefix >> hi;
+  for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long long)gridDim.x * blockDim.x) {
+    const float s = scales[b];
+    const unsigned u = __float_as_uint(s);
+    if (s > 0.f && s > tau * mx && (u >> hi) == pre)
+      atomicAdd(&h->hist[(u >> fb_shift(L)) & ((1u << fb_width(L)) - 1)], 1);
+  }
+}
+
+// the bin, from the top, where the running count passes the capacity left
+template <int L>
+__global__ void __launch_bounds__(256) fb_scan_k(FbHdr *h, int cap) {
+  __shared__ int part[256];
+  __shared__ int found;
+  if (h->done) return;
+  constexpr int nbin = 1 << fb_width(L), per = nbin / 256 > 0 ? nbin / 256 : 1;
+  const int t = threadIdx.x;
+  const int top = nbin - 1 - t * per;  // this thread's bins: top, top-1, ..., top-per+1 (t * per < nbin)
+  int v[8], sum = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    v[i] = (i < per && t * per < nbin) ? h->hist[top - i] : 0;
+    sum += v[i];
+  }
+  part[t] = sum;
+  if (t == 0) found = 0;
+  __syncthreads();
+  for (int o = 1; o < 256; o <<= 1) {  // inclusive scan (Hillis-Steele)
+    const int x = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += x;
+    __syncthreads();
+  }
+  const int rem = L == 0 ? cap : h->rem;  // read by all before the one write below
+  const int before = part[t] - sum;  // candidates in the bins above this thread's
+  if (before <= rem && part[t] > rem) {  // the boundary bin is one of this thread's
+    int cum = before, k = 0;
+    while (cum + v[k] <= rem) cum += v[k++];
+    const unsigned bin = (unsigned)(top - k);
+    if (L == 2) {
+      h->thr = h->prefix + (bin + 1);  // the bins above the boundary (bin + 1 may carry into the prefix)
+      h->done = 1;
+    } else {
+      h->prefix |= bin << fb_shift(L);
+      h->rem = rem - cum;
+    }
+    found = 1;
+  }
+  __syncthreads();
+  if (t == 0 && !found) {  // every candidate inside the prefix fits
+    h->thr = h->prefix;
+    h->done = 1;
+  }
+  for (int i = t; i < kFbBins; i += 256) h->hist[i] = 0;  // for the next level
+}
+
+// the chosen blocks: index and FP16 copy of v / scale (one CTA of 512 per block)
+__global__ void __launch_bounds__(512) fb_store_k(const float *__restrict__ w, const float *__restrict__ scales,
+                                                  long long nb, float tau, int nx, int ny, int nz, FbHdr *h, int *idx,
+                                                  __half *data) {
+  __shared__ int slot;
+  const float mx = __uint_as_float(h->maxbits);
+  for (long long b = blockIdx.x; b < nb; b += gridDim.x) {
+    const float s = scales[b];
+    if (!(s > 0.f && s > tau * mx && __float_as_uint(s) >= h->thr)) continue;  // uniform over the CTA
+    if (threadIdx.x == 0) {
+      slot = atomicAdd(&h->count, 1);
+      idx[slot] = (int)b;
+    }
+    __syncthreads();
+    const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+    const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
+    const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;
+    const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
+    const float v = (x < nx && y < ny && z < nz) ? w[((long long)y * nx + x) * nz + z] : 0.f;
+    data[(long long)slot * 512 + threadIdx.x] = __float2half_rn(v / s);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(512) fb_apply_k(const float *__restrict__ scales, const FbHdr *h, const int *idx,
+                                                  const __half *data, int cap, int nx, int ny, int nz, float *w) {
+  const int n = min(h->count, cap);  // a slot never stored holds no valid count: clamp, check each index
+  const long long nb = (long long)((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8);
+  for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    const long long b = idx[t];
+    if (b < 0 || b >= nb) continue;
+    const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+    const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
+    const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;
+    const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
+    if (x < nx && y < ny && z < nz)
+      w[((long long)y * nx + x) * nz + z] = __half2float(data[(long long)t * 512 + threadIdx.x]) * scales[b];
+  }
+}
+
+}  // namespace
+
+size_t ae_fallback_bytes(long long cap) { return sizeof(FbHdr) + (size_t)cap * 4 + (size_t)cap * 1024; }
+
+void ae_fallback_store(const float *w, const float *scales, int nx, int ny, int nz, float tau, long long cap, void *fb,
+                       cudaStream_t st) {
+  const long long nb = ae_volume_blocks(nx, ny, nz);
+  FbHdr *h = static_cast<FbHdr *>(fb);
+  int *idx = reinterpret_cast<int *>(h + 1);
+  __half *data = reinterpret_cast<__half *>(idx + cap);
+  cudaMemsetAsync(h, 0, sizeof(FbHdr), st);
+  const unsigned g = (unsigned)std::min<long long>((nb + 255) / 256, 1184);
+  fb_max_k<<<g, 256, 0, st>>>(scales, nb, h);
+  fb_hist_k<0><<<g, 256, 0, st>>>(scales, nb, tau, h);
+  fb_scan_k<0><<<1, 256, 0, st>>>(h, (int)cap);
+  fb_hist_k<1><<<g, 256, 0, st>>>(scales, nb, tau, h);
+  fb_scan_k<1><<<1, 256, 0, st>>>(h, (int)cap);
+  fb_hist_k<2><<<g, 256, 0, st>>>(scales, nb, tau, h);
+  fb_scan_k<2><<<1, 256, 0, st>>>(h, (int)cap);
+  fb_store_k<<<(unsigned)std::min<long long>(nb, 4096), 512, 0, st>>>(w, scales, nb, tau, nx, ny, nz, h, idx, data);
+}
+
+void ae_fallback_apply(const float *scales, int nx, int ny, int nz, long long cap, const void *fb, float *w,
+                       cudaStream_t st) {
+  const FbHdr *h = static_cast<const FbHdr *>(fb);
+  const int *idx = reinterpret_cast<const int *>(h + 1);
+  const __half *data = reinterpret_cast<const __half *>(idx + cap);
+  fb_apply_k<<<(unsigned)std::max<long long>(1, std::min<long long>(cap, 4096)), 512, 0, st>>>(scales, h, idx, data,
+                                                                                                  (int)cap, nx, ny, nz, w);
 }
 
 }  // namespace rtm

@@ -168,6 +168,14 @@ int launch_ic_inversion(void *plans, const FusedIo &io, const float *u, float *S
                         float *Sh, float *Rh, float *Th, int nx, int ny, int nz, float dx, float dy, float dz,
                         cudaStream_t st);
 
+// FP16 fallback of the high-energy blocks of a learned snapshot (ae.cu): the
+// blocks whose scale exceeds tau x the largest, largest first, at most cap
+void ae_fallback_store(const float *w, const float *scales, int nx, int ny, int nz, float tau, long long cap, void *fb,
+                       cudaStream_t st);
+void ae_fallback_apply(const float *scales, int nx, int ny, int nz, long long cap, const void *fb, float *w,
+                       cudaStream_t st);
+size_t ae_fallback_bytes(long long cap);
+
 // ---- compact FD (kernels_cfd.cu) -------------------------------------------
 struct CfdPlanDev {
   int n;

@@ -110,6 +110,8 @@ struct Engine {
   int *dflag = nullptr;
   int *nfflag = nullptr;  // result of the non-finite scan (allocated on first use)
   rtm_ae *ae = nullptr;      // learned compressor of RTM_SNAP_AE snapshots
+  float ae_fb_tau = 0.f;     // FP16 fallback of learned snapshots: blocks above tau x the largest scale,
+  float ae_fb_frac = 0.f;    // at most this fraction of the blocks (0: no fallback)
   // FP16 wavefield state (state_fp16): h0 / h1 play w0 / w1, value = half * s[iy];
   // sn is the scale of the field the current step writes; m0 / m1 slab maxima
   int f16 = 0;
@@ -771,14 +773,27 @@ static float *ae_latent(Engine *h, int slot) { return (float *)(h->snaps + (size
 static float *ae_scales(Engine *h, int slot) {
   return ae_latent(h, slot) + (size_t)ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 32;
 }
+// fallback blocks per slot and the slot's fallback area (after latents and scales)
+static long long ae_fb_cap(Engine *h) {
+  const long long nb = ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz);
+  return h->ae_fb_frac > 0.f ? std::max(1LL, (long long)std::ceil((double)h->ae_fb_frac * nb)) : 0;
+}
+static void *ae_fb(Engine *h, int slot) {
+  const size_t lat = ((size_t)ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4 + 15) / 16 * 16;
+  return (char *)ae_latent(h, slot) + lat;
+}
 static int ae_store(Engine *h, int slot, const float *w) {
   KScope k(h, RTM_K_IO);
   TRY(ae_compress(h->ae, w, h->d.nx, h->d.ny, h->d.nz, ae_latent(h, slot), ae_scales(h, slot), h->st));
+  if (const long long cap = ae_fb_cap(h))
+    ae_fallback_store(w, ae_scales(h, slot), h->d.nx, h->d.ny, h->d.nz, h->ae_fb_tau, cap, ae_fb(h, slot), h->st);
   return check_launch(h, "ae_compress");
 }
 static int ae_load(Engine *h, int slot, float *w) {
   KScope k(h, RTM_K_IO);
   TRY(ae_decompress(h->ae, ae_latent(h, slot), ae_scales(h, slot), h->d.nx, h->d.ny, h->d.nz, w, h->st));
+  if (const long long cap = ae_fb_cap(h))
+    ae_fallback_apply(ae_scales(h, slot), h->d.nx, h->d.ny, h->d.nz, cap, ae_fb(h, slot), w, h->st);
   return check_launch(h, "ae_decompress");
 }
 // imaging-condition term with the source snapshot decoded into ae_scratch
@@ -1532,7 +1547,8 @@ int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots) {
   h->snap_fmt = fmt, h->nslots = nslots;
   h->slot_bytes = fmt == RTM_SNAP_FP32  ? (size_t)h->n * 4
                   : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2
-                  : fmt == RTM_SNAP_AE  ? (size_t)rtm::ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4
+                  : fmt == RTM_SNAP_AE  ? ((size_t)rtm::ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4 + 15) / 16 * 16 +
+                                              (rtm::ae_fb_cap(h) ? rtm::ae_fallback_bytes(rtm::ae_fb_cap(h)) : 0)
                                         : (size_t)h->n * 2;
   h->slot_bytes = (h->slot_bytes + 255) / 256 * 256;
   h->stored.assign(nslots, 0);
@@ -1551,6 +1567,13 @@ int rtm_set_compressor(rtm_handle *h, rtm_ae *a) {
     h->err = "compressor workspace allocation failed";
     return RTM_ERR_NOMEM;
   }
+  return RTM_OK;
+}
+
+int rtm_set_compressor_fallback(rtm_handle *h, float tau, float max_fraction) {
+  if (!h || tau < 0.f || tau >= 1.f || max_fraction < 0.f || max_fraction > 1.f) return RTM_ERR_ARG;
+  h->ae_fb_tau = tau, h->ae_fb_frac = max_fraction;
+  if (h->snap_fmt == RTM_SNAP_AE && h->nslots) TRY(rtm_snapshot_setup(h, RTM_SNAP_AE, h->nslots));  // new slot size
   return RTM_OK;
 }
 

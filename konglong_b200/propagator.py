@@ -153,6 +153,11 @@ class Propagator:
         self._ck(self.L.rtm_autotune(self.h, steps, C.byref(ch)), "rtm_autotune")
         return ch.value
 
+    def set_compressor_fallback(self, tau=1e-3, max_fraction=0.1):
+        """Keep the high-energy blocks of learned snapshots as FP16 (max_fraction 0: off)."""
+        self._ck(self.L.rtm_set_compressor_fallback(self.h, float(tau), float(max_fraction)),
+                 "rtm_set_compressor_fallback")
+
     def image_condition(self, option):
         """spec.IC_IMAGE1 (zero-lag, default) or spec.IC_INVERSION (k-domain derivative terms)."""
         self._ck(self.L.rtm_image_condition(self.h, int(option)), "rtm_image_condition")

@@ -55,3 +55,26 @@ def test_bf16_rounding():
     r = O.bf16(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6  # ties to even
     assert abs(r[3] + 3.140625) < 1e-7 and r[4] == 0.0
+
+
+def test_fallback_selection_is_the_top_candidates():
+    """The FP16 fallback keeps the candidate blocks (scale > tau x max) above the
+    (cap+1)-th largest candidate scale: never more than cap, ties left out."""
+    rng = np.random.default_rng(3)
+    s = np.exp(rng.standard_normal(5000) * 3).astype(np.float32)
+    s[:40] = s.max()  # a tie at the top
+    s[40:90] = 0.0
+    for tau, frac in [(1e-3, 0.05), (0.0, 0.2), (0.5, 0.5), (1e-3, 1.0), (1e-3, 0.005)]:
+        sel = AE.fallback_selection(s, tau, frac)
+        cap = int(np.ceil(float(np.float32(frac)) * s.size))  # as the library: float max_fraction, double product
+        cand = np.flatnonzero((s > 0) & (s > np.float32(tau) * s.max()))
+        assert sel.size <= cap and np.isin(sel, cand).all()
+        rest = np.setdiff1d(cand, sel)
+        if rest.size:  # everything kept is larger than everything left out
+            assert s[sel].min(initial=np.inf) > s[rest].max()
+            assert (s[cand] >= s[rest].max()).sum() > cap  # and the next value would overflow
+    assert AE.fallback_selection(s, 1e-3, 0.005).size == 0  # 40 tied maxima > cap 25
+    w = rng.standard_normal((9, 17, 12)).astype(np.float32)
+    _, sc = AE.volume_to_blocks(w)
+    rec = AE.apply_fallback(np.zeros_like(w), w, sc, np.arange(sc.size))
+    assert np.abs(rec - w).max() <= 1e-3 * np.abs(w).max()

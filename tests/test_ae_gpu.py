@@ -90,16 +90,33 @@ def test_learned_snapshots_in_rtm(data):
     b, sc = AE.volume_to_blocks(w)
     host = AE.blocks_to_volume(ae.reconstruct(b)[0], sc, s.shape)
     assert rel_l2(dev, host) < 1e-6
+    # with the FP16 fallback of the high-energy blocks
+    m.set_compressor_fallback(1e-3, 0.05)
+    m.snapshot_setup(SNAP_AE, 1)
+    m.put(FIELD_W0, w)
+    m.snapshot_store(0)
+    dev = m.snapshot_load(0).reshape(s.shape)
+    sel = AE.fallback_selection(sc, 1e-3, 0.05)
+    assert 0 < sel.size <= int(np.ceil(0.05 * sc.size))
+    assert rel_l2(dev, AE.apply_fallback(host, w, sc, sel)) < 1e-6
+    assert rel_l2(dev, w) < 0.5 * rel_l2(host, w)
     m.close()
     imgs = {}
-    for fmt in (SNAP_FP32, SNAP_C16, SNAP_AE):
+    runs = [(SNAP_FP32, 0), (SNAP_C16, 0), (SNAP_AE, 0), (SNAP_AE, 0.05), (SNAP_AE, 0.15)]
+    for fmt, frac in runs:
         q = Propagator(s)
         q.set_model(**sh.model_arrays())
         if fmt == SNAP_AE:
             q.set_compressor(ae)
-        imgs[fmt] = q.rtm_shot(src, sh.wavelet[None, :], rcv, rec, 300, 210, 5, snap_fmt=fmt, ntaper_t=3,
-                               ntaper_z=4)[0].reshape(s.shape)
+            q.set_compressor_fallback(1e-3, frac)
+        imgs[fmt, frac] = q.rtm_shot(src, sh.wavelet[None, :], rcv, rec, 300, 210, 5, snap_fmt=fmt, ntaper_t=3,
+                                     ntaper_z=4)[0].reshape(s.shape)
         q.close()
+    fb = {frac: rel_l2(imgs[SNAP_AE, frac], imgs[SNAP_FP32, 0]) for frac in (0.05, 0.15)}
+    print("learned snapshots + FP16 fallback, image NRMSE vs FP32 store: "
+          + ", ".join(f"{100 * f:.0f}% of blocks {e:.4f}" for f, e in fb.items()))
+    assert fb[0.15] <= fb[0.05] < rel_l2(imgs[SNAP_AE, 0], imgs[SNAP_FP32, 0])
+    imgs = {fmt: imgs[fmt, 0] for fmt in (SNAP_FP32, SNAP_C16, SNAP_AE)}
     ref = imgs[SNAP_FP32]
     assert np.isfinite(imgs[SNAP_AE]).all() and np.abs(ref).max() > 0
     assert rel_l2(imgs[SNAP_C16], ref) < 2e-3
