@@ -61,7 +61,10 @@ typedef enum rtm_status {
   RTM_ERR_TIMEOUT = -7      /* a bounded device wait gave up */
 } rtm_status;
 
-enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1 };      /* FD::FD, FD::CFD */
+/* FD::FD, FD::CFD, FD::FFTWR2C (pseudo-spectral: FFT derivative along each
+ * axis, PML along the derivative's own axis only, so pml3d is ignored;
+ * bgprtm/FdEngine_r2c.cpp) */
+enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2 };
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
 enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
@@ -82,7 +85,7 @@ typedef struct rtm_dims {
 } rtm_dims;
 
 typedef struct rtm_config {
-  int engine;         /* RTM_ENGINE_FD8 or RTM_ENGINE_CFD */
+  int engine;         /* RTM_ENGINE_FD8, RTM_ENGINE_CFD or RTM_ENGINE_R2C */
   int model_type;     /* RTM_ISO, RTM_VTI, RTM_TTI */
   int use_q;          /* visco-acoustic memory variables (Q::order terms) */
   int q_order;        /* number of memory variables, default 4 */

@@ -222,6 +222,16 @@ struct CfdDivEpiArgs {  // PML round 2 on raw divergence parts + update
 };
 void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st);
 
+// ---- pseudo-spectral first derivative, FFTWR2C engine (kernels_fft.cu) -------
+struct FftPlans;
+// cuFFT plans of the three axes (y skipped when ny == 1) bound to stream st,
+// the wavenumber tables and the spectrum / transpose scratch
+int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st);
+void fft_plans_destroy(FftPlans *p);
+// raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML);
+// isign +1 / -1 as FdEngine_r2c::fftderiv1_r2c's (the sign of bin n/2 for odd n)
+int launch_fft_deriv(FftPlans *p, int axis, int isign, const float *in, float *out, cudaStream_t st);
+
 // ---- wavefield I/O, sources, receivers, snapshots (kernels_io.cu) -----------
 void launch_update2nd(float *w0, const float *w1, const QDev *q, long long n, cudaStream_t st);
 // atomic scatter of every trace of `t` (Receiver::apply_src)

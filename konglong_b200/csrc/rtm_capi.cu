@@ -65,6 +65,8 @@ struct Engine {
   float *scr = nullptr, *scr2 = nullptr;              // CFD raw-derivative scratch
   float c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
   CfdPlanDev cfd[3][2] = {};
+  FftPlans *fft = nullptr;   // FFTWR2C engine: cuFFT plans and scratch
+  int fft_err = 0;           // a cuFFT execution failed
   PmlDev pml{};
   int model_set = 0;
   // Q
@@ -190,6 +192,11 @@ int cuda_fail(cudaError_t e, const char *what, Engine *h) {
 static int check_launch(Engine *h, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what, h);
+  if (h->fft_err) {
+    h->fft_err = 0;
+    h->err = std::string(what) + ": cuFFT execution failed";
+    return RTM_ERR_CUDA;
+  }
   return RTM_OK;
 }
 
@@ -387,6 +394,10 @@ static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out, int
 // nz % 4 == 0) or the plain staged tile kernel (2)
 static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out) {
   const rtm_dims &d = h->d;
+  if (h->fft) {  // FFTWR2C: isign +1 in the gradient pass, -1 in the divergence pass
+    if (launch_fft_deriv(h->fft, axis, sgn ? -1 : 1, in, out, h->st) != RTM_OK) h->fft_err = 1;
+    return;
+  }
   if (axis != DZ && h->cfd_xy == 0) {
     launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
     return;
@@ -1195,6 +1206,7 @@ int rtm_destroy(rtm_handle *h) {
   h->allocs.clear();
   if (h->st_copy) cudaStreamSynchronize(h->st_copy);
   if (h->ic_plans) rtm::ic_plans_destroy(h->ic_plans);
+  if (h->fft) rtm::fft_plans_destroy(h->fft);
   if (h->host_snaps) cudaFreeHost(h->host_snaps);
   for (cudaEvent_t e : h->stage_ev)
     if (e) cudaEventDestroy(e);
@@ -1212,7 +1224,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (!d || !c || !out) return RTM_ERR_ARG;
   *out = nullptr;
   if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
-      c->engine < 0 || c->engine > 1 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
+      c->engine < 0 || c->engine > 2 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
       c->pml_eps <= 0 || c->pml_eps >= 1) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
@@ -1224,6 +1236,9 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   rtm_handle *h = new rtm_handle();
   h->d = *d;
   h->c = *c;
+  // FdEngine_r2c damps only along each derivative's own axis (fftderiv1_r2c,
+  // bgprtm/FdEngine_r2c.cpp:240-243): no pml3d cross terms
+  if (c->engine == RTM_ENGINE_R2C) h->c.pml3d = 0;
   h->n = (long long)d->nx * d->ny * d->nz;
   h->nxz = (long long)d->nx * d->nz;
   int rc = RTM_OK;
@@ -1257,6 +1272,13 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (first_deriv) {
     if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
       return fail(rc);
+  }
+  if (c->engine == RTM_ENGINE_R2C) {
+    if ((rc = h->alloc(h->scr, h->n)) || (rc = h->alloc(h->scr2, h->n))) return fail(rc);
+    if ((rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
+      h->err = "cuFFT plan set-up failed";
+      return fail(rc);
+    }
   }
   if (c->engine == RTM_ENGINE_CFD) {
     if (cfd_init() != 0) {

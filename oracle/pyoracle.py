@@ -65,6 +65,7 @@ def _load_orc():
     lib.orc_c16_uncompress.argtypes = [_u16p, _f32p, C.c_int, C.c_int, C.c_int]
     lib.orc_taylor_weights.argtypes = [C.c_int, _f64p, _f64p]
     lib.orc_cfd_plan.argtypes = [C.c_int, C.c_float, C.c_int, _f32p, _f32p, _f32p]
+    lib.orc_r2c_line.argtypes = [C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
     return lib
 
 
@@ -218,6 +219,14 @@ def cfd_plan(n, d, s):
 # The reference's own compiled kernels
 # ---------------------------------------------------------------------------
 _ref = None
+
+
+def r2c_line(x, d, isign):
+    """FdEngine_r2c's derivative of one line (double), the oracle's circulant."""
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.zeros_like(x)
+    orc_lib().orc_r2c_line(x.size, d, isign, x.ctypes.data, out.ctypes.data)
+    return out
 
 
 def ref_available():

@@ -1,8 +1,18 @@
-// Stand-in for fftw3.h: only the types named by engine headers; no FFT is run.
+// Stand-in for fftw3.h: the types the engine headers name and the six
+// single-precision 1-D r2c / c2r calls FdEngine_r2c makes, computed as plain
+// DFTs in double by the definitions FFTW documents (ref_shim.cpp).
 #ifndef RTM_SHIM_FFTW3_H
 #define RTM_SHIM_FFTW3_H
 typedef float fftwf_complex[2];
 typedef struct fftwf_plan_s *fftwf_plan;
 typedef double fftw_complex[2];
 typedef struct fftw_plan_s *fftw_plan;
+#define FFTW_MEASURE (0U)
+#define FFTW_DESTROY_INPUT (1U << 0)
+#define FFTW_ESTIMATE (1U << 6)
+fftwf_plan fftwf_plan_dft_r2c_1d(int n, float *in, fftwf_complex *out, unsigned flags);
+fftwf_plan fftwf_plan_dft_c2r_1d(int n, fftwf_complex *in, float *out, unsigned flags);
+void fftwf_execute_dft_r2c(const fftwf_plan p, float *in, fftwf_complex *out);
+void fftwf_execute_dft_c2r(const fftwf_plan p, fftwf_complex *in, float *out);
+void fftwf_destroy_plan(fftwf_plan p);
 #endif

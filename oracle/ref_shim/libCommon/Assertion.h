@@ -1,0 +1,5 @@
+// Stand-in for libCommon/Assertion.h: assertion() comes with the GetPar stand-in.
+#ifndef RTM_SHIM_ASSERTION_H
+#define RTM_SHIM_ASSERTION_H
+#include "libCommon/GetPar.h"
+#endif

@@ -1,10 +1,13 @@
 // ref_shim.cpp - definitions the reference's compiled CPU kernels need from
 // libraries that are absent from the reference tree (libCommon, MPI printing,
-// the FFT engines KernelCPU's constructor can name but our runs never select).
+// FFTW's 1-D real transforms, the engines KernelCPU's constructor can name
+// but our runs never select).
 // TEST INFRASTRUCTURE ONLY: linked into oracle/_ref/libbgprtm_ref.so.
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "GetPar.h"
 #include "MpiPrint.h"
@@ -12,6 +15,7 @@
 #include "FdEngine_r2c.h"
 #include "FdEngine_r2r.h"
 #include "FdEngine_hfd.h"
+#include "Util.h"
 #include "libCommon/Taylor.h"
 #include "../oracle_common.hpp"
 
@@ -53,16 +57,56 @@ static struct TaylorInit {
 } taylor_init;
 }  // namespace libCommon
 
-// Engines KernelCPU's constructor can name (FFT / HFD); never selected here.
+// FFTW's single-precision 1-D real transforms, by their documented
+// definitions (unnormalised; forward sign -1):
+//   r2c  X_j = sum_t x_t e^{-2 pi i j t / n},  j = 0 .. n/2
+//   c2r  y_t = sum_{j=0}^{n-1} X_j e^{+2 pi i j t / n} with X_{n-j} = conj(X_j);
+//        the imaginary parts of X_0 and (n even) X_{n/2} are not read.
+// Plain DFTs in double rounded to float: FFTW's results, not its rounding.
+struct fftwf_plan_s {
+  int n, c2r;
+};
+fftwf_plan fftwf_plan_dft_r2c_1d(int n, float *, fftwf_complex *, unsigned) { return new fftwf_plan_s{n, 0}; }
+fftwf_plan fftwf_plan_dft_c2r_1d(int n, fftwf_complex *, float *, unsigned) { return new fftwf_plan_s{n, 1}; }
+void fftwf_destroy_plan(fftwf_plan p) { delete p; }
+void fftwf_execute_dft_r2c(const fftwf_plan p, float *in, fftwf_complex *out) {
+  const int n = p->n;
+  std::vector<double> re(n / 2 + 1), im(n / 2 + 1);
+  for (int j = 0; j <= n / 2; j++) {
+    double a = 0, b = 0;
+    for (int t = 0; t < n; t++) {
+      const double th = 2.0 * M_PI * (double)(((long long)j * t) % n) / n;
+      a += in[t] * std::cos(th), b -= in[t] * std::sin(th);
+    }
+    re[j] = a, im[j] = b;
+  }
+  for (int j = 0; j <= n / 2; j++) out[j][0] = (float)re[j], out[j][1] = (float)im[j];
+}
+void fftwf_execute_dft_c2r(const fftwf_plan p, fftwf_complex *in, float *out) {
+  const int n = p->n, top = n % 2 == 0 ? n / 2 - 1 : n / 2;
+  std::vector<double> y(n);
+  for (int t = 0; t < n; t++) {
+    double v = in[0][0];
+    if (n % 2 == 0) v += (t % 2 ? -1.0 : 1.0) * in[n / 2][0];
+    for (int j = 1; j <= top; j++) {
+      const double th = 2.0 * M_PI * (double)(((long long)j * t) % n) / n;
+      v += 2.0 * (in[j][0] * std::cos(th) - in[j][1] * std::sin(th));
+    }
+    y[t] = v;
+  }
+  for (int t = 0; t < n; t++) out[t] = (float)y[t];
+}
+
+// Util::transpose (bgprtm/Util.cpp:25-76) as intended: out[ix][iy] =
+// in[iy][ix] for nx x ny, row pitches dimIn / dimOut.  The reference's SSE
+// body omits the store of the third transposed row (Util.cpp:51-54).
+void Util::transpose(int nx, int ny, int dimIn, int dimOut, float *in, float *out) {
+  for (int ix = 0; ix < nx; ix++)
+    for (int iy = 0; iy < ny; iy++) out[(size_t)ix * dimOut + iy] = in[(size_t)iy * dimIn + ix];
+}
+
+// Engines KernelCPU's constructor can name (r2r / HFD); never selected here.
 #define NOT_BUILT(...) assertion(false, "engine not built in the oracle harness")
-FdEngine_r2c::FdEngine_r2c(int a, int b, int c, float d, float e, float f, int g) : FdEngine(a, b, c, d, e, f, g) { NOT_BUILT(); }
-FdEngine_r2c::~FdEngine_r2c() {}
-void FdEngine_r2c::dx1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2c::dy1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2c::dz1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2c::dx1_2D(float *, float *, float *, int, int, int, float *, float *) {}
-void FdEngine_r2c::dy1_2D(float *, float *, float *, int, int, int, float *, float *) {}
-void FdEngine_r2c::dz1_2D(float *, float *, float *, int, int, int, float *, float *) {}
 FdEngine_r2r::FdEngine_r2r(int a, int b, int c, float d, float e, float f, int g) : FdEngine(a, b, c, d, e, f, g) { NOT_BUILT(); }
 FdEngine_r2r::~FdEngine_r2r() {}
 void FdEngine_r2r::dx1_2D(float *, float *, float *, int, int, int) {}

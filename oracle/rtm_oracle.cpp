@@ -31,7 +31,7 @@ using std::min;
 using std::vector;
 
 enum { ISO = 1, VTI = 2, TTI = 3 };
-enum { FD8 = 0, CFD = 1 };
+enum { FD8 = 0, CFD = 1, R2C = 2 };
 enum { X = 0, Y = 1, Z = 2 };
 enum { TOP = 0, BOT = 1 };
 
@@ -157,6 +157,39 @@ static void cfd_line(const CfdPlan<R> &p, int s, const R *x, R *b, size_t ld) {
                 bm[i * 5];
 }
 
+// FdEngine_r2c::fftderiv1_r2c (bgprtm/FdEngine_r2c.cpp:212-246) as the
+// circulant it applies to a line of n points: FFTW's unnormalised r2c, bin j
+// times i k_j (k_j = -j dk, dk = 2 pi / (d n) / n, assignW :52-56; bin n/2
+// also times isign), unnormalised c2r.  The c2r reads only the real parts of
+// the DC and Nyquist bins, where the product has none, so
+//   out_t = sum_u c[(t - u) mod n] x_u,  c[m] = -2 sum_{j=1..J} s_j k_j sin(2 pi j m / n)
+// with J = n/2 - 1 (n even) or (n - 1)/2 (n odd) and s_j = isign for j = n/2.
+// k_j and dk are rounded to float as there; the sums are in double.
+static vector<double> r2c_circulant(int n, float d, int isign) {
+  const float scale = 1.0f / float(n);
+  const float dk = (float)(2.0f * M_PI / (double)(d * (float)n) * (double)scale);
+  const int J = n % 2 == 0 ? n / 2 - 1 : (n - 1) / 2;
+  vector<double> c(n, 0.0);
+  for (int m = 0; m < n; m++) {
+    double v = 0;
+    for (int j = 1; j <= J; j++) {
+      const double kj = (double)((float)(-j) * dk), sj = j == n / 2 ? (double)isign : 1.0;
+      v += sj * kj * std::sin(2.0 * M_PI * (double)(((long long)j * m) % n) / n);
+    }
+    c[m] = -2.0 * v;
+  }
+  return c;
+}
+
+template <typename R>
+static void r2c_line(const vector<double> &c, int n, const R *x, R *b, size_t ld) {
+  for (int t = 0; t < n; t++) {
+    double v = 0;
+    for (int u = 0; u < n; u++) v += c[(t - u + n) % n] * (double)x[u * ld];
+    b[t * ld] = (R)v;
+  }
+}
+
 template <typename R> struct TraceSet {
   int ntr = 0, lx = 0, ly = 0, lz = 0, nt = 0;
   vector<int> off, len;
@@ -176,6 +209,7 @@ public:
   // FD tables: c1*[m], c2*[m] for m = 0..4 (m = 0 is the centre of c2)
   R c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
   CfdPlan<R> cfdx, cfdy, cfdz;
+  vector<double> r2c[3][2];  // FFTWR2C circulants [axis][round]: round 0 isign +1, round 1 isign -1
   // PML: profile per dim/side (coef, distance from the outer edge) and memory
   // pml[dim][side][round][comp] (bgprtm/FdEngine.h:178)
   bool has_pml[3][2] = {};
@@ -213,6 +247,14 @@ public:
       cfdx.build(nx, dx);
       cfdy.build(ny, dy);
       cfdz.build(nz, dz);
+    }
+    if (cfg.engine == R2C) {
+      cfg.pml3d = 0;  // fftderiv1_r2c damps along the derivative's own axis only
+      const int nn[3] = {nx, ny, nz};
+      const float dd[3] = {(float)dx, (float)dy, (float)dz};
+      for (int a = 0; a < 3; a++)
+        if (nn[a] > 1)
+          for (int r = 0; r < 2; r++) r2c[a][r] = r2c_circulant(nn[a], dd[a], r == 0 ? 1 : -1);
     }
     build_pml();
     c16_tables(codec_table, wtaper20, wtaper10);
@@ -445,11 +487,27 @@ public:
           }
       return;
     }
-    // CFD: solve along lines, then PML and accumulate (FdEngine_cfd.cpp:83-153)
+    // CFD: solve along lines, then PML and accumulate (FdEngine_cfd.cpp:83-153);
+    // FFTWR2C: the spectral circulant along lines, then the same
     vector<R> d(nxyz);
     const CfdPlan<R> &p = axis == X ? cfdx : axis == Y ? cfdy : cfdz;
     int s = round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
-    if (axis == Z) {
+    if (cfg.engine == R2C) {
+      const vector<double> &c = r2c[axis][s];
+      if (axis == Z) {
+#pragma omp parallel for schedule(static)
+        for (long l = 0; l < (long)nx * ny; l++) r2c_line(c, nz, in + l * nz, d.data() + l * nz, 1);
+      } else if (axis == X) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int iy = 0; iy < ny; iy++)
+          for (int iz = 0; iz < nz; iz++) r2c_line(c, nx, in + iy * nxz + iz, d.data() + iy * nxz + iz, nz);
+      } else {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int ix = 0; ix < nx; ix++)
+          for (int iz = 0; iz < nz; iz++)
+            r2c_line(c, ny, in + (size_t)ix * nz + iz, d.data() + (size_t)ix * nz + iz, nxz);
+      }
+    } else if (axis == Z) {
 #pragma omp parallel for schedule(static)
       for (long c = 0; c < (long)nx * ny; c++) cfd_line(p, s, in + c * nz, d.data() + c * nz, 1);
     } else if (axis == X) {
@@ -870,5 +928,10 @@ void orc_cfd_plan(int n, float d, int s, float *bm, float *bl, float *am) {
   std::copy(p.bm[s].begin(), p.bm[s].end(), bm);
   std::copy(p.bl[s].begin(), p.bl[s].end(), bl);
   std::copy(p.am[s].begin(), p.am[s].end(), am);
+}
+// The FFTWR2C derivative of one line of n points (double in and out).
+void orc_r2c_line(int n, float d, int isign, const double *x, double *out) {
+  const std::vector<double> c = orc::r2c_circulant(n, d, isign);
+  orc::r2c_line<double>(c, n, x, out, 1);
 }
 }

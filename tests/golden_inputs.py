@@ -3,7 +3,7 @@ and the tests; numpy's default_rng is reproducible across platforms)."""
 import numpy as np
 from scipy.ndimage import gaussian_filter
 
-from konglong_b200.spec import ENGINE_CFD, ENGINE_FD8, ISO, TTI, VTI, PropSpec
+from konglong_b200.spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ISO, TTI, VTI, PropSpec
 
 # nx*nz kept a multiple of 4: the reference's SSE loops step 4 floats across
 # a y slab (bgprtm/KernelCPU.cpp:328-338).
@@ -16,6 +16,10 @@ CASES = {
     "iso_cfd": dict(engine=ENGINE_CFD, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=15),
     "vti_cfd": dict(engine=ENGINE_CFD, model=VTI, shape=(24, 20, 28), pml=6, steps=3, seed=16),
     "tti_cfd": dict(engine=ENGINE_CFD, model=TTI, shape=(24, 20, 28), pml=6, steps=3, seed=17),
+    # FFTWR2C: even lines, odd x (the isign bin n/2), odd y and z
+    "iso_r2c": dict(engine=ENGINE_R2C, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=18),
+    "vti_r2c": dict(engine=ENGINE_R2C, model=VTI, shape=(23, 20, 28), pml=6, steps=3, seed=19),
+    "tti_r2c": dict(engine=ENGINE_R2C, model=TTI, shape=(24, 21, 27), pml=6, steps=3, seed=20),
 }
 
 

@@ -1,7 +1,8 @@
 """The oracle (CPU restatement) against the reference's own compiled kernels.
 
 Fixtures come from oracle/_ref (bgprtm's KernelCPU / FdEngine_fd /
-FdEngine_cfd / Cfd_plan / PML / WaveFieldCompress built from source), see
+FdEngine_cfd / FdEngine_r2c / Cfd_plan / PML / WaveFieldCompress built from
+source), see
 tests/golden/make_golden.py.  FD8 must agree to FP32 rounding; the compact-FD
 line solve (band LU without pivoting, pivots down to ~0.016) amplifies FP32
 rounding, so its bound is the reference's own FP32-vs-FP64 spread.
@@ -45,6 +46,54 @@ def test_cfd_matches_reference_within_fp32_conditioning(golden, name):
     assert spread < 5e-3
     assert rel_l2(got, ref) < 2.0 * spread + 1e-6
     assert rel_l2(got, exact) < 2.0 * spread + 1e-6
+
+
+@pytest.mark.parametrize("name", [k for k in CASES if "r2c" in k])
+def test_r2c_matches_reference(golden, name):
+    """FFTWR2C: the reference's FdEngine_r2c (FFTW calls answered by DFTs in
+    double, Util::transpose completed) against the oracle's circulant form."""
+    got = run_oracle(CASES[name])
+    assert rel_l2(got, golden[f"{name}__w1"]) < FD8_TOL
+    assert rel_l2(run_oracle(CASES[name], double=True), golden[f"{name}__w1"]) < FD8_TOL
+
+
+@pytest.mark.parametrize("n", [16, 17, 30, 27])
+@pytest.mark.parametrize("isign", [1, -1])
+def test_r2c_line_is_the_spectral_product(n, isign):
+    """The oracle's circulant equals rfft -> i k_j (bin n/2 times isign) ->
+    unnormalised irfft written with numpy's FFT, k_j = -j dk in float as
+    FdEngine_r2c::assignW."""
+    x = np.random.default_rng(n).standard_normal(n)
+    sc = np.float32(1.0) / np.float32(n)
+    dk = np.float32(2.0 * np.pi / np.float64(np.float32(10.0) * np.float32(n)) * np.float64(sc))
+    k = np.array([np.float32(-j) * dk for j in range(n // 2 + 1)], np.float64)
+    m = 1j * k
+    m[n // 2] *= isign
+    want = np.fft.irfft(np.fft.rfft(x) * m, n) * n
+    np.testing.assert_allclose(O.r2c_line(x, 10.0, isign), want, rtol=0, atol=1e-12 * np.abs(want).max())
+
+
+def test_r2c_known_answer_sine():
+    """FdEngine_r2c's k_j = -j dk makes the engine's first derivative the
+    negative of d/dx: sin(2 pi t / n) -> -(2 pi / (n d)) cos(2 pi t / n)."""
+    n, d = 48, 10.0
+    t = np.arange(n)
+    got = O.r2c_line(np.sin(2 * np.pi * 3 * t / n), d, 1)
+    want = -(2 * np.pi * 3 / (n * d)) * np.cos(2 * np.pi * 3 * t / n)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-6 * np.abs(want).max())
+
+
+def test_r2c_odd_lines_have_a_growing_mode():
+    """The isign factor on bin n/2 (FdEngine_r2c.cpp:228-231) is +1 in the
+    gradient pass and -1 in the divergence pass: for even n that bin is the
+    Nyquist bin and drops out, for odd n it is an ordinary bin whose two-pass
+    product is +k^2, a growing mode of the time stepping."""
+    for n, grows in ((50, False), (51, True)):
+        e = np.eye(n)
+        dp = np.stack([O.r2c_line(e[i], 10.0, 1) for i in range(n)], 1)
+        dm = np.stack([O.r2c_line(e[i], 10.0, -1) for i in range(n)], 1)
+        top = np.linalg.eigvals(dm @ dp).real.max()
+        assert (top > 1e-3) == grows, (n, top)
 
 
 def test_codec_bit_exact(golden):
