@@ -61,10 +61,11 @@ typedef enum rtm_status {
   RTM_ERR_TIMEOUT = -7      /* a bounded device wait gave up */
 } rtm_status;
 
-/* FD::FD, FD::CFD, FD::FFTWR2C (pseudo-spectral: FFT derivative along each
- * axis, PML along the derivative's own axis only, so pml3d is ignored;
- * bgprtm/FdEngine_r2c.cpp) */
-enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2 };
+/* FD::FD, FD::CFD, FD::FFTWR2C and FD::FFTWR2R (pseudo-spectral: FFT or
+ * cosine / sine transform derivative along each axis, PML along the
+ * derivative's own axis only, so pml3d is ignored; bgprtm/FdEngine_r2c.cpp,
+ * bgprtm/FdEngine_r2r.cpp) */
+enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2, RTM_ENGINE_R2R = 3 };
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
 enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
@@ -85,7 +86,7 @@ typedef struct rtm_dims {
 } rtm_dims;
 
 typedef struct rtm_config {
-  int engine;         /* RTM_ENGINE_FD8, RTM_ENGINE_CFD or RTM_ENGINE_R2C */
+  int engine;         /* RTM_ENGINE_FD8, RTM_ENGINE_CFD, RTM_ENGINE_R2C or RTM_ENGINE_R2R */
   int model_type;     /* RTM_ISO, RTM_VTI, RTM_TTI */
   int use_q;          /* visco-acoustic memory variables (Q::order terms) */
   int q_order;        /* number of memory variables, default 4 */
@@ -157,6 +158,12 @@ int rtm_swap(rtm_handle *h);
  * taper length (0 = none).  Returns the first grid index in *off. */
 int rtm_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper,
                       float *coeff, int *off);
+
+/* The FFTWR2R first derivative along one axis of n points with spacing d as
+ * the row-major n x n matrix D the engine applies to every line (out_t =
+ * sum_u D[t][u] x_u): FdEngine_r2r::fftderiv1_r2r, bgprtm/FdEngine_r2r.cpp:73-102;
+ * isign +1 (gradient pass) or -1 (divergence pass).  Host only. */
+int rtm_r2r_line_matrix(int n, float d, int isign, float *D);
 
 /* Traces injected into w0 each step (Receiver::apply, no FK/true-amp path):
  * w0[c] += traces[r][it] * scaler * kx[r][ix] * ky[r][iy] * kz[r][iz] * (v dt)^2[c]

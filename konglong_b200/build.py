@@ -79,7 +79,7 @@ def build(verbose=False, extra_flags=()):
             if out and verbose:
                 print(out)
     if relink:
-        cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcufft"]
+        cmd = [cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcufft", "-lcublas"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + p.stdout + p.stderr)

@@ -7,6 +7,8 @@
 //                    recursion constants of bgprtm/PML.cpp:126-134
 //   spread_coeffs    Util::CompactOrmsbySpreadCoeff (bgprtm/Util.cpp:317-397)
 //                    with Receiver's taper_kernel (bgprtm/Receiver.cpp:291-303)
+//   r2r_line_matrix  FdEngine_r2r's derivative (bgprtm/FdEngine_r2r.cpp:4-102)
+//                    as one matrix per axis and pass
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -146,6 +148,45 @@ void pml_profile(int w, double d, double dt, double vmax, double eps, double sca
 
 // libCommon's sincf_unnorm / blackman / dipole_unnorm are not in the reference
 // tree; they are restated from their definitions.
+// FdEngine_r2r::fftderiv1_r2r composes three linear maps on a line of n
+// points, all unnormalised FFTW real-to-real transforms:
+//   isign +1: F = DCT-II (REDFT10)  F[q][u] = 2 cos(pi (u + 1/2) q / n)
+//             S: bin i <- -k_i bin i+1 (i < n-1), bin n-1 <- 0
+//             B = DST-III (RODFT01) B[t][j] = 2 sin(pi (j + 1) (t + 1/2) / n), j < n-1;
+//                                   B[t][n-1] = (-1)^t
+//   isign -1: F = DST-II (RODFT10)  F[q][u] = 2 sin(pi (u + 1/2) (q + 1) / n)
+//             S: bin i <- k_{i-1} bin i-1 (i >= 1), bin 0 <- 0
+//             B = DCT-III (REDFT01) B[t][0] = 1, B[t][j] = 2 cos(pi j (t + 1/2) / n)
+// with k_i = -(i + 1) dk and dk = pi / (d n) / 2 / n in float (constructor
+// :11-13, assignW :66-70).  D = B S F in FP64, rounded once.
+void r2r_line_matrix(int n, float d, int isign, std::vector<float> &D) {
+  const float dk = (float)(M_PI / (double)(d * (float)n) * 0.5 * (double)(1.0f / float(n)));
+  std::vector<double> SF((size_t)n * n, 0.0);  // S F: row i = the multiplied bin i
+  for (int i = 0; i < n; i++) {
+    const int q = isign == 1 ? i + 1 : i - 1;  // the bin moved into i
+    if (q < 0 || q >= n) continue;
+    const double ki = (double)((float)(-((isign == 1 ? i : i - 1) + 1)) * dk);
+    const double m = isign == 1 ? -ki : ki;
+    for (int u = 0; u < n; u++) {
+      const double f = isign == 1 ? 2.0 * std::cos(M_PI * (u + 0.5) * q / n)
+                                  : 2.0 * std::sin(M_PI * (u + 0.5) * (q + 1) / n);
+      SF[(size_t)i * n + u] = m * f;
+    }
+  }
+  D.assign((size_t)n * n, 0.f);
+  std::vector<double> b(n);
+  for (int t = 0; t < n; t++) {
+    for (int j = 0; j < n; j++)
+      b[j] = isign == 1 ? (j == n - 1 ? (t % 2 ? -1.0 : 1.0) : 2.0 * std::sin(M_PI * (j + 1) * (t + 0.5) / n))
+                        : (j == 0 ? 1.0 : 2.0 * std::cos(M_PI * j * (t + 0.5) / n));
+    for (int u = 0; u < n; u++) {
+      double v = 0;
+      for (int j = 0; j < n; j++) v += b[j] * SF[(size_t)j * n + u];
+      D[(size_t)t * n + u] = (float)v;
+    }
+  }
+}
+
 static float sinc_u(float x) { return x == 0.0f ? 1.0f : sinf(x) / x; }
 static float dipole_u(float x) { return x == 0.0f ? 0.0f : (x * cosf(x) - sinf(x)) / (x * x); }
 static float blackman_w(float t) { return 0.42f - 0.5f * cosf(t) + 0.08f * cosf(2.0f * t); }

@@ -231,6 +231,12 @@ void fft_plans_destroy(FftPlans *p);
 // raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML);
 // isign +1 / -1 as FdEngine_r2c::fftderiv1_r2c's (the sign of bin n/2 for odd n)
 int launch_fft_deriv(FftPlans *p, int axis, int isign, const float *in, float *out, cudaStream_t st);
+// FFTWR2R engine: one line matrix per axis and pass, applied as FP32 GEMMs on
+// stream st (cuBLAS handle, fixed workspace)
+struct R2rPlans;
+int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st);
+void r2r_plans_destroy(R2rPlans *p);
+int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *out);
 
 // ---- wavefield I/O, sources, receivers, snapshots (kernels_io.cu) -----------
 void launch_update2nd(float *w0, const float *w1, const QDev *q, long long n, cudaStream_t st);

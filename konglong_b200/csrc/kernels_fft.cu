@@ -20,12 +20,22 @@
 // strides (z and y), so each y plane is transposed to [nz][nx] through a
 // shared-memory tile, transformed as contiguous lines and transposed back.
 // cuFFT does the transforms; the bin products and the transposes are ours.
+//
+// FFTWR2R (FdEngine_r2r, bgprtm/FdEngine_r2r.cpp): the derivative of a line
+// is a cosine (or sine) transform, a shifted bin product and the opposite
+// inverse transform - one fixed n x n matrix per axis and pass (built on the
+// host in FP64, host_setup.cpp).  Applied to every line at once it is a plain
+// FP32 GEMM on the volume as it lies: z lines [nx ny][nz] x D^T, y lines
+// D x [ny][nx nz], x lines D x [nx][nz] per y plane (strided batch); cuBLAS
+// (pedantic FP32 math, workspace fixed for graph capture) runs them.
+#include <cublas_v2.h>
 #include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
+#include "host_setup.h"
 #include "kernel_api.h"
 #include "rtm_b200.h"
 
@@ -192,6 +202,83 @@ int launch_fft_deriv(FftPlans *p, int axis, int isign, const float *in, float *o
   if (axis == 0)  // [ny][nz][nx] -> [ny][nx][nz]
     transpose_k<<<dim3((nx + 31) / 32, (nz + 31) / 32, ny), 256, 0, st>>>(p->tr, out, nz, nx);
   return RTM_OK;
+}
+
+struct R2rPlans {
+  cublasHandle_t blas = nullptr;
+  void *ws = nullptr;
+  float *D[3][2] = {};  // [axis][pass: 0 isign +1, 1 isign -1], row-major n x n
+  int nx = 0, ny = 0, nz = 0;
+};
+
+constexpr size_t kBlasWorkspace = 32u << 20;
+
+void r2r_plans_destroy(R2rPlans *p) {
+  if (!p) return;
+  if (p->blas) cublasDestroy(p->blas);
+  for (auto &a : p->D)
+    for (float *m : a)
+      if (m) cudaFree(m);
+  if (p->ws) cudaFree(p->ws);
+  delete p;
+}
+
+int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st) {
+  *out = nullptr;
+  R2rPlans *p = new R2rPlans();
+  p->nx = nx, p->ny = ny, p->nz = nz;
+  if (cublasCreate(&p->blas) != CUBLAS_STATUS_SUCCESS) {
+    p->blas = nullptr;
+    r2r_plans_destroy(p);
+    return RTM_ERR_CUDA;
+  }
+  if (cudaMalloc(&p->ws, kBlasWorkspace) != cudaSuccess) {
+    cudaGetLastError();
+    r2r_plans_destroy(p);
+    return RTM_ERR_NOMEM;
+  }
+  if (cublasSetStream(p->blas, st) != CUBLAS_STATUS_SUCCESS ||
+      cublasSetWorkspace(p->blas, p->ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS ||
+      cublasSetMathMode(p->blas, CUBLAS_PEDANTIC_MATH) != CUBLAS_STATUS_SUCCESS) {
+    r2r_plans_destroy(p);
+    return RTM_ERR_CUDA;
+  }
+  const int nn[3] = {nx, ny, nz};
+  const float dd[3] = {dx, dy, dz};
+  std::vector<float> D;
+  for (int a = 0; a < 3; a++) {
+    if (nn[a] < 2) continue;
+    for (int s = 0; s < 2; s++) {
+      r2r_line_matrix(nn[a], dd[a], s == 0 ? 1 : -1, D);
+      if (cudaMalloc(&p->D[a][s], D.size() * 4) != cudaSuccess ||
+          cudaMemcpy(p->D[a][s], D.data(), D.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        r2r_plans_destroy(p);
+        return RTM_ERR_NOMEM;
+      }
+    }
+  }
+  *out = p;
+  return RTM_OK;
+}
+
+int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *out) {
+  const float *D = p->D[axis][isign == 1 ? 0 : 1];
+  if (!D) return RTM_ERR_ARG;
+  const int nx = p->nx, ny = p->ny, nz = p->nz;
+  const long long nxz = (long long)nx * nz, lines = (long long)nx * ny;
+  if (nxz > 0x7fffffffLL || lines > 0x7fffffffLL) return RTM_ERR_ARG;
+  const float one = 1.f, zero = 0.f;
+  cublasStatus_t r;
+  if (axis == 2)  // out[l][t] = sum_u D[t][u] in[l][u]
+    r = cublasSgemm(p->blas, CUBLAS_OP_T, CUBLAS_OP_N, nz, (int)lines, nz, &one, D, nz, in, nz, &zero, out, nz);
+  else if (axis == 1)  // out[t][c] = sum_u D[t][u] in[u][c], c over nx nz
+    r = cublasSgemm(p->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)nxz, ny, ny, &one, in, (int)nxz, D, ny, &zero, out,
+                    (int)nxz);
+  else  // per y plane: out[t][z] = sum_u D[t][u] in[u][z]
+    r = cublasSgemmStridedBatched(p->blas, CUBLAS_OP_N, CUBLAS_OP_N, nz, nx, nx, &one, in, nz, nxz, D, nx, 0, &zero,
+                                  out, nz, nxz, ny);
+  return r == CUBLAS_STATUS_SUCCESS ? RTM_OK : RTM_ERR_CUDA;
 }
 
 }  // namespace rtm

@@ -66,6 +66,7 @@ struct Engine {
   float c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
   CfdPlanDev cfd[3][2] = {};
   FftPlans *fft = nullptr;   // FFTWR2C engine: cuFFT plans and scratch
+  R2rPlans *r2r = nullptr;   // FFTWR2R engine: line matrices and the GEMM handle
   int fft_err = 0;           // a cuFFT execution failed
   PmlDev pml{};
   int model_set = 0;
@@ -194,7 +195,7 @@ static int check_launch(Engine *h, const char *what) {
   if (e != cudaSuccess) return cuda_fail(e, what, h);
   if (h->fft_err) {
     h->fft_err = 0;
-    h->err = std::string(what) + ": cuFFT execution failed";
+    h->err = std::string(what) + ": cuFFT / cuBLAS execution failed";
     return RTM_ERR_CUDA;
   }
   return RTM_OK;
@@ -396,6 +397,10 @@ static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out)
   const rtm_dims &d = h->d;
   if (h->fft) {  // FFTWR2C: isign +1 in the gradient pass, -1 in the divergence pass
     if (launch_fft_deriv(h->fft, axis, sgn ? -1 : 1, in, out, h->st) != RTM_OK) h->fft_err = 1;
+    return;
+  }
+  if (h->r2r) {  // FFTWR2R, the same pass signs
+    if (launch_r2r_deriv(h->r2r, axis, sgn ? -1 : 1, in, out) != RTM_OK) h->fft_err = 1;
     return;
   }
   if (axis != DZ && h->cfd_xy == 0) {
@@ -1207,6 +1212,7 @@ int rtm_destroy(rtm_handle *h) {
   if (h->st_copy) cudaStreamSynchronize(h->st_copy);
   if (h->ic_plans) rtm::ic_plans_destroy(h->ic_plans);
   if (h->fft) rtm::fft_plans_destroy(h->fft);
+  if (h->r2r) rtm::r2r_plans_destroy(h->r2r);
   if (h->host_snaps) cudaFreeHost(h->host_snaps);
   for (cudaEvent_t e : h->stage_ev)
     if (e) cudaEventDestroy(e);
@@ -1224,7 +1230,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (!d || !c || !out) return RTM_ERR_ARG;
   *out = nullptr;
   if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
-      c->engine < 0 || c->engine > 2 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
+      c->engine < 0 || c->engine > 3 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
       c->pml_eps <= 0 || c->pml_eps >= 1) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
@@ -1236,9 +1242,9 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   rtm_handle *h = new rtm_handle();
   h->d = *d;
   h->c = *c;
-  // FdEngine_r2c damps only along each derivative's own axis (fftderiv1_r2c,
-  // bgprtm/FdEngine_r2c.cpp:240-243): no pml3d cross terms
-  if (c->engine == RTM_ENGINE_R2C) h->c.pml3d = 0;
+  // FdEngine_r2c / _r2r damp only along each derivative's own axis
+  // (bgprtm/FdEngine_r2c.cpp:240-243, FdEngine_r2r.cpp:95-98): no pml3d cross terms
+  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R) h->c.pml3d = 0;
   h->n = (long long)d->nx * d->ny * d->nz;
   h->nxz = (long long)d->nx * d->nz;
   int rc = RTM_OK;
@@ -1273,10 +1279,16 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
       return fail(rc);
   }
-  if (c->engine == RTM_ENGINE_R2C) {
+  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R) {
     if ((rc = h->alloc(h->scr, h->n)) || (rc = h->alloc(h->scr2, h->n))) return fail(rc);
-    if ((rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
+    if (c->engine == RTM_ENGINE_R2C &&
+        (rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
       h->err = "cuFFT plan set-up failed";
+      return fail(rc);
+    }
+    if (c->engine == RTM_ENGINE_R2R &&
+        (rc = r2r_plans_create(&h->r2r, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
+      h->err = "FFTWR2R line-matrix set-up failed";
       return fail(rc);
     }
   }
@@ -1489,6 +1501,14 @@ int rtm_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipol
   if (!nlimit || !coeff || !off || n < 1 || !(k1 > 0.f) || k1 > k2 || k2 > 0.5f || !std::isfinite(x)) return RTM_ERR_ARG;
   if (n > 1 && (x < 0.f || x > (float)(n - 1))) return RTM_ERR_ARG;
   *off = rtm::spread_coeffs(n, x, k1, k2, nlimit, dipole, ntaper, coeff);
+  return RTM_OK;
+}
+
+int rtm_r2r_line_matrix(int n, float d, int isign, float *D) {
+  if (!D || n < 2 || n > 65536 || !(d > 0.f) || (isign != 1 && isign != -1)) return RTM_ERR_ARG;
+  std::vector<float> m;
+  rtm::r2r_line_matrix(n, d, isign, m);
+  std::memcpy(D, m.data(), m.size() * 4);
   return RTM_OK;
 }
 

@@ -18,7 +18,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ISO, TTI, VTI, PropSpec, TraceSet
+from .spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ENGINE_R2R, ISO, TTI, VTI, PropSpec, TraceSet
 
 
 @dataclass
@@ -154,7 +154,7 @@ def spread_band(spec: PropSpec):
     engine's dispersion factor (bgprtm/FdEngine.cpp:241-256)."""
     if spec.engine == ENGINE_CFD:
         disp = 0.9
-    elif spec.engine == ENGINE_R2C:
+    elif spec.engine in (ENGINE_R2C, ENGINE_R2R):
         disp = 1.0  # pseudo-spectral engines keep FdEngine::getFdDispersion's default
     else:
         disp = 0.46 if spec.model_type >= VTI else 0.6

@@ -66,6 +66,7 @@ def _load_orc():
     lib.orc_taylor_weights.argtypes = [C.c_int, _f64p, _f64p]
     lib.orc_cfd_plan.argtypes = [C.c_int, C.c_float, C.c_int, _f32p, _f32p, _f32p]
     lib.orc_r2c_line.argtypes = [C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+    lib.orc_r2r_line.argtypes = [C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
     return lib
 
 
@@ -226,6 +227,14 @@ def r2c_line(x, d, isign):
     x = np.ascontiguousarray(x, np.float64)
     out = np.zeros_like(x)
     orc_lib().orc_r2c_line(x.size, d, isign, x.ctypes.data, out.ctypes.data)
+    return out
+
+
+def r2r_line(x, d, isign):
+    """FdEngine_r2r's derivative of one line (double), the oracle's matrix."""
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.zeros_like(x)
+    orc_lib().orc_r2r_line(x.size, d, isign, x.ctypes.data, out.ctypes.data)
     return out
 
 

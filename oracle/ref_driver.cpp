@@ -46,7 +46,7 @@ struct RefHandle {
 
 void set_globals(int engine, int model, float pml_eps, int pml3d, float scaler, int top_pml) {
   shim_store().kv.clear();
-  global_pars["Engine"] = engine == 1 ? "CFD" : engine == 2 ? "FFTWR2C" : "FD";
+  global_pars["Engine"] = engine == 1 ? "CFD" : engine == 2 ? "FFTWR2C" : engine == 3 ? "FFTWR2R" : "FD";
   global_pars["fd_use_taylor"] = 1;
   global_pars["pml_eps"] = pml_eps;
   global_pars["pml3d"] = pml3d;
@@ -74,7 +74,10 @@ void *ref_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt,
   h->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
   h->n = (size_t)nx * ny * nz;
   h->w0 = vol_alloc(h->n), h->w1 = vol_alloc(h->n), h->wr = vol_alloc(h->n), h->vel = vol_alloc(h->n);
-  h->k = new KernelCPU(nx, ny, nz, dx, dy, dz, engine == 1 ? FD::CFD : engine == 2 ? FD::FFTWR2C : FD::FD,
+  h->k = new KernelCPU(nx, ny, nz, dx, dy, dz, engine == 1   ? FD::CFD
+                       : engine == 2 ? FD::FFTWR2C
+                       : engine == 3 ? FD::FFTWR2R
+                                     : FD::FD,
                        h->nthreads);
   h->k->setJacob(nullptr, nullptr, nullptr, nullptr);
   h->k->setBoundary(nbnd[0], nbnd[1], nbnd[2], nbnd[3], nbnd[4], nbnd[5], dt, vmax);

@@ -13,7 +13,6 @@
 #include "MpiPrint.h"
 #include "TimeRecorder.h"
 #include "FdEngine_r2c.h"
-#include "FdEngine_r2r.h"
 #include "FdEngine_hfd.h"
 #include "Util.h"
 #include "libCommon/Taylor.h"
@@ -64,10 +63,45 @@ static struct TaylorInit {
 //        the imaginary parts of X_0 and (n even) X_{n/2} are not read.
 // Plain DFTs in double rounded to float: FFTW's results, not its rounding.
 struct fftwf_plan_s {
-  int n, c2r;
+  int n, c2r, kind;
 };
-fftwf_plan fftwf_plan_dft_r2c_1d(int n, float *, fftwf_complex *, unsigned) { return new fftwf_plan_s{n, 0}; }
-fftwf_plan fftwf_plan_dft_c2r_1d(int n, fftwf_complex *, float *, unsigned) { return new fftwf_plan_s{n, 1}; }
+fftwf_plan fftwf_plan_dft_r2c_1d(int n, float *, fftwf_complex *, unsigned) { return new fftwf_plan_s{n, 0, -1}; }
+fftwf_plan fftwf_plan_dft_c2r_1d(int n, fftwf_complex *, float *, unsigned) { return new fftwf_plan_s{n, 1, -1}; }
+fftwf_plan fftwf_plan_r2r_1d(int n, float *, float *, fftwf_r2r_kind kind, unsigned) {
+  return new fftwf_plan_s{n, 0, (int)kind};
+}
+// The four r2r kinds FdEngine_r2r plans (unnormalised, FFTW's definitions):
+//   REDFT10  Y_k = 2 sum_j X_j cos(pi (j + 1/2) k / n)
+//   REDFT01  Y_k = X_0 + 2 sum_{j>=1} X_j cos(pi j (k + 1/2) / n)
+//   RODFT10  Y_k = 2 sum_j X_j sin(pi (j + 1/2) (k + 1) / n)
+//   RODFT01  Y_k = (-1)^k X_{n-1} + 2 sum_{j<=n-2} X_j sin(pi (j + 1) (k + 1/2) / n)
+void fftwf_execute_r2r(const fftwf_plan p, float *in, float *out) {
+  const int n = p->n;
+  std::vector<double> y(n);
+  for (int k = 0; k < n; k++) {
+    double v = 0;
+    switch (p->kind) {
+      case FFTW_REDFT10:
+        for (int j = 0; j < n; j++) v += 2.0 * in[j] * std::cos(M_PI * (j + 0.5) * k / n);
+        break;
+      case FFTW_REDFT01:
+        v = in[0];
+        for (int j = 1; j < n; j++) v += 2.0 * in[j] * std::cos(M_PI * j * (k + 0.5) / n);
+        break;
+      case FFTW_RODFT10:
+        for (int j = 0; j < n; j++) v += 2.0 * in[j] * std::sin(M_PI * (j + 0.5) * (k + 1) / n);
+        break;
+      case FFTW_RODFT01:
+        v = (k % 2 ? -1.0 : 1.0) * in[n - 1];
+        for (int j = 0; j < n - 1; j++) v += 2.0 * in[j] * std::sin(M_PI * (j + 1) * (k + 0.5) / n);
+        break;
+      default:
+        assertion(false, "r2r kind not in the stand-in");
+    }
+    y[k] = v;
+  }
+  for (int k = 0; k < n; k++) out[k] = (float)y[k];
+}
 void fftwf_destroy_plan(fftwf_plan p) { delete p; }
 void fftwf_execute_dft_r2c(const fftwf_plan p, float *in, fftwf_complex *out) {
   const int n = p->n;
@@ -105,16 +139,8 @@ void Util::transpose(int nx, int ny, int dimIn, int dimOut, float *in, float *ou
     for (int iy = 0; iy < ny; iy++) out[(size_t)ix * dimOut + iy] = in[(size_t)iy * dimIn + ix];
 }
 
-// Engines KernelCPU's constructor can name (r2r / HFD); never selected here.
+// Engines KernelCPU's constructor can name (HFD); never selected here.
 #define NOT_BUILT(...) assertion(false, "engine not built in the oracle harness")
-FdEngine_r2r::FdEngine_r2r(int a, int b, int c, float d, float e, float f, int g) : FdEngine(a, b, c, d, e, f, g) { NOT_BUILT(); }
-FdEngine_r2r::~FdEngine_r2r() {}
-void FdEngine_r2r::dx1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2r::dy1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2r::dz1_2D(float *, float *, float *, int, int, int) {}
-void FdEngine_r2r::dx1_2D(float *, float *, float *, int, int, int, float *, float *) {}
-void FdEngine_r2r::dy1_2D(float *, float *, float *, int, int, int, float *, float *) {}
-void FdEngine_r2r::dz1_2D(float *, float *, float *, int, int, int, float *, float *) {}
 FdEngine_hfd::FdEngine_hfd(int a, int b, int c, float d, float e, float f, int g) : FdEngine(a, b, c, d, e, f, g) { NOT_BUILT(); }
 FdEngine_hfd::~FdEngine_hfd() {}
 void FdEngine_hfd::dx1_2D(float *, float *, float *, int, int, int) {}

@@ -31,7 +31,7 @@ using std::min;
 using std::vector;
 
 enum { ISO = 1, VTI = 2, TTI = 3 };
-enum { FD8 = 0, CFD = 1, R2C = 2 };
+enum { FD8 = 0, CFD = 1, R2C = 2, R2R = 3 };
 enum { X = 0, Y = 1, Z = 2 };
 enum { TOP = 0, BOT = 1 };
 
@@ -190,6 +190,57 @@ static void r2c_line(const vector<double> &c, int n, const R *x, R *b, size_t ld
   }
 }
 
+// FdEngine_r2r::fftderiv1_r2r (bgprtm/FdEngine_r2r.cpp:73-102) as the n x n
+// matrix it applies to a line.  isign +1: DCT-II (FFTW REDFT10), bin i <- -k_i
+// times bin i+1, last bin 0, DST-III (RODFT01); isign -1: DST-II (RODFT10),
+// bin i <- k_{i-1} times bin i-1, bin 0 0, DCT-III (REDFT01).  k_i = -(i+1) dk,
+// dk = pi / (d n) / 2 / n in float (constructor :11-13, assignW :66-70).  The
+// transforms are FFTW's unnormalised definitions:
+//   REDFT10 Y_k = 2 sum_j x_j cos(pi (j+1/2) k / n)
+//   REDFT01 Y_k = x_0 + 2 sum_{j>=1} x_j cos(pi j (k+1/2) / n)
+//   RODFT10 Y_k = 2 sum_j x_j sin(pi (j+1/2) (k+1) / n)
+//   RODFT01 Y_k = (-1)^k x_{n-1} + 2 sum_{j<=n-2} x_j sin(pi (j+1) (k+1/2) / n)
+// Row-major D[t][u] (out_t = sum_u D[t][u] x_u), in double.
+static vector<double> r2r_matrix(int n, float d, int isign) {
+  const float scale = 1.0f / float(n);
+  const float dk = (float)(M_PI / (double)(d * (float)n) * 0.5 * (double)scale);
+  vector<double> k(n), D((size_t)n * n);
+  for (int i = 0; i < n; i++) k[i] = (double)((float)(-(i + 1)) * dk);
+  vector<double> X(n), Y(n);
+  for (int u = 0; u < n; u++) {  // column u: the response to the unit line e_u
+    for (int q = 0; q < n; q++)
+      X[q] = isign == 1 ? 2.0 * std::cos(M_PI * (u + 0.5) * q / n) : 2.0 * std::sin(M_PI * (u + 0.5) * (q + 1) / n);
+    if (isign == 1) {
+      for (int i = 0; i < n - 1; i++) Y[i] = -k[i] * X[i + 1];
+      Y[n - 1] = 0;
+    } else {
+      for (int i = n - 1; i > 0; i--) Y[i] = k[i - 1] * X[i - 1];
+      Y[0] = 0;
+    }
+    for (int t = 0; t < n; t++) {
+      double v;
+      if (isign == 1) {
+        v = (t % 2 ? -1.0 : 1.0) * Y[n - 1];
+        for (int j = 0; j < n - 1; j++) v += 2.0 * Y[j] * std::sin(M_PI * (j + 1) * (t + 0.5) / n);
+      } else {
+        v = Y[0];
+        for (int j = 1; j < n; j++) v += 2.0 * Y[j] * std::cos(M_PI * j * (t + 0.5) / n);
+      }
+      D[(size_t)t * n + u] = v;
+    }
+  }
+  return D;
+}
+
+template <typename R>
+static void r2r_line(const vector<double> &D, int n, const R *x, R *b, size_t ld) {
+  for (int t = 0; t < n; t++) {
+    double v = 0;
+    for (int u = 0; u < n; u++) v += D[(size_t)t * n + u] * (double)x[u * ld];
+    b[t * ld] = (R)v;
+  }
+}
+
 template <typename R> struct TraceSet {
   int ntr = 0, lx = 0, ly = 0, lz = 0, nt = 0;
   vector<int> off, len;
@@ -210,6 +261,7 @@ public:
   R c1x[5], c1y[5], c1z[5], c2x[5], c2y[5], c2z[5];
   CfdPlan<R> cfdx, cfdy, cfdz;
   vector<double> r2c[3][2];  // FFTWR2C circulants [axis][round]: round 0 isign +1, round 1 isign -1
+  vector<double> r2r[3][2];  // FFTWR2R line matrices [axis][round]
   // PML: profile per dim/side (coef, distance from the outer edge) and memory
   // pml[dim][side][round][comp] (bgprtm/FdEngine.h:178)
   bool has_pml[3][2] = {};
@@ -248,13 +300,16 @@ public:
       cfdy.build(ny, dy);
       cfdz.build(nz, dz);
     }
-    if (cfg.engine == R2C) {
-      cfg.pml3d = 0;  // fftderiv1_r2c damps along the derivative's own axis only
+    if (cfg.engine == R2C || cfg.engine == R2R) {
+      cfg.pml3d = 0;  // fftderiv1_r2c / _r2r damp along the derivative's own axis only
       const int nn[3] = {nx, ny, nz};
       const float dd[3] = {(float)dx, (float)dy, (float)dz};
       for (int a = 0; a < 3; a++)
         if (nn[a] > 1)
-          for (int r = 0; r < 2; r++) r2c[a][r] = r2c_circulant(nn[a], dd[a], r == 0 ? 1 : -1);
+          for (int r = 0; r < 2; r++) {
+            if (cfg.engine == R2C) r2c[a][r] = r2c_circulant(nn[a], dd[a], r == 0 ? 1 : -1);
+            else r2r[a][r] = r2r_matrix(nn[a], dd[a], r == 0 ? 1 : -1);
+          }
     }
     build_pml();
     c16_tables(codec_table, wtaper20, wtaper10);
@@ -492,20 +547,24 @@ public:
     vector<R> d(nxyz);
     const CfdPlan<R> &p = axis == X ? cfdx : axis == Y ? cfdy : cfdz;
     int s = round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
-    if (cfg.engine == R2C) {
-      const vector<double> &c = r2c[axis][s];
+    if (cfg.engine == R2C || cfg.engine == R2R) {
+      const bool fft = cfg.engine == R2C;
+      const vector<double> &c = fft ? r2c[axis][s] : r2r[axis][s];
+      auto line = [&](int n, const R *x, R *b, size_t ld) {
+        if (fft) r2c_line(c, n, x, b, ld);
+        else r2r_line(c, n, x, b, ld);
+      };
       if (axis == Z) {
 #pragma omp parallel for schedule(static)
-        for (long l = 0; l < (long)nx * ny; l++) r2c_line(c, nz, in + l * nz, d.data() + l * nz, 1);
+        for (long l = 0; l < (long)nx * ny; l++) line(nz, in + l * nz, d.data() + l * nz, 1);
       } else if (axis == X) {
 #pragma omp parallel for collapse(2) schedule(static)
         for (int iy = 0; iy < ny; iy++)
-          for (int iz = 0; iz < nz; iz++) r2c_line(c, nx, in + iy * nxz + iz, d.data() + iy * nxz + iz, nz);
+          for (int iz = 0; iz < nz; iz++) line(nx, in + iy * nxz + iz, d.data() + iy * nxz + iz, nz);
       } else {
 #pragma omp parallel for collapse(2) schedule(static)
         for (int ix = 0; ix < nx; ix++)
-          for (int iz = 0; iz < nz; iz++)
-            r2c_line(c, ny, in + (size_t)ix * nz + iz, d.data() + (size_t)ix * nz + iz, nxz);
+          for (int iz = 0; iz < nz; iz++) line(ny, in + (size_t)ix * nz + iz, d.data() + (size_t)ix * nz + iz, nxz);
       }
     } else if (axis == Z) {
 #pragma omp parallel for schedule(static)
@@ -928,6 +987,11 @@ void orc_cfd_plan(int n, float d, int s, float *bm, float *bl, float *am) {
   std::copy(p.bm[s].begin(), p.bm[s].end(), bm);
   std::copy(p.bl[s].begin(), p.bl[s].end(), bl);
   std::copy(p.am[s].begin(), p.am[s].end(), am);
+}
+// The FFTWR2R derivative of one line of n points (double in and out).
+void orc_r2r_line(int n, float d, int isign, const double *x, double *out) {
+  const std::vector<double> D = orc::r2r_matrix(n, d, isign);
+  orc::r2r_line<double>(D, n, x, out, 1);
 }
 // The FFTWR2C derivative of one line of n points (double in and out).
 void orc_r2c_line(int n, float d, int isign, const double *x, double *out) {

@@ -3,7 +3,7 @@ and the tests; numpy's default_rng is reproducible across platforms)."""
 import numpy as np
 from scipy.ndimage import gaussian_filter
 
-from konglong_b200.spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ISO, TTI, VTI, PropSpec
+from konglong_b200.spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ENGINE_R2R, ISO, TTI, VTI, PropSpec
 
 # nx*nz kept a multiple of 4: the reference's SSE loops step 4 floats across
 # a y slab (bgprtm/KernelCPU.cpp:328-338).
@@ -20,6 +20,10 @@ CASES = {
     "iso_r2c": dict(engine=ENGINE_R2C, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=18),
     "vti_r2c": dict(engine=ENGINE_R2C, model=VTI, shape=(23, 20, 28), pml=6, steps=3, seed=19),
     "tti_r2c": dict(engine=ENGINE_R2C, model=TTI, shape=(24, 21, 27), pml=6, steps=3, seed=20),
+    # FFTWR2R: even and odd lines
+    "iso_r2r": dict(engine=ENGINE_R2R, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=21),
+    "vti_r2r": dict(engine=ENGINE_R2R, model=VTI, shape=(23, 20, 28), pml=6, steps=3, seed=22),
+    "tti_r2r": dict(engine=ENGINE_R2R, model=TTI, shape=(24, 21, 27), pml=6, steps=3, seed=23),
 }
 
 

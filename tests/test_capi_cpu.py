@@ -73,3 +73,18 @@ def test_config_defaults_follow_reference():
     L.rtm_config_default(C.byref(c))
     assert (c.pml3d, c.top_pml, c.q_order) == (1, 1, 4)
     assert abs(c.pml_eps - 1e-3) < 1e-9 and abs(c.pml3d_scaler - 0.3) < 1e-7
+
+
+@pytest.mark.parametrize("n", [20, 27, 64])
+@pytest.mark.parametrize("isign", [1, -1])
+def test_r2r_line_matrix_matches_oracle(n, isign):
+    """The engine's FFTWR2R line matrix (built on the host, applied on the GPU
+    as GEMMs) against the oracle's line derivative, column by column."""
+    D = np.zeros(n * n, np.float32)
+    assert _lib.lib().rtm_r2r_line_matrix(n, 10.0, isign, D) == 0
+    D = D.reshape(n, n).astype(np.float64)
+    want = np.stack([O.r2r_line(np.eye(n)[u], 10.0, isign) for u in range(n)], 1)
+    assert np.abs(D - want).max() <= 1e-6 * np.abs(want).max()
+    x = np.random.default_rng(n).standard_normal(n)
+    np.testing.assert_allclose(D @ x, O.r2r_line(x, 10.0, isign), rtol=0, atol=1e-5 * np.abs(D @ x).max())
+    assert _lib.lib().rtm_r2r_line_matrix(n, 10.0, 0, np.zeros(n * n, np.float32)) != 0

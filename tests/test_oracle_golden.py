@@ -48,10 +48,11 @@ def test_cfd_matches_reference_within_fp32_conditioning(golden, name):
     assert rel_l2(got, exact) < 2.0 * spread + 1e-6
 
 
-@pytest.mark.parametrize("name", [k for k in CASES if "r2c" in k])
+@pytest.mark.parametrize("name", [k for k in CASES if "r2c" in k or "r2r" in k])
 def test_r2c_matches_reference(golden, name):
-    """FFTWR2C: the reference's FdEngine_r2c (FFTW calls answered by DFTs in
-    double, Util::transpose completed) against the oracle's circulant form."""
+    """FFTWR2C / FFTWR2R: the reference's FdEngine_r2c / FdEngine_r2r (FFTW
+    calls answered by their defining sums in double, Util::transpose
+    completed) against the oracle's circulant / line-matrix forms."""
     got = run_oracle(CASES[name])
     assert rel_l2(got, golden[f"{name}__w1"]) < FD8_TOL
     assert rel_l2(run_oracle(CASES[name], double=True), golden[f"{name}__w1"]) < FD8_TOL
@@ -94,6 +95,21 @@ def test_r2c_odd_lines_have_a_growing_mode():
         dm = np.stack([O.r2c_line(e[i], 10.0, -1) for i in range(n)], 1)
         top = np.linalg.eigvals(dm @ dp).real.max()
         assert (top > 1e-3) == grows, (n, top)
+
+
+def test_r2r_is_stable_and_close_to_the_spectral_second_derivative():
+    """FFTWR2R's two passes (DCT-II -> shifted bins -> DST-III, then DST-II ->
+    DCT-III) make a non-positive operator for even and odd n whose low
+    eigenvalues are -(pi m / (n d))^2 to high accuracy."""
+    n, d = 40, 10.0
+    for nn in (n, n + 1):
+        e = np.eye(nn)
+        dp = np.stack([O.r2r_line(e[i], d, 1) for i in range(nn)], 1)
+        dm = np.stack([O.r2r_line(e[i], d, -1) for i in range(nn)], 1)
+        ev = np.sort(np.linalg.eigvals(dm @ dp).real)[::-1]
+        assert ev[0] < 1e-9
+        m = np.arange(1, 6)
+        np.testing.assert_allclose(-ev[1:6], (np.pi * m / (nn * d)) ** 2, rtol=1e-6)
 
 
 def test_codec_bit_exact(golden):
