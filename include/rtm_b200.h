@@ -159,6 +159,30 @@ int rtm_swap(rtm_handle *h);
 int rtm_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper,
                       float *coeff, int *off);
 
+/* Receiver FK true-amplitude / deghost spreading, space domain
+ * (Receiver::spread_sdomain, bgprtm/Receiver.cpp:851-1010, the default of
+ * Receiver::spread): the traces are spread onto the (ny, nx) receiver grid with
+ * their separable kernels, transformed over (y, x, t), filtered per bin
+ * (obliquity sqrt(1 - kh^2 / k^2) when trueamp; with deghost 1 / (2 sin(kz z))
+ * capped at 1 / ghost_threshold, the low-cut ramp, a quarter-period phase
+ * turn signed by side) and transformed back.  The result, one trace per grid
+ * column, is what the injection then spreads in z (a trace set with x / y
+ * kernels of length one).  Host in, host out, on the current device. */
+typedef struct rtm_fk_args {
+  int nx, ny, nt, ntfft; /* receiver grid (x, y), samples per trace, time FFT length (>= nt;
+                            libfftv::padfftv is not in the reference tree) */
+  float dt, dx, dy;      /* sample interval (s), grid spacing (m) */
+  float vsurf, z;        /* surface velocity (m/s), mean receiver depth below the surface (m) */
+  int trueamp, deghost;  /* obliquity factor; ghost removal */
+  int side;              /* -1 receivers (backward propagation), +1 sources */
+  float flcut, flpass;   /* souLowCut / souLowPass (Hz): low-cut ramp, with deghost */
+  float ghost_threshold; /* ghost_zerofreq_threshold (reference default 0.1) */
+  float khpass, khcut;   /* spread kernel band, as rtm_spread_coeffs */
+  int nlimit;            /* spread kernel length cap (2 x spread size) */
+} rtm_fk_args;
+/* xy [nr][2]: fractional grid indices (x, y); traces [nr][nt]; out [ny][nx][nt] */
+int rtm_fk_spread(const rtm_fk_args *a, int nr, const float *xy, const float *traces, float *out);
+
 /* The FFTWR2R first derivative along one axis of n points with spacing d as
  * the row-major n x n matrix D the engine applies to every line (out_t =
  * sum_u D[t][u] x_u): FdEngine_r2r::fftderiv1_r2r, bgprtm/FdEngine_r2r.cpp:73-102;

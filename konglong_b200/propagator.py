@@ -302,6 +302,28 @@ def spread_coeffs(n, x, k1, k2, nlimit, dipole=False, ntaper=0):
     return off.value, buf[:nl.value].copy()
 
 
+class FkArgs(C.Structure):
+    """rtm_fk_args (include/rtm_b200.h)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nt", C.c_int), ("ntfft", C.c_int),
+                ("dt", C.c_float), ("dx", C.c_float), ("dy", C.c_float), ("vsurf", C.c_float), ("z", C.c_float),
+                ("trueamp", C.c_int), ("deghost", C.c_int), ("side", C.c_int), ("flcut", C.c_float),
+                ("flpass", C.c_float), ("ghost_threshold", C.c_float), ("khpass", C.c_float), ("khcut", C.c_float),
+                ("nlimit", C.c_int)]
+
+
+def fk_spread(nx, ny, nt, ntfft, dt, dx, dy, xy, traces, vsurf, z, trueamp=1, deghost=0, side=-1, flcut=0.0,
+              flpass=0.0, ghost_threshold=0.1, khpass=0.4, khcut=0.48, nlimit=20):
+    """Receiver::spread_sdomain on the GPU: grid traces [ny][nx][nt] from traces
+    [nr][nt] at fractional grid positions xy [nr][2]."""
+    a = FkArgs(nx, ny, nt, ntfft, dt, dx, dy, vsurf, z, int(trueamp), int(deghost), int(side), flcut, flpass,
+               ghost_threshold, khpass, khcut, nlimit)
+    xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+    tr = np.ascontiguousarray(traces, np.float32).reshape(len(xy), nt)
+    out = np.zeros((ny, nx, nt), np.float32)
+    _lib.check(_lib.lib().rtm_fk_spread(C.byref(a), len(xy), xy.ravel(), tr.ravel(), out.ravel()), "rtm_fk_spread")
+    return out
+
+
 def c16_compress(a, nx, ny, nz):
     out = np.zeros((nx * nz + 2) * ny, np.uint16)
     _lib.check(_lib.lib().rtm_c16_compress(_arr(a), out, nx, ny, nz), "rtm_c16_compress")
