@@ -185,12 +185,17 @@ def build_workload(name, steps_total, scale=1.0):
         shot.spec.engine = 0
         shot.name = "vti_fd8"
         return shot
+    if name in ("vti_r2c", "vti_r2r"):  # the compact-FD model and shot through the pseudo-spectral engines
+        shot = W.vti_cfd(scale=scale, nt=steps_total)
+        shot.spec.engine = 2 if name == "vti_r2c" else 3
+        shot.name = name
+        return shot
     raise SystemExit(f"unknown workload {name}")
 
 
 def config_of(shot, snap_fmt, steps):
     s = shot.spec
-    return {"workload": f"{shot.name}: {s.nx}x{s.ny}x{s.nz} {'CFD' if s.engine else 'FD8'} "
+    return {"workload": f"{shot.name}: {s.nx}x{s.ny}x{s.nz} {['FD8', 'CFD', 'FFTWR2C', 'FFTWR2R'][s.engine]} "
                         f"{['', 'ISO', 'VTI', 'TTI'][s.model_type]}{'+Q' if s.use_q else ''}, PML {s.nbnd[0]}, "
                         f"dt {s.dt * 1e3:.4f} ms, forward RTM step, snapshots every {shot.interval} steps",
             "grid": [s.nx, s.ny, s.nz], "cells": s.n, "snapshot_format": ["fp32", "c16", "fp16s"][snap_fmt],
@@ -443,7 +448,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="vti_cfd",
-                    choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512", "small_shots"])
+                    choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512", "vti_r2c", "vti_r2r", "small_shots"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="grid scale of the workload (1.0 = the configuration the metric is quoted on; "
                          "smaller values are for profiler captures)")

@@ -179,6 +179,10 @@ typedef struct rtm_fk_args {
   float ghost_threshold; /* ghost_zerofreq_threshold (reference default 0.1) */
   float khpass, khcut;   /* spread kernel band, as rtm_spread_coeffs */
   int nlimit;            /* spread kernel length cap (2 x spread size) */
+  int domain;            /* 0: space domain (fk_domain SDOMAIN, the reference default);
+                            1: wavenumber domain (KDOMAIN, Receiver::spread_kdomain,
+                            bgprtm/Receiver.cpp:641-849; nx > 1, khpass < khcut) */
+  float fmax;            /* KDOMAIN: highest data frequency (Hz), scales the ghost threshold */
 } rtm_fk_args;
 /* xy [nr][2]: fractional grid indices (x, y); traces [nr][nt]; out [ny][nx][nt] */
 int rtm_fk_spread(const rtm_fk_args *a, int nr, const float *xy, const float *traces, float *out);

@@ -308,15 +308,15 @@ class FkArgs(C.Structure):
                 ("dt", C.c_float), ("dx", C.c_float), ("dy", C.c_float), ("vsurf", C.c_float), ("z", C.c_float),
                 ("trueamp", C.c_int), ("deghost", C.c_int), ("side", C.c_int), ("flcut", C.c_float),
                 ("flpass", C.c_float), ("ghost_threshold", C.c_float), ("khpass", C.c_float), ("khcut", C.c_float),
-                ("nlimit", C.c_int)]
+                ("nlimit", C.c_int), ("domain", C.c_int), ("fmax", C.c_float)]
 
 
 def fk_spread(nx, ny, nt, ntfft, dt, dx, dy, xy, traces, vsurf, z, trueamp=1, deghost=0, side=-1, flcut=0.0,
-              flpass=0.0, ghost_threshold=0.1, khpass=0.4, khcut=0.48, nlimit=20):
-    """Receiver::spread_sdomain on the GPU: grid traces [ny][nx][nt] from traces
-    [nr][nt] at fractional grid positions xy [nr][2]."""
+              flpass=0.0, ghost_threshold=0.1, khpass=0.4, khcut=0.48, nlimit=20, kdomain=False, fmax=60.0):
+    """Receiver::spread_sdomain (or spread_kdomain) on the GPU: grid traces
+    [ny][nx][nt] from traces [nr][nt] at fractional grid positions xy [nr][2]."""
     a = FkArgs(nx, ny, nt, ntfft, dt, dx, dy, vsurf, z, int(trueamp), int(deghost), int(side), flcut, flpass,
-               ghost_threshold, khpass, khcut, nlimit)
+               ghost_threshold, khpass, khcut, nlimit, int(bool(kdomain)), fmax)
     xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
     tr = np.ascontiguousarray(traces, np.float32).reshape(len(xy), nt)
     out = np.zeros((ny, nx, nt), np.float32)

@@ -52,15 +52,16 @@ def spread_grid(nx, ny, nt, ntfft, xy, traces, khpass, khcut, nlimit, ntaper=10)
     return g
 
 
-def fk_filter(spec, nx, ny, ntfft, dt, dx, dy, vsurf, z, trueamp, deghost, side, flcut, flpass, thr):
-    """The per-bin product of spread_sdomain on the half spectrum [ny][nx][nw]."""
+def fk_filter(spec, nx, ny, ntfft, dt, dx, dy, vsurf, z, trueamp, deghost, side, flcut, flpass, thr, scalar=None):
+    """The per-bin product on the half spectrum [ny][nx][nw]; `scalar` is
+    spread_sdomain's sqrt(1 / (nx ny ntfft)) unless given (spread_kdomain: 1)."""
     nw = ntfft // 2 + 1
     dkx = F32(0.0) if nx == 1 else F32(2.0 * np.pi / np.float64(F32(dx) * F32(nx)))
     dky = F32(0.0) if ny == 1 else F32(2.0 * np.pi / np.float64(F32(dy) * F32(ny)))
     dwv = F32(2.0 * np.pi / np.float64(F32(F32(dt) * F32(ntfft)) * F32(vsurf)))
     kx, ky = wavenumbers(nx, dkx), wavenumbers(ny, dky)
     kw = np.arange(nw).astype(F32) * dwv
-    scalar = F32(np.sqrt(1.0 / nx / ny / ntfft))
+    scalar = F32(np.sqrt(1.0 / nx / ny / ntfft)) if scalar is None else F32(scalar)
     iw_lc = int(np.rint(F32(F32(F32(flcut) * F32(dt)) * F32(ntfft))))
     iw_lp = int(np.rint(F32(F32(F32(flpass) * F32(dt)) * F32(ntfft))))
     out = np.zeros_like(spec)
@@ -96,5 +97,49 @@ def fk_deghost(nx, ny, nt, ntfft, dt, dx, dy, xy, traces, vsurf, z, trueamp, deg
     g = spread_grid(nx, ny, nt, ntfft, xy, traces, khpass, khcut, nlimit).astype(np.float64)
     spec = np.fft.rfftn(g, axes=(0, 1, 2))
     spec = fk_filter(spec, nx, ny, ntfft, dt, dx, dy, vsurf, z, trueamp, deghost, side, flcut, flpass, thr)
+    out = np.fft.irfftn(spec, s=(ny, nx, ntfft), axes=(0, 1, 2)) * (nx * ny * ntfft)
+    return out[:, :, :nt]
+
+
+def ktaper(n, k, k1, k2):
+    """Receiver::get_ktaper (bgprtm/Receiver.cpp:619-639): 1 below 2 k1 kmax,
+    0 above 2 k2 kmax, cos^2 between (float)."""
+    kmax = abs(F32(k[n // 2]))
+    a, b = F32(kmax * F32(k1 * 2)), F32(kmax * F32(k2 * 2))
+    ak = np.abs(k).astype(F32)
+    t = np.cos((ak - a) / (b - a) * np.pi / 2.0) ** 2
+    return np.where(ak < a, F32(1), np.where(ak > b, F32(0), t)).astype(F32)
+
+
+def fk_deghost_kdomain(nx, ny, nt, ntfft, dt, dx, dy, xy_m, traces, vsurf, z, trueamp, deghost, side=-1,
+                       flcut=0.0, flpass=0.0, thr=0.1, fmax=60.0, khpass=0.4, khcut=0.48):
+    """Receiver::spread_kdomain (bgprtm/Receiver.cpp:641-849): each trace,
+    scaled by sqrt(1 / (nx ny ntfft)), is transformed in time and summed into
+    the (ky, kx) grid with the phase shifts exp(-i (kx x + ky y)) of its offsets
+    from the grid origin and the k tapers; the per-bin product is
+    spread_sdomain's without the scalar, with the ghost threshold scaled by
+    sin(2 pi fmax z / vsurf) when that angle is below pi / 2 (:792-794); then
+    the inverse FFT over (y, x, t).  nx > 1 (with nx = 1 the reference's x taper
+    is 0 / 0)."""
+    nw = ntfft // 2 + 1
+    dkx = F32(2.0 * np.pi / np.float64(F32(dx) * F32(nx)))
+    dky = F32(0.0) if ny == 1 else F32(2.0 * np.pi / np.float64(F32(dy) * F32(ny)))
+    kx, ky = wavenumbers(nx, dkx), wavenumbers(ny, dky)
+    tkx = ktaper(nx, kx, khpass, khcut)
+    tky = ktaper(ny, ky, khpass, khcut) if ny > 1 else np.ones(1, F32)
+    scalar = F32(np.sqrt(1.0 / nx / ny / ntfft))
+    tw = np.zeros((len(traces), ntfft), np.float64)
+    tw[:, :nt] = (np.asarray(traces, F32)[:, :nt] * scalar).astype(F32)
+    T = np.fft.rfft(tw, axis=1)                                   # [nr][nw]
+    xy_m = np.asarray(xy_m, F32)
+    sx = np.exp(-1j * (xy_m[:, 0:1] * kx[None, :]).astype(F32)) * tkx[None, :]      # [nr][nx]
+    sy = np.exp(-1j * (xy_m[:, 1:2] * ky[None, :]).astype(F32)) * tky[None, :]      # [nr][ny]
+    spec = np.einsum("ry,rx,rw->yxw", sy, sx, T)
+    thr_eff = F32(thr)
+    kzdzmax = F32(F32(F32(F32(fmax) * F32(2 * np.pi)) / F32(vsurf)) * F32(z))
+    if kzdzmax < F32(np.pi / 2):
+        thr_eff = F32(thr_eff * np.sin(kzdzmax))
+    spec = fk_filter(spec, nx, ny, ntfft, dt, dx, dy, vsurf, z, trueamp, deghost, side, flcut, flpass, thr_eff,
+                     scalar=F32(1))
     out = np.fft.irfftn(spec, s=(ny, nx, ntfft), axes=(0, 1, 2)) * (nx * ny * ntfft)
     return out[:, :, :nt]

@@ -43,3 +43,21 @@ def test_evanescent_wavenumbers_are_removed():
                            nlimit=1)
         energy = np.abs(out[0, 4:-4]).max()
         assert (energy > 1e-2) == passes, (kx_idx, energy)
+
+
+def test_kdomain_equals_sdomain_on_grid_node_receivers():
+    """With one receiver on every grid node, delta spread kernels and k tapers
+    that pass every propagating wavenumber, the two forms filter the same
+    grid data: spread_kdomain's phase-shift sums are then the DFT of
+    spread_sdomain's grid."""
+    nx, ny, nt, ntfft = 16, 12, 64, 96
+    rng = np.random.default_rng(0)
+    xy = [(float(i), float(j)) for j in range(ny) for i in range(nx)]
+    t = np.arange(nt) * 0.004
+    tr = np.array([np.sin(2 * np.pi * 15 * t) * np.exp(-((t - 0.1) / 0.03) ** 2) * rng.uniform(0.5, 1) for _ in xy],
+                  np.float32)
+    for trueamp, deghost in ((1, 0), (0, 1), (1, 1)):
+        s = F.fk_deghost(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, xy, tr, 1500.0, 10.0, trueamp, deghost, nlimit=1)
+        k = F.fk_deghost_kdomain(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, [(x * 10.0, y * 10.0) for x, y in xy], tr,
+                                 1500.0, 10.0, trueamp, deghost, khpass=0.45, khcut=0.5, fmax=1000.0)
+        assert np.abs(s - k).max() <= 1e-6 * np.abs(s).max()
