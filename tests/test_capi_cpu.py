@@ -88,3 +88,33 @@ def test_r2r_line_matrix_matches_oracle(n, isign):
     x = np.random.default_rng(n).standard_normal(n)
     np.testing.assert_allclose(D @ x, O.r2r_line(x, 10.0, isign), rtol=0, atol=1e-5 * np.abs(D @ x).max())
     assert _lib.lib().rtm_r2r_line_matrix(n, 10.0, 0, np.zeros(n * n, np.float32)) != 0
+
+
+def test_new_entry_points_validate_arguments_without_gpu():
+    """Engines 0-3 only; the FK spreading and the learned-snapshot fallback
+    refuse bad arguments before touching a device."""
+    from konglong_b200.propagator import FkArgs
+    L = _lib.lib()
+    d = _lib.RtmDims(32, 32, 32, 10, 10, 10, 0.001)
+    c = _lib.RtmConfig()
+    L.rtm_config_default(C.byref(c))
+    c.engine = 4
+    h = C.c_void_p()
+    assert L.rtm_create(C.byref(d), C.byref(c), C.byref(h)) == -1 and not h.value
+    assert L.rtm_set_compressor_fallback(None, 1e-3, 0.1) == -1
+    good = dict(nx=16, ny=8, nt=50, ntfft=64, dt=0.004, dx=10.0, dy=10.0, vsurf=1500.0, z=10.0, trueamp=1,
+                deghost=1, side=-1, flcut=0.0, flpass=0.0, ghost_threshold=0.1, khpass=0.4, khcut=0.48, nlimit=20,
+                domain=0, fmax=60.0)
+    xy = np.array([[3.5, 2.0]], np.float32)
+    tr = np.zeros((1, 50), np.float32)
+    out = np.zeros((8, 16, 50), np.float32)
+    bad = [dict(ntfft=40), dict(side=0), dict(khpass=0.5, khcut=0.4), dict(domain=2), dict(domain=1, nx=1),
+           dict(domain=1, khpass=0.48), dict(ghost_threshold=0.0), dict(vsurf=0.0)]
+    for b in bad:
+        a = FkArgs(**{**good, **b})
+        o = np.zeros((a.ny, a.nx, a.nt), np.float32)
+        assert L.rtm_fk_spread(C.byref(a), 1, xy.ravel(), tr.ravel(), o.ravel()) == -1, b
+    a = FkArgs(**good)
+    for pos in ([[16.0, 2.0]], [[3.0, -0.5]], [[np.nan, 1.0]]):  # off the grid
+        p = np.array(pos, np.float32)
+        assert L.rtm_fk_spread(C.byref(a), 1, p.ravel(), tr.ravel(), out.ravel()) == -1, pos
