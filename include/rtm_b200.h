@@ -341,7 +341,8 @@ int rtm_set_compressor(rtm_handle *h, rtm_ae *a);
  * FP16 values of v / block scale, the 8^3 blocks whose scale exceeds tau x the
  * slot's largest, largest first, at most ceil(max_fraction x blocks) of them;
  * decoding overwrites those blocks.  max_fraction = 0 turns it off (default).
- * Clears existing RTM_SNAP_AE slots (their size changes).  No counterpart in the
+ * Clears existing RTM_SNAP_AE slots (their size changes) and their host
+ * offload (call rtm_snapshot_offload again).  No counterpart in the
  * reference (its WaveFieldCompress has no learned code). */
 int rtm_set_compressor_fallback(rtm_handle *h, float tau, float max_fraction);
 
