@@ -45,3 +45,26 @@ def test_fk_spread_matches_restatement(case):
         want = F.fk_deghost(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, xy, traces, **kw)
     assert np.abs(want).max() > 0
     assert rel_l2(got, want) < 1e-5
+
+
+@pytest.mark.parametrize("kdomain", [False, True])
+def test_fk_spread_edges(kdomain):
+    """No receivers gives a zero grid; receivers on the last grid node and at
+    the origin are accepted and match the restatement."""
+    nx, ny, nt, ntfft = 20, 12, 64, 96
+    z = fk_spread(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, np.zeros((0, 2), np.float32), np.zeros((0, nt), np.float32),
+                  1500.0, 10.0, kdomain=kdomain)
+    assert z.shape == (ny, nx, nt) and not np.any(z)
+    xy = np.array([[nx - 1, ny - 1], [0.0, 0.0], [7.25, 3.5]], np.float32)
+    t = np.arange(nt) * 0.004
+    traces = np.stack([np.sin(2 * np.pi * f * t) * np.exp(-((t - 0.1) / 0.03) ** 2) for f in (12, 18, 25)]
+                      ).astype(np.float32)
+    kw = dict(vsurf=1500.0, z=10.0, trueamp=1, deghost=1, side=-1)
+    got = fk_spread(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, xy, traces, kdomain=kdomain, fmax=40.0, **kw)
+    if kdomain:
+        want = F.fk_deghost_kdomain(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, xy * np.float32(10.0), traces, fmax=40.0,
+                                    **kw)
+    else:
+        want = F.fk_deghost(nx, ny, nt, ntfft, 0.004, 10.0, 10.0, xy, traces, **kw)
+    assert np.abs(want).max() > 0
+    assert rel_l2(got, want) < 1e-5

@@ -56,3 +56,30 @@ def test_r2c_rtm_image(engine):
     want = _rtm(shot, O.Oracle(shot.spec), spread_coeffs, SNAP_FP32, nt, nt, shot.interval)
     assert np.abs(want).max() > 0
     assert rel_l2(got.reshape(want.shape), want) < 1e-4
+
+
+@pytest.mark.parametrize("engine", [ENGINE_R2C, ENGINE_R2R])
+def test_pseudo_spectral_2d_grid(engine):
+    """A 2-D grid (ny = 1: no y derivative, no y plans) through both engines:
+    operator steps against the oracle."""
+    from konglong_b200.spec import VTI, PropSpec
+    nx, nz = 40, 36
+    s = PropSpec(nx=nx, ny=1, nz=nz, dx=10.0, dy=10.0, dz=10.0, dt=0.0006, engine=engine, model_type=VTI,
+                 nbnd=(6, 6, 0, 0, 6, 6), vmax=4500.0)
+    rng = np.random.default_rng(4)
+    model = dict(vel=(1800.0 + 2000.0 * rng.random(s.shape)).astype(np.float32),
+                 eps=(0.2 * rng.random(s.shape)).astype(np.float32), dl=(0.08 * rng.random(s.shape)).astype(np.float32))
+    w1 = rng.standard_normal(s.shape).astype(np.float32)
+    out = []
+    for cls in (Propagator, O.Oracle):
+        x = cls(s)
+        x.set_model(**model)
+        x.put(0, np.zeros_like(w1))
+        x.put(1, w1)
+        for _ in range(3):
+            x.kernel()
+            x.update2nd()
+            x.swap()
+        out.append(np.asarray(x.get(1), np.float64).ravel())
+    assert np.abs(out[1]).max() > 0
+    assert rel_l2(out[0], out[1]) < 1e-5
