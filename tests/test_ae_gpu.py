@@ -1,8 +1,9 @@
 """Learned snapshot compressor on the GPU: tensor-core forward and gradients
 against the CPU oracle, training on the engine's own forward wavefields, the
 gain of the trained network over the code without learning, and the learned
-snapshots inside an RTM shot next to the plain FP32 store (the fallback that
-judges its image error) and COMPRESS_16."""
+snapshots inside an RTM shot next to the plain FP32 store (the reference
+image their error is measured against) and COMPRESS_16, with and without the
+FP16 fallback of the high-energy blocks."""
 import numpy as np
 import pytest
 
