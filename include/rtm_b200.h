@@ -64,8 +64,11 @@ typedef enum rtm_status {
 /* FD::FD, FD::CFD, FD::FFTWR2C and FD::FFTWR2R (pseudo-spectral: FFT or
  * cosine / sine transform derivative along each axis, PML along the
  * derivative's own axis only, so pml3d is ignored; bgprtm/FdEngine_r2c.cpp,
- * bgprtm/FdEngine_r2r.cpp) */
-enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2, RTM_ENGINE_R2R = 3 };
+ * bgprtm/FdEngine_r2r.cpp), FD::CFD_BATCH (the Derivative path of
+ * Propagator::kernel, bgprtm/Propagator.cpp:901-943: compact FD through
+ * Derivative_cfd, Boundary's per-axis PML so pml3d is ignored, the
+ * divergence-pass plan of iswitch) */
+enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2, RTM_ENGINE_R2R = 3, RTM_ENGINE_CFDB = 4 };
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
 enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
@@ -86,7 +89,7 @@ typedef struct rtm_dims {
 } rtm_dims;
 
 typedef struct rtm_config {
-  int engine;         /* RTM_ENGINE_FD8, RTM_ENGINE_CFD, RTM_ENGINE_R2C or RTM_ENGINE_R2R */
+  int engine;         /* RTM_ENGINE_FD8 / _CFD / _R2C / _R2R / _CFDB */
   int model_type;     /* RTM_ISO, RTM_VTI, RTM_TTI */
   int use_q;          /* visco-acoustic memory variables (Q::order terms) */
   int q_order;        /* number of memory variables, default 4 */

@@ -403,6 +403,9 @@ static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out)
     if (launch_r2r_deriv(h->r2r, axis, sgn ? -1 : 1, in, out) != RTM_OK) h->fft_err = 1;
     return;
   }
+  // CFD_BATCH (the Derivative path) takes the divergence-pass plan from
+  // iswitch: plan 1 for TTI, plan 2 otherwise (bgprtm/Derivative.cpp:4-8, 92-112)
+  if (sgn && h->c.engine == RTM_ENGINE_CFDB && h->c.model_type == RTM_TTI) sgn = 0;
   if (axis != DZ && h->cfd_xy == 0) {
     launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
     return;
@@ -1230,7 +1233,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (!d || !c || !out) return RTM_ERR_ARG;
   *out = nullptr;
   if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
-      c->engine < 0 || c->engine > 3 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
+      c->engine < 0 || c->engine > 4 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
       c->pml_eps <= 0 || c->pml_eps >= 1) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
@@ -1242,9 +1245,10 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   rtm_handle *h = new rtm_handle();
   h->d = *d;
   h->c = *c;
-  // FdEngine_r2c / _r2r damp only along each derivative's own axis
-  // (bgprtm/FdEngine_r2c.cpp:240-243, FdEngine_r2r.cpp:95-98): no pml3d cross terms
-  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R) h->c.pml3d = 0;
+  // FdEngine_r2c / _r2r and the Derivative path's Boundary damp only along
+  // each derivative's own axis (bgprtm/FdEngine_r2c.cpp:240-243,
+  // FdEngine_r2r.cpp:95-98, Boundary.cpp:153-213): no pml3d cross terms
+  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R || c->engine == RTM_ENGINE_CFDB) h->c.pml3d = 0;
   h->n = (long long)d->nx * d->ny * d->nz;
   h->nxz = (long long)d->nx * d->nz;
   int rc = RTM_OK;
@@ -1292,7 +1296,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
       return fail(rc);
     }
   }
-  if (c->engine == RTM_ENGINE_CFD) {
+  if (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) {
     if (cfd_init() != 0) {
       h->err = "compact-FD kernel set-up failed";
       cudaGetLastError();
@@ -1385,7 +1389,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     h->an4_yseg = yseg_an4(h);
     if ((rc = an4_tiles(h))) return fail(rc);
   }
-  h->cfd_tma = c->engine == RTM_ENGINE_CFD && tma_supported(d->nz);
+  h->cfd_tma = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && tma_supported(d->nz);
   h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
@@ -2113,7 +2117,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     for (int y : {32, 64})
       if (ym != y && h->d.ny > y) cands.push_back({0, 0, y, h->tma_shape, h->tx, h->cfd_xy, 1});
   }
-  else if (h->c.engine == RTM_ENGINE_CFD && h->c.kernel_variant == 0) {
+  else if ((h->c.engine == RTM_ENGINE_CFD || h->c.engine == RTM_ENGINE_CFDB) && h->c.kernel_variant == 0) {
     cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
     if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
   }

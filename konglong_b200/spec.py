@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ENGINE_FD8, ENGINE_CFD, ENGINE_R2C, ENGINE_R2R = 0, 1, 2, 3  # FD::FD, FD::CFD, FD::FFTWR2C, FD::FFTWR2R
+ENGINE_FD8, ENGINE_CFD, ENGINE_R2C, ENGINE_R2R, ENGINE_CFDB = 0, 1, 2, 3, 4  # FD::FD, CFD, FFTWR2C, FFTWR2R, CFD_BATCH
 ISO, VTI, TTI = 1, 2, 3
 FORWARD, BACKWARD = 0, 1
 SNAP_FP32, SNAP_C16, SNAP_FP16S, SNAP_AE = 0, 1, 2, 3

@@ -18,7 +18,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .spec import ENGINE_CFD, ENGINE_FD8, ENGINE_R2C, ENGINE_R2R, ISO, TTI, VTI, PropSpec, TraceSet
+from .spec import ENGINE_CFD, ENGINE_CFDB, ENGINE_FD8, ENGINE_R2C, ENGINE_R2R, ISO, TTI, VTI, PropSpec, TraceSet
 
 
 @dataclass
@@ -152,7 +152,7 @@ def make_traceset(points, nx, ny, nz, spread, k1, k2, coeff_fn, ntaper_xy=10):
 def spread_band(spec: PropSpec):
     """src_apply_khpass / khcut defaults (bgprtm/ModelRegrid.cpp:86-87) from the
     engine's dispersion factor (bgprtm/FdEngine.cpp:241-256)."""
-    if spec.engine == ENGINE_CFD:
+    if spec.engine in (ENGINE_CFD, ENGINE_CFDB):  # names starting with "CFD" take the compact-FD factor
         disp = 0.9
     elif spec.engine in (ENGINE_R2C, ENGINE_R2R):
         disp = 1.0  # pseudo-spectral engines keep FdEngine::getFdDispersion's default

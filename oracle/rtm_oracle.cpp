@@ -31,7 +31,7 @@ using std::min;
 using std::vector;
 
 enum { ISO = 1, VTI = 2, TTI = 3 };
-enum { FD8 = 0, CFD = 1, R2C = 2, R2R = 3 };
+enum { FD8 = 0, CFD = 1, R2C = 2, R2R = 3, CFDB = 4 };
 enum { X = 0, Y = 1, Z = 2 };
 enum { TOP = 0, BOT = 1 };
 
@@ -295,7 +295,8 @@ public:
     py.assign(nxyz, 0);
     pz.assign(nxyz, 0);
     build_fd();
-    if (cfg.engine == CFD) {
+    if (cfg.engine == CFD || cfg.engine == CFDB) {
+      if (cfg.engine == CFDB) cfg.pml3d = 0;  // Boundary::applyX/Y/Z damp along their own axis only
       cfdx.build(nx, dx);
       cfdy.build(ny, dy);
       cfdz.build(nz, dz);
@@ -528,7 +529,7 @@ public:
 
   // derivative of a whole volume along axis, PML round `round`, then either
   // store (iacc = 0) or out -= deriv * vel (iacc = 1).
-  void deriv_volume(const R *in, R *out, int axis, int round, int iacc) {
+  void deriv_volume(const R *in, R *out, int axis, int round, int iacc, int plan = -1) {
     if (cfg.engine == FD8) {
 #pragma omp parallel for collapse(2) schedule(static)
       for (int iy = 0; iy < ny; iy++)
@@ -546,7 +547,7 @@ public:
     // FFTWR2C: the spectral circulant along lines, then the same
     vector<R> d(nxyz);
     const CfdPlan<R> &p = axis == X ? cfdx : axis == Y ? cfdy : cfdz;
-    int s = round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
+    int s = plan >= 0 ? plan : round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
     if (cfg.engine == R2C || cfg.engine == R2R) {
       const bool fft = cfg.engine == R2C;
       const vector<double> &c = fft ? r2c[axis][s] : r2r[axis][s];
@@ -638,8 +639,35 @@ public:
     if (ny > 1) deriv_volume(py.data(), w0.data(), Y, 1, 1);
   }
 
+  // The Derivative path of Propagator::kernel for Engine CFD_BATCH
+  // (bgprtm/Propagator.cpp:901-943): Derivative::getGradient (Derivative.cpp:
+  // 47-66: dx1 / dy1 / dz1 with isign 1, Boundary::apply* round 1),
+  // CalVTIscaler / CalTTIscaler (Propagator.cpp:1362-1492, the ScalarVTI / TTI
+  // arithmetic), getDiverge0 (Derivative.cpp:92-112: dz1, dx1, dy1 with isign
+  // iswitch = 1 for TTI and 2 otherwise, Boundary round 2, wb = (dz + dx) + dy),
+  // applyVel (wb *= vel, :1734-1746) and w0 -= wb.  Derivative_cfd's line
+  // operator is FdEngine_cfd's (Cfd_plan plans 1 / 2); Boundary's PML is
+  // PML::apply along each derivative's own axis.
+  void cfd_batch_kernel() {
+    if (nx > 1) deriv_volume(w1.data(), px.data(), X, 0, 0, 0);
+    if (ny > 1) deriv_volume(w1.data(), py.data(), Y, 0, 0, 0);
+    deriv_volume(w1.data(), pz.data(), Z, 0, 0, 0);
+    if (cfg.model_type == TTI || cfg.model_type == VTI) scale_gradient();
+    const int sw = cfg.model_type == TTI ? 0 : 1;
+    vector<R> wb(nxyz), buf(nxyz);
+    deriv_volume(pz.data(), wb.data(), Z, 1, 0, sw);
+    deriv_volume(px.data(), buf.data(), X, 1, 0, sw);
+    for (size_t i = 0; i < nxyz; i++) wb[i] = wb[i] + buf[i];
+    if (ny > 1) {
+      deriv_volume(py.data(), buf.data(), Y, 1, 0, sw);
+      for (size_t i = 0; i < nxyz; i++) wb[i] = wb[i] + buf[i];
+    }
+    for (size_t i = 0; i < nxyz; i++) w0[i] = w0[i] - wb[i] * vel[i];
+  }
+
   void kernel() {
     if (cfg.engine == FD8 && cfg.model_type == ISO) iso_fd8_kernel();
+    else if (cfg.engine == CFDB) cfd_batch_kernel();
     else aniso_kernel();
   }
 

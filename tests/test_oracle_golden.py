@@ -172,3 +172,29 @@ def test_pml_profile(golden):
     t = (np.float32(w) - np.arange(w, dtype=np.float32)) / np.float32(w)
     coef = np.float32(0.75) * t * t * dg1
     np.testing.assert_allclose(coef, golden["pml_coef_20"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_cfd_batch_is_the_compact_fd_path_without_cross_damping(model):
+    """Engine CFD_BATCH (the Derivative path: Derivative_cfd + Boundary) and
+    Engine CFD (KernelCPU + FdEngine_cfd) with pml3d off differ for ISO and
+    VTI only in the order of the divergence sum, so in float64 they agree to
+    rounding; for TTI the divergence pass takes plan 1 (iswitch) instead of 2."""
+    from konglong_b200.spec import ENGINE_CFD, ENGINE_CFDB
+    from tests.golden_inputs import case_inputs
+
+    def run(engine, model, double):
+        c = dict(engine=engine, model=model, shape=(24, 20, 28), pml=6, steps=3, seed=31, pml3d=False)
+        spec, m, w0, w1 = case_inputs(c)
+        o = O.Oracle(spec, double=double)
+        o.set_model(**m)
+        o.put(0, w0)
+        o.put(1, w1)
+        for _ in range(3):
+            o.kernel()
+            o.update2nd()
+            o.swap()
+        return o.get(1)
+
+    assert rel_l2(run(ENGINE_CFDB, model, True), run(ENGINE_CFD, model, True)) < 1e-11
+    assert rel_l2(run(ENGINE_CFDB, 3, True), run(ENGINE_CFD, 3, True)) > 1e-3
