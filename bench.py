@@ -391,7 +391,7 @@ def cpu_baseline(shot, max_seconds=20.0):
     if not O.ref_available():
         return None, "port"
     s = shot.spec
-    if s.use_q:
+    if s.use_q or s.engine not in (0, 1):  # the FFT engines' FFTW calls are answered by DFT sums here
         return None, "reference"
     threads = os.cpu_count() or 1
     r = O.Reference(s, nthreads=threads)
@@ -414,6 +414,9 @@ def run_reference(args, rank, world):
     shot = build_workload(args.workload, args.steps + args.warmup + 8, args.scale)
     s = shot.spec
     threads = os.cpu_count() or 1
+    if s.engine not in (0, 1):
+        return {"unavailable": "the reference's FFT engines call FFTW, absent from this image; the harness answers "
+                               "those calls with plain DFT sums, which would time the stand-in, not the reference"}
     if O.ref_available() and not s.use_q:
         r = O.Reference(s, nthreads=threads)
         r.set_model(shot.vel, shot.eps, shot.dl, shot.pjx, shot.pjy)
@@ -471,6 +474,9 @@ def main():
         if not R.runs_reference_arm(ranks):
             return
         r = run_reference(args, rank, world)
+        if "unavailable" in r:
+            print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}), flush=True)
+            return
         shot = r["shot"]
         line = {"metric": "Gpts/s per step", "value": r["value"], "unit": "Gpts/s", "n_gpus": args.gpus,
                 "steps": r["k"], "warmup": min(args.warmup, 1), "ms_per_step": r["t"] / r["k"] * 1e3,

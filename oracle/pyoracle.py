@@ -281,6 +281,8 @@ class Reference:
         self.h = self.lib.ref_create(s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.dt, s.engine,
                                      s.model_type, nb, s.vmax, s.pml_eps, int(s.pml3d),
                                      s.pml3d_scaler, int(s.top_pml), nthreads)
+        if not self.h:
+            raise ValueError(f"engine {s.engine}: not a KernelCPU engine of the compiled reference")
         self.n = s.nx * s.ny * s.nz
         self._keep = []
 

@@ -68,6 +68,7 @@ extern "C" {
 void *ref_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt, int engine, int model,
                  const int *nbnd, float vmax, float pml_eps, int pml3d, float pml3d_scaler, int top_pml,
                  int nthreads) {
+  if (engine < 0 || engine > 3) return nullptr;  // KernelCPU engines only (FD, CFD, FFTWR2C, FFTWR2R)
   set_globals(engine, model, pml_eps, pml3d, pml3d_scaler, top_pml);
   RefHandle *h = new RefHandle();
   h->nx = nx, h->ny = ny, h->nz = nz, h->model = model, h->engine = engine, h->dt = dt;
