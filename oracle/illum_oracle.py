@@ -9,8 +9,11 @@
   image *= factor.
 
 Volumes are numpy arrays of shape (ny, nx, nz) (z fastest, the reference layout).
-Parity: restated from the reference's sources; not run against the reference itself
-(the functions sit in files whose build needs the absent libCommon)."""
+Parity: the box averages are pinned against the reference's own volumefilter.cpp
+(compiled into oracle/_ref with a stand-in for libFFTV's transpose; fixtures in
+tests/golden, agreement 1e-6 under the reference build's -ffast-math);
+computeDamping / applyDamping are restated (ImagingCondition.cpp needs libFFTV's
+filters to build)."""
 import numpy as np
 
 F32 = np.float32

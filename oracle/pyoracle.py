@@ -266,6 +266,8 @@ def ref_lib():
         lib.ref_cfd_plan.argtypes = [C.c_int, C.c_float, C.c_int, _f32p, _f32p, _f32p]
         lib.ref_pml_coef.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                      C.c_float, _f32p]
+        lib.ref_avg_volume3d.argtypes = [C.c_void_p] + [C.c_int] * 6
+        lib.ref_avg_volume2d.argtypes = [C.c_void_p] + [C.c_int] * 4
         _ref = lib
     return _ref
 
@@ -349,6 +351,19 @@ def ref_cfd_plan(n, d, s):
     am = np.zeros(60, np.float32)
     ref_lib().ref_cfd_plan(n, d, s, bm, bl, am)
     return bm, bl, am
+
+
+def ref_avg_volume(a, sx, sz, sy=None):
+    """volumefilter.cpp's avgVolume3D (ny > 1, half widths sx, sy, sz) or
+    avgVolume2D (x, z) on a copy of a [ny][nx][nz]."""
+    L = ref_lib()
+    v = np.ascontiguousarray(a, np.float32).copy()
+    ny, nx, nz = v.shape
+    if ny > 1:
+        L.ref_avg_volume3d(v.ctypes.data, nx, ny, nz, sx, sx if sy is None else sy, sz)
+    else:
+        L.ref_avg_volume2d(v.ctypes.data, nx, nz, sx, sz)
+    return v
 
 
 def ref_pml_coef(n, npml, d, dt, vmax, pml_eps=1e-3):

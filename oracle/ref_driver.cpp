@@ -21,6 +21,7 @@
 #include "FdEngine.h"
 #include "GetPar.h"
 #include "KernelCPU.h"
+#include "volumefilter.h"
 #include "PML.h"
 #include "WaveFieldCompress.h"
 
@@ -214,4 +215,8 @@ void ref_pml_coef(int n, int npml, float d, float dt, float vmax, float pml_eps,
   PML pml(n, npml, 1, d, dt, vmax, false);
   memcpy(coef, pml.coef.data(), sizeof(float) * npml);
 }
+
+// volumefilter.cpp's running box averages (illumination smoothing), in place
+void ref_avg_volume3d(float *a, int nx, int ny, int nz, int sx, int sy, int sz) { avgVolume3D(a, nx, ny, nz, sx, sy, sz); }
+void ref_avg_volume2d(float *a, int nx, int nz, int sx, int sz) { avgVolume2D(a, nx, nz, sx, sz); }
 }

@@ -15,6 +15,7 @@
 #include "FdEngine_r2c.h"
 #include "FdEngine_hfd.h"
 #include "Util.h"
+#include "libFFTV/transpose.h"
 #include "libCommon/Taylor.h"
 #include "../oracle_common.hpp"
 
@@ -130,6 +131,15 @@ void fftwf_execute_dft_c2r(const fftwf_plan p, fftwf_complex *in, float *out) {
   }
   for (int t = 0; t < n; t++) out[t] = (float)y[t];
 }
+
+// libfftv::ssetranspose, as volumefilter.cpp uses it (a plain transpose of
+// n2 rows of n1 values)
+namespace libfftv {
+void ssetranspose(int n1, int n2, float *in, int ldin, float *out, int ldout) {
+  for (int r = 0; r < n2; r++)
+    for (int c = 0; c < n1; c++) out[(size_t)c * ldout + r] = in[(size_t)r * ldin + c];
+}
+}  // namespace libfftv
 
 // Util::transpose (bgprtm/Util.cpp:25-76) as intended: out[ix][iy] =
 // in[iy][ix] for nx x ny, row pitches dimIn / dimOut.  The reference's SSE

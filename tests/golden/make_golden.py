@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import pyoracle as O  # noqa: E402
-from tests.golden_inputs import CASES, case_inputs, codec_input  # noqa: E402
+from tests.golden_inputs import CASES, ILLUM_SMOOTH, case_inputs, codec_input, illum_input  # noqa: E402
 
 
 def main():
@@ -47,6 +47,9 @@ def main():
         for s in (0, 1):
             bm, bl, am = O.ref_cfd_plan(n, 10.0, s)
             out[f"cfd_plan_{n}_{s}__bm"], out[f"cfd_plan_{n}_{s}__bl"], out[f"cfd_plan_{n}_{s}__am"] = bm, bl, am
+    # illumination smoothing: volumefilter.cpp's running box averages
+    for name, (shape, hxy, hz) in ILLUM_SMOOTH.items():
+        out[f"illum_smooth_{name}"] = O.ref_avg_volume(illum_input(name), hxy, hz)
     out["pml_coef_20"] = O.ref_pml_coef(128, 20, 10.0, 0.001, 4500.0)
     out["pml_coef_32"] = O.ref_pml_coef(512, 32, 10.0, 0.0007, 4500.0)
     np.savez_compressed(os.path.join(HERE, "reference_kernels.npz"), **out)

@@ -59,3 +59,13 @@ def codec_input():
     a[6] *= np.float32(1e-20)                  # sub-threshold slab
     b = rng.standard_normal((8, 16, 12)).astype(np.float32)  # no tapers (small grid)
     return {"wave": (a, nx, ny, nz), "small": (b, 16, 8, 12)}
+
+
+# illumination smoothing (avgVolume3D / avgVolume2D): volume shape, half widths (xy, z)
+ILLUM_SMOOTH = {"grid": ((20, 24, 28), 6, 4), "line": ((1, 30, 26), 5, 7), "deep": ((12, 16, 40), 3, 10)}
+
+
+def illum_input(name):
+    shape = ILLUM_SMOOTH[name][0]
+    rng = np.random.default_rng(100 + len(name))
+    return (rng.random(shape) ** 2 * 10).astype(np.float32)
