@@ -268,6 +268,8 @@ def ref_lib():
                                      C.c_float, _f32p]
         lib.ref_avg_volume3d.argtypes = [C.c_void_p] + [C.c_int] * 6
         lib.ref_avg_volume2d.argtypes = [C.c_void_p] + [C.c_int] * 4
+        lib.ref_spread_coeffs.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_int), C.c_int,
+                                          _f32p]
         _ref = lib
     return _ref
 
@@ -364,6 +366,14 @@ def ref_avg_volume(a, sx, sz, sy=None):
     else:
         L.ref_avg_volume2d(v.ctypes.data, nx, nz, sx, sz)
     return v
+
+
+def ref_spread_coeffs(n, x, k1, k2, nlimit, dipole=False):
+    """The reference's Util::CompactOrmsbySpreadCoeff: (first index, coefficients)."""
+    nl = C.c_int(nlimit)
+    buf = np.zeros(max(nlimit, 1), np.float32)
+    off = ref_lib().ref_spread_coeffs(n, x, k1, k2, C.byref(nl), int(dipole), buf)
+    return off, buf[:nl.value].copy()
 
 
 def ref_pml_coef(n, npml, d, dt, vmax, pml_eps=1e-3):

@@ -21,6 +21,7 @@
 #include "FdEngine.h"
 #include "GetPar.h"
 #include "KernelCPU.h"
+#include "Util.h"
 #include "volumefilter.h"
 #include "PML.h"
 #include "WaveFieldCompress.h"
@@ -214,6 +215,11 @@ void ref_pml_coef(int n, int npml, float d, float dt, float vmax, float pml_eps,
   global_pars["pml_eps"] = pml_eps;
   PML pml(n, npml, 1, d, dt, vmax, false);
   memcpy(coef, pml.coef.data(), sizeof(float) * npml);
+}
+
+// Util::CompactOrmsbySpreadCoeff with a kernel-length cap; returns the first index
+int ref_spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, float *coeff) {
+  return Util::CompactOrmsbySpreadCoeff(n, coeff, x, k1, k2, nlimit, dipole != 0, false);
 }
 
 // volumefilter.cpp's running box averages (illumination smoothing), in place

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import pyoracle as O  # noqa: E402
-from tests.golden_inputs import CASES, ILLUM_SMOOTH, case_inputs, codec_input, illum_input  # noqa: E402
+from tests.golden_inputs import CASES, ILLUM_SMOOTH, case_inputs, codec_input, illum_input, spread_cases  # noqa: E402
 
 
 def main():
@@ -47,6 +47,14 @@ def main():
         for s in (0, 1):
             bm, bl, am = O.ref_cfd_plan(n, 10.0, s)
             out[f"cfd_plan_{n}_{s}__bm"], out[f"cfd_plan_{n}_{s}__bl"], out[f"cfd_plan_{n}_{s}__am"] = bm, bl, am
+    # spread kernels: Util::CompactOrmsbySpreadCoeff
+    offs, coefs = [], []
+    for n, x, k1, k2, nl, dip in spread_cases():
+        o, c = O.ref_spread_coeffs(n, x, k1, k2, nl, dip)
+        offs.append((o, len(c)))
+        coefs.append(np.pad(c, (0, 40 - len(c))))
+    out["spread_offsets"] = np.array(offs, np.int32)
+    out["spread_coeffs"] = np.array(coefs, np.float32)
     # illumination smoothing: volumefilter.cpp's running box averages
     for name, (shape, hxy, hz) in ILLUM_SMOOTH.items():
         out[f"illum_smooth_{name}"] = O.ref_avg_volume(illum_input(name), hxy, hz)

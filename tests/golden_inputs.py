@@ -69,3 +69,19 @@ def illum_input(name):
     shape = ILLUM_SMOOTH[name][0]
     rng = np.random.default_rng(100 + len(name))
     return (rng.random(shape) ** 2 * 10).astype(np.float32)
+
+
+def spread_cases(count=120):
+    """(n, x, k1, k2, nlimit, dipole) of the spread-kernel fixtures: Ormsby bands,
+    sinc (k1 == k2) and dipole kernels, caps from 1 to 40."""
+    rng = np.random.default_rng(55)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(2, 300))
+        x = float(np.float32(rng.uniform(0, n - 1)))
+        k1 = float(np.float32(rng.uniform(0.05, 0.5)))
+        k2 = float(np.float32(rng.uniform(k1, 0.5))) if rng.random() < 0.5 else k1
+        nl = int(rng.integers(1, 40))
+        dip = bool(rng.random() < 0.3) and nl >= 2
+        out.append((n, x, k1, k2, nl, dip))
+    return out

@@ -198,3 +198,22 @@ def test_cfd_batch_is_the_compact_fd_path_without_cross_damping(model):
 
     assert rel_l2(run(ENGINE_CFDB, model, True), run(ENGINE_CFD, model, True)) < 1e-11
     assert rel_l2(run(ENGINE_CFDB, 3, True), run(ENGINE_CFD, 3, True)) > 1e-3
+
+
+def test_spread_coeffs_match_reference(golden):
+    """The restated CompactOrmsbySpreadCoeff against the reference's own
+    Util.cpp:317-397 (its libCommon sinc / dipole / Blackman from the
+    stand-ins): same offsets and lengths; values to 1e-5 of the kernel's peak,
+    plus the conditioning of the Ormsby difference (a2^2 sinc2^2 - a1^2 sinc1^2)
+    / (a2 - a1) for nearly equal bands, where the reference's -ffast-math
+    rounding differs."""
+    from tests.golden_inputs import spread_cases
+    offs, coefs = golden["spread_offsets"], golden["spread_coeffs"]
+    for j, (n, x, k1, k2, nl, dip) in enumerate(spread_cases()):
+        o, c = O.spread_coeffs(n, x, k1, k2, nl, dip, 0)
+        assert (o, len(c)) == tuple(offs[j]), (j, n, x, nl)
+        if len(c) == 0:  # x within half a cell of the edge: an empty kernel on both sides
+            continue
+        ref = coefs[j][:len(c)]
+        tol = 1e-5 + (1e-7 / max(k2 - k1, 1e-6) if k1 != k2 and not dip else 0.0)
+        assert np.abs(c - ref).max() <= tol * max(np.abs(ref).max(), 1e-30), (j, k2 - k1)
