@@ -118,3 +118,25 @@ def test_new_entry_points_validate_arguments_without_gpu():
     for pos in ([[16.0, 2.0]], [[3.0, -0.5]], [[np.nan, 1.0]]):  # off the grid
         p = np.array(pos, np.float32)
         assert L.rtm_fk_spread(C.byref(a), 1, p.ravel(), tr.ravel(), out.ravel()) == -1, pos
+
+
+def test_every_handle_entry_point_rejects_a_null_handle():
+    """Every call that takes a handle (engine, batch or compressor) returns a
+    negative status for a null one and touches nothing else - no device, no
+    crash: the reference's assertion()/exit paths become status codes."""
+    raw = C.CDLL(_lib.lib()._name)
+    skip = {"rtm_config_default", "rtm_last_error", "rtm_ae_nparams", "rtm_spread_coeffs", "rtm_r2r_line_matrix",
+            "rtm_fk_spread", "rtm_c16_compress_noalloc", "rtm_create", "rtm_batch_create", "rtm_ae_create"}
+    checked = 0
+    for name in _lib.EXPORTS:
+        typed = getattr(_lib.lib(), name)
+        at = list(typed.argtypes or [])
+        if name in skip or not at or at[0] is not C.c_void_p:
+            continue
+        f = getattr(raw, name)
+        conv = [t if t in (C.c_int, C.c_float, C.c_double, C.c_longlong, C.c_size_t) else C.c_void_p for t in at]
+        f.argtypes, f.restype = conv, C.c_int
+        args = [0.0 if t in (C.c_float, C.c_double) else (None if t is C.c_void_p else 0) for t in conv]
+        assert f(*args) < 0, name
+        checked += 1
+    assert checked >= 40
