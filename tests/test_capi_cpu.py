@@ -140,3 +140,25 @@ def test_every_handle_entry_point_rejects_a_null_handle():
         assert f(*args) < 0, name
         checked += 1
     assert checked >= 40
+
+
+@pytest.mark.parametrize("bad", [dict(model_type=0), dict(model_type=4), dict(q_order=0), dict(q_order=9),
+                                 dict(pml_eps=0.0), dict(pml_eps=1.0), dict(vmax=0.0), dict(engine=-1)])
+def test_create_rejects_bad_configuration_without_gpu(bad):
+    L = _lib.lib()
+    d = _lib.RtmDims(32, 32, 32, 10, 10, 10, 0.001)
+    c = _lib.RtmConfig()
+    L.rtm_config_default(C.byref(c))
+    for k, v in bad.items():
+        setattr(c, k, v)
+    h = C.c_void_p()
+    assert L.rtm_create(C.byref(d), C.byref(c), C.byref(h)) == -1 and not h.value
+
+
+def test_noalloc_codec_rejects_bad_arguments_without_gpu():
+    L = _lib.lib()
+    f = C.CDLL(L._name).rtm_c16_compress_noalloc
+    f.argtypes, f.restype = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int
+    assert f(None, None, 8, 8, 8, None) == -1
+    assert f(C.c_void_p(16), C.c_void_p(32), 8, 0, 8, None) == -1
+    assert f(C.c_void_p(16), C.c_void_p(32), 8, 1 << 20, 8, None) == -1  # more y slabs than the fixed scratch
