@@ -83,7 +83,7 @@ enum {
 };
 
 typedef struct rtm_dims {
-  int nx, ny, nz;   /* grid incl. PML; nx, nz >= 9 */
+  int nx, ny, nz;   /* grid incl. PML; nx, nz >= 9, 1 <= ny <= 65535 */
   float dx, dy, dz; /* spacing (m) */
   float dt;         /* time step (s) */
 } rtm_dims;
@@ -284,24 +284,27 @@ int rtm_put(rtm_handle *h, int field, const float *src);
 
 /* The reference's COMPRESS_16 codec on host buffers, run on the device
  * (bit-exact with WaveFieldCompress::compress16/uncompress16).  out holds
- * (nx*nz + 2) * ny uint16 values.  uncompress applies the decode tapers. */
+ * (nx*nz + 2) * ny uint16 values, ny <= 65535.  uncompress applies the decode
+ * tapers. */
 int rtm_c16_compress(const float *in, unsigned short *out, int nx, int ny, int nz);
 int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int nz);
 
 /* No counterpart in the reference.  COMPRESS_16 encoding of a wavefield that is
- * already on the device, for callers that cannot allocate GPU memory (a fixed
- * up-front memory budget, work recorded into the caller's own CUDA graph, a
+ * already on the device, for callers that cannot allocate GPU memory (a host
+ * program that carves all of HBM up front with its own pool allocator, or a
  * thread that must not wait on the allocator).  d_in: nx*ny*nz floats,
  * d_out: (nx*nz + 2)*ny uint16, both device memory of the current device, same
  * layout and bit-exact codes as rtm_c16_compress.  Allocates nothing: its
  * scratch (one float per y slab) is a fixed array of RTM_NOALLOC_MAX_SLABS
  * floats that every GPU loading the library holds until exit; ny above that
- * limit returns RTM_ERR_ARG.  The first call on a device looks the array's
- * device address up (cudaGetSymbolAddress), so make that first call before
- * any stream capture.  Runs asynchronously on `stream` (a cudaStream_t, NULL
- * = default stream).  All calls on a device share the scratch: calls that can
- * overlap on the GPU (different streams without ordering) race. */
-#define RTM_NOALLOC_MAX_SLABS 65536
+ * limit returns RTM_ERR_ARG.  The first call in a CUDA context (the runtime's
+ * primary context of a device, or a context the caller made current) looks
+ * the array's device address up (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  Runs asynchronously on `stream` (a
+ * cudaStream_t, NULL = default stream).  All calls on a device share the
+ * scratch, which keeps the last call's contents: calls that can overlap on the
+ * GPU (different streams without ordering) race, so order or serialise them. */
+#define RTM_NOALLOC_MAX_SLABS 65535
 int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, int ny, int nz, void *stream);
 
 /* Device time of the last rtm_modelling / rtm_migration call (ms, CUDA events). */

@@ -1232,7 +1232,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   using namespace rtm;
   if (!d || !c || !out) return RTM_ERR_ARG;
   *out = nullptr;
-  if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
+  if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->ny > 65535 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
       c->engine < 0 || c->engine > 4 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
       c->pml_eps <= 0 || c->pml_eps >= 1) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
@@ -1944,7 +1944,8 @@ int rtm_put(rtm_handle *h, int field, const float *src) {
 }
 
 int rtm_c16_compress(const float *in, unsigned short *out, int nx, int ny, int nz) {
-  if (!in || !out || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  // the encode kernel runs one grid row per y slab (gridDim.y <= 65535)
+  if (!in || !out || nx < 1 || ny < 1 || nz < 1 || ny > 65535) return RTM_ERR_ARG;
   const size_t n = (size_t)nx * ny * nz, nc = ((size_t)nx * nz + 2) * ny;
   float *din = nullptr, *slab = nullptr;
   uint16_t *dout = nullptr;
@@ -1962,7 +1963,8 @@ int rtm_c16_compress(const float *in, unsigned short *out, int nx, int ny, int n
 }
 
 int rtm_c16_uncompress(const unsigned short *in, float *out, int nx, int ny, int nz) {
-  if (!in || !out || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
+  // the decode kernel runs one grid layer per y slab (gridDim.z <= 65535)
+  if (!in || !out || nx < 1 || ny < 1 || nz < 1 || ny > 65535) return RTM_ERR_ARG;
   const size_t n = (size_t)nx * ny * nz, nc = ((size_t)nx * nz + 2) * ny;
   float *dout = nullptr, *slab = nullptr, *ex = nullptr, *ey = nullptr, *ez = nullptr;
   uint16_t *din = nullptr;

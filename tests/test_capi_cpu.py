@@ -162,3 +162,4 @@ def test_noalloc_codec_rejects_bad_arguments_without_gpu():
     assert f(None, None, 8, 8, 8, None) == -1
     assert f(C.c_void_p(16), C.c_void_p(32), 8, 0, 8, None) == -1
     assert f(C.c_void_p(16), C.c_void_p(32), 8, 1 << 20, 8, None) == -1  # more y slabs than the fixed scratch
+    assert f(C.c_void_p(16), C.c_void_p(32), 1, 65536, 1, None) == -1    # one above RTM_NOALLOC_MAX_SLABS

@@ -1,9 +1,9 @@
 """The allocation-free COMPRESS_16 entry point (rtm_c16_compress_noalloc).
 
-It serves callers that cannot allocate GPU memory (a fixed memory budget, work
-recorded into their own CUDA graph, threads that must not wait on the
-allocator): they pass device buffers and the entry point's scratch lives in a
-fixed array of the library.  Its codes must equal those of the allocating
+It serves callers that cannot allocate GPU memory (a host program that carves
+all of HBM up front with its own pool allocator, or a thread that must not
+wait on the allocator): they pass device buffers and the entry point's scratch
+lives in a fixed array of the library.  Its codes must equal those of the allocating
 entry point rtm_c16_compress bit for bit, on two calls in a row (the second
 call reuses the scratch the first one left behind).  This file is collected
 last so a run that stops at the first failure has run every other test.
@@ -36,7 +36,25 @@ def test_noalloc_compress_matches_allocating_entry_point():
         np.testing.assert_array_equal(got, want)
 
 
-def test_noalloc_rejects_too_many_slabs():
+def test_noalloc_at_the_slab_limit_matches_allocating_entry_point():
+    """ny = RTM_NOALLOC_MAX_SLABS (65535, the largest y extent a launch grid
+    row count allows) with one cell per slab runs and equals the allocating
+    entry point; one slab more is refused before anything is launched."""
+    import torch
     from konglong_b200 import _lib
+    from konglong_b200.propagator import c16_compress
+
     L = _lib.lib()
-    assert L.rtm_c16_compress_noalloc(1, 1, 4, 65537, 4, None) == _lib.STATUS_CODE["RTM_ERR_ARG"]
+    ny = 65535
+    rng = np.random.default_rng(7)
+    a = (rng.standard_normal(ny) * np.exp(rng.uniform(-20, 5, ny))).astype(np.float32)
+    want = c16_compress(a, 1, ny, 1)
+    d_in = torch.from_numpy(a).cuda()
+    for _ in range(2):
+        d_out = torch.zeros(want.size, dtype=torch.int16, device="cuda")
+        assert L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), 1, ny, 1, None) == 0
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint16), want)
+    err = _lib.STATUS_CODE["RTM_ERR_ARG"]
+    assert L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), 1, ny + 1, 1, None) == err
+    assert L.rtm_c16_compress_noalloc(1, 1, 4, 65537, 4, None) == err
