@@ -74,10 +74,26 @@ def kernel_alg_bytes(spec, m):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
 # launch, from ncu captures of the same kernels on the 0.75-scale grid of the
-# vti_cfd workload (profiles/*_vti_cfd_384x384x300.md).  The PML slabs scale
-# with the grid, so bytes per cell carry over to the full grid.
+# vti_cfd workload.  The PML slabs scale with the grid, so bytes per cell carry
+# over to the full grid.  Each entry records the SHA-256 prefix of the kernel
+# source it was captured on; when the source has changed since, the figure no
+# longer describes the kernel that runs and the bench reports traffic as null.
 MEASURED_DRAM_B_PER_CELL = {"vti_cfd": {"cfd_div_epilogue": 36.98, "cfd_grad_epilogue": 40.64,
                                         "cfd_x": 6.87, "cfd_y": 6.87}}
+MEASURED_DRAM_SOURCE = {"vti_cfd": ("konglong_b200/csrc/kernels_cfd.cu", "cdae83a8a550fc67")}
+
+
+def measured_traffic_current(workload):
+    """True when the kernel source behind MEASURED_DRAM_B_PER_CELL[workload] is unchanged."""
+    import hashlib
+    src = MEASURED_DRAM_SOURCE.get(workload)
+    if not src:
+        return False
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), src[0]), "rb") as f:
+            return hashlib.sha256(f.read()).hexdigest()[:16] == src[1]
+    except OSError:
+        return False
 
 
 class ClockSampler:
@@ -267,9 +283,11 @@ def run_cuda(args, rank, world):
             "kernels_ms_per_step": {k: round(v[0] / K, 4) for k, v in prof.items()}}
     roof["frac"] = roof["achieved"] / peak
     bpc = MEASURED_DRAM_B_PER_CELL.get(args.workload, {}).get(dom)
-    if bpc is not None:
+    if bpc is not None and measured_traffic_current(args.workload):
         roof["traffic"] = bpc * cells
         roof["traffic_source"] = "ncu DRAM bytes per cell at 0.75 scale x cells of one launch"
+    elif bpc is not None:
+        roof["traffic_source"] = "stale: the kernel source changed since the ncu capture"
 
     # end to end through the public API with host buffers: modelling run of K
     # steps with the receiver samples read back (set_injection H2D of the

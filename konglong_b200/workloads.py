@@ -85,33 +85,65 @@ def fd8_k1max():
     return float(np.sqrt(np.float32(s)) * np.float32(1.01))
 
 
-def cfl_dt(spec: PropSpec, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None, maxfreq=None):
-    """ModelPrepare::calcDeltaTime restated (bgprtm/ModelPrepare.cpp:647-881),
-    rectangular grid, no density: FD engines use k1max of the Taylor table, the
-    others pi; VTI/TTI take the largest phase velocity over the grid-axis
-    combinations and divide by sqrt(1+2 eps) again; Q rescales."""
-    k1 = fd8_k1max() if spec.engine == ENGINE_FD8 else np.pi
-    rd = np.array([1 / spec.dx ** 2, 1 / spec.dy ** 2 if spec.ny > 1 else 0.0, 1 / spec.dz ** 2])
+def cfl_dt(spec: PropSpec, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None, maxfreq=None, rho=None,
+           qref=None):
+    """ModelPrepare::calcDeltaTime restated (bgprtm/ModelPrepare.cpp:647-881)
+    for a rectangular grid.  k1max: FdEngine_fd::get_k1max for the FD engine
+    (bgprtm/FdEngine_fd.cpp:69-81), pi otherwise (:652-654).  Per cell:
+      ISO  lambda = v sqrt(rdx2 + rdy2 + rdz2)                        (:702-716)
+      VTI  tmp = (1 + 2e)(rdx2 + rdy2) + rdz2,
+           lambda = v sqrt((tmp + sqrt(tmp^2 - 8 (e - d)(rdx2 + rdy2) rdz2)) / 2),
+           dt_cell = 2 / k1max / lambda / sqrt(1 + 2e)                (:741-757)
+      TTI  the wavenumbers 1/dx, 1/dy, 1/dz rotated into the symmetry axis
+           frame (sin theta = |(pjx, pjy)|, cos phi = -pjx / sin theta,
+           sin phi = -pjy / sin theta), then the largest VTI lambda over the
+           axis combinations ic = 1 .. nc-1 (nc 8 in 3-D, 4 in 2-D)   (:838-881)
+    With a density model lambda is multiplied by sqrt(rho) per cell and the
+    minimum dt by sqrt(min rho) (:679-700, :720-738, :795-836).  With Q:
+    dt *= 1 - max(1/Q) (3 + 2/pi ln(maxfreq / qref)), qref = maxfreq / 3 by
+    default (:885-891)."""
+    k1 = fd8_k1max() if spec.engine == ENGINE_FD8 else float(np.float32(np.pi))
+    three_d = spec.ny > 1
+    v = np.asarray(vel, np.float64).ravel()
+    sr = np.sqrt(np.asarray(rho, np.float64).ravel()) if rho is not None else 1.0
+    rdx2, rdz2 = 1.0 / spec.dx ** 2, 1.0 / spec.dz ** 2
+    rdy2 = 1.0 / spec.dy ** 2 if three_d else 0.0
     if spec.model_type == ISO or eps is None:
-        lam = float(vel.max()) * np.sqrt(rd.sum())
-        dt = 2.0 / k1 / lam
+        lam = v * sr * np.sqrt(rdx2 + rdy2 + rdz2)
+        dt = float(np.min(2.0 / k1 / lam))
     else:
-        # VTI (axis along z): the reference loops every cell; the bound is
-        # monotone in v and eps, so the per-cell maximum is taken directly
-        v = vel.ravel().astype(np.float64)
-        e = eps.ravel().astype(np.float64)
-        d = dl.ravel().astype(np.float64)
-        lam = np.zeros_like(v)
-        for ic in range(1, 8):
-            icz, icx, icy = ic & 1, (ic >> 1) & 1, (ic >> 2) & 1
-            h2 = rd[0] * icx + rd[1] * icy
-            z2 = rd[2] * icz
-            t1 = (1 + 2 * e) * h2 + z2
-            lam = np.maximum(lam, v * np.sqrt((t1 + np.sqrt(np.maximum(t1 * t1 - 8 * (e - d) * h2 * z2, 0))) / 2))
+        e = np.asarray(eps, np.float64).ravel()
+        d = np.asarray(dl, np.float64).ravel()
+        if spec.model_type == VTI or pjx is None:
+            h2 = rdx2 + rdy2
+            tmp = (1 + 2 * e) * h2 + rdz2
+            lam = v * np.sqrt((tmp + np.sqrt(np.maximum(tmp * tmp - 8 * (e - d) * h2 * rdz2, 0))) / 2)
+        else:
+            px_ = np.asarray(pjx, np.float64).ravel()
+            py_ = np.asarray(pjy, np.float64).ravel() if pjy is not None else np.zeros_like(px_)
+            st = np.sqrt(px_ * px_ + py_ * py_)
+            ct = np.sqrt(np.maximum(1 - st * st, 0))
+            big = st > 1e-15
+            cp = np.where(big, -px_ / np.where(big, st, 1), 1.0)
+            sp = np.where(big, -py_ / np.where(big, st, 1), 0.0)
+            akx, aky, akz = 1 / spec.dx, 1 / spec.dy, 1 / spec.dz
+            rx = (cp * ct * akx + sp * ct * aky - st * akz) ** 2
+            ry = (-sp * akx + cp * aky) ** 2 if three_d else np.zeros_like(v)
+            rz = (cp * st * akx + sp * st * aky + ct * akz) ** 2
+            lam = np.zeros_like(v)
+            for ic in range(1, 8 if three_d else 4):
+                icz, icx, icy = ic & 1, (ic >> 1) & 1, (ic >> 2) & 1
+                h2 = rx * icx + ry * icy
+                z2 = rz * icz
+                t1 = (1 + 2 * e) * h2 + z2
+                lam = np.maximum(lam, v * np.sqrt((t1 + np.sqrt(np.maximum(t1 * t1 - 8 * (e - d) * h2 * z2, 0))) / 2))
+        lam = lam * sr
         dt = float(np.min(2.0 / k1 / lam / np.sqrt(1 + 2 * e)))
+    if rho is not None:
+        dt *= float(np.sqrt(np.min(np.asarray(rho, np.float64))))
     if spec.use_q and invq is not None and maxfreq:
-        qref = maxfreq / 3
-        dt *= 1 - float(invq.max()) * (3 + 2 / np.pi * np.log(maxfreq / qref))
+        qr = maxfreq / 3 if qref is None else qref
+        dt *= 1 - float(np.max(invq)) * (3 + 2 / np.pi * np.log(maxfreq / qr))
     return dt
 
 
