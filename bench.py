@@ -63,10 +63,18 @@ def kernel_alg_bytes(spec, m):
     """Compulsory HBM bytes per cell of one launch of each kernel kind (inputs
     read once, outputs written once, PML memory of the cells in PML slabs)."""
     aniso = 8.0 * (spec.model_type >= 2) + 8.0 * (spec.model_type == 3)
+    q = (4.0 + 3 * 4.0 * spec.q_order) if spec.use_q else 0.0
     return {"iso_fd8_step": 16.0 + 16.0 * m,
             "grad_fd8": 4.0 + aniso + 12.0 + 24.0 * m,
             "div_fd8": 12.0 + 12.0 + 4.0 + 24.0 * m,
             "cfd_z": 8.0, "cfd_x": 8.0, "cfd_y": 8.0,
+            # segment-parallel pipeline: a line solve with one first-derivative
+            # PML component round (Z, X), the fused y kernel (w1, gx, gz and the
+            # anisotropy parameters in; px, pz, dy out; two PML rounds), the fused
+            # x kernel (px, dz, dy, vel, w0, w1 in; w0 out; one PML round)
+            "cfd_z_seg": 8.0 + 8.0 * m, "cfd_x_seg": 8.0 + 8.0 * m,
+            "cfd_y_fused": 4.0 + 8.0 + aniso + 12.0 + 16.0 * m,
+            "cfd_x_fused": 24.0 + 4.0 + 8.0 * m + q,
             "cfd_grad_epilogue": 24.0 + aniso + 24.0 * m,
             "cfd_div_epilogue": 28.0 + 24.0 * m,
             "fused_io": 6.0, "slab_max": 4.0}
@@ -271,6 +279,8 @@ def run_cuda(args, rank, world):
     except Exception:
         pass
     kbytes = kernel_alg_bytes(s, pml_fraction(s))
+    if "cfd_y_fused" in prof:  # segment-parallel pipeline: its Z / X launches carry a PML round
+        kbytes["cfd_z"], kbytes["cfd_x"] = kbytes["cfd_z_seg"], kbytes["cfd_x_seg"]
     dom = max(prof, key=lambda k: prof[k][0])
     dom_ms = prof[dom][0] / prof[dom][1]
     dom_bytes = kbytes.get(dom, 8.0) * cells

@@ -104,12 +104,21 @@ typedef struct rtm_config {
                          drivers only (the stepwise seam calls return RTM_ERR_UNSUPPORTED) */
   int kernel_variant; /* 0: auto (FD8: 4 z cells per thread with TMA rings when nz % 4 == 0 and,
                          for VTI / TTI, the state is FP32; the autotuner picks among all FD8
-                         kernels; compact FD: register-streamed x / y line solves, the autotuner
-                         may pick TMA tiles), 1: one cell per thread / plain staged tiles, 2:
-                         compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline, 3: FD8 4 z
-                         cells per thread with TMA rings, 4: ISO FD8 4 z cells per thread with
-                         register prefetch (the 4-cell variants fall back to 1 when they do not
-                         apply) */
+                         kernels; compact FD on a 3-D grid: the segment-parallel line solves
+                         with the PML, scaling and update fused into them, else register-streamed
+                         x / y line solves; the autotuner may pick any compact-FD form), 1: one
+                         cell per thread / plain staged tiles, 2: compact-FD x / y TMA tiles, ISO
+                         FD8 one-cell TMA plane pipeline, 3: FD8 4 z cells per thread with TMA
+                         rings, 4: ISO FD8 4 z cells per thread with register prefetch, 5:
+                         compact FD split into line solves and pointwise epilogues with
+                         register-streamed x / y lines, 6: compact FD segment-parallel with plain
+                         tile loads (the 4-cell and segment-parallel variants fall back when
+                         they do not apply) */
+  int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):
+                         the gradient is divided by rho (KernelCPU::divideRho) and the divergence
+                         accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes
+                         the first-derivative passes (bgprtm/KernelCPU.cpp:128).  FD8 density runs
+                         use the one-cell passes; not with state_fp16 */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;
@@ -131,11 +140,13 @@ const char *rtm_last_error(const rtm_handle *h);
  * precede rtm_set_model when use_q. */
 int rtm_set_q_coeffs(rtm_handle *h, float cq0, const float *cq, const float *wq);
 
-/* KernelCPU::setModel + Propagator::Vel2 (bgprtm/KernelCPU.cpp:76-83,
- * bgprtm/Propagator.cpp:711-742).  vel is velocity in m/s; it is converted to
- * (v*dt)^2 on the device (Q-corrected when use_q).  eps/del are needed for
- * VTI/TTI, pjx/pjy for TTI, invq (1/Q) for use_q; others may be NULL. */
-int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float *del,
+/* KernelCPU::setModel(vel, rho, del, eps, pjx, pjy) + Propagator::Vel2
+ * (bgprtm/KernelCPU.cpp:76-83, bgprtm/Propagator.cpp:711-742).  vel is
+ * velocity in m/s; it is converted to (v*dt)^2 on the device (Q-corrected when
+ * use_q).  rho (density, > 0) is required when the configuration sets use_rho
+ * and must be NULL otherwise; eps/del are needed for VTI/TTI, pjx/pjy for TTI,
+ * invq (1/Q) for use_q; others may be NULL. */
+int rtm_set_model(rtm_handle *h, const float *vel, const float *rho, const float *eps, const float *del,
                   const float *pjx, const float *pjy, const float *invq);
 
 /* Zero wavefields, PML memory, Q memory and the extracted traces
@@ -399,7 +410,9 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice);
  * prefetch, 2 ISO 4 z cells with TMA rings, 3 ISO one-cell TMA pipeline,
  * 4 FD8 VTI / TTI 4 z cells with TMA rings),
  * desc[1] its tile width or shape index, desc[2] its y segment (0: default),
- * desc[3] the compact-FD x / y kernel; *ms the time of its `steps` steps.
+ * desc[3] the compact-FD form (0 streamed, 1 TMA or 2 plain x / y tiles of the
+ * split pipeline, 3 / 4 segment-parallel with TMA / plain tile loads); *ms the
+ * time of its `steps` steps.
  * RTM_ERR_ARG when idx is out of range. */
 int rtm_autotune_result(rtm_handle *h, int idx, int desc[4], float *ms);
 
@@ -420,7 +433,9 @@ enum {
   RTM_K_EXTRACT = 9,
   RTM_K_SLAB = 10,     /* per-slab max of the 16-bit snapshot formats */
   RTM_K_IO = 11,       /* standalone snapshot store / imaging condition */
-  RTM_NKINDS = 12
+  RTM_K_CFD_YF = 12,   /* compact FD, segment-parallel: fused y kernel (y gradient, scaling, y divergence part) */
+  RTM_K_CFD_XF = 13,   /* compact FD, segment-parallel: fused x kernel (x divergence part, accumulation, update) */
+  RTM_NKINDS = 14
 };
 /* on = 1: the time loops run eagerly (no CUDA graph) with CUDA events around
  * every launch, and the per-kind device time accumulates; on = 0 resets. */

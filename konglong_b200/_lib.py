@@ -36,7 +36,7 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_ae_compress_volume", "rtm_ae_decompress_volume", "rtm_set_compressor"]
 
 KERNEL_KINDS = ["iso_fd8_step", "grad_fd8", "div_fd8", "cfd_z", "cfd_x", "cfd_y", "cfd_grad_epilogue",
-                "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io"]
+                "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io", "cfd_y_fused", "cfd_x_fused"]
 
 
 class RtmDims(C.Structure):
@@ -48,7 +48,8 @@ class RtmConfig(C.Structure):
     _fields_ = [("engine", C.c_int), ("model_type", C.c_int), ("use_q", C.c_int),
                 ("q_order", C.c_int), ("nbnd", C.c_int * 6), ("vmax", C.c_float),
                 ("pml_eps", C.c_float), ("pml3d", C.c_int), ("pml3d_scaler", C.c_float),
-                ("top_pml", C.c_int), ("state_fp16", C.c_int), ("kernel_variant", C.c_int)]
+                ("top_pml", C.c_int), ("state_fp16", C.c_int), ("kernel_variant", C.c_int),
+                ("use_rho", C.c_int)]
 
 
 class RtmError(RuntimeError):
@@ -79,7 +80,7 @@ def lib():
     L.rtm_last_error.argtypes = [vp]
     L.rtm_last_error.restype = C.c_char_p
     L.rtm_set_q_coeffs.argtypes = [vp, f, _f32p, _f32p]
-    L.rtm_set_model.argtypes = [vp] + [vp] * 6
+    L.rtm_set_model.argtypes = [vp] + [vp] * 7
     for name in ("rtm_reset", "rtm_kernel", "rtm_update2nd", "rtm_swap"):
         getattr(L, name).argtypes = [vp]
     L.rtm_spread_coeffs.argtypes = [i, f, f, f, C.POINTER(i), i, i, _f32p, C.POINTER(i)]

@@ -52,6 +52,7 @@ struct GradArgs {
   const float *w1;
   float *px, *py, *pz;
   const float *eps, *del, *pjx, *pjy;
+  const float *rho;  // density (null: none); one-cell passes only
   float c1x[5], c1y[5], c1z[5];
   PmlDev pml;
   FusedIo io;
@@ -64,6 +65,7 @@ struct DivArgs {
   const float *w1;
   float *w0;
   const float *vel;
+  const float *rho;  // density (null: none); one-cell passes only
   float c1x[5], c1y[5], c1z[5];
   PmlDev pml;
   QDev q;
@@ -187,6 +189,13 @@ struct CfdPlanDev {
   int c0, c1;
   float lmc[4], buc[4], rdc;
   float a[60];  // copy of am, read from the kernel-parameter (constant) bank
+  // segment-parallel solve: nseg segments of seglen rows (the last one takes
+  // the remainder, >= 8 rows); [n][4] tables: hf = response of the forward
+  // value of row i to unit entering forward states of its segment, gb = the
+  // segment-local back substitution of hf, hb = response of the backward
+  // value to unit entering backward states (zero where a segment has none)
+  int nseg, seglen;
+  const float *hf, *gb, *hb;
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();
@@ -201,10 +210,43 @@ void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out
 void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                              cudaStream_t st);
 
+// ---- segment-parallel compact-FD step (engine CFD, 3-D grids) --------------
+// Five launches per step:
+//   Z(w1) -> gz, X(w1) -> gx                     first derivatives, PML round 1
+//   Y fused: Y(w1) -> gy, PML round 1; rho division and VTI / TTI scaling of
+//            (gx, gy, gz) -> px, pz in place, py kept in shared memory;
+//            Y(py) -> dy with PML round 2
+//   Z(pz) -> dz                                  PML round 2
+//   X fused: X(px) -> dx with PML round 2; w0 - vel (dx + dz + dy) (x, z, y in
+//            turn, KernelCPU::TTI's order), then update2nd / the Q update
+struct CfdSegArgs {
+  int nx, ny, nz, pml3d, model, mode;
+  PmlDev pml;
+  QDev q;
+  const float *w1, *vel, *eps, *del, *pjx, *pjy, *rho;  // rho null: no density model
+  float *w0;
+  float *gx, *gz;  // x / z gradients, overwritten by the scaled px / pz
+  float *dz, *dy;  // divergence parts along z and y
+};
+int cfd_seg_init();
+// largest line length the segment-parallel kernels take along axis (shared memory)
+int cfd_seg_max_n(int axis);
+// Z or X line derivative of `in` into `out`, PML round `round` on that component;
+// tin: tensor map of `in` with box (32, R, 1) for X (null: plain loads)
+void launch_cfd_seg_line(int axis, int round, const CfdPlanDev &p, const float *in, float *out, const CfdSegArgs &a,
+                         const CUtensorMap *tin, int *err, cudaStream_t st);
+// the fused y kernel (plans pg: gradient pass, pd: divergence pass; tin: map of
+// w1 with box (32, 1, R)) and the fused x kernel (tin: map of px, box (32, R, 1))
+void launch_cfd_seg_yfused(const CfdPlanDev &pg, const CfdPlanDev &pd, const CfdSegArgs &a, const CUtensorMap *tin,
+                           int *err, cudaStream_t st);
+void launch_cfd_seg_xfused(const CfdPlanDev &p, const CfdSegArgs &a, const CUtensorMap *tin, int *err,
+                           cudaStream_t st);
+
 struct CfdGradEpiArgs {  // PML round 1 + scaling on raw gradients, in place
   int nx, ny, nz, pml3d, model;
   float *gx, *gy, *gz;
   const float *eps, *del, *pjx, *pjy;
+  const float *rho;  // density (null: none): the gradient is divided by it
   PmlDev pml;
   FusedIo io;
   const float *w1;
@@ -217,6 +259,10 @@ struct CfdDivEpiArgs {  // PML round 2 on raw divergence parts + update
   const float *w1;
   float *w0;
   const float *vel;
+  // density (null: none) and the engine's form of the accumulation with it:
+  // 0 FdEngine_cfd, 1 FdEngine_r2c / _r2r, 2 the Derivative path
+  const float *rho;
+  int rho_form;
   PmlDev pml;
   QDev q;
 };

@@ -587,6 +587,7 @@ __device__ __forceinline__ void grad_cell(const CfdGradEpiArgs &a, const Grid3 &
   if (a.model >= 2) ep = __ldg(a.eps + i), dl = __ldg(a.del + i);
   if (a.model == 3) ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
   if (PML) pml1_all<0, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
+  if (a.rho) divide_rho(__ldg(a.rho + i), do_y, gx, gy, gz);
   if (a.model >= 2) {
     float e = ep;
     const float d = e - dl;
@@ -629,9 +630,17 @@ __device__ __forceinline__ void div_cell(const CfdDivEpiArgs &a, const Grid3 &g,
   const float w0 = a.w0[i];
   const float w1 = MODE != 0 ? __ldg(a.w1 + i) : 0.f;
   if (PML) pml1_all<1, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
-  float t = w0 - dxv * vel;
-  t = t - dzv * vel;
-  t = t - dyv * vel;
+  float t;
+  if (a.rho) {
+    const float r = __ldg(a.rho + i);
+    t = a.rho_form == 2   ? div_accumulate_rho<2>(w0, vel, r, dxv, dzv, dyv)
+        : a.rho_form == 1 ? div_accumulate_rho<1>(w0, vel, r, dxv, dzv, dyv)
+                          : div_accumulate_rho<0>(w0, vel, r, dxv, dzv, dyv);
+  } else {
+    t = w0 - dxv * vel;
+    t = t - dzv * vel;
+    t = t - dyv * vel;
+  }
   float out;
   if (MODE == 0) out = t;
   else out = MODE == 1 ? (w1 + w1) - t : q_update(a.q, i, g.nxz * a.ny, t, w1);
@@ -772,6 +781,639 @@ void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
     else if (a.mode == 1) div_box<K, 1>(a, bx[K], all, st);
     else div_box<K, 2>(a, bx[K], all, st);
   });
+}
+
+
+// ============================================================================
+// Segment-parallel line solves and the fused compact-FD step.
+//
+// A tile of 32 lines (lane = line) is cut along the line into nseg segments
+// of seglen rows, one warp each.  Both recurrences are linear, so every warp
+// runs both passes over its segment from zero incoming states (the particular
+// solutions yp, then fp = the segment-local back substitution of yp), and the
+// true values follow from the four values carried across each boundary:
+//   S_j = (y_{b-1}, y_{b-2}, y_{b-3}, y_{b-4})   forward state entering segment j
+//   T_j = (f_e, f_{e+1}, f_{e+2}, f_{e+3})       backward state entering it
+//   f_i = fp_i + gb[i] . S_j + hb[i] . T_j
+// hf[i] is the response of the forward recurrence to unit entering states,
+// gb[i] the segment-local back substitution of those responses and hb[i] the
+// response of the back substitution to unit entering states; all three are
+// built once per axis on the host in FP64 from the device's FP32 factors
+// (every line of an axis shares them).  The states follow from the segments'
+// end values by two scans over the segments (one 4x4 step per segment):
+//   S_{k+1}[m] = yp_{e_k-1-m} + hf[e_k-1-m] . S_k
+//   T_{k-1}[m] = fp_{b_k+m} + gb[b_k+m] . S_k + hb[b_k+m] . T_k
+// In exact arithmetic this is the sequential solve; in FP32 it differs from it
+// by rounding only (the interior recurrences decay with ratios <= 0.9, so the
+// corrections never amplify).  The right-hand sides are formed in place
+// first (cfd_rhs_range, ends parked until the neighbours have read them).
+// ============================================================================
+namespace {
+
+constexpr int kSegMax = 8;  // segments (warps) per tile
+
+struct SegSmem {
+  float endf[kSegMax][4][32];  // yp_{e-1} .. yp_{e-4} per segment and line
+  float endb[kSegMax][4][32];  // fp_b .. fp_{b+3}
+  float sin[kSegMax][4][32];   // S_j
+};
+constexpr size_t kSegHdr = 128 + sizeof(SegSmem);  // mbarrier slot + SegSmem, then the tile
+
+__device__ __forceinline__ void seg_range(const CfdPlanDev &p, int j, int &b, int &e) {
+  b = j * p.seglen;
+  e = j == p.nseg - 1 ? p.n : b + p.seglen;
+}
+
+// Forward elimination over rows [b, e) from a zero incoming state, in place
+// (b a multiple of the chunk).  On return (y1 .. y4) = (y_{e-1} .. y_{e-4}).
+template <int S>
+__device__ __forceinline__ void seg_fwd(const CfdPlanDev &p, float *L, int b, int e, Chain &y) {
+  constexpr int C = kChunk;
+  const float4 *__restrict__ lm = reinterpret_cast<const float4 *>(p.lm);
+  const float4 mc = make_float4(p.lmc[0], p.lmc[1], p.lmc[2], p.lmc[3]);
+  y = Chain{0.f, 0.f, 0.f, 0.f};
+  float rv[C];
+#pragma unroll
+  for (int k = 0; k < C; k++) rv[k] = L[min(b + k, e - 1) * S];
+  for (int i0 = b; i0 < e; i0 += C) {
+    const bool more = i0 + C < e;
+    float nrv[C];
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) nrv[k] = L[min(i0 + C + k, e - 1) * S];
+    }
+    if (i0 >= p.c0 && i0 + C - 1 <= p.c1) {  // constant chunks are full (c1 < n)
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        float v = rv[k];
+        v = v - mc.w * y.y4;
+        v = v - mc.z * y.y3;
+        v = v - mc.y * y.y2;
+        v = v - mc.x * y.y1;
+        y.y4 = y.y3, y.y3 = y.y2, y.y2 = y.y1, y.y1 = v;
+        rv[k] = v;
+      }
+    } else {
+      float4 m[C];
+#pragma unroll
+      for (int k = 0; k < C; k++) m[k] = __ldg(lm + min(i0 + k, e - 1));
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        if (i0 + k < e) {
+          float v = rv[k];
+          v = v - m[k].w * y.y4;
+          v = v - m[k].z * y.y3;
+          v = v - m[k].y * y.y2;
+          v = v - m[k].x * y.y1;
+          y.y4 = y.y3, y.y3 = y.y2, y.y2 = y.y1, y.y1 = v;
+          rv[k] = v;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++)
+      if (i0 + k < e) L[(i0 + k) * S] = rv[k];
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) rv[k] = nrv[k];
+    }
+  }
+}
+
+// Back substitution over rows e-1 down to b from a zero incoming state, in
+// place.  On return (z1 .. z4) = (f_b .. f_{b+3}).
+template <int S>
+__device__ __forceinline__ void seg_bwd(const CfdPlanDev &p, float *L, int b, int e, Chain &z) {
+  constexpr int C = kChunk;
+  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
+  const float *__restrict__ rd = p.rdiag;
+  const float4 uc = make_float4(p.buc[0], p.buc[1], p.buc[2], p.buc[3]);
+  const float rc = p.rdc;
+  z = Chain{0.f, 0.f, 0.f, 0.f};
+  float yv[C];
+#pragma unroll
+  for (int k = 0; k < C; k++) yv[k] = L[max(e - 1 - k, b) * S];
+  for (int t = e - 1; t >= b; t -= C) {
+    const int tn = t - C;
+    const bool more = tn >= b;
+    float nyv[C];
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) nyv[k] = L[max(tn - k, b) * S];
+    }
+    if (t - C + 1 >= b && t - C + 1 >= p.c0 && t <= p.c1) {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        float w = yv[k];
+        w = w - uc.w * z.y4;
+        w = w - uc.z * z.y3;
+        w = w - uc.y * z.y2;
+        w = w - uc.x * z.y1;
+        w = w * rc;
+        z.y4 = z.y3, z.y3 = z.y2, z.y2 = z.y1, z.y1 = w;
+        yv[k] = w;
+      }
+    } else {
+      float4 u[C];
+      float rr[C];
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        const int i = max(t - k, b);
+        u[k] = __ldg(bu4 + i), rr[k] = __ldg(rd + i);
+      }
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        if (t - k >= b) {
+          float w = yv[k];
+          w = w - u[k].w * z.y4;
+          w = w - u[k].z * z.y3;
+          w = w - u[k].y * z.y2;
+          w = w - u[k].x * z.y1;
+          w = w * rr[k];
+          z.y4 = z.y3, z.y3 = z.y2, z.y2 = z.y1, z.y1 = w;
+          yv[k] = w;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++)
+      if (t - k >= b) L[(t - k) * S] = yv[k];
+    if (more) {
+#pragma unroll
+      for (int k = 0; k < C; k++) yv[k] = nyv[k];
+    }
+  }
+}
+
+__device__ __forceinline__ float dot4_acc(float v, const float4 &h, const float (&s)[4]) {
+  v = v + h.x * s[0];
+  v = v + h.y * s[1];
+  v = v + h.z * s[2];
+  v = v + h.w * s[3];
+  return v;
+}
+
+// Right-hand sides and both particular recurrences of this warp's segment
+// (warp < p.nseg; every thread of the CTA calls it), then the two scans:
+// leaves fp in the tile and this segment's entering states in sv / tv.  The
+// final value of row i is seg_final.
+template <int S>
+__device__ __forceinline__ void seg_solve(const CfdPlanDev &p, float *L, int lane, int warp, SegSmem &ss,
+                                          float (&sv)[4], float (&tv)[4]) {
+  int b, e;
+  seg_range(p, warp, b, e);
+  {
+    float head[5], tail[5];
+    cfd_rhs_range<S, kChunk>(p.a, L, p.n, b, e, head, tail);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 5; k++) L[(b + k) * S] = head[k];
+    if ((e - b) % kChunk == 0) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) L[(e - 5 + k) * S] = tail[k];
+    }
+  }
+  {
+    Chain y;
+    seg_fwd<S>(p, L, b, e, y);
+    ss.endf[warp][0][lane] = y.y1, ss.endf[warp][1][lane] = y.y2;
+    ss.endf[warp][2][lane] = y.y3, ss.endf[warp][3][lane] = y.y4;
+  }
+  {
+    Chain z;
+    seg_bwd<S>(p, L, b, e, z);
+    ss.endb[warp][0][lane] = z.y1, ss.endb[warp][1][lane] = z.y2;
+    ss.endb[warp][2][lane] = z.y3, ss.endb[warp][3][lane] = z.y4;
+  }
+  __syncthreads();
+  // forward scan up to this segment
+  const float4 *__restrict__ hf = reinterpret_cast<const float4 *>(p.hf);
+  sv[0] = sv[1] = sv[2] = sv[3] = 0.f;
+  for (int k = 0; k < warp; k++) {
+    const int ek = (k + 1) * p.seglen;
+    float ns[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) ns[m] = dot4_acc(ss.endf[k][m][lane], __ldg(hf + ek - 1 - m), sv);
+#pragma unroll
+    for (int m = 0; m < 4; m++) sv[m] = ns[m];
+  }
+#pragma unroll
+  for (int m = 0; m < 4; m++) ss.sin[warp][m][lane] = sv[m];
+  __syncthreads();
+  // backward scan down to this segment
+  const float4 *__restrict__ gb = reinterpret_cast<const float4 *>(p.gb);
+  const float4 *__restrict__ hb = reinterpret_cast<const float4 *>(p.hb);
+  tv[0] = tv[1] = tv[2] = tv[3] = 0.f;
+  for (int k = p.nseg - 1; k > warp; k--) {
+    const int bk = k * p.seglen;
+    float sk[4], nt[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) sk[m] = ss.sin[k][m][lane];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+      nt[m] = dot4_acc(dot4_acc(ss.endb[k][m][lane], __ldg(gb + bk + m), sk), __ldg(hb + bk + m), tv);
+#pragma unroll
+    for (int m = 0; m < 4; m++) tv[m] = nt[m];
+  }
+}
+
+// f_i = fp_i + gb[i] . S_j + hb[i] . T_j (the tables are zero where a
+// segment has no entering state)
+__device__ __forceinline__ float seg_final(const CfdPlanDev &p, int i, float fp, const float (&sv)[4],
+                                           const float (&tv)[4]) {
+  const float4 g = __ldg(reinterpret_cast<const float4 *>(p.gb) + i);
+  const float4 h = __ldg(reinterpret_cast<const float4 *>(p.hb) + i);
+  return dot4_acc(dot4_acc(fp, g, sv), h, tv);
+}
+
+// cells handled together by the epilogues (their PML memory in one round trip)
+constexpr int kSegU = 4;
+
+// First-derivative PML round `round` on component AXIS of a batch of cells.
+template <int AXIS, int U>
+__device__ __forceinline__ void seg_pml(const CfdSegArgs &a, const Grid3 &g, int round, float (&v)[U],
+                                        const int (&ix)[U], const int (&iy)[U], const int (&iz)[U],
+                                        const bool (&act)[U]) {
+  if (round) pml1_batch<AXIS, 1, U>(a.pml, g, a.pml3d, v, ix, iy, iz, act);
+  else pml1_batch<AXIS, 0, U>(a.pml, g, a.pml3d, v, ix, iy, iz, act);
+}
+
+// Strided tile (x or y lines of 32 z columns, rows [0, n) at sm[i * 32 + lane])
+// loaded by TMA boxes (R rows each, zero fill past the tensor) or by plain
+// loads; false when the bounded wait gave up (the CTA then returns).
+template <int AXIS, bool TMA>
+__device__ __forceinline__ bool seg_load_strided(unsigned char *smraw, float *sm, const CUtensorMap *tin,
+                                                 const float *in, long long base, long long es, int n, int nl, int iz0,
+                                                 int o, int R, int nb, int *err) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (TMA) {
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw);
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(bar, (uint32_t)nb * (uint32_t)R * 32u * 4u);
+      for (int b = 0; b < nb; b++) {
+        if (AXIS == DX) tma_load_3d(sm + (size_t)b * R * 32, tin, bar, iz0, b * R, o);
+        else tma_load_3d(sm + (size_t)b * R * 32, tin, bar, iz0, o, b * R);
+      }
+    }
+    const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
+    if (!ok && threadIdx.x == 0) mbar_drain(bar, 0);  // its own copies land before the CTA leaves
+    return ok;
+  }
+  constexpr int U = 16;
+  for (int i0 = warp * U; i0 < n; i0 += nw * U) {
+    float v[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const int i = i0 + k;
+      v[k] = (i < n && lane < nl) ? __ldcg(in + base + lane + (long long)i * es) : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++)
+      if (i0 + k < n) sm[(i0 + k) * 32 + lane] = v[k];
+  }
+  __syncthreads();
+  return true;
+}
+
+// Z or X (or Y) line derivative with the first-derivative PML round `round` of
+// that component: out = PML(D in).
+template <int AXIS, bool TMA>
+__global__ void __launch_bounds__(256, 2) cfd_seg_line_k(const CfdPlanDev p, const float *__restrict__ in,
+                                                         float *__restrict__ out, const CfdSegArgs a,
+                                                         const __grid_constant__ CUtensorMap tin, int round, int R,
+                                                         int nb, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  SegSmem &ss = *reinterpret_cast<SegSmem *>(smraw + 128);
+  float *sm = reinterpret_cast<float *>(smraw + kSegHdr);
+  const int n = p.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  float sv[4], tv[4];
+  int b, e;
+  seg_range(p, warp, b, e);
+  if (AXIS == DZ) {
+    const long long nlines = (long long)a.nx * a.ny, l0 = (long long)blockIdx.x * 32;
+    const int nl = (int)min(32LL, nlines - l0);
+    const int st = n + 1;
+    for (int l = warp; l < nl; l += nw) {
+      const float *src = in + (l0 + l) * n;
+      float *dst = sm + l * st;
+#pragma unroll 4
+      for (int i = lane; i < n; i += 32) cp_async4(dst + i, src + i);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    float *L = sm + lane * st;
+    seg_solve<1>(p, L, lane, warp, ss, sv, tv);
+    for (int i = b; i < e; i++) L[i] = seg_final(p, i, L[i], sv, tv);
+    __syncthreads();
+    constexpr int U = kSegU;
+    for (int l = warp; l < nl; l += nw) {
+      const long long line = l0 + l;
+      const int ix = (int)(line % a.nx), iy = (int)(line / a.nx);
+      const float *row = sm + l * st;
+      float *dst = out + line * n;
+      for (int i0 = lane; i0 < n; i0 += 32 * U) {
+        float v[U];
+        int xs[U], ys[U], zs[U];
+        bool act[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int i = i0 + 32 * u;
+          act[u] = i < n;
+          v[u] = act[u] ? row[i] : 0.f;
+          xs[u] = ix, ys[u] = iy, zs[u] = min(i, n - 1);
+        }
+        seg_pml<DZ, U>(a, g, round, v, xs, ys, zs, act);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (act[u]) __stcg(dst + i0 + 32 * u, v[u]);
+      }
+    }
+    return;
+  }
+  const int iz0 = blockIdx.x * 32, o = blockIdx.y;
+  const int nl = min(32, a.nz - iz0);
+  const long long es = AXIS == DX ? (long long)a.nz : g.nxz;
+  const long long base = AXIS == DX ? (long long)o * g.nxz + iz0 : (long long)o * a.nz + iz0;
+  if (!seg_load_strided<AXIS, TMA>(smraw, sm, &tin, in, base, es, n, nl, iz0, o, R, nb, err)) return;
+  float *L = sm + lane;
+  seg_solve<32>(p, L, lane, warp, ss, sv, tv);
+  if (lane < nl) {
+    constexpr int U = kSegU;
+    for (int i0 = b; i0 < e; i0 += U) {
+      float v[U];
+      int xs[U], ys[U], zs[U];
+      bool act[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = min(i0 + u, e - 1);
+        act[u] = i0 + u < e;
+        v[u] = seg_final(p, i, L[i * 32], sv, tv);
+        xs[u] = AXIS == DX ? i : o, ys[u] = AXIS == DX ? o : i, zs[u] = iz0 + lane;
+      }
+      seg_pml<AXIS, U>(a, g, round, v, xs, ys, zs, act);
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (act[u]) __stcg(out + base + lane + (long long)(i0 + u) * es, v[u]);
+    }
+  }
+}
+
+// The fused y kernel: y lines of w1 (x = o, 32 z columns).  Gradient pass:
+// gy = Dy w1 with PML round 1; with the x / z gradients (already through
+// their PML) each cell is divided by rho (KernelCPU::divideRho) and scaled
+// (ScalarVTI / ScalarTTI); px, pz go back to global memory, py stays in the
+// tile.  Divergence pass along y: dy = Dy py with PML round 2.
+template <int MODEL, bool RHO, bool TMA>
+__global__ void __launch_bounds__(256, 2) cfd_seg_yf_k(const CfdPlanDev pg, const CfdPlanDev pd, const CfdSegArgs a,
+                                                       const __grid_constant__ CUtensorMap tin, int R, int nb,
+                                                       int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  SegSmem &ss = *reinterpret_cast<SegSmem *>(smraw + 128);
+  float *sm = reinterpret_cast<float *>(smraw + kSegHdr);
+  const int n = pg.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int iz0 = blockIdx.x * 32, o = blockIdx.y;
+  const int nl = min(32, a.nz - iz0);
+  const long long es = g.nxz, base = (long long)o * a.nz + iz0;
+  if (!seg_load_strided<DY, TMA>(smraw, sm, &tin, a.w1, base, es, n, nl, iz0, o, R, nb, err)) return;
+  float *L = sm + lane;
+  float sv[4], tv[4];
+  seg_solve<32>(pg, L, lane, warp, ss, sv, tv);
+  int b, e;
+  seg_range(pg, warp, b, e);
+  const int iz = iz0 + lane;
+  constexpr int U = kSegU;
+  if (lane < nl) {
+    for (int i0 = b; i0 < e; i0 += U) {
+      float gx[U], gz[U], gy[U], r[U];
+      float4 m[U];
+      int xs[U], ys[U], zs[U];
+      bool act[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = min(i0 + u, e - 1);
+        const long long c = base + lane + (long long)i * es;
+        gx[u] = a.gx[c], gz[u] = a.gz[c];
+        if (RHO) r[u] = __ldg(a.rho + c);
+        if (MODEL >= 2) m[u].x = __ldg(a.eps + c), m[u].y = __ldg(a.del + c);
+        if (MODEL == 3) m[u].z = __ldg(a.pjx + c), m[u].w = __ldg(a.pjy + c);
+        gy[u] = seg_final(pg, i, L[i * 32], sv, tv);
+        act[u] = i0 + u < e;
+        xs[u] = o, ys[u] = i, zs[u] = iz;
+      }
+      seg_pml<DY, U>(a, g, 0, gy, xs, ys, zs, act);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (act[u]) {
+          const long long c = base + lane + (long long)i * es;
+          float x = gx[u], y = gy[u], z = gz[u];
+          if (RHO) divide_rho(r[u], true, x, y, z);
+          if (MODEL >= 2) aniso_scale<MODEL>(m[u], x, y, z);
+          a.gx[c] = x, a.gz[c] = z;
+          L[i * 32] = y;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  seg_solve<32>(pd, L, lane, warp, ss, sv, tv);
+  if (lane < nl) {
+    for (int i0 = b; i0 < e; i0 += U) {
+      float v[U];
+      int xs[U], ys[U], zs[U];
+      bool act[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = min(i0 + u, e - 1);
+        v[u] = seg_final(pd, i, L[i * 32], sv, tv);
+        act[u] = i0 + u < e;
+        xs[u] = o, ys[u] = i, zs[u] = iz;
+      }
+      seg_pml<DY, U>(a, g, 1, v, xs, ys, zs, act);
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (act[u]) __stcg(a.dy + base + lane + (long long)(i0 + u) * es, v[u]);
+    }
+  }
+}
+
+// The fused x kernel: x lines of px (y = o, 32 z columns).  dx = Dx px with
+// PML round 2; then w0 - vel dx, - vel dz, - vel dy (with rho: (d vel) rho for
+// x and z, d (vel rho) for y, FdEngine_cfd::d{x,z,y}1_2D's forms) and the
+// leapfrog / Q update of MODE.
+template <int MODE, bool RHO, bool TMA>
+__global__ void __launch_bounds__(256, 2) cfd_seg_xf_k(const CfdPlanDev p, const CfdSegArgs a,
+                                                       const __grid_constant__ CUtensorMap tin, int R, int nb,
+                                                       int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  SegSmem &ss = *reinterpret_cast<SegSmem *>(smraw + 128);
+  float *sm = reinterpret_cast<float *>(smraw + kSegHdr);
+  const int n = p.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
+  const int iz0 = blockIdx.x * 32, o = blockIdx.y;
+  const int nl = min(32, a.nz - iz0);
+  const long long es = a.nz, base = (long long)o * g.nxz + iz0;
+  if (!seg_load_strided<DX, TMA>(smraw, sm, &tin, a.gx, base, es, n, nl, iz0, o, R, nb, err)) return;
+  float *L = sm + lane;
+  float sv[4], tv[4];
+  seg_solve<32>(p, L, lane, warp, ss, sv, tv);
+  int b, e;
+  seg_range(p, warp, b, e);
+  const int iz = iz0 + lane;
+  const long long ntot = g.nxz * a.ny;
+  if (lane < nl) {
+    constexpr int U = kSegU;
+    for (int i0 = b; i0 < e; i0 += U) {
+      float dz[U], dy[U], vel[U], w0[U], w1[U], r[U], dxs[U];
+      int xs[U], ys[U], zs[U];
+      bool act[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = min(i0 + u, e - 1);
+        const long long c = base + lane + (long long)i * es;
+        dz[u] = __ldcs(a.dz + c), dy[u] = __ldcs(a.dy + c);
+        vel[u] = __ldg(a.vel + c), w0[u] = a.w0[c];
+        if (MODE != 0) w1[u] = __ldg(a.w1 + c);
+        if (RHO) r[u] = __ldg(a.rho + c);
+        dxs[u] = seg_final(p, i, L[i * 32], sv, tv);
+        act[u] = i0 + u < e;
+        xs[u] = i, ys[u] = o, zs[u] = iz;
+      }
+      seg_pml<DX, U>(a, g, 1, dxs, xs, ys, zs, act);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u;
+        if (act[u]) {
+          const long long c = base + lane + (long long)i * es;
+          const float dx = dxs[u];
+          float t;
+          if (RHO) {
+            t = div_accumulate_rho<0>(w0[u], vel[u], r[u], dx, dz[u], dy[u]);
+          } else {
+            t = div_accumulate(w0[u], vel[u], dx, dz[u], dy[u]);
+          }
+          float out;
+          if (MODE == 0) out = t;
+          else if (MODE == 1) out = (w1[u] + w1[u]) - t;
+          else out = q_update(a.q, c, ntot, t, w1[u]);
+          a.w0[c] = out;
+        }
+      }
+    }
+  }
+}
+
+size_t seg_smem_strided(int n, bool tma) {
+  int R = n, nb = 1;
+  if (tma) cfd_tma_box(n, &R, &nb);
+  return kSegHdr + (size_t)nb * R * 32 * sizeof(float);
+}
+size_t seg_smem_z(int n) { return kSegHdr + (size_t)32 * (n + 1) * sizeof(float); }
+
+}  // namespace
+
+int cfd_seg_max_n(int axis) {
+  const size_t cap = 227 * 1024;
+  int n = 16;
+  while (n < 8192 && (axis == DZ ? seg_smem_z(n + 1) : seg_smem_strided(n + 1, true)) <= cap &&
+         (axis == DZ || seg_smem_strided(n + 1, false) <= cap))
+    n++;
+  return n;
+}
+
+int cfd_seg_init() {
+  const int mx = 227 * 1024;
+  bool ok = true;
+  auto set = [&](const void *f) {
+    ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  };
+  set((const void *)cfd_seg_line_k<DZ, false>);
+  set((const void *)cfd_seg_line_k<DX, false>);
+  set((const void *)cfd_seg_line_k<DX, true>);
+  set((const void *)cfd_seg_line_k<DY, false>);
+  set((const void *)cfd_seg_line_k<DY, true>);
+  set((const void *)cfd_seg_yf_k<1, false, false>), set((const void *)cfd_seg_yf_k<1, false, true>);
+  set((const void *)cfd_seg_yf_k<1, true, false>), set((const void *)cfd_seg_yf_k<1, true, true>);
+  set((const void *)cfd_seg_yf_k<2, false, false>), set((const void *)cfd_seg_yf_k<2, false, true>);
+  set((const void *)cfd_seg_yf_k<2, true, false>), set((const void *)cfd_seg_yf_k<2, true, true>);
+  set((const void *)cfd_seg_yf_k<3, false, false>), set((const void *)cfd_seg_yf_k<3, false, true>);
+  set((const void *)cfd_seg_yf_k<3, true, false>), set((const void *)cfd_seg_yf_k<3, true, true>);
+  set((const void *)cfd_seg_xf_k<0, false, false>), set((const void *)cfd_seg_xf_k<0, false, true>);
+  set((const void *)cfd_seg_xf_k<0, true, false>), set((const void *)cfd_seg_xf_k<0, true, true>);
+  set((const void *)cfd_seg_xf_k<1, false, false>), set((const void *)cfd_seg_xf_k<1, false, true>);
+  set((const void *)cfd_seg_xf_k<1, true, false>), set((const void *)cfd_seg_xf_k<1, true, true>);
+  set((const void *)cfd_seg_xf_k<2, false, false>), set((const void *)cfd_seg_xf_k<2, false, true>);
+  set((const void *)cfd_seg_xf_k<2, true, false>), set((const void *)cfd_seg_xf_k<2, true, true>);
+  return ok ? 0 : -1;
+}
+
+void launch_cfd_seg_line(int axis, int round, const CfdPlanDev &p, const float *in, float *out, const CfdSegArgs &a,
+                         const CUtensorMap *tin, int *err, cudaStream_t st) {
+  const dim3 block(32 * p.nseg);
+  CUtensorMap none{};
+  if (axis == DZ) {
+    const long long nlines = (long long)a.nx * a.ny;
+    cfd_seg_line_k<DZ, false><<<(unsigned)((nlines + 31) / 32), block, seg_smem_z(p.n), st>>>(p, in, out, a, none,
+                                                                                               round, 0, 0, err);
+    return;
+  }
+  const dim3 grid((a.nz + 31) / 32, axis == DX ? a.ny : a.nx);
+  int R = p.n, nb = 1;
+  if (tin) cfd_tma_box(p.n, &R, &nb);
+  const size_t smem = seg_smem_strided(p.n, tin != nullptr);
+  if (axis == DX) {
+    if (tin) cfd_seg_line_k<DX, true><<<grid, block, smem, st>>>(p, in, out, a, *tin, round, R, nb, err);
+    else cfd_seg_line_k<DX, false><<<grid, block, smem, st>>>(p, in, out, a, none, round, R, nb, err);
+  } else {
+    if (tin) cfd_seg_line_k<DY, true><<<grid, block, smem, st>>>(p, in, out, a, *tin, round, R, nb, err);
+    else cfd_seg_line_k<DY, false><<<grid, block, smem, st>>>(p, in, out, a, none, round, R, nb, err);
+  }
+}
+
+template <int MODEL, bool RHO>
+static void yf_launch(const CfdPlanDev &pg, const CfdPlanDev &pd, const CfdSegArgs &a, const CUtensorMap *tin,
+                      int *err, cudaStream_t st) {
+  const dim3 grid((a.nz + 31) / 32, a.nx), block(32 * pg.nseg);
+  int R = pg.n, nb = 1;
+  if (tin) cfd_tma_box(pg.n, &R, &nb);
+  const size_t smem = seg_smem_strided(pg.n, tin != nullptr);
+  CUtensorMap none{};
+  if (tin) cfd_seg_yf_k<MODEL, RHO, true><<<grid, block, smem, st>>>(pg, pd, a, *tin, R, nb, err);
+  else cfd_seg_yf_k<MODEL, RHO, false><<<grid, block, smem, st>>>(pg, pd, a, none, R, nb, err);
+}
+
+void launch_cfd_seg_yfused(const CfdPlanDev &pg, const CfdPlanDev &pd, const CfdSegArgs &a, const CUtensorMap *tin,
+                           int *err, cudaStream_t st) {
+  const bool rho = a.rho != nullptr;
+  if (a.model == 3) rho ? yf_launch<3, true>(pg, pd, a, tin, err, st) : yf_launch<3, false>(pg, pd, a, tin, err, st);
+  else if (a.model == 2) rho ? yf_launch<2, true>(pg, pd, a, tin, err, st) : yf_launch<2, false>(pg, pd, a, tin, err, st);
+  else rho ? yf_launch<1, true>(pg, pd, a, tin, err, st) : yf_launch<1, false>(pg, pd, a, tin, err, st);
+}
+
+template <int MODE, bool RHO>
+static void xf_launch(const CfdPlanDev &p, const CfdSegArgs &a, const CUtensorMap *tin, int *err, cudaStream_t st) {
+  const dim3 grid((a.nz + 31) / 32, a.ny), block(32 * p.nseg);
+  int R = p.n, nb = 1;
+  if (tin) cfd_tma_box(p.n, &R, &nb);
+  const size_t smem = seg_smem_strided(p.n, tin != nullptr);
+  CUtensorMap none{};
+  if (tin) cfd_seg_xf_k<MODE, RHO, true><<<grid, block, smem, st>>>(p, a, *tin, R, nb, err);
+  else cfd_seg_xf_k<MODE, RHO, false><<<grid, block, smem, st>>>(p, a, none, R, nb, err);
+}
+
+void launch_cfd_seg_xfused(const CfdPlanDev &p, const CfdSegArgs &a, const CUtensorMap *tin, int *err,
+                           cudaStream_t st) {
+  const bool rho = a.rho != nullptr;
+  if (a.mode == 0) rho ? xf_launch<0, true>(p, a, tin, err, st) : xf_launch<0, false>(p, a, tin, err, st);
+  else if (a.mode == 1) rho ? xf_launch<1, true>(p, a, tin, err, st) : xf_launch<1, false>(p, a, tin, err, st);
+  else rho ? xf_launch<2, true>(p, a, tin, err, st) : xf_launch<2, false>(p, a, tin, err, st);
 }
 
 }  // namespace rtm

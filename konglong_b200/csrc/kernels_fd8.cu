@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__re
       }
       if (a.io.store | a.io.ic) fused_io(a.io, g, i, ix, iy, iz, col, q[R]);
       if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<0>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
+      if (a.rho) divide_rho(__ldg(a.rho + i), do_y, gx, gy, gz);
       if (MODEL == 2 || MODEL == 3) aniso_scale<MODEL>(cm, gx, gy, gz);
       a.px[i] = gx;
       a.pz[i] = gz;
@@ -361,7 +362,8 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__rest
         if (do_y) dyv = d1_acc(dyv, a.c1y[m], q[R + m], q[R - m]);
       }
       if (EDGE && in_pml(a.pml, g, ix, iy, iz)) pml1_all<1>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
-      const float t = div_accumulate(cw0, cvel, dxv, dzv, dyv);
+      const float t = a.rho ? div_accumulate_rho<-1>(cw0, cvel, __ldg(a.rho + i), dxv, dzv, dyv)
+                            : div_accumulate(cw0, cvel, dxv, dzv, dyv);
       float out;
       if (MODE == 0) out = t;
       else out = MODE == 1 ? __fsub_rn(__fadd_rn(cw1, cw1), t) : q_update(a.q, i, (long long)a.ny * g.nxz, t, cw1);

@@ -51,6 +51,10 @@ struct TileSet {
 struct Engine {
   rtm_dims d{};
   rtm_config c{};
+  // FD8 ISO without density: the Laplacian path (KernelCPU::ISO, do_laplacian);
+  // every other configuration takes the two first-derivative passes
+  // (bgprtm/KernelCPU.cpp:125-174)
+  bool lap_iso() const { return c.engine == RTM_ENGINE_FD8 && c.model_type == RTM_ISO && !c.use_rho; }
   int device = 0;
   cudaStream_t st = nullptr;
   long long n = 0, nxz = 0;
@@ -59,6 +63,7 @@ struct Engine {
   // state
   float *w0 = nullptr, *w1 = nullptr, *vel = nullptr;
   float *eps = nullptr, *del = nullptr, *pjx = nullptr, *pjy = nullptr, *invq = nullptr;
+  float *rho = nullptr;  // density (KernelCPU::setModel's rho), null without a density model
   float *wq[2] = {nullptr, nullptr};
   int iq0 = 0;
   float *px = nullptr, *py = nullptr, *pz = nullptr;  // gradient scratch (anisotropic / CFD)
@@ -140,7 +145,10 @@ struct Engine {
   std::vector<std::array<int, 4>> tune_desc;  // candidates of the last rtm_autotune and their times
   std::vector<float> tune_ms;
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
-  int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile
+  int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile (the split
+                    // pipeline: line solves + pointwise epilogues); 3 / 4 the segment-parallel
+                    // fused pipeline with TMA / plain tile loads
+  int cfd_seg_ok = 0;  // the segment-parallel pipeline applies (engine CFD, 3-D, lines fit)
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -348,6 +356,55 @@ static int yseg_iso4(Engine *h) {
   return yseg_v4(h, h->v4_tx, iso_v4_ctas_per_sm(h->v4_tx, h->c.pml3d));
 }
 
+// Segment layout of the segment-parallel solve of an n-point line (segments
+// of seglen rows, a multiple of 8, at most 8 of them, the last one >= 8 rows)
+// and its correction tables [n][4] (see kernels_cfd.cu): hf = forward
+// responses to unit entering states y_{b-1-k}, gb = their segment-local back
+// substitutions, hb = backward responses to unit entering states f_{e+k}.
+// FP64 recurrences on the FP32 factors the kernels use.
+static void cfd_seg_tables(int n, const std::vector<float> &lm, const std::vector<float> &bu,
+                           const std::vector<float> &rd, int &nseg, int &seglen, std::vector<float> &hf,
+                           std::vector<float> &gb, std::vector<float> &hb) {
+  seglen = ((n + 7) / 8 + 7) / 8 * 8;
+  nseg = (n + seglen - 1) / seglen;
+  if (nseg > 1 && n - (nseg - 1) * seglen < 8) nseg--;
+  hf.assign(4 * (size_t)n, 0.f), gb.assign(4 * (size_t)n, 0.f), hb.assign(4 * (size_t)n, 0.f);
+  // back substitution of y over rows [b, e) with f_{e..e+3} given in f[e-b ..]
+  auto back = [&](int b, int e, const std::vector<double> &y, std::vector<double> &f) {
+    for (int i = e - 1; i >= b; i--) {
+      const float *u = &bu[4 * (size_t)i];
+      double w = y[i - b];
+      for (int k = 3; k >= 0; k--) w -= (double)u[k] * f[i - b + 1 + k];
+      f[i - b] = w * (double)rd[i];
+    }
+  };
+  for (int j = 0; j < nseg; j++) {
+    const int b = j * seglen, e = j == nseg - 1 ? n : b + seglen, len = e - b;
+    for (int k = 0; k < 4; k++) {
+      if (j > 0) {
+        std::vector<double> y(len + 4, 0.0);  // y[4 + i - b] = y_i; y[3 - q] = y_{b-1-q}
+        y[3 - k] = 1.0;
+        for (int i = b; i < e; i++) {
+          const float *m = &lm[4 * (size_t)i];  // multipliers of y_{i-1} .. y_{i-4}
+          double v = 0.0;
+          for (int q = 3; q >= 0; q--) v -= (double)m[q] * y[4 + i - b - 1 - q];
+          y[4 + i - b] = v;
+          hf[4 * (size_t)i + k] = (float)v;
+        }
+        std::vector<double> yi(y.begin() + 4, y.end()), f(len + 4, 0.0);
+        back(b, e, yi, f);
+        for (int i = b; i < e; i++) gb[4 * (size_t)i + k] = (float)f[i - b];
+      }
+      if (j < nseg - 1) {
+        std::vector<double> y(len, 0.0), f(len + 4, 0.0);
+        f[len + k] = 1.0;
+        back(b, e, y, f);
+        for (int i = b; i < e; i++) hb[4 * (size_t)i + k] = (float)f[i - b];
+      }
+    }
+  }
+}
+
 // Longest run of rows whose (lm, bu, rdiag) are bitwise identical: in the
 // interior of a line the LU of the Toeplitz band matrix has converged, and
 // the line kernels hold those factors in registers instead of loading them.
@@ -426,7 +483,7 @@ static int setup_pml(Engine *h) {
   const rtm_config &c = h->c;
   const int nn[3] = {h->d.nx, h->d.ny, h->d.nz};
   const double dd[3] = {h->d.dx, h->d.dy, h->d.dz};
-  const bool second = c.engine == RTM_ENGINE_FD8 && c.model_type == RTM_ISO;
+  const bool second = h->lap_iso();
   const int ncomp = (!c.pml3d || second) ? 1 : 3;
   for (int dim = 0; dim < 3; dim++)
     for (int s = 0; s < 2; s++) {
@@ -500,10 +557,54 @@ static QDev q_dev(Engine *h) {
 // One application of the spatial operator, optionally fused with update2nd
 // (mode 1 leapfrog, 2 Q) and with the snapshot / imaging access of the
 // previous step's wavefield (io).
+// Engine CFD on a 3-D grid: the segment-parallel fused pipeline (five
+// launches: Z(w1), X(w1), the fused y kernel, Z(pz), the fused x kernel).
+static int cfd_seg_step(Engine *h, int mode, const QDev &q) {
+  const rtm_dims &d = h->d;
+  CfdSegArgs a{};
+  a.nx = d.nx, a.ny = d.ny, a.nz = d.nz, a.pml3d = h->c.pml3d, a.model = h->c.model_type, a.mode = mode;
+  a.pml = pml_dev(h);
+  a.q = q;
+  a.w1 = h->w1, a.w0 = h->w0, a.vel = h->vel;
+  a.eps = h->eps, a.del = h->del, a.pjx = h->pjx, a.pjy = h->pjy, a.rho = h->rho;
+  a.gx = h->px, a.gz = h->pz, a.dz = h->scr2, a.dy = h->scr;
+  CUtensorMap mx1, my1, mxp;
+  bool tx1 = false, ty1 = false, txp = false;
+  if (h->cfd_xy == 3 && h->cfd_tma) {
+    int Rx, nbx, Ry, nby;
+    cfd_tma_box(d.nx, &Rx, &nbx);
+    cfd_tma_box(d.ny, &Ry, &nby);
+    tx1 = tmap(h, h->w1, 32, Rx, &mx1);
+    ty1 = tmap(h, h->w1, 32, 1, &my1, Ry);
+    txp = tmap(h, h->px, 32, Rx, &mxp);
+  }
+  {
+    KScope k(h, RTM_K_CFD_Z);
+    launch_cfd_seg_line(DZ, 0, h->cfd[DZ][0], h->w1, h->pz, a, nullptr, h->dflag, h->st);
+  }
+  {
+    KScope k(h, RTM_K_CFD_X);
+    launch_cfd_seg_line(DX, 0, h->cfd[DX][0], h->w1, h->px, a, tx1 ? &mx1 : nullptr, h->dflag, h->st);
+  }
+  {
+    KScope k(h, RTM_K_CFD_YF);
+    launch_cfd_seg_yfused(h->cfd[DY][0], h->cfd[DY][1], a, ty1 ? &my1 : nullptr, h->dflag, h->st);
+  }
+  {
+    KScope k(h, RTM_K_CFD_Z);
+    launch_cfd_seg_line(DZ, 1, h->cfd[DZ][1], h->pz, h->scr2, a, nullptr, h->dflag, h->st);
+  }
+  {
+    KScope k(h, RTM_K_CFD_XF);
+    launch_cfd_seg_xfused(h->cfd[DX][1], a, txp ? &mxp : nullptr, h->dflag, h->st);
+  }
+  return check_launch(h, "cfd_seg_step");
+}
+
 static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   const rtm_dims &d = h->d;
   QDev q = q_dev(h);
-  if (h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO) {
+  if (h->lap_iso()) {
     IsoArgs a{};
     a.nx = d.nx, a.ny = d.ny, a.nz = d.nz, a.yseg = h->yseg;
     a.w1 = h->w1, a.w0 = h->w0, a.vel = h->vel;
@@ -609,7 +710,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = h->yseg, g.pml3d = h->c.pml3d;
     g.w1 = h->w1, g.px = h->px, g.py = h->py, g.pz = h->pz;
     g.h = StateF16{h->h1, h->s1, h->h0, h->s0, h->sn, h->m0};
-    g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy;
+    g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy, g.rho = h->rho;
     memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
     g.pml = pml_dev(h);
     g.io = io;
@@ -626,7 +727,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     DivArgs v{};
     v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = h->yseg, v.pml3d = h->c.pml3d;
     v.h = StateF16{h->h1, h->s1, h->h0, h->s0, h->sn, h->m0};
-    v.px = h->px, v.py = h->py, v.pz = h->pz, v.w1 = h->w1, v.w0 = h->w0, v.vel = h->vel;
+    v.px = h->px, v.py = h->py, v.pz = h->pz, v.w1 = h->w1, v.w0 = h->w0, v.vel = h->vel, v.rho = h->rho;
     memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
     v.pml = pml_dev(h);
     v.q = q;
@@ -644,6 +745,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     launch_fused_io(io, h->w1, d.nx, d.ny, d.nz, h->st);
   }
   TRY(check_launch(h, "fused_io"));
+  if (h->cfd_xy >= 3) return cfd_seg_step(h, mode, q);
   {
     KScope k(h, RTM_K_CFD_Z);
     cfd_deriv(h, DZ, 0, h->w1, h->pz);
@@ -660,7 +762,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   CfdGradEpiArgs ge{};
   ge.nx = d.nx, ge.ny = d.ny, ge.nz = d.nz, ge.pml3d = h->c.pml3d, ge.model = h->c.model_type;
   ge.gx = h->px, ge.gy = h->py, ge.gz = h->pz;
-  ge.eps = h->eps, ge.del = h->del, ge.pjx = h->pjx, ge.pjy = h->pjy;
+  ge.eps = h->eps, ge.del = h->del, ge.pjx = h->pjx, ge.pjy = h->pjy, ge.rho = h->rho;
   ge.pml = pml_dev(h);
   {
     KScope k(h, RTM_K_CFD_GEPI);
@@ -687,7 +789,8 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   CfdDivEpiArgs de{};
   de.nx = d.nx, de.ny = d.ny, de.nz = d.nz, de.pml3d = h->c.pml3d, de.mode = mode;
   de.dx = h->scr2, de.dz = dzp, de.dy = dyp;
-  de.w1 = h->w1, de.w0 = h->w0, de.vel = h->vel;
+  de.w1 = h->w1, de.w0 = h->w0, de.vel = h->vel, de.rho = h->rho;
+  de.rho_form = h->c.engine == RTM_ENGINE_CFDB ? 2 : (h->c.engine == RTM_ENGINE_R2C || h->c.engine == RTM_ENGINE_R2R) ? 1 : 0;
   de.pml = pml_dev(h);
   de.q = q;
   {
@@ -1238,8 +1341,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
   }
-  if (c->state_fp16 && (c->engine != RTM_ENGINE_FD8 || c->model_type < RTM_VTI)) {
-    g_create_error = "rtm_create: FP16 wavefield state is built for the FD8 VTI / TTI (+Q) path";
+  if (c->state_fp16 && (c->engine != RTM_ENGINE_FD8 || c->model_type < RTM_VTI || c->use_rho)) {
+    g_create_error = "rtm_create: FP16 wavefield state is built for the FD8 VTI / TTI (+Q) path without density";
     return RTM_ERR_UNSUPPORTED;
   }
   rtm_handle *h = new rtm_handle();
@@ -1278,7 +1381,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     return fail(rc);
   }
   if ((rc = h->alloc(h->vel, h->n)) || (rc = h->alloc(h->dflag, 1))) return fail(rc);
-  const bool first_deriv = !(c->engine == RTM_ENGINE_FD8 && c->model_type == RTM_ISO);
+  const bool first_deriv = !h->lap_iso();
   if (first_deriv) {
     if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
       return fail(rc);
@@ -1332,6 +1435,17 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
         CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f, {}};
         for (int k = 0; k < 60; k++) pd.a[k] = am[k];
         cfd_constant_run(nn[a], lm, bu, rd, pd);
+        {  // segment layout and correction tables of the segment-parallel solve
+          std::vector<float> hf, gb, hb;
+          cfd_seg_tables(nn[a], lm, bu, rd, pd.nseg, pd.seglen, hf, gb, hb);
+          float *dhf, *dgb, *dhb;
+          if ((rc = h->alloc(dhf, hf.size())) || (rc = h->alloc(dgb, gb.size())) || (rc = h->alloc(dhb, hb.size())))
+            return fail(rc);
+          cudaMemcpy(dhf, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice);
+          cudaMemcpy(dgb, gb.data(), gb.size() * 4, cudaMemcpyHostToDevice);
+          cudaMemcpy(dhb, hb.data(), hb.size() * 4, cudaMemcpyHostToDevice);
+          pd.hf = dhf, pd.gb = dgb, pd.hb = dhb;
+        }
         h->cfd[a][s] = pd;
       }
     }
@@ -1339,6 +1453,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (c->model_type >= RTM_VTI) {
     if ((rc = h->alloc(h->eps, h->n)) || (rc = h->alloc(h->del, h->n))) return fail(rc);
   }
+  if (c->use_rho && (rc = h->alloc(h->rho, h->n))) return fail(rc);
   if (c->model_type == RTM_TTI) {
     if ((rc = h->alloc(h->pjx, h->n)) || (d->ny > 1 && (rc = h->alloc(h->pjy, h->n)))) return fail(rc);
   }
@@ -1376,21 +1491,30 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   cudaMemcpy(h->taper_z, one.data(), 4 * d->nz, cudaMemcpyHostToDevice);
   choose_shape(h);
   h->use_tma = (c->kernel_variant == 0 || c->kernel_variant == 2) && tma_supported(d->nz) && iso_tma_init();
-  if (c->engine == RTM_ENGINE_FD8 && c->model_type == RTM_ISO && d->nz % 4 == 0 &&
+  if (h->lap_iso() && d->nz % 4 == 0 &&
       (c->kernel_variant == 0 || c->kernel_variant == 3 || c->kernel_variant == 4)) {
     h->iso4 = c->kernel_variant != 4 && tma_supported(d->nz) && iso_tma4_init() ? 2 : 1;
     h->v4_yseg = yseg_iso4(h);
     if (h->iso4 == 2 && (rc = iso4_tiles(h))) return fail(rc);
   }
-  if (c->engine == RTM_ENGINE_FD8 && c->model_type != RTM_ISO && (rc = fd8_tiles(h))) return fail(rc);
-  if (c->engine == RTM_ENGINE_FD8 && c->model_type != RTM_ISO && !c->state_fp16 && d->nz % 4 == 0 &&
+  if (c->engine == RTM_ENGINE_FD8 && !h->lap_iso() && (rc = fd8_tiles(h))) return fail(rc);
+  // the 4-cell passes carry no density term: a density model runs the one-cell passes
+  if (c->engine == RTM_ENGINE_FD8 && !h->lap_iso() && !c->use_rho && !c->state_fp16 && d->nz % 4 == 0 &&
       (c->kernel_variant == 0 || c->kernel_variant == 3) && tma_supported(d->nz) && aniso4_init()) {
     h->aniso4 = 1;
     h->an4_yseg = yseg_an4(h);
     if ((rc = an4_tiles(h))) return fail(rc);
   }
   h->cfd_tma = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && tma_supported(d->nz);
-  h->cfd_xy = c->kernel_variant == 0 ? 0 : c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
+  // compact FD on 3-D grids whose lines fit a tile: the segment-parallel fused
+  // pipeline by default (kernel_variant 0; 6 forces its plain-load form); 5
+  // and 1 / 2 select the split pipeline (streamed, plain or TMA x / y tiles)
+  h->cfd_seg_ok = c->engine == RTM_ENGINE_CFD && d->ny > 1 && d->nx <= cfd_seg_max_n(DX) &&
+                  d->ny <= cfd_seg_max_n(DY) && d->nz <= cfd_seg_max_n(DZ) && cfd_seg_init() == 0;
+  if (c->kernel_variant == 0) h->cfd_xy = h->cfd_seg_ok ? (h->cfd_tma ? 3 : 4) : 0;
+  else if (c->kernel_variant == 5) h->cfd_xy = 0;
+  else if (c->kernel_variant == 6 && h->cfd_seg_ok) h->cfd_xy = 4;
+  else h->cfd_xy = c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
   if ((rc = zero_state(h))) return fail(rc);
@@ -1416,8 +1540,8 @@ int rtm_set_q_coeffs(rtm_handle *h, float cq0, const float *cq, const float *wq)
   return RTM_OK;
 }
 
-int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float *del, const float *pjx,
-                  const float *pjy, const float *invq) {
+int rtm_set_model(rtm_handle *h, const float *vel, const float *rho, const float *eps, const float *del,
+                  const float *pjx, const float *pjy, const float *invq) {
   using namespace rtm;
   if (!h || !vel) return RTM_ERR_ARG;
   cudaSetDevice(h->device);
@@ -1427,6 +1551,17 @@ int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float
     h->err = "model arrays required by the model type are missing";
     return RTM_ERR_ARG;
   }
+  if (!h->c.use_rho != !rho) {
+    h->err = h->c.use_rho ? "use_rho is set: rtm_set_model needs the density volume"
+                          : "a density volume needs use_rho in the configuration of rtm_create";
+    return RTM_ERR_ARG;
+  }
+  if (rho)
+    for (long long i = 0; i < h->n; i++)
+      if (!std::isfinite(rho[i]) || rho[i] <= 0.f) {
+        h->err = "density not finite or not positive at cell " + std::to_string(i);
+        return RTM_ERR_NONFINITE;
+      }
   if (h->c.use_q && !h->q_set) {
     h->err = "rtm_set_q_coeffs must precede rtm_set_model when use_q";
     return RTM_ERR_STATE;
@@ -1452,6 +1587,7 @@ int rtm_set_model(rtm_handle *h, const float *vel, const float *eps, const float
     if (h->d.ny > 1) CK(cudaMemcpyAsync(h->pjy, pjy, bytes, cudaMemcpyHostToDevice, h->st));
   }
   if (h->c.use_q) CK(cudaMemcpyAsync(h->invq, invq, bytes, cudaMemcpyHostToDevice, h->st));
+  if (rho) CK(cudaMemcpyAsync(h->rho, rho, bytes, cudaMemcpyHostToDevice, h->st));
   launch_vel2(h->vel, h->invq, h->n, h->d.dt * h->d.dt, h->cq0, h->c.use_q, h->st);
   TRY(check_launch(h, "vel2"));
   CK(cudaStreamSynchronize(h->st));
@@ -1994,7 +2130,7 @@ int rtm_batch_create(rtm_handle *const *shots, int nshots, rtm_batch **out) {
   rtm_batch *b = new rtm_batch();
   for (int k = 0; k < nshots; k++) {
     rtm::Engine *h = shots[k];
-    if (!h || !h->model_set || h->c.engine != RTM_ENGINE_FD8 || h->c.model_type != RTM_ISO || h->c.use_q ||
+    if (!h || !h->model_set || !h->lap_iso() || h->c.use_q ||
         h->device != shots[0]->device || h->c.pml3d != shots[0]->c.pml3d) {
       delete b;
       return !h || !h->model_set ? RTM_ERR_STATE : RTM_ERR_UNSUPPORTED;
@@ -2088,7 +2224,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     int an4 = 0;  // FD8 VTI / TTI 4-cell kernels (y segment in yseg)
   };
   std::vector<Cand> cands;
-  const bool iso = h->c.engine == RTM_ENGINE_FD8 && h->c.model_type == RTM_ISO;
+  const bool iso = h->lap_iso();
   const bool v4_ok = iso && h->d.nz % 4 == 0 &&
                      (h->c.kernel_variant == 0 || h->c.kernel_variant == 3 || h->c.kernel_variant == 4);
   const int iso4_0 = h->iso4, v4_tx0 = h->v4_tx, v4_shape0 = h->v4_shape;
@@ -2120,6 +2256,10 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
       if (ym != y && h->d.ny > y) cands.push_back({0, 0, y, h->tma_shape, h->tx, h->cfd_xy, 1});
   }
   else if ((h->c.engine == RTM_ENGINE_CFD || h->c.engine == RTM_ENGINE_CFDB) && h->c.kernel_variant == 0) {
+    if (h->cfd_seg_ok) {
+      if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 3});
+      cands.push_back({0, 0, 0, h->tma_shape, h->tx, 4});
+    }
     cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
     if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
   }
@@ -2142,7 +2282,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
     if (c.iso4) h->v4_yseg = c.yseg;
     h->tma_shape = c.tma_shape, h->tx = c.tx, h->cfd_xy = c.cfd_xy;
     h->yseg = iso && h->use_tma ? yseg0 : rtm::yseg_for(h, h->tx);
-    if (h->c.engine == RTM_ENGINE_FD8 && h->c.model_type != RTM_ISO) TRY(rtm::fd8_tiles(h));
+    if (h->c.engine == RTM_ENGINE_FD8 && !h->lap_iso()) TRY(rtm::fd8_tiles(h));
     return h->iso4 == 2 ? rtm::iso4_tiles(h) : (int)RTM_OK;
   };
   float best = 1e30f;

@@ -115,6 +115,68 @@ __device__ __forceinline__ void pml1(const PmlDev &P, const Grid3 &g, int pml3d,
   }
 }
 
+// Index of cell (ix, iy, iz) in the memory arrays of the face of dimension d
+// that holds it, with its side in bit 30 (the two sides of a dimension never
+// overlap), or -1 outside both; *layer = its distance from the outer edge.
+// Same indexing as pml_at; every face array has fewer than 2^30 cells.
+__device__ __forceinline__ int pml_face_index(const PmlDev &P, const Grid3 &g, int d, int ix, int iy, int iz,
+                                              int &layer) {
+  const int wl = P.f[d][SIDE_LO].w, wh = P.f[d][SIDE_HI].w;
+  if (d == DZ) {
+    if (iz < wl) return layer = iz, (int)(((long long)iy * g.nx + ix) * wl + iz);
+    if (wh && iz >= g.nz - wh)
+      return layer = g.nz - 1 - iz, (1 << 30) | (int)(((long long)iy * g.nx + ix) * wh + (iz - (g.nz - wh)));
+  } else if (d == DX) {
+    if (ix < wl) return layer = ix, (int)(((long long)iy * wl + ix) * g.nz + iz);
+    if (wh && ix >= g.nx - wh)
+      return layer = g.nx - 1 - ix, (1 << 30) | (int)(((long long)iy * wh + ix - (g.nx - wh)) * g.nz + iz);
+  } else {
+    if (iy < wl) return layer = iy, (int)(((long long)iy * g.nx + ix) * g.nz + iz);
+    if (wh && iy >= g.ny - wh)
+      return layer = g.ny - 1 - iy, (1 << 30) | (int)(((long long)(iy - (g.ny - wh)) * g.nx + ix) * g.nz + iz);
+  }
+  return -1;
+}
+
+// First-derivative PML round R on component AXIS of U cells at once (pml1's
+// arithmetic and order per cell: own dimension unscaled, then the two cross
+// dimensions scaled when pml3d).  Every memory value of the U cells is loaded
+// before the first recursion, so the batch costs one memory round trip
+// instead of one per face and cell.
+template <int AXIS, int R, int U>
+__device__ __forceinline__ void pml1_batch(const PmlDev &P, const Grid3 &g, int pml3d, float (&v)[U], const int (&ix)[U],
+                                           const int (&iy)[U], const int (&iz)[U], const bool (&act)[U]) {
+  // dimensions in pml1's order for this component and the memory component
+  // each keeps for it (bgprtm/FdEngine.cpp:301-350)
+  constexpr int D1 = AXIS == DZ ? DX : DZ, D2 = AXIS == DY ? DX : DY;
+  constexpr int C1 = AXIS == DY ? 2 : 1, C2 = AXIS == DZ ? 1 : 2;
+  const bool cross = pml3d != 0 && (AXIS != DY || g.ny > 1);
+  int enc[U][3], lay[U][3];
+  float q[U][3];
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int d = k == 0 ? AXIS : k == 1 ? D1 : D2, c = k == 0 ? 0 : k == 1 ? C1 : C2;
+      enc[u][k] = act[u] && (k == 0 || cross) ? pml_face_index(P, g, d, ix[u], iy[u], iz[u], lay[u][k]) : -1;
+      if (enc[u][k] >= 0) q[u][k] = P.f[d][enc[u][k] >> 30].q[R][c][enc[u][k] & 0x3fffffff];
+    }
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int d = k == 0 ? AXIS : k == 1 ? D1 : D2;
+      if (enc[u][k] >= 0) pml_round(P.f[d][enc[u][k] >> 30].co + lay[u][k] * 6 + (k ? 3 : 0), v[u], &q[u][k]);
+    }
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int d = k == 0 ? AXIS : k == 1 ? D1 : D2, c = k == 0 ? 0 : k == 1 ? C1 : C2;
+      if (enc[u][k] >= 0) P.f[d][enc[u][k] >> 30].q[R][c][enc[u][k] & 0x3fffffff] = q[u][k];
+    }
+}
+
 // Where a cell sits in the split-field PML faces: for each dimension d and
 // side s (lo, hi) the layer L (-1 outside the face) and the cell's index in
 // the face arrays.  Same indexing as pml_at.
@@ -246,6 +308,33 @@ __device__ __forceinline__ float div_accumulate(float w0, float vel, float dx, f
   float t = __fmaf_rn(-dx, vel, w0);
   t = __fmaf_rn(-dz, vel, t);
   return __fmaf_rn(-dy, vel, t);
+}
+
+// The same with a density model, in each engine's association of d vel rho:
+// FdEngine_fd (d vel) rho on every axis (bgprtm/FdEngine_fd.cpp:411, 437,
+// 463); FORM 0 FdEngine_cfd: (d vel) rho on x and z, d (vel rho) on y
+// (bgprtm/FdEngine_cfd.cpp:42, 64-67, 91); FORM 1 FdEngine_r2c / _r2r: vel
+// (rho d) on x and y (Util::transposeAndAdd, bgprtm/Util.cpp:155-175), (d vel)
+// rho on z; FORM 2 the Derivative path: ((dz + dx) + dy) rho, then vel
+// (getDiverge0, multiplyRho, applyVel; bgprtm/Derivative.cpp:92-112,
+// bgprtm/Propagator.cpp:1722-1746).  FORM -1: the FD form.
+template <int FORM>
+__device__ __forceinline__ float div_accumulate_rho(float w0, float vel, float rho, float dx, float dz, float dy) {
+  if (FORM == 2) return __fmaf_rn(-__fmul_rn(__fadd_rn(__fadd_rn(dz, dx), dy), rho), vel, w0);
+  float t;
+  if (FORM == 1) t = __fmaf_rn(-vel, __fmul_rn(rho, dx), w0);
+  else t = __fmaf_rn(-__fmul_rn(dx, vel), rho, w0);
+  t = __fmaf_rn(-__fmul_rn(dz, vel), rho, t);
+  if (FORM == 0) return __fmaf_rn(-dy, __fmul_rn(vel, rho), t);
+  if (FORM == 1) return __fmaf_rn(-vel, __fmul_rn(rho, dy), t);
+  return __fmaf_rn(-__fmul_rn(dy, vel), rho, t);
+}
+
+// KernelCPU::divideRho (bgprtm/KernelCPU.cpp:340-348)
+__device__ __forceinline__ void divide_rho(float rho, bool do_y, float &gx, float &gy, float &gz) {
+  gx = __fdiv_rn(gx, rho);
+  if (do_y) gy = __fdiv_rn(gy, rho);
+  gz = __fdiv_rn(gz, rho);
 }
 
 // pseudo-acoustic scaling of the gradient (ScalarVTI / ScalarTTI,

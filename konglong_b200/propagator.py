@@ -36,6 +36,7 @@ class Propagator:
         c.vmax, c.pml_eps = spec.vmax, spec.pml_eps
         c.pml3d, c.pml3d_scaler, c.top_pml = int(spec.pml3d), spec.pml3d_scaler, int(spec.top_pml)
         c.state_fp16 = int(spec.state_fp16)
+        c.use_rho = int(getattr(spec, "use_rho", False))
         c.kernel_variant = int(getattr(spec, "kernel_variant", 0))
         h = C.c_void_p()
         _lib.check(L.rtm_create(C.byref(d), C.byref(c), C.byref(h)), "rtm_create")
@@ -68,8 +69,9 @@ class Propagator:
     def set_q_coeffs(self, cq0, cq, wq):
         self._ck(self.L.rtm_set_q_coeffs(self.h, float(cq0), _arr(cq), _arr(wq)), "rtm_set_q_coeffs")
 
-    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None):
-        arrs = [_arr(a) for a in (vel, eps, dl, pjx, pjy, invq)]
+    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None, rho=None):
+        """KernelCPU::setModel(vel, rho, del, eps, pjx, pjy) + Vel2; rho with spec.use_rho."""
+        arrs = [_arr(a) for a in (vel, rho, eps, dl, pjx, pjy, invq)]
         for a in arrs:
             if a is not None and a.size != self.n:
                 raise ValueError("model volume size does not match the grid")

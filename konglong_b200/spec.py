@@ -39,6 +39,7 @@ class PropSpec:
     pml3d_scaler: float = 0.3
     top_pml: bool = True
     state_fp16: bool = False
+    use_rho: bool = False         # density model (KernelCPU::setModel's rho)
     kernel_variant: int = 0       # 0 auto, 1 one cell per thread / plain tiles, 2 TMA (CFD x/y tiles,
                                   # ISO one-cell plane pipeline), 3 FD8 4 z cells per thread with TMA
                                   # rings, 4 ISO 4 z cells with register prefetch

@@ -35,11 +35,11 @@ def _load_orc():
     vp = C.c_void_p
     lib.orc_create.restype = vp
     lib.orc_create.argtypes = [C.c_int] * 3 + [C.c_float] * 4 + [C.c_int] * 4 + [
-        _i32p, C.c_float, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int]
+        _i32p, C.c_float, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
     lib.orc_destroy.argtypes = [vp]
     lib.orc_set_q_coeffs.argtypes = [vp, C.c_float, _f32p, _f32p]
     optf = C.c_void_p
-    lib.orc_set_model.argtypes = [vp] + [optf] * 6
+    lib.orc_set_model.argtypes = [vp] + [optf] * 7
     for name in ("orc_reset", "orc_kernel", "orc_update2nd", "orc_swap"):
         getattr(lib, name).argtypes = [vp]
     lib.orc_set_injection.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p,
@@ -95,7 +95,7 @@ class Oracle:
         self.h = self.lib.orc_create(s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.dt, s.engine,
                                      s.model_type, int(s.use_q), s.q_order, nb, s.vmax,
                                      s.pml_eps, int(s.pml3d), s.pml3d_scaler, int(s.top_pml),
-                                     1 if double else 0)
+                                     1 if double else 0, int(getattr(s, "use_rho", False)))
         self.n = s.nx * s.ny * s.nz
         self._keep = []
 
@@ -110,9 +110,9 @@ class Oracle:
         self.lib.orc_set_q_coeffs(self.h, cq0, np.ascontiguousarray(cq, np.float32),
                                   np.ascontiguousarray(wq, np.float32))
 
-    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None):
+    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, invq=None, rho=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float32).ravel()
-                for a in (vel, eps, dl, pjx, pjy, invq)]
+                for a in (vel, rho, eps, dl, pjx, pjy, invq)]
         self._keep = arrs
         self.lib.orc_set_model(self.h, *[_ptr(a) for a in arrs])
 
@@ -249,9 +249,9 @@ def ref_lib():
         vp = C.c_void_p
         lib.ref_create.restype = vp
         lib.ref_create.argtypes = [C.c_int] * 3 + [C.c_float] * 4 + [C.c_int] * 2 + [
-            _i32p, C.c_float, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int]
+            _i32p, C.c_float, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         lib.ref_destroy.argtypes = [vp]
-        lib.ref_set_model.argtypes = [vp] + [C.c_void_p] * 5
+        lib.ref_set_model.argtypes = [vp] + [C.c_void_p] * 6
         for name in ("ref_reset", "ref_kernel", "ref_update2nd", "ref_swap"):
             getattr(lib, name).argtypes = [vp]
         lib.ref_put.argtypes = [vp, C.c_int, _f32p]
@@ -259,6 +259,10 @@ def ref_lib():
         lib.ref_set_injection.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p,
                                           _f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float]
         lib.ref_inject.argtypes = [vp, C.c_int]
+        lib.ref_set_extraction.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p,
+                                           _f32p, _f32p, _f32p, C.c_int]
+        lib.ref_get_traces.argtypes = [vp, _f32p]
+        lib.ref_modelling.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         lib.ref_run.restype = C.c_double
         lib.ref_run.argtypes = [vp, C.c_int, C.c_int]
         lib.ref_c16_compress.argtypes = [_f32p, _u16p, C.c_int, C.c_int, C.c_int]
@@ -284,7 +288,8 @@ class Reference:
         nb = np.ascontiguousarray(s.nbnd, dtype=np.int32)
         self.h = self.lib.ref_create(s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.dt, s.engine,
                                      s.model_type, nb, s.vmax, s.pml_eps, int(s.pml3d),
-                                     s.pml3d_scaler, int(s.top_pml), nthreads)
+                                     s.pml3d_scaler, int(s.top_pml), nthreads,
+                                     int(getattr(s, "use_rho", False)))
         if not self.h:
             raise ValueError(f"engine {s.engine}: not a KernelCPU engine of the compiled reference")
         self.n = s.nx * s.ny * s.nz
@@ -297,9 +302,9 @@ class Reference:
 
     __del__ = close
 
-    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None):
+    def set_model(self, vel, eps=None, dl=None, pjx=None, pjy=None, rho=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float32).ravel()
-                for a in (vel, eps, dl, pjx, pjy)]
+                for a in (vel, rho, eps, dl, pjx, pjy)]
         self._keep = arrs
         self.lib.ref_set_model(self.h, *[_ptr(a) for a in arrs])
 
@@ -322,6 +327,20 @@ class Reference:
 
     def inject(self, it):
         self.lib.ref_inject(self.h, it)
+
+    def set_extraction(self, ts, nt_out):
+        self._ext = (ts, nt_out)
+        self.lib.ref_set_extraction(self.h, ts.ntr, ts.lx, ts.ly, ts.lz, ts.off, ts.len, ts.kx, ts.ky, ts.kz,
+                                    nt_out)
+
+    def modelling(self, nts, it_shift, ntratio):
+        self.lib.ref_modelling(self.h, nts, it_shift, ntratio)
+
+    def traces(self):
+        ts, nt_out = self._ext
+        out = np.zeros(ts.ntr * nt_out, np.float32)
+        self.lib.ref_get_traces(self.h, out)
+        return out.reshape(ts.ntr, nt_out)
 
     def run(self, it0, nsteps):
         return self.lib.ref_run(self.h, it0, nsteps)

@@ -38,15 +38,19 @@ struct RefHandle {
   float dt;
   size_t n;
   KernelCPU *k = nullptr;
-  float *w0, *w1, *wr, *vel, *eps = nullptr, *del = nullptr, *pjx = nullptr, *pjy = nullptr;
+  float *w0, *w1, *wr, *vel, *eps = nullptr, *del = nullptr, *pjx = nullptr, *pjy = nullptr, *rho = nullptr;
   // injection traces (restated Receiver::apply_src)
   int ntr = 0, lx = 0, ly = 0, lz = 0, nt = 0;
   std::vector<int> off, len;
   std::vector<float> kx, ky, kz, traces;
   float scaler = 1;
+  // receivers (restated ExtractReceiverData::extract / Receiver::extract_value)
+  int nrc = 0, rlx = 0, rly = 0, rlz = 0, nt_out = 0;
+  std::vector<int> roff, rlen;
+  std::vector<float> rkx, rky, rkz, out;
 };
 
-void set_globals(int engine, int model, float pml_eps, int pml3d, float scaler, int top_pml) {
+void set_globals(int engine, int model, float pml_eps, int pml3d, float scaler, int top_pml, int use_rho) {
   shim_store().kv.clear();
   global_pars["Engine"] = engine == 1 ? "CFD" : engine == 2 ? "FFTWR2C" : engine == 3 ? "FFTWR2R" : "FD";
   global_pars["fd_use_taylor"] = 1;
@@ -62,6 +66,9 @@ void set_globals(int engine, int model, float pml_eps, int pml3d, float scaler, 
   // the VTI path needs.
   if (model == 3) global_pars["global"]["pjx"] = 1;
   if (model == 2) global_pars["global"]["epsilon"] = 1, global_pars["force_tti"] = 1;
+  // a density model sends ISO through KernelCPU::TTI (bgprtm/KernelCPU.cpp:128),
+  // which needs the three-component PML allocation as above
+  if (use_rho) global_pars["global"]["rho"] = 1, global_pars["force_tti"] = 1;
 }
 }  // namespace
 
@@ -69,9 +76,9 @@ extern "C" {
 
 void *ref_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt, int engine, int model,
                  const int *nbnd, float vmax, float pml_eps, int pml3d, float pml3d_scaler, int top_pml,
-                 int nthreads) {
+                 int nthreads, int use_rho) {
   if (engine < 0 || engine > 3) return nullptr;  // KernelCPU engines only (FD, CFD, FFTWR2C, FFTWR2R)
-  set_globals(engine, model, pml_eps, pml3d, pml3d_scaler, top_pml);
+  set_globals(engine, model, pml_eps, pml3d, pml3d_scaler, top_pml, use_rho);
   RefHandle *h = new RefHandle();
   h->nx = nx, h->ny = ny, h->nz = nz, h->model = model, h->engine = engine, h->dt = dt;
   h->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
@@ -90,13 +97,16 @@ void *ref_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt,
 void ref_destroy(void *p) {
   RefHandle *h = (RefHandle *)p;
   delete h->k;
-  for (float *a : {h->w0, h->w1, h->wr, h->vel, h->eps, h->del, h->pjx, h->pjy})
+  for (float *a : {h->w0, h->w1, h->wr, h->vel, h->eps, h->del, h->pjx, h->pjy, h->rho})
     if (a) _mm_free(a);
   delete h;
 }
 
-// Propagator::Vel2, no-Q branch (bgprtm/Propagator.cpp:715-725)
-void ref_set_model(void *p, const float *v, const float *eps, const float *del, const float *pjx, const float *pjy) {
+// Propagator::Vel2, no-Q branch (bgprtm/Propagator.cpp:715-725); rho (may be
+// null) goes to KernelCPU::setModel as Propagator passes volModel[RHO]
+// (bgprtm/Propagator.cpp:299)
+void ref_set_model(void *p, const float *v, const float *rho, const float *eps, const float *del, const float *pjx,
+                   const float *pjy) {
   RefHandle *h = (RefHandle *)p;
   float dt2 = h->dt * h->dt;
   for (size_t i = 0; i < h->n; i++) h->vel[i] = (v[i] * v[i]) * dt2;
@@ -105,8 +115,8 @@ void ref_set_model(void *p, const float *v, const float *eps, const float *del, 
     if (!dst) dst = vol_alloc(h->n);
     memcpy(dst, src, h->n * 4);
   };
-  cp(h->eps, eps), cp(h->del, del), cp(h->pjx, pjx), cp(h->pjy, pjy);
-  h->k->setModel(h->vel, nullptr, h->del, h->eps, h->pjx, h->pjy);
+  cp(h->eps, eps), cp(h->del, del), cp(h->pjx, pjx), cp(h->pjy, pjy), cp(h->rho, rho);
+  h->k->setModel(h->vel, h->rho, h->del, h->eps, h->pjx, h->pjy);
 }
 
 void ref_reset(void *p) {
@@ -174,6 +184,53 @@ void ref_inject(void *p, int it) {
         for (int iz = 0; iz < l[2]; iz++) h->w0[off + iz] += cx * h->kz[(size_t)r * h->lz + iz] * h->vel[off + iz];
       }
     }
+  }
+}
+
+void ref_set_extraction(void *p, int ntr, int lx, int ly, int lz, const int *off, const int *len, const float *kx,
+                        const float *ky, const float *kz, int nt_out) {
+  RefHandle *h = (RefHandle *)p;
+  h->nrc = ntr, h->rlx = lx, h->rly = ly, h->rlz = lz, h->nt_out = nt_out;
+  h->roff.assign(off, off + 3 * ntr), h->rlen.assign(len, len + 3 * ntr);
+  h->rkx.assign(kx, kx + (size_t)ntr * lx), h->rky.assign(ky, ky + (size_t)ntr * ly);
+  h->rkz.assign(kz, kz + (size_t)ntr * lz);
+  h->out.assign((size_t)ntr * nt_out, 0.f);
+}
+
+// Receiver::extract_value for every receiver (bgprtm/Receiver.cpp:394-426),
+// sample jt
+void ref_extract(void *p, int jt) {
+  RefHandle *h = (RefHandle *)p;
+  if (jt < 0 || jt >= h->nt_out) return;
+#pragma omp parallel for num_threads(h->nthreads) schedule(static)
+  for (int r = 0; r < h->nrc; r++) {
+    float val = 0.f;
+    const int *o = &h->roff[3 * r], *l = &h->rlen[3 * r];
+    for (int iy = 0; iy < l[1]; iy++) {
+      float cy = h->rky[(size_t)r * h->rly + iy];
+      for (int ix = 0; ix < l[0]; ix++) {
+        float cx = cy * h->rkx[(size_t)r * h->rlx + ix];
+        size_t off = ((size_t)(iy + o[1]) * h->nx + ix + o[0]) * h->nz + o[2];
+        for (int iz = 0; iz < l[2]; iz++) val += cx * h->rkz[(size_t)r * h->rlz + iz] * h->w0[off + iz];
+      }
+    }
+    h->out[(size_t)r * h->nt_out + jt] = val;
+  }
+}
+void ref_get_traces(void *p, float *dst) {
+  RefHandle *h = (RefHandle *)p;
+  std::copy(h->out.begin(), h->out.end(), dst);
+}
+
+// Propagator::modelling's loop body (bgprtm/Propagator.cpp:1099-1153): kernel,
+// update2nd, inject(it + it_shift), extract(it / ntratio), swap
+void ref_modelling(void *p, int nts, int it_shift, int ntratio) {
+  for (int it = 0; it < nts; it++) {
+    ref_kernel(p);
+    ref_update2nd(p);
+    ref_inject(p, it + it_shift);
+    if (it % ntratio == 0) ref_extract(p, it / ntratio);
+    ref_swap(p);
   }
 }
 

@@ -42,6 +42,7 @@ struct Config {
   int pml3d;
   float pml3d_scaler;
   int top_pml;
+  int use_rho;  // density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78)
 };
 
 // Compact FD plan (bgprtm/Cfd_plan.cpp:54-290): B (9-band) LU factors bm
@@ -254,7 +255,7 @@ public:
   R dx, dy, dz, dt;
   size_t nxz, nxyz;
   Config cfg;
-  vector<R> w0, w1, vel, eps, del, pjx, pjy, invq, px, py, pz;
+  vector<R> w0, w1, vel, eps, del, pjx, pjy, invq, px, py, pz, rho;
   vector<R> wq[2];  // [order][nxyz] each
   int iq0 = 0, iq1 = 1;
   // FD tables: c1*[m], c2*[m] for m = 0..4 (m = 0 is the centre of c2)
@@ -339,7 +340,9 @@ public:
   // FdEngine::setBoundary + PML::init (bgprtm/FdEngine.cpp:108-182,
   // bgprtm/PML.cpp:87-124, limit_slope = false).
   void build_pml() {
-    bool is2nd = (cfg.engine == FD8 && cfg.model_type == ISO);
+    // a density model takes ISO through the first-derivative path
+    // (bgprtm/KernelCPU.cpp:128)
+    bool is2nd = (cfg.engine == FD8 && cfg.model_type == ISO && !cfg.use_rho);
     dimPML = (!cfg.pml3d || is2nd) ? 1 : (ny == 1 ? 2 : 3);
     const int nn[3] = {nx, ny, nz};
     const R dd[3] = {dx, dy, dz};
@@ -527,8 +530,22 @@ public:
     return v;
   }
 
+  // out - v * vel, or with a density model the engine's own form of
+  // out - v * vel * rho: FdEngine_fd (v vel) rho on every axis
+  // (bgprtm/FdEngine_fd.cpp:411, 437, 463); FdEngine_cfd (v vel) rho on x and
+  // z, v (vel rho) on y (bgprtm/FdEngine_cfd.cpp:42, 64-67, 91);
+  // FdEngine_r2c / _r2r (v vel) rho on z, vel (rho v) on x and y through
+  // Util::transposeAndAdd (bgprtm/FdEngine_r2c.cpp:177-181,
+  // bgprtm/Util.cpp:155-175)
+  inline R acc(R o, R v, size_t i, int axis) const {
+    if (!cfg.use_rho) return o - v * vel[i];
+    if (cfg.engine == CFD && axis == Y) return o - v * (vel[i] * rho[i]);
+    if ((cfg.engine == R2C || cfg.engine == R2R) && axis != Z) return o - vel[i] * (rho[i] * v);
+    return o - v * vel[i] * rho[i];
+  }
+
   // derivative of a whole volume along axis, PML round `round`, then either
-  // store (iacc = 0) or out -= deriv * vel (iacc = 1).
+  // store (iacc = 0) or accumulate into out (iacc = 1, acc).
   void deriv_volume(const R *in, R *out, int axis, int round, int iacc, int plan = -1) {
     if (cfg.engine == FD8) {
 #pragma omp parallel for collapse(2) schedule(static)
@@ -538,7 +555,7 @@ public:
             R v = d1_fd(in, axis, ix, iy, iz);
             pml1(axis, round, v, ix, iy, iz);
             size_t i = iy * nxz + (size_t)ix * nz + iz;
-            if (iacc) out[i] = out[i] - v * vel[i];
+            if (iacc) out[i] = acc(out[i], v, i, axis);
             else out[i] = v;
           }
       return;
@@ -587,7 +604,7 @@ public:
           size_t i = iy * nxz + (size_t)ix * nz + iz;
           R v = d[i];
           pml1(axis, round, v, ix, iy, iz);
-          if (iacc) out[i] = out[i] - v * vel[i];
+          if (iacc) out[i] = acc(out[i], v, i, axis);
           else out[i] = v;
         }
   }
@@ -627,12 +644,24 @@ public:
     }
   }
 
+  // KernelCPU::divideRho (bgprtm/KernelCPU.cpp:340-348): px, py (ny > 1), pz / rho
+  void divide_rho() {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nxyz; i++) {
+      px[i] /= rho[i];
+      if (ny > 1) py[i] /= rho[i];
+      pz[i] /= rho[i];
+    }
+  }
+
   // KernelCPU::TTI (bgprtm/KernelCPU.cpp:93-119): gradient with PML round 1,
-  // pseudo-acoustic scaling, divergence accumulated into w0 with PML round 2.
+  // division by the density, pseudo-acoustic scaling, divergence accumulated
+  // into w0 with PML round 2.
   void aniso_kernel() {
     if (ny > 1) deriv_volume(w1.data(), py.data(), Y, 0, 0);
     deriv_volume(w1.data(), pz.data(), Z, 0, 0);
     deriv_volume(w1.data(), px.data(), X, 0, 0);
+    if (cfg.use_rho) divide_rho();
     if (cfg.model_type == TTI || cfg.model_type == VTI) scale_gradient();
     deriv_volume(px.data(), w0.data(), X, 1, 1);
     deriv_volume(pz.data(), w0.data(), Z, 1, 1);
@@ -652,6 +681,7 @@ public:
     if (nx > 1) deriv_volume(w1.data(), px.data(), X, 0, 0, 0);
     if (ny > 1) deriv_volume(w1.data(), py.data(), Y, 0, 0, 0);
     deriv_volume(w1.data(), pz.data(), Z, 0, 0, 0);
+    if (cfg.use_rho) divide_rho();  // Propagator::divideRho (bgprtm/Propagator.cpp:1703-1718)
     if (cfg.model_type == TTI || cfg.model_type == VTI) scale_gradient();
     const int sw = cfg.model_type == TTI ? 0 : 1;
     vector<R> wb(nxyz), buf(nxyz);
@@ -662,11 +692,14 @@ public:
       deriv_volume(py.data(), buf.data(), Y, 1, 0, sw);
       for (size_t i = 0; i < nxyz; i++) wb[i] = wb[i] + buf[i];
     }
+    // multiplyRho (wb *= rho, bgprtm/Propagator.cpp:1722-1732), applyVel, w0 -= wb
+    if (cfg.use_rho)
+      for (size_t i = 0; i < nxyz; i++) wb[i] = wb[i] * rho[i];
     for (size_t i = 0; i < nxyz; i++) w0[i] = w0[i] - wb[i] * vel[i];
   }
 
   void kernel() {
-    if (cfg.engine == FD8 && cfg.model_type == ISO) iso_fd8_kernel();
+    if (cfg.engine == FD8 && cfg.model_type == ISO && !cfg.use_rho) iso_fd8_kernel();
     else if (cfg.engine == CFDB) cfd_batch_kernel();
     else aniso_kernel();
   }
@@ -699,8 +732,10 @@ public:
   }
 
   // Propagator::Vel2 (bgprtm/Propagator.cpp:711-742)
-  void set_model(const float *v, const float *e, const float *d, const float *ax, const float *ay, const float *iq) {
+  void set_model(const float *v, const float *rh, const float *e, const float *d, const float *ax, const float *ay,
+                 const float *iq) {
     R dt2 = dt * dt;
+    if (cfg.use_rho) rho.assign(rh, rh + nxyz);
     if (cfg.model_type >= VTI) {
       eps.assign(e, e + nxyz);
       del.assign(d, d + nxyz);
@@ -893,8 +928,8 @@ extern "C" {
 
 void *orc_create(int nx, int ny, int nz, float dx, float dy, float dz, float dt, int engine, int model_type,
                  int use_q, int q_order, const int *nbnd, float vmax, float pml_eps, int pml3d, float pml3d_scaler,
-                 int top_pml, int prec) {
-  orc::Config c{engine, model_type, use_q, q_order, {0}, vmax, pml_eps, pml3d, pml3d_scaler, top_pml};
+                 int top_pml, int prec, int use_rho) {
+  orc::Config c{engine, model_type, use_q, q_order, {0}, vmax, pml_eps, pml3d, pml3d_scaler, top_pml, use_rho};
   for (int i = 0; i < 6; i++) c.nbnd[i] = nbnd[i];
   Handle *h = new Handle();
   h->prec = prec;
@@ -917,9 +952,9 @@ void orc_set_q_coeffs(void *p, float cq0, const float *cq, const float *wq) {
   if (h->prec) set(*h->d);
   else set(*h->f);
 }
-void orc_set_model(void *p, const float *v, const float *e, const float *d, const float *ax, const float *ay,
-                   const float *iq) {
-  DISPATCH((Handle *)p, set_model(v, e, d, ax, ay, iq));
+void orc_set_model(void *p, const float *v, const float *rh, const float *e, const float *d, const float *ax,
+                   const float *ay, const float *iq) {
+  DISPATCH((Handle *)p, set_model(v, rh, e, d, ax, ay, iq));
 }
 void orc_reset(void *p) { DISPATCH((Handle *)p, clean()); }
 void orc_kernel(void *p) { DISPATCH((Handle *)p, kernel()); }

@@ -24,6 +24,15 @@ CASES = {
     "iso_r2r": dict(engine=ENGINE_R2R, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=21),
     "vti_r2r": dict(engine=ENGINE_R2R, model=VTI, shape=(23, 20, 28), pml=6, steps=3, seed=22),
     "tti_r2r": dict(engine=ENGINE_R2R, model=TTI, shape=(24, 21, 27), pml=6, steps=3, seed=23),
+    # density models (KernelCPU::setModel's rho): ISO through the first-derivative
+    # passes, the gradient divided by rho, each engine's vel * rho accumulation
+    "iso_fd8_rho": dict(engine=ENGINE_FD8, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=24, rho=True),
+    "vti_fd8_rho": dict(engine=ENGINE_FD8, model=VTI, shape=(24, 20, 28), pml=6, steps=3, seed=25, rho=True),
+    "tti_fd8_rho": dict(engine=ENGINE_FD8, model=TTI, shape=(24, 20, 28), pml=6, steps=3, seed=26, rho=True),
+    "iso_cfd_rho": dict(engine=ENGINE_CFD, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=27, rho=True),
+    "tti_cfd_rho": dict(engine=ENGINE_CFD, model=TTI, shape=(24, 20, 28), pml=6, steps=3, seed=28, rho=True),
+    "vti_r2c_rho": dict(engine=ENGINE_R2C, model=VTI, shape=(24, 20, 28), pml=6, steps=3, seed=29, rho=True),
+    "iso_r2r_rho": dict(engine=ENGINE_R2R, model=ISO, shape=(24, 20, 28), pml=6, steps=3, seed=30, rho=True),
 }
 
 
@@ -46,6 +55,9 @@ def case_inputs(c):
     # smooth-ish wavefields (a band-limited field like a propagating wave)
     w0 = gaussian_filter(rng.standard_normal(sh), 1.5).astype(np.float32)
     w1 = gaussian_filter(rng.standard_normal(sh), 1.5).astype(np.float32)
+    if c.get("rho"):  # density 1000-2500 kg/m^3 from its own stream (the other inputs stay as they are)
+        spec.use_rho = True
+        model["rho"] = (1000.0 + 1500.0 * np.random.default_rng(c["seed"] + 1000).random(sh)).astype(np.float32)
     return spec, model, w0, w1
 
 

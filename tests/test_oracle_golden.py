@@ -278,3 +278,53 @@ def test_first_derivative_engines_match_the_homogeneous_green_function(engine):
     cc = tr @ want / np.linalg.norm(tr) / np.linalg.norm(want)
     amp = (tr @ want) / (want @ want)
     assert cc > 0.9995 and abs(amp - 1) < 0.005, (cc, amp)
+
+
+@pytest.mark.parametrize("name", [k for k in CASES if k.endswith("_rho")])
+def test_density_changes_the_reference_result(golden, name):
+    """The density fixtures carry the density: the same step without it (rho
+    = 1, ISO FD8 then on its Laplacian path) is far from the reference's."""
+    c = dict(CASES[name])
+    spec, model, w0, w1 = case_inputs(c)
+    spec.use_rho = False
+    model.pop("rho")
+    o = O.Oracle(spec)
+    o.set_model(**model)
+    o.put(0, w0)
+    o.put(1, w1)
+    for _ in range(c["steps"]):
+        o.kernel()
+        o.update2nd()
+        o.swap()
+    assert rel_l2(o.get(1), golden[f"{name}__w1"]) > 1e-2
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference not built")
+def test_reference_compact_fd_tti_grows_in_a_tilted_medium():
+    """Recorded behaviour of the reference: its compact-FD TTI step (KernelCPU
+    + FdEngine_cfd, compiled) grows without bound in a homogeneous medium with
+    a 30-degree tilt, while its FD8 TTI step on the same model stays bounded;
+    the oracle follows the compact-FD growth.  Long compact-FD runs are
+    therefore compared on untilted TTI models."""
+    from konglong_b200 import workloads as W
+    from konglong_b200.propagator import spread_coeffs
+    from konglong_b200.spec import ENGINE_CFD, ENGINE_FD8, TTI, PropSpec
+    th, ph = np.deg2rad(30.0), np.deg2rad(45.0)
+    peak = {}
+    for eng in (ENGINE_CFD, ENGINE_FD8):
+        s = PropSpec(nx=52, ny=52, nz=40, engine=eng, model_type=TTI, nbnd=(6,) * 6, vmax=4500.0, dt=0.0005)
+        sh = s.shape
+        m = dict(vel=np.full(sh, 3000, np.float32), eps=np.full(sh, 0.2, np.float32), dl=np.full(sh, 0.1, np.float32),
+                 pjx=np.full(sh, -np.sin(th) * np.cos(ph), np.float32),
+                 pjy=np.full(sh, -np.sin(th) * np.sin(ph), np.float32))
+        k1, k2 = W.spread_band(s)
+        src = W.make_traceset([(26, 26, 20)], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+        r = O.Reference(s, nthreads=4)
+        r.set_model(**m)
+        r.set_injection(src, W.ricker(20.0, s.dt, 30)[None, :], s.dt_dxyz)
+        r.reset()
+        r.run(0, 30)
+        peak[eng] = float(np.abs(r.get(1)).max())
+        r.close()
+    assert peak[ENGINE_CFD] > 1e6
+    assert peak[ENGINE_FD8] < 1e3
