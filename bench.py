@@ -412,6 +412,112 @@ def run_small_shots(args, ranks):
                        "cell_steps": cell_steps, "shots": nshots}}
 
 
+RTM_FORMS = {
+    # plain FP32 GPU form: FP32 state, Q memory and snapshots
+    "plain": dict(q_bf16=False, snap="fp32"),
+    # mixed precision: BF16 Q memory, FP16 snapshots with a per-slab scale
+    "mixed": dict(q_bf16=True, snap="fp16s"),
+    # mixed precision + learned compression: BF16 Q memory, learned 8^3-block
+    # snapshots (16:1) with the FP16 store of their 5 % highest-energy blocks
+    "chosen": dict(q_bf16=True, snap="ae"),
+}
+
+
+def train_compressor(seed=5, nblocks=20000, steps=3000):
+    """The learned snapshot code trained as the workload describes: about 20k
+    8^3 blocks of forward wavefields of the compact-FD VTI model family, Adam
+    on the GPU by the project's own kernels."""
+    from konglong_b200 import compressor as CP
+    from konglong_b200 import workloads as W
+    from konglong_b200.propagator import Propagator, spread_coeffs
+    shot = W.vti_cfd(scale=0.25, seed=seed, nt=400)
+    blocks, scales = CP.training_blocks(shot, Propagator, spread_coeffs, nblocks=nblocks, every=20, seed=seed)
+    ae = CP.AutoEncoder(seed=seed)
+    ae.fit(blocks, steps=steps, weights=scales ** 2)
+    return ae, int(blocks.shape[0])
+
+
+def rtm_form_propagator(shot, form, ae=None):
+    import dataclasses
+    from konglong_b200 import workloads as W
+    from konglong_b200.propagator import Propagator
+    from konglong_b200.spec import SNAP_AE, SNAP_FP16S, SNAP_FP32
+    f = RTM_FORMS[form]
+    s = dataclasses.replace(shot.spec, q_bf16=f["q_bf16"])
+    p = Propagator(s)
+    p.set_q_coeffs(*W.q_coefficients(s.dt, shot.fpeak))
+    p.set_model(**shot.model_arrays())
+    fmt = {"fp32": SNAP_FP32, "fp16s": SNAP_FP16S, "ae": SNAP_AE}[f["snap"]]
+    if fmt == SNAP_AE:
+        p.set_compressor(ae)
+        p.set_compressor_fallback(1e-3, 0.05)
+    return p, fmt
+
+
+def run_rtm_shot(args, ranks):
+    """RTM s/shot of the TTI + Q workload (640 x 640 x 512, PML 32, 5000 steps)
+    in the plain FP32 form and the chosen form (mixed precision + learned
+    snapshot compression; RTM_FORMS).  Each form runs K forward steps (a
+    snapshot every 8 steps) and K backward steps (the 128 x 128 receiver traces
+    injected, the imaging condition fused into the step) on the full grid,
+    timed with CUDA events; s/shot = (forward + backward ms per step) x 5000.
+    Image NRMSE of each form against the plain form: the same shot at 0.08
+    scale (51 x 51 x 41, 160 steps)."""
+    from konglong_b200 import workloads as W
+    from konglong_b200.propagator import spread_coeffs
+    from konglong_b200.spec import BACKWARD, FORWARD
+    K, Wm = args.steps, args.warmup
+    forms = ["plain", "mixed", "chosen"]
+    ae, ntrain = train_compressor()
+    interval = 8
+    res = {}
+    shot = W.tti_q(scale=args.scale, nt=2 * (K + Wm) + 8)
+    s = shot.spec
+    k1, k2 = W.spread_band(s)
+    src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    rcv = W.make_traceset(shot.rcv_pos, s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
+    data = (np.random.default_rng(7).standard_normal((rcv.ntr, shot.nt)) * 1e3).astype(np.float32)
+    clk_all = []
+    for form in forms:
+        p, fmt = rtm_form_propagator(shot, form, ae)
+        p.snapshot_setup(fmt, (Wm + K) // interval + 2)
+        p.reset()
+        p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
+        p.migration(FORWARD, 0, Wm, -1, interval)          # warm-up (graph capture, first launches)
+        with ClockSampler(ranks.local_rank) as clk:
+            p.migration(FORWARD, Wm, Wm + K, -1, interval)
+            fwd = p.last_loop_ms
+            p.reset()
+            p.image_setup(3, 4, 1)
+            p.set_injection(rcv, data, s.dt_dxyz)
+            p.migration(BACKWARD, Wm + K - 1, Wm - 1, -1, interval)
+            bwd = p.last_loop_ms
+        clk_all.append(clk.summary())
+        p.close()
+        res[form] = {"forward_ms_per_step": fwd / K, "backward_ms_per_step": bwd / K,
+                     "s_per_shot": (fwd + bwd) / K * 5000 / 1e3}
+    # image error of each form against the plain FP32 form on the same shot at
+    # 0.08 scale (160 steps); the tests state both against the FP64 oracle
+    small = W.tti_q(scale=0.08, nt=160)
+    ss = small.spec
+    k1, k2 = W.spread_band(ss)
+    s_src = W.make_traceset([small.src_pos], ss.nx, ss.ny, ss.nz, 10, k1, k2, spread_coeffs)
+    s_rcv = W.make_traceset(small.rcv_pos, ss.nx, ss.ny, ss.nz, 10, k1, k2, spread_coeffs)
+    s_data = (np.random.default_rng(7).standard_normal((s_rcv.ntr, 160)) * 1e3).astype(np.float32)
+    imgs = {}
+    for form in forms:
+        p, fmt = rtm_form_propagator(small, form, ae)
+        imgs[form] = p.rtm_shot(s_src, small.wavelet[None, :], s_rcv, s_data, 160, 112, 4, snap_fmt=fmt,
+                                ntaper_t=3, ntaper_z=4)[0]
+        p.close()
+    ref = imgs["plain"].astype(np.float64).ravel()
+    for form in forms:
+        res[form]["image_nrmse_vs_plain"] = float(np.linalg.norm(imgs[form].astype(np.float64).ravel() - ref) /
+                                                  max(np.linalg.norm(ref), 1e-300))
+    ae.close()
+    return {"forms": res, "clocks": clk_all, "ntrain": ntrain, "shot": shot}
+
+
 def cpu_baseline(shot, max_seconds=20.0):
     """The reference's own CPU kernels (oracle/_ref) on the full grid, all host
     threads, a bounded number of time steps."""
@@ -479,13 +585,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="vti_cfd",
-                    choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512", "vti_r2c", "vti_r2r", "small_shots"])
+                    choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512", "vti_r2c", "vti_r2r", "small_shots",
+                             "tti_q_rtm"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="grid scale of the workload (1.0 = the configuration the metric is quoted on; "
                          "smaller values are for profiler captures)")
     ap.add_argument("--state-fp16", action="store_true",
                     help="FP16 wavefield state with per-slab scales (FD8 VTI / TTI workloads)")
-    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
                     help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiler runs: timings under a profiler mislead the tuner)")
@@ -536,6 +643,33 @@ def main():
                     "speedup_vs_per_shot": r["value"] / r["per_shot"]["value"] if world == 1 else None,
                     "gpts": r["gpts"], "roofline": r["roofline"], "cpu_baseline": None, "e2e": r["e2e"],
                     "clocks": r["clocks"], "tuned_shape": r["tuned_shape"]}
+            print(json.dumps(line), flush=True)
+        R.finish(ranks)
+        return
+    if args.workload == "tti_q_rtm":
+        r = run_rtm_shot(args, ranks)
+        if rank == 0:
+            f = r["forms"]
+            s = r["shot"].spec
+            line = {"metric": "RTM s/shot", "value": f["chosen"]["s_per_shot"], "unit": "s/shot", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f32 arithmetic; bf16 Q memory and learned / fp16 snapshots "
+                                                  "in the mixed and chosen forms",
+                    "data": "synthetic (seeded model)",
+                    "config": {"workload": f"tti_q RTM shot: {s.nx}x{s.ny}x{s.nz} FD8 TTI+Q, PML {s.nbnd[0]}, "
+                                           f"dt {s.dt * 1e3:.4f} ms, 5000 steps, snapshots every 8 steps",
+                               "extrapolation": f"{args.steps} forward + {args.steps} backward full-grid steps "
+                                                "timed, x 5000 steps per pass",
+                               "image_nrmse": "each form's image vs the plain FP32 form's on the same shot at "
+                                              "0.08 scale (51x51x41, 160 steps)",
+                               "compressor_training_blocks": r["ntrain"],
+                               "forms": {k: RTM_FORMS[k] for k in f}},
+                    "s_per_shot": {k: v["s_per_shot"] for k, v in f.items()},
+                    "speedup_vs_plain": {k: f["plain"]["s_per_shot"] / v["s_per_shot"] for k, v in f.items()},
+                    "image_nrmse_vs_plain": {k: v["image_nrmse_vs_plain"] for k, v in f.items()},
+                    "ms_per_step": {k: {"forward": v["forward_ms_per_step"], "backward": v["backward_ms_per_step"]}
+                                    for k, v in f.items()},
+                    "cpu_baseline": None, "clocks": r["clocks"]}
             print(json.dumps(line), flush=True)
         R.finish(ranks)
         return

@@ -67,8 +67,22 @@ typedef enum rtm_status {
  * bgprtm/FdEngine_r2r.cpp), FD::CFD_BATCH (the Derivative path of
  * Propagator::kernel, bgprtm/Propagator.cpp:901-943: compact FD through
  * Derivative_cfd, Boundary's per-axis PML so pml3d is ignored, the
- * divergence-pass plan of iswitch) */
-enum { RTM_ENGINE_FD8 = 0, RTM_ENGINE_CFD = 1, RTM_ENGINE_R2C = 2, RTM_ENGINE_R2R = 3, RTM_ENGINE_CFDB = 4 };
+ * divergence-pass plan of iswitch), FD::FFTV and FD::SINCOS (the same
+ * Derivative path with Derivative_fftv's spectral first derivative and
+ * Derivative_sincos's cosine / sine transform pair, bgprtm/Derivative_fftv.cpp,
+ * bgprtm/Derivative_sincos.cpp; libfftv, which implements both, is not in the
+ * reference tree: here the plain spectral derivative (every bin below Nyquist
+ * times i k, an even line's Nyquist bin zeroed) and the FFTWR2R line
+ * operators) */
+enum {
+  RTM_ENGINE_FD8 = 0,
+  RTM_ENGINE_CFD = 1,
+  RTM_ENGINE_R2C = 2,
+  RTM_ENGINE_R2R = 3,
+  RTM_ENGINE_CFDB = 4,
+  RTM_ENGINE_FFTV = 5,
+  RTM_ENGINE_SINCOS = 6
+};
 enum { RTM_ISO = 1, RTM_VTI = 2, RTM_TTI = 3 };       /* ModelType (bgprtm/Model.h:13) */
 enum { RTM_FORWARD = 0, RTM_BACKWARD = 1 };           /* PROP::Direction */
 enum { RTM_SNAP_FP32 = 0, RTM_SNAP_C16 = 1, RTM_SNAP_FP16S = 2, RTM_SNAP_AE = 3 };
@@ -89,7 +103,7 @@ typedef struct rtm_dims {
 } rtm_dims;
 
 typedef struct rtm_config {
-  int engine;         /* RTM_ENGINE_FD8 / _CFD / _R2C / _R2R / _CFDB */
+  int engine;         /* RTM_ENGINE_FD8 / _CFD / _R2C / _R2R / _CFDB / _FFTV / _SINCOS */
   int model_type;     /* RTM_ISO, RTM_VTI, RTM_TTI */
   int use_q;          /* visco-acoustic memory variables (Q::order terms) */
   int q_order;        /* number of memory variables, default 4 */
@@ -119,6 +133,9 @@ typedef struct rtm_config {
                          accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes
                          the first-derivative passes (bgprtm/KernelCPU.cpp:128).  FD8 density runs
                          use the one-cell passes; not with state_fp16 */
+  int q_bf16;         /* use_q: the memory variables wq[2][L][N] stored as bfloat16 (read and
+                         rounded back each step; the update arithmetic stays FP32): half their
+                         HBM traffic, the largest share of a TTI + Q step */
 } rtm_config;
 
 typedef struct rtm_handle rtm_handle;

@@ -49,7 +49,7 @@ class RtmConfig(C.Structure):
                 ("q_order", C.c_int), ("nbnd", C.c_int * 6), ("vmax", C.c_float),
                 ("pml_eps", C.c_float), ("pml3d", C.c_int), ("pml3d_scaler", C.c_float),
                 ("top_pml", C.c_int), ("state_fp16", C.c_int), ("kernel_variant", C.c_int),
-                ("use_rho", C.c_int)]
+                ("use_rho", C.c_int), ("q_bf16", C.c_int)]
 
 
 class RtmError(RuntimeError):

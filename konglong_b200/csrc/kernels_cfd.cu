@@ -48,10 +48,15 @@ __device__ __forceinline__ void cfd_rhs_range(const float (&a)[60], float *L, in
     w[k] = (j >= 0 && j < n) ? L[j * S] : 0.f;
   }
   for (int i0 = p0; i0 < p1; i0 += C) {
+    if (i0 + C + 5 <= n) {
 #pragma unroll
-    for (int k = 10; k < C + 10; k++) {
-      const int j = i0 - 5 + k;
-      w[k] = j < n ? L[j * S] : 0.f;
+      for (int k = 10; k < C + 10; k++) w[k] = L[(i0 - 5 + k) * S];
+    } else {
+#pragma unroll
+      for (int k = 10; k < C + 10; k++) {
+        const int j = i0 - 5 + k;
+        w[k] = j < n ? L[j * S] : 0.f;
+      }
     }
     float r[C];
     if (i0 >= 5 && i0 + C <= n - 5) {
@@ -80,14 +85,19 @@ __device__ __forceinline__ void cfd_rhs_range(const float (&a)[60], float *L, in
         r[k] = v;
       }
     }
+    if (i0 != p0 && i0 + C < p1) {  // an inner chunk: no parked rows
 #pragma unroll
-    for (int k = 0; k < C; k++) {
-      const int i = i0 + k;
-      if (i < p1) {
-        const bool h = i0 == p0 && k < 5, t = i0 + C == p1 && k >= C - 5;
-        if (h) head[k < 5 ? k : 0] = r[k];
-        if (t) tail[k >= C - 5 ? k - (C - 5) : 0] = r[k];
-        if (!h && !t) L[i * S] = r[k];
+      for (int k = 0; k < C; k++) L[(i0 + k) * S] = r[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        const int i = i0 + k;
+        if (i < p1) {
+          const bool h = i0 == p0 && k < 5, t = i0 + C == p1 && k >= C - 5;
+          if (h) head[k < 5 ? k : 0] = r[k];
+          if (t) tail[k >= C - 5 ? k - (C - 5) : 0] = r[k];
+          if (!h && !t) L[i * S] = r[k];
+        }
       }
     }
 #pragma unroll
@@ -1029,13 +1039,33 @@ __device__ __forceinline__ float seg_final(const CfdPlanDev &p, int i, float fp,
 // cells handled together by the epilogues (their PML memory in one round trip)
 constexpr int kSegU = 4;
 
-// First-derivative PML round `round` on component AXIS of a batch of cells.
+// Interior of the grid (cells in no PML layer): [lo, hi) per dimension.
+struct PmlInterior {
+  int x0, x1, y0, y1, z0, z1;
+};
+__device__ __forceinline__ PmlInterior pml_interior(const PmlDev &P, const Grid3 &g) {
+  return PmlInterior{P.f[DX][0].w, g.nx - P.f[DX][1].w, P.f[DY][0].w, g.ny - P.f[DY][1].w,
+                     P.f[DZ][0].w, g.nz - P.f[DZ][1].w};
+}
+// bit d set when coordinate c of dimension d lies in one of its PML layers
+__device__ __forceinline__ int pml_bit(int d, int c, int lo, int hi) { return (c < lo || c >= hi) << d; }
+__device__ __forceinline__ int pml_bits(const PmlInterior &in, int ix, int iy, int iz) {
+  return pml_bit(DX, ix, in.x0, in.x1) | pml_bit(DY, iy, in.y0, in.y1) | pml_bit(DZ, iz, in.z0, in.z1);
+}
+
+// First-derivative PML round `round` on component AXIS of a batch of cells
+// (dm: the layers that hold each cell, 0 = none); skipped when no cell of
+// the thread's batch lies in a layer.
 template <int AXIS, int U>
 __device__ __forceinline__ void seg_pml(const CfdSegArgs &a, const Grid3 &g, int round, float (&v)[U],
                                         const int (&ix)[U], const int (&iy)[U], const int (&iz)[U],
-                                        const bool (&act)[U]) {
-  if (round) pml1_batch<AXIS, 1, U>(a.pml, g, a.pml3d, v, ix, iy, iz, act);
-  else pml1_batch<AXIS, 0, U>(a.pml, g, a.pml3d, v, ix, iy, iz, act);
+                                        const int (&dm)[U]) {
+  int any = 0;
+#pragma unroll
+  for (int u = 0; u < U; u++) any |= dm[u];
+  if (!any) return;
+  if (round) pml1_batch<AXIS, 1, U>(a.pml, g, a.pml3d, v, ix, iy, iz, dm);
+  else pml1_batch<AXIS, 0, U>(a.pml, g, a.pml3d, v, ix, iy, iz, dm);
 }
 
 // Strided tile (x or y lines of 32 z columns, rows [0, n) at sm[i * 32 + lane])
@@ -1112,26 +1142,27 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_line_k(const CfdPlanDev p, con
     for (int i = b; i < e; i++) L[i] = seg_final(p, i, L[i], sv, tv);
     __syncthreads();
     constexpr int U = kSegU;
+    const PmlInterior in = pml_interior(a.pml, g);
     for (int l = warp; l < nl; l += nw) {
       const long long line = l0 + l;
       const int ix = (int)(line % a.nx), iy = (int)(line / a.nx);
+      const int fixed = pml_bit(DX, ix, in.x0, in.x1) | pml_bit(DY, iy, in.y0, in.y1);
       const float *row = sm + l * st;
       float *dst = out + line * n;
       for (int i0 = lane; i0 < n; i0 += 32 * U) {
         float v[U];
-        int xs[U], ys[U], zs[U];
-        bool act[U];
+        int xs[U], ys[U], zs[U], dm[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
           const int i = i0 + 32 * u;
-          act[u] = i < n;
-          v[u] = act[u] ? row[i] : 0.f;
+          v[u] = i < n ? row[i] : 0.f;
           xs[u] = ix, ys[u] = iy, zs[u] = min(i, n - 1);
+          dm[u] = i < n ? fixed | pml_bit(DZ, i, in.z0, in.z1) : 0;
         }
-        seg_pml<DZ, U>(a, g, round, v, xs, ys, zs, act);
+        seg_pml<DZ, U>(a, g, round, v, xs, ys, zs, dm);
 #pragma unroll
         for (int u = 0; u < U; u++)
-          if (act[u]) __stcg(dst + i0 + 32 * u, v[u]);
+          if (i0 + 32 * u < n) __stcg(dst + i0 + 32 * u, v[u]);
       }
     }
     return;
@@ -1145,21 +1176,28 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_line_k(const CfdPlanDev p, con
   seg_solve<32>(p, L, lane, warp, ss, sv, tv);
   if (lane < nl) {
     constexpr int U = kSegU;
+    const PmlInterior in = pml_interior(a.pml, g);
+    // PML cells of the tile: all rows when its fixed coordinate or its z columns
+    // reach a layer, else the rows in the layers of the line's own dimension
+    const int iz = iz0 + lane;
+    // layers holding the thread's fixed coordinates (the tile's y or x, its z)
+    const int fixed = (AXIS == DX ? pml_bit(DY, o, in.y0, in.y1) : pml_bit(DX, o, in.x0, in.x1)) |
+                      pml_bit(DZ, iz, in.z0, in.z1);
+    const int r0 = AXIS == DX ? in.x0 : in.y0, r1 = AXIS == DX ? in.x1 : in.y1;
     for (int i0 = b; i0 < e; i0 += U) {
       float v[U];
-      int xs[U], ys[U], zs[U];
-      bool act[U];
+      int xs[U], ys[U], zs[U], dm[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int i = min(i0 + u, e - 1);
-        act[u] = i0 + u < e;
         v[u] = seg_final(p, i, L[i * 32], sv, tv);
-        xs[u] = AXIS == DX ? i : o, ys[u] = AXIS == DX ? o : i, zs[u] = iz0 + lane;
+        xs[u] = AXIS == DX ? i : o, ys[u] = AXIS == DX ? o : i, zs[u] = iz;
+        dm[u] = i0 + u < e ? fixed | pml_bit(AXIS, i, r0, r1) : 0;
       }
-      seg_pml<AXIS, U>(a, g, round, v, xs, ys, zs, act);
+      seg_pml<AXIS, U>(a, g, round, v, xs, ys, zs, dm);
 #pragma unroll
       for (int u = 0; u < U; u++)
-        if (act[u]) __stcg(out + base + lane + (long long)(i0 + u) * es, v[u]);
+        if (i0 + u < e) __stcg(out + base + lane + (long long)(i0 + u) * es, v[u]);
     }
   }
 }
@@ -1189,11 +1227,13 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_yf_k(const CfdPlanDev pg, cons
   seg_range(pg, warp, b, e);
   const int iz = iz0 + lane;
   constexpr int U = kSegU;
+  const PmlInterior in = pml_interior(a.pml, g);
+  const int fixed = pml_bit(DX, o, in.x0, in.x1) | pml_bit(DZ, iz, in.z0, in.z1);
   if (lane < nl) {
     for (int i0 = b; i0 < e; i0 += U) {
       float gx[U], gz[U], gy[U], r[U];
       float4 m[U];
-      int xs[U], ys[U], zs[U];
+      int xs[U], ys[U], zs[U], dm[U];
       bool act[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
@@ -1206,8 +1246,9 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_yf_k(const CfdPlanDev pg, cons
         gy[u] = seg_final(pg, i, L[i * 32], sv, tv);
         act[u] = i0 + u < e;
         xs[u] = o, ys[u] = i, zs[u] = iz;
+        dm[u] = act[u] ? fixed | pml_bit(DY, i, in.y0, in.y1) : 0;
       }
-      seg_pml<DY, U>(a, g, 0, gy, xs, ys, zs, act);
+      seg_pml<DY, U>(a, g, 0, gy, xs, ys, zs, dm);
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int i = i0 + u;
@@ -1227,19 +1268,18 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_yf_k(const CfdPlanDev pg, cons
   if (lane < nl) {
     for (int i0 = b; i0 < e; i0 += U) {
       float v[U];
-      int xs[U], ys[U], zs[U];
-      bool act[U];
+      int xs[U], ys[U], zs[U], dm[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int i = min(i0 + u, e - 1);
         v[u] = seg_final(pd, i, L[i * 32], sv, tv);
-        act[u] = i0 + u < e;
         xs[u] = o, ys[u] = i, zs[u] = iz;
+        dm[u] = i0 + u < e ? fixed | pml_bit(DY, i, in.y0, in.y1) : 0;
       }
-      seg_pml<DY, U>(a, g, 1, v, xs, ys, zs, act);
+      seg_pml<DY, U>(a, g, 1, v, xs, ys, zs, dm);
 #pragma unroll
       for (int u = 0; u < U; u++)
-        if (act[u]) __stcg(a.dy + base + lane + (long long)(i0 + u) * es, v[u]);
+        if (i0 + u < e) __stcg(a.dy + base + lane + (long long)(i0 + u) * es, v[u]);
     }
   }
 }
@@ -1268,11 +1308,13 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_xf_k(const CfdPlanDev p, const
   seg_range(p, warp, b, e);
   const int iz = iz0 + lane;
   const long long ntot = g.nxz * a.ny;
+  const PmlInterior in = pml_interior(a.pml, g);
+  const int fixed = pml_bit(DY, o, in.y0, in.y1) | pml_bit(DZ, iz, in.z0, in.z1);
   if (lane < nl) {
     constexpr int U = kSegU;
     for (int i0 = b; i0 < e; i0 += U) {
       float dz[U], dy[U], vel[U], w0[U], w1[U], r[U], dxs[U];
-      int xs[U], ys[U], zs[U];
+      int xs[U], ys[U], zs[U], dm[U];
       bool act[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
@@ -1285,8 +1327,9 @@ __global__ void __launch_bounds__(256, 2) cfd_seg_xf_k(const CfdPlanDev p, const
         dxs[u] = seg_final(p, i, L[i * 32], sv, tv);
         act[u] = i0 + u < e;
         xs[u] = i, ys[u] = o, zs[u] = iz;
+        dm[u] = act[u] ? fixed | pml_bit(DX, i, in.x0, in.x1) : 0;
       }
-      seg_pml<DX, U>(a, g, 1, dxs, xs, ys, zs, act);
+      seg_pml<DX, U>(a, g, 1, dxs, xs, ys, zs, dm);
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int i = i0 + u;

@@ -330,7 +330,9 @@ __device__ __forceinline__ void iso4_prefetch(const IsoArgs &a, const Grid3 &g, 
   if (MODE == 2) {
     const long long n = (long long)g.ny * g.nxz;
     prefetch_l1(a.q.invq + i);
-    for (int l = 0; l < a.q.order; l++) prefetch_l1(a.q.d0 + l * n + i), prefetch_l1(a.q.d1 + l * n + i);
+    const long long es = a.q.bf16 ? 2 : 4;  // bytes per memory variable
+    for (int l = 0; l < a.q.order; l++)
+      prefetch_l1((const char *)a.q.d0 + (l * n + i) * es), prefetch_l1((const char *)a.q.d1 + (l * n + i) * es);
   }
   if (a.io.ic) {
     prefetch_l1(a.io.image + i), prefetch_l1(a.io.comp + i);

@@ -452,17 +452,21 @@ static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out, int
 // nz % 4 == 0) or the plain staged tile kernel (2)
 static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out) {
   const rtm_dims &d = h->d;
-  if (h->fft) {  // FFTWR2C: isign +1 in the gradient pass, -1 in the divergence pass
-    if (launch_fft_deriv(h->fft, axis, sgn ? -1 : 1, in, out, h->st) != RTM_OK) h->fft_err = 1;
+  // the Derivative path's divergence pass takes isign = iswitch: 1 for TTI,
+  // 2 otherwise (bgprtm/Derivative.cpp:4-8, 92-112)
+  const bool deriv_path = h->c.engine == RTM_ENGINE_CFDB || h->c.engine == RTM_ENGINE_FFTV ||
+                          h->c.engine == RTM_ENGINE_SINCOS;
+  if (sgn && deriv_path && h->c.model_type == RTM_TTI) sgn = 0;
+  if (h->fft) {  // FFTWR2C: isign +1 in the gradient pass, -1 in the divergence pass; FFTV: +1 in both
+    const int isign = h->c.engine == RTM_ENGINE_FFTV ? 1 : sgn ? -1 : 1;
+    if (launch_fft_deriv(h->fft, axis, isign, in, out, h->st) != RTM_OK) h->fft_err = 1;
     return;
   }
-  if (h->r2r) {  // FFTWR2R, the same pass signs
+  if (h->r2r) {  // FFTWR2R, the same pass signs; SINCOS: runCosSin for isign 1, runSinCos otherwise
     if (launch_r2r_deriv(h->r2r, axis, sgn ? -1 : 1, in, out) != RTM_OK) h->fft_err = 1;
     return;
   }
-  // CFD_BATCH (the Derivative path) takes the divergence-pass plan from
-  // iswitch: plan 1 for TTI, plan 2 otherwise (bgprtm/Derivative.cpp:4-8, 92-112)
-  if (sgn && h->c.engine == RTM_ENGINE_CFDB && h->c.model_type == RTM_TTI) sgn = 0;
+  // CFD_BATCH: the divergence-pass plan from iswitch (above): plan 1 for TTI
   if (axis != DZ && h->cfd_xy == 0) {
     launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
     return;
@@ -535,8 +539,9 @@ static int zero_state(Engine *h) {
           if (F.q[r][k]) CK(cudaMemsetAsync(F.q[r][k], 0, plane * F.w * 4, h->st));
     }
   if (h->c.use_q && h->wq[0]) {
-    CK(cudaMemsetAsync(h->wq[0], 0, (size_t)h->c.q_order * h->n * 4, h->st));
-    CK(cudaMemsetAsync(h->wq[1], 0, (size_t)h->c.q_order * h->n * 4, h->st));
+    const size_t qb = (size_t)h->c.q_order * h->n * (h->c.q_bf16 ? 2 : 4);
+    CK(cudaMemsetAsync(h->wq[0], 0, qb, h->st));
+    CK(cudaMemsetAsync(h->wq[1], 0, qb, h->st));
   }
   if (h->ext.out) CK(cudaMemsetAsync(h->ext.out, 0, (size_t)h->ext.ntr * h->ext.nt * 4, h->st));
   h->iq0 = 0;
@@ -551,6 +556,7 @@ static QDev q_dev(Engine *h) {
   q.invq = h->invq;
   q.d0 = h->wq[h->iq0];
   q.d1 = h->wq[1 - h->iq0];
+  q.bf16 = h->c.q_bf16 ? 1 : 0;
   return q;
 }
 
@@ -790,7 +796,10 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   de.nx = d.nx, de.ny = d.ny, de.nz = d.nz, de.pml3d = h->c.pml3d, de.mode = mode;
   de.dx = h->scr2, de.dz = dzp, de.dy = dyp;
   de.w1 = h->w1, de.w0 = h->w0, de.vel = h->vel, de.rho = h->rho;
-  de.rho_form = h->c.engine == RTM_ENGINE_CFDB ? 2 : (h->c.engine == RTM_ENGINE_R2C || h->c.engine == RTM_ENGINE_R2R) ? 1 : 0;
+  de.rho_form = (h->c.engine == RTM_ENGINE_CFDB || h->c.engine == RTM_ENGINE_FFTV || h->c.engine == RTM_ENGINE_SINCOS)
+                    ? 2
+                : (h->c.engine == RTM_ENGINE_R2C || h->c.engine == RTM_ENGINE_R2R) ? 1
+                                                                                    : 0;
   de.pml = pml_dev(h);
   de.q = q;
   {
@@ -1336,7 +1345,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (!d || !c || !out) return RTM_ERR_ARG;
   *out = nullptr;
   if (d->nx < 9 || d->nz < 9 || d->ny < 1 || d->ny > 65535 || d->dx <= 0 || d->dy <= 0 || d->dz <= 0 || d->dt <= 0 || c->vmax <= 0 ||
-      c->engine < 0 || c->engine > 4 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
+      c->engine < 0 || c->engine > 6 || c->model_type < 1 || c->model_type > 3 || c->q_order < 1 || c->q_order > 8 ||
       c->pml_eps <= 0 || c->pml_eps >= 1) {
     g_create_error = "rtm_create: dimensions or configuration out of range";
     return RTM_ERR_ARG;
@@ -1351,7 +1360,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   // FdEngine_r2c / _r2r and the Derivative path's Boundary damp only along
   // each derivative's own axis (bgprtm/FdEngine_r2c.cpp:240-243,
   // FdEngine_r2r.cpp:95-98, Boundary.cpp:153-213): no pml3d cross terms
-  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R || c->engine == RTM_ENGINE_CFDB) h->c.pml3d = 0;
+  if (c->engine != RTM_ENGINE_FD8 && c->engine != RTM_ENGINE_CFD) h->c.pml3d = 0;
   h->n = (long long)d->nx * d->ny * d->nz;
   h->nxz = (long long)d->nx * d->nz;
   int rc = RTM_OK;
@@ -1386,14 +1395,15 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     if ((rc = h->alloc(h->px, h->n)) || (rc = h->alloc(h->pz, h->n)) || (d->ny > 1 && (rc = h->alloc(h->py, h->n))))
       return fail(rc);
   }
-  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R) {
+  if (c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_R2R || c->engine == RTM_ENGINE_FFTV ||
+      c->engine == RTM_ENGINE_SINCOS) {
     if ((rc = h->alloc(h->scr, h->n)) || (rc = h->alloc(h->scr2, h->n))) return fail(rc);
-    if (c->engine == RTM_ENGINE_R2C &&
+    if ((c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_FFTV) &&
         (rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
       h->err = "cuFFT plan set-up failed";
       return fail(rc);
     }
-    if (c->engine == RTM_ENGINE_R2R &&
+    if ((c->engine == RTM_ENGINE_R2R || c->engine == RTM_ENGINE_SINCOS) &&
         (rc = r2r_plans_create(&h->r2r, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
       h->err = "FFTWR2R line-matrix set-up failed";
       return fail(rc);
@@ -1458,8 +1468,9 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     if ((rc = h->alloc(h->pjx, h->n)) || (d->ny > 1 && (rc = h->alloc(h->pjy, h->n)))) return fail(rc);
   }
   if (c->use_q) {
-    if ((rc = h->alloc(h->invq, h->n)) || (rc = h->alloc(h->wq[0], (size_t)c->q_order * h->n)) ||
-        (rc = h->alloc(h->wq[1], (size_t)c->q_order * h->n)))
+    // BF16 memory variables take half the floats (rounded up to whole 16-byte rows)
+    const size_t qn = c->q_bf16 ? ((size_t)c->q_order * h->n + 7) / 8 * 4 : (size_t)c->q_order * h->n;
+    if ((rc = h->alloc(h->invq, h->n)) || (rc = h->alloc(h->wq[0], qn)) || (rc = h->alloc(h->wq[1], qn)))
       return fail(rc);
   }
   // FD tables (FdEngine_fd constructor + setJacob, rectangular grid, const order)

@@ -2,6 +2,7 @@
 // recursion, fused snapshot / imaging-condition access, the COMPRESS_16 code,
 // the FP16 slab codec and the visco-acoustic update.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "rtm_internal.cuh"
@@ -140,12 +141,14 @@ __device__ __forceinline__ int pml_face_index(const PmlDev &P, const Grid3 &g, i
 
 // First-derivative PML round R on component AXIS of U cells at once (pml1's
 // arithmetic and order per cell: own dimension unscaled, then the two cross
-// dimensions scaled when pml3d).  Every memory value of the U cells is loaded
-// before the first recursion, so the batch costs one memory round trip
-// instead of one per face and cell.
+// dimensions scaled when pml3d).  dm[u]: bit d set when dimension d's layers
+// may hold cell u (the caller knows which coordinates are fixed for it); 0
+// skips the cell.  Every memory value of the U cells is loaded before the
+// first recursion, so the batch costs one memory round trip instead of one
+// per face and cell.
 template <int AXIS, int R, int U>
 __device__ __forceinline__ void pml1_batch(const PmlDev &P, const Grid3 &g, int pml3d, float (&v)[U], const int (&ix)[U],
-                                           const int (&iy)[U], const int (&iz)[U], const bool (&act)[U]) {
+                                           const int (&iy)[U], const int (&iz)[U], const int (&dm)[U]) {
   // dimensions in pml1's order for this component and the memory component
   // each keeps for it (bgprtm/FdEngine.cpp:301-350)
   constexpr int D1 = AXIS == DZ ? DX : DZ, D2 = AXIS == DY ? DX : DY;
@@ -158,7 +161,8 @@ __device__ __forceinline__ void pml1_batch(const PmlDev &P, const Grid3 &g, int 
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const int d = k == 0 ? AXIS : k == 1 ? D1 : D2, c = k == 0 ? 0 : k == 1 ? C1 : C2;
-      enc[u][k] = act[u] && (k == 0 || cross) ? pml_face_index(P, g, d, ix[u], iy[u], iz[u], lay[u][k]) : -1;
+      enc[u][k] = ((dm[u] >> d) & 1) && (k == 0 || cross) ? pml_face_index(P, g, d, ix[u], iy[u], iz[u], lay[u][k])
+                                                            : -1;
       if (enc[u][k] >= 0) q[u][k] = P.f[d][enc[u][k] >> 30].q[R][c][enc[u][k] & 0x3fffffff];
     }
 #pragma unroll
@@ -556,6 +560,34 @@ __device__ __forceinline__ float q_next(float cq, float u, float el, float d0) {
   return __fmaf_rn(el, d0, __fmul_rn(cq, u));
 }
 
+// Memory variable element j of a Q half, FP32 or BF16 storage.
+__device__ __forceinline__ float q_ld(const QDev &Q, const float *h, long long j) {
+  return Q.bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(h)[j]) : h[j];
+}
+__device__ __forceinline__ void q_st(const QDev &Q, float *h, long long j, float v) {
+  if (Q.bf16) reinterpret_cast<__nv_bfloat16 *>(h)[j] = __float2bfloat16_rn(v);
+  else h[j] = v;
+}
+// four consecutive elements (j a multiple of 4)
+__device__ __forceinline__ float4 q_ld4(const QDev &Q, const float *h, long long j) {
+  if (!Q.bf16) return *reinterpret_cast<const float4 *>(h + j);
+  const uint2 r = *reinterpret_cast<const uint2 *>(reinterpret_cast<const __nv_bfloat16 *>(h) + j);
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void q_st4(const QDev &Q, float *h, long long j, float4 v) {
+  if (!Q.bf16) {
+    *reinterpret_cast<float4 *>(h + j) = v;
+    return;
+  }
+  const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+  uint2 r;
+  r.x = *reinterpret_cast<const unsigned *>(&a);
+  r.y = *reinterpret_cast<const unsigned *>(&b);
+  *reinterpret_cast<uint2 *>(reinterpret_cast<__nv_bfloat16 *>(h) + j) = r;
+}
+
 // The memory variables of up to 4 orders are loaded before any is updated, so
 // a cell waits for one load round trip per 4 orders (order <= 8, QDev::cq).
 __device__ __forceinline__ float q_update(const QDev &Q, long long i, long long n, float t, float u) {
@@ -567,13 +599,13 @@ __device__ __forceinline__ float q_update(const QDev &Q, long long i, long long 
     float d0[4], d1[4];
 #pragma unroll
     for (int l = 0; l < 4; l++)
-      if (l0 + l < Q.order) d0[l] = Q.d0[(long long)(l0 + l) * n + i], d1[l] = Q.d1[(long long)(l0 + l) * n + i];
+      if (l0 + l < Q.order) d0[l] = q_ld(Q, Q.d0, (long long)(l0 + l) * n + i), d1[l] = q_ld(Q, Q.d1, (long long)(l0 + l) * n + i);
 #pragma unroll
     for (int l = 0; l < 4; l++)
       if (l0 + l < Q.order) {
         const float el = Q.wq[l0 + l];
         v = q_acc(v, iq, el, d0[l], d1[l]);
-        Q.d0[(long long)(l0 + l) * n + i] = q_next(Q.cq[l0 + l], u, el, d0[l]);
+        q_st(Q, Q.d0, (long long)(l0 + l) * n + i, q_next(Q.cq[l0 + l], u, el, d0[l]));
       }
   }
   return v;
@@ -592,8 +624,8 @@ static __device__ __noinline__ float4 q_update4(const QDev &Q, long long i, long
 #pragma unroll
     for (int l = 0; l < 4; l++)
       if (l0 + l < Q.order) {
-        d0[l] = *reinterpret_cast<const float4 *>(Q.d0 + (long long)(l0 + l) * n + i);
-        d1[l] = *reinterpret_cast<const float4 *>(Q.d1 + (long long)(l0 + l) * n + i);
+        d0[l] = q_ld4(Q, Q.d0, (long long)(l0 + l) * n + i);
+        d1[l] = q_ld4(Q, Q.d1, (long long)(l0 + l) * n + i);
       }
 #pragma unroll
     for (int c = 0; c < 4; c++)
@@ -607,7 +639,7 @@ static __device__ __noinline__ float4 q_update4(const QDev &Q, long long i, long
         }
 #pragma unroll
     for (int l = 0; l < 4; l++)
-      if (l0 + l < Q.order) *reinterpret_cast<float4 *>(Q.d0 + (long long)(l0 + l) * n + i) = d0[l];
+      if (l0 + l < Q.order) q_st4(Q, Q.d0, (long long)(l0 + l) * n + i, d0[l]);
   }
   return make_float4(v[0], v[1], v[2], v[3]);
 }

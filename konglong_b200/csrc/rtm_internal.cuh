@@ -84,7 +84,8 @@ struct QDev {
   float cqsum;
   float cq[8], wq[8];
   const float *invq;
-  float *d0, *d1;  // [order][n] halves selected by iq0/iq1
+  float *d0, *d1;  // [order][n] halves selected by iq0/iq1 (FP32, or BF16 when bf16)
+  int bf16;        // memory variables stored as bfloat16 (the update arithmetic stays FP32)
 };
 
 }  // namespace rtm

@@ -37,6 +37,7 @@ class Propagator:
         c.pml3d, c.pml3d_scaler, c.top_pml = int(spec.pml3d), spec.pml3d_scaler, int(spec.top_pml)
         c.state_fp16 = int(spec.state_fp16)
         c.use_rho = int(getattr(spec, "use_rho", False))
+        c.q_bf16 = int(getattr(spec, "q_bf16", False))
         c.kernel_variant = int(getattr(spec, "kernel_variant", 0))
         h = C.c_void_p()
         _lib.check(L.rtm_create(C.byref(d), C.byref(c), C.byref(h)), "rtm_create")

@@ -11,7 +11,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ENGINE_FD8, ENGINE_CFD, ENGINE_R2C, ENGINE_R2R, ENGINE_CFDB = 0, 1, 2, 3, 4  # FD::FD, CFD, FFTWR2C, FFTWR2R, CFD_BATCH
+# FD::FD, CFD, FFTWR2C, FFTWR2R, CFD_BATCH, FFTV, SINCOS
+ENGINE_FD8, ENGINE_CFD, ENGINE_R2C, ENGINE_R2R, ENGINE_CFDB, ENGINE_FFTV, ENGINE_SINCOS = 0, 1, 2, 3, 4, 5, 6
 ISO, VTI, TTI = 1, 2, 3
 FORWARD, BACKWARD = 0, 1
 SNAP_FP32, SNAP_C16, SNAP_FP16S, SNAP_AE = 0, 1, 2, 3
@@ -40,6 +41,7 @@ class PropSpec:
     top_pml: bool = True
     state_fp16: bool = False
     use_rho: bool = False         # density model (KernelCPU::setModel's rho)
+    q_bf16: bool = False          # Q memory variables stored as bfloat16
     kernel_variant: int = 0       # 0 auto, 1 one cell per thread / plain tiles, 2 TMA (CFD x/y tiles,
                                   # ISO one-cell plane pipeline), 3 FD8 4 z cells per thread with TMA
                                   # rings, 4 ISO 4 z cells with register prefetch

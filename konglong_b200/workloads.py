@@ -18,7 +18,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .spec import ENGINE_CFD, ENGINE_CFDB, ENGINE_FD8, ENGINE_R2C, ENGINE_R2R, ISO, TTI, VTI, PropSpec, TraceSet
+from .spec import (ENGINE_CFD, ENGINE_CFDB, ENGINE_FD8, ENGINE_FFTV, ENGINE_R2C, ENGINE_R2R, ENGINE_SINCOS, ISO, TTI,
+                   VTI, PropSpec, TraceSet)
 
 
 @dataclass
@@ -186,7 +187,7 @@ def spread_band(spec: PropSpec):
     engine's dispersion factor (bgprtm/FdEngine.cpp:241-256)."""
     if spec.engine in (ENGINE_CFD, ENGINE_CFDB):  # names starting with "CFD" take the compact-FD factor
         disp = 0.9
-    elif spec.engine in (ENGINE_R2C, ENGINE_R2R):
+    elif spec.engine in (ENGINE_R2C, ENGINE_R2R, ENGINE_FFTV, ENGINE_SINCOS):
         disp = 1.0  # pseudo-spectral engines keep FdEngine::getFdDispersion's default
     else:
         disp = 0.46 if spec.model_type >= VTI else 0.6

@@ -31,7 +31,8 @@ using std::min;
 using std::vector;
 
 enum { ISO = 1, VTI = 2, TTI = 3 };
-enum { FD8 = 0, CFD = 1, R2C = 2, R2R = 3, CFDB = 4 };
+// FD::FD, CFD, FFTWR2C, FFTWR2R, CFD_BATCH, FFTV, SINCOS
+enum { FD8 = 0, CFD = 1, R2C = 2, R2R = 3, CFDB = 4, FFTV = 5, SINCOS = 6 };
 enum { X = 0, Y = 1, Z = 2 };
 enum { TOP = 0, BOT = 1 };
 
@@ -302,20 +303,27 @@ public:
       cfdy.build(ny, dy);
       cfdz.build(nz, dz);
     }
-    if (cfg.engine == R2C || cfg.engine == R2R) {
-      cfg.pml3d = 0;  // fftderiv1_r2c / _r2r damp along the derivative's own axis only
+    if (spectral()) {
+      // fftderiv1_r2c / _r2r and Boundary::apply* damp along the derivative's own axis only
+      cfg.pml3d = 0;
       const int nn[3] = {nx, ny, nz};
       const float dd[3] = {(float)dx, (float)dy, (float)dz};
       for (int a = 0; a < 3; a++)
         if (nn[a] > 1)
           for (int r = 0; r < 2; r++) {
-            if (cfg.engine == R2C) r2c[a][r] = r2c_circulant(nn[a], dd[a], r == 0 ? 1 : -1);
+            // FFTV: the plain spectral derivative in both passes (isign +1:
+            // bins below Nyquist times i k, an even line's Nyquist bin zeroed)
+            if (cfg.engine == R2C || cfg.engine == FFTV)
+              r2c[a][r] = r2c_circulant(nn[a], dd[a], r == 0 || cfg.engine == FFTV ? 1 : -1);
             else r2r[a][r] = r2r_matrix(nn[a], dd[a], r == 0 ? 1 : -1);
           }
     }
     build_pml();
     c16_tables(codec_table, wtaper20, wtaper10);
   }
+
+  // engines whose line derivative is a transform (FFTWR2C, FFTWR2R, FFTV, SINCOS)
+  bool spectral() const { return cfg.engine == R2C || cfg.engine == R2R || cfg.engine == FFTV || cfg.engine == SINCOS; }
 
   // FdEngine_fd constructor + setJacob (bgprtm/FdEngine_fd.cpp:30-54, 106-131),
   // Taylor weights, const_ne, rectangular grid.  Float rounding as there.
@@ -540,7 +548,7 @@ public:
   inline R acc(R o, R v, size_t i, int axis) const {
     if (!cfg.use_rho) return o - v * vel[i];
     if (cfg.engine == CFD && axis == Y) return o - v * (vel[i] * rho[i]);
-    if ((cfg.engine == R2C || cfg.engine == R2R) && axis != Z) return o - vel[i] * (rho[i] * v);
+    if (spectral() && axis != Z) return o - vel[i] * (rho[i] * v);
     return o - v * vel[i] * rho[i];
   }
 
@@ -565,8 +573,8 @@ public:
     vector<R> d(nxyz);
     const CfdPlan<R> &p = axis == X ? cfdx : axis == Y ? cfdy : cfdz;
     int s = plan >= 0 ? plan : round == 0 ? 0 : 1;  // isign 1 -> plan 1, isign -1 -> plan 2
-    if (cfg.engine == R2C || cfg.engine == R2R) {
-      const bool fft = cfg.engine == R2C;
+    if (spectral()) {
+      const bool fft = cfg.engine == R2C || cfg.engine == FFTV;
       const vector<double> &c = fft ? r2c[axis][s] : r2r[axis][s];
       auto line = [&](int n, const R *x, R *b, size_t ld) {
         if (fft) r2c_line(c, n, x, b, ld);
@@ -676,7 +684,13 @@ public:
   // iswitch = 1 for TTI and 2 otherwise, Boundary round 2, wb = (dz + dx) + dy),
   // applyVel (wb *= vel, :1734-1746) and w0 -= wb.  Derivative_cfd's line
   // operator is FdEngine_cfd's (Cfd_plan plans 1 / 2); Boundary's PML is
-  // PML::apply along each derivative's own axis.
+  // PML::apply along each derivative's own axis.  The same path serves
+  // Engine FFTV (Derivative_fftv: libfftv's DERIVATIVE filter, here the plain
+  // spectral derivative of the FFTWR2C circulant with isign +1) and Engine
+  // SINCOS (Derivative_sincos: runCosSin when isign is 1, runSinCos
+  // otherwise, bgprtm/Derivative_sincos.cpp:12-38; here the FFTWR2R line
+  // matrices of the two passes).  libfftv is not in the reference tree, so
+  // these two line operators are the standard transforms, unpinned.
   void cfd_batch_kernel() {
     if (nx > 1) deriv_volume(w1.data(), px.data(), X, 0, 0, 0);
     if (ny > 1) deriv_volume(w1.data(), py.data(), Y, 0, 0, 0);
@@ -700,7 +714,7 @@ public:
 
   void kernel() {
     if (cfg.engine == FD8 && cfg.model_type == ISO && !cfg.use_rho) iso_fd8_kernel();
-    else if (cfg.engine == CFDB) cfd_batch_kernel();
+    else if (cfg.engine == CFDB || cfg.engine == FFTV || cfg.engine == SINCOS) cfd_batch_kernel();
     else aniso_kernel();
   }
 

@@ -126,6 +126,47 @@ def test_learned_snapshots_in_rtm(data):
     deep = rel_l2(imgs[SNAP_AE][:, :, z0:], ref[:, :, z0:])
     full = rel_l2(imgs[SNAP_AE], ref)
     print(f"learned-snapshot image NRMSE vs FP32 store: full {full:.3f}, below z={z0}: {deep:.3f}")
-    # measured: full 0.96, below the mute 0.51 (the 16:1 code does not hold the
-    # near-source blocks, which carry most of the energy); regression bounds
-    assert full < 1.2 and deep < 0.7
+    # measured: full 0.96, below the mute 0.46-0.51 (the 16:1 code does not hold
+    # the near-source blocks, which carry most of the energy); the learned code
+    # alone is not the product form: it runs with the FP16 fallback (above, and
+    # the ablation below)
+    assert full < 1.0 and deep < 0.7
+
+
+def test_ablation_at_equal_bytes(data):
+    """What the trained network adds at the same bytes per block: every code
+    below keeps the same FP16 copies of the 5 % highest-energy blocks and
+    spends 32 floats + the block scale on each other block.  The residual
+    error of a held-out snapshot (a compact-FD VTI forward wavefield of a model
+    not trained on) with: the trained code; the same network untrained; the
+    16:1 2^3-average code; no code (those blocks zero)."""
+    train, _ = data
+    ae = AE.AutoEncoder(seed=5)
+    raw = AE.AutoEncoder(seed=5)
+    ae.fit(train, steps=1500, batch=256, lr=3e-3)
+    sh = W.vti_cfd(scale=0.2, seed=11, nt=400)
+    s = sh.spec
+    m = Propagator(s)
+    m.set_model(**sh.model_arrays())
+    k1, k2 = W.spread_band(s)
+    m.set_injection(W.make_traceset([sh.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs),
+                    sh.wavelet[None, :], s.dt_dxyz)
+    m.reset()
+    m.modelling(300, -1, 1)
+    w = np.ascontiguousarray(m.get(FIELD_W0).reshape(s.shape))
+    m.close()
+    b, sc = AE.volume_to_blocks(w)
+    sel = AE.fallback_selection(sc, 1e-3, 0.05)
+    codes = {"trained": ae.reconstruct(b)[0], "untrained": raw.reconstruct(b)[0],
+             "naive 16:1": AE.naive_16to1(b), "zero": np.zeros_like(b)}
+    err = {k: rel_l2(AE.apply_fallback(AE.blocks_to_volume(v, sc, s.shape), w, sc, sel), w) for k, v in codes.items()}
+    print("held-out snapshot NRMSE with the 5 % FP16 fallback: " + ", ".join(f"{k} {v:.2e}" for k, v in err.items()))
+    # measured: trained 0.59, untrained 0.73, naive 16:1 0.15, zero 0.73.  Training
+    # helps, but at equal bytes the 2^3-average code (64 FP16 values per block)
+    # beats the 32-float latent on these band-limited wavefields: the learned
+    # code does not earn its place over it.  Bounds: the trained network must
+    # beat no code and the untrained network; the ordering against the naive
+    # code is recorded as it stands.
+    assert err["trained"] < 0.9 * err["untrained"]
+    assert err["trained"] < 0.9 * err["zero"]
+    assert err["naive 16:1"] < err["trained"]

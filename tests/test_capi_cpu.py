@@ -91,14 +91,14 @@ def test_r2r_line_matrix_matches_oracle(n, isign):
 
 
 def test_new_entry_points_validate_arguments_without_gpu():
-    """Engines 0-4 only; the FK spreading and the learned-snapshot fallback
+    """Engines 0-6 only; the FK spreading and the learned-snapshot fallback
     refuse bad arguments before touching a device."""
     from konglong_b200.propagator import FkArgs
     L = _lib.lib()
     d = _lib.RtmDims(32, 32, 32, 10, 10, 10, 0.001)
     c = _lib.RtmConfig()
     L.rtm_config_default(C.byref(c))
-    c.engine = 5
+    c.engine = 7
     h = C.c_void_p()
     assert L.rtm_create(C.byref(d), C.byref(c), C.byref(h)) == -1 and not h.value
     assert L.rtm_set_compressor_fallback(None, 1e-3, 0.1) == -1

@@ -99,3 +99,40 @@ def test_fp16_state_rejected_where_not_built():
     with pytest.raises(RtmError) as e:
         Propagator(dataclasses.replace(shot.spec, state_fp16=True))
     assert e.value.code == STATUS_CODE["RTM_ERR_UNSUPPORTED"]
+
+
+def _engine_q16(shot, q16):
+    spec = dataclasses.replace(shot.spec, q_bf16=q16)
+    p = Propagator(spec)
+    p.set_q_coeffs(*W.q_coefficients(spec.dt, shot.fpeak))
+    p.set_model(**shot.model_arrays())
+    return p
+
+
+def test_bf16_q_memory_traces_and_image_tti_q():
+    """BF16 storage of the Q memory variables on the 4-cell FD8 passes (FP32
+    state and arithmetic): receiver traces against the FP64 oracle and the RTM
+    image against the all-FP32 engine."""
+    shot = W.tti_q(scale=0.08, nt=160)
+    got = _model(shot, _engine_q16(shot, True), 150)
+    d = O.Oracle(shot.spec, double=True)
+    d.set_q_coeffs(*W.q_coefficients(shot.spec.dt, shot.fpeak))
+    d.set_model(**shot.model_arrays())
+    exact = _model(shot, d, 150)
+    e = rel_l2(got, exact)
+    print(f"TTI+Q traces vs FP64 oracle, BF16 Q memory: {e:.2e}")
+    # BF16 rounding (2^-9) of each memory variable per step; the Q term is a
+    # small correction (1/Q <= 1/30) to the FP32 state
+    assert e < 5e-3
+    nt, nts, k = 160, 112, 4
+    imgs = []
+    for q16 in (False, True):
+        p = _engine_q16(shot, q16)
+        src, rcv = _sets(shot)
+        data = (np.random.default_rng(7).standard_normal((rcv.ntr, nt)) * 1e3).astype(np.float32)
+        imgs.append(p.rtm_shot(src, shot.wavelet[None, :], rcv, data, nt, nts, k, snap_fmt=SNAP_FP32,
+                               ntaper_t=3, ntaper_z=4)[0])
+    assert np.abs(imgs[0]).max() > 0
+    ei = rel_l2(imgs[1], imgs[0])
+    print(f"TTI+Q image, BF16 Q memory vs FP32: {ei:.2e}")
+    assert ei < 1e-2

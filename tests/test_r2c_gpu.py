@@ -1,7 +1,8 @@
 """Pseudo-spectral engines on the GPU against the oracle: FFTWR2C
-(FdEngine_r2c: cuFFT line transforms) and FFTWR2R (FdEngine_r2r: cosine /
-sine transform derivatives as line-matrix GEMMs) - modelling traces of a VTI
-and a TTI + Q shot, and an RTM image.  FP32 transforms against the oracle's
+(FdEngine_r2c: cuFFT line transforms), FFTWR2R (FdEngine_r2r: cosine / sine
+transform derivatives as line-matrix GEMMs), and the Derivative-path engines
+FFTV and SINCOS on the same line operators - modelling traces of a VTI and a
+TTI + Q shot, and an RTM image.  FP32 transforms against the oracle's
 double sums: 1e-4, the engine's trace tolerance; images 1e-4 (atomic
 receiver injection reorders sums).  Line lengths are even: for odd n the
 FFTWR2C isign factor on bin n/2 gives its two passes a growing mode (the
@@ -12,7 +13,7 @@ import pytest
 
 from konglong_b200 import workloads as W
 from konglong_b200.propagator import Propagator, spread_coeffs
-from konglong_b200.spec import ENGINE_R2C, ENGINE_R2R, SNAP_FP32
+from konglong_b200.spec import ENGINE_FFTV, ENGINE_R2C, ENGINE_R2R, ENGINE_SINCOS, SNAP_FP32
 from oracle import pyoracle as O
 from tests.conftest import rel_l2
 from tests.test_gpu_parity import _modelling, _rtm
@@ -26,7 +27,10 @@ def _vti(nt, engine):
     return shot
 
 
-@pytest.mark.parametrize("engine", [ENGINE_R2C, ENGINE_R2R])
+SPECTRAL = [ENGINE_R2C, ENGINE_R2R, ENGINE_FFTV, ENGINE_SINCOS]
+
+
+@pytest.mark.parametrize("engine", SPECTRAL)
 @pytest.mark.parametrize("which", ["vti", "tti_q"])
 def test_r2c_modelling_traces(which, engine):
     nts = 160
@@ -46,7 +50,7 @@ def test_r2c_modelling_traces(which, engine):
     assert rel_l2(got, want) < 1e-4
 
 
-@pytest.mark.parametrize("engine", [ENGINE_R2C, ENGINE_R2R])
+@pytest.mark.parametrize("engine", SPECTRAL)
 def test_r2c_rtm_image(engine):
     nt = 120
     shot = _vti(nt, engine)
@@ -58,7 +62,7 @@ def test_r2c_rtm_image(engine):
     assert rel_l2(got.reshape(want.shape), want) < 1e-4
 
 
-@pytest.mark.parametrize("engine", [ENGINE_R2C, ENGINE_R2R])
+@pytest.mark.parametrize("engine", SPECTRAL)
 def test_pseudo_spectral_2d_grid(engine):
     """A 2-D grid (ny = 1: no y derivative, no y plans) through both engines:
     operator steps against the oracle."""
