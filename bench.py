@@ -55,6 +55,8 @@ def alg_bytes_per_cell(spec, snap_fmt, interval):
         core += 4.0 + 3 * 4.0 * spec.q_order
     if getattr(spec, "state_fp16", False):
         core -= 3 * 2.0  # w1 read, w0 read and write in 2 bytes (3s with s = 2)
+    if spec.use_q and getattr(spec, "q_bf16", False):
+        core -= 3 * 2.0 * spec.q_order  # Q memory d0 / d1 read, d0 write in 2 bytes
     snap = {0: 4.0, 1: 2.0, 2: 2.0, 3: 33 * 4.0 / 512}[snap_fmt] / interval
     return core + pml + snap, core, pml
 
@@ -236,8 +238,9 @@ def run_cuda(args, rank, world):
     shot = build_workload(args.workload, 2 * K + Wm + 8, args.scale)
     s = shot.spec
     s.state_fp16 = bool(args.state_fp16)
+    s.q_bf16 = bool(args.q_bf16)
     s.kernel_variant = args.kernel_variant
-    snap_fmt = SNAP_C16
+    snap_fmt = {"c16": SNAP_C16, "fp32": 0, "fp16s": 2}[args.snap]
     k1, k2 = W.spread_band(s)
     src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
     rcv = W.make_traceset(shot.rcv_pos, s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
@@ -331,6 +334,8 @@ def run_cuda(args, rank, world):
     cfg["autotuned_shape"] = tuned
     cfg["kernel_variant"] = args.kernel_variant
     cfg["state"] = "fp16 per-slab scale" if s.state_fp16 else "fp32"
+    if s.use_q:
+        cfg["q_memory"] = "bf16" if s.q_bf16 else "fp32"
     if args.snap_offload:
         cfg["snapshots"] = f"pinned host memory, {args.snap_offload} device staging slots"
     return dict(value=value, ms=ms, ms_step=ms_step, roofline=roof, e2e=e2e, clocks=clk.summary(),
@@ -415,6 +420,8 @@ def run_small_shots(args, ranks):
 RTM_FORMS = {
     # plain FP32 GPU form: FP32 state, Q memory and snapshots
     "plain": dict(q_bf16=False, snap="fp32"),
+    # the same with the reference's default snapshot codec (COMPRESS_16)
+    "plain_c16": dict(q_bf16=False, snap="c16"),
     # mixed precision: BF16 Q memory, FP16 snapshots with a per-slab scale
     "mixed": dict(q_bf16=True, snap="fp16s"),
     # mixed precision + learned compression: BF16 Q memory, learned 8^3-block
@@ -441,37 +448,65 @@ def rtm_form_propagator(shot, form, ae=None):
     import dataclasses
     from konglong_b200 import workloads as W
     from konglong_b200.propagator import Propagator
-    from konglong_b200.spec import SNAP_AE, SNAP_FP16S, SNAP_FP32
+    from konglong_b200.spec import SNAP_AE, SNAP_C16, SNAP_FP16S, SNAP_FP32
     f = RTM_FORMS[form]
     s = dataclasses.replace(shot.spec, q_bf16=f["q_bf16"])
     p = Propagator(s)
     p.set_q_coeffs(*W.q_coefficients(s.dt, shot.fpeak))
     p.set_model(**shot.model_arrays())
-    fmt = {"fp32": SNAP_FP32, "fp16s": SNAP_FP16S, "ae": SNAP_AE}[f["snap"]]
+    fmt = {"fp32": SNAP_FP32, "c16": SNAP_C16, "fp16s": SNAP_FP16S, "ae": SNAP_AE}[f["snap"]]
     if fmt == SNAP_AE:
         p.set_compressor(ae)
         p.set_compressor_fallback(1e-3, 0.05)
     return p, fmt
 
 
+def rtm_schedule(p, fmt, nt, interval, reserve_bytes):
+    """Store / recompute plan of one shot on this GPU: the snapshot slots and
+    checkpoints that fit the HBM left after the engine's own arrays (less
+    reserve_bytes).  Returns the plan and the figures behind it."""
+    import torch
+    from konglong_b200.propagator import checkpoint_plan, checkpoint_slots_for_budget
+    nsnap = (nt - 1) // interval + 1
+    slot_b = p.snapshot_slot_bytes(fmt)
+    ckpt_b = p.checkpoint_setup(0)
+    free = torch.cuda.mem_get_info()[0]
+    budget = free - reserve_bytes
+    s = checkpoint_slots_for_budget(nt, interval, slot_b, ckpt_b, budget)
+    if s == 0:
+        raise SystemExit("rtm_schedule: not even one snapshot slot and its checkpoints fit")
+    seg = checkpoint_plan(nt, interval, s)
+    return {"snapshots": nsnap, "slot_bytes": slot_b, "snapshot_gb_per_shot": nsnap * slot_b / 1e9,
+            "hbm_budget_gb": budget / 1e9, "fits": s >= nsnap, "seg_slots": s, "segments": len(seg),
+            "checkpoint_gb": ckpt_b / 1e9, "recomputed_steps": sum(b - a for a, b in seg[:-1])}
+
+
 def run_rtm_shot(args, ranks):
-    """RTM s/shot of the TTI + Q workload (640 x 640 x 512, PML 32, 5000 steps)
-    in the plain FP32 form and the chosen form (mixed precision + learned
-    snapshot compression; RTM_FORMS).  Each form runs K forward steps (a
-    snapshot every 8 steps) and K backward steps (the 128 x 128 receiver traces
-    injected, the imaging condition fused into the step) on the full grid,
-    timed with CUDA events; s/shot = (forward + backward ms per step) x 5000.
-    Image NRMSE of each form against the plain form: the same shot at 0.08
-    scale (51 x 51 x 41, 160 steps)."""
+    """RTM s/shot of the TTI + Q workload (640 x 640 x 512, PML 32, 5000 steps,
+    a snapshot every 8 steps: 625 snapshots) in the plain FP32 form, the
+    plain form with COMPRESS_16 snapshots, and the mixed and chosen forms
+    (RTM_FORMS).  A form whose snapshots do not fit the GPU's memory runs
+    store / recompute (Propagator.rtm_shot_checkpointed): checkpoints of the
+    propagation state at segment starts, each earlier segment's snapshots
+    recomputed in the backward pass.  Each form runs K forward steps
+    (snapshots stored) and K backward steps (128 x 128 receiver traces
+    injected, imaging condition fused into the step) on the full grid, timed
+    with CUDA events, and one checkpoint save + load;
+      s/shot = forward ms/step x (5000 + recomputed steps)
+             + backward ms/step x 5000 + 4 checkpoint copies per extra segment.
+    --full-shot runs the whole checkpointed shot instead and reports its
+    measured time.  Image NRMSE of each form against the plain form: the same
+    shot at 0.08 scale (51 x 51 x 41, 160 steps)."""
+    import torch
     from konglong_b200 import workloads as W
     from konglong_b200.propagator import spread_coeffs
     from konglong_b200.spec import BACKWARD, FORWARD
     K, Wm = args.steps, args.warmup
-    forms = ["plain", "mixed", "chosen"]
+    forms = ["plain", "plain_c16", "mixed", "chosen"]
     ae, ntrain = train_compressor()
-    interval = 8
+    interval, NT = 8, 5000
     res = {}
-    shot = W.tti_q(scale=args.scale, nt=2 * (K + Wm) + 8)
+    shot = W.tti_q(scale=args.scale, nt=NT if args.full_shot else 2 * (K + Wm) + 8)
     s = shot.spec
     k1, k2 = W.spread_band(s)
     src = W.make_traceset([shot.src_pos], s.nx, s.ny, s.nz, 10, k1, k2, spread_coeffs)
@@ -480,7 +515,18 @@ def run_rtm_shot(args, ranks):
     clk_all = []
     for form in forms:
         p, fmt = rtm_form_propagator(shot, form, ae)
-        p.snapshot_setup(fmt, (Wm + K) // interval + 2)
+        p.image_setup(3, 4, 1)  # the image volumes are allocated before the budget is taken
+        reserve = (1 << 30) + (s.n * 4 if fmt == 3 else 0)  # 1 GiB margin (+ the learned decode scratch)
+        plan = rtm_schedule(p, fmt, NT, interval, reserve)
+        if args.full_shot:
+            with ClockSampler(ranks.local_rank) as clk:
+                img, ms = p.rtm_shot_checkpointed(src, shot.wavelet[None, :], rcv, data, NT, NT, interval,
+                                                  plan["seg_slots"], snap_fmt=fmt, ntaper_t=3, ntaper_z=4)
+            clk_all.append(clk.summary())
+            p.close()
+            res[form] = {"plan": plan, "measured_ms": ms, "s_per_shot": sum(ms.values()) / 1e3}
+            continue
+        p.snapshot_setup(fmt, min(plan["seg_slots"], (Wm + K) // interval + 2))
         p.reset()
         p.set_injection(src, shot.wavelet[None, :], s.dt_dxyz)
         p.migration(FORWARD, 0, Wm, -1, interval)          # warm-up (graph capture, first launches)
@@ -493,9 +539,21 @@ def run_rtm_shot(args, ranks):
             p.migration(BACKWARD, Wm + K - 1, Wm - 1, -1, interval)
             bwd = p.last_loop_ms
         clk_all.append(clk.summary())
+        copy_ms = 0.0
+        if plan["segments"] > 1:
+            p.snapshot_setup(fmt, 0)
+            p.checkpoint_setup(1)
+            p.checkpoint_save(0), p.checkpoint_load(0)  # warm
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p.checkpoint_save(0), p.checkpoint_load(0)
+            torch.cuda.synchronize()
+            copy_ms = (time.perf_counter() - t0) * 1e3 / 2
         p.close()
-        res[form] = {"forward_ms_per_step": fwd / K, "backward_ms_per_step": bwd / K,
-                     "s_per_shot": (fwd + bwd) / K * 5000 / 1e3}
+        fwd_step, bwd_step = fwd / K, bwd / K
+        total = fwd_step * (NT + plan["recomputed_steps"]) + bwd_step * NT + copy_ms * 4 * (plan["segments"] - 1)
+        res[form] = {"plan": plan, "forward_ms_per_step": fwd_step, "backward_ms_per_step": bwd_step,
+                     "checkpoint_copy_ms": copy_ms, "s_per_shot": total / 1e3}
     # image error of each form against the plain FP32 form on the same shot at
     # 0.08 scale (160 steps); the tests state both against the FP64 oracle
     small = W.tti_q(scale=0.08, nt=160)
@@ -592,12 +650,18 @@ def main():
                          "smaller values are for profiler captures)")
     ap.add_argument("--state-fp16", action="store_true",
                     help="FP16 wavefield state with per-slab scales (FD8 VTI / TTI workloads)")
-    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
+    ap.add_argument("--snap", default="c16", choices=["c16", "fp32", "fp16s"],
+                    help="snapshot format of the forward step workloads (default: the reference's COMPRESS_16)")
+    ap.add_argument("--q-bf16", action="store_true",
+                    help="Q memory variables stored as bfloat16 (TTI + Q workloads)")
+    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6, 7],
                     help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiler runs: timings under a profiler mislead the tuner)")
     ap.add_argument("--snap-offload", type=int, default=0,
                     help="keep the snapshots in pinned host memory with this many device staging slots")
+    ap.add_argument("--full-shot", action="store_true",
+                    help="tti_q_rtm: run every form's whole 5000-step checkpointed shot instead of timed samples")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -658,8 +722,15 @@ def main():
                     "data": "synthetic (seeded model)",
                     "config": {"workload": f"tti_q RTM shot: {s.nx}x{s.ny}x{s.nz} FD8 TTI+Q, PML {s.nbnd[0]}, "
                                            f"dt {s.dt * 1e3:.4f} ms, 5000 steps, snapshots every 8 steps",
-                               "extrapolation": f"{args.steps} forward + {args.steps} backward full-grid steps "
-                                                "timed, x 5000 steps per pass",
+                               "timing": ("the whole checkpointed shot run and timed (device ms of its loops)"
+                                          if args.full_shot else
+                                          f"{args.steps} forward + {args.steps} backward full-grid steps timed; "
+                                          "s/shot = forward ms/step x (5000 + recomputed steps) + backward ms/step "
+                                          "x 5000 + 4 checkpoint copies per extra segment"),
+                               "memory": "snapshots that do not fit the HBM left after the engine's arrays run "
+                                         "store / recompute (checkpoints at segment starts, earlier segments "
+                                         "recomputed in the backward pass); the host (196 GB on these boxes) "
+                                         "cannot hold 524 GB of FP32 snapshots either",
                                "image_nrmse": "each form's image vs the plain FP32 form's on the same shot at "
                                               "0.08 scale (51x51x41, 160 steps)",
                                "compressor_training_blocks": r["ntrain"],
@@ -667,8 +738,10 @@ def main():
                     "s_per_shot": {k: v["s_per_shot"] for k, v in f.items()},
                     "speedup_vs_plain": {k: f["plain"]["s_per_shot"] / v["s_per_shot"] for k, v in f.items()},
                     "image_nrmse_vs_plain": {k: v["image_nrmse_vs_plain"] for k, v in f.items()},
-                    "ms_per_step": {k: {"forward": v["forward_ms_per_step"], "backward": v["backward_ms_per_step"]}
-                                    for k, v in f.items()},
+                    "ms_per_step": {k: {"forward": v.get("forward_ms_per_step"),
+                                        "backward": v.get("backward_ms_per_step")} for k, v in f.items()},
+                    "measured_ms": {k: v["measured_ms"] for k, v in f.items() if "measured_ms" in v},
+                    "store_recompute_plan": {k: v["plan"] for k, v in f.items()},
                     "cpu_baseline": None, "clocks": r["clocks"]}
             print(json.dumps(line), flush=True)
         R.finish(ranks)

@@ -126,8 +126,9 @@ typedef struct rtm_config {
                          rings, 4: ISO FD8 4 z cells per thread with register prefetch, 5:
                          compact FD split into line solves and pointwise epilogues with
                          register-streamed x / y lines, 6: compact FD segment-parallel with plain
-                         tile loads (the 4-cell and segment-parallel variants fall back when
-                         they do not apply) */
+                         tile loads, 7: as 3 with the visco-acoustic update loading its Q memory
+                         itself instead of from the divergence pass's TMA ring (the 4-cell and
+                         segment-parallel variants fall back when they do not apply) */
   int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):
                          the gradient is divided by rho (KernelCPU::divideRho) and the divergence
                          accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes
@@ -264,6 +265,28 @@ int rtm_snapshot_load(rtm_handle *h, int slot, float *dst);
  * slots ahead of the imaging condition.  Clears the slots; nstage = 0 returns
  * to device slots.  FP32, COMPRESS_16 and FP16 formats. */
 int rtm_snapshot_offload(rtm_handle *h, int nstage);
+/* Bytes of one snapshot slot of format fmt on this handle (the learned
+ * format with the current FP16 fallback setting); allocates nothing. */
+int rtm_snapshot_slot_bytes(rtm_handle *h, int fmt, size_t *bytes);
+/* Snapshot slot window: the loops put the snapshot of step it in slot
+ * it / interval - first and skip steps whose slot falls outside
+ * [0, nslots); clears the stored flags.  rtm_snapshot_setup sets it to 0.  With checkpoints
+ * (below) a backward pass over a long shot images one segment at a time
+ * from slots that hold only that segment's snapshots. */
+int rtm_snapshot_window(rtm_handle *h, int first);
+/* Checkpoints of the propagation state, the store / recompute alternative to
+ * spilling snapshots (the reference spills them to a cache file,
+ * bgprtm/CacheFile.cpp:32-109; it has no checkpoints): nckpt device slots
+ * that each hold the wavefields w0 / w1 (FP16 state: codes, slab scales and
+ * maxima), the Q memory of both time levels and every PML memory array;
+ * *bytes_each (optional) receives the bytes per slot.  Save / load copy on
+ * the engine's stream: loading slot k and running the loop from step it
+ * reproduces, bit for bit, what the loop computed from the step at which
+ * slot k was saved.  The source / receiver traces and the image are not part
+ * of the state. */
+int rtm_checkpoint_setup(rtm_handle *h, int nckpt, size_t *bytes_each);
+int rtm_checkpoint_save(rtm_handle *h, int k);
+int rtm_checkpoint_load(rtm_handle *h, int k);
 
 /* Imaging condition set-up: ntaper_t source time-taper snapshots, ntaper_z
  * depth-taper cells (ImagingCondition::calTapes), edge_taper=1 applies the

@@ -33,7 +33,8 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_batch_create", "rtm_batch_destroy", "rtm_batch_modelling", "rtm_batch_last_ms",
            "rtm_batch_autotune", "rtm_ae_nparams", "rtm_ae_create", "rtm_ae_destroy", "rtm_ae_set_params",
            "rtm_ae_get_params", "rtm_ae_loss_grad", "rtm_ae_train_step", "rtm_ae_reconstruct",
-           "rtm_ae_compress_volume", "rtm_ae_decompress_volume", "rtm_set_compressor"]
+           "rtm_ae_compress_volume", "rtm_ae_decompress_volume", "rtm_set_compressor",
+           "rtm_snapshot_window", "rtm_snapshot_slot_bytes", "rtm_checkpoint_setup", "rtm_checkpoint_save", "rtm_checkpoint_load"]
 
 KERNEL_KINDS = ["iso_fd8_step", "grad_fd8", "div_fd8", "cfd_z", "cfd_x", "cfd_y", "cfd_grad_epilogue",
                 "cfd_div_epilogue", "inject", "extract", "slab_max", "fused_io", "cfd_y_fused", "cfd_x_fused"]
@@ -107,6 +108,11 @@ def lib():
     L.rtm_autotune.argtypes = [vp, i, C.POINTER(i)]
     L.rtm_autotune_result.argtypes = [vp, i, C.POINTER(i), C.POINTER(C.c_float)]
     L.rtm_snapshot_offload.argtypes = [vp, i]
+    L.rtm_snapshot_window.argtypes = [vp, i]
+    L.rtm_snapshot_slot_bytes.argtypes = [vp, i, C.POINTER(C.c_size_t)]
+    L.rtm_checkpoint_setup.argtypes = [vp, i, C.POINTER(C.c_size_t)]
+    L.rtm_checkpoint_save.argtypes = [vp, i]
+    L.rtm_checkpoint_load.argtypes = [vp, i]
     L.rtm_illum_setup.argtypes = [vp, i]
     L.rtm_image_condition.argtypes = [vp, i]
     L.rtm_set_compressor_fallback.argtypes = [vp, C.c_float, C.c_float]

@@ -118,6 +118,8 @@ bool tma_supported(int nz);
 void launch_selftest_wait(int *err, cudaStream_t st);
 // fp32 volume [ny][nx][nz], box (bz, bx, 1)
 bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz, int bx, int by = 1);
+// Q memory variables [L][ny][nx][nz] (FP32 or BF16), 4-D box (bz, bx, 1, L)
+bool make_tmap_q(CUtensorMap *m, const void *base, int nx, int ny, int nz, int L, bool bf16, int bz, int bx);
 struct TmaShape {
   int tx, depth;  // tile width (x) and planes prefetched beyond the stencil window
 };
@@ -146,7 +148,14 @@ struct Grad4Maps {
 };
 struct Div4Maps {
   CUtensorMap py, px, pz, w0, vel, w1;  // py (32, tx); px (32, tx + 8); pz (40, tx); w0 / vel / w1 (32, tx)
+  // visco-acoustic update with its operands in the ring (qring 1: FP32 Q
+  // memory, 2: BF16; 0: loaded by the update itself): the d0 / d1 halves
+  // (box (32, tx, 1, order)) and 1/Q (box (32, tx))
+  CUtensorMap qa, qb, iq;
+  int qring;
 };
+// orders of the Q memory the divergence ring carries
+constexpr int kDiv4QMax = 4;
 bool aniso4_init();         // shared-memory attributes (call outside any capture)
 int aniso4_ctas_per_sm();   // resident CTAs per SM of the interior divergence kernel
 void launch_grad4(const GradArgs &a, const Tile4 *tiles, int ntiles, bool edge, int model, const Grad4Maps &m,

@@ -12,6 +12,8 @@
 // keep the x / z face memory of their 4 cells (pointers advancing by a constant stride per
 // plane) and load every memory value of a plane before its recursion.
 // Requires nz % 4 == 0.
+#include <type_traits>
+
 #include "kernel_api.h"
 #include "rtm_device.cuh"
 #include "tma.cuh"
@@ -343,15 +345,38 @@ struct __align__(128) Div4Smem {
   uint64_t bar_b[SB];
 };
 
-template <int TX, int P, int MODE, bool EDGE>
+// The visco-acoustic operands of ring B's planes (after Div4Smem in shared
+// memory): the d0 / d1 halves of the Q memory, orders [0, kDiv4QMax), and 1/Q.
+template <int TX, int SB, typename QT>
+struct __align__(128) Div4QRing {
+  QT qa[SB][kDiv4QMax][TX][32];
+  QT qb[SB][kDiv4QMax][TX][32];
+  float iq[SB][TX][32];
+};
+
+template <int QR>
+using QType = typename std::conditional<QR == 2, __nv_bfloat16, float>::type;
+
+template <int TX, int P, int QR>
+constexpr size_t div4_smem() {
+  return sizeof(Div4Smem<TX, P>) + (QR ? sizeof(Div4QRing<TX, Div4Smem<TX, P>::SB, QType<QR>>) : 0);
+}
+
+// QR: 0 the Q update loads its own operands; 1 / 2 ring B also carries the Q
+// memory (FP32 / BF16) and 1/Q of its planes (MODE 2, order <= kDiv4QMax)
+template <int TX, int P, int MODE, bool EDGE, int QR>
 __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 384 / (8 * TX) : 0)
     div4_k(const __grid_constant__ DivArgs a, const Tile4 *__restrict__ tiles, const __grid_constant__ Div4Maps mp,
            int *err) {
   using S = Div4Smem<TX, P>;
   constexpr int SA = S::SA, SB = S::SB;
+  using QT = QType<QR>;
+  using QRing = Div4QRing<TX, SB, QT>;
   constexpr uint32_t BYTES_A = TX * 128, BYTES_B = (TX + 2 * R4) * 128 + TX * 160 + 3 * TX * 128;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
+  QRing &qr = *reinterpret_cast<QRing *>(smem_raw + sizeof(S));
+  const uint32_t bytes_q = QR ? (uint32_t)(2 * a.q.order * TX * 32 * sizeof(QT) + TX * 32 * 4) : 0u;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const Grid3 g{nx, ny, nz, (long long)nx * nz};
   const int tzq = threadIdx.x, tx = threadIdx.y;
@@ -380,12 +405,17 @@ __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 384 / (8 * TX) : 0
   };
   auto issue_b = [&](int p) {
     const int st = (p - y0) % SB;
-    mbar_expect_tx(&s.bar_b[st], BYTES_B);
+    mbar_expect_tx(&s.bar_b[st], BYTES_B + bytes_q);
     tma_load_3d(&s.px[st][0][0], &mp.px, &s.bar_b[st], iz0, ix0 - R4, p);
     tma_load_3d(&s.pz[st][0][0], &mp.pz, &s.bar_b[st], iz0 - R4, ix0, p);
     tma_load_3d(&s.w[st][0][0][0], &mp.w0, &s.bar_b[st], iz0, ix0, p);
     tma_load_3d(&s.w[st][1][0][0], &mp.vel, &s.bar_b[st], iz0, ix0, p);
     tma_load_3d(&s.w[st][2][0][0], &mp.w1, &s.bar_b[st], iz0, ix0, p);
+    if constexpr (QR != 0) {
+      tma_load_4d(&qr.qa[st][0][0][0], &mp.qa, &s.bar_b[st], iz0, ix0, p, 0);
+      tma_load_4d(&qr.qb[st][0][0][0], &mp.qb, &s.bar_b[st], iz0, ix0, p, 0);
+      tma_load_3d(&qr.iq[st][0][0], &mp.iq, &s.bar_b[st], iz0, ix0, p);
+    }
   };
   if (producer) {
     for (int k = 0; k < SA; k++) mbar_init(&s.bar_a[k], 1);
@@ -466,6 +496,10 @@ __global__ void __launch_bounds__(8 * TX, EDGE && MODE != 2 ? 384 / (8 * TX) : 0
       } else if (MODE == 1) {
 #pragma unroll
         for (int c = 0; c < 4; c++) set4(out4, c, __fsub_rn(__fadd_rn(cmp4(cw1, c), cmp4(cw1, c)), cmp4(t4, c)));
+      } else if constexpr (QR != 0) {
+        const float4 iq4 = *reinterpret_cast<const float4 *>(&qr.iq[sb][tx][4 * tzq]);
+        out4 = q_update4_ring<QT>(a.q, i0, (long long)ny * g.nxz, t4, cw1, &qr.qa[sb][0][tx][4 * tzq],
+                                  &qr.qb[sb][0][tx][4 * tzq], TX * 32, iq4);
       } else {
         out4 = q_update4(a.q, i0, (long long)ny * g.nxz, t4, cw1);
       }
@@ -494,10 +528,10 @@ bool grad4_attr1() {
   return cudaFuncSetAttribute(grad4_k<TX, P, MODEL, EDGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)grad4_smem<TX, P, MODEL>()) == cudaSuccess;
 }
-template <int TX, int P, int MODE, bool EDGE>
+template <int TX, int P, int MODE, bool EDGE, int QR = 0>
 bool div4_attr1() {
-  return cudaFuncSetAttribute(div4_k<TX, P, MODE, EDGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(Div4Smem<TX, P>)) == cudaSuccess;
+  return cudaFuncSetAttribute(div4_k<TX, P, MODE, EDGE, QR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)div4_smem<TX, P, QR>()) == cudaSuccess;
 }
 
 constexpr int kTX = kAniso4TX, kP = 2;
@@ -511,12 +545,14 @@ bool aniso4_init() {
   ok &= div4_attr1<kTX, kP, 0, false>() && div4_attr1<kTX, kP, 0, true>();
   ok &= div4_attr1<kTX, kP, 1, false>() && div4_attr1<kTX, kP, 1, true>();
   ok &= div4_attr1<kTX, kP, 2, false>() && div4_attr1<kTX, kP, 2, true>();
+  ok &= div4_attr1<kTX, kP, 2, false, 1>() && div4_attr1<kTX, kP, 2, true, 1>();
+  ok &= div4_attr1<kTX, kP, 2, false, 2>() && div4_attr1<kTX, kP, 2, true, 2>();
   return ok;
 }
 
 int aniso4_ctas_per_sm() {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, div4_k<kTX, kP, 1, false>, 8 * kTX, sizeof(Div4Smem<kTX, kP>));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, div4_k<kTX, kP, 1, false, 0>, 8 * kTX, div4_smem<kTX, kP, 0>());
   return n > 0 ? n : 1;
 }
 
@@ -539,17 +575,22 @@ void launch_div4(const DivArgs &a, const Tile4 *tiles, int ntiles, bool edge, in
                  cudaStream_t st) {
   if (ntiles <= 0) return;
   const dim3 block(8, kTX);
-  const size_t smem = sizeof(Div4Smem<kTX, kP>);
-#define D_(MD, E) div4_k<kTX, kP, MD, E><<<ntiles, block, smem, st>>>(a, tiles, m, err)
+#define D_(MD, E, QR) div4_k<kTX, kP, MD, E, QR><<<ntiles, block, div4_smem<kTX, kP, QR>(), st>>>(a, tiles, m, err)
   if (mode == 0) {
-    if (edge) D_(0, true);
-    else D_(0, false);
+    if (edge) D_(0, true, 0);
+    else D_(0, false, 0);
   } else if (mode == 1) {
-    if (edge) D_(1, true);
-    else D_(1, false);
+    if (edge) D_(1, true, 0);
+    else D_(1, false, 0);
+  } else if (m.qring == 1) {
+    if (edge) D_(2, true, 1);
+    else D_(2, false, 1);
+  } else if (m.qring == 2) {
+    if (edge) D_(2, true, 2);
+    else D_(2, false, 2);
   } else {
-    if (edge) D_(2, true);
-    else D_(2, false);
+    if (edge) D_(2, true, 0);
+    else D_(2, false, 0);
   }
 #undef D_
 }

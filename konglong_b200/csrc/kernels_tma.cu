@@ -210,6 +210,24 @@ bool make_tmap(CUtensorMap *m, const void *base, int nx, int ny, int nz, int bz,
   return r == CUDA_SUCCESS;
 }
 
+// Q memory variables [L][ny][nx][nz] (FP32 or BF16) as one 4-D tensor with a
+// box of (bz, bx, 1, L): every order of a column tile in one copy.  The row,
+// plane and order strides must be multiples of 16 bytes (nz % 4 == 0 for
+// FP32, nz % 8 == 0 for BF16).
+bool make_tmap_q(CUtensorMap *m, const void *base, int nx, int ny, int nz, int L, bool bf16, int bz, int bx) {
+  EncodeTiledFn fn = encode_fn();
+  const int es = bf16 ? 2 : 4;
+  if (!fn || L < 1 || L > 8 || (nz * es) % 16 != 0 || ((uintptr_t)base & 15)) return false;
+  cuuint64_t dims[4] = {(cuuint64_t)nz, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)L};
+  cuuint64_t strides[3] = {(cuuint64_t)nz * es, (cuuint64_t)nz * nx * es, (cuuint64_t)nz * nx * ny * es};
+  cuuint32_t box[4] = {(cuuint32_t)bz, (cuuint32_t)bx, 1, (cuuint32_t)L};
+  cuuint32_t est[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                  const_cast<void *>(base), dims, strides, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 template <int TX, int P>
 static void iso_tma_shape(const IsoArgs &a, const CUtensorMap &w1, const CUtensorMap &w0, const CUtensorMap &vel,
                           int *err, int mode, int pml3d, cudaStream_t st) {

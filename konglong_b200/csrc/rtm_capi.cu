@@ -156,6 +156,13 @@ struct Engine {
     CUtensorMap m;
   };
   std::vector<TMap> tmaps;
+  // checkpoints of the propagation state (rtm_checkpoint_setup): nckpt slots of
+  // ckpt_bytes; the loops map step it to snapshot slot it / interval - slot0
+  char *ckpts = nullptr;
+  int nckpt = 0;
+  size_t ckpt_bytes = 0;
+  int slot0 = 0;
+  int qring_ok = 1;  // the divergence ring may carry the Q memory (not kernel_variant 7)
   int prof_on = 0;
   struct ProfRec {
     int kind;
@@ -432,6 +439,22 @@ static void cfd_constant_run(int n, const std::vector<float> &lm, const std::vec
 
 static PmlDev pml_dev(Engine *h) { return h->pml; }
 
+// tensor map of the Q memory half at p ([order][ny][nx][nz], FP32 or BF16)
+// with box (32, bx, 1, order), cached like tmap (by = -order marks the 4-D map)
+static bool tmap_q(Engine *h, const void *p, int bx, CUtensorMap *out) {
+  const int L = h->c.q_order;
+  for (const auto &t : h->tmaps)
+    if (t.p == p && t.bz == 32 && t.bx == bx && t.by == -L) {
+      *out = t.m;
+      return true;
+    }
+  Engine::TMap t{p, 32, bx, -L, {}};
+  if (!make_tmap_q(&t.m, p, h->d.nx, h->d.ny, h->d.nz, L, h->c.q_bf16 != 0, 32, bx)) return false;
+  h->tmaps.push_back(t);
+  *out = t.m;
+  return true;
+}
+
 // tensor map of a device volume with box (bz, bx, 1), built once per buffer;
 // returned by value (the cache may grow and move its entries)
 static bool tmap(Engine *h, const void *p, int bz, int bx, CUtensorMap *out, int by = 1) {
@@ -690,6 +713,12 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     ok = ok && tmap(h, h->px, 32, T + 8, &dm.px) && tmap(h, h->pz, 40, T, &dm.pz) &&
          tmap(h, h->py ? h->py : h->px, 32, T, &dm.py) && tmap(h, h->w0, 32, T, &dm.w0) &&
          tmap(h, h->vel, 32, T, &dm.vel) && tmap(h, h->w1, 32, T, &dm.w1);
+    // the visco-acoustic update takes its Q memory and 1/Q from ring B when
+    // they fit it (order <= kDiv4QMax; BF16 rows need nz % 8 == 0)
+    dm.qring = 0;
+    if (ok && mode == 2 && h->c.q_order <= kDiv4QMax && h->qring_ok &&
+        tmap_q(h, q.d0, T, &dm.qa) && tmap_q(h, q.d1, T, &dm.qb) && tmap(h, h->invq, 32, T, &dm.iq))
+      dm.qring = h->c.q_bf16 ? 2 : 1;
     if (ok) {
       {
         KScope k(h, RTM_K_GRAD, (t.n_int > 0) + (t.n_edge > 0));
@@ -1301,6 +1330,57 @@ static int batch_run(rtm_batch *b, const std::vector<int> &order, const std::vec
 }
 }  // namespace rtm
 
+namespace rtm {
+// The time-dependent propagation state, in a fixed order: the wavefields of
+// the current step (w0, w1; FP16 state: the codes, the three slab scales and
+// the two slab maxima in their current roles), the Q memory of both time
+// levels (current first) and every PML memory array.  Saving and loading in
+// the same order keeps the roles that the per-step swaps rotate.
+static void state_pieces(Engine *h, std::vector<std::pair<void *, size_t>> &v) {
+  const size_t n = (size_t)h->n, ny = (size_t)h->d.ny;
+  if (h->f16) {
+    v.push_back({h->h0, n * 2}), v.push_back({h->h1, n * 2});
+    v.push_back({h->s0, ny * 4}), v.push_back({h->s1, ny * 4}), v.push_back({h->sn, ny * 4});
+    v.push_back({h->m0, ny * 4}), v.push_back({h->m1, ny * 4});
+  } else {
+    v.push_back({h->w0, n * 4}), v.push_back({h->w1, n * 4});
+  }
+  if (h->c.use_q && h->wq[0]) {
+    const size_t qb = (size_t)h->c.q_order * n * (h->c.q_bf16 ? 2 : 4);
+    v.push_back({h->wq[h->iq0], qb}), v.push_back({h->wq[1 - h->iq0], qb});
+  }
+  for (int dim = 0; dim < 3; dim++)
+    for (int sd = 0; sd < 2; sd++) {
+      const PmlFace &F = h->pml.f[dim][sd];
+      if (!F.w) continue;
+      const long long plane = dim == DX ? (long long)h->d.ny * h->d.nz
+                              : dim == DY ? (long long)h->d.nx * h->d.nz : (long long)h->d.nx * h->d.ny;
+      for (int r = 0; r < 2; r++)
+        for (int k = 0; k < 3; k++)
+          if (F.q[r][k]) v.push_back({F.q[r][k], (size_t)plane * F.w * 4});
+    }
+}
+
+// bytes of one snapshot slot of format fmt (256-byte multiples); the learned
+// format with the handle's current FP16 fallback
+static size_t slot_size(Engine *h, int fmt) {
+  const size_t b = fmt == RTM_SNAP_FP32  ? (size_t)h->n * 4
+                   : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2
+                   : fmt == RTM_SNAP_AE  ? ((size_t)ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4 + 15) / 16 * 16 +
+                                              (ae_fb_cap(h) ? ae_fallback_bytes(ae_fb_cap(h)) : 0)
+                                         : (size_t)h->n * 2;
+  return (b + 255) / 256 * 256;
+}
+
+static size_t state_size(Engine *h) {
+  std::vector<std::pair<void *, size_t>> v;
+  state_pieces(h, v);
+  size_t b = 0;
+  for (auto &p : v) b += (p.second + 255) / 256 * 256;
+  return b;
+}
+}  // namespace rtm
+
 extern "C" {
 
 void rtm_config_default(rtm_config *c) {
@@ -1511,11 +1591,14 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   if (c->engine == RTM_ENGINE_FD8 && !h->lap_iso() && (rc = fd8_tiles(h))) return fail(rc);
   // the 4-cell passes carry no density term: a density model runs the one-cell passes
   if (c->engine == RTM_ENGINE_FD8 && !h->lap_iso() && !c->use_rho && !c->state_fp16 && d->nz % 4 == 0 &&
-      (c->kernel_variant == 0 || c->kernel_variant == 3) && tma_supported(d->nz) && aniso4_init()) {
+      (c->kernel_variant == 0 || c->kernel_variant == 3 || c->kernel_variant == 7) && tma_supported(d->nz) &&
+      aniso4_init()) {
     h->aniso4 = 1;
     h->an4_yseg = yseg_an4(h);
     if ((rc = an4_tiles(h))) return fail(rc);
   }
+  // BF16 rows of the Q-memory tensor maps need nz % 8 == 0 (16-byte strides)
+  h->qring_ok = c->kernel_variant != 7 && (!c->q_bf16 || d->nz % 8 == 0);
   h->cfd_tma = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && tma_supported(d->nz);
   // compact FD on 3-D grids whose lines fit a tile: the segment-parallel fused
   // pipeline by default (kernel_variant 0; 6 forces its plain-load form); 5
@@ -1737,18 +1820,58 @@ int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots) {
   h->host_snaps = nullptr, h->nstage = 0;
   h->release(h->snaps), h->release(h->slabs), h->release(h->ae_scratch);
   h->snaps = nullptr, h->slabs = nullptr, h->ae_scratch = nullptr;
-  h->snap_fmt = fmt, h->nslots = nslots;
-  h->slot_bytes = fmt == RTM_SNAP_FP32  ? (size_t)h->n * 4
-                  : fmt == RTM_SNAP_C16 ? (size_t)(h->nxz + 2) * h->d.ny * 2
-                  : fmt == RTM_SNAP_AE  ? ((size_t)rtm::ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 33 * 4 + 15) / 16 * 16 +
-                                              (rtm::ae_fb_cap(h) ? rtm::ae_fallback_bytes(rtm::ae_fb_cap(h)) : 0)
-                                        : (size_t)h->n * 2;
-  h->slot_bytes = (h->slot_bytes + 255) / 256 * 256;
+  h->snap_fmt = fmt, h->nslots = nslots, h->slot0 = 0;
+  h->slot_bytes = rtm::slot_size(h, fmt);
   h->stored.assign(nslots, 0);
   if (!nslots) return RTM_OK;
   TRY(h->alloc(h->snaps, h->slot_bytes * nslots));
   if (fmt == RTM_SNAP_C16 || fmt == RTM_SNAP_FP16S) TRY(h->alloc(h->slabs, (size_t)nslots * h->d.ny));
   if (fmt == RTM_SNAP_AE) TRY(h->alloc(h->ae_scratch, h->n));
+  return RTM_OK;
+}
+
+
+int rtm_checkpoint_setup(rtm_handle *h, int nckpt, size_t *bytes_each) {
+  if (!h || nckpt < 0) return RTM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaStreamSynchronize(h->st));
+  h->release(h->ckpts);
+  h->ckpts = nullptr, h->nckpt = 0;
+  h->ckpt_bytes = rtm::state_size(h);
+  if (bytes_each) *bytes_each = h->ckpt_bytes;
+  if (!nckpt) return RTM_OK;
+  TRY(h->alloc(h->ckpts, h->ckpt_bytes * (size_t)nckpt));
+  h->nckpt = nckpt;
+  return RTM_OK;
+}
+
+static int checkpoint_copy(rtm_handle *h, int k, bool save) {
+  if (!h || k < 0 || k >= h->nckpt) return RTM_ERR_ARG;
+  TRY(rtm::ready(h));
+  std::vector<std::pair<void *, size_t>> v;
+  rtm::state_pieces(h, v);
+  char *base = h->ckpts + (size_t)k * h->ckpt_bytes;
+  for (auto &p : v) {
+    if (save) CK(cudaMemcpyAsync(base, p.first, p.second, cudaMemcpyDeviceToDevice, h->st));
+    else CK(cudaMemcpyAsync(p.first, base, p.second, cudaMemcpyDeviceToDevice, h->st));
+    base += (p.second + 255) / 256 * 256;
+  }
+  return RTM_OK;
+}
+
+int rtm_checkpoint_save(rtm_handle *h, int k) { return checkpoint_copy(h, k, true); }
+int rtm_checkpoint_load(rtm_handle *h, int k) { return checkpoint_copy(h, k, false); }
+
+int rtm_snapshot_window(rtm_handle *h, int first) {
+  if (!h) return RTM_ERR_ARG;
+  h->slot0 = first;
+  std::fill(h->stored.begin(), h->stored.end(), 0);
+  return RTM_OK;
+}
+
+int rtm_snapshot_slot_bytes(rtm_handle *h, int fmt, size_t *bytes) {
+  if (!h || !bytes || fmt < RTM_SNAP_FP32 || fmt > RTM_SNAP_AE) return RTM_ERR_ARG;
+  *bytes = rtm::slot_size(h, fmt);
   return RTM_OK;
 }
 
@@ -1979,7 +2102,7 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
     pending = rtm::io_none(), pending_slot = -1;
     TRY(rtm::do_inject(h, it + it_shift * inc));
     if (it % interval == 0) {
-      const int slot = it / interval;
+      const int slot = it / interval - h->slot0;
       if (slot >= 0 && slot < h->nslots) {
         if (dir == RTM_FORWARD) {
           if (h->snap_fmt == RTM_SNAP_AE) {

@@ -644,4 +644,55 @@ static __device__ __noinline__ float4 q_update4(const QDev &Q, long long i, long
   return make_float4(v[0], v[1], v[2], v[3]);
 }
 
+// four consecutive memory-variable values staged in shared memory
+__device__ __forceinline__ float4 q_sm4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 q_sm4(const __nv_bfloat16 *p) {
+  const uint2 r = *reinterpret_cast<const uint2 *>(p);
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&r.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+// four consecutive memory-variable values to global memory (j a multiple of 4)
+__device__ __forceinline__ void q_gst4(float *h, long long j, float4 v) { *reinterpret_cast<float4 *>(h + j) = v; }
+__device__ __forceinline__ void q_gst4(__nv_bfloat16 *h, long long j, float4 v) {
+  const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+  uint2 r;
+  r.x = *reinterpret_cast<const unsigned *>(&a);
+  r.y = *reinterpret_cast<const unsigned *>(&b);
+  *reinterpret_cast<uint2 *>(h + j) = r;
+}
+
+// q_update4 with its operands already in shared memory (staged by a TMA ring
+// ahead of the step that needs them): qa / qb point at order 0 of the d0 / d1
+// halves for the thread's 4 cells, order l at + l * ostride elements, iq is
+// 1/Q of the cells; order <= 4.  The new d0 values go to global memory.  The
+// arithmetic and its order are q_update4's, so the results are bitwise equal.
+template <typename QT>
+__device__ __forceinline__ float4 q_update4_ring(const QDev &Q, long long i, long long n, float4 t, float4 u,
+                                                 const QT *qa, const QT *qb, int ostride, float4 iq) {
+  const float uv[4] = {u.x, u.y, u.z, u.w}, iv[4] = {iq.x, iq.y, iq.z, iq.w};
+  float v[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+  for (int c = 0; c < 4; c++) v[c] = q_init(uv[c], iv[c], Q.cqsum, v[c]);
+  float4 d0[4], d1[4];
+#pragma unroll
+  for (int l = 0; l < 4; l++)
+    if (l < Q.order) d0[l] = q_sm4(qa + l * ostride), d1[l] = q_sm4(qb + l * ostride);
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      if (l < Q.order) {
+        const float e0 = io4_get(d0[l], c), e1 = io4_get(d1[l], c);
+        const float el = Q.wq[l];
+        v[c] = q_acc(v[c], iv[c], el, e0, e1);
+        io4_set(d0[l], c, q_next(Q.cq[l], uv[c], el, e0));
+      }
+  QT *gd = reinterpret_cast<QT *>(Q.d0);
+#pragma unroll
+  for (int l = 0; l < 4; l++)
+    if (l < Q.order) q_gst4(gd, (long long)l * n + i, d0[l]);
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
 }  // namespace rtm

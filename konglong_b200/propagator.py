@@ -174,6 +174,26 @@ class Propagator:
         self._ck(self.L.rtm_illum_compensate(self.h, smooth_xy, smooth_z, amp_damping, damp_weight),
                  "rtm_illum_compensate")
 
+    def snapshot_slot_bytes(self, fmt):
+        b = C.c_size_t(0)
+        self._ck(self.L.rtm_snapshot_slot_bytes(self.h, int(fmt), C.byref(b)), "rtm_snapshot_slot_bytes")
+        return int(b.value)
+
+    def snapshot_window(self, first):
+        self._ck(self.L.rtm_snapshot_window(self.h, int(first)), "rtm_snapshot_window")
+
+    def checkpoint_setup(self, nckpt):
+        """Allocates nckpt checkpoint slots; returns the bytes of one slot."""
+        b = C.c_size_t(0)
+        self._ck(self.L.rtm_checkpoint_setup(self.h, int(nckpt), C.byref(b)), "rtm_checkpoint_setup")
+        return int(b.value)
+
+    def checkpoint_save(self, k):
+        self._ck(self.L.rtm_checkpoint_save(self.h, int(k)), "rtm_checkpoint_save")
+
+    def checkpoint_load(self, k):
+        self._ck(self.L.rtm_checkpoint_load(self.h, int(k)), "rtm_checkpoint_load")
+
     def snapshot_offload(self, nstage):
         """Keep the snapshot slots in pinned host memory with `nstage` device staging slots (0: device slots)."""
         self._ck(self.L.rtm_snapshot_offload(self.h, int(nstage)), "rtm_snapshot_offload")
@@ -246,6 +266,75 @@ class Propagator:
         self.migration(1, nt - 1, -1, it_shift, interval)
         bwd_ms = self.last_loop_ms
         return self.get(FIELD_IMAGE), fwd_ms, bwd_ms
+
+    def rtm_shot_checkpointed(self, src: TraceSet, src_traces, rcv: TraceSet, rcv_traces, nt, nts_fwd, interval,
+                              seg_slots, snap_fmt=0, ntaper_t=0, ntaper_z=0, edge=1, it_shift=-1):
+        """Propagator::rtm for one shot whose snapshots do not all fit: store /
+        recompute.  The snapshot slots hold seg_slots snapshots (one segment of
+        seg_slots * interval steps).  The forward pass saves a checkpoint of the
+        propagation state at the start of every segment but the last and
+        stores the last segment's snapshots; the backward pass images the last
+        segment, then for each earlier segment saves the receiver state,
+        reloads the segment's source checkpoint, recomputes its snapshots,
+        restores the receiver state and images the segment.  The result equals
+        rtm_shot's (same arithmetic per step; the backward receiver injection's
+        atomic adds may order differently).  Returns the image and the device
+        ms of the forward, recompute and backward loops."""
+        seg = checkpoint_plan(nts_fwd, interval, seg_slots)
+        nseg = len(seg)
+        self.snapshot_setup(snap_fmt, seg_slots)
+        # checkpoint slots 0 .. nseg-2: the source segments; nseg-1: the receiver state
+        self.checkpoint_setup(nseg if nseg > 1 else 0)
+        self.reset()
+        self.set_injection(src, src_traces, self.spec.dt_dxyz)
+        self.snapshot_window(seg[-1][0] // interval)
+        ms = {"forward": 0.0, "recompute": 0.0, "backward": 0.0}
+        for j, (a, b) in enumerate(seg):
+            if j < nseg - 1:
+                self.checkpoint_save(j)
+            self.migration(FORWARD, a, b, it_shift, interval)
+            ms["forward"] += self.last_loop_ms
+        self.reset()
+        self.image_setup(ntaper_t, ntaper_z, edge)
+        self.set_injection(rcv, rcv_traces, self.spec.dt_dxyz)
+        hi = nt - 1
+        for j in range(nseg - 1, -1, -1):
+            a, b = seg[j]
+            if j < nseg - 1:
+                self.checkpoint_save(nseg - 1)
+                self.checkpoint_load(j)
+                self.snapshot_window(a // interval)
+                self.set_injection(src, src_traces, self.spec.dt_dxyz)
+                self.migration(FORWARD, a, b, it_shift, interval)
+                ms["recompute"] += self.last_loop_ms
+                self.checkpoint_load(nseg - 1)
+                self.set_injection(rcv, rcv_traces, self.spec.dt_dxyz)
+            self.migration(1, hi, a - 1, it_shift, interval)
+            ms["backward"] += self.last_loop_ms
+            hi = a - 1
+        return self.get(FIELD_IMAGE), ms
+
+
+def checkpoint_plan(nts_fwd, interval, seg_slots):
+    """Segments [a, b) of the forward steps [0, nts_fwd) for store / recompute:
+    each holds seg_slots snapshots (seg_slots * interval steps), the last one
+    the remainder."""
+    if interval < 1 or seg_slots < 1 or nts_fwd < 1:
+        raise ValueError("checkpoint_plan: interval, seg_slots and nts_fwd must be positive")
+    step = seg_slots * interval
+    return [(a, min(a + step, nts_fwd)) for a in range(0, nts_fwd, step)]
+
+
+def checkpoint_slots_for_budget(nts_fwd, interval, slot_bytes, ckpt_bytes, budget_bytes):
+    """The largest segment (in snapshots) whose slots plus one checkpoint per
+    segment (and one for the receiver state) fit budget_bytes; 0 when none
+    does.  All snapshots fit when the return value covers nts_fwd."""
+    nsnap = (nts_fwd - 1) // interval + 1
+    for s in range(nsnap, 0, -1):
+        nseg = -(-nsnap // s)
+        if s * slot_bytes + (nseg if nseg > 1 else 0) * ckpt_bytes <= budget_bytes:
+            return s
+    return 0
 
 
 class Batch:

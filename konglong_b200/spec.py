@@ -44,7 +44,9 @@ class PropSpec:
     q_bf16: bool = False          # Q memory variables stored as bfloat16
     kernel_variant: int = 0       # 0 auto, 1 one cell per thread / plain tiles, 2 TMA (CFD x/y tiles,
                                   # ISO one-cell plane pipeline), 3 FD8 4 z cells per thread with TMA
-                                  # rings, 4 ISO 4 z cells with register prefetch
+                                  # rings, 4 ISO 4 z cells with register prefetch, 5 / 6 compact-FD
+                                  # split / segment-parallel plain tiles, 7 as 3 with the Q update
+                                  # loading its own operands
 
     @property
     def n(self):

@@ -98,14 +98,15 @@ def test_variants_bit_equal(grid):
     nx, ny, nz, model, pml, use_q, pml3d = grid
     shot = _aniso_shot(nx, ny, nz, model, pml=pml, use_q=use_q, pml3d=pml3d)
     out = {}
-    for v in (1, 3, 0):
+    variants = (1, 3, 7, 0) if use_q else (1, 3, 0)
+    for v in variants:
         p, src, rcv = _engine(shot, v)
         out[v] = _modelling(shot, p, src, rcv) + (_rtm(shot, p, src, rcv, SNAP_FP32), _rtm(shot, p, src, rcv, SNAP_C16))
         p.close()
     assert np.abs(out[1][0]).max() > 0 and np.abs(out[1][3]).max() > 0
     names = ("traces", "w1", "w0", "image fp32 snapshots", "image c16 snapshots")
     bad = []
-    for v in (3, 0):
+    for v in variants[1:]:
         for k, (a, b) in enumerate(zip(out[1], out[v])):
             if k < 3 and not np.array_equal(a, b):
                 bad.append(f"variant {v} {names[k]}: {int((a != b).sum())} cells differ")
@@ -140,3 +141,23 @@ def test_4cell_kernels_match_oracle(model, use_q):
     assert np.abs(want[0]).max() > 0
     assert rel_l2(got[0], want[0]) < 1e-4
     assert rel_l2(got[1], want[1]) < 1e-4
+
+
+@pytest.mark.parametrize("q_bf16", [False, True])
+def test_q_memory_ring_bit_equal(q_bf16):
+    """The divergence pass's TMA ring carries the Q memory (FP32 or BF16) and 1/Q
+    of its planes (variant 3 / 0); variant 7 keeps the update loading them
+    itself and variant 1 is the one-cell pass: all compute the same bits,
+    with ragged x / y / z tiles and PML tiles."""
+    shot = _aniso_shot(45, 26, 56, TTI, use_q=True, nt=70)
+    shot.spec.q_bf16 = q_bf16
+    out = {}
+    for v in (1, 7, 3, 0):
+        p, src, rcv = _engine(shot, v)
+        out[v] = _modelling(shot, p, src, rcv)
+        p.close()
+    assert np.abs(out[1][0]).max() > 0
+    for v in (7, 3, 0):
+        for k, name in enumerate(("traces", "w1", "w0")):
+            np.testing.assert_array_equal(out[v][k], out[1][k], err_msg=f"variant {v} {name}")
+
