@@ -118,17 +118,21 @@ typedef struct rtm_config {
                          drivers only (the stepwise seam calls return RTM_ERR_UNSUPPORTED) */
   int kernel_variant; /* 0: auto (FD8: 4 z cells per thread with TMA rings when nz % 4 == 0 and,
                          for VTI / TTI, the state is FP32; the autotuner picks among all FD8
-                         kernels; compact FD on a 3-D grid: the segment-parallel line solves
-                         with the PML, scaling and update fused into them, else register-streamed
-                         x / y line solves; the autotuner may pick any compact-FD form), 1: one
-                         cell per thread / plain staged tiles, 2: compact-FD x / y TMA tiles, ISO
-                         FD8 one-cell TMA plane pipeline, 3: FD8 4 z cells per thread with TMA
-                         rings, 4: ISO FD8 4 z cells per thread with register prefetch, 5:
-                         compact FD split into line solves and pointwise epilogues with
-                         register-streamed x / y lines, 6: compact FD segment-parallel with plain
-                         tile loads, 7: as 3 with the visco-acoustic update loading its Q memory
-                         itself instead of from the divergence pass's TMA ring (the 4-cell and
-                         segment-parallel variants fall back when they do not apply) */
+                         kernels; compact FD: line solves and pointwise epilogues with TMA x / y
+                         tiles when nz % 4 == 0, else register-streamed x / y lines; the
+                         autotuner may pick any compact-FD form), 1: one cell per thread / plain
+                         staged tiles, 2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane
+                         pipeline, 3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z
+                         cells per thread with register prefetch, 5: compact FD with
+                         register-streamed x / y lines, 6: compact FD segment-parallel (line
+                         solves with the PML, scaling and update fused into them) with plain tile
+                         loads, 7: as 3 with the visco-acoustic update loading its Q memory
+                         itself instead of from the divergence pass's TMA ring, 8: compact FD
+                         segment-parallel with TMA tile loads where the tensor maps can be made,
+                         9: compact FD line solves segment-parallel with each segment in
+                         registers (lines of at most 1024 points) and the pointwise epilogues
+                         (the 4-cell and segment-parallel variants fall back when they do not
+                         apply) */
   int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):
                          the gradient is divided by rho (KernelCPU::divideRho) and the divergence
                          accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes
@@ -270,7 +274,9 @@ int rtm_snapshot_offload(rtm_handle *h, int nstage);
 int rtm_snapshot_slot_bytes(rtm_handle *h, int fmt, size_t *bytes);
 /* Snapshot slot window: the loops put the snapshot of step it in slot
  * it / interval - first and skip steps whose slot falls outside
- * [0, nslots); clears the stored flags.  rtm_snapshot_setup sets it to 0.  With checkpoints
+ * [0, nslots); clears the stored flags; the imaging condition's time taper
+ * still follows the snapshot's number in the shot (slot + first).
+ * rtm_snapshot_setup sets it to 0.  With checkpoints
  * (below) a backward pass over a long shot images one segment at a time
  * from slots that hold only that segment's snapshots. */
 int rtm_snapshot_window(rtm_handle *h, int first);

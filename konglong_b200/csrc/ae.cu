@@ -177,45 +177,6 @@ __host__ __device__ __forceinline__ int morton8(int x, int y, int z) {
   return m;
 }
 
-// volume (z fastest) -> scale-normalised Morton blocks; cells outside the
-// volume are 0.  One CTA of 512 threads per block; blocks b0 .. b0+gridDim.x
-// of the (bx, by, bz) grid with bz fastest.
-__global__ void __launch_bounds__(512) blockify_k(const float *__restrict__ w, int nx, int ny, int nz, long long b0,
-                                                  float *__restrict__ blocks, float *__restrict__ scales) {
-  __shared__ float red[16];
-  const long long b = b0 + blockIdx.x;
-  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
-  const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
-  const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;  // z, x, y within the block
-  const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
-  const float v = (x < nx && y < ny && z < nz) ? w[((long long)y * nx + x) * nz + z] : 0.f;
-  float a = fabsf(v);
-  for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    a = threadIdx.x < 16 ? red[threadIdx.x] : 0.f;
-    for (int o = 8; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-    if (threadIdx.x == 0) red[0] = a;
-  }
-  __syncthreads();
-  const float s = red[0];
-  blocks[blockIdx.x * (long long)kBlock + morton8(i, j, k)] = s > 0.f ? v / s : 0.f;
-  if (threadIdx.x == 0) scales[blockIdx.x] = s;
-}
-
-// Morton blocks x scale -> volume (cells outside the volume dropped)
-__global__ void __launch_bounds__(512) unblockify_k(const float *__restrict__ blocks, const float *__restrict__ scales,
-                                                    long long b0, int nx, int ny, int nz, float *__restrict__ w) {
-  const long long b = b0 + blockIdx.x;
-  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
-  const int bz = (int)(b % nbz), bx = (int)((b / nbz) % nbx), by = (int)(b / ((long long)nbz * nbx));
-  const int k = threadIdx.x & 7, i = (threadIdx.x >> 3) & 7, j = threadIdx.x >> 6;
-  const int x = bx * 8 + i, y = by * 8 + j, z = bz * 8 + k;
-  if (x < nx && y < ny && z < nz)
-    w[((long long)y * nx + x) * nz + z] = scales[blockIdx.x] * blocks[blockIdx.x * (long long)kBlock + morton8(i, j, k)];
-}
-
 }  // namespace
 }  // namespace rtm
 
@@ -321,6 +282,198 @@ void ae_loss_grad(rtm_ae *a, int n) {
 
 constexpr int kChunkBlocks = 8192;  // blocks per encode / decode pass over a volume
 
+// ---- fused inference over a volume -------------------------------------------
+// One warp per 8^3 block, a CTA of 4 warps per 4 blocks consecutive in z (32 z
+// cells of each x / y row: 128-byte rows in and out).  The CTA stages the
+// encoder (or decoder) weights once as BF16 in shared memory; each warp runs
+// its block through the four layers with the layer outputs in shared memory
+// (BF16: the next layer's operand rounding) and writes only the latent and the
+// scale (or the decoded cells).  Each output element is the same mma.sync
+// chain over k in steps of 16 as in gemm_bf16_k, with the same operand
+// roundings, bias and activation, so the results equal the layer-by-layer
+// path bit for bit.  Rows of a layer beyond its M (8 or 1 per block) and
+// columns beyond K (8 in E1) enter the MMA as zeros.
+constexpr int kFusedWarps = 4;
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  __nv_bfloat162 v;
+  v.x = lo, v.y = hi;
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// out(m, n, v) for m < M, n < N: v = act(bias[n] + sum_k A[m][k] W[k][n]),
+// A bf16 [M][K] and W bf16 [K][N] in shared memory
+template <int M, int K, int N, bool ACT, typename Out>
+__device__ __forceinline__ void warp_layer(const __nv_bfloat16 *A, const __nv_bfloat16 *W, const float *bias,
+                                           Out out) {
+  const int lane = threadIdx.x & 31, gr = lane >> 2, t = lane & 3;
+  const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+  auto a_at = [&](int m, int k) { return (m < M && k < K) ? A[m * K + k] : z; };
+  auto b_at = [&](int k, int n) { return k < K ? W[k * N + n] : z; };
+#pragma unroll 1
+  for (int m0 = 0; m0 < M; m0 += 16) {
+#pragma unroll 1
+    for (int n0 = 0; n0 < N; n0 += 8) {
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k0 = 0; k0 < K; k0 += 16) {
+        const int r0 = m0 + gr, r1 = r0 + 8, c0 = k0 + 2 * t, c1 = c0 + 8, n = n0 + gr;
+        uint32_t a[4];
+        a[0] = pack2(a_at(r0, c0), a_at(r0, c0 + 1));
+        a[1] = pack2(a_at(r1, c0), a_at(r1, c0 + 1));
+        a[2] = pack2(a_at(r0, c1), a_at(r0, c1 + 1));
+        a[3] = pack2(a_at(r1, c1), a_at(r1, c1 + 1));
+        mma_bf16(acc, a, pack2(b_at(c0, n), b_at(c0 + 1, n)), pack2(b_at(c1, n), b_at(c1 + 1, n)));
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int m = m0 + gr + (q >= 2 ? 8 : 0), n = n0 + 2 * t + (q & 1);
+        if (m >= M) continue;
+        float v = acc[q] + bias[n];
+        if (ACT) v = v > 0.f ? v : kSlope * v;
+        out(m, n, v);
+      }
+    }
+  }
+}
+
+// weights of layers [l0, l0 + 4) as bf16 [K][N] and biases as FP32, packed in
+// layer order (w_off without the biases)
+constexpr int half_w(int l0) { return kL_K[l0] * kL_N[l0] + kL_K[l0 + 1] * kL_N[l0 + 1] + kL_K[l0 + 2] * kL_N[l0 + 2] +
+                                      kL_K[l0 + 3] * kL_N[l0 + 3]; }
+constexpr int half_b(int l0) { return kL_N[l0] + kL_N[l0 + 1] + kL_N[l0 + 2] + kL_N[l0 + 3]; }
+static_assert(half_w(0) == half_w(4), "encoder and decoder weight counts");
+
+template <int L>
+__device__ __forceinline__ void stage_layer(const float *__restrict__ p, __nv_bfloat16 *w, float *b) {
+  constexpr int kn = kL_K[L] * kL_N[L], n = kL_N[L], wo = w_off(L);
+  for (int i = threadIdx.x; i < kn; i += blockDim.x) w[i] = __float2bfloat16_rn(p[wo + i]);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = p[wo + kn + i];
+}
+template <int L0>
+__device__ __forceinline__ void stage_weights(const float *__restrict__ p, __nv_bfloat16 *w, float *b) {
+  constexpr int w1 = kL_K[L0] * kL_N[L0], w2 = w1 + kL_K[L0 + 1] * kL_N[L0 + 1],
+                w3 = w2 + kL_K[L0 + 2] * kL_N[L0 + 2];
+  constexpr int b1 = kL_N[L0], b2 = b1 + kL_N[L0 + 1], b3 = b2 + kL_N[L0 + 2];
+  stage_layer<L0>(p, w, b);
+  stage_layer<L0 + 1>(p, w + w1, b + b1);
+  stage_layer<L0 + 2>(p, w + w2, b + b2);
+  stage_layer<L0 + 3>(p, w + w3, b + b3);
+}
+
+struct __align__(16) AeEncSmem {
+  __nv_bfloat16 w[half_w(0)];
+  float b[half_b(0)];
+  float raw[kFusedWarps][kBlock];          // the blocks' cells, Morton order
+  __nv_bfloat16 x[kFusedWarps][kBlock];    // E1 input [64][8]
+  __nv_bfloat16 h1[kFusedWarps][64 * 16];  // E1 output = E2 input [8][128]
+  __nv_bfloat16 h2[kFusedWarps][8 * 16];
+  __nv_bfloat16 h3[kFusedWarps][8 * 16];   // E3 output = E4 input [1][128]
+};
+
+// grid (ceil(nbz / 4), nbx, nby): block (bz = 4 blockIdx.x + warp, bx, by)
+__global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__restrict__ p,
+                                                               const float *__restrict__ vol, int nx, int ny, int nz,
+                                                               float *__restrict__ latent, float *__restrict__ scales) {
+  __shared__ AeEncSmem s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+  const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
+  stage_weights<0>(p, s.w, s.b);
+  // 32 z x 8 x x 8 y cells: thread -> (z quad, x, y) rows of 128 bytes
+  for (int i = threadIdx.x; i < 8 * 8 * 8; i += blockDim.x) {
+    const int zq = i & 7, xi = (i >> 3) & 7, yj = i >> 6;
+    const int x = bx * 8 + xi, y = by * 8 + yj;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int zl = zq * 4 + c, z = z0 + zl;
+      const float v = (x < nx && y < ny && z < nz) ? vol[((long long)y * nx + x) * nz + z] : 0.f;
+      s.raw[zl >> 3][morton8(xi, yj, zl & 7)] = v;
+    }
+  }
+  __syncthreads();
+  const int bz = blockIdx.x * kFusedWarps + warp;
+  if (bz < nbz) {
+    float a = 0.f;
+    for (int i = lane; i < kBlock; i += 32) a = fmaxf(a, fabsf(s.raw[warp][i]));
+    for (int o = 16; o; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+    const float sc = a;
+    for (int i = lane; i < kBlock; i += 32)
+      s.x[warp][i] = __float2bfloat16_rn(sc > 0.f ? s.raw[warp][i] / sc : 0.f);
+    __syncwarp();
+    const __nv_bfloat16 *w = s.w;
+    const float *b = s.b;
+    __nv_bfloat16 *h1 = s.h1[warp], *h2 = s.h2[warp], *h3 = s.h3[warp];
+    warp_layer<64, 8, 16, true>(s.x[warp], w, b, [&](int m, int n, float v) { h1[m * 16 + n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 8 * 16, b += 16;
+    warp_layer<8, 128, 16, true>(h1, w, b, [&](int m, int n, float v) { h2[m * 16 + n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 128 * 16, b += 16;
+    warp_layer<8, 16, 16, true>(h2, w, b, [&](int m, int n, float v) { h3[m * 16 + n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 16 * 16, b += 16;
+    const long long blk = ((long long)by * nbx + bx) * nbz + bz;
+    float *lat = latent + blk * kLatent;
+    warp_layer<1, 128, 32, false>(h3, w, b, [&](int, int n, float v) { lat[n] = v; });
+    if (lane == 0) scales[blk] = sc;
+  }
+}
+
+struct __align__(16) AeDecSmem {
+  __nv_bfloat16 w[half_w(4)];
+  float b[half_b(4)];
+  __nv_bfloat16 l[kFusedWarps][32];        // D1 input [1][32]
+  __nv_bfloat16 g1[kFusedWarps][128];      // D1 output = D2 input [8][16]
+  __nv_bfloat16 g2[kFusedWarps][128];      // D2 output [8][16]
+  __nv_bfloat16 g3[kFusedWarps][8 * 128];  // D3 output = D4 input [64][16]
+  float out[kFusedWarps][kBlock];          // D4 output x scale, Morton order
+};
+
+__global__ void __launch_bounds__(32 * kFusedWarps) ae_decode_k(const float *__restrict__ p,
+                                                               const float *__restrict__ latent,
+                                                               const float *__restrict__ scales, int nx, int ny, int nz,
+                                                               float *__restrict__ vol) {
+  __shared__ AeDecSmem s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
+  const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
+  stage_weights<4>(p, s.w, s.b);
+  __syncthreads();
+  const int bz = blockIdx.x * kFusedWarps + warp;
+  if (bz < nbz) {
+    const long long blk = ((long long)by * nbx + bx) * nbz + bz;
+    s.l[warp][lane] = __float2bfloat16_rn(latent[blk * kLatent + lane]);
+    const float sc = scales[blk];
+    __syncwarp();
+    const __nv_bfloat16 *w = s.w;
+    const float *b = s.b;
+    __nv_bfloat16 *g1 = s.g1[warp], *g2 = s.g2[warp], *g3 = s.g3[warp];
+    float *o = s.out[warp];
+    warp_layer<1, 32, 128, true>(s.l[warp], w, b, [&](int, int n, float v) { g1[n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 32 * 128, b += 128;
+    warp_layer<8, 16, 16, true>(g1, w, b, [&](int m, int n, float v) { g2[m * 16 + n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 16 * 16, b += 16;
+    warp_layer<8, 16, 128, true>(g2, w, b, [&](int m, int n, float v) { g3[m * 128 + n] = __float2bfloat16_rn(v); });
+    __syncwarp();
+    w += 16 * 128, b += 128;
+    warp_layer<64, 16, 8, false>(g3, w, b, [&](int m, int n, float v) { o[m * 8 + n] = sc * v; });
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * 8 * 8; i += blockDim.x) {
+    const int zq = i & 7, xi = (i >> 3) & 7, yj = i >> 6;
+    const int x = bx * 8 + xi, y = by * 8 + yj;
+    if (x >= nx || y >= ny) continue;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int zl = zq * 4 + c, z = z0 + zl;
+      if (z < nz) vol[((long long)y * nx + x) * nz + z] = s.out[zl >> 3][morton8(xi, yj, zl & 7)];
+    }
+  }
+}
+
 }  // namespace
 
 long long ae_volume_blocks(int nx, int ny, int nz) {
@@ -330,28 +483,19 @@ long long ae_volume_blocks(int nx, int ny, int nz) {
 int ae_prepare(rtm_ae *a) { return ae_reserve(a, kChunkBlocks, false); }
 
 // volume -> latents [nb][32] + scales [nb] (device), on stream st
+// (the fused kernel)
 int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, float *latent, float *scales, cudaStream_t st) {
-  const long long nb = ae_volume_blocks(nx, ny, nz);
-  if (int rc = ae_reserve(a, kChunkBlocks, false)) return rc;
-  for (long long b0 = 0; b0 < nb; b0 += kChunkBlocks) {
-    const int n = (int)std::min<long long>(kChunkBlocks, nb - b0);
-    blockify_k<<<n, 512, 0, st>>>(w, nx, ny, nz, b0, a->x0, scales + b0);
-    ae_forward(a, n, a->x0, 0, 4, false, st);
-    cudaMemcpyAsync(latent + b0 * kLatent, a->y[3], (size_t)n * kLatent * 4, cudaMemcpyDeviceToDevice, st);
-  }
+  const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
+  if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
+  ae_encode_k<<<grid, 32 * kFusedWarps, 0, st>>>(a->p, w, nx, ny, nz, latent, scales);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
-
-// latents + scales -> volume (device), on stream st
+// latents + scales -> volume (device), on stream st (the fused kernel)
 int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, int ny, int nz, float *w,
                   cudaStream_t st) {
-  const long long nb = ae_volume_blocks(nx, ny, nz);
-  if (int rc = ae_reserve(a, kChunkBlocks, false)) return rc;
-  for (long long b0 = 0; b0 < nb; b0 += kChunkBlocks) {
-    const int n = (int)std::min<long long>(kChunkBlocks, nb - b0);
-    ae_forward(a, n, latent + b0 * kLatent, 4, kLayers, false, st);
-    unblockify_k<<<n, 512, 0, st>>>(a->y[kLayers - 1], scales + b0, b0, nx, ny, nz, w);
-  }
+  const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
+  if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
+  ae_decode_k<<<grid, 32 * kFusedWarps, 0, st>>>(a->p, latent, scales, nx, ny, nz, w);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 

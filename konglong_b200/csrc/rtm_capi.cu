@@ -147,8 +147,10 @@ struct Engine {
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
   int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile (the split
                     // pipeline: line solves + pointwise epilogues); 3 / 4 the segment-parallel
-                    // fused pipeline with TMA / plain tile loads
+                    // fused pipeline with TMA / plain tile loads; 5 the split pipeline with the
+                    // register-resident segment solve on every axis
   int cfd_seg_ok = 0;  // the segment-parallel pipeline applies (engine CFD, 3-D, lines fit)
+  int cfd_reg_ok = 0;  // the register-resident segment solve applies (cfd_xy 5: lines <= kCfdRegMaxN)
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -369,12 +371,20 @@ static int yseg_iso4(Engine *h) {
 // responses to unit entering states y_{b-1-k}, gb = their segment-local back
 // substitutions, hb = backward responses to unit entering states f_{e+k}.
 // FP64 recurrences on the FP32 factors the kernels use.
-static void cfd_seg_tables(int n, const std::vector<float> &lm, const std::vector<float> &bu,
-                           const std::vector<float> &rd, int &nseg, int &seglen, std::vector<float> &hf,
-                           std::vector<float> &gb, std::vector<float> &hb) {
+static void cfd_seg_layout(int n, int &nseg, int &seglen) {
   seglen = ((n + 7) / 8 + 7) / 8 * 8;
   nseg = (n + seglen - 1) / seglen;
   if (nseg > 1 && n - (nseg - 1) * seglen < 8) nseg--;
+}
+// the register-resident solve: segments of at most 64 rows, as even as the
+// line allows (the last one >= 17 rows when there are several)
+static void cfd_reg_layout(int n, int &nseg, int &seglen) {
+  nseg = (n + 63) / 64;
+  seglen = (n + nseg - 1) / nseg;
+}
+static void cfd_seg_tables(int n, const std::vector<float> &lm, const std::vector<float> &bu,
+                           const std::vector<float> &rd, int nseg, int seglen, std::vector<float> &hf,
+                           std::vector<float> &gb, std::vector<float> &hb) {
   hf.assign(4 * (size_t)n, 0.f), gb.assign(4 * (size_t)n, 0.f), hb.assign(4 * (size_t)n, 0.f);
   // back substitution of y over rows [b, e) with f_{e..e+3} given in f[e-b ..]
   auto back = [&](int b, int e, const std::vector<double> &y, std::vector<double> &f) {
@@ -490,6 +500,10 @@ static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out)
     return;
   }
   // CFD_BATCH: the divergence-pass plan from iswitch (above): plan 1 for TTI
+  if (h->cfd_xy == 5) {
+    launch_cfd_deriv_reg(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
+    return;
+  }
   if (axis != DZ && h->cfd_xy == 0) {
     launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
     return;
@@ -780,7 +794,7 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
     launch_fused_io(io, h->w1, d.nx, d.ny, d.nz, h->st);
   }
   TRY(check_launch(h, "fused_io"));
-  if (h->cfd_xy >= 3) return cfd_seg_step(h, mode, q);
+  if (h->cfd_xy == 3 || h->cfd_xy == 4) return cfd_seg_step(h, mode, q);
   {
     KScope k(h, RTM_K_CFD_Z);
     cfd_deriv(h, DZ, 0, h->w1, h->pz);
@@ -918,8 +932,10 @@ static FusedIo io_image(Engine *h, int slot) {
   io.ic = 1;
   io.src = slot_dev(h, slot);
   io.image = h->image, io.comp = h->comp;
-  io.use_t = slot < (int)h->taper_t.size();
-  io.tscale = io.use_t ? h->taper_t[slot] : 1.f;
+  // the time taper follows the snapshot's place in the shot, not its slot
+  const int snap = slot + h->slot0;
+  io.use_t = snap >= 0 && snap < (int)h->taper_t.size();
+  io.tscale = io.use_t ? h->taper_t[snap] : 1.f;
   io.taper_z = h->taper_z;
   io.ex = h->ic_edge ? h->ex : h->one_x;
   io.ey = h->ic_edge ? h->ey : h->one_y;
@@ -1525,16 +1541,21 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
         CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f, {}};
         for (int k = 0; k < 60; k++) pd.a[k] = am[k];
         cfd_constant_run(nn[a], lm, bu, rd, pd);
-        {  // segment layout and correction tables of the segment-parallel solve
+        // segment layouts and correction tables of the segment-parallel solves
+        for (int reg = 0; reg < 2; reg++) {
+          int nseg, seglen;
+          if (reg) cfd_reg_layout(nn[a], nseg, seglen);
+          else cfd_seg_layout(nn[a], nseg, seglen);
           std::vector<float> hf, gb, hb;
-          cfd_seg_tables(nn[a], lm, bu, rd, pd.nseg, pd.seglen, hf, gb, hb);
+          cfd_seg_tables(nn[a], lm, bu, rd, nseg, seglen, hf, gb, hb);
           float *dhf, *dgb, *dhb;
           if ((rc = h->alloc(dhf, hf.size())) || (rc = h->alloc(dgb, gb.size())) || (rc = h->alloc(dhb, hb.size())))
             return fail(rc);
           cudaMemcpy(dhf, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice);
           cudaMemcpy(dgb, gb.data(), gb.size() * 4, cudaMemcpyHostToDevice);
           cudaMemcpy(dhb, hb.data(), hb.size() * 4, cudaMemcpyHostToDevice);
-          pd.hf = dhf, pd.gb = dgb, pd.hb = dhb;
+          if (reg) pd.rnseg = nseg, pd.rseglen = seglen, pd.rhf = dhf, pd.rgb = dgb, pd.rhb = dhb;
+          else pd.nseg = nseg, pd.seglen = seglen, pd.hf = dhf, pd.gb = dgb, pd.hb = dhb;
         }
         h->cfd[a][s] = pd;
       }
@@ -1600,14 +1621,21 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   // BF16 rows of the Q-memory tensor maps need nz % 8 == 0 (16-byte strides)
   h->qring_ok = c->kernel_variant != 7 && (!c->q_bf16 || d->nz % 8 == 0);
   h->cfd_tma = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && tma_supported(d->nz);
-  // compact FD on 3-D grids whose lines fit a tile: the segment-parallel fused
-  // pipeline by default (kernel_variant 0; 6 forces its plain-load form); 5
-  // and 1 / 2 select the split pipeline (streamed, plain or TMA x / y tiles)
+  // compact FD: the split pipeline (line solves + pointwise epilogues) with TMA
+  // x / y tiles by default (register-streamed lines without tensor maps), the
+  // faster form on the 512x512x400 workload; 5 / 1 / 2 force its streamed /
+  // plain / TMA x / y lines.  On 3-D grids whose lines fit a tile, 8 selects
+  // the segment-parallel fused pipeline (TMA tile loads where the tensor maps
+  // can be made) and 6 its plain-load form; the autotuner tries both forms.
   h->cfd_seg_ok = c->engine == RTM_ENGINE_CFD && d->ny > 1 && d->nx <= cfd_seg_max_n(DX) &&
                   d->ny <= cfd_seg_max_n(DY) && d->nz <= cfd_seg_max_n(DZ) && cfd_seg_init() == 0;
-  if (c->kernel_variant == 0) h->cfd_xy = h->cfd_seg_ok ? (h->cfd_tma ? 3 : 4) : 0;
+  h->cfd_reg_ok = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && d->nx <= kCfdRegMaxN &&
+                  d->ny <= kCfdRegMaxN && d->nz <= kCfdRegMaxN;
+  if (c->kernel_variant == 0) h->cfd_xy = h->cfd_tma ? 1 : 0;
+  else if (c->kernel_variant == 9 && h->cfd_reg_ok) h->cfd_xy = 5;
   else if (c->kernel_variant == 5) h->cfd_xy = 0;
   else if (c->kernel_variant == 6 && h->cfd_seg_ok) h->cfd_xy = 4;
+  else if (c->kernel_variant == 8 && h->cfd_seg_ok) h->cfd_xy = h->cfd_tma ? 3 : 4;
   else h->cfd_xy = c->kernel_variant == 2 && h->cfd_tma ? 1 : 2;
   cudaGetLastError();
   CK(cudaMemset(h->dflag, 0, sizeof(int)));
@@ -2394,6 +2422,7 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
       if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 3});
       cands.push_back({0, 0, 0, h->tma_shape, h->tx, 4});
     }
+    if (h->cfd_reg_ok) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 5});
     cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
     if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
   }

@@ -44,9 +44,10 @@ class PropSpec:
     q_bf16: bool = False          # Q memory variables stored as bfloat16
     kernel_variant: int = 0       # 0 auto, 1 one cell per thread / plain tiles, 2 TMA (CFD x/y tiles,
                                   # ISO one-cell plane pipeline), 3 FD8 4 z cells per thread with TMA
-                                  # rings, 4 ISO 4 z cells with register prefetch, 5 / 6 compact-FD
-                                  # split / segment-parallel plain tiles, 7 as 3 with the Q update
-                                  # loading its own operands
+                                  # rings, 4 ISO 4 z cells with register prefetch, 5 compact FD with
+                                  # streamed x / y lines, 6 / 8 compact FD segment-parallel with
+                                  # plain / TMA tile loads, 7 as 3 with the Q update loading its own
+                                  # operands, 9 compact FD with register-resident segment line solves
 
     @property
     def n(self):

@@ -300,7 +300,7 @@ public:
     if (cfg.engine == CFD || cfg.engine == CFDB) {
       if (cfg.engine == CFDB) cfg.pml3d = 0;  // Boundary::applyX/Y/Z damp along their own axis only
       cfdx.build(nx, dx);
-      cfdy.build(ny, dy);
+      if (ny > 1) cfdy.build(ny, dy);  // a 2-D grid has no y lines (no y derivative is taken)
       cfdz.build(nz, dz);
     }
     if (spectral()) {

@@ -170,3 +170,39 @@ def test_ablation_at_equal_bytes(data):
     assert err["trained"] < 0.9 * err["untrained"]
     assert err["trained"] < 0.9 * err["zero"]
     assert err["naive 16:1"] < err["trained"]
+
+
+def test_fused_volume_codec_equals_layered(data):
+    """The fused encode / decode kernels that the snapshot store uses (one
+    warp per block, the layers in shared memory) give the bits of the
+    layer-by-layer GEMM path: the latents and scales of a device volume equal
+    rtm_ae_reconstruct's on the host-blocked volume, and the decoded volume
+    equals that reconstruction times the scales; partial blocks at every face
+    included."""
+    import torch
+    from konglong_b200 import _lib
+    train, _ = data
+    ae = AE.AutoEncoder(seed=5)
+    ae.fit(train, steps=300, batch=256, lr=3e-3)
+    rng = np.random.default_rng(3)
+    L = _lib.lib()
+    for shape in [(19, 27, 45), (16, 24, 64), (8, 9, 70)]:
+        ny, nx, nz = shape
+        w = (rng.standard_normal(shape) * np.linspace(0.1, 3.0, nz)).astype(np.float32)
+        w[:, :, 5] = 0.0
+        b, sc = AE.volume_to_blocks(w)
+        rec, lat = ae.reconstruct(b)
+        nb = b.shape[0]
+        dv = torch.from_numpy(w).cuda()
+        dl = torch.zeros(nb * 32, device="cuda")
+        ds = torch.zeros(nb, device="cuda")
+        out = torch.zeros_like(dv)
+        _lib.check(L.rtm_ae_compress_volume(ae.a, dv.data_ptr(), nx, ny, nz, dl.data_ptr(), ds.data_ptr(), None),
+                   "rtm_ae_compress_volume")
+        _lib.check(L.rtm_ae_decompress_volume(ae.a, dl.data_ptr(), ds.data_ptr(), nx, ny, nz, out.data_ptr(), None),
+                   "rtm_ae_decompress_volume")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(ds.cpu().numpy(), sc)
+        np.testing.assert_array_equal(dl.cpu().numpy().reshape(nb, 32), lat)
+        np.testing.assert_array_equal(out.cpu().numpy(), AE.blocks_to_volume(rec, sc, shape))
+    ae.close()

@@ -1,5 +1,8 @@
-"""The segment-parallel compact-FD pipeline (engine CFD on 3-D grids, the
-default form) against the FP64 oracle and the split pipeline.
+"""The segment-parallel compact-FD solves against the FP64 oracle and the
+split pipeline: the fused pipeline (engine CFD on 3-D grids, kernel_variant
+8, or 6 with plain tile loads) and the register-resident segment line solves
+under the pointwise epilogues (kernel_variant 9, every axis, also 2-D grids
+and the Derivative path).
 
 Its line solves run each segment of a line from zero entering states and
 correct with the carried states, so its FP32 rounding differs from the
@@ -18,6 +21,9 @@ from oracle import pyoracle as O
 from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
+
+SEG = 8  # kernel_variant: the segment-parallel pipeline (TMA tile loads where possible)
+REG = 9  # kernel_variant: register-resident segment line solves + epilogues
 
 
 def _inputs(model, shape, seed, pml=9):
@@ -53,10 +59,12 @@ def _steps(x, spec, model, w0, w1, n):
 # several segments per axis with a last segment longer than the others, ragged
 # 32-wide z tiles; TMA tile loads for (70, 45, 52) (nz % 4 == 0), plain loads
 # for (33, 130, 17)
+@pytest.mark.parametrize("variant", [SEG, REG])
 @pytest.mark.parametrize("model", [ISO, VTI, TTI])
 @pytest.mark.parametrize("shape", [(70, 45, 52), (33, 130, 17)])
-def test_operator_steps_within_the_conditioning_bound(model, shape):
+def test_operator_steps_within_the_conditioning_bound(model, shape, variant):
     spec, m, w0, w1 = _inputs(model, shape, seed=30 + model, pml=6 if shape[2] < 24 else 9)
+    spec.kernel_variant = variant
     got = _steps(Propagator(spec), spec, m, w0, w1, 3)
     ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 3)
     exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 3)
@@ -66,10 +74,10 @@ def test_operator_steps_within_the_conditioning_bound(model, shape):
 
 
 def test_tma_and_plain_tile_loads_bit_equal():
-    """Variant 0 (TMA tile loads) and 6 (plain loads) run the same arithmetic."""
+    """Variant 8 (TMA tile loads) and 6 (plain loads) run the same arithmetic."""
     shot = W.vti_cfd(scale=0.2, nt=40)
     out = []
-    for variant in (0, 6):
+    for variant in (SEG, 6):
         s = shot.spec
         s.kernel_variant = variant
         p = Propagator(s)
@@ -83,8 +91,9 @@ def test_tma_and_plain_tile_loads_bit_equal():
     np.testing.assert_array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("variant", [SEG, REG])
 @pytest.mark.parametrize("case", ["tti_q", "iso"])
-def test_modelling_traces_vs_fp64(case):
+def test_modelling_traces_vs_fp64(case, variant):
     """Receiver traces of compact-FD shots: TTI + Q (the Q update in the fused x
     kernel) and ISO through the first-derivative path.  The TTI model is
     untilted: the reference's compact-FD TTI step grows without bound in tilted
@@ -101,6 +110,7 @@ def test_modelling_traces_vs_fp64(case):
         shot.eps = shot.dl = None
     nts = 150
     s = shot.spec
+    s.kernel_variant = variant
     if s.use_q:
         cq0, cq, wq = W.q_coefficients(s.dt, shot.fpeak)
     res = []
@@ -122,13 +132,14 @@ def test_modelling_traces_vs_fp64(case):
     assert rel_l2(got, exact) < 2 * spread + 1e-5, (rel_l2(got, exact), spread)
 
 
-def test_split_pipeline_agrees():
+@pytest.mark.parametrize("variant", [SEG, REG])
+def test_split_pipeline_agrees(variant):
     """Variant 5 (split pipeline: sequential line solves and pointwise
-    epilogues) and the default segment-parallel pipeline give the same shot to
-    within their FP32 rounding differences."""
+    epilogues) and the segment-parallel solves give the same shot to within
+    their FP32 rounding differences."""
     shot = W.vti_cfd(scale=0.15, nt=80)
     out = []
-    for variant in (0, 5):
+    for variant in (variant, 5):
         s = shot.spec
         s.kernel_variant = variant
         p = Propagator(s)
@@ -141,3 +152,35 @@ def test_split_pipeline_agrees():
         out.append(p.get(FIELD_W1))
     assert np.abs(out[1]).max() > 0
     assert rel_l2(out[0], out[1]) < 1e-3
+
+
+@pytest.mark.parametrize("nz", [400, 512, 130, 65, 20])
+def test_register_solve_lines_within_the_conditioning_bound(nz):
+    """The register-resident segment solve on lines of 1 to 8 segments (short
+    last segments, one-sided rows in the first and last segment) and a grid
+    larger in x and y: one operator step of the compact-FD VTI engine against
+    the FP64 oracle, x lines of 400, y lines of 96, z lines of nz."""
+    spec, m, w0, w1 = _inputs(VTI, (400, 96, nz), seed=7, pml=6)
+    spec.kernel_variant = REG
+    got = _steps(Propagator(spec), spec, m, w0, w1, 1)
+    ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 1)
+    exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 1)
+    spread = rel_l2(ref32, exact)
+    assert rel_l2(got, exact) < 2 * spread + 1e-6, (rel_l2(got, exact), spread)
+
+
+def test_register_solve_derivative_path_and_2d():
+    """The Derivative path (CFD_BATCH) and a 2-D grid (no y lines) on the
+    register-resident solves, against the FP64 oracle."""
+    for shape, engine in [((70, 45, 52), 4), ((90, 1, 75), 1)]:
+        spec, m, w0, w1 = _inputs(VTI, shape, seed=11, pml=6)
+        spec.engine = engine
+        if shape[1] == 1:
+            spec.nbnd = (6, 6, 0, 0, 6, 6)  # no y faces on a 2-D grid
+        spec.kernel_variant = REG
+        got = _steps(Propagator(spec), spec, m, w0, w1, 2)
+        ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 2)
+        exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 2)
+        spread = rel_l2(ref32, exact)
+        assert rel_l2(got, exact) < 2 * spread + 1e-6, (shape, engine, rel_l2(got, exact), spread)
+
