@@ -128,9 +128,7 @@ typedef struct rtm_config {
                          solves with the PML, scaling and update fused into them) with plain tile
                          loads, 7: as 3 with the visco-acoustic update loading its Q memory
                          itself instead of from the divergence pass's TMA ring, 8: compact FD
-                         segment-parallel with TMA tile loads where the tensor maps can be made,
-                         9: compact FD line solves segment-parallel with each segment in
-                         registers (lines of at most 1024 points) and the pointwise epilogues
+                         segment-parallel with TMA tile loads where the tensor maps can be made
                          (the 4-cell and segment-parallel variants fall back when they do not
                          apply) */
   int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):

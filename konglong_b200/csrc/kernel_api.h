@@ -205,10 +205,6 @@ struct CfdPlanDev {
   // value to unit entering backward states (zero where a segment has none)
   int nseg, seglen;
   const float *hf, *gb, *hb;
-  // the same for the register-resident segment solve: rnseg (<= 16) segments
-  // of rseglen (<= 64) rows, the last one the remainder
-  int rnseg, rseglen;
-  const float *rhf, *rgb, *rhb;
 };
 // one-time attribute set-up of the compact-FD kernels (outside any capture)
 int cfd_init();
@@ -219,11 +215,6 @@ void cfd_tma_box(int n, int *R, int *nb);
 // TMA tile kernel (null: plain loads and stores); err receives wait timeouts.
 void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                       const CUtensorMap *tin, const CUtensorMap *tout, int *err, cudaStream_t st);
-// raw derivative along axis by the register-resident segment solve (lines of
-// at most 1024 points)
-void launch_cfd_deriv_reg(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
-                          cudaStream_t st);
-constexpr int kCfdRegMaxN = 1024;
 // x / y derivative by the register-streamed kernel (no shared memory)
 void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                              cudaStream_t st);

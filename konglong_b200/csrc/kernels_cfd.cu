@@ -739,15 +739,12 @@ void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, flo
   else cfd_stream_k<kStreamDWide, long long><<<blocks, 128, 0, st>>>(p, in, out, nz, es, other, ntask);
 }
 
-int cfd_reg_init();
-
 int cfd_init() {
   const int mx = 227 * 1024;
   bool ok = cudaFuncSetAttribute(cfd_lines_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
-  ok = ok && cfd_reg_init() == 0;
   return ok ? 0 : -1;
 }
 
@@ -1364,230 +1361,6 @@ size_t seg_smem_strided(int n, bool tma) {
 size_t seg_smem_z(int n) { return kSegHdr + (size_t)32 * (n + 1) * sizeof(float); }
 
 }  // namespace
-
-// ============================================================================
-// Segment-parallel line solve with each segment held in registers.
-//
-// A CTA takes 32 lines (lane = line) and cuts them into p.rnseg segments of
-// p.rseglen rows, one warp each.  A warp loads its rows with a 5-row halo on
-// either side into registers, forms the right-hand sides in place, runs the
-// forward elimination and the back substitution from zero entering states
-// (the particular solutions), trades its four end values of each pass with
-// the other warps through shared memory, and corrects every row with the
-// carried states (the algebra of the segment-parallel solve above: the two
-// scans and f_i = fp_i + gb[i] . S_j + hb[i] . T_j).  Only those end values
-// pass through shared memory, so a tile stays resident for one segment's
-// worth of work instead of a whole line's: x / y lines are read from and
-// written to global memory directly (32 z columns per row, 128-byte rows);
-// z lines are staged through a [32][n + 1] shared tile so that their loads
-// and stores stay coalesced.  The result is the raw derivative D in, as from
-// the sequential kernels, to within FP32 rounding.
-// ============================================================================
-namespace {
-
-constexpr int kRS = 64;      // rows of a segment, at most
-constexpr int kRSMax = 16;   // segments (warps) per tile
-
-struct RegSegSmem {
-  float endf[kRSMax][4][32];  // yp_{e-1} .. yp_{e-4}
-  float endb[kRSMax][4][32];  // fp_b .. fp_{b+3}
-  float sin[kRSMax][4][32];   // S_j
-};
-
-// rows [b, b + len) of this lane's line: ld(i) reads row i, st(i, v) writes
-// it; both are called with rows in increasing order (ld from max(b - 5, 0),
-// st from b), so they may walk a pointer
-template <typename LD, typename ST>
-__device__ __forceinline__ void reg_seg_solve(const CfdPlanDev &p, RegSegSmem &ss, LD ld, ST st) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n = p.n;
-  const int b = warp * p.rseglen, len = min(p.rseglen, n - b);
-  float w[kRS + 10];
-#pragma unroll
-  for (int k = 0; k < kRS + 10; k++) {
-    const int i = b - 5 + k;
-    w[k] = (k < len + 10 && i >= 0 && i < n) ? ld(i) : 0.f;
-  }
-  // right-hand sides in place: w[k] = (A x)_{b+k}, one-sided rows at the ends
-  // (banmul_dev_z_c, bgprtm/FdEngine_cfd.cpp:304-327)
-  const float a55 = p.a[55], a56 = p.a[56], a57 = p.a[57], a58 = p.a[58], a59 = p.a[59];
-#pragma unroll
-  for (int k = 0; k < kRS; k++) {
-    if (k < len) {
-      const int i = b + k;
-      float v = 0.f;
-      if (i >= 5 && i < n - 5) {
-        v = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
-            a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
-      } else if (i < 5) {
-#pragma unroll
-        for (int j = 0; j < 11; j++)
-          if (j >= 5 - i) v = v + p.a[j * 5 + i] * w[k + j];
-      } else {
-        const int t = n - i;
-#pragma unroll
-        for (int j = 0; j < 11; j++)
-          if (j < t + 5) v = v - p.a[t + 49 - 5 * j] * w[k + j];
-      }
-      w[k] = v;
-    }
-  }
-  // forward elimination from a zero entering state
-  {
-    const float4 *__restrict__ lm = reinterpret_cast<const float4 *>(p.lm);
-    const float4 mc = make_float4(p.lmc[0], p.lmc[1], p.lmc[2], p.lmc[3]);
-    float y1 = 0.f, y2 = 0.f, y3 = 0.f, y4 = 0.f;
-#pragma unroll
-    for (int k = 0; k < kRS; k++) {
-      if (k < len) {
-        const int i = b + k;
-        const float4 m = (i >= p.c0 && i <= p.c1) ? mc : __ldg(lm + i);
-        float v = w[k];
-        v = v - m.w * y4;
-        v = v - m.z * y3;
-        v = v - m.y * y2;
-        v = v - m.x * y1;
-        y4 = y3, y3 = y2, y2 = y1, y1 = v;
-        w[k] = v;
-      }
-    }
-    ss.endf[warp][0][lane] = y1, ss.endf[warp][1][lane] = y2;
-    ss.endf[warp][2][lane] = y3, ss.endf[warp][3][lane] = y4;
-  }
-  // back substitution from a zero entering state
-  {
-    const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
-    const float4 uc = make_float4(p.buc[0], p.buc[1], p.buc[2], p.buc[3]);
-    float z1 = 0.f, z2 = 0.f, z3 = 0.f, z4 = 0.f;
-#pragma unroll
-    for (int k = kRS - 1; k >= 0; k--) {
-      if (k < len) {
-        const int i = b + k;
-        const bool c = i >= p.c0 && i <= p.c1;
-        const float4 u = c ? uc : __ldg(bu4 + i);
-        const float r = c ? p.rdc : __ldg(p.rdiag + i);
-        float v = w[k];
-        v = v - u.w * z4;
-        v = v - u.z * z3;
-        v = v - u.y * z2;
-        v = v - u.x * z1;
-        v = v * r;
-        z4 = z3, z3 = z2, z2 = z1, z1 = v;
-        w[k] = v;
-      }
-    }
-    ss.endb[warp][0][lane] = z1, ss.endb[warp][1][lane] = z2;
-    ss.endb[warp][2][lane] = z3, ss.endb[warp][3][lane] = z4;
-  }
-  __syncthreads();
-  // forward states entering this segment, then the backward ones
-  float sv[4] = {0.f, 0.f, 0.f, 0.f}, tv[4] = {0.f, 0.f, 0.f, 0.f};
-  {
-    const float4 *__restrict__ hf = reinterpret_cast<const float4 *>(p.rhf);
-    for (int k = 0; k < warp; k++) {
-      const int ek = (k + 1) * p.rseglen;
-      float ns[4];
-#pragma unroll
-      for (int m = 0; m < 4; m++) ns[m] = dot4_acc(ss.endf[k][m][lane], __ldg(hf + ek - 1 - m), sv);
-#pragma unroll
-      for (int m = 0; m < 4; m++) sv[m] = ns[m];
-    }
-#pragma unroll
-    for (int m = 0; m < 4; m++) ss.sin[warp][m][lane] = sv[m];
-  }
-  __syncthreads();
-  const float4 *__restrict__ gb = reinterpret_cast<const float4 *>(p.rgb);
-  const float4 *__restrict__ hb = reinterpret_cast<const float4 *>(p.rhb);
-  for (int k = p.rnseg - 1; k > warp; k--) {
-    const int bk = k * p.rseglen;
-    float sk[4], nt[4];
-#pragma unroll
-    for (int m = 0; m < 4; m++) sk[m] = ss.sin[k][m][lane];
-#pragma unroll
-    for (int m = 0; m < 4; m++)
-      nt[m] = dot4_acc(dot4_acc(ss.endb[k][m][lane], __ldg(gb + bk + m), sk), __ldg(hb + bk + m), tv);
-#pragma unroll
-    for (int m = 0; m < 4; m++) tv[m] = nt[m];
-  }
-#pragma unroll
-  for (int k = 0; k < kRS; k++)
-    if (k < len) st(b + k, dot4_acc(dot4_acc(w[k], __ldg(gb + b + k), sv), __ldg(hb + b + k), tv));
-}
-
-// x / y lines: tile = 32 z columns (blockIdx.x) of the line set blockIdx.y,
-// element i of line (z) l at base + l + i * es, staged through shared memory
-// [n][32] by coalesced 128-byte rows (the registers then read it at fixed
-// offsets)
-template <typename Off>
-__global__ void __launch_bounds__(32 * kRSMax, 1) cfd_reg_strided_k(const CfdPlanDev p, const float *__restrict__ in,
-                                                                   float *__restrict__ out, int nz, long long es,
-                                                                   long long other) {
-  extern __shared__ __align__(16) float zt[];
-  __shared__ RegSegSmem ss;
-  const int n = p.n, lane = threadIdx.x & 31, nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
-  const int iz = blockIdx.x * 32 + lane;
-  const bool act = iz < nz;
-  const long long base = (long long)blockIdx.y * other + min(iz, nz - 1);
-  const Off e = (Off)es;
-  for (int i = warp; i < n; i += nw) zt[i * 32 + lane] = __ldcs(in + base + (Off)i * e);
-  __syncthreads();
-  float *L = zt + lane;
-  reg_seg_solve(
-      p, ss, [&](int i) { return L[i * 32]; }, [&](int i, float v) { L[i * 32] = v; });
-  __syncthreads();
-  if (act)
-    for (int i = warp; i < n; i += nw) __stcs(out + base + (Off)i * e, zt[i * 32 + lane]);
-}
-
-// z lines (contiguous): 32 lines staged through shared memory [l][n + 1]
-__global__ void __launch_bounds__(32 * kRSMax, 1) cfd_reg_z_k(const CfdPlanDev p, const float *__restrict__ in,
-                                                             float *__restrict__ out, long long nlines) {
-  extern __shared__ __align__(16) float zt[];
-  __shared__ RegSegSmem ss;
-  const int n = p.n, st = n + 1, lane = threadIdx.x & 31, nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
-  const long long l0 = (long long)blockIdx.x * 32;
-  const int nl = (int)min(32LL, nlines - l0);
-  for (int l = warp; l < nl; l += nw)
-    for (int i = lane; i < n; i += 32) zt[l * st + i] = __ldcs(in + (l0 + l) * n + i);
-  __syncthreads();
-  float *L = zt + lane * st;
-  reg_seg_solve(
-      p, ss, [&](int i) { return L[i]; }, [&](int i, float v) { L[i] = v; });
-  __syncthreads();
-  for (int l = warp; l < nl; l += nw)
-    for (int i = lane; i < n; i += 32) __stcs(out + (l0 + l) * n + i, zt[l * st + i]);
-}
-
-}  // namespace
-
-void launch_cfd_deriv_reg(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
-                          cudaStream_t st) {
-  const dim3 block(32 * p.rnseg);
-  if (axis == DZ) {
-    const long long nlines = (long long)nx * ny;
-    cfd_reg_z_k<<<(unsigned)((nlines + 31) / 32), block, (size_t)32 * (nz + 1) * sizeof(float), st>>>(p, in, out,
-                                                                                                     nlines);
-    return;
-  }
-  const long long nxz = (long long)nx * nz;
-  const dim3 grid((nz + 31) / 32, axis == DX ? ny : nx);
-  const long long es = axis == DX ? nz : nxz, other = axis == DX ? nxz : nz;
-  const size_t smem = (size_t)32 * p.n * sizeof(float);
-  // 32-bit element offsets along a line when they cannot overflow
-  if ((long long)p.n * es < (1LL << 31))
-    cfd_reg_strided_k<unsigned><<<grid, block, smem, st>>>(p, in, out, nz, es, other);
-  else
-    cfd_reg_strided_k<long long><<<grid, block, smem, st>>>(p, in, out, nz, es, other);
-}
-
-int cfd_reg_init() {
-  const int mx = 227 * 1024 - (int)sizeof(RegSegSmem);
-  bool ok = cudaFuncSetAttribute(cfd_reg_z_k, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
-  ok = ok && cudaFuncSetAttribute(cfd_reg_strided_k<unsigned>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) ==
-                 cudaSuccess;
-  ok = ok && cudaFuncSetAttribute(cfd_reg_strided_k<long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) ==
-                 cudaSuccess;
-  return ok ? 0 : -1;
-}
 
 int cfd_seg_max_n(int axis) {
   const size_t cap = 227 * 1024;

@@ -147,10 +147,8 @@ struct Engine {
   int cfd_tma = 0;  // tensor maps of the volume can be made (nz % 4 == 0)
   int cfd_xy = 0;   // compact-FD x / y kernel: 0 streamed, 1 TMA tile, 2 plain tile (the split
                     // pipeline: line solves + pointwise epilogues); 3 / 4 the segment-parallel
-                    // fused pipeline with TMA / plain tile loads; 5 the split pipeline with the
-                    // register-resident segment solve on every axis
+                    // fused pipeline with TMA / plain tile loads
   int cfd_seg_ok = 0;  // the segment-parallel pipeline applies (engine CFD, 3-D, lines fit)
-  int cfd_reg_ok = 0;  // the register-resident segment solve applies (cfd_xy 5: lines <= kCfdRegMaxN)
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -376,12 +374,6 @@ static void cfd_seg_layout(int n, int &nseg, int &seglen) {
   nseg = (n + seglen - 1) / seglen;
   if (nseg > 1 && n - (nseg - 1) * seglen < 8) nseg--;
 }
-// the register-resident solve: segments of at most 64 rows, as even as the
-// line allows (the last one >= 17 rows when there are several)
-static void cfd_reg_layout(int n, int &nseg, int &seglen) {
-  nseg = (n + 63) / 64;
-  seglen = (n + nseg - 1) / nseg;
-}
 static void cfd_seg_tables(int n, const std::vector<float> &lm, const std::vector<float> &bu,
                            const std::vector<float> &rd, int nseg, int seglen, std::vector<float> &hf,
                            std::vector<float> &gb, std::vector<float> &hb) {
@@ -500,10 +492,6 @@ static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out)
     return;
   }
   // CFD_BATCH: the divergence-pass plan from iswitch (above): plan 1 for TTI
-  if (h->cfd_xy == 5) {
-    launch_cfd_deriv_reg(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
-    return;
-  }
   if (axis != DZ && h->cfd_xy == 0) {
     launch_cfd_deriv_stream(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, h->st);
     return;
@@ -1541,21 +1529,17 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
         CfdPlanDev pd{nn[a], dbu, dbl, dam, drd, dlm, 1, 0, {0, 0, 0, 0}, {0, 0, 0, 0}, 0.f, {}};
         for (int k = 0; k < 60; k++) pd.a[k] = am[k];
         cfd_constant_run(nn[a], lm, bu, rd, pd);
-        // segment layouts and correction tables of the segment-parallel solves
-        for (int reg = 0; reg < 2; reg++) {
-          int nseg, seglen;
-          if (reg) cfd_reg_layout(nn[a], nseg, seglen);
-          else cfd_seg_layout(nn[a], nseg, seglen);
+        {  // segment layout and correction tables of the segment-parallel solve
           std::vector<float> hf, gb, hb;
-          cfd_seg_tables(nn[a], lm, bu, rd, nseg, seglen, hf, gb, hb);
+          cfd_seg_layout(nn[a], pd.nseg, pd.seglen);
+          cfd_seg_tables(nn[a], lm, bu, rd, pd.nseg, pd.seglen, hf, gb, hb);
           float *dhf, *dgb, *dhb;
           if ((rc = h->alloc(dhf, hf.size())) || (rc = h->alloc(dgb, gb.size())) || (rc = h->alloc(dhb, hb.size())))
             return fail(rc);
           cudaMemcpy(dhf, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice);
           cudaMemcpy(dgb, gb.data(), gb.size() * 4, cudaMemcpyHostToDevice);
           cudaMemcpy(dhb, hb.data(), hb.size() * 4, cudaMemcpyHostToDevice);
-          if (reg) pd.rnseg = nseg, pd.rseglen = seglen, pd.rhf = dhf, pd.rgb = dgb, pd.rhb = dhb;
-          else pd.nseg = nseg, pd.seglen = seglen, pd.hf = dhf, pd.gb = dgb, pd.hb = dhb;
+          pd.hf = dhf, pd.gb = dgb, pd.hb = dhb;
         }
         h->cfd[a][s] = pd;
       }
@@ -1629,10 +1613,7 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   // can be made) and 6 its plain-load form; the autotuner tries both forms.
   h->cfd_seg_ok = c->engine == RTM_ENGINE_CFD && d->ny > 1 && d->nx <= cfd_seg_max_n(DX) &&
                   d->ny <= cfd_seg_max_n(DY) && d->nz <= cfd_seg_max_n(DZ) && cfd_seg_init() == 0;
-  h->cfd_reg_ok = (c->engine == RTM_ENGINE_CFD || c->engine == RTM_ENGINE_CFDB) && d->nx <= kCfdRegMaxN &&
-                  d->ny <= kCfdRegMaxN && d->nz <= kCfdRegMaxN;
   if (c->kernel_variant == 0) h->cfd_xy = h->cfd_tma ? 1 : 0;
-  else if (c->kernel_variant == 9 && h->cfd_reg_ok) h->cfd_xy = 5;
   else if (c->kernel_variant == 5) h->cfd_xy = 0;
   else if (c->kernel_variant == 6 && h->cfd_seg_ok) h->cfd_xy = 4;
   else if (c->kernel_variant == 8 && h->cfd_seg_ok) h->cfd_xy = h->cfd_tma ? 3 : 4;
@@ -2422,7 +2403,6 @@ int rtm_autotune(rtm_handle *h, int steps, int *choice) {
       if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 3});
       cands.push_back({0, 0, 0, h->tma_shape, h->tx, 4});
     }
-    if (h->cfd_reg_ok) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 5});
     cands.push_back({0, 0, 0, h->tma_shape, h->tx, 0});
     if (h->cfd_tma) cands.push_back({0, 0, 0, h->tma_shape, h->tx, 1});
   }

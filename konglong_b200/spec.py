@@ -47,7 +47,7 @@ class PropSpec:
                                   # rings, 4 ISO 4 z cells with register prefetch, 5 compact FD with
                                   # streamed x / y lines, 6 / 8 compact FD segment-parallel with
                                   # plain / TMA tile loads, 7 as 3 with the Q update loading its own
-                                  # operands, 9 compact FD with register-resident segment line solves
+                                  # operands
 
     @property
     def n(self):

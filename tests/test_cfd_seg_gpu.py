@@ -1,8 +1,6 @@
-"""The segment-parallel compact-FD solves against the FP64 oracle and the
-split pipeline: the fused pipeline (engine CFD on 3-D grids, kernel_variant
-8, or 6 with plain tile loads) and the register-resident segment line solves
-under the pointwise epilogues (kernel_variant 9, every axis, also 2-D grids
-and the Derivative path).
+"""The segment-parallel compact-FD pipeline (engine CFD on 3-D grids,
+kernel_variant 8, or 6 with plain tile loads) against the FP64 oracle and the
+split pipeline.
 
 Its line solves run each segment of a line from zero entering states and
 correct with the carried states, so its FP32 rounding differs from the
@@ -23,7 +21,6 @@ from tests.conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 SEG = 8  # kernel_variant: the segment-parallel pipeline (TMA tile loads where possible)
-REG = 9  # kernel_variant: register-resident segment line solves + epilogues
 
 
 def _inputs(model, shape, seed, pml=9):
@@ -59,12 +56,11 @@ def _steps(x, spec, model, w0, w1, n):
 # several segments per axis with a last segment longer than the others, ragged
 # 32-wide z tiles; TMA tile loads for (70, 45, 52) (nz % 4 == 0), plain loads
 # for (33, 130, 17)
-@pytest.mark.parametrize("variant", [SEG, REG])
 @pytest.mark.parametrize("model", [ISO, VTI, TTI])
 @pytest.mark.parametrize("shape", [(70, 45, 52), (33, 130, 17)])
-def test_operator_steps_within_the_conditioning_bound(model, shape, variant):
+def test_operator_steps_within_the_conditioning_bound(model, shape):
     spec, m, w0, w1 = _inputs(model, shape, seed=30 + model, pml=6 if shape[2] < 24 else 9)
-    spec.kernel_variant = variant
+    spec.kernel_variant = SEG
     got = _steps(Propagator(spec), spec, m, w0, w1, 3)
     ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 3)
     exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 3)
@@ -91,9 +87,8 @@ def test_tma_and_plain_tile_loads_bit_equal():
     np.testing.assert_array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("variant", [SEG, REG])
 @pytest.mark.parametrize("case", ["tti_q", "iso"])
-def test_modelling_traces_vs_fp64(case, variant):
+def test_modelling_traces_vs_fp64(case):
     """Receiver traces of compact-FD shots: TTI + Q (the Q update in the fused x
     kernel) and ISO through the first-derivative path.  The TTI model is
     untilted: the reference's compact-FD TTI step grows without bound in tilted
@@ -110,7 +105,7 @@ def test_modelling_traces_vs_fp64(case, variant):
         shot.eps = shot.dl = None
     nts = 150
     s = shot.spec
-    s.kernel_variant = variant
+    s.kernel_variant = SEG
     if s.use_q:
         cq0, cq, wq = W.q_coefficients(s.dt, shot.fpeak)
     res = []
@@ -132,14 +127,13 @@ def test_modelling_traces_vs_fp64(case, variant):
     assert rel_l2(got, exact) < 2 * spread + 1e-5, (rel_l2(got, exact), spread)
 
 
-@pytest.mark.parametrize("variant", [SEG, REG])
-def test_split_pipeline_agrees(variant):
+def test_split_pipeline_agrees():
     """Variant 5 (split pipeline: sequential line solves and pointwise
-    epilogues) and the segment-parallel solves give the same shot to within
+    epilogues) and the segment-parallel pipeline give the same shot to within
     their FP32 rounding differences."""
     shot = W.vti_cfd(scale=0.15, nt=80)
     out = []
-    for variant in (variant, 5):
+    for variant in (SEG, 5):
         s = shot.spec
         s.kernel_variant = variant
         p = Propagator(s)
@@ -154,33 +148,18 @@ def test_split_pipeline_agrees(variant):
     assert rel_l2(out[0], out[1]) < 1e-3
 
 
-@pytest.mark.parametrize("nz", [400, 512, 130, 65, 20])
-def test_register_solve_lines_within_the_conditioning_bound(nz):
-    """The register-resident segment solve on lines of 1 to 8 segments (short
-    last segments, one-sided rows in the first and last segment) and a grid
-    larger in x and y: one operator step of the compact-FD VTI engine against
-    the FP64 oracle, x lines of 400, y lines of 96, z lines of nz."""
-    spec, m, w0, w1 = _inputs(VTI, (400, 96, nz), seed=7, pml=6)
-    spec.kernel_variant = REG
-    got = _steps(Propagator(spec), spec, m, w0, w1, 1)
-    ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 1)
-    exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 1)
-    spread = rel_l2(ref32, exact)
-    assert rel_l2(got, exact) < 2 * spread + 1e-6, (rel_l2(got, exact), spread)
 
-
-def test_register_solve_derivative_path_and_2d():
-    """The Derivative path (CFD_BATCH) and a 2-D grid (no y lines) on the
-    register-resident solves, against the FP64 oracle."""
-    for shape, engine in [((70, 45, 52), 4), ((90, 1, 75), 1)]:
+def test_default_pipeline_2d_grid_and_derivative_path():
+    """The default compact-FD pipeline on a 2-D grid (no y lines, no y faces)
+    and on the Derivative path (CFD_BATCH), against the FP64 oracle."""
+    for shape, engine in [((90, 1, 75), 1), ((70, 45, 52), 4)]:
         spec, m, w0, w1 = _inputs(VTI, shape, seed=11, pml=6)
         spec.engine = engine
         if shape[1] == 1:
-            spec.nbnd = (6, 6, 0, 0, 6, 6)  # no y faces on a 2-D grid
-        spec.kernel_variant = REG
+            spec.nbnd = (6, 6, 0, 0, 6, 6)
         got = _steps(Propagator(spec), spec, m, w0, w1, 2)
         ref32 = _steps(O.Oracle(spec), spec, m, w0, w1, 2)
         exact = _steps(O.Oracle(spec, double=True), spec, m, w0, w1, 2)
         spread = rel_l2(ref32, exact)
+        assert np.abs(exact).max() > 0
         assert rel_l2(got, exact) < 2 * spread + 1e-6, (shape, engine, rel_l2(got, exact), spread)
-
