@@ -88,9 +88,9 @@ def kernel_alg_bytes(spec, m):
 # over to the full grid.  Each entry records the SHA-256 prefix of the kernel
 # source it was captured on; when the source has changed since, the figure no
 # longer describes the kernel that runs and the bench reports traffic as null.
-MEASURED_DRAM_B_PER_CELL = {"vti_cfd": {"cfd_div_epilogue": 36.98, "cfd_grad_epilogue": 40.64,
-                                        "cfd_x": 6.87, "cfd_y": 6.87}}
-MEASURED_DRAM_SOURCE = {"vti_cfd": ("konglong_b200/csrc/kernels_cfd.cu", "cdae83a8a550fc67")}
+MEASURED_DRAM_B_PER_CELL = {"vti_cfd": {"cfd_div_epilogue": 38.0, "cfd_grad_epilogue": 38.8,
+                                        "cfd_x": 6.75, "cfd_y": 6.83, "cfd_z": 6.83}}
+MEASURED_DRAM_SOURCE = {"vti_cfd": ("konglong_b200/csrc/kernels_cfd.cu", "740b6d93b94baba7")}
 
 
 def measured_traffic_current(workload):
@@ -343,14 +343,17 @@ def run_cuda(args, rank, world):
 
 
 def run_small_shots(args, ranks):
-    """Batched small-shot ISO workload (64 seeded shots, grids 96-256 per axis,
-    500-2000 steps, receivers every step): every shot's full modelling run,
-    once per shot with its own CUDA-graph loop (per-shot launches) and once
-    for all shots together (one persistent launch per step, batched I/O).
-    Metric: shots per second of the batched run."""
+    """Batched small-shot workload (64 seeded shots, grids 96-256 per axis,
+    500-2000 steps, receivers every step; ISO, or VTI with per-layer Thomsen
+    parameters for small_shots_vti): every shot's full modelling run, once per
+    shot with its own CUDA-graph loop (per-shot launches) and once for all
+    shots together (persistent launches per step over every shot, batched
+    I/O).  Metric: shots per second of the batched run."""
     from konglong_b200 import workloads as W
     from konglong_b200.propagator import Batch, Propagator, spread_coeffs
-    shots = W.small_shots(nshots=64, seed=4 + ranks.rank)
+    from konglong_b200.spec import ISO, VTI
+    vti = args.workload == "small_shots_vti"
+    shots = W.small_shots(nshots=64, seed=4 + ranks.rank, model=VTI if vti else ISO)
 
     def setup(sh):
         s = sh.spec
@@ -391,7 +394,8 @@ def run_small_shots(args, ranks):
     wall = R.max_over_ranks(ranks, time.perf_counter() - t0, device="cuda")
     b.close()
     m = [sum(2 * w / n for w, n in zip(sh.spec.nbnd[0::2], (sh.spec.nx, sh.spec.ny, sh.spec.nz))) for sh in shots]
-    alg = sum((16.0 + 16.0 * mm) * sh.spec.n * sh.nt for mm, sh in zip(m, shots))
+    core, pml = (24.0, 48.0) if vti else (16.0, 16.0)
+    alg = sum((core + pml * mm) * sh.spec.n * sh.nt for mm, sh in zip(m, shots))
     peak, peak_src = 6650.0, "fallback"
     try:
         peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
@@ -404,16 +408,21 @@ def run_small_shots(args, ranks):
             "per_shot": {"value": len(shots) / (per_ms * 1e-3), "ms": per_ms,
                          "what": "the same shots, one rtm_modelling (own CUDA-graph loop) per shot"},
             "gpts": R.aggregate_gpts(ranks.world, cell_steps, 1, ms),
-            "roofline": {"bound": "hbm", "kernel": "iso_fd8_batch (whole batched step)", "achieved": achieved,
+            "roofline": {"bound": "hbm",
+                         "kernel": ("grad_fd8_batch + div_fd8_batch" if vti else "iso_fd8_batch") +
+                                   " (whole batched step)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": peak_src,
-                         "alg_bytes": "16 + 16 m per cell-step (ISO FD8), m = PML slab fraction per shot"},
+                         "alg_bytes": ("24 + 48 m per cell-step (VTI FD8)" if vti else
+                                       "16 + 16 m per cell-step (ISO FD8)") + ", m = PML slab fraction per shot"},
             "e2e": {"value": nshots / wall, "unit": "shots/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(tr_bytes / max(nts)),
                     "what": "batched modelling through the C ABI, all receiver traces read back; wall clock"},
             "clocks": clk.summary(), "tuned_shape": choice,
-            "config": {"workload": "small_shots: 64 ISO FD8 shots, grids uniform 96-256 per axis, "
-                                   "500-2000 steps, 3-5 layers, 10-25 Hz Ricker, 16x16 receivers, PML 16",
+            "config": {"workload": f"{args.workload}: 64 {'VTI' if vti else 'ISO'} FD8 shots, grids uniform "
+                                   "96-256 per axis, 500-2000 steps, 3-5 layers"
+                                   f"{' (epsilon 0-0.2, delta 0-0.1 per layer, CFL dt)' if vti else ''}, "
+                                   "10-25 Hz Ricker, 16x16 receivers, PML 16",
                        "cell_steps": cell_steps, "shots": nshots}}
 
 
@@ -576,6 +585,56 @@ def run_rtm_shot(args, ranks):
     return {"forms": res, "clocks": clk_all, "ntrain": ntrain, "shot": shot}
 
 
+def run_ae_codec(args, ranks):
+    """The learned compressor's fused encoder and decoder on one snapshot of
+    the C3 grid (640 x 640 x 512 at scale 1): K timed calls each after W
+    warm-up calls, CUDA events on the default stream.  Reports ms per
+    snapshot, TFLOP/s (61440 FLOP per 8^3 block each way: the four layers'
+    MACs x 2) against bf16_tflops_sustained, and GB/s of the volume and the
+    codes read and written."""
+    import torch
+    from konglong_b200 import _lib
+    from konglong_b200 import compressor as AE
+    from konglong_b200 import workloads as W
+    s = W.tti_q(scale=args.scale, nt=8).spec
+    nx, ny, nz = s.nx, s.ny, s.nz
+    L = _lib.lib()
+    ae = AE.AutoEncoder(seed=5)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    w = torch.randn(ny, nx, nz, device="cuda", generator=g)
+    nb = ((nx + 7) // 8) * ((ny + 7) // 8) * ((nz + 7) // 8)
+    lat = torch.zeros(nb * AE.LATENT, device="cuda", dtype=torch.bfloat16)
+    sc = torch.zeros(nb, device="cuda")
+    out = torch.zeros_like(w)
+    enc = lambda: _lib.check(L.rtm_ae_compress_volume(ae.a, w.data_ptr(), nx, ny, nz, lat.data_ptr(), sc.data_ptr(),
+                                                       None), "rtm_ae_compress_volume")
+    dec = lambda: _lib.check(L.rtm_ae_decompress_volume(ae.a, lat.data_ptr(), sc.data_ptr(), nx, ny, nz,
+                                                         out.data_ptr(), None), "rtm_ae_decompress_volume")
+    res = {}
+    with ClockSampler(ranks.local_rank) as clk:
+        for name, f in (("encode", enc), ("decode", dec)):
+            for _ in range(args.warmup):
+                f()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(args.steps):
+                f()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            res[name] = {"ms": ms, "tflops": nb * 61440 / (ms * 1e-3) / 1e12,
+                         "gbs": (s.n * 4 + nb * (AE.LATENT * 2 + 4)) / (ms * 1e-3) / 1e9}
+    ae.close()
+    peak = {}
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    return {"res": res, "clocks": clk.summary(), "grid": [nx, ny, nz], "blocks": nb,
+            "tflops_peak": peak.get("bf16_tflops_sustained", 1400.0), "hbm_peak": peak.get("hbm_gbs", 6650.0)}
+
+
 def cpu_baseline(shot, max_seconds=20.0):
     """The reference's own CPU kernels (oracle/_ref) on the full grid, all host
     threads, a bounded number of time steps."""
@@ -644,7 +703,7 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="vti_cfd",
                     choices=["vti_cfd", "iso128", "tti_q", "vti_fd8", "iso512", "vti_r2c", "vti_r2r", "small_shots",
-                             "tti_q_rtm"])
+                             "small_shots_vti", "tti_q_rtm", "ae_codec"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="grid scale of the workload (1.0 = the configuration the metric is quoted on; "
                          "smaller values are for profiler captures)")
@@ -697,7 +756,7 @@ def main():
             torch.cuda.set_device(0)
         except Exception:
             pass
-    if args.workload == "small_shots":
+    if args.workload in ("small_shots", "small_shots_vti"):
         r = run_small_shots(args, ranks)
         if rank == 0:
             line = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "n_gpus": world,
@@ -707,6 +766,25 @@ def main():
                     "speedup_vs_per_shot": r["value"] / r["per_shot"]["value"] if world == 1 else None,
                     "gpts": r["gpts"], "roofline": r["roofline"], "cpu_baseline": None, "e2e": r["e2e"],
                     "clocks": r["clocks"], "tuned_shape": r["tuned_shape"]}
+            print(json.dumps(line), flush=True)
+        R.finish(ranks)
+        return
+    if args.workload == "ae_codec":
+        r = run_ae_codec(args, ranks)
+        if rank == 0:
+            e = r["res"]["encode"]
+            line = {"metric": "learned snapshot codec ms per snapshot (encode)", "value": e["ms"], "unit": "ms",
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "bf16 operands, fp32 accumulation",
+                    "data": "synthetic (random volume)",
+                    "config": {"workload": "ae_codec: fused encoder / decoder of one {}x{}x{} snapshot ({} 8^3 blocks)"
+                               .format(*r["grid"], r["blocks"])},
+                    "codec": r["res"],
+                    "roofline": {"bound": "hbm", "achieved": e["gbs"], "peak": r["hbm_peak"], "unit": "GB/s",
+                                 "frac": e["gbs"] / r["hbm_peak"], "traffic": None,
+                                 "tensor": {"achieved_tflops": e["tflops"], "peak_tflops": r["tflops_peak"],
+                                            "frac": e["tflops"] / r["tflops_peak"]}},
+                    "clocks": r["clocks"]}
             print(json.dumps(line), flush=True)
         R.finish(ranks)
         return

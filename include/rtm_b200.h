@@ -253,7 +253,7 @@ int rtm_get_traces(rtm_handle *h, float *dst);
  * (RTM_SNAP_FP32 uncompressed, RTM_SNAP_C16 = the reference's COMPRESS_16
  * codec, bit-exact, RTM_SNAP_FP16S = FP16 with a per-y-slab scale,
  * RTM_SNAP_AE = the learned compressor attached by rtm_set_compressor:
- * 32 latent floats + 1 scale per 8^3 block, 15.5:1). */
+ * 64 BF16 latent values + 1 scale per 8^3 block, 15.5:1). */
 int rtm_snapshot_setup(rtm_handle *h, int fmt, int nslots);
 /* Store w0 into slot (WaveFieldCompress::compress + CacheFile write). */
 int rtm_snapshot_store(rtm_handle *h, int slot);
@@ -366,7 +366,7 @@ int rtm_c16_compress_noalloc(const float *d_in, unsigned short *d_out, int nx, i
 int rtm_last_loop_ms(rtm_handle *h, float *ms);
 /* ---- Learned snapshot compressor ------------------------------------------
  * A 3-D convolutional autoencoder on 8^3-cell blocks (4 encoder + 4 decoder
- * layers, 16 channels, 512 cells -> 32 latent floats + the block's max |w|),
+ * layers, 16 channels, 512 cells -> 64 BF16 latent values + the block's max |w|),
  * trained and run on the GPU with BF16 tensor-core GEMMs and FP32
  * accumulation.  Replaces WaveFieldCompress (bgprtm/WaveFieldCompress.cpp
  * compress/uncompress) for the forward-wavefield snapshots when attached to a
@@ -387,13 +387,14 @@ int rtm_ae_loss_grad(rtm_ae *a, const float *blocks, int n, float *loss, float *
 /* One Adam step (learning rate lr) on a batch of n host blocks; returns the
  * batch loss before the step. */
 int rtm_ae_train_step(rtm_ae *a, const float *blocks, int n, float lr, float *loss);
-/* Reconstruction [n][512] (and latents [n][32] when latent != NULL). */
+/* Reconstruction [n][512] (and the FP32 latents [n][64] when latent != NULL). */
 int rtm_ae_reconstruct(rtm_ae *a, const float *blocks, int n, float *out, float *latent);
-/* Device volume (z fastest) <-> latents [nb][32] + scales [nb], nb = the 8^3
- * blocks covering the volume (zero-padded); on `stream` (NULL = default). */
-int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, float *d_latent, float *d_scales,
+/* Device volume (z fastest) <-> latents [nb][64] as bfloat16 (128 bytes per
+ * block) + scales [nb] (float), nb = the 8^3 blocks covering the volume
+ * (zero-padded); on `stream` (NULL = default). */
+int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, void *d_latent, float *d_scales,
                            void *stream);
-int rtm_ae_decompress_volume(rtm_ae *a, const float *d_latent, const float *d_scales, int nx, int ny, int nz,
+int rtm_ae_decompress_volume(rtm_ae *a, const void *d_latent, const float *d_scales, int nx, int ny, int nz,
                              float *d_vol, void *stream);
 /* Attach a compressor to a handle (same device) for RTM_SNAP_AE snapshots. */
 int rtm_set_compressor(rtm_handle *h, rtm_ae *a);
@@ -408,11 +409,13 @@ int rtm_set_compressor(rtm_handle *h, rtm_ae *a);
 int rtm_set_compressor_fallback(rtm_handle *h, float tau, float max_fraction);
 
 /* ---- Batched small shots (many shots, one persistent launch per step) ----
- * A batch steps several ISO FD8 handles (no Q) of different grids and step
- * counts together: each time step is one persistent kernel over the column
- * tiles of every active shot, one batched injection and one batched
- * extraction launch, and the time loop runs as CUDA graphs.  Each handle must
- * have its model, injection (and, optionally, extraction) set and be reset.
+ * A batch steps several FD8 handles (no Q) of different grids and step counts
+ * together: all ISO (each time step one persistent kernel over the column
+ * tiles of every active shot) or all VTI, or all TTI (each step two persistent
+ * kernels, the gradient and the divergence pass of the one-cell kernels; no
+ * density, FP32 state), then one batched injection and one batched extraction
+ * launch; the time loop runs as CUDA graphs.  Each handle must have its model,
+ * injection (and, optionally, extraction) set and be reset.
  * No reference counterpart: bgprtm runs one shot per process
  * (bgprtm/Propagator.cpp:1054-1260 per shot). */
 typedef struct rtm_batch rtm_batch;

@@ -1,7 +1,8 @@
 """Learned snapshot compressor: host side of the rtm_ae_* C ABI.
 
 A 3-D convolutional autoencoder on 8^3-cell wavefield blocks (4 encoder +
-4 decoder layers, 16 channels, 512 cells -> 32 latent floats + the block's
+4 decoder layers, 16 channels, 512 cells -> 64 latent values (stored as BF16,
+the decoder's operand precision) + the block's
 max |w|, 15.5:1), trained on blocks of the engine's own forward wavefields and
 run inside the RTM loop as snapshot format RTM_SNAP_AE.  Training and
 inference run in the library's BF16 tensor-core kernels (FP32 accumulation,
@@ -13,9 +14,9 @@ import numpy as np
 
 from . import _lib
 
-LAYERS = [(8, 16, 64, True), (128, 16, 8, True), (16, 16, 8, True), (128, 32, 1, False),
-          (32, 128, 1, True), (16, 16, 8, True), (16, 128, 8, True), (16, 8, 64, False)]  # K, N, rows/block, act
-LATENT = 32
+LAYERS = [(8, 16, 64, True), (128, 16, 8, True), (16, 16, 8, True), (128, 64, 1, False),
+          (64, 128, 1, True), (16, 16, 8, True), (16, 128, 8, True), (16, 8, 64, False)]  # K, N, rows/block, act
+LATENT = 64
 BLOCK = 512
 
 

@@ -8,12 +8,15 @@
 //   E1  2^3 patch conv, stride 2   1 -> 16 ch   rows/block 64  K   8 N  16  leaky ReLU
 //   E2  2^3 patch conv, stride 2  16 -> 16 ch              8   K 128 N  16  leaky ReLU
 //   E3  pointwise                 16 -> 16 ch              8   K  16 N  16  leaky ReLU
-//   E4  2^3 patch conv, stride 2  16 -> 32 ch (latent)     1   K 128 N  32  linear
-//   D1  transposed 2^3, stride 2  32 -> 16 ch              1   K  32 N 128  leaky ReLU
+//   E4  2^3 patch conv, stride 2  16 -> 64 ch (latent)     1   K 128 N  64  linear
+//   D1  transposed 2^3, stride 2  64 -> 16 ch              1   K  64 N 128  leaky ReLU
 //   D2  pointwise                 16 -> 16 ch              8   K  16 N  16  leaky ReLU
 //   D3  transposed 2^3, stride 2  16 -> 16 ch              8   K  16 N 128  leaky ReLU
 //   D4  transposed 2^3, stride 2  16 ->  1 ch              64  K  16 N   8  linear
-// 512 cells -> 32 latent floats (16:1) plus the block's max |value| scale.
+// 512 cells -> 64 latent values stored as BF16 (the decoder's first GEMM rounds
+// its operand to BF16, so BF16 storage keeps everything the decoder can use:
+// 64 values in the bytes of 32 floats, 15.5:1 with the block's max |value|
+// scale).
 // GEMMs: mma.sync m16n8k16, BF16 operands (rounded from the FP32 activations
 // and FP32 master weights), FP32 accumulation.  Training: MSE loss on the
 // scale-normalised block, backward GEMMs, Adam on the FP32 master weights.
@@ -34,12 +37,12 @@ namespace rtm {
 namespace {
 
 constexpr int kLayers = 8;
-constexpr int kL_K[kLayers] = {8, 128, 16, 128, 32, 16, 16, 16};
-constexpr int kL_N[kLayers] = {16, 16, 16, 32, 128, 16, 128, 8};
+constexpr int kL_K[kLayers] = {8, 128, 16, 128, 64, 16, 16, 16};
+constexpr int kL_N[kLayers] = {16, 16, 16, 64, 128, 16, 128, 8};
 constexpr int kL_R[kLayers] = {64, 8, 8, 1, 1, 8, 8, 64};  // rows per block
 constexpr int kL_ACT[kLayers] = {1, 1, 1, 0, 1, 1, 1, 0};
 constexpr float kSlope = 0.1f;  // leaky ReLU
-constexpr int kLatent = 32;
+constexpr int kLatent = 64;
 constexpr int kBlock = 512;
 
 constexpr int w_off(int l) {
@@ -295,21 +298,27 @@ constexpr int kChunkBlocks = 8192;  // blocks per encode / decode pass over a vo
 // columns beyond K (8 in E1) enter the MMA as zeros.
 constexpr int kFusedWarps = 4;
 
-__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-  __nv_bfloat162 v;
-  v.x = lo, v.y = hi;
-  return *reinterpret_cast<uint32_t *>(&v);
-}
+// Row strides (bf16 elements) of the operands in shared memory: K + 8 for a
+// layer's transposed weights and its input rows, so that the 32-bit loads of
+// a fragment's column pairs fall in distinct banks (a row of K + 8 bf16 moves
+// the bank by 4 words: the 8 row groups x 4 column pairs of a fragment cover
+// the 32 banks once).  Rows of E1's input (K = 8) stay unpadded (4 words).
+constexpr int kpad(int k) { return k == 8 ? 8 : k + 8; }
 
 // out(m, n, v) for m < M, n < N: v = act(bias[n] + sum_k A[m][k] W[k][n]),
-// A bf16 [M][K] and W bf16 [K][N] in shared memory
-template <int M, int K, int N, bool ACT, typename Out>
-__device__ __forceinline__ void warp_layer(const __nv_bfloat16 *A, const __nv_bfloat16 *W, const float *bias,
+// A bf16 [M][LDA] and the weights transposed, Wt bf16 [N][kpad(K)], in shared
+// memory.  Each pair of adjacent columns is one 32-bit load.
+template <int M, int K, int N, int LDA, bool ACT, typename Out>
+__device__ __forceinline__ void warp_layer(const __nv_bfloat16 *A, const __nv_bfloat16 *Wt, const float *bias,
                                            Out out) {
+  constexpr int LDW = kpad(K);
   const int lane = threadIdx.x & 31, gr = lane >> 2, t = lane & 3;
-  const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
-  auto a_at = [&](int m, int k) { return (m < M && k < K) ? A[m * K + k] : z; };
-  auto b_at = [&](int k, int n) { return k < K ? W[k * N + n] : z; };
+  auto a2 = [&](int m, int k) -> uint32_t {
+    return (m < M && k < K) ? *reinterpret_cast<const uint32_t *>(A + m * LDA + k) : 0u;
+  };
+  auto b2 = [&](int k, int n) -> uint32_t {
+    return k < K ? *reinterpret_cast<const uint32_t *>(Wt + n * LDW + k) : 0u;
+  };
 #pragma unroll 1
   for (int m0 = 0; m0 < M; m0 += 16) {
 #pragma unroll 1
@@ -319,11 +328,11 @@ __device__ __forceinline__ void warp_layer(const __nv_bfloat16 *A, const __nv_bf
       for (int k0 = 0; k0 < K; k0 += 16) {
         const int r0 = m0 + gr, r1 = r0 + 8, c0 = k0 + 2 * t, c1 = c0 + 8, n = n0 + gr;
         uint32_t a[4];
-        a[0] = pack2(a_at(r0, c0), a_at(r0, c0 + 1));
-        a[1] = pack2(a_at(r1, c0), a_at(r1, c0 + 1));
-        a[2] = pack2(a_at(r0, c1), a_at(r0, c1 + 1));
-        a[3] = pack2(a_at(r1, c1), a_at(r1, c1 + 1));
-        mma_bf16(acc, a, pack2(b_at(c0, n), b_at(c0 + 1, n)), pack2(b_at(c1, n), b_at(c1 + 1, n)));
+        a[0] = a2(r0, c0);
+        a[1] = a2(r1, c0);
+        a[2] = a2(r0, c1);
+        a[3] = a2(r1, c1);
+        mma_bf16(acc, a, b2(c0, n), b2(c1, n));
       }
 #pragma unroll
       for (int q = 0; q < 4; q++) {
@@ -337,23 +346,24 @@ __device__ __forceinline__ void warp_layer(const __nv_bfloat16 *A, const __nv_bf
   }
 }
 
-// weights of layers [l0, l0 + 4) as bf16 [K][N] and biases as FP32, packed in
-// layer order (w_off without the biases)
-constexpr int half_w(int l0) { return kL_K[l0] * kL_N[l0] + kL_K[l0 + 1] * kL_N[l0 + 1] + kL_K[l0 + 2] * kL_N[l0 + 2] +
-                                      kL_K[l0 + 3] * kL_N[l0 + 3]; }
+// transposed, padded weights of a layer and of four consecutive layers
+template <int L> constexpr int wt_size() { return kL_N[L] * kpad(kL_K[L]); }
+template <int L0> constexpr int half_wt() { return wt_size<L0>() + wt_size<L0 + 1>() + wt_size<L0 + 2>() + wt_size<L0 + 3>(); }
 constexpr int half_b(int l0) { return kL_N[l0] + kL_N[l0 + 1] + kL_N[l0 + 2] + kL_N[l0 + 3]; }
-static_assert(half_w(0) == half_w(4), "encoder and decoder weight counts");
 
+// layer L's weights W[k][n] (FP32 master) into Wt[n][kpad(K)] as bf16, its biases as FP32
 template <int L>
-__device__ __forceinline__ void stage_layer(const float *__restrict__ p, __nv_bfloat16 *w, float *b) {
-  constexpr int kn = kL_K[L] * kL_N[L], n = kL_N[L], wo = w_off(L);
-  for (int i = threadIdx.x; i < kn; i += blockDim.x) w[i] = __float2bfloat16_rn(p[wo + i]);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = p[wo + kn + i];
+__device__ __forceinline__ void stage_layer(const float *__restrict__ p, __nv_bfloat16 *wt, float *b) {
+  constexpr int K = kL_K[L], N = kL_N[L], wo = w_off(L);
+  for (int i = threadIdx.x; i < K * N; i += blockDim.x) {
+    const int k = i / N, n = i % N;
+    wt[n * kpad(K) + k] = __float2bfloat16_rn(p[wo + i]);
+  }
+  for (int i = threadIdx.x; i < N; i += blockDim.x) b[i] = p[wo + K * N + i];
 }
 template <int L0>
 __device__ __forceinline__ void stage_weights(const float *__restrict__ p, __nv_bfloat16 *w, float *b) {
-  constexpr int w1 = kL_K[L0] * kL_N[L0], w2 = w1 + kL_K[L0 + 1] * kL_N[L0 + 1],
-                w3 = w2 + kL_K[L0 + 2] * kL_N[L0 + 2];
+  constexpr int w1 = wt_size<L0>(), w2 = w1 + wt_size<L0 + 1>(), w3 = w2 + wt_size<L0 + 2>();
   constexpr int b1 = kL_N[L0], b2 = b1 + kL_N[L0 + 1], b3 = b2 + kL_N[L0 + 2];
   stage_layer<L0>(p, w, b);
   stage_layer<L0 + 1>(p, w + w1, b + b1);
@@ -361,21 +371,27 @@ __device__ __forceinline__ void stage_weights(const float *__restrict__ p, __nv_
   stage_layer<L0 + 3>(p, w + w3, b + b3);
 }
 
+// input row strides: E2 reads E1's output as [8][128], E3 E2's as [8][16],
+// D2 D1's as [8][16], D3 D2's as [8][16], D4 D3's as [64][16]
+constexpr int kLdE2 = kpad(128), kLdE3 = kpad(16), kLdD2 = kpad(16), kLdD3 = kpad(16), kLdD4 = kpad(16);
+
 struct __align__(16) AeEncSmem {
-  __nv_bfloat16 w[half_w(0)];
+  __nv_bfloat16 w[half_wt<0>()];
   float b[half_b(0)];
-  float raw[kFusedWarps][kBlock];          // the blocks' cells, Morton order
-  __nv_bfloat16 x[kFusedWarps][kBlock];    // E1 input [64][8]
-  __nv_bfloat16 h1[kFusedWarps][64 * 16];  // E1 output = E2 input [8][128]
-  __nv_bfloat16 h2[kFusedWarps][8 * 16];
-  __nv_bfloat16 h3[kFusedWarps][8 * 16];   // E3 output = E4 input [1][128]
+  float raw[kFusedWarps][kBlock];           // the blocks' cells, Morton order
+  __nv_bfloat16 x[kFusedWarps][kBlock];     // E1 input [64][8]
+  __nv_bfloat16 h1[kFusedWarps][8 * kLdE2]; // E1 output = E2 input [8][128]
+  __nv_bfloat16 h2[kFusedWarps][8 * kLdE3]; // E2 output = E3 input [8][16]
+  __nv_bfloat16 h3[kFusedWarps][8 * 16];    // E3 output = E4 input [1][128]
 };
 
 // grid (ceil(nbz / 4), nbx, nby): block (bz = 4 blockIdx.x + warp, bx, by)
 __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__restrict__ p,
                                                                const float *__restrict__ vol, int nx, int ny, int nz,
-                                                               float *__restrict__ latent, float *__restrict__ scales) {
-  __shared__ AeEncSmem s;
+                                                               __nv_bfloat16 *__restrict__ latent,
+                                                               float *__restrict__ scales) {
+  extern __shared__ __align__(16) unsigned char smem_ae[];
+  AeEncSmem &s = *reinterpret_cast<AeEncSmem *>(smem_ae);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
   const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
@@ -404,37 +420,42 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__r
     const __nv_bfloat16 *w = s.w;
     const float *b = s.b;
     __nv_bfloat16 *h1 = s.h1[warp], *h2 = s.h2[warp], *h3 = s.h3[warp];
-    warp_layer<64, 8, 16, true>(s.x[warp], w, b, [&](int m, int n, float v) { h1[m * 16 + n] = __float2bfloat16_rn(v); });
+    warp_layer<64, 8, 16, 8, true>(s.x[warp], w, b, [&](int m, int n, float v) {
+      h1[(m >> 3) * kLdE2 + (m & 7) * 16 + n] = __float2bfloat16_rn(v);
+    });
     __syncwarp();
-    w += 8 * 16, b += 16;
-    warp_layer<8, 128, 16, true>(h1, w, b, [&](int m, int n, float v) { h2[m * 16 + n] = __float2bfloat16_rn(v); });
+    w += wt_size<0>(), b += 16;
+    warp_layer<8, 128, 16, kLdE2, true>(h1, w, b, [&](int m, int n, float v) {
+      h2[m * kLdE3 + n] = __float2bfloat16_rn(v);
+    });
     __syncwarp();
-    w += 128 * 16, b += 16;
-    warp_layer<8, 16, 16, true>(h2, w, b, [&](int m, int n, float v) { h3[m * 16 + n] = __float2bfloat16_rn(v); });
+    w += wt_size<1>(), b += 16;
+    warp_layer<8, 16, 16, kLdE3, true>(h2, w, b, [&](int m, int n, float v) { h3[m * 16 + n] = __float2bfloat16_rn(v); });
     __syncwarp();
-    w += 16 * 16, b += 16;
+    w += wt_size<2>(), b += 16;
     const long long blk = ((long long)by * nbx + bx) * nbz + bz;
-    float *lat = latent + blk * kLatent;
-    warp_layer<1, 128, 32, false>(h3, w, b, [&](int, int n, float v) { lat[n] = v; });
+    __nv_bfloat16 *lat = latent + blk * kLatent;
+    warp_layer<1, 128, kLatent, 128, false>(h3, w, b, [&](int, int n, float v) { lat[n] = __float2bfloat16_rn(v); });
     if (lane == 0) scales[blk] = sc;
   }
 }
 
 struct __align__(16) AeDecSmem {
-  __nv_bfloat16 w[half_w(4)];
+  __nv_bfloat16 w[half_wt<4>()];
   float b[half_b(4)];
-  __nv_bfloat16 l[kFusedWarps][32];        // D1 input [1][32]
-  __nv_bfloat16 g1[kFusedWarps][128];      // D1 output = D2 input [8][16]
-  __nv_bfloat16 g2[kFusedWarps][128];      // D2 output [8][16]
-  __nv_bfloat16 g3[kFusedWarps][8 * 128];  // D3 output = D4 input [64][16]
-  float out[kFusedWarps][kBlock];          // D4 output x scale, Morton order
+  __nv_bfloat16 l[kFusedWarps][kLatent];     // D1 input [1][kLatent]
+  __nv_bfloat16 g1[kFusedWarps][8 * kLdD2];  // D1 output = D2 input [8][16]
+  __nv_bfloat16 g2[kFusedWarps][8 * kLdD3];  // D2 output = D3 input [8][16]
+  __nv_bfloat16 g3[kFusedWarps][64 * kLdD4]; // D3 output = D4 input [64][16]
+  float out[kFusedWarps][kBlock];            // D4 output x scale, Morton order
 };
 
 __global__ void __launch_bounds__(32 * kFusedWarps) ae_decode_k(const float *__restrict__ p,
-                                                               const float *__restrict__ latent,
+                                                               const __nv_bfloat16 *__restrict__ latent,
                                                                const float *__restrict__ scales, int nx, int ny, int nz,
                                                                float *__restrict__ vol) {
-  __shared__ AeDecSmem s;
+  extern __shared__ __align__(16) unsigned char smem_ae[];
+  AeDecSmem &s = *reinterpret_cast<AeDecSmem *>(smem_ae);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
   const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
@@ -443,23 +464,29 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_decode_k(const float *__r
   const int bz = blockIdx.x * kFusedWarps + warp;
   if (bz < nbz) {
     const long long blk = ((long long)by * nbx + bx) * nbz + bz;
-    s.l[warp][lane] = __float2bfloat16_rn(latent[blk * kLatent + lane]);
+    for (int k = lane; k < kLatent; k += 32) s.l[warp][k] = latent[blk * kLatent + k];
     const float sc = scales[blk];
     __syncwarp();
     const __nv_bfloat16 *w = s.w;
     const float *b = s.b;
     __nv_bfloat16 *g1 = s.g1[warp], *g2 = s.g2[warp], *g3 = s.g3[warp];
     float *o = s.out[warp];
-    warp_layer<1, 32, 128, true>(s.l[warp], w, b, [&](int, int n, float v) { g1[n] = __float2bfloat16_rn(v); });
+    warp_layer<1, kLatent, 128, kLatent, true>(s.l[warp], w, b, [&](int, int n, float v) {
+      g1[(n >> 4) * kLdD2 + (n & 15)] = __float2bfloat16_rn(v);
+    });
     __syncwarp();
-    w += 32 * 128, b += 128;
-    warp_layer<8, 16, 16, true>(g1, w, b, [&](int m, int n, float v) { g2[m * 16 + n] = __float2bfloat16_rn(v); });
+    w += wt_size<4>(), b += 128;
+    warp_layer<8, 16, 16, kLdD2, true>(g1, w, b, [&](int m, int n, float v) {
+      g2[m * kLdD3 + n] = __float2bfloat16_rn(v);
+    });
     __syncwarp();
-    w += 16 * 16, b += 16;
-    warp_layer<8, 16, 128, true>(g2, w, b, [&](int m, int n, float v) { g3[m * 128 + n] = __float2bfloat16_rn(v); });
+    w += wt_size<5>(), b += 16;
+    warp_layer<8, 16, 128, kLdD3, true>(g2, w, b, [&](int m, int n, float v) {
+      g3[(m * 8 + (n >> 4)) * kLdD4 + (n & 15)] = __float2bfloat16_rn(v);
+    });
     __syncwarp();
-    w += 16 * 128, b += 128;
-    warp_layer<64, 16, 8, false>(g3, w, b, [&](int m, int n, float v) { o[m * 8 + n] = sc * v; });
+    w += wt_size<6>(), b += 128;
+    warp_layer<64, 16, 8, kLdD4, false>(g3, w, b, [&](int m, int n, float v) { o[m * 8 + n] = sc * v; });
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 8 * 8 * 8; i += blockDim.x) {
@@ -482,20 +509,30 @@ long long ae_volume_blocks(int nx, int ny, int nz) {
 
 int ae_prepare(rtm_ae *a) { return ae_reserve(a, kChunkBlocks, false); }
 
-// volume -> latents [nb][32] + scales [nb] (device), on stream st
+// shared-memory size of the fused encoder / decoder (beyond the 48 KB default)
+static bool ae_fused_init() {
+  return cudaFuncSetAttribute(ae_encode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeEncSmem)) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(ae_decode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeDecSmem)) ==
+             cudaSuccess;
+}
+
+// volume -> latents [nb][64] (bfloat16) + scales [nb] (device), on stream st
 // (the fused kernel)
-int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, float *latent, float *scales, cudaStream_t st) {
+int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, void *latent, float *scales, cudaStream_t st) {
   const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
   if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
-  ae_encode_k<<<grid, 32 * kFusedWarps, 0, st>>>(a->p, w, nx, ny, nz, latent, scales);
+  ae_encode_k<<<grid, 32 * kFusedWarps, sizeof(AeEncSmem), st>>>(a->p, w, nx, ny, nz,
+                                                                static_cast<__nv_bfloat16 *>(latent), scales);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 // latents + scales -> volume (device), on stream st (the fused kernel)
-int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, int ny, int nz, float *w,
+int ae_decompress(rtm_ae *a, const void *latent, const float *scales, int nx, int ny, int nz, float *w,
                   cudaStream_t st) {
   const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
   if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
-  ae_decode_k<<<grid, 32 * kFusedWarps, 0, st>>>(a->p, latent, scales, nx, ny, nz, w);
+  ae_decode_k<<<grid, 32 * kFusedWarps, sizeof(AeDecSmem), st>>>(a->p, static_cast<const __nv_bfloat16 *>(latent),
+                                                                scales, nx, ny, nz, w);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 
@@ -680,6 +717,11 @@ int rtm_ae_create(rtm_ae **out) {
     rtm_ae_destroy(a);
     return RTM_ERR_NOMEM;
   }
+  if (!rtm::ae_fused_init()) {
+    cudaGetLastError();
+    rtm_ae_destroy(a);
+    return RTM_ERR_CUDA;
+  }
   *out = a;
   return RTM_OK;
 }
@@ -748,14 +790,14 @@ int rtm_ae_reconstruct(rtm_ae *a, const float *blocks, int n, float *out, float 
   return cudaStreamSynchronize(a->st) == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 
-int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, float *d_latent, float *d_scales,
+int rtm_ae_compress_volume(rtm_ae *a, const float *d_vol, int nx, int ny, int nz, void *d_latent, float *d_scales,
                            void *stream) {
   if (!a || !d_vol || !d_latent || !d_scales || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
   cudaSetDevice(a->device);
   return rtm::ae_compress(a, d_vol, nx, ny, nz, d_latent, d_scales, (cudaStream_t)stream);
 }
 
-int rtm_ae_decompress_volume(rtm_ae *a, const float *d_latent, const float *d_scales, int nx, int ny, int nz,
+int rtm_ae_decompress_volume(rtm_ae *a, const void *d_latent, const float *d_scales, int nx, int ny, int nz,
                              float *d_vol, void *stream) {
   if (!a || !d_vol || !d_latent || !d_scales || nx < 1 || ny < 1 || nz < 1) return RTM_ERR_ARG;
   cudaSetDevice(a->device);

@@ -71,6 +71,21 @@ struct DivArgs {
   QDev q;
 };
 
+// one VTI / TTI shot of a batched two-pass step (device array): its pass
+// arguments, its two wavefield buffers (w1 = wa on even steps, as in
+// IsoBatchShot), its tile grid and y segment
+struct AnisoBatchShot {
+  GradArgs g;
+  DivArgs d;
+  float *wa, *wb;
+  int tiles_z, tiles_x, tiles_y, yseg;
+};
+constexpr int kAnisoBatchTX = 8;  // tile width of the batched two-pass kernels
+// one step (both passes) of every active VTI / TTI shot of a batch
+void launch_aniso_fd8_batch(const AnisoBatchShot *shots, const int *start, int nactive, int total, int it, int model,
+                            int ctas, cudaStream_t st);
+int aniso_batch_ctas_per_sm();
+
 // mode: 0 = operator only (w0 -= vel*L), 1 = + leapfrog update, 2 = + Q update
 void launch_iso_fd8(const IsoArgs &a, int mode, int pml3d, int tx, cudaStream_t st);
 // the same step with 4 z cells per thread (float4 rows; nz % 4 == 0), tile
@@ -324,8 +339,8 @@ void launch_nonfinite_scan(const float *w, long long n, int *flag, cudaStream_t 
 long long ae_volume_blocks(int nx, int ny, int nz);  // 8^3 blocks covering a volume
 int ae_prepare(rtm_ae *a);                           // workspace (call outside any capture)
 // volume -> latents [nb][32] + scales [nb]; latents + scales -> volume (device, stream st)
-int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, float *latent, float *scales, cudaStream_t st);
-int ae_decompress(rtm_ae *a, const float *latent, const float *scales, int nx, int ny, int nz, float *w,
+int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, void *latent, float *scales, cudaStream_t st);
+int ae_decompress(rtm_ae *a, const void *latent, const float *scales, int nx, int ny, int nz, float *w,
                   cudaStream_t st);
 
 }  // namespace rtm

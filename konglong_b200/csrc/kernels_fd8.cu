@@ -217,19 +217,17 @@ __global__ void __launch_bounds__(TZ *TX) iso_fd8_batch(const IsoBatchShot *__re
 // ---- anisotropic two-pass ----------------------------------------------------
 // One CTA per tile of the table; EDGE = false tiles hold no PML cell and are
 // compiled without the PML code (fewer registers, more resident warps).
+// The gradient pass of one column tile (z tile bz, x tile bx, planes [y0, y1))
+// reading the field w1; every thread of the CTA calls it.
 template <int TX, int MODEL, bool F16, bool EDGE>
-__global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__restrict__ tiles) {
-  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+__device__ __forceinline__ void grad_tile(const GradArgs &a, const float *__restrict__ w1, int bz, int bx, int y0,
+                                          int y1, float (&tile)[TX + 2 * R][TZ + 2 * R]) {
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
   const int tz = threadIdx.x, tx = threadIdx.y;
-  const Tile4 tl = tiles[blockIdx.x];
-  const int iz = tl.bz * TZ + tz;
-  const int ix = tl.bx * TX + tx;
-  const int y0 = tl.y0;
-  const int y1 = tl.y1;
+  const int iz = bz * TZ + tz;
+  const int ix = bx * TX + tx;
   const bool act = iz < a.nz && ix < a.nx;
   const long long col = (long long)ix * a.nz + iz;
-  const float *__restrict__ w1 = a.w1;
   const bool do_y = a.ny > 1;
   auto v1 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w1, a.h.s1, i, iy) : __ldg(w1 + i); };
 
@@ -282,6 +280,13 @@ __global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__re
   }
 }
 
+template <int TX, int MODEL, bool F16, bool EDGE>
+__global__ void __launch_bounds__(TZ *TX) grad_fd8(GradArgs a, const Tile4 *__restrict__ tiles) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  const Tile4 tl = tiles[blockIdx.x];
+  grad_tile<TX, MODEL, F16, EDGE>(a, a.w1, tl.bz, tl.bx, tl.y0, tl.y1, tile);
+}
+
 struct DivPlane {
   float pxc, pzc, zl, zh, xl, xh;
 };
@@ -307,17 +312,15 @@ __device__ __forceinline__ DivPlane fetch_div(const DivArgs &a, int iy, int ix, 
   return d;
 }
 
+// The divergence pass of one column tile reading w1 and the previous field w0,
+// which it overwrites with the new one; every thread of the CTA calls it.
 template <int TX, int MODE, bool F16, bool EDGE>
-__global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__restrict__ tiles) {
-  __shared__ float tpx[TX + 2 * R][TZ];
-  __shared__ float tpz[TX][TZ + 2 * R];
+__device__ __forceinline__ void div_tile(const DivArgs &a, const float *__restrict__ w1, float *w0, int bz, int bx,
+                                         int y0, int y1, float (&tpx)[TX + 2 * R][TZ], float (&tpz)[TX][TZ + 2 * R]) {
   const Grid3 g{a.nx, a.ny, a.nz, (long long)a.nx * a.nz};
   const int tz = threadIdx.x, tx = threadIdx.y;
-  const Tile4 tl = tiles[blockIdx.x];
-  const int iz = tl.bz * TZ + tz;
-  const int ix = tl.bx * TX + tx;
-  const int y0 = tl.y0;
-  const int y1 = tl.y1;
+  const int iz = bz * TZ + tz;
+  const int ix = bx * TX + tx;
   const bool act = iz < a.nz && ix < a.nx;
   const long long col = (long long)ix * a.nz + iz;
   const bool do_y = a.ny > 1;
@@ -330,8 +333,8 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__rest
   }
   DivPlane d0 = fetch_div<TX>(a, y0, ix, iz, g.nxz, tx, tz, act);
   DivPlane d1 = fetch_div<TX>(a, y0 + 1 < y1 ? y0 + 1 : a.ny, ix, iz, g.nxz, tx, tz, act);
-  auto v0 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w0, a.h.s0, i, iy) : a.w0[i]; };
-  auto v1 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w1, a.h.s1, i, iy) : __ldg(a.w1 + i); };
+  auto v0 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w0, a.h.s0, i, iy) : w0[i]; };
+  auto v1 = [&](long long i, int iy) -> float { return F16 ? f16v(a.h.w1, a.h.s1, i, iy) : __ldg(w1 + i); };
   float nw0 = act ? v0((long long)y0 * g.nxz + col, y0) : 0.f;
   float nvel = act ? __ldg(a.vel + (long long)y0 * g.nxz + col) : 0.f;
   float nw1 = act && MODE != 0 ? v1((long long)y0 * g.nxz + col, y0) : 0.f;
@@ -374,7 +377,7 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__rest
         a.h.w0[i] = __float2half_rn(hv);
         amax = fabsf(out);
       } else {
-        a.w0[i] = out;
+        w0[i] = out;
       }
     }
     if (F16) {  // slab max of the new field (all lanes of a warp are on plane iy)
@@ -385,6 +388,58 @@ __global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__rest
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 2 * R; k++) q[k] = q[k + 1];
+  }
+}
+
+template <int TX, int MODE, bool F16, bool EDGE>
+__global__ void __launch_bounds__(TZ *TX) div_fd8(DivArgs a, const Tile4 *__restrict__ tiles) {
+  __shared__ float tpx[TX + 2 * R][TZ];
+  __shared__ float tpz[TX][TZ + 2 * R];
+  const Tile4 tl = tiles[blockIdx.x];
+  div_tile<TX, MODE, F16, EDGE>(a, a.w1, a.w0, tl.bz, tl.bx, tl.y0, tl.y1, tpx, tpz);
+}
+
+// Many VTI / TTI shots in two persistent launches per step (gradient pass
+// over every active shot's column tiles, then the divergence pass), the work
+// items laid out as in iso_fd8_batch; every tile takes the PML code path;
+// leapfrog update (MODE 1), FP32 state.
+template <int TX, int MODEL>
+__global__ void __launch_bounds__(TZ *TX) grad_fd8_batch(const AnisoBatchShot *__restrict__ shots,
+                                                          const int *__restrict__ start, int nactive, int total,
+                                                          int it) {
+  __shared__ float tile[TX + 2 * R][TZ + 2 * R];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int lo = 0, hi = nactive - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const AnisoBatchShot &S = shots[lo];
+    const int l = w - __ldg(start + lo);
+    const int bz = l % S.tiles_z, bx = (l / S.tiles_z) % S.tiles_x, by = l / (S.tiles_z * S.tiles_x);
+    const int y0 = by * S.yseg, y1 = min(S.g.ny, y0 + S.yseg);
+    grad_tile<TX, MODEL, false, true>(S.g, (it & 1) ? S.wb : S.wa, bz, bx, y0, y1, tile);
+  }
+}
+
+template <int TX>
+__global__ void __launch_bounds__(TZ *TX) div_fd8_batch(const AnisoBatchShot *__restrict__ shots,
+                                                         const int *__restrict__ start, int nactive, int total, int it) {
+  __shared__ float tpx[TX + 2 * R][TZ];
+  __shared__ float tpz[TX][TZ + 2 * R];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int lo = 0, hi = nactive - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(start + mid) <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const AnisoBatchShot &S = shots[lo];
+    const int l = w - __ldg(start + lo);
+    const int bz = l % S.tiles_z, bx = (l / S.tiles_z) % S.tiles_x, by = l / (S.tiles_z * S.tiles_x);
+    const int y0 = by * S.yseg, y1 = min(S.d.ny, y0 + S.yseg);
+    div_tile<TX, 1, false, true>(S.d, (it & 1) ? S.wb : S.wa, (it & 1) ? S.wa : S.wb, bz, bx, y0, y1, tpx, tpz);
   }
 }
 
@@ -441,6 +496,23 @@ int iso_batch_ctas_per_sm(int tx, int pml3d) {
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, iso_fd8_batch<8, false>, TZ * 8, 0);
   }
   return std::max(1, n);
+}
+
+void launch_aniso_fd8_batch(const AnisoBatchShot *shots, const int *start, int nactive, int total, int it, int model,
+                            int ctas, cudaStream_t st) {
+  if (total <= 0 || nactive <= 0) return;
+  const unsigned grid = (unsigned)std::max(1, std::min(total, ctas));
+  const dim3 block(TZ, kAnisoBatchTX);
+  if (model == 3) grad_fd8_batch<kAnisoBatchTX, 3><<<grid, block, 0, st>>>(shots, start, nactive, total, it);
+  else grad_fd8_batch<kAnisoBatchTX, 2><<<grid, block, 0, st>>>(shots, start, nactive, total, it);
+  div_fd8_batch<kAnisoBatchTX><<<grid, block, 0, st>>>(shots, start, nactive, total, it);
+}
+
+int aniso_batch_ctas_per_sm() {
+  int a = 0, b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, grad_fd8_batch<kAnisoBatchTX, 3>, TZ * kAnisoBatchTX, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, div_fd8_batch<kAnisoBatchTX>, TZ * kAnisoBatchTX, 0);
+  return std::max(1, std::min(a, b));
 }
 
 template <int TX, bool F16, bool EDGE>

@@ -932,7 +932,7 @@ static FusedIo io_image(Engine *h, int slot) {
   return io;
 }
 
-// learned-compressor slot: latents [nb][32], then scales [nb]
+// learned-compressor slot: latents [nb][64] (bfloat16, 128 bytes per block), then scales [nb]
 static float *ae_latent(Engine *h, int slot) { return (float *)(h->snaps + (size_t)slot * h->slot_bytes); }
 static float *ae_scales(Engine *h, int slot) {
   return ae_latent(h, slot) + (size_t)ae_volume_blocks(h->d.nx, h->d.ny, h->d.nz) * 32;
@@ -1221,14 +1221,17 @@ struct rtm_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int tx = 8, yseg = 0;  // tile width, y segment (0: whole y extent)
-  rtm::IsoBatchShot *d_shots = nullptr;
+  rtm::IsoBatchShot *d_shots = nullptr;    // every shot's I/O (and ISO step) arguments
+  rtm::AnisoBatchShot *d_ashots = nullptr;  // VTI / TTI batches: the two passes' arguments
   int *d_start = nullptr;
   int cap = 0;
+  int model = RTM_ISO;  // the shots' model type (ISO: one-pass kernel; VTI / TTI: two passes)
   std::string err;
 };
 
 namespace rtm {
-// tile-shape candidates of the batched ISO kernel: {tile width, y segment (0 = whole y)}
+// tile-shape candidates of the batched kernels: {tile width, y segment (0 =
+// whole y)}; the VTI / TTI passes take those of width kAnisoBatchTX
 static const int kBatchShapes[][2] = {{8, 0}, {8, 32}, {16, 0}, {16, 32}, {8, 16}};
 static const int kBatchNShapes = 5;
 
@@ -1237,7 +1240,10 @@ static const int kBatchNShapes = 5;
 static int batch_upload(rtm_batch *b, const std::vector<int> &order, std::vector<int> &start, int &max_inj,
                         int &max_ly, int &max_ext) {
   const int n = (int)order.size();
+  const bool aniso = b->model != RTM_ISO;
+  const int tx = aniso ? kAnisoBatchTX : b->tx;
   std::vector<IsoBatchShot> hs(n);
+  std::vector<AnisoBatchShot> ha(aniso ? n : 0);
   start.assign(n + 1, 0);
   max_inj = max_ly = max_ext = 0;
   for (int k = 0; k < n; k++) {
@@ -1253,17 +1259,34 @@ static int batch_upload(rtm_batch *b, const std::vector<int> &order, std::vector
     a.io = FusedIo{};
     a.q = QDev{};
     S.wa = h->w1, S.wb = h->w0;
-    S.tiles_z = (d.nz + 31) / 32, S.tiles_x = (d.nx + b->tx - 1) / b->tx, S.tiles_y = (d.ny + a.yseg - 1) / a.yseg;
+    S.tiles_z = (d.nz + 31) / 32, S.tiles_x = (d.nx + tx - 1) / tx, S.tiles_y = (d.ny + a.yseg - 1) / a.yseg;
     S.inj = h->inj.dev(), S.ext = h->ext.dev(), S.ext_out = h->ext.out;
     S.inj.ids = nullptr, S.ext.ids = nullptr;
+    if (aniso) {  // the one-cell passes' arguments of the engine's own step (no density, no Q, FP32 state)
+      AnisoBatchShot &A = ha[k];
+      GradArgs &g = A.g;
+      g.nx = d.nx, g.ny = d.ny, g.nz = d.nz, g.yseg = a.yseg, g.pml3d = h->c.pml3d;
+      g.px = h->px, g.py = h->py, g.pz = h->pz;
+      g.eps = h->eps, g.del = h->del, g.pjx = h->pjx, g.pjy = h->pjy;
+      memcpy(g.c1x, h->c1x, sizeof g.c1x), memcpy(g.c1y, h->c1y, sizeof g.c1y), memcpy(g.c1z, h->c1z, sizeof g.c1z);
+      g.pml = pml_dev(h);
+      DivArgs &v = A.d;
+      v.nx = d.nx, v.ny = d.ny, v.nz = d.nz, v.yseg = a.yseg, v.pml3d = h->c.pml3d;
+      v.px = h->px, v.py = h->py, v.pz = h->pz, v.vel = h->vel;
+      memcpy(v.c1x, h->c1x, sizeof v.c1x), memcpy(v.c1y, h->c1y, sizeof v.c1y), memcpy(v.c1z, h->c1z, sizeof v.c1z);
+      v.pml = pml_dev(h);
+      A.wa = S.wa, A.wb = S.wb;
+      A.tiles_z = S.tiles_z, A.tiles_x = S.tiles_x, A.tiles_y = S.tiles_y, A.yseg = a.yseg;
+    }
     start[k + 1] = start[k] + S.tiles_z * S.tiles_x * S.tiles_y;
     max_inj = std::max(max_inj, h->inj.ntr), max_ly = std::max(max_ly, h->inj.ly);
     max_ext = std::max(max_ext, h->ext.ntr);
   }
   if (n > b->cap) {
-    cudaFree(b->d_shots), cudaFree(b->d_start);
-    b->d_shots = nullptr, b->d_start = nullptr, b->cap = 0;
+    cudaFree(b->d_shots), cudaFree(b->d_ashots), cudaFree(b->d_start);
+    b->d_shots = nullptr, b->d_ashots = nullptr, b->d_start = nullptr, b->cap = 0;
     if (cudaMalloc(&b->d_shots, n * sizeof(IsoBatchShot)) != cudaSuccess ||
+        (aniso && cudaMalloc(&b->d_ashots, n * sizeof(AnisoBatchShot)) != cudaSuccess) ||
         cudaMalloc(&b->d_start, (n + 1) * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       b->err = "batch table allocation failed";
@@ -1272,6 +1295,7 @@ static int batch_upload(rtm_batch *b, const std::vector<int> &order, std::vector
     b->cap = n;
   }
   if (cudaMemcpyAsync(b->d_shots, hs.data(), n * sizeof(IsoBatchShot), cudaMemcpyHostToDevice, b->st) ||
+      (aniso && cudaMemcpyAsync(b->d_ashots, ha.data(), n * sizeof(AnisoBatchShot), cudaMemcpyHostToDevice, b->st)) ||
       cudaMemcpyAsync(b->d_start, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, b->st)) {
     b->err = "batch table upload failed";
     return RTM_ERR_CUDA;
@@ -1289,12 +1313,15 @@ static int batch_run(rtm_batch *b, const std::vector<int> &order, const std::vec
   TRY(batch_upload(b, order, start, max_inj, max_ly, max_ext));
   int num_sms = 0;
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, b->device);
-  const int grid = iso_batch_ctas_per_sm(b->tx, b->pml3d) * (num_sms > 0 ? num_sms : 148);
+  const bool aniso = b->model != RTM_ISO;
+  const int grid = (aniso ? aniso_batch_ctas_per_sm() : iso_batch_ctas_per_sm(b->tx, b->pml3d)) *
+                   (num_sms > 0 ? num_sms : 148);
   const int n = (int)order.size();
   auto step = [&](int it) {
     int na = 0;
     while (na < n && nts_sorted[na] > it) na++;
-    launch_iso_fd8_batch(b->d_shots, b->d_start, na, start[na], it, b->pml3d, b->tx, grid, b->st);
+    if (aniso) launch_aniso_fd8_batch(b->d_ashots, b->d_start, na, start[na], it, b->model, grid, b->st);
+    else launch_iso_fd8_batch(b->d_shots, b->d_start, na, start[na], it, b->pml3d, b->tx, grid, b->st);
     launch_batch_inject(b->d_shots, na, max_inj, max_ly, it + it_shift, it, b->st);
     if (ntratio > 0 && it % ntratio == 0) launch_batch_extract(b->d_shots, na, max_ext, it / ntratio, it, b->st);
   };
@@ -2273,14 +2300,19 @@ int rtm_batch_create(rtm_handle *const *shots, int nshots, rtm_batch **out) {
   rtm_batch *b = new rtm_batch();
   for (int k = 0; k < nshots; k++) {
     rtm::Engine *h = shots[k];
-    if (!h || !h->model_set || !h->lap_iso() || h->c.use_q ||
+    // every shot ISO on the Laplacian kernel, or every shot FD8 VTI (or TTI) on
+    // the two passes, leapfrog without Q or density, FP32 state, one device and
+    // PML mode
+    const bool iso = h && h->lap_iso();
+    const bool aniso = h && h->c.engine == RTM_ENGINE_FD8 && h->c.model_type >= RTM_VTI && !h->c.use_rho && !h->f16;
+    if (!h || !h->model_set || !(iso || aniso) || h->c.use_q || h->c.model_type != shots[0]->c.model_type ||
         h->device != shots[0]->device || h->c.pml3d != shots[0]->c.pml3d) {
       delete b;
       return !h || !h->model_set ? RTM_ERR_STATE : RTM_ERR_UNSUPPORTED;
     }
     b->shots.push_back(h);
   }
-  b->device = shots[0]->device, b->pml3d = shots[0]->c.pml3d;
+  b->device = shots[0]->device, b->pml3d = shots[0]->c.pml3d, b->model = shots[0]->c.model_type;
   cudaSetDevice(b->device);
   if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) || cudaEventCreate(&b->ev0) ||
       cudaEventCreate(&b->ev1)) {
@@ -2296,7 +2328,7 @@ int rtm_batch_destroy(rtm_batch *b) {
   if (!b) return RTM_ERR_ARG;
   cudaSetDevice(b->device);
   if (b->st) cudaStreamSynchronize(b->st);
-  cudaFree(b->d_shots), cudaFree(b->d_start);
+  cudaFree(b->d_shots), cudaFree(b->d_ashots), cudaFree(b->d_start);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->st) cudaStreamDestroy(b->st);
@@ -2343,6 +2375,7 @@ int rtm_batch_autotune(rtm_batch *b, int steps, int *choice) {
   float best = 1e30f;
   int bi = 0;
   for (int c = 0; c < rtm::kBatchNShapes; c++) {
+    if (b->model != RTM_ISO && rtm::kBatchShapes[c][0] != rtm::kAnisoBatchTX) continue;
     b->tx = rtm::kBatchShapes[c][0], b->yseg = rtm::kBatchShapes[c][1];
     TRY(rtm::batch_run(b, order, sorted, 1, 0, 0));  // warm-up
     TRY(rtm::batch_run(b, order, sorted, steps, 0, 0));

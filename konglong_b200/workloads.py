@@ -221,30 +221,40 @@ def iso128(scale=1.0, seed=1, nt=1000):
                 fpeak=15.0, name="iso128")
 
 
-def small_shots(nshots=64, seed=4, size=(96, 256), steps=(500, 2000), nrec=16):
-    """Batched small-shot ISO workload: every shot draws its grid (each axis
+def small_shots(nshots=64, seed=4, size=(96, 256), steps=(500, 2000), nrec=16, model=ISO):
+    """Batched small-shot workload: every shot draws its grid (each axis
     uniform in `size`), step count, 3-5 flat layers between 1500 and 4500 m/s
     and a 10-25 Hz Ricker source from one seed.  10 m spacing, dt = 1 ms (inside
     the FD8 leapfrog bound at 4500 m/s), PML 16, source at the surface centre,
-    nrec x nrec receivers two cells below the top PML."""
+    nrec x nrec receivers two cells below the top PML.  model=VTI adds a
+    Thomsen epsilon in [0, 0.2] and delta in [0, 0.1] per layer, and each shot
+    takes the time step of the CFL rule (at most 1 ms), since epsilon raises
+    the horizontal velocity."""
     rng = np.random.default_rng(seed)
     shots = []
     for k in range(nshots):
         nx, ny, nz = (int(v) for v in rng.integers(size[0], size[1] + 1, 3))
         nt = int(rng.integers(steps[0], steps[1] + 1))
         pml = 16
-        spec = PropSpec(nx=nx, ny=ny, nz=nz, dx=10.0, dy=10.0, dz=10.0, dt=0.001, engine=ENGINE_FD8, model_type=ISO,
+        spec = PropSpec(nx=nx, ny=ny, nz=nz, dx=10.0, dy=10.0, dz=10.0, dt=0.001, engine=ENGINE_FD8, model_type=model,
                         nbnd=(pml,) * 6, vmax=4500.0)
         nl = int(rng.integers(3, 6))
         vals = np.sort(rng.uniform(1500.0, 4500.0, nl)).astype(np.float32)
         cuts = np.sort(rng.uniform(0.1, 0.9, nl - 1)) * nz
-        prof = vals[np.searchsorted(cuts, np.arange(nz))]
-        vel = np.ascontiguousarray(np.broadcast_to(prof, spec.shape), np.float32)
+        layer = np.searchsorted(cuts, np.arange(nz))
+        vel = np.ascontiguousarray(np.broadcast_to(vals[layer], spec.shape), np.float32)
+        eps = dl = None
+        if model == VTI:
+            ev = rng.uniform(0.0, 0.2, nl).astype(np.float32)
+            dv = np.minimum(rng.uniform(0.0, 0.1, nl), ev).astype(np.float32)
+            eps = np.ascontiguousarray(np.broadcast_to(ev[layer], spec.shape), np.float32)
+            dl = np.ascontiguousarray(np.broadcast_to(dv[layer], spec.shape), np.float32)
+            spec.dt = float(min(0.001, cfl_dt(spec, vel, eps, dl)))
         f = float(rng.uniform(10.0, 25.0))
         step_x, step_y = max(1, (nx - 2) // nrec), max(1, (ny - 2) // nrec)
         rxx, ryy = np.meshgrid(1 + step_x * np.arange(nrec), 1 + step_y * np.arange(nrec), indexing="xy")
         rcv = np.stack([rxx.ravel(), ryy.ravel(), np.full(rxx.size, pml + 2.0)], 1).astype(np.float32)
-        shots.append(Shot(spec, nt, vel, wavelet=ricker(f, spec.dt, nt), src_pos=(nx / 2, ny / 2, pml + 1),
+        shots.append(Shot(spec, nt, vel, eps=eps, dl=dl, wavelet=ricker(f, spec.dt, nt), src_pos=(nx / 2, ny / 2, pml + 1),
                           rcv_pos=rcv, interval=4, fpeak=f, name=f"small{k}"))
     return shots
 

@@ -13,8 +13,8 @@ WaveFieldCompress is the non-learned fallback).
 """
 import numpy as np
 
-LAYERS = [(8, 16, 64, True), (128, 16, 8, True), (16, 16, 8, True), (128, 32, 1, False),
-          (32, 128, 1, True), (16, 16, 8, True), (16, 128, 8, True), (16, 8, 64, False)]
+LAYERS = [(8, 16, 64, True), (128, 16, 8, True), (16, 16, 8, True), (128, 64, 1, False),
+          (64, 128, 1, True), (16, 16, 8, True), (16, 128, 8, True), (16, 8, 64, False)]
 SLOPE = 0.1
 
 

@@ -175,10 +175,11 @@ def test_ablation_at_equal_bytes(data):
 def test_fused_volume_codec_equals_layered(data):
     """The fused encode / decode kernels that the snapshot store uses (one
     warp per block, the layers in shared memory) give the bits of the
-    layer-by-layer GEMM path: the latents and scales of a device volume equal
-    rtm_ae_reconstruct's on the host-blocked volume, and the decoded volume
-    equals that reconstruction times the scales; partial blocks at every face
-    included."""
+    layer-by-layer GEMM path: the stored BF16 latents and the scales of a
+    device volume equal rtm_ae_reconstruct's FP32 latents rounded to BF16 (the
+    decoder's operand rounding) and its scales on the host-blocked volume, and
+    the decoded volume equals that reconstruction times the scales; partial
+    blocks at every face included."""
     import torch
     from konglong_b200 import _lib
     train, _ = data
@@ -194,7 +195,7 @@ def test_fused_volume_codec_equals_layered(data):
         rec, lat = ae.reconstruct(b)
         nb = b.shape[0]
         dv = torch.from_numpy(w).cuda()
-        dl = torch.zeros(nb * 32, device="cuda")
+        dl = torch.zeros(nb * AE.LATENT, device="cuda", dtype=torch.bfloat16)
         ds = torch.zeros(nb, device="cuda")
         out = torch.zeros_like(dv)
         _lib.check(L.rtm_ae_compress_volume(ae.a, dv.data_ptr(), nx, ny, nz, dl.data_ptr(), ds.data_ptr(), None),
@@ -203,6 +204,6 @@ def test_fused_volume_codec_equals_layered(data):
                    "rtm_ae_decompress_volume")
         torch.cuda.synchronize()
         np.testing.assert_array_equal(ds.cpu().numpy(), sc)
-        np.testing.assert_array_equal(dl.cpu().numpy().reshape(nb, 32), lat)
+        np.testing.assert_array_equal(dl.float().cpu().numpy().reshape(nb, AE.LATENT), O.bf16(lat).astype(np.float32))
         np.testing.assert_array_equal(out.cpu().numpy(), AE.blocks_to_volume(rec, sc, shape))
     ae.close()
