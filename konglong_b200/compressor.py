@@ -99,6 +99,46 @@ def init_params(seed=5):
     return np.concatenate(out)
 
 
+def init_params_average():
+    """Parameters with which the network computes the 16:1 2^3-average code
+    exactly (up to BF16 rounding): the latent holds the 64 averages (scaled),
+    the decoder repeats each over its 2^3 cube.  A leaky ReLU passes a value
+    x linearly through two channels, x = (lr(x) - lr(-x)) / (1 + slope), so
+    every layer carries the averages as (+, -) channel pairs: E1 forms them
+    from the 8 children of each 2^3 cube, E2 / E3 and D1 / D2 / D3 re-split
+    them (each re-split scales them by 1 + slope), E4 writes the 64 values
+    to the latent and D4 removes the accumulated scale.  All weights are +-1,
+    +-1/8 or the one D4 factor; biases are zero.  Training from here starts
+    at the non-learned code's error."""
+    g = 1.0 + 0.1  # the leaky ReLU's (+, -) pair gain, slope 0.1
+    W = [np.zeros((K, N), np.float64) for K, N, _, _ in LAYERS]
+    for k in range(8):  # E1: rows = 2^3 cubes, K = their 8 children
+        W[0][k, 0], W[0][k, 1] = 1.0 / 8, -1.0 / 8
+    for c in range(8):  # E2: K = 8 cubes x 16 channels -> (+, -) of cube c in channels 2c, 2c+1
+        W[1][c * 16, 2 * c], W[1][c * 16 + 1, 2 * c] = 1.0, -1.0
+        W[1][c * 16, 2 * c + 1], W[1][c * 16 + 1, 2 * c + 1] = -1.0, 1.0
+    for c in range(8):  # E3 and D2: pointwise re-split of the 8 pairs
+        for l in (2, 5):
+            W[l][2 * c, 2 * c], W[l][2 * c + 1, 2 * c] = 1.0, -1.0
+            W[l][2 * c, 2 * c + 1], W[l][2 * c + 1, 2 * c + 1] = -1.0, 1.0
+    for r in range(8):  # E4: K = 8 rows x 16 channels -> latent 8 r + c; D1 back to (+, -) pairs
+        for c in range(8):
+            W[3][r * 16 + 2 * c, 8 * r + c], W[3][r * 16 + 2 * c + 1, 8 * r + c] = 1.0, -1.0
+            W[4][8 * r + c, r * 16 + 2 * c], W[4][8 * r + c, r * 16 + 2 * c + 1] = 1.0, -1.0
+    for c in range(8):  # D3: pair c -> the (+, -) channels of child cube c
+        W[6][2 * c, c * 16], W[6][2 * c + 1, c * 16] = 1.0, -1.0
+        W[6][2 * c, c * 16 + 1], W[6][2 * c + 1, c * 16 + 1] = -1.0, 1.0
+    # D4: every one of a cube's 8 cells is its average; six (+, -) re-splits
+    # (E2, E3, E4, D2, D3, D4) have scaled it by g each
+    for k in range(8):
+        W[7][0, k], W[7][1, k] = 1.0 / g ** 6, -1.0 / g ** 6
+    out = []
+    for w, (K, N, _, _) in zip(W, LAYERS):
+        out.append(w.astype(np.float32).ravel())
+        out.append(np.zeros(N, np.float32))
+    return np.concatenate(out)
+
+
 def naive_16to1(blocks):
     """Reference 16:1 code without learning: 2^3 averages (64 values) in FP16."""
     return np.repeat(blocks.reshape(-1, 64, 8).mean(axis=2, keepdims=True).astype(np.float16).astype(np.float32),
@@ -155,16 +195,17 @@ class AutoEncoder:
         _lib.check(self.L.rtm_ae_reconstruct(self.a, b, b.shape[0], out, lat), "rtm_ae_reconstruct")
         return out, lat
 
-    def fit(self, blocks, steps=2000, batch=256, lr=2e-3, seed=0, lr_final=2e-4, weights=None):
+    def fit(self, blocks, steps=2000, batch=256, lr=2e-3, seed=0, lr_final=2e-4, weights=None, uniform=0.5):
         """Adam on random batches of `blocks` with a cosine-decayed learning
         rate; `weights` (e.g. the blocks' energy, scale^2) sets the sampling
         probability, so the loss follows the volume-level error the imaging
-        condition sees.  Returns the batch losses."""
+        condition sees, mixed with a fraction `uniform` of uniform sampling.
+        Returns the batch losses."""
         rng = np.random.default_rng(seed)
         prob = None
         if weights is not None:
             w = np.asarray(weights, np.float64)
-            prob = 0.5 * w / w.sum() + 0.5 / w.size  # half energy-weighted, half uniform
+            prob = (1.0 - uniform) * w / w.sum() + uniform / w.size
         losses = []
         for k in range(steps):
             idx = rng.choice(blocks.shape[0], batch, p=prob) if prob is not None else \

@@ -385,7 +385,9 @@ struct __align__(16) AeEncSmem {
   __nv_bfloat16 h3[kFusedWarps][8 * 16];    // E3 output = E4 input [1][128]
 };
 
-// grid (ceil(nbz / 4), nbx, nby): block (bz = 4 blockIdx.x + warp, bx, by)
+// Persistent: each CTA stages the weights once, then takes groups of 4
+// blocks consecutive in z (group g: z group g % nbzg, then x, then y; block
+// bz = 4 (g % nbzg) + warp) until none is left.
 __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__restrict__ p,
                                                                const float *__restrict__ vol, int nx, int ny, int nz,
                                                                __nv_bfloat16 *__restrict__ latent,
@@ -393,9 +395,11 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__r
   extern __shared__ __align__(16) unsigned char smem_ae[];
   AeEncSmem &s = *reinterpret_cast<AeEncSmem *>(smem_ae);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
-  const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8, nby = (ny + 7) / 8, nbzg = (nbz + kFusedWarps - 1) / kFusedWarps;
+  const long long ngroups = (long long)nbzg * nbx * nby;
   stage_weights<0>(p, s.w, s.b);
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+  const int bx = (int)((grp / nbzg) % nbx), by = (int)(grp / ((long long)nbzg * nbx)), z0 = (int)(grp % nbzg) * 32;
   // 32 z x 8 x x 8 y cells: thread -> (z quad, x, y) rows of 128 bytes
   for (int i = threadIdx.x; i < 8 * 8 * 8; i += blockDim.x) {
     const int zq = i & 7, xi = (i >> 3) & 7, yj = i >> 6;
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__r
     }
   }
   __syncthreads();
-  const int bz = blockIdx.x * kFusedWarps + warp;
+  const int bz = (int)(grp % nbzg) * kFusedWarps + warp;
   if (bz < nbz) {
     float a = 0.f;
     for (int i = lane; i < kBlock; i += 32) a = fmaxf(a, fabsf(s.raw[warp][i]));
@@ -438,6 +442,8 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_encode_k(const float *__r
     warp_layer<1, 128, kLatent, 128, false>(h3, w, b, [&](int, int n, float v) { lat[n] = __float2bfloat16_rn(v); });
     if (lane == 0) scales[blk] = sc;
   }
+  __syncthreads();  // the next group overwrites raw
+  }
 }
 
 struct __align__(16) AeDecSmem {
@@ -457,11 +463,13 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_decode_k(const float *__r
   extern __shared__ __align__(16) unsigned char smem_ae[];
   AeDecSmem &s = *reinterpret_cast<AeDecSmem *>(smem_ae);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8;
-  const int bx = blockIdx.y, by = blockIdx.z, z0 = blockIdx.x * 32;
+  const int nbz = (nz + 7) / 8, nbx = (nx + 7) / 8, nby = (ny + 7) / 8, nbzg = (nbz + kFusedWarps - 1) / kFusedWarps;
+  const long long ngroups = (long long)nbzg * nbx * nby;
   stage_weights<4>(p, s.w, s.b);
   __syncthreads();
-  const int bz = blockIdx.x * kFusedWarps + warp;
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+  const int bx = (int)((grp / nbzg) % nbx), by = (int)(grp / ((long long)nbzg * nbx)), z0 = (int)(grp % nbzg) * 32;
+  const int bz = (int)(grp % nbzg) * kFusedWarps + warp;
   if (bz < nbz) {
     const long long blk = ((long long)by * nbx + bx) * nbz + bz;
     for (int k = lane; k < kLatent; k += 32) s.l[warp][k] = latent[blk * kLatent + k];
@@ -499,6 +507,8 @@ __global__ void __launch_bounds__(32 * kFusedWarps) ae_decode_k(const float *__r
       if (z < nz) vol[((long long)y * nx + x) * nz + z] = s.out[zl >> 3][morton8(xi, yj, zl & 7)];
     }
   }
+  __syncthreads();  // the next group overwrites out
+  }
 }
 
 }  // namespace
@@ -509,30 +519,47 @@ long long ae_volume_blocks(int nx, int ny, int nz) {
 
 int ae_prepare(rtm_ae *a) { return ae_reserve(a, kChunkBlocks, false); }
 
+// CTAs of one wave of the persistent codec kernels (set by ae_fused_init)
+static int g_ae_wave = 0;
+
 // shared-memory size of the fused encoder / decoder (beyond the 48 KB default)
+// and the CTAs of one wave; called when a compressor is created (outside any
+// stream capture)
 static bool ae_fused_init() {
-  return cudaFuncSetAttribute(ae_encode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeEncSmem)) ==
-             cudaSuccess &&
-         cudaFuncSetAttribute(ae_decode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeDecSmem)) ==
-             cudaSuccess;
+  if (cudaFuncSetAttribute(ae_encode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeEncSmem)) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(ae_decode_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AeDecSmem)) !=
+          cudaSuccess)
+    return false;
+  int dev = 0, sms = 0, occ_e = 0, occ_d = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e, ae_encode_k, 32 * kFusedWarps, sizeof(AeEncSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, ae_decode_k, 32 * kFusedWarps, sizeof(AeDecSmem));
+  g_ae_wave = std::max(1, sms) * std::max(1, std::min(occ_e, occ_d));
+  return true;
 }
 
 // volume -> latents [nb][64] (bfloat16) + scales [nb] (device), on stream st
 // (the fused kernel)
+// CTAs of a persistent codec launch over `groups` work items: one wave
+static unsigned ae_grid(long long groups) {
+  return (unsigned)std::max(1LL, std::min<long long>(groups, std::max(1, g_ae_wave)));
+}
+static long long ae_groups(int nx, int ny, int nz) {
+  return (long long)((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps) * ((nx + 7) / 8) * ((ny + 7) / 8);
+}
+
 int ae_compress(rtm_ae *a, const float *w, int nx, int ny, int nz, void *latent, float *scales, cudaStream_t st) {
-  const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
-  if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
-  ae_encode_k<<<grid, 32 * kFusedWarps, sizeof(AeEncSmem), st>>>(a->p, w, nx, ny, nz,
-                                                                static_cast<__nv_bfloat16 *>(latent), scales);
+  ae_encode_k<<<ae_grid(ae_groups(nx, ny, nz)), 32 * kFusedWarps, sizeof(AeEncSmem), st>>>(
+      a->p, w, nx, ny, nz, static_cast<__nv_bfloat16 *>(latent), scales);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 // latents + scales -> volume (device), on stream st (the fused kernel)
 int ae_decompress(rtm_ae *a, const void *latent, const float *scales, int nx, int ny, int nz, float *w,
                   cudaStream_t st) {
-  const dim3 grid((((nz + 7) / 8) + kFusedWarps - 1) / kFusedWarps, (nx + 7) / 8, (ny + 7) / 8);
-  if (grid.y > 65535 || grid.z > 65535) return RTM_ERR_ARG;
-  ae_decode_k<<<grid, 32 * kFusedWarps, sizeof(AeDecSmem), st>>>(a->p, static_cast<const __nv_bfloat16 *>(latent),
-                                                                scales, nx, ny, nz, w);
+  ae_decode_k<<<ae_grid(ae_groups(nx, ny, nz)), 32 * kFusedWarps, sizeof(AeDecSmem), st>>>(
+      a->p, static_cast<const __nv_bfloat16 *>(latent), scales, nx, ny, nz, w);
   return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
 }
 

@@ -78,3 +78,18 @@ def test_fallback_selection_is_the_top_candidates():
     _, sc = AE.volume_to_blocks(w)
     rec = AE.apply_fallback(np.zeros_like(w), w, sc, np.arange(sc.size))
     assert np.abs(rec - w).max() <= 1e-3 * np.abs(w).max()
+
+
+def test_average_code_initialisation_reproduces_the_average_code():
+    """init_params_average makes the network compute the 16:1 2^3-average
+    code: through the BF16-emulating oracle its reconstruction equals the
+    non-learned code up to BF16 rounding (0.5 %), its latents are the 64
+    averages times the (+, -) pair gain 1.1^3."""
+    rng = np.random.default_rng(2)
+    b = rng.standard_normal((48, AE.BLOCK)).astype(np.float32)
+    b /= np.abs(b).max(axis=1, keepdims=True)
+    rec, lat = O.reconstruct(AE.init_params_average(), b, round_bf16=True)
+    naive = AE.naive_16to1(b)
+    assert np.linalg.norm(rec - naive) / np.linalg.norm(naive) < 1e-2
+    avg = b.reshape(-1, 64, 8).mean(axis=2)
+    np.testing.assert_allclose(lat, 1.1 ** 3 * avg, rtol=2e-2, atol=2e-3)
