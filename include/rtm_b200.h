@@ -128,9 +128,11 @@ typedef struct rtm_config {
                          solves with the PML, scaling and update fused into them) with plain tile
                          loads, 7: as 3 with the visco-acoustic update loading its Q memory
                          itself instead of from the divergence pass's TMA ring, 8: compact FD
-                         segment-parallel with TMA tile loads where the tensor maps can be made
-                         (the 4-cell and segment-parallel variants fall back when they do not
-                         apply) */
+                         segment-parallel with TMA tile loads where the tensor maps can be made,
+                         9: as 0 with each compact-FD z line solve carrying the interior cells of
+                         the pointwise epilogue that follows it (the PML cells stay separate
+                         launches) (the 4-cell and segment-parallel variants fall back when they
+                         do not apply) */
   int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):
                          the gradient is divided by rho (KernelCPU::divideRho) and the divergence
                          accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes

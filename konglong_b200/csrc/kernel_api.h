@@ -275,7 +275,7 @@ struct CfdGradEpiArgs {  // PML round 1 + scaling on raw gradients, in place
   FusedIo io;
   const float *w1;
 };
-void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st);
+void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st, bool pml_only = false);
 
 struct CfdDivEpiArgs {  // PML round 2 on raw divergence parts + update
   int nx, ny, nz, pml3d, mode;
@@ -290,7 +290,12 @@ struct CfdDivEpiArgs {  // PML round 2 on raw divergence parts + update
   PmlDev pml;
   QDev q;
 };
-void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st);
+void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st, bool pml_only = false);
+// the z line solve of `in` fused with the gradient / divergence epilogue (the
+// raw z part stays in shared memory; the x / y parts come from a.gx, a.gy /
+// a.dx, a.dy)
+void launch_cfd_zgrad(const CfdPlanDev &p, const float *in, const CfdGradEpiArgs &a, cudaStream_t st);
+void launch_cfd_zdiv(const CfdPlanDev &p, const float *in, const CfdDivEpiArgs &a, cudaStream_t st);  // mode 0 / 1
 
 // ---- pseudo-spectral first derivative, FFTWR2C engine (kernels_fft.cu) -------
 struct FftPlans;

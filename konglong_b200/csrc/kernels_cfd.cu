@@ -586,46 +586,49 @@ struct EpiBox {
   int z0, z1, x0, x1, y0, y1;
 };
 
+// density division and VTI / TTI scaling of one cell's gradients after PML
+// round 1 (KernelCPU::ScalarVTI / ScalarTTI), every rounding explicit so that
+// each kernel inlining it gives the same bits
+__device__ __forceinline__ void grad_finish(const CfdGradEpiArgs &a, bool do_y, float &gx, float &gy, float &gz,
+                                            float ep, float dl, float ax, float ay, float r) {
+  if (a.rho) divide_rho(r, do_y, gx, gy, gz);
+  if (a.model == 3) aniso_scale<3>(make_float4(ep, dl, ax, ay), gx, gy, gz);
+  else if (a.model == 2) aniso_scale<2>(make_float4(ep, dl, 0.f, 0.f), gx, gy, gz);
+}
+
 // PML round 1 + VTI / TTI scaling of the raw gradients of one cell, in place
-// (pml1 on each component, then KernelCPU::ScalarVTI / ScalarTTI).
+// (pml1 on each component, then grad_finish)
 template <bool PML, int MASK>
 __device__ __forceinline__ void grad_cell(const CfdGradEpiArgs &a, const Grid3 &g, int ix, int iy, int iz) {
   const bool do_y = a.ny > 1;
   const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
-  float gz = a.gz[i], gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f;
+  float gx = a.gx[i], gy = do_y ? a.gy[i] : 0.f, gz = a.gz[i];
   float ep = 0.f, dl = 0.f, ax = 0.f, ay = 0.f;
   if (a.model >= 2) ep = __ldg(a.eps + i), dl = __ldg(a.del + i);
   if (a.model == 3) ax = __ldg(a.pjx + i), ay = do_y ? __ldg(a.pjy + i) : 0.f;
   if (PML) pml1_all<0, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, gz, gx, gy);
-  if (a.rho) divide_rho(__ldg(a.rho + i), do_y, gx, gy, gz);
-  if (a.model >= 2) {
-    float e = ep;
-    const float d = e - dl;
-    e = 1.0f + 2.0f * e;
-    if (a.model == 3) {
-      const float az = sqrtf(1.0f - (ax * ax + ay * ay));
-      const float v2 = gx * gx + gy * gy + gz * gz;
-      const float vzz = gx * ax + gy * ay + gz * az;
-      const float vz2 = vzz * vzz, vh2 = v2 - vz2;
-      const float ecl = e * vh2 + vz2;
-      const float parts = sqrtf(1.0f - 8.0f * (d * (vh2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-      const float sc = fminf(0.5f * (1.0f + parts), 1.0f);
-      const float bx = vzz * ax, by = vzz * ay, bz = vzz * az;
-      gx = (bx + (gx - bx) * e) * sc;
-      gy = (by + (gy - by) * e) * sc;
-      gz = (bz + (gz - bz) * e) * sc;
-    } else {
-      const float vx2 = gx * gx + gy * gy, vz2 = gz * gz;
-      const float ecl = e * vx2 + vz2;
-      const float parts = sqrtf(1.0f - 8.0f * (d * (vx2 * vz2)) * __frcp_rn(ecl * ecl + 1e-32f));
-      const float sc2 = e * fminf(0.5f * (1.0f + parts), 1.0f);
-      gx *= sc2;
-      gy *= sc2;
-    }
-  }
+  grad_finish(a, do_y, gx, gy, gz, ep, dl, ax, ay, a.rho ? __ldg(a.rho + i) : 0.f);
   a.gz[i] = gz;
   a.gx[i] = gx;
   if (do_y) a.gy[i] = gy;
+}
+
+// accumulation w0 - vel (dx + dz + dy) (with density in the engine's form)
+// and the update of MODE 0 (none) or 1 (leapfrog)
+template <int MODE>
+__device__ __forceinline__ float div_finish(const CfdDivEpiArgs &a, float dxv, float dyv, float dzv, float vel,
+                                            float w0, float w1, float r) {
+  float t;
+  if (a.rho) {
+    t = a.rho_form == 2   ? div_accumulate_rho<2>(w0, vel, r, dxv, dzv, dyv)
+        : a.rho_form == 1 ? div_accumulate_rho<1>(w0, vel, r, dxv, dzv, dyv)
+                          : div_accumulate_rho<0>(w0, vel, r, dxv, dzv, dyv);
+  } else {
+    t = __fmaf_rn(-dxv, vel, w0);
+    t = __fmaf_rn(-dzv, vel, t);
+    t = __fmaf_rn(-dyv, vel, t);
+  }
+  return MODE == 1 ? __fsub_rn(__fadd_rn(w1, w1), t) : t;
 }
 
 // PML round 2 on the raw divergence parts of one cell, then
@@ -635,26 +638,137 @@ template <bool PML, int MASK, int MODE>
 __device__ __forceinline__ void div_cell(const CfdDivEpiArgs &a, const Grid3 &g, int ix, int iy, int iz) {
   const bool do_y = a.ny > 1 && a.dy;
   const long long i = (long long)iy * g.nxz + (long long)ix * a.nz + iz;
-  float dxv = a.dx[i], dzv = a.dz[i], dyv = do_y ? a.dy[i] : 0.f;
+  float dxv = a.dx[i], dyv = do_y ? a.dy[i] : 0.f, dzv = a.dz[i];
   const float vel = __ldg(a.vel + i);
   const float w0 = a.w0[i];
   const float w1 = MODE != 0 ? __ldg(a.w1 + i) : 0.f;
   if (PML) pml1_all<1, MASK>(a.pml, g, a.pml3d, do_y, ix, iy, iz, dzv, dxv, dyv);
-  float t;
-  if (a.rho) {
-    const float r = __ldg(a.rho + i);
-    t = a.rho_form == 2   ? div_accumulate_rho<2>(w0, vel, r, dxv, dzv, dyv)
-        : a.rho_form == 1 ? div_accumulate_rho<1>(w0, vel, r, dxv, dzv, dyv)
-                          : div_accumulate_rho<0>(w0, vel, r, dxv, dzv, dyv);
-  } else {
-    t = w0 - dxv * vel;
-    t = t - dzv * vel;
-    t = t - dyv * vel;
-  }
+  const float r = a.rho ? __ldg(a.rho + i) : 0.f;
   float out;
-  if (MODE == 0) out = t;
-  else out = MODE == 1 ? (w1 + w1) - t : q_update(a.q, i, g.nxz * a.ny, t, w1);
+  if (MODE == 2) out = q_update(a.q, i, g.nxz * a.ny, div_finish<0>(a, dxv, dyv, dzv, vel, w0, w1, r), w1);
+  else out = div_finish<MODE>(a, dxv, dyv, dzv, vel, w0, w1, r);
   a.w0[i] = out;
+}
+
+// 32 z lines of `in` (line l at l * n) staged through shared memory [l][n + 1]
+// and solved in place (cfd_lines_k's z path); returns the lines in the tile
+__device__ __forceinline__ int zlines_solve(const CfdPlanDev &p, const float *__restrict__ in, float *sm,
+                                            long long nlines) {
+  const int n = p.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long l0 = (long long)blockIdx.x * 32;
+  const int nl = (int)min(32LL, nlines - l0);
+  for (int l = warp; l < nl; l += nw) {
+    const float *src = in + (l0 + l) * n;
+    float *dst = sm + l * (n + 1);
+#pragma unroll 4
+    for (int i = lane; i < n; i += 32) cp_async4(dst + i, src + i);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  cfd_tile_compute<1>(p, sm + lane * (n + 1), n, nl, lane, warp, nw);
+  __syncthreads();
+  return nl;
+}
+
+constexpr int kZfU = 4;  // cells per lane whose loads are in flight together
+
+// The z line solve of the gradient pass fused with the gradient epilogue of
+// the interior box (no PML cell): the raw z gradient of the tile's 32 lines
+// stays in shared memory while every interior cell of those lines takes the
+// density division and the VTI / TTI scaling with the raw x / y gradients of
+// the earlier line solves (grad_cell's arithmetic: the same bits as the
+// separate z solve and epilogue launches).  PML cells get their raw z
+// gradient stored for the six PML face-box launches that follow.  A warp
+// takes whole lines; each lane kZfU cells 32 apart, all loads issued before
+// any store.
+__global__ void __launch_bounds__(128) cfd_zgrad_k(CfdPlanDev p, const float *__restrict__ in, CfdGradEpiArgs a,
+                                                   EpiBox ib, long long nlines) {
+  extern __shared__ float sm[];
+  const int nl = zlines_solve(p, in, sm, nlines);
+  const int n = p.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool do_y = a.ny > 1;
+  for (int l = warp; l < nl; l += nw) {
+    const long long line = (long long)blockIdx.x * 32 + l;
+    const int ix = (int)(line % a.nx), iy = (int)(line / a.nx);
+    const bool xy_in = ix >= ib.x0 && ix < ib.x1 && iy >= ib.y0 && iy < ib.y1;
+    const long long base = line * n;
+    const float *zs = sm + l * (n + 1);
+    for (int iz0 = lane; iz0 < n; iz0 += 32 * kZfU) {
+      float gx[kZfU], gy[kZfU], ep[kZfU], dl[kZfU], ax[kZfU], ay[kZfU], r[kZfU];
+#pragma unroll
+      for (int u = 0; u < kZfU; u++) {
+        const int iz = iz0 + 32 * u;
+        const long long i = base + iz;
+        gx[u] = gy[u] = ep[u] = dl[u] = ax[u] = ay[u] = r[u] = 0.f;
+        if (iz < n && xy_in && iz >= ib.z0 && iz < ib.z1) {
+          gx[u] = a.gx[i];
+          if (do_y) gy[u] = a.gy[i];
+          if (a.model >= 2) ep[u] = __ldg(a.eps + i), dl[u] = __ldg(a.del + i);
+          if (a.model == 3) ax[u] = __ldg(a.pjx + i), ay[u] = do_y ? __ldg(a.pjy + i) : 0.f;
+          if (a.rho) r[u] = __ldg(a.rho + i);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kZfU; u++) {
+        const int iz = iz0 + 32 * u;
+        if (iz >= n) continue;
+        const long long i = base + iz;
+        float gz = zs[iz];
+        if (xy_in && iz >= ib.z0 && iz < ib.z1) {
+          grad_finish(a, do_y, gx[u], gy[u], gz, ep[u], dl[u], ax[u], ay[u], r[u]);
+          a.gx[i] = gx[u];
+          if (do_y) a.gy[i] = gy[u];
+        }
+        a.gz[i] = gz;
+      }
+    }
+  }
+}
+
+// The z line solve of the divergence pass fused with the divergence epilogue
+// of the interior box (accumulation and update of MODE 0 / 1; div_cell's
+// arithmetic).  PML cells get their raw z part stored in a.dz for the PML
+// face-box launches.
+template <int MODE>
+__global__ void __launch_bounds__(128) cfd_zdiv_k(CfdPlanDev p, const float *__restrict__ in, CfdDivEpiArgs a,
+                                                  EpiBox ib, long long nlines) {
+  extern __shared__ float sm[];
+  const int nl = zlines_solve(p, in, sm, nlines);
+  const int n = p.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool do_y = a.ny > 1 && a.dy;
+  float *dz_raw = const_cast<float *>(a.dz);
+  for (int l = warp; l < nl; l += nw) {
+    const long long line = (long long)blockIdx.x * 32 + l;
+    const int ix = (int)(line % a.nx), iy = (int)(line / a.nx);
+    const bool xy_in = ix >= ib.x0 && ix < ib.x1 && iy >= ib.y0 && iy < ib.y1;
+    const long long base = line * n;
+    const float *zs = sm + l * (n + 1);
+    for (int iz0 = lane; iz0 < n; iz0 += 32 * kZfU) {
+      float dxv[kZfU], dyv[kZfU], vel[kZfU], w0[kZfU], w1[kZfU], r[kZfU];
+#pragma unroll
+      for (int u = 0; u < kZfU; u++) {
+        const int iz = iz0 + 32 * u;
+        const long long i = base + iz;
+        dxv[u] = dyv[u] = vel[u] = w0[u] = w1[u] = r[u] = 0.f;
+        if (iz < n && xy_in && iz >= ib.z0 && iz < ib.z1) {
+          dxv[u] = a.dx[i];
+          if (do_y) dyv[u] = a.dy[i];
+          vel[u] = __ldg(a.vel + i);
+          w0[u] = a.w0[i];
+          if (MODE != 0) w1[u] = __ldg(a.w1 + i);
+          if (a.rho) r[u] = __ldg(a.rho + i);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kZfU; u++) {
+        const int iz = iz0 + 32 * u;
+        if (iz >= n) continue;
+        const long long i = base + iz;
+        if (xy_in && iz >= ib.z0 && iz < ib.z1) a.w0[i] = div_finish<MODE>(a, dxv[u], dyv[u], zs[iz], vel[u], w0[u], w1[u], r[u]);
+        else dz_raw[i] = zs[iz];
+      }
+    }
+  }
 }
 
 // one box: block (32 z, 8 x), grid (z tiles, x tiles, y count) from (z0, x0, y0);
@@ -745,6 +859,9 @@ int cfd_init() {
   ok = ok && cudaFuncSetAttribute(cfd_lines_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_zgrad_k, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_zdiv_k<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_zdiv_k<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   return ok ? 0 : -1;
 }
 
@@ -762,9 +879,10 @@ static bool pml_overlap(const PmlDev &P, int nx, int ny, int nz) {
   return P.f[DZ][0].w + P.f[DZ][1].w > nz || P.f[DX][0].w + P.f[DX][1].w > nx || P.f[DY][0].w + P.f[DY][1].w > ny;
 }
 
-void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st) {
+void launch_cfd_grad_epilogue(const CfdGradEpiArgs &a, cudaStream_t st, bool pml_only) {
   EpiBox bx[7];
   epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  if (pml_only) bx[0].z1 = bx[0].z0;
   const bool all = pml_overlap(a.pml, a.nx, a.ny, a.nz);
   each_box<0>(bx, [&](auto k) {
     constexpr int K = decltype(k)::value;
@@ -781,9 +899,10 @@ static void div_box(const CfdDivEpiArgs &a, const EpiBox &b, bool all, cudaStrea
   else cfd_div_box_k<(K > 0), kBoxMask[K], MODE><<<g, block, 0, st>>>(a, b);
 }
 
-void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
+void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st, bool pml_only) {
   EpiBox bx[7];
   epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  if (pml_only) bx[0].z1 = bx[0].z0;
   const bool all = pml_overlap(a.pml, a.nx, a.ny, a.nz);
   each_box<0>(bx, [&](auto k) {
     constexpr int K = decltype(k)::value;
@@ -791,6 +910,28 @@ void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st) {
     else if (a.mode == 1) div_box<K, 1>(a, bx[K], all, st);
     else div_box<K, 2>(a, bx[K], all, st);
   });
+}
+
+void launch_cfd_zgrad(const CfdPlanDev &p, const float *in, const CfdGradEpiArgs &a, cudaStream_t st) {
+  const long long nlines = (long long)a.nx * a.ny;
+  EpiBox bx[7];
+  epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  if (pml_overlap(a.pml, a.nx, a.ny, a.nz)) bx[0].z1 = bx[0].z0;  // every cell goes through the PML boxes
+  cfd_zgrad_k<<<(unsigned)((nlines + 31) / 32), 128, (size_t)32 * (a.nz + 1) * sizeof(float), st>>>(p, in, a, bx[0],
+                                                                                                     nlines);
+  launch_cfd_grad_epilogue(a, st, true);
+}
+
+void launch_cfd_zdiv(const CfdPlanDev &p, const float *in, const CfdDivEpiArgs &a, cudaStream_t st) {
+  const long long nlines = (long long)a.nx * a.ny;
+  const unsigned grid = (unsigned)((nlines + 31) / 32);
+  const size_t smem = (size_t)32 * (a.nz + 1) * sizeof(float);
+  EpiBox bx[7];
+  epi_boxes(a.pml, a.nx, a.ny, a.nz, bx);
+  if (pml_overlap(a.pml, a.nx, a.ny, a.nz)) bx[0].z1 = bx[0].z0;
+  if (a.mode == 0) cfd_zdiv_k<0><<<grid, 128, smem, st>>>(p, in, a, bx[0], nlines);
+  else cfd_zdiv_k<1><<<grid, 128, smem, st>>>(p, in, a, bx[0], nlines);
+  launch_cfd_div_epilogue(a, st, true);
 }
 
 

@@ -149,6 +149,7 @@ struct Engine {
                     // pipeline: line solves + pointwise epilogues); 3 / 4 the segment-parallel
                     // fused pipeline with TMA / plain tile loads
   int cfd_seg_ok = 0;  // the segment-parallel pipeline applies (engine CFD, 3-D, lines fit)
+  int cfd_zfuse = 0;   // the z line solves carry the interior box of the epilogues (kernel_variant 9)
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -783,7 +784,11 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   }
   TRY(check_launch(h, "fused_io"));
   if (h->cfd_xy == 3 || h->cfd_xy == 4) return cfd_seg_step(h, mode, q);
-  {
+  // the z line solve fused with the epilogue's interior box (x / y first):
+  // compact-FD line solves only (not the transform engines), not the
+  // visco-acoustic update of the divergence pass
+  const bool zfuse = h->cfd_zfuse && !h->fft && !h->r2r;
+  if (!zfuse) {
     KScope k(h, RTM_K_CFD_Z);
     cfd_deriv(h, DZ, 0, h->w1, h->pz);
   }
@@ -803,16 +808,18 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   ge.pml = pml_dev(h);
   {
     KScope k(h, RTM_K_CFD_GEPI);
-    launch_cfd_grad_epilogue(ge, h->st);
+    if (zfuse) launch_cfd_zgrad(h->cfd[DZ][0], h->w1, ge, h->st);
+    else launch_cfd_grad_epilogue(ge, h->st);
   }
   TRY(check_launch(h, "cfd_grad_epilogue"));
-  // divergence parts: d/dx px -> scr, d/dz pz -> scr2, d/dy py -> px (px is free now)
+  // divergence parts: d/dx px -> scr2, d/dz pz -> scr, d/dy py -> px (px is free now)
+  const bool zfuse_div = zfuse && mode != 2;
   {
     KScope k(h, RTM_K_CFD_X);
     cfd_deriv(h, DX, 1, h->px, h->scr2);
   }
   float *dzp = h->scr;
-  {
+  if (!zfuse_div) {
     KScope k(h, RTM_K_CFD_Z);
     cfd_deriv(h, DZ, 1, h->pz, dzp);
   }
@@ -835,7 +842,13 @@ static int step_kernel(Engine *h, int mode, const FusedIo &io) {
   de.q = q;
   {
     KScope k(h, RTM_K_CFD_DEPI);
-    launch_cfd_div_epilogue(de, h->st);
+    if (zfuse_div) {
+      // the Derivative path's divergence pass takes plan iswitch (cfd_deriv)
+      const bool deriv_path = h->c.engine == RTM_ENGINE_CFDB;
+      launch_cfd_zdiv(h->cfd[DZ][deriv_path && h->c.model_type == RTM_TTI ? 0 : 1], h->pz, de, h->st);
+    } else {
+      launch_cfd_div_epilogue(de, h->st);
+    }
   }
   return check_launch(h, "cfd_div_epilogue");
 }
@@ -1640,7 +1653,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   // can be made) and 6 its plain-load form; the autotuner tries both forms.
   h->cfd_seg_ok = c->engine == RTM_ENGINE_CFD && d->ny > 1 && d->nx <= cfd_seg_max_n(DX) &&
                   d->ny <= cfd_seg_max_n(DY) && d->nz <= cfd_seg_max_n(DZ) && cfd_seg_init() == 0;
-  if (c->kernel_variant == 0) h->cfd_xy = h->cfd_tma ? 1 : 0;
+  h->cfd_zfuse = c->kernel_variant == 9;
+  if (c->kernel_variant == 0 || c->kernel_variant == 9) h->cfd_xy = h->cfd_tma ? 1 : 0;
   else if (c->kernel_variant == 5) h->cfd_xy = 0;
   else if (c->kernel_variant == 6 && h->cfd_seg_ok) h->cfd_xy = 4;
   else if (c->kernel_variant == 8 && h->cfd_seg_ok) h->cfd_xy = h->cfd_tma ? 3 : 4;

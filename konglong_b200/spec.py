@@ -47,7 +47,8 @@ class PropSpec:
                                   # rings, 4 ISO 4 z cells with register prefetch, 5 compact FD with
                                   # streamed x / y lines, 6 / 8 compact FD segment-parallel with
                                   # plain / TMA tile loads, 7 as 3 with the Q update loading its own
-                                  # operands
+                                  # operands, 9 compact FD with the z line solves carrying the epilogues'
+                                  # interior cells
 
     @property
     def n(self):
