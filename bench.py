@@ -713,7 +713,7 @@ def main():
                     help="snapshot format of the forward step workloads (default: the reference's COMPRESS_16)")
     ap.add_argument("--q-bf16", action="store_true",
                     help="Q memory variables stored as bfloat16 (TTI + Q workloads)")
-    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8, 9],
+    ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10],
                     help="rtm_config.kernel_variant (0 auto; the autotuner then picks among its shapes)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiler runs: timings under a profiler mislead the tuner)")

@@ -231,6 +231,11 @@ void cfd_tma_box(int n, int *R, int *nb);
 void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                       const CUtensorMap *tin, const CUtensorMap *tout, int *err, cudaStream_t st);
 // x / y derivative by the register-streamed kernel (no shared memory)
+// pipelined persistent x / y line solves over TMA tiles (one CTA per SM, a
+// ring of tile buffers, right-hand side fused into the forward pass); false
+// when a ring of three tiles does not fit in shared memory (nothing launched)
+bool launch_cfd_deriv_pipe(int axis, const CfdPlanDev &p, int nx, int ny, int nz, const CUtensorMap *tin,
+                           const CUtensorMap *tout, int *err, cudaStream_t st);
 void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                              cudaStream_t st);
 

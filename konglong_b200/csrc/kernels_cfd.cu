@@ -15,6 +15,8 @@
 // KernelCPU::TTI run as pointwise epilogues afterwards.
 #include <type_traits>
 
+#include <algorithm>
+
 #include "kernel_api.h"
 #include "rtm_device.cuh"
 #include "tma.cuh"
@@ -28,6 +30,39 @@ constexpr int kChunk = 8;  // points per register chunk (both phases)
 // offsets: the deepest that fits 128 registers without spilling
 constexpr int kStreamD = 3, kStreamDWide = 2;
 
+// One right-hand-side row of the 11-band A with every rounding explicit, so
+// that each line kernel (staged, streamed, pipelined) gives the same bits:
+// interior rows sum_d a[54 + d] (x[i + d] - x[i - d]), d = 1 .. 5, and the
+// one-sided rows within 5 of a line end (banmul_dev_z_c,
+// bgprtm/FdEngine_cfd.cpp:304-327) accumulated in the reference order.
+struct RhsCoef {
+  float c1, c2, c3, c4, c5;
+};
+__device__ __forceinline__ float rhs_interior(const RhsCoef &c, float m5, float m4, float m3, float m2, float m1,
+                                              float p1, float p2, float p3, float p4, float p5) {
+  float t = __fmul_rn(c.c1, __fsub_rn(p1, m1));
+  t = __fmaf_rn(c.c2, __fsub_rn(p2, m2), t);
+  t = __fmaf_rn(c.c3, __fsub_rn(p3, m3), t);
+  t = __fmaf_rn(c.c4, __fsub_rn(p4, m4), t);
+  return __fmaf_rn(c.c5, __fsub_rn(p5, m5), t);
+}
+// row i < 5 from x[i - 5 + j], j = 0 .. 10 (x[j] here)
+__device__ __forceinline__ float rhs_low(const float (&a)[60], int i, const float *x) {
+  float v = 0.f;
+#pragma unroll
+  for (int j = 0; j < 11; j++)
+    if (j >= 5 - i) v = __fmaf_rn(a[j * 5 + i], x[j], v);
+  return v;
+}
+// row i = n - t, t = 1 .. 5, from x[i - 5 + j], j = 0 .. 10
+__device__ __forceinline__ float rhs_high(const float (&a)[60], int t, const float *x) {
+  float v = 0.f;
+#pragma unroll
+  for (int j = 0; j < 11; j++)
+    if (j < t + 5) v = __fmaf_rn(-a[t + 49 - 5 * j], x[j], v);
+  return v;
+}
+
 // Phase 1: right-hand sides of positions [p0, p1) of one line (element i at
 // L[i * S]), in place, C outputs per chunk from a window of C + 10 inputs
 // carried in registers.  The first and the last five outputs of the range
@@ -40,7 +75,7 @@ constexpr int kStreamD = 3, kStreamDWide = 2;
 template <int S, int C>
 __device__ __forceinline__ void cfd_rhs_range(const float (&a)[60], float *L, int n, int p0, int p1, float (&head)[5],
                                               float (&tail)[5]) {
-  const float a55 = a[55], a56 = a[56], a57 = a[57], a58 = a[58], a59 = a[59];
+  const RhsCoef rc{a[55], a[56], a[57], a[58], a[59]};
   float w[C + 10];
 #pragma unroll
   for (int k = 0; k < 10; k++) {
@@ -62,26 +97,18 @@ __device__ __forceinline__ void cfd_rhs_range(const float (&a)[60], float *L, in
     if (i0 >= 5 && i0 + C <= n - 5) {
 #pragma unroll
       for (int k = 0; k < C; k++)
-        r[k] = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
-               a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
+        r[k] = rhs_interior(rc, w[k], w[k + 1], w[k + 2], w[k + 3], w[k + 4], w[k + 6], w[k + 7], w[k + 8],
+                            w[k + 9], w[k + 10]);
     } else {
 #pragma unroll
       for (int k = 0; k < C; k++) {
         const int i = i0 + k;
-        float v = 0.f;
-        if (i < 5) {
-#pragma unroll
-          for (int j = 0; j < 11; j++)
-            if (j >= 5 - i) v = v + a[j * 5 + i] * w[k + j];
-        } else if (i >= n - 5) {
-          const int t = n - i;
-#pragma unroll
-          for (int j = 0; j < 11; j++)
-            if (j < t + 5) v = v - a[t + 49 - 5 * j] * w[k + j];
-        } else {
-          v = a55 * (w[k + 6] - w[k + 4]) + a56 * (w[k + 7] - w[k + 3]) + a57 * (w[k + 8] - w[k + 2]) +
-              a58 * (w[k + 9] - w[k + 1]) + a59 * (w[k + 10] - w[k]);
-        }
+        float v;
+        if (i < 5) v = rhs_low(a, i, w + k);
+        else if (i >= n - 5) v = rhs_high(a, n - i, w + k);
+        else
+          v = rhs_interior(rc, w[k], w[k + 1], w[k + 2], w[k + 3], w[k + 4], w[k + 6], w[k + 7], w[k + 8],
+                           w[k + 9], w[k + 10]);
         r[k] = v;
       }
     }
@@ -361,7 +388,7 @@ __global__ void __launch_bounds__(128, 4) cfd_stream_k(const CfdPlanDev p, const
   const Off e = (Off)es;
   const int n = p.n;
   const int nch = (n + C - 1) / C;
-  const float a55 = p.a[55], a56 = p.a[56], a57 = p.a[57], a58 = p.a[58], a59 = p.a[59];
+  const RhsCoef rhc{p.a[55], p.a[56], p.a[57], p.a[58], p.a[59]};
 
   // ---- right-hand sides of the one-sided end rows
   float rbf[5], rbb[5];
@@ -373,14 +400,14 @@ __global__ void __launch_bounds__(128, 4) cfd_stream_k(const CfdPlanDev p, const
     for (int i = 0; i < 5; i++) {
       float v = 0.f;
 #pragma unroll
-      for (int j = 5 - i; j < 11; j++) v = v + p.a[j * 5 + i] * xf[i - 5 + j];
+      for (int j = 5 - i; j < 11; j++) v = __fmaf_rn(p.a[j * 5 + i], xf[i - 5 + j], v);
       rbf[i] = v;
     }
 #pragma unroll
     for (int t = 5; t >= 1; t--) {
       float v = 0.f;
 #pragma unroll
-      for (int j = 0; j < t + 5; j++) v = v - p.a[t + 49 - 5 * j] * xb[6 - t + j];
+      for (int j = 0; j < t + 5; j++) v = __fmaf_rn(-p.a[t + 49 - 5 * j], xb[6 - t + j], v);
       rbb[5 - t] = v;
     }
   }
@@ -421,8 +448,8 @@ __global__ void __launch_bounds__(128, 4) cfd_stream_k(const CfdPlanDev p, const
         float r[C];
 #pragma unroll
         for (int k = 0; k < C; k++)
-          r[k] = a55 * (xa(k + 1) - xa(k - 1)) + a56 * (xa(k + 2) - xa(k - 2)) + a57 * (xa(k + 3) - xa(k - 3)) +
-                 a58 * (xa(k + 4) - xa(k - 4)) + a59 * (xa(k + 5) - xa(k - 5));
+          r[k] = rhs_interior(rhc, xa(k - 5), xa(k - 4), xa(k - 3), xa(k - 2), xa(k - 1), xa(k + 1), xa(k + 2),
+                              xa(k + 3), xa(k + 4), xa(k + 5));
         if (i0 < 5 || i0 + C > n - 5) {
 #pragma unroll
           for (int k = 0; k < C; k++) {
@@ -574,6 +601,180 @@ __global__ void __launch_bounds__(128) cfd_lines_tma_k(CfdPlanDev p, const __gri
     }
     bulk_commit();
     bulk_wait_read();
+  }
+}
+
+// Forward elimination with the right-hand side formed on the fly (one warp,
+// lane = line, element i of the lane's line at L[i * S]): rows [b, e) in
+// chunks of C; w carries the inputs x[b - 5 .. b + 4] in and x[e - 5 .. e + 4]
+// out.  The inputs ahead of the elimination are still in place (row i + 5 is
+// read before row i + 5 is overwritten), so no separate right-hand-side pass
+// or barrier is needed; the rows are those of cfd_rhs_range and fwd_region
+// (same roundings, same bits).  CST / PART as in fwd_region.
+template <int S, int C, bool CST, bool PART>
+__device__ __forceinline__ void fwd_rhs_region(const CfdPlanDev &p, const RhsCoef &rc, const float4 *__restrict__ lm,
+                                               float4 mc, float *L, int b, int e, int n, float (&w)[10], Chain &y) {
+  for (int i0 = b; i0 < e; i0 += C) {
+    float x[C + 10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) x[k] = w[k];
+#pragma unroll
+    for (int k = 10; k < C + 10; k++) {
+      const int j = i0 - 5 + k;
+      x[k] = j < n ? L[j * S] : 0.f;
+    }
+    float4 m[C];
+    if (!CST) {
+#pragma unroll
+      for (int k = 0; k < C; k++) m[k] = __ldg(lm + min(i0 + k, n - 1));
+    }
+    float r[C];
+#pragma unroll
+    for (int k = 0; k < C; k++)
+      r[k] = rhs_interior(rc, x[k], x[k + 1], x[k + 2], x[k + 3], x[k + 4], x[k + 6], x[k + 7], x[k + 8], x[k + 9],
+                          x[k + 10]);
+    if (i0 < 5 || i0 + C > n - 5) {
+#pragma unroll
+      for (int k = 0; k < C; k++) {
+        const int i = i0 + k;
+        if (i < 5) r[k] = rhs_low(p.a, i, x + k);
+        else if (i >= n - 5 && i < n) r[k] = rhs_high(p.a, n - i, x + k);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+      const float4 c = CST ? mc : m[k];
+      float v = r[k];
+      v = v - c.w * y.y4;
+      v = v - c.z * y.y3;
+      v = v - c.y * y.y2;
+      v = v - c.x * y.y1;
+      y.y4 = y.y3, y.y3 = y.y2, y.y2 = y.y1, y.y1 = v;
+      r[k] = v;
+    }
+    if (!PART || i0 + C <= e) {
+#pragma unroll
+      for (int k = 0; k < C; k++) L[(i0 + k) * S] = r[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < C; k++)
+        if (i0 + k < e) L[(i0 + k) * S] = r[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 10; k++) w[k] = x[k + C];
+  }
+}
+
+// Both recurrences of one line with the right-hand side fused into the
+// forward pass (cfd_solve's regions and backward pass)
+template <int S, int C>
+__device__ __forceinline__ void cfd_solve_fused(const CfdPlanDev &p, float *L, int n) {
+  const float4 *__restrict__ lm = reinterpret_cast<const float4 *>(p.lm);
+  const float4 *__restrict__ bu4 = reinterpret_cast<const float4 *>(p.bu);
+  const float4 mc = make_float4(p.lmc[0], p.lmc[1], p.lmc[2], p.lmc[3]);
+  const float4 uc = make_float4(p.buc[0], p.buc[1], p.buc[2], p.buc[3]);
+  const RhsCoef rc{p.a[55], p.a[56], p.a[57], p.a[58], p.a[59]};
+  int ka = (p.c0 + C - 1) / C, kb = (p.c1 + 1) / C;
+  if (p.c0 > p.c1 || ka >= kb) ka = kb = 0;
+  float w[10];
+#pragma unroll
+  for (int k = 0; k < 10; k++) w[k] = (k >= 5 && k - 5 < n) ? L[(k - 5) * S] : 0.f;
+  Chain y{0.f, 0.f, 0.f, 0.f};
+  fwd_rhs_region<S, C, false, false>(p, rc, lm, mc, L, 0, ka * C, n, w, y);
+  fwd_rhs_region<S, C, true, false>(p, rc, lm, mc, L, ka * C, kb * C, n, w, y);
+  fwd_rhs_region<S, C, false, true>(p, rc, lm, mc, L, kb * C, n, n, w, y);
+  int ja = (n - 1 - p.c1 + C - 1) / C, jb = (n - p.c0) / C;
+  if (p.c0 > p.c1 || ja >= jb) ja = jb = 0;
+  Chain z{0.f, 0.f, 0.f, 0.f};
+  bwd_region<S, C, false, false>(bu4, p.rdiag, uc, p.rdc, L, n - 1, n - ja * C, z);
+  bwd_region<S, C, true, false>(bu4, p.rdiag, uc, p.rdc, L, n - 1 - ja * C, n - jb * C, z);
+  bwd_region<S, C, false, true>(bu4, p.rdiag, uc, p.rdc, L, n - 1 - jb * C, 0, z);
+}
+
+// Pipelined persistent x / y line solves.  One CTA per SM walks the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... (tile = 32 z lines of one y (x
+// lines) or x (y lines) column) through a ring of nbuf shared-memory tile
+// buffers.  Warp nbuf - 1 is the producer: its lane 0 loads tile j into
+// buffer j % nbuf by TMA, and once the worker of tile j - nbuf has released
+// that buffer stores its result by TMA and loads the next tile into it.
+// Warps 0 .. nbuf - 2 are workers: worker w takes tiles w, w + nbuf - 1, ...
+// and runs both recurrences with the right-hand side fused into the forward
+// pass, so a worker goes from one loaded tile to the next without waiting on
+// a load or a store.  Barriers full[b] (TMA bytes landed) and done[b] (the
+// worker's writes fenced to the async proxy) alternate parity per reuse of
+// buffer b; every wait is bounded and raises *err.
+template <int AXIS>
+__global__ void __launch_bounds__(256, 1) cfd_pipe_k(CfdPlanDev p, const __grid_constant__ CUtensorMap tin,
+                                                     const __grid_constant__ CUtensorMap tout, int nz, int nzt,
+                                                     long long ntiles, int R, int nb, int nbuf, int *err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
+  uint64_t *done = full + 8;
+  float *buf = reinterpret_cast<float *>(smraw + 128);
+  const int n = p.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwork = nbuf - 1;
+  const size_t tile = (size_t)nb * R * 32;
+  const long long G = gridDim.x;
+  const int J = (int)((ntiles - blockIdx.x + G - 1) / G);
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < nbuf; b++) mbar_init(full + b, 1), mbar_init(done + b, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto coords = [&](int j, int &iz0, int &o) {
+    const long long t = blockIdx.x + (long long)j * G;
+    iz0 = (int)(t % nzt) * 32;
+    o = (int)(t / nzt);
+  };
+  if (warp == nwork) {
+    if (lane != 0) return;
+    int loaded = 0;  // tiles whose loads were issued
+    bool ok = true;
+    for (int j = 0; j < J + nbuf && ok; j++) {
+      const int b = j % nbuf;
+      float *sb = buf + (size_t)b * tile;
+      if (j >= nbuf) {
+        const int jd = j - nbuf;
+        if (jd >= J) continue;
+        ok = mbar_wait(done + b, (uint32_t)(jd / nbuf) & 1u, err);
+        if (!ok) break;
+        int iz0, o;
+        coords(jd, iz0, o);
+        for (int q = 0; q < nb; q++) {
+          if (AXIS == DX) tma_store_3d(&tout, sb + (size_t)q * R * 32, iz0, q * R, o);
+          else tma_store_3d(&tout, sb + (size_t)q * R * 32, iz0, o, q * R);
+        }
+        bulk_commit();
+        bulk_wait_read();
+      }
+      if (j < J) {
+        int iz0, o;
+        coords(j, iz0, o);
+        mbar_expect_tx(full + b, (uint32_t)tile * 4u);
+        for (int q = 0; q < nb; q++) {
+          if (AXIS == DX) tma_load_3d(sb + (size_t)q * R * 32, &tin, full + b, iz0, q * R, o);
+          else tma_load_3d(sb + (size_t)q * R * 32, &tin, full + b, iz0, o, q * R);
+        }
+        loaded = j + 1;
+      }
+    }
+    if (!ok) {
+      // loads issued for tiles no worker consumed must land before exit
+      for (int j = max(0, loaded - nbuf); j < loaded; j++) mbar_drain(full + j % nbuf, (uint32_t)(j / nbuf) & 1u);
+    }
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    return;
+  }
+  for (int j = warp; j < J; j += nwork) {
+    const int b = j % nbuf;
+    if (!mbar_wait(full + b, (uint32_t)(j / nbuf) & 1u, err)) break;
+    int iz0, o;
+    coords(j, iz0, o);
+    const int nl = min(32, nz - iz0);
+    if (lane < nl) cfd_solve_fused<32, kChunk>(p, buf + (size_t)b * tile + lane, n);
+    fence_proxy_async();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(done + b);
   }
 }
 
@@ -842,6 +1043,25 @@ void launch_cfd_deriv(int axis, const CfdPlanDev &p, const float *in, float *out
   else cfd_lines_k<true><<<grid, 128, smem, st>>>(p, in, out, nz, nxz, nz, nx, 0);
 }
 
+static int g_cfd_sms = 0;  // SM count of the device cfd_init ran on
+
+bool launch_cfd_deriv_pipe(int axis, const CfdPlanDev &p, int nx, int ny, int nz, const CUtensorMap *tin,
+                           const CUtensorMap *tout, int *err, cudaStream_t st) {
+  const int n = axis == DX ? nx : ny;
+  int R, nb;
+  cfd_tma_box(n, &R, &nb);
+  const size_t tile = (size_t)nb * R * 32 * sizeof(float);
+  const int nbuf = (int)std::min<size_t>(8, (227 * 1024 - 128) / tile);
+  if (nbuf < 3 || g_cfd_sms <= 0) return false;
+  const int nzt = (nz + 31) / 32;
+  const long long ntiles = (long long)nzt * (axis == DX ? ny : nx);
+  const unsigned grid = (unsigned)std::min<long long>(ntiles, g_cfd_sms);
+  const size_t smem = 128 + (size_t)nbuf * tile;
+  if (axis == DX) cfd_pipe_k<DX><<<grid, nbuf * 32, smem, st>>>(p, *tin, *tout, nz, nzt, ntiles, R, nb, nbuf, err);
+  else cfd_pipe_k<DY><<<grid, nbuf * 32, smem, st>>>(p, *tin, *tout, nz, nzt, ntiles, R, nb, nbuf, err);
+  return true;
+}
+
 void launch_cfd_deriv_stream(int axis, const CfdPlanDev &p, const float *in, float *out, int nx, int ny, int nz,
                              cudaStream_t st) {
   const long long nxz = (long long)nx * nz;
@@ -859,9 +1079,14 @@ int cfd_init() {
   ok = ok && cudaFuncSetAttribute(cfd_lines_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_lines_tma_k<DY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_pipe_k<DX>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  ok = ok && cudaFuncSetAttribute(cfd_pipe_k<DY>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_zgrad_k, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_zdiv_k<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
   ok = ok && cudaFuncSetAttribute(cfd_zdiv_k<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  int dev = 0;
+  ok = ok && cudaGetDevice(&dev) == cudaSuccess &&
+       cudaDeviceGetAttribute(&g_cfd_sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
   return ok ? 0 : -1;
 }
 

@@ -150,6 +150,7 @@ struct Engine {
                     // fused pipeline with TMA / plain tile loads
   int cfd_seg_ok = 0;  // the segment-parallel pipeline applies (engine CFD, 3-D, lines fit)
   int cfd_zfuse = 0;   // the z line solves carry the interior box of the epilogues (kernel_variant 9)
+  int cfd_pipe = 0;    // x / y line solves by the pipelined persistent TMA kernel (kernel_variant 10)
   int tma_shape = 1;  // index into kIsoTmaShapes
   struct TMap {
     const void *p;
@@ -505,6 +506,9 @@ static void cfd_deriv(Engine *h, int axis, int sgn, const float *in, float *out)
     const int bx = axis == DX ? R : 1, by = axis == DX ? 1 : R;
     tma = tmap(h, in, 32, bx, &mi, by) && tmap(h, out, 32, bx, &mo, by);
   }
+  if (tma && h->cfd_pipe &&
+      launch_cfd_deriv_pipe(axis, h->cfd[axis][sgn], d.nx, d.ny, d.nz, &mi, &mo, h->dflag, h->st))
+    return;
   launch_cfd_deriv(axis, h->cfd[axis][sgn], in, out, d.nx, d.ny, d.nz, tma ? &mi : nullptr, tma ? &mo : nullptr,
                    h->dflag, h->st);
 }
@@ -1654,7 +1658,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
   h->cfd_seg_ok = c->engine == RTM_ENGINE_CFD && d->ny > 1 && d->nx <= cfd_seg_max_n(DX) &&
                   d->ny <= cfd_seg_max_n(DY) && d->nz <= cfd_seg_max_n(DZ) && cfd_seg_init() == 0;
   h->cfd_zfuse = c->kernel_variant == 9;
-  if (c->kernel_variant == 0 || c->kernel_variant == 9) h->cfd_xy = h->cfd_tma ? 1 : 0;
+  h->cfd_pipe = c->kernel_variant == 10;
+  if (c->kernel_variant == 0 || c->kernel_variant == 9 || c->kernel_variant == 10) h->cfd_xy = h->cfd_tma ? 1 : 0;
   else if (c->kernel_variant == 5) h->cfd_xy = 0;
   else if (c->kernel_variant == 6 && h->cfd_seg_ok) h->cfd_xy = 4;
   else if (c->kernel_variant == 8 && h->cfd_seg_ok) h->cfd_xy = h->cfd_tma ? 3 : 4;
