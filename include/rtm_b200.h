@@ -310,6 +310,28 @@ int rtm_image_accumulate(rtm_handle *h, int slot);
  * cuFFT at each imaging step.  The first INVERSION call creates the FFT plans and 4
  * volumes + 3 spectra of scratch (call it before any stream capture). */
 int rtm_image_condition(rtm_handle *h, int option);
+/* Double-grid IMAGE1 (ImagingCondition with ic_double_z / _x / _y = 2; stackImageInterp,
+ * applyFFTV and interp, bgprtm/ImagingCondition.cpp:104-141, 169-178, 1084-1111;
+ * ImagingCorrelator::imaging1 and interleave2d / interleave3d,
+ * bgprtm/ImagingCorrelator.cpp:363-372, 440-507): at every imaging step both tapered
+ * fields are high-cut along each doubled axis (above high_z / high_xy of the Nyquist
+ * wavenumber, cosine roll-off; the reference's defaults are 0.9 and 0.7), half-shifted
+ * into the 2, 4 or 8 copies that sit on the doubled grid's sub-lattices (line FFTs:
+ * value at x + d/2), and copy i of the source is correlated with copy i of the receiver
+ * into image cube i.  The filters restate libfftv's HIGHTAPE / SHIFTHALF from their use
+ * (libfftv is not in the reference tree).  Factors (z, x, y): (2, 1, 1) or (2, 2, 1) on
+ * 2-D grids, (2, 2, 2) on 3-D grids; (1, 1, 1) turns it off.  IMAGE1 only (not with
+ * RTM_IC_INVERSION).  Replaces the fused image term of the backward loop and of
+ * rtm_image_accumulate while on; rtm_image_setup clears its cubes.  Allocates the
+ * line-FFT plans and 2 * nloop + 2 * nloop volumes (call it before any stream capture). */
+int rtm_image_double(rtm_handle *h, int ndbl_z, int ndbl_x, int ndbl_y, float high_z, float high_xy);
+/* The double-grid image on the doubled grid [ny * ndbl_y][nx * ndbl_x][nz * ndbl_z]
+ * (ImagingCorrelator::interleave); dst holds nloop * nx * ny * nz floats. */
+int rtm_get_image_double(rtm_handle *h, float *dst);
+/* The source illumination interpolated onto the doubled grid
+ * (ImagingCondition::interpIllum, bgprtm/ImagingCondition.cpp:759-808, its arithmetic
+ * and write order); needs rtm_illum_setup. */
+int rtm_get_illum_double(rtm_handle *h, float *dst);
 /* Source illumination (ImagingCondition::calIllum, bgprtm/ImagingCondition.cpp:143-149):
  * on = 1 allocates and zeroes a volume that every later imaging-condition term adds the
  * squared source value to (after the time / depth and edge tapers); on = 0 stops. */

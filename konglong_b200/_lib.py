@@ -29,7 +29,7 @@ EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", 
            "rtm_snapshot_load", "rtm_image_setup", "rtm_image_accumulate", "rtm_modelling",
            "rtm_migration", "rtm_get", "rtm_put", "rtm_c16_compress", "rtm_c16_uncompress",
            "rtm_last_loop_ms", "rtm_last_loop_launches", "rtm_profile", "rtm_profile_read",
-           "rtm_c16_compress_noalloc", "rtm_autotune", "rtm_autotune_result", "rtm_snapshot_offload", "rtm_illum_setup", "rtm_image_condition", "rtm_set_compressor_fallback", "rtm_illum_compensate", "rtm_check_finite", "rtm_selftest_bounded_wait",
+           "rtm_c16_compress_noalloc", "rtm_autotune", "rtm_autotune_result", "rtm_snapshot_offload", "rtm_illum_setup", "rtm_image_condition", "rtm_image_double", "rtm_get_image_double", "rtm_get_illum_double", "rtm_set_compressor_fallback", "rtm_illum_compensate", "rtm_check_finite", "rtm_selftest_bounded_wait",
            "rtm_batch_create", "rtm_batch_destroy", "rtm_batch_modelling", "rtm_batch_last_ms",
            "rtm_batch_autotune", "rtm_ae_nparams", "rtm_ae_create", "rtm_ae_destroy", "rtm_ae_set_params",
            "rtm_ae_get_params", "rtm_ae_loss_grad", "rtm_ae_train_step", "rtm_ae_reconstruct",
@@ -115,6 +115,9 @@ def lib():
     L.rtm_checkpoint_load.argtypes = [vp, i]
     L.rtm_illum_setup.argtypes = [vp, i]
     L.rtm_image_condition.argtypes = [vp, i]
+    L.rtm_image_double.argtypes = [vp, i, i, i, f, f]
+    L.rtm_get_image_double.argtypes = [vp, vp]
+    L.rtm_get_illum_double.argtypes = [vp, vp]
     L.rtm_set_compressor_fallback.argtypes = [vp, C.c_float, C.c_float]
     L.rtm_illum_compensate.argtypes = [vp, i, i, C.c_float, C.c_float]
     L.rtm_check_finite.argtypes = [vp, i, C.POINTER(i)]

@@ -302,6 +302,27 @@ void launch_cfd_div_epilogue(const CfdDivEpiArgs &a, cudaStream_t st, bool pml_o
 void launch_cfd_zgrad(const CfdPlanDev &p, const float *in, const CfdGradEpiArgs &a, cudaStream_t st);
 void launch_cfd_zdiv(const CfdPlanDev &p, const float *in, const CfdDivEpiArgs &a, cudaStream_t st);  // mode 0 / 1
 
+// ---- double-grid IMAGE1 imaging condition (kernels_ic.cu) -------------------
+// dz / dx / dy: 1 or 2 per axis; iv[k]: the copy holding the z, x, y, zx, zy,
+// xy, zxy half shift (0: not made; ImagingCorrelator's ivz .. ivzxy); nloop
+// copies (1, 2, 4 or 8); slot[c]: the copy on doubled-grid points of class
+// c = 4 (y odd) + 2 (x odd) + (z odd)
+struct DblMap {
+  int dz, dx, dy, nloop;
+  int iv[7];
+  int slot[8];
+};
+struct FftPlans;
+// one imaging step: S[0..nloop) / Rv[0..nloop) scratch volumes, image / comp
+// nloop cubes each, illum (null: off) on the base grid
+int launch_ic_double(FftPlans *fft, const DblMap &m, const FusedIo &io, const float *u, float *const *S,
+                     float *const *Rv, float *image, float *comp, float *illum, int nx, int ny, int nz, float high_z,
+                     float high_xy, cudaStream_t st);
+void launch_dbl_interleave(const float *cubes, float *out, const DblMap &m, int nx, int ny, int nz, cudaStream_t st);
+void launch_dbl_illum(const float *in, float *out, const DblMap &m, int nx, int ny, int nz, cudaStream_t st);
+// kind 0: half shift to x + d/2; kind 1: high cut above `high` of Nyquist (in may equal out)
+int launch_fft_filter(FftPlans *p, int axis, int kind, float high, const float *in, float *out, cudaStream_t st);
+
 // ---- pseudo-spectral first derivative, FFTWR2C engine (kernels_fft.cu) -------
 struct FftPlans;
 // cuFFT plans of the three axes (y skipped when ny == 1) bound to stream st,

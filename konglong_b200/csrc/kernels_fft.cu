@@ -64,6 +64,39 @@ __global__ void fft_ik_k(float2 *__restrict__ s, const float *__restrict__ k, lo
   }
 }
 
+// Line filters of the double-grid imaging condition (libfftv's SHIFTHALF and
+// HIGHTAPE filters): bin j of the half spectrum times
+//   kind 0, half shift:  e^{i pi j / n} / n, so the inverse transform gives the
+//          band-limited line at x + d/2 (the odd points of the doubled grid);
+//          for even n the Nyquist bin is zero (its cosine vanishes at the
+//          midpoints);
+//   kind 1, high cut:    w(j / (n/2)) / n with w = 1 up to `high` of the
+//          Nyquist wavenumber and a cosine roll-off to 0 at Nyquist.
+__global__ void fft_filter_k(float2 *__restrict__ s, long long total, int nh, long long inner, int n, int kind,
+                             float high) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)((t / inner) % nh);
+    const float2 v = s[t];
+    const float inv_n = 1.0f / float(n);
+    float2 r;
+    if (kind == 0) {
+      if (n % 2 == 0 && j == n / 2) {
+        r = make_float2(0.f, 0.f);
+      } else {
+        float sn, cs;
+        sincospif(float(j) / float(n), &sn, &cs);
+        r = make_float2((v.x * cs - v.y * sn) * inv_n, (v.x * sn + v.y * cs) * inv_n);
+      }
+    } else {
+      const float q = float(j) / (0.5f * float(n));
+      const float w = q <= high ? 1.0f : 0.5f * (1.0f + cospif(fminf((q - high) / (1.0f - high), 1.0f)));
+      r = make_float2(v.x * w * inv_n, v.y * w * inv_n);
+    }
+    s[t] = r;
+  }
+}
+
 // out[p][c][r] = in[p][r][c] for rows x cols planes (32 x 32 tiles)
 __global__ void __launch_bounds__(256) transpose_k(const float *__restrict__ in, float *__restrict__ out, int rows,
                                                    int cols) {
@@ -279,6 +312,30 @@ int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *o
     r = cublasSgemmStridedBatched(p->blas, CUBLAS_OP_N, CUBLAS_OP_N, nz, nx, nx, &one, in, nz, nxz, D, nx, 0, &zero,
                                   out, nz, nxz, ny);
   return r == CUBLAS_STATUS_SUCCESS ? RTM_OK : RTM_ERR_CUDA;
+}
+
+}  // namespace rtm
+
+namespace rtm {
+
+int launch_fft_filter(FftPlans *p, int axis, int kind, float high, const float *in, float *out, cudaStream_t st) {
+  const FftAxis &f = p->ax[axis];
+  if ((f.made & 3) != 3 || (kind != 0 && kind != 1) || (kind == 1 && !(high >= 0.f && high < 1.f)))
+    return RTM_ERR_ARG;
+  const int nx = p->nx, ny = p->ny, nz = p->nz;
+  const float *src = in;
+  float *dst = out;
+  if (axis == 0) {  // [ny][nx][nz] -> [ny][nz][nx]
+    transpose_k<<<dim3((nz + 31) / 32, (nx + 31) / 32, ny), 256, 0, st>>>(in, p->tr, nx, nz);
+    src = dst = p->tr;
+  }
+  if (cufftExecR2C(f.fwd, const_cast<float *>(src), (cufftComplex *)p->spec) != CUFFT_SUCCESS) return RTM_ERR_CUDA;
+  const long long total = (long long)f.nh * f.lines;
+  fft_filter_k<<<grid_for(total), 256, 0, st>>>(p->spec, total, f.nh, f.inner, f.n, kind, high);
+  if (cufftExecC2R(f.inv, (cufftComplex *)p->spec, dst) != CUFFT_SUCCESS) return RTM_ERR_CUDA;
+  if (axis == 0)
+    transpose_k<<<dim3((nx + 31) / 32, (nz + 31) / 32, ny), 256, 0, st>>>(p->tr, out, nz, nx);
+  return RTM_OK;
 }
 
 }  // namespace rtm

@@ -97,6 +97,14 @@ struct Engine {
   void *ic_plans = nullptr;
   float *icS = nullptr, *icR = nullptr, *icDs = nullptr, *icDr = nullptr, *icSh = nullptr, *icRh = nullptr,
         *icTh = nullptr;
+  // double-grid IMAGE1 (rtm_image_double): copy map, filters, line-FFT plans,
+  // the fields' nloop copies and the nloop image cubes (+ compensation)
+  int dbl = 0;
+  DblMap dmap{};
+  float dbl_hz = 0.9f, dbl_hxy = 0.7f;
+  FftPlans *dbl_fft = nullptr;
+  float *dblS[8] = {}, *dblR[8] = {};
+  float *dbl_img = nullptr, *dbl_comp = nullptr;
   char *host_snaps = nullptr;
   int nstage = 0;
   cudaStream_t st_copy = nullptr;
@@ -996,6 +1004,20 @@ static int ic_explicit(Engine *h, int slot, const float *u) {
   return check_launch(h, "ic_inversion");
 }
 
+// double-grid IMAGE1 term of slot `slot` against receiver field u, at once
+static int ic_double_explicit(Engine *h, int slot, const float *u) {
+  const FusedIo io = h->snap_fmt == RTM_SNAP_AE ? io_image_ae(h, slot) : io_image(h, slot);
+  KScope k(h, RTM_K_IO, 12);
+  const int rc = launch_ic_double(h->dbl_fft, h->dmap, io, u, h->dblS, h->dblR, h->dbl_img, h->dbl_comp,
+                                  h->illum_on ? h->illum : nullptr, h->d.nx, h->d.ny, h->d.nz, h->dbl_hz, h->dbl_hxy,
+                                  h->st);
+  if (rc != RTM_OK) {
+    h->err = "double-grid imaging: a line transform failed";
+    return rc;
+  }
+  return check_launch(h, "ic_double");
+}
+
 // per-slot slab statistics for the 16-bit formats, taken on w0 after injection
 static int snap_prepare(Engine *h, int slot) {
   if (h->snap_fmt == RTM_SNAP_FP32 || h->snap_fmt == RTM_SNAP_AE) return RTM_OK;
@@ -1455,6 +1477,7 @@ int rtm_destroy(rtm_handle *h) {
   if (h->st_copy) cudaStreamSynchronize(h->st_copy);
   if (h->ic_plans) rtm::ic_plans_destroy(h->ic_plans);
   if (h->fft) rtm::fft_plans_destroy(h->fft);
+  if (h->dbl_fft) rtm::fft_plans_destroy(h->dbl_fft);
   if (h->r2r) rtm::r2r_plans_destroy(h->r2r);
   if (h->host_snaps) cudaFreeHost(h->host_snaps);
   for (cudaEvent_t e : h->stage_ev)
@@ -2039,6 +2062,10 @@ int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
   }
   CK(cudaMemsetAsync(h->image, 0, 4 * (size_t)h->n, h->st));
   CK(cudaMemsetAsync(h->comp, 0, 4 * (size_t)h->n, h->st));
+  if (h->dbl) {
+    CK(cudaMemsetAsync(h->dbl_img, 0, 4 * (size_t)h->n * h->dmap.nloop, h->st));
+    CK(cudaMemsetAsync(h->dbl_comp, 0, 4 * (size_t)h->n * h->dmap.nloop, h->st));
+  }
   // ImagingCondition::calTapes (bgprtm/ImagingCondition.cpp:180-198)
   h->taper_t.resize(ntaper_t);
   for (int i = 0; i < ntaper_t; i++) h->taper_t[i] = 0.5f * (1.0f - cosf((float)M_PI * float(i) / float(ntaper_t)));
@@ -2052,6 +2079,10 @@ int rtm_image_setup(rtm_handle *h, int ntaper_t, int ntaper_z, int edge) {
 
 int rtm_image_condition(rtm_handle *h, int option) {
   if (!h || (option != RTM_IC_IMAGE1 && option != RTM_IC_INVERSION)) return RTM_ERR_ARG;
+  if (option == RTM_IC_INVERSION && h->dbl) {
+    h->err = "the double-grid imaging condition runs with RTM_IC_IMAGE1 only";
+    return RTM_ERR_UNSUPPORTED;
+  }
   cudaSetDevice(h->device);
   if (option == RTM_IC_INVERSION && !h->ic_plans) {
     h->ic_plans = rtm::ic_plans_create(h->d.nx, h->d.ny, h->d.nz);
@@ -2071,6 +2102,102 @@ int rtm_image_condition(rtm_handle *h, int option) {
   h->ic_opt = option;
   return RTM_OK;
 }
+
+int rtm_image_double(rtm_handle *h, int ndbl_z, int ndbl_x, int ndbl_y, float high_z, float high_xy) {
+  if (!h) return RTM_ERR_ARG;
+  auto in12 = [](int v) { return v == 1 || v == 2; };
+  if (!in12(ndbl_z) || !in12(ndbl_x) || !in12(ndbl_y) || !(high_z >= 0.f && high_z < 1.f) ||
+      !(high_xy >= 0.f && high_xy < 1.f))
+    return RTM_ERR_ARG;
+  const rtm_dims &d = h->d;
+  const bool on = ndbl_z == 2 || ndbl_x == 2 || ndbl_y == 2;
+  if (on) {
+    // ImagingCorrelator (bgprtm/ImagingCorrelator.cpp:57-74) needs z doubled whenever x or y
+    // is; its interleave of a 3-D grid is complete only with all three doubled
+    // (interleave2d moves one xz plane), and x / y are never doubled on a 1-cell axis
+    const bool ok = ndbl_z == 2 && (d.nx > 1 || ndbl_x == 1) &&
+                    (d.ny == 1 ? ndbl_y == 1 : (d.nx > 1 && ndbl_x == 2 && ndbl_y == 2));
+    if (!ok) {
+      h->err = "double-grid imaging: supported factors are (z, x, y) = (2, 1, 1) or (2, 2, 1) on 2-D grids and "
+               "(2, 2, 2) on 3-D grids";
+      return RTM_ERR_ARG;
+    }
+    if (h->ic_opt == RTM_IC_INVERSION) {
+      h->err = "the double-grid imaging condition runs with RTM_IC_IMAGE1 only";
+      return RTM_ERR_UNSUPPORTED;
+    }
+  }
+  cudaSetDevice(h->device);
+  CK(cudaStreamSynchronize(h->st));
+  // release an earlier set-up
+  for (float *&p : h->dblS) h->release(p), p = nullptr;
+  for (float *&p : h->dblR) h->release(p), p = nullptr;
+  h->release(h->dbl_img), h->release(h->dbl_comp);
+  h->dbl_img = h->dbl_comp = nullptr;
+  if (h->dbl_fft) rtm::fft_plans_destroy(h->dbl_fft), h->dbl_fft = nullptr;
+  h->dbl = 0;
+  if (!on) return RTM_OK;
+  // copy slots as ImagingCorrelator: ivz = 1, ivx = 2, ivy = 3, ivzx = 4, ivzy = 5, ivxy = 6,
+  // ivzxy = 7, renumbered when an axis is not doubled
+  int ivz = 1, ivx = 2, ivy = 3, ivzx = 4, ivzy = 5, ivxy = 6, ivzxy = 7;
+  if (ndbl_y == 1) {
+    if (ndbl_x == 1) ivz = 1;
+    else ivz = 1, ivx = 2, ivzx = 3;
+    ivy = ivxy = ivzy = ivzxy = 0;
+  }
+  if (ndbl_x == 1) ivx = ivxy = ivzx = ivzxy = 0;
+  rtm::DblMap m{};
+  m.dz = ndbl_z, m.dx = ndbl_x, m.dy = ndbl_y;
+  m.nloop = ivzxy ? 8 : ivzx ? 4 : 2;
+  const int iv[7] = {ivz, ivx, ivy, ivzx, ivzy, ivxy, ivzxy};
+  for (int k = 0; k < 7; k++) m.iv[k] = iv[k];
+  // point class c = 4 (y odd) + 2 (x odd) + (z odd)
+  m.slot[0] = 0, m.slot[1] = ivz, m.slot[2] = ivx, m.slot[3] = ivzx, m.slot[4] = ivy, m.slot[5] = ivzy,
+  m.slot[6] = ivxy, m.slot[7] = ivzxy;
+  const int rc = rtm::fft_plans_create(&h->dbl_fft, d.nx, d.ny, d.nz, (float)d.dx, (float)d.dy, (float)d.dz, h->st);
+  if (rc != RTM_OK) {
+    h->err = "double-grid imaging: line-FFT plan creation failed";
+    return rc;
+  }
+  for (int i = 0; i < m.nloop; i++) {
+    TRY(h->alloc(h->dblS[i], h->n));
+    TRY(h->alloc(h->dblR[i], h->n));
+  }
+  TRY(h->alloc(h->dbl_img, (size_t)h->n * m.nloop));
+  TRY(h->alloc(h->dbl_comp, (size_t)h->n * m.nloop));
+  CK(cudaMemsetAsync(h->dbl_img, 0, 4 * (size_t)h->n * m.nloop, h->st));
+  CK(cudaMemsetAsync(h->dbl_comp, 0, 4 * (size_t)h->n * m.nloop, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->dmap = m;
+  h->dbl_hz = high_z, h->dbl_hxy = high_xy;
+  h->dbl = 1;
+  return RTM_OK;
+}
+
+// the doubled-grid image or illumination into host memory (dst: n * nloop floats)
+static int get_double(Engine *h, bool illum, float *dst) {
+  if (!h || !dst) return RTM_ERR_ARG;
+  if (!h->dbl || (illum && !h->illum)) {
+    h->err = illum ? "no double-grid imaging set-up or no illumination" : "no double-grid imaging set-up";
+    return RTM_ERR_STATE;
+  }
+  cudaSetDevice(h->device);
+  const size_t n2 = (size_t)h->n * h->dmap.nloop;
+  float *tmp = nullptr;
+  TRY(h->alloc(tmp, n2));
+  if (illum) rtm::launch_dbl_illum(h->illum, tmp, h->dmap, h->d.nx, h->d.ny, h->d.nz, h->st);
+  else rtm::launch_dbl_interleave(h->dbl_img, tmp, h->dmap, h->d.nx, h->d.ny, h->d.nz, h->st);
+  int rc = rtm::check_launch(h, illum ? "dbl_illum" : "dbl_interleave");
+  if (rc == RTM_OK) {
+    cudaError_t e = cudaMemcpyAsync(dst, tmp, 4 * n2, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) rc = rtm::cuda_fail(e, "double-grid readout", h);
+  }
+  h->release(tmp);
+  return rc;
+}
+int rtm_get_image_double(rtm_handle *h, float *dst) { return get_double(h, false, dst); }
+int rtm_get_illum_double(rtm_handle *h, float *dst) { return get_double(h, true, dst); }
 
 int rtm_illum_setup(rtm_handle *h, int on) {
   if (!h) return RTM_ERR_ARG;
@@ -2112,9 +2239,10 @@ int rtm_image_accumulate(rtm_handle *h, int slot) {
     TRY(rtm::offload_h2d(h, slot));
     TRY(rtm::stage_ready(h, slot));
   }
-  if (h->ic_opt == RTM_IC_INVERSION) {
+  if (h->ic_opt == RTM_IC_INVERSION || h->dbl) {
     if (h->snap_fmt == RTM_SNAP_AE) TRY(rtm::ae_load(h, slot, h->ae_scratch));
-    TRY(rtm::ic_explicit(h, slot, h->w0));
+    if (h->dbl) TRY(rtm::ic_double_explicit(h, slot, h->w0));
+    else TRY(rtm::ic_explicit(h, slot, h->w0));
   } else {
     rtm::launch_fused_io(rtm::io_image(h, slot), h->w0, h->d.nx, h->d.ny, h->d.nz, h->st);
     TRY(rtm::check_launch(h, "image_accumulate"));
@@ -2171,7 +2299,9 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
         } else if (h->stored[slot]) {
           if (h->snap_fmt == RTM_SNAP_AE) {
             TRY(rtm::ae_load(h, slot, h->ae_scratch));
-            if (h->ic_opt == RTM_IC_INVERSION)
+            if (h->dbl)
+              TRY(rtm::ic_double_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
+            else if (h->ic_opt == RTM_IC_INVERSION)
               TRY(rtm::ic_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
             else
               pending = rtm::io_image_ae(h, slot);
@@ -2186,7 +2316,9 @@ int rtm_migration(rtm_handle *h, int dir, int it_begin, int it_end, int it_shift
                 if (h->stored[sn] && h->stage_slot[sn % h->nstage] != sn) TRY(rtm::offload_h2d(h, sn));
               }
             }
-            if (h->ic_opt == RTM_IC_INVERSION)  // now, on this step's field (the pending term's)
+            if (h->dbl)  // now, on this step's field (the pending term's)
+              TRY(rtm::ic_double_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
+            else if (h->ic_opt == RTM_IC_INVERSION)
               TRY(rtm::ic_explicit(h, slot, h->f16 ? rtm::f16_view(h, 2) : h->w0));
             else
               pending = rtm::io_image(h, slot);

@@ -165,6 +165,28 @@ class Propagator:
         """spec.IC_IMAGE1 (zero-lag, default) or spec.IC_INVERSION (k-domain derivative terms)."""
         self._ck(self.L.rtm_image_condition(self.h, int(option)), "rtm_image_condition")
 
+    def image_double(self, ndbl_z=2, ndbl_x=2, ndbl_y=2, high_z=0.9, high_xy=0.7):
+        """Double-grid IMAGE1: the imaging condition on the grid doubled along z (and x, y),
+        from half-shifted copies of both high-cut fields; (1, 1, 1) turns it off."""
+        self._ck(self.L.rtm_image_double(self.h, int(ndbl_z), int(ndbl_x), int(ndbl_y), float(high_z),
+                                         float(high_xy)), "rtm_image_double")
+        self._dbl = (int(ndbl_y), int(ndbl_x), int(ndbl_z))
+
+    def _get_double(self, fn, what):
+        dy, dx, dz = self._dbl
+        s = self.spec
+        out = np.empty((s.ny * dy, s.nx * dx, s.nz * dz), np.float32)
+        self._ck(fn(self.h, out.ctypes.data), what)
+        return out
+
+    def get_image_double(self):
+        """The double-grid image, shape (ny * ndbl_y, nx * ndbl_x, nz * ndbl_z)."""
+        return self._get_double(self.L.rtm_get_image_double, "rtm_get_image_double")
+
+    def get_illum_double(self):
+        """The source illumination interpolated onto the doubled grid."""
+        return self._get_double(self.L.rtm_get_illum_double, "rtm_get_illum_double")
+
     def illum_setup(self, on=True):
         """Accumulate the source illumination (sum of squared source values) in the imaging condition."""
         self._ck(self.L.rtm_illum_setup(self.h, int(bool(on))), "rtm_illum_setup")
