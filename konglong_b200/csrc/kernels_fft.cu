@@ -241,6 +241,11 @@ struct R2rPlans {
   cublasHandle_t blas = nullptr;
   void *ws = nullptr;
   float *D[3][2] = {};  // [axis][pass: 0 isign +1, 1 isign -1], row-major n x n
+  // z lines on the tensor cores: D split into its TF32 parts (kernels_r2r_tc.cu)
+  float *Dh[2] = {}, *Dl[2] = {};
+  int tc = 0;
+  int *err = nullptr;
+  cudaStream_t st = nullptr;
   int nx = 0, ny = 0, nz = 0;
 };
 
@@ -252,14 +257,20 @@ void r2r_plans_destroy(R2rPlans *p) {
   for (auto &a : p->D)
     for (float *m : a)
       if (m) cudaFree(m);
+  for (int s = 0; s < 2; s++) {
+    if (p->Dh[s]) cudaFree(p->Dh[s]);
+    if (p->Dl[s]) cudaFree(p->Dl[s]);
+  }
   if (p->ws) cudaFree(p->ws);
   delete p;
 }
 
-int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st) {
+int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st,
+                     bool tensor_cores, int *err) {
   *out = nullptr;
   R2rPlans *p = new R2rPlans();
   p->nx = nx, p->ny = ny, p->nz = nz;
+  p->st = st, p->err = err;
   if (cublasCreate(&p->blas) != CUBLAS_STATUS_SUCCESS) {
     p->blas = nullptr;
     r2r_plans_destroy(p);
@@ -291,6 +302,27 @@ int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy,
       }
     }
   }
+  if (tensor_cores && r2r_tc_supported(nz) && (long long)nx * ny <= 0x7fffffffLL * 128LL) {
+    if (r2r_tc_init() != 0) {
+      cudaGetLastError();
+    } else {
+      const long long nn2 = (long long)nz * nz;
+      for (int s = 0; s < 2; s++) {
+        if (cudaMalloc(&p->Dh[s], nn2 * 4) != cudaSuccess || cudaMalloc(&p->Dl[s], nn2 * 4) != cudaSuccess) {
+          cudaGetLastError();
+          r2r_plans_destroy(p);
+          return RTM_ERR_NOMEM;
+        }
+        launch_tf32_split(p->D[2][s], p->Dh[s], p->Dl[s], nn2, st);
+      }
+      if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        r2r_plans_destroy(p);
+        return RTM_ERR_CUDA;
+      }
+      p->tc = 1;
+    }
+  }
   *out = p;
   return RTM_OK;
 }
@@ -303,6 +335,11 @@ int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *o
   if (nxz > 0x7fffffffLL || lines > 0x7fffffffLL) return RTM_ERR_ARG;
   const float one = 1.f, zero = 0.f;
   cublasStatus_t r;
+  if (axis == 2 && p->tc) {  // the same product on the tensor cores (split TF32)
+    const int s = isign == 1 ? 0 : 1;
+    launch_r2r_tc_z(in, out, p->Dh[s], p->Dl[s], nz, lines, p->err, p->st);
+    return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+  }
   if (axis == 2)  // out[l][t] = sum_u D[t][u] in[l][u]
     r = cublasSgemm(p->blas, CUBLAS_OP_T, CUBLAS_OP_N, nz, (int)lines, nz, &one, D, nz, in, nz, &zero, out, nz);
   else if (axis == 1)  // out[t][c] = sum_u D[t][u] in[u][c], c over nx nz

@@ -1555,7 +1555,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
       return fail(rc);
     }
     if ((c->engine == RTM_ENGINE_R2R || c->engine == RTM_ENGINE_SINCOS) &&
-        (rc = r2r_plans_create(&h->r2r, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
+        (rc = r2r_plans_create(&h->r2r, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st, c->kernel_variant != 1,
+                               h->dflag))) {
       h->err = "FFTWR2R line-matrix set-up failed";
       return fail(rc);
     }

@@ -58,3 +58,33 @@ def test_noalloc_at_the_slab_limit_matches_allocating_entry_point():
     err = _lib.STATUS_CODE["RTM_ERR_ARG"]
     assert L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), 1, ny + 1, 1, None) == err
     assert L.rtm_c16_compress_noalloc(1, 1, 4, 65537, 4, None) == err
+
+
+def test_noalloc_compress_replayed_from_a_captured_graph():
+    """The stated use: a warm-up call, then the call recorded on the caller's own
+    (non-default) stream into a CUDA graph and replayed; every replay writes
+    the allocating entry point's codes."""
+    import torch
+    from konglong_b200 import _lib
+    from konglong_b200.propagator import c16_compress
+    from tests.golden_inputs import codec_input
+
+    L = _lib.lib()
+    a, nx, ny, nz = codec_input()["wave"]
+    want = c16_compress(a, nx, ny, nz)
+    d_in = torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).cuda()
+    d_out = torch.zeros(want.size, dtype=torch.int16, device="cuda")
+    s = torch.cuda.Stream()
+    assert L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), nx, ny, nz, s.cuda_stream) == 0  # warm-up
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        rc = L.rtm_c16_compress_noalloc(d_in.data_ptr(), d_out.data_ptr(), nx, ny, nz, s.cuda_stream)
+        g.capture_end()
+    assert rc == 0
+    for _ in range(2):
+        d_out.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint16), want)
