@@ -335,17 +335,19 @@ int launch_fft_deriv(FftPlans *p, int axis, int isign, const float *in, float *o
 // FFTWR2R engine: one line matrix per axis and pass, applied as FP32 GEMMs on
 // stream st (cuBLAS handle, fixed workspace)
 struct R2rPlans;
-// tensor_cores: the z lines by the split-TF32 tcgen05 kernel where it applies
-// (nz % 4 == 0, 16 <= nz <= 512); err: device flag its bounded waits raise
+// tensor_cores: the line operators by the split-TF32 tcgen05 kernel where it
+// applies (nz % 4 == 0, lines of at most 512 points); err: device flag its
+// bounded waits raise
 int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st,
                      bool tensor_cores, int *err);
 // tcgen05 z-line operator (kernels_r2r_tc.cu)
 size_t r2r_tc_smem(int n);
-bool r2r_tc_supported(int n);
+bool r2r_tc_supported(int axis, int nx, int ny, int nz);
+size_t r2r_tc_bytes(int n);  // the pre-arranged TF32 parts of one n x n line matrix
 int r2r_tc_init();
-void launch_tf32_split(const float *D, float *Dh, float *Dl, long long count, cudaStream_t st);
-void launch_r2r_tc_z(const float *in, float *out, const float *Dh, const float *Dl, int n, long long lines, int *err,
-                     cudaStream_t st);
+void launch_tf32_arrange(const float *D, unsigned char *Bg, int n, cudaStream_t st);
+void launch_r2r_tc(int axis, const float *in, float *out, const unsigned char *Bg, int nx, int ny, int nz, int *err,
+                   cudaStream_t st);
 void r2r_plans_destroy(R2rPlans *p);
 int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *out);
 

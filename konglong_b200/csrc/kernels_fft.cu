@@ -241,9 +241,10 @@ struct R2rPlans {
   cublasHandle_t blas = nullptr;
   void *ws = nullptr;
   float *D[3][2] = {};  // [axis][pass: 0 isign +1, 1 isign -1], row-major n x n
-  // z lines on the tensor cores: D split into its TF32 parts (kernels_r2r_tc.cu)
-  float *Dh[2] = {}, *Dl[2] = {};
-  int tc = 0;
+  // line operators on the tensor cores: D split into its TF32 parts and laid
+  // out as the kernel's B stages (kernels_r2r_tc.cu), per axis and pass
+  unsigned char *Bg[3][2] = {};
+  int tc[3] = {};
   int *err = nullptr;
   cudaStream_t st = nullptr;
   int nx = 0, ny = 0, nz = 0;
@@ -257,10 +258,9 @@ void r2r_plans_destroy(R2rPlans *p) {
   for (auto &a : p->D)
     for (float *m : a)
       if (m) cudaFree(m);
-  for (int s = 0; s < 2; s++) {
-    if (p->Dh[s]) cudaFree(p->Dh[s]);
-    if (p->Dl[s]) cudaFree(p->Dl[s]);
-  }
+  for (auto &a : p->Bg)
+    for (unsigned char *b : a)
+      if (b) cudaFree(b);
   if (p->ws) cudaFree(p->ws);
   delete p;
 }
@@ -302,27 +302,26 @@ int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy,
       }
     }
   }
-  if (tensor_cores && r2r_tc_supported(nz) && (long long)nx * ny <= 0x7fffffffLL * 128LL) {
-    if (r2r_tc_init() != 0) {
-      cudaGetLastError();
-    } else {
-      const long long nn2 = (long long)nz * nz;
+  if (tensor_cores && r2r_tc_init() == 0) {
+    for (int a = 0; a < 3; a++) {
+      if (!p->D[a][0] || !r2r_tc_supported(a, nx, ny, nz)) continue;
       for (int s = 0; s < 2; s++) {
-        if (cudaMalloc(&p->Dh[s], nn2 * 4) != cudaSuccess || cudaMalloc(&p->Dl[s], nn2 * 4) != cudaSuccess) {
+        if (cudaMalloc(&p->Bg[a][s], r2r_tc_bytes(nn[a])) != cudaSuccess) {
           cudaGetLastError();
           r2r_plans_destroy(p);
           return RTM_ERR_NOMEM;
         }
-        launch_tf32_split(p->D[2][s], p->Dh[s], p->Dl[s], nn2, st);
+        launch_tf32_arrange(p->D[a][s], p->Bg[a][s], nn[a], st);
       }
-      if (cudaStreamSynchronize(st) != cudaSuccess) {
-        cudaGetLastError();
-        r2r_plans_destroy(p);
-        return RTM_ERR_CUDA;
-      }
-      p->tc = 1;
+      p->tc[a] = 1;
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      cudaGetLastError();
+      r2r_plans_destroy(p);
+      return RTM_ERR_CUDA;
     }
   }
+  cudaGetLastError();
   *out = p;
   return RTM_OK;
 }
@@ -335,9 +334,8 @@ int launch_r2r_deriv(R2rPlans *p, int axis, int isign, const float *in, float *o
   if (nxz > 0x7fffffffLL || lines > 0x7fffffffLL) return RTM_ERR_ARG;
   const float one = 1.f, zero = 0.f;
   cublasStatus_t r;
-  if (axis == 2 && p->tc) {  // the same product on the tensor cores (split TF32)
-    const int s = isign == 1 ? 0 : 1;
-    launch_r2r_tc_z(in, out, p->Dh[s], p->Dl[s], nz, lines, p->err, p->st);
+  if (p->tc[axis]) {  // the same products on the tensor cores (split TF32)
+    launch_r2r_tc(axis, in, out, p->Bg[axis][isign == 1 ? 0 : 1], nx, ny, nz, p->err, p->st);
     return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
   }
   if (axis == 2)  // out[l][t] = sum_u D[t][u] in[l][u]

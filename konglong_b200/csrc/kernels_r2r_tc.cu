@@ -1,12 +1,17 @@
 // kernels_r2r_tc.cu - FFTWR2R line operators on the 5th-generation tensor
 // cores (tcgen05, sm_100a).
 //
-// The FFTWR2R derivative of every z line is one fixed n x n matrix D applied
-// to the line (FdEngine_r2r's transform, bin product and inverse transform,
+// The FFTWR2R derivative along an axis is one fixed n x n matrix D applied to
+// every line (FdEngine_r2r's transform, bin product and inverse transform,
 // bgprtm/FdEngine_r2r.cpp; the matrix is built on the host in FP64):
-//   out[l][j] = sum_k D[j][k] in[l][k],   l over the nx ny lines.
-// As a GEMM, A = in ([lines][n], K-major), B = D ([n][n], K-major), and the
-// accumulator tile [128 lines][n] lives in tensor memory (n <= 512 columns).
+//   z lines:  out[l][j] = sum_k D[j][k] in[l][k],  l over the nx ny lines
+//   y lines:  out[j][c] = sum_k D[j][k] in[k][c],  c over the nx nz columns
+//   x lines:  the y form per y plane, c over nz.
+// As a GEMM D_acc[m][j] = sum_k A[m][k] B[j][k] with B = D (K-major) and
+// A[m][k] the input: for z lines m is the line (k contiguous), for x / y
+// lines m is the column c (m contiguous: each 16-byte copy brings 4 m of one
+// k, and the split pass transposes them into the K-major layout).  The
+// accumulator tile [128 m][n] lives in tensor memory (n <= 512 columns).
 // FP32 accuracy comes from split TF32: x = x_hi + x_lo with x_hi the TF32
 // rounding of x and x_lo the TF32 rounding of x - x_hi, and
 //   A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi
@@ -14,16 +19,21 @@
 // is below 2^-22 of the product).  D is split once when the plans are made;
 // the lines are split while they are staged.
 //
-// Per CTA: 128 lines; K in blocks of 16 through two shared-memory stages.  All
-// 128 threads load a block (float4 loads, rows contiguous), split it and store
-// hi / lo into the canonical no-swizzle K-major layout (8-row x 16-byte core
-// matrices: rows of a core matrix 16 B apart, its two K halves of one MMA
-// k-step 128 B apart (LBO), 8-row groups 256 B apart (SBO)); one thread issues
-// the MMAs of the block and commits them to the stage's mbarrier, which the
-// threads wait on before they refill that stage.  After the last block every
-// warp reads its 32 accumulator lanes (tcgen05.ld 32x32b) and stores its lines.
-// Every wait is bounded (2^16 polls, error flag); a CTA that gives up waits for
-// its committed MMAs and frees its tensor memory before it returns.
+// Per CTA: 128 lines; K in blocks of 8 (one MMA k-step) through 2 to 6
+// shared-memory stages.  A block of lines arrives raw by 16-byte asynchronous copies
+// (cp.async, zero-filled past the grid) S - 1 blocks ahead and is split into
+// hi / lo shared-to-shared at the same offsets; D's TF32 parts are
+// pre-arranged in global memory exactly as a stage's B region, so B arrives by
+// one bulk copy per block on an mbarrier.  Operands sit in the canonical
+// no-swizzle K-major layout (8-row x 16-byte core matrices: rows of a core
+// matrix 16 B apart, the two K halves of one MMA k-step 128 B apart (LBO),
+// 8-row groups 256 B apart (SBO)).  One thread issues a block's MMAs and
+// commits them to the stage's mbarrier; a stage is refilled once that
+// commit has arrived.  After the last block every warp reads its 32
+// accumulator lanes (tcgen05.ld 32x32b) and stores its lines.  Every wait is
+// bounded (2^16 polls, error flag); a CTA that gives up waits for its
+// committed MMAs and issued copies and frees its tensor memory before it
+// returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,7 +47,8 @@ namespace rtm {
 namespace {
 
 constexpr int kTcM = 128;   // lines per CTA (MMA M)
-constexpr int kTcBK = 16;   // K per stage (two MMA k-steps of 8)
+constexpr int kTcBK = 8;    // K per stage (one MMA k-step)
+constexpr int kTcCh = kTcBK / 4;  // 16-byte chunks per row of a stage
 constexpr int kTcThreads = 128;
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -73,6 +84,18 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// 32 consecutive accumulator columns of the warp's 32 lanes
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
 // byte offset of (row r, 4-float chunk q) of a [rows][16] block in the
 // canonical layout: k-step q / 2 at (q / 2) rows 32 B, then 8-row groups
 // (256 B), the k-step's two halves (128 B) and the row in the group (16 B)
@@ -82,23 +105,65 @@ __device__ __forceinline__ uint32_t kblock_off(int r, int q, int rows) {
 
 }  // namespace
 
-// out[l][j] = sum_k D[j][k] in[l][k] for the lines of this CTA; D given as its
-// TF32 parts Dh, Dl ([n][n]); npad = n rounded up to 16
+// geometry of one launch: MODE 0 `lines` lines along K; MODE 1 tiles of 128
+// consecutive m in groups (x lines: one group per y plane of nz m; y lines:
+// one group of nx nz m), k stepping by ldk
+struct TcGeom {
+  long long lines;
+  long long ldk, group_stride, group_m;
+  long long tiles_per_group;
+};
+
+// 16-byte asynchronous copy, zero-filled when src_bytes is 0
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src)),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// out[l][j] = sum_k D[j][k] in[l][k] for the 128 lines of this CTA.  Bg holds
+// D's TF32 parts pre-arranged per K block exactly as a stage's B region (hi
+// then lo, canonical layout, rows n .. npad-1 and columns past n zero), so a
+// stage's B arrives by one bulk copy.  A arrives raw by 16-byte asynchronous
+// copies S - 1 blocks ahead and is split into hi / lo in shared memory.
+// Stage s: raw A | A hi | A lo | B hi | B lo.
+template <int MODE, int S>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    r2r_tc_z_k(const float *__restrict__ in, float *__restrict__ out, const float *__restrict__ Dh,
-               const float *__restrict__ Dl, int n, int npad, long long M, int *err) {
+    r2r_tc_k(const float *__restrict__ in, float *__restrict__ out, const unsigned char *__restrict__ Bg, int n, int npad,
+             TcGeom geo, int *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw);            // [2] stage MMA commits
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(smraw + 64);      // tensor-memory base
+  uint64_t *full = reinterpret_cast<uint64_t *>(smraw);  // [S] B bulk copy landed
+  uint64_t *done = full + 8;                              // [S] the block's MMAs finished reading the stage
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smraw + 128);
   unsigned char *ops = smraw + 1024;
   const uint32_t a_bytes = kTcM * kTcBK * 4, b_bytes = (uint32_t)npad * kTcBK * 4;
-  const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
+  const uint32_t stage_bytes = 3 * a_bytes + 2 * b_bytes;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long m0 = (long long)blockIdx.x * kTcM;
+  // MODE 0: lines m0 .. m0 + 127 of length n, element (m, k) at in[m n + k];
+  // MODE 1: element (m, k) at in[base + k ldk + m], m < mvalid
+  long long m0 = 0, base = 0, M = 0;
+  int mvalid = 0;
+  if (MODE == 0) {
+    m0 = (long long)blockIdx.x * kTcM, M = geo.lines;
+  } else {
+    const long long g = blockIdx.x / geo.tiles_per_group, mt = blockIdx.x % geo.tiles_per_group;
+    base = g * geo.group_stride + mt * kTcM;
+    mvalid = (int)min((long long)kTcM, geo.group_m - mt * kTcM);
+  }
   const uint32_t ncols = npad <= 32 ? 32 : npad <= 64 ? 64 : npad <= 128 ? 128 : npad <= 256 ? 256 : 512;
+  const int nkb = (n + kTcBK - 1) / kTcBK;
 
   if (tid == 0) {
-    mbar_init(bar, 1), mbar_init(bar + 1, 1);
+    for (int i = 0; i < S; i++) mbar_init(full + i, 1), mbar_init(done + i, 1);
     mbar_fence_init();
   }
   if (warp == 0) {
@@ -112,40 +177,68 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tbase = *tslot;
 
-  const int nkb = (n + kTcBK - 1) / kTcBK;
+  // loads of block kb into stage kb % S: raw A by every thread (one commit
+  // group per block, empty past the last block), B by thread 0
+  auto issue_a = [&](int kb) {
+    if (kb < nkb) {
+      unsigned char *raw = ops + (size_t)(kb % S) * stage_bytes;
+      const int k0 = kb * kTcBK;
+      if (MODE == 0) {
+        for (int idx = tid; idx < kTcM * kTcCh; idx += kTcThreads) {
+          const int r = idx / kTcCh, q = idx % kTcCh, k = k0 + 4 * q;
+          const bool v = m0 + r < M && k < n;
+          cp_async16(raw + kblock_off(r, q, kTcM), v ? in + (m0 + r) * n + k : in, v ? 16u : 0u);
+        }
+      } else {  // raw chunk (m group g, k row kr) at g * 128 + kr * 16: 4 consecutive m of one k
+        for (int idx = tid; idx < kTcBK * (kTcM / 4); idx += kTcThreads) {
+          const int kr = idx / (kTcM / 4), g = idx % (kTcM / 4), k = k0 + kr;
+          const bool v = k < n && 4 * g < mvalid;
+          cp_async16(raw + g * 128 + kr * 16, v ? in + base + (long long)k * geo.ldk + 4 * g : in, v ? 16u : 0u);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  auto issue_b = [&](int kb) {
+    if (kb < nkb && tid == 0) {
+      unsigned char *st = ops + (size_t)(kb % S) * stage_bytes;
+      mbar_expect_tx(full + kb % S, 2 * b_bytes);
+      bulk_load(st + 3 * a_bytes, Bg + (size_t)kb * 2 * b_bytes, 2 * b_bytes, full + kb % S);
+    }
+  };
+  for (int p = 0; p < S - 1; p++) issue_a(p), issue_b(p);
+
   bool ok = true;
-  int issued = 0;  // K blocks committed
+  int issued = 0, b_issued = min(nkb, S - 1);  // blocks whose MMAs are committed / whose B copy is issued
   for (int kb = 0; kb < nkb && ok; kb++) {
-    const int s = kb & 1;
+    const int s = kb % S;
     unsigned char *st = ops + (size_t)s * stage_bytes;
-    // the MMAs of block kb - 2 read this stage
-    if (kb >= 2) ok = __syncthreads_and(mbar_wait(bar + s, (uint32_t)((kb - 2) >> 1) & 1u, err));
+    cp_async_wait<S - 2>();
+    // this block's B landed (its copy was issued after block kb - S's MMAs finished)
+    ok = __syncthreads_and(mbar_wait(full + s, (uint32_t)(kb / S) & 1u, err));
     if (!ok) break;
-    const int k0 = kb * kTcBK;
-    // A: 128 rows x 4 chunks of 4 floats
-    for (int idx = tid; idx < kTcM * 4; idx += kTcThreads) {
-      const int r = idx >> 2, q = idx & 3, k = k0 + 4 * q;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (m0 + r < M && k < n) v = __ldcs(reinterpret_cast<const float4 *>(in + (m0 + r) * n + k));
+    // split the raw block into TF32 hi / lo: MODE 0 at the same offsets;
+    // MODE 1 transposed from the raw m-contiguous chunks (4 m of one k) into
+    // the K-major layout of MODE 0
+    for (int c = tid; c < kTcM * kTcBK / 4; c += kTcThreads) {
+      const float4 v = *reinterpret_cast<const float4 *>(st + 16 * c);
       uint4 hi, lo;
       hi.x = tf32_round(v.x), hi.y = tf32_round(v.y), hi.z = tf32_round(v.z), hi.w = tf32_round(v.w);
       lo.x = tf32_round(v.x - __uint_as_float(hi.x)), lo.y = tf32_round(v.y - __uint_as_float(hi.y));
       lo.z = tf32_round(v.z - __uint_as_float(hi.z)), lo.w = tf32_round(v.w - __uint_as_float(hi.w));
-      const uint32_t o = kblock_off(r, q, kTcM);
-      *reinterpret_cast<uint4 *>(st + o) = hi;
-      *reinterpret_cast<uint4 *>(st + a_bytes + o) = lo;
-    }
-    // B: npad rows of D x 4 chunks (rows >= n zero)
-    for (int idx = tid; idx < npad * 4; idx += kTcThreads) {
-      const int r = idx >> 2, q = idx & 3, k = k0 + 4 * q;
-      float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-      if (r < n && k < n) {
-        h = __ldg(reinterpret_cast<const float4 *>(Dh + (long long)r * n + k));
-        l = __ldg(reinterpret_cast<const float4 *>(Dl + (long long)r * n + k));
+      if (MODE == 0) {
+        *reinterpret_cast<uint4 *>(st + a_bytes + 16 * c) = hi;
+        *reinterpret_cast<uint4 *>(st + 2 * a_bytes + 16 * c) = lo;
+      } else {
+        const int g = c >> 3, kr = c & 7;
+        const uint32_t h4[4] = {hi.x, hi.y, hi.z, hi.w}, l4[4] = {lo.x, lo.y, lo.z, lo.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const uint32_t o = kblock_off(4 * g + e, kr >> 2, kTcM) + (kr & 3) * 4;
+          *reinterpret_cast<uint32_t *>(st + a_bytes + o) = h4[e];
+          *reinterpret_cast<uint32_t *>(st + 2 * a_bytes + o) = l4[e];
+        }
       }
-      const uint32_t o = kblock_off(r, q, npad);
-      *reinterpret_cast<float4 *>(st + 2 * a_bytes + o) = h;
-      *reinterpret_cast<float4 *>(st + 2 * a_bytes + b_bytes + o) = l;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -153,45 +246,76 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const uint32_t sa = smem_u32(st);
       for (int ks = 0; ks < kTcBK / 8; ks++) {
-        const uint32_t ah = sa + ks * kTcM * 32, al = ah + a_bytes;
+        const uint32_t ah = sa + a_bytes + ks * kTcM * 32, al = ah + a_bytes;
         for (int h0 = 0; h0 < npad; h0 += 256) {
           const int nh = min(256, npad - h0);
-          const uint32_t bh = sa + 2 * a_bytes + ks * npad * 32 + (h0 >> 3) * 256, bl = bh + b_bytes;
+          const uint32_t bh = sa + 3 * a_bytes + ks * npad * 32 + (h0 >> 3) * 256, bl = bh + b_bytes;
           const uint32_t idesc = tf32_idesc(nh), d = tbase + (uint32_t)h0;
           const uint32_t first = (kb == 0 && ks == 0) ? 0u : 1u;
-          mma_tf32(d, kmajor_desc(ah, 128, 256), kmajor_desc(bh, 128, 256), idesc, first);
-          mma_tf32(d, kmajor_desc(ah, 128, 256), kmajor_desc(bl, 128, 256), idesc, 1u);
-          mma_tf32(d, kmajor_desc(al, 128, 256), kmajor_desc(bh, 128, 256), idesc, 1u);
+          const uint64_t dah = kmajor_desc(ah, 128, 256), dal = kmajor_desc(al, 128, 256);
+          mma_tf32(d, dah, kmajor_desc(bh, 128, 256), idesc, first);
+          mma_tf32(d, dah, kmajor_desc(bl, 128, 256), idesc, 1u);
+          mma_tf32(d, dal, kmajor_desc(bh, 128, 256), idesc, 1u);
         }
       }
-      mma_commit(bar + s);
+      mma_commit(done + s);
     }
     issued = kb + 1;
+    // block kb + S - 1 goes into the stage block kb - 1 used: its raw A at once
+    // (only the split read it, before the barrier above), its B and, at the
+    // next use, its hi / lo once block kb - 1's MMAs are done
+    const int nb = kb + S - 1;
+    if (nb < nkb && kb >= 1) {
+      const int sp = (kb - 1) % S;
+      ok = __syncthreads_and(mbar_wait(done + sp, (uint32_t)((kb - 1) / S) & 1u, err));
+      if (!ok) break;
+    }
+    issue_a(nb);
+    issue_b(nb);
+    if (nb < nkb) b_issued = nb + 1;
   }
-  // every committed block done (the last commit covers all earlier MMAs)
+  cp_async_wait<0>();
   if (issued > 0) {
     const int kl = issued - 1;
-    if (ok) ok = __syncthreads_and(mbar_wait(bar + (kl & 1), (uint32_t)(kl >> 1) & 1u, err));
-    else mbar_drain(bar + (kl & 1), (uint32_t)(kl >> 1) & 1u);
+    if (ok) ok = __syncthreads_and(mbar_wait(done + (kl % S), (uint32_t)(kl / S) & 1u, err));
+    else mbar_drain(done + (kl % S), (uint32_t)(kl / S) & 1u);
   }
+  if (!ok && tid == 0) {  // B copies issued but not consumed must land before the shared memory is released
+    for (int kb = issued; kb < b_issued; kb++) mbar_drain(full + kb % S, (uint32_t)(kb / S) & 1u);
+  }
+  __syncthreads();
   tc_fence_after();
-  if (ok) {
+  if (ok && MODE == 1) {  // lane = m: for each column j the warp writes 32 consecutive floats
+    const int m = warp * 32 + lane;
+    const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < npad; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(taddr + (uint32_t)c0, v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < mvalid) {
+        float *o = out + base + (long long)c0 * geo.ldk + m;
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          if (c0 + j < n) __stcs(o + (long long)j * geo.ldk, __uint_as_float(v[j]));
+      }
+    }
+  }
+  if (ok && MODE == 0) {
     const long long row = m0 + warp * 32 + lane;
     const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < npad; c0 += 8) {
-      uint32_t v[8];
-      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                   : "r"(taddr + (uint32_t)c0));
+    // 32 accumulator columns per load (npad is a multiple of 16: the last
+    // load may read 16 columns past npad, inside the allocation)
+    for (int c0 = 0; c0 < npad; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(taddr + (uint32_t)c0, v);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
         float *o = out + row * n + c0;
-        if (c0 + 4 <= n)
-          __stcs(reinterpret_cast<float4 *>(o),
-                 make_float4(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]), __uint_as_float(v[3])));
-        if (c0 + 8 <= n)
-          __stcs(reinterpret_cast<float4 *>(o + 4),
-                 make_float4(__uint_as_float(v[4]), __uint_as_float(v[5]), __uint_as_float(v[6]), __uint_as_float(v[7])));
+#pragma unroll
+        for (int j = 0; j < 32; j += 4)
+          if (c0 + j + 4 <= n)
+            __stcs(reinterpret_cast<float4 *>(o + j), make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                                  __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])));
       }
     }
   }
@@ -204,38 +328,102 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 namespace {
-__global__ void tf32_split_k(const float *__restrict__ D, float *Dh, float *Dl, long long n) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float x = D[i];
-    const uint32_t h = tf32_round(x);
-    Dh[i] = __uint_as_float(h);
-    Dl[i] = __uint_as_float(tf32_round(x - __uint_as_float(h)));
+// D's TF32 parts in the per-K-block stage layout of B (hi then lo)
+__global__ void tf32_arrange_k(const float *__restrict__ D, unsigned char *Bg, int n, int npad) {
+  const int nkb = (n + kTcBK - 1) / kTcBK;
+  const long long total = (long long)nkb * npad * kTcCh;
+  const uint32_t b_bytes = (uint32_t)npad * kTcBK * 4;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t % kTcCh), r = (int)((t / kTcCh) % npad), kb = (int)(t / ((long long)kTcCh * npad));
+    const int k = kb * kTcBK + 4 * q;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (r < n)
+      for (int e = 0; e < 4; e++)
+        if (k + e < n) v[e] = D[(long long)r * n + k + e];
+    uint32_t h[4], l[4];
+    for (int e = 0; e < 4; e++) {
+      h[e] = tf32_round(v[e]);
+      l[e] = tf32_round(v[e] - __uint_as_float(h[e]));
+    }
+    unsigned char *blk = Bg + (size_t)kb * 2 * b_bytes;
+    const uint32_t o = kblock_off(r, q, npad);
+    *reinterpret_cast<uint4 *>(blk + o) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4 *>(blk + b_bytes + o) = make_uint4(l[0], l[1], l[2], l[3]);
   }
 }
 }  // namespace
 
+// stages: lines up to 256 points keep a CTA within half the shared memory
+// (two CTAs of at most 256 accumulator columns share an SM), longer lines
+// take the whole of it; at most kTcMaxS stages
+constexpr int kTcMaxS = 6;
+static int tc_stages(int npad) {
+  const size_t stage = 3 * (size_t)kTcM * kTcBK * 4 + 2 * (size_t)npad * kTcBK * 4;
+  const size_t budget = (npad <= 256 ? 116 * 1024 : 227 * 1024) - 1024;
+  return (int)std::min<size_t>(npad <= 256 ? 4 : kTcMaxS, budget / stage);
+}
+
 size_t r2r_tc_smem(int n) {
   const int npad = (n + 15) / 16 * 16;
-  return 1024 + 2 * (2 * (size_t)kTcM * kTcBK * 4 + 2 * (size_t)npad * kTcBK * 4);
+  return 1024 + (size_t)tc_stages(npad) * (3 * (size_t)kTcM * kTcBK * 4 + 2 * (size_t)npad * kTcBK * 4);
 }
 
-bool r2r_tc_supported(int n) { return n % 4 == 0 && n >= 16 && n <= 512 && r2r_tc_smem(n) <= 227 * 1024; }
+// axis 2 reads its lines as float4 runs (n % 4 == 0); every axis needs nz % 4 == 0
+// (16-byte copies along z) and a line matrix of at most 512 rows
+bool r2r_tc_supported(int axis, int nx, int ny, int nz) {
+  const int n = axis == 0 ? nx : axis == 1 ? ny : nz;
+  return nz % 4 == 0 && n >= 2 && n <= 512 && tc_stages((n + 15) / 16 * 16) >= 2 && r2r_tc_smem(n) <= 227 * 1024;
+}
+
+size_t r2r_tc_bytes(int n) {
+  const int npad = (n + 15) / 16 * 16;
+  return (size_t)((n + kTcBK - 1) / kTcBK) * 2 * npad * kTcBK * 4;
+}
+
+#define RTM_TC_ALL(X) X(0, 2) X(0, 3) X(0, 4) X(0, 5) X(0, 6) X(1, 2) X(1, 3) X(1, 4) X(1, 5) X(1, 6)
 
 int r2r_tc_init() {
-  return cudaFuncSetAttribute(r2r_tc_z_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) == cudaSuccess
-             ? 0
-             : -1;
+  const int mx = 227 * 1024;
+  bool ok = true;
+#define RTM_TC_ATTR(MODE, S) \
+  ok = ok && cudaFuncSetAttribute(r2r_tc_k<MODE, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) == cudaSuccess;
+  RTM_TC_ALL(RTM_TC_ATTR)
+#undef RTM_TC_ATTR
+  return ok ? 0 : -1;
 }
 
-void launch_tf32_split(const float *D, float *Dh, float *Dl, long long count, cudaStream_t st) {
-  tf32_split_k<<<(unsigned)std::min<long long>((count + 255) / 256, 148LL * 8), 256, 0, st>>>(D, Dh, Dl, count);
-}
-
-void launch_r2r_tc_z(const float *in, float *out, const float *Dh, const float *Dl, int n, long long lines, int *err,
-                     cudaStream_t st) {
+void launch_tf32_arrange(const float *D, unsigned char *Bg, int n, cudaStream_t st) {
   const int npad = (n + 15) / 16 * 16;
-  const unsigned grid = (unsigned)((lines + kTcM - 1) / kTcM);
-  r2r_tc_z_k<<<grid, kTcThreads, r2r_tc_smem(n), st>>>(in, out, Dh, Dl, n, npad, lines, err);
+  const long long total = (long long)((n + kTcBK - 1) / kTcBK) * npad * kTcCh;
+  tf32_arrange_k<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 8), 256, 0, st>>>(D, Bg, n, npad);
+}
+
+// axis 2 (z): out[l][j] = sum_k D[j][k] in[l][k]; axis 1 (y): out[j][c] = sum_k D[j][k] in[k][c] over
+// c < nx nz; axis 0 (x): per y plane out[j][z] = sum_k D[j][k] in[k][z]
+void launch_r2r_tc(int axis, const float *in, float *out, const unsigned char *Bg, int nx, int ny, int nz,
+                   int *err, cudaStream_t st) {
+  const int n = axis == 0 ? nx : axis == 1 ? ny : nz;
+  const int npad = (n + 15) / 16 * 16;
+  const long long nxz = (long long)nx * nz;
+  TcGeom geo{};
+  long long tiles;
+  if (axis == 2) {
+    geo.lines = (long long)nx * ny;
+    tiles = (geo.lines + kTcM - 1) / kTcM;
+  } else if (axis == 1) {
+    geo.ldk = nxz, geo.group_stride = 0, geo.group_m = nxz, geo.tiles_per_group = (nxz + kTcM - 1) / kTcM;
+    tiles = geo.tiles_per_group;
+  } else {
+    geo.ldk = nz, geo.group_stride = nxz, geo.group_m = nz, geo.tiles_per_group = (nz + kTcM - 1) / kTcM;
+    tiles = geo.tiles_per_group * ny;
+  }
+  const size_t sm = r2r_tc_smem(n);
+  const int S = tc_stages(npad), mode = axis == 2 ? 0 : 1;
+#define RTM_TC_LAUNCH(MODE, SS) \
+  if (mode == MODE && S == SS) r2r_tc_k<MODE, SS><<<(unsigned)tiles, kTcThreads, sm, st>>>(in, out, Bg, n, npad, geo, err);
+  RTM_TC_ALL(RTM_TC_LAUNCH)
+#undef RTM_TC_LAUNCH
 }
 
 }  // namespace rtm

@@ -1,9 +1,11 @@
-"""FFTWR2R z-line operators on the tensor cores (split-TF32 tcgen05 kernel,
-kernel_variant 0) against the same operators as FP32 cuBLAS GEMMs
+"""FFTWR2R line operators on the tensor cores (split-TF32 tcgen05 kernel,
+kernel_variant 0: z lines as a K-major product, x and y lines with the volume
+as an MN-major operand) against the same operators as FP32 cuBLAS GEMMs
 (kernel_variant 1) and against the FP64 oracle (FdEngine_r2r's line matrices,
-bgprtm/FdEngine_r2r.cpp).  Line lengths 28 to 512 cover one and two 256-column
-accumulator halves and a last 16-column pad; 20 x 24 = 480 lines leave a
-partial last 128-line tile."""
+bgprtm/FdEngine_r2r.cpp).  Line lengths 20 to 512 cover one and two
+256-column accumulator halves and a last 16-column pad; 20 x 24 = 480 z lines
+and 20 x 28 = 560 y columns leave partial last 128-line tiles; a grid whose nz
+is not a multiple of 4 takes the cuBLAS products on every axis."""
 import numpy as np
 import pytest
 
@@ -42,3 +44,15 @@ def test_tensor_core_z_lines_match_fp32_gemm_and_fp64(nz, model):
         exact = _steps(O.Oracle(spec, double=True), m, w0, w1, 2)
         ref32 = _steps(O.Oracle(spec), m, w0, w1, 2)
         assert rel_l2(out[0], exact) < 2 * rel_l2(ref32, exact) + 1e-6
+
+
+@pytest.mark.parametrize("shape", [(300, 20, 36), (36, 300, 20), (40, 30, 30)])
+def test_tensor_core_x_y_lines(shape):
+    c = dict(engine=ENGINE_R2R, model=VTI, shape=shape, pml=6, seed=77)
+    spec, m, w0, w1 = case_inputs(c)
+    out = {}
+    for variant in (0, 1):
+        spec.kernel_variant = variant
+        out[variant] = _steps(Propagator(spec), m, w0, w1, 2)
+    assert np.abs(out[1]).max() > 0
+    assert rel_l2(out[0], out[1]) < 2e-6, rel_l2(out[0], out[1])
