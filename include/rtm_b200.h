@@ -122,8 +122,8 @@ typedef struct rtm_config {
                          tiles when nz % 4 == 0, else register-streamed x / y lines; the
                          autotuner may pick any compact-FD form; FFTWR2R / SINCOS: line
                          operators on the tensor cores, split TF32), 1: one cell per thread /
-                         plain staged tiles (FFTWR2R / SINCOS: FP32 cuBLAS line products), 2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane
-                         pipeline, 3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z
+                         plain staged tiles (FFTWR2R / SINCOS: FP32 cuBLAS line products),
+                         2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline, 3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z
                          cells per thread with register prefetch, 5: compact FD with
                          register-streamed x / y lines, 6: compact FD segment-parallel (line
                          solves with the PML, scaling and update fused into them) with plain tile
