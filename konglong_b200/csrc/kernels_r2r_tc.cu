@@ -49,6 +49,7 @@ namespace {
 constexpr int kTcM = 128;   // lines per CTA (MMA M)
 constexpr int kTcBK = 8;    // K per stage (one MMA k-step)
 constexpr int kTcCh = kTcBK / 4;  // 16-byte chunks per row of a stage
+constexpr int kTcMaxS = 6;        // pipeline stages at most
 constexpr int kTcThreads = 128;
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -141,9 +142,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     r2r_tc_k(const float *__restrict__ in, float *__restrict__ out, const unsigned char *__restrict__ Bg, int n, int npad,
              TcGeom geo, int *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smraw);  // [S] B bulk copy landed
-  uint64_t *done = full + 8;                              // [S] the block's MMAs finished reading the stage
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(smraw + 128);
+  uint64_t *rawf = reinterpret_cast<uint64_t *>(smraw);  // [S] raw A copies and B bytes landed
+  uint64_t *conv = rawf + 8;                              // [S] hi / lo written
+  uint64_t *empty = rawf + 16;                            // [S] the block's MMAs finished reading the stage
+  uint64_t *accf = rawf + 24;                             // every MMA finished
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smraw + 256);
   unsigned char *ops = smraw + 1024;
   const uint32_t a_bytes = kTcM * kTcBK * 4, b_bytes = (uint32_t)npad * kTcBK * 4;
   const uint32_t stage_bytes = 3 * a_bytes + 2 * b_bytes;
@@ -163,7 +166,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int nkb = (n + kTcBK - 1) / kTcBK;
 
   if (tid == 0) {
-    for (int i = 0; i < S; i++) mbar_init(full + i, 1), mbar_init(done + i, 1);
+    for (int i = 0; i < S; i++) mbar_init(rawf + i, 33), mbar_init(conv + i, 64), mbar_init(empty + i, 1);
+    mbar_init(accf, 1);
     mbar_fence_init();
   }
   if (warp == 0) {
@@ -177,111 +181,115 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_fence_after();
   const uint32_t tbase = *tslot;
 
-  // loads of block kb into stage kb % S: raw A by every thread (one commit
-  // group per block, empty past the last block), B by thread 0
-  auto issue_a = [&](int kb) {
-    if (kb < nkb) {
-      unsigned char *raw = ops + (size_t)(kb % S) * stage_bytes;
+  // Warp roles over the K blocks (stage s = kb % S, use u = kb / S):
+  //  warp 0     producer: after empty[s] of use u - 1, the raw A block by 16-byte
+  //             copies (every lane: cp.async.mbarrier.arrive.noinc on rawf[s])
+  //             and the B block by one bulk copy (lane 0: expect_tx on rawf[s])
+  //  warps 1-2  split: after rawf[s], hi / lo (MODE 1: transposed), then conv[s]
+  //  warp 3     lane 0 issues the block's MMAs after conv[s] and commits them to
+  //             empty[s]; after the last block a commit to accf
+  bool ok = true;
+  int kb_last = -1;  // producer: last block whose copies were issued
+  if (warp == 0) {
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % S, u = kb / S;
+      if (u > 0 && !mbar_wait(empty + s, (uint32_t)(u - 1) & 1u, err)) {
+        ok = false;
+        break;
+      }
+      unsigned char *raw = ops + (size_t)s * stage_bytes;
       const int k0 = kb * kTcBK;
       if (MODE == 0) {
-        for (int idx = tid; idx < kTcM * kTcCh; idx += kTcThreads) {
+        for (int idx = lane; idx < kTcM * kTcCh; idx += 32) {
           const int r = idx / kTcCh, q = idx % kTcCh, k = k0 + 4 * q;
           const bool v = m0 + r < M && k < n;
           cp_async16(raw + kblock_off(r, q, kTcM), v ? in + (m0 + r) * n + k : in, v ? 16u : 0u);
         }
       } else {  // raw chunk (m group g, k row kr) at g * 128 + kr * 16: 4 consecutive m of one k
-        for (int idx = tid; idx < kTcBK * (kTcM / 4); idx += kTcThreads) {
+        for (int idx = lane; idx < kTcBK * (kTcM / 4); idx += 32) {
           const int kr = idx / (kTcM / 4), g = idx % (kTcM / 4), k = k0 + kr;
           const bool v = k < n && 4 * g < mvalid;
           cp_async16(raw + g * 128 + kr * 16, v ? in + base + (long long)k * geo.ldk + 4 * g : in, v ? 16u : 0u);
         }
       }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rawf + s)) : "memory");
+      if (lane == 0) {
+        mbar_expect_tx(rawf + s, 2 * b_bytes);
+        bulk_load(raw + 3 * a_bytes, Bg + (size_t)kb * 2 * b_bytes, 2 * b_bytes, rawf + s);
+      }
+      kb_last = kb;
     }
-    cp_async_commit();
-  };
-  auto issue_b = [&](int kb) {
-    if (kb < nkb && tid == 0) {
-      unsigned char *st = ops + (size_t)(kb % S) * stage_bytes;
-      mbar_expect_tx(full + kb % S, 2 * b_bytes);
-      bulk_load(st + 3 * a_bytes, Bg + (size_t)kb * 2 * b_bytes, 2 * b_bytes, full + kb % S);
-    }
-  };
-  for (int p = 0; p < S - 1; p++) issue_a(p), issue_b(p);
-
-  bool ok = true;
-  int issued = 0, b_issued = min(nkb, S - 1);  // blocks whose MMAs are committed / whose B copy is issued
-  for (int kb = 0; kb < nkb && ok; kb++) {
-    const int s = kb % S;
-    unsigned char *st = ops + (size_t)s * stage_bytes;
-    cp_async_wait<S - 2>();
-    // this block's B landed (its copy was issued after block kb - S's MMAs finished)
-    ok = __syncthreads_and(mbar_wait(full + s, (uint32_t)(kb / S) & 1u, err));
-    if (!ok) break;
-    // split the raw block into TF32 hi / lo: MODE 0 at the same offsets;
-    // MODE 1 transposed from the raw m-contiguous chunks (4 m of one k) into
-    // the K-major layout of MODE 0
-    for (int c = tid; c < kTcM * kTcBK / 4; c += kTcThreads) {
-      const float4 v = *reinterpret_cast<const float4 *>(st + 16 * c);
-      uint4 hi, lo;
-      hi.x = tf32_round(v.x), hi.y = tf32_round(v.y), hi.z = tf32_round(v.z), hi.w = tf32_round(v.w);
-      lo.x = tf32_round(v.x - __uint_as_float(hi.x)), lo.y = tf32_round(v.y - __uint_as_float(hi.y));
-      lo.z = tf32_round(v.z - __uint_as_float(hi.z)), lo.w = tf32_round(v.w - __uint_as_float(hi.w));
-      if (MODE == 0) {
-        *reinterpret_cast<uint4 *>(st + a_bytes + 16 * c) = hi;
-        *reinterpret_cast<uint4 *>(st + 2 * a_bytes + 16 * c) = lo;
-      } else {
-        const int g = c >> 3, kr = c & 7;
-        const uint32_t h4[4] = {hi.x, hi.y, hi.z, hi.w}, l4[4] = {lo.x, lo.y, lo.z, lo.w};
+    cp_async_wait<0>();
+  } else if (warp <= 2) {
+    const int ct = tid - 32;
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % S;
+      if (!mbar_wait(rawf + s, (uint32_t)(kb / S) & 1u, err)) {
+        ok = false;
+        break;
+      }
+      unsigned char *st = ops + (size_t)s * stage_bytes;
+      for (int c = ct; c < kTcM * kTcBK / 4; c += 64) {
+        const float4 v = *reinterpret_cast<const float4 *>(st + 16 * c);
+        uint4 hi, lo;
+        hi.x = tf32_round(v.x), hi.y = tf32_round(v.y), hi.z = tf32_round(v.z), hi.w = tf32_round(v.w);
+        lo.x = tf32_round(v.x - __uint_as_float(hi.x)), lo.y = tf32_round(v.y - __uint_as_float(hi.y));
+        lo.z = tf32_round(v.z - __uint_as_float(hi.z)), lo.w = tf32_round(v.w - __uint_as_float(hi.w));
+        if (MODE == 0) {
+          *reinterpret_cast<uint4 *>(st + a_bytes + 16 * c) = hi;
+          *reinterpret_cast<uint4 *>(st + 2 * a_bytes + 16 * c) = lo;
+        } else {
+          const int g = c >> 3, kr = c & 7;
+          const uint32_t h4[4] = {hi.x, hi.y, hi.z, hi.w}, l4[4] = {lo.x, lo.y, lo.z, lo.w};
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const uint32_t o = kblock_off(4 * g + e, kr >> 2, kTcM) + (kr & 3) * 4;
-          *reinterpret_cast<uint32_t *>(st + a_bytes + o) = h4[e];
-          *reinterpret_cast<uint32_t *>(st + 2 * a_bytes + o) = l4[e];
+          for (int e = 0; e < 4; e++) {
+            const uint32_t o = kblock_off(4 * g + e, kr >> 2, kTcM) + (kr & 3) * 4;
+            *reinterpret_cast<uint32_t *>(st + a_bytes + o) = h4[e];
+            *reinterpret_cast<uint32_t *>(st + 2 * a_bytes + o) = l4[e];
+          }
         }
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(conv + s);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+  } else if (lane == 0) {
+    int issued = 0;
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % S;
+      if (!mbar_wait(conv + s, (uint32_t)(kb / S) & 1u, err)) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      const uint32_t sa = smem_u32(st);
-      for (int ks = 0; ks < kTcBK / 8; ks++) {
-        const uint32_t ah = sa + a_bytes + ks * kTcM * 32, al = ah + a_bytes;
-        for (int h0 = 0; h0 < npad; h0 += 256) {
-          const int nh = min(256, npad - h0);
-          const uint32_t bh = sa + 3 * a_bytes + ks * npad * 32 + (h0 >> 3) * 256, bl = bh + b_bytes;
-          const uint32_t idesc = tf32_idesc(nh), d = tbase + (uint32_t)h0;
-          const uint32_t first = (kb == 0 && ks == 0) ? 0u : 1u;
-          const uint64_t dah = kmajor_desc(ah, 128, 256), dal = kmajor_desc(al, 128, 256);
-          mma_tf32(d, dah, kmajor_desc(bh, 128, 256), idesc, first);
-          mma_tf32(d, dah, kmajor_desc(bl, 128, 256), idesc, 1u);
-          mma_tf32(d, dal, kmajor_desc(bh, 128, 256), idesc, 1u);
-        }
+      const uint32_t sa = smem_u32(ops + (size_t)s * stage_bytes);
+      const uint32_t ah = sa + a_bytes, al = ah + a_bytes;
+      for (int h0 = 0; h0 < npad; h0 += 256) {
+        const int nh = min(256, npad - h0);
+        const uint32_t bh = sa + 3 * a_bytes + (h0 >> 3) * 256, bl = bh + b_bytes;
+        const uint32_t idesc = tf32_idesc(nh), d = tbase + (uint32_t)h0;
+        const uint64_t dah = kmajor_desc(ah, 128, 256), dal = kmajor_desc(al, 128, 256);
+        mma_tf32(d, dah, kmajor_desc(bh, 128, 256), idesc, kb == 0 ? 0u : 1u);
+        mma_tf32(d, dah, kmajor_desc(bl, 128, 256), idesc, 1u);
+        mma_tf32(d, dal, kmajor_desc(bh, 128, 256), idesc, 1u);
       }
-      mma_commit(done + s);
+      mma_commit(empty + s);
+      issued = kb + 1;
     }
-    issued = kb + 1;
-    // block kb + S - 1 goes into the stage block kb - 1 used: its raw A at once
-    // (only the split read it, before the barrier above), its B and, at the
-    // next use, its hi / lo once block kb - 1's MMAs are done
-    const int nb = kb + S - 1;
-    if (nb < nkb && kb >= 1) {
-      const int sp = (kb - 1) % S;
-      ok = __syncthreads_and(mbar_wait(done + sp, (uint32_t)((kb - 1) / S) & 1u, err));
-      if (!ok) break;
-    }
-    issue_a(nb);
-    issue_b(nb);
-    if (nb < nkb) b_issued = nb + 1;
+    (void)issued;
+    mma_commit(accf);  // completes once every MMA issued above has finished
   }
-  cp_async_wait<0>();
-  if (issued > 0) {
-    const int kl = issued - 1;
-    if (ok) ok = __syncthreads_and(mbar_wait(done + (kl % S), (uint32_t)(kl / S) & 1u, err));
-    else mbar_drain(done + (kl % S), (uint32_t)(kl / S) & 1u);
-  }
-  if (!ok && tid == 0) {  // B copies issued but not consumed must land before the shared memory is released
-    for (int kb = issued; kb < b_issued; kb++) mbar_drain(full + kb % S, (uint32_t)(kb / S) & 1u);
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    ok = __syncthreads_and(mbar_wait(accf, 0u, err));
+  } else {
+    // MMAs issued before the failure, and bulk copies issued but not consumed,
+    // finish before the shared and tensor memory are released
+    mbar_drain(accf, 0u);
+    if (tid == 0)
+      for (int i = 0; i < S && i <= kb_last; i++) {
+        const int kb = kb_last - ((kb_last - i) % S);  // the last block issued into stage i
+        mbar_drain(rawf + i, (uint32_t)(kb / S) & 1u);
+      }
   }
   __syncthreads();
   tc_fence_after();
@@ -357,7 +365,6 @@ __global__ void tf32_arrange_k(const float *__restrict__ D, unsigned char *Bg, i
 // stages: lines up to 256 points keep a CTA within half the shared memory
 // (two CTAs of at most 256 accumulator columns share an SM), longer lines
 // take the whole of it; at most kTcMaxS stages
-constexpr int kTcMaxS = 6;
 static int tc_stages(int npad) {
   const size_t stage = 3 * (size_t)kTcM * kTcBK * 4 + 2 * (size_t)npad * kTcBK * 4;
   const size_t budget = (npad <= 256 ? 116 * 1024 : 227 * 1024) - 1024;
