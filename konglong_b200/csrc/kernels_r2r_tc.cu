@@ -19,21 +19,22 @@
 // is below 2^-22 of the product).  D is split once when the plans are made;
 // the lines are split while they are staged.
 //
-// Per CTA: 128 lines; K in blocks of 8 (one MMA k-step) through 2 to 6
-// shared-memory stages.  A block of lines arrives raw by 16-byte asynchronous copies
-// (cp.async, zero-filled past the grid) S - 1 blocks ahead and is split into
-// hi / lo shared-to-shared at the same offsets; D's TF32 parts are
-// pre-arranged in global memory exactly as a stage's B region, so B arrives by
-// one bulk copy per block on an mbarrier.  Operands sit in the canonical
-// no-swizzle K-major layout (8-row x 16-byte core matrices: rows of a core
-// matrix 16 B apart, the two K halves of one MMA k-step 128 B apart (LBO),
-// 8-row groups 256 B apart (SBO)).  One thread issues a block's MMAs and
-// commits them to the stage's mbarrier; a stage is refilled once that
-// commit has arrived.  After the last block every warp reads its 32
-// accumulator lanes (tcgen05.ld 32x32b) and stores its lines.  Every wait is
-// bounded (2^16 polls, error flag); a CTA that gives up waits for its
-// committed MMAs and issued copies and frees its tensor memory before it
-// returns.
+// Per CTA: 128 m and all n output columns (at most 512 accumulator columns);
+// K in blocks of 8 (one MMA k-step) through 2 to 6 shared-memory stages,
+// each holding the raw A block, its hi / lo parts and
+// the B block's hi / lo rows of the CTA's columns.  Operands sit in the
+// canonical no-swizzle K-major layout (8-row x 16-byte core matrices: rows of
+// a core matrix 16 B apart, the two K halves of one MMA k-step 128 B apart
+// (LBO), 8-row groups 256 B apart (SBO)).  Warp roles, handing off through
+// mbarriers only: warp 0 copies the raw A block by 16-byte cp.async
+// (zero-filled past the grid; completion counted on the stage barrier) and
+// the B rows by bulk copies from D's TF32 parts, pre-arranged in global
+// memory in that layout; warps 1-2 split A into hi / lo; one thread of warp 3
+// issues the MMAs and commits each stage back to the producer.  After the
+// last block all four warps read their 32 accumulator lanes (tcgen05.ld
+// 32x32b, 32 columns per load) and store.  Every wait is bounded (2^16
+// polls, error flag); a CTA that gives up drains its committed MMAs and
+// issued copies and frees its tensor memory before it returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,7 +50,6 @@ namespace {
 constexpr int kTcM = 128;   // lines per CTA (MMA M)
 constexpr int kTcBK = 8;    // K per stage (one MMA k-step)
 constexpr int kTcCh = kTcBK / 4;  // 16-byte chunks per row of a stage
-constexpr int kTcMaxS = 6;        // pipeline stages at most
 constexpr int kTcThreads = 128;
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -148,7 +148,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint64_t *accf = rawf + 24;                             // every MMA finished
   uint32_t *tslot = reinterpret_cast<uint32_t *>(smraw + 256);
   unsigned char *ops = smraw + 1024;
-  const uint32_t a_bytes = kTcM * kTcBK * 4, b_bytes = (uint32_t)npad * kTcBK * 4;
+  // this CTA's output columns [c_lo, c_lo + nw) (all npad of them: one column block per line tile)
+  const int c_lo = 0, nw = npad;
+  const uint32_t a_bytes = kTcM * kTcBK * 4, b_bytes = (uint32_t)nw * kTcBK * 4;
+  const size_t bfull = (size_t)npad * kTcBK * 4;  // one part of a K block of Bg
   const uint32_t stage_bytes = 3 * a_bytes + 2 * b_bytes;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // MODE 0: lines m0 .. m0 + 127 of length n, element (m, k) at in[m n + k];
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     base = g * geo.group_stride + mt * kTcM;
     mvalid = (int)min((long long)kTcM, geo.group_m - mt * kTcM);
   }
-  const uint32_t ncols = npad <= 32 ? 32 : npad <= 64 ? 64 : npad <= 128 ? 128 : npad <= 256 ? 256 : 512;
+  const uint32_t ncols = nw <= 32 ? 32 : nw <= 64 ? 64 : nw <= 128 ? 128 : nw <= 256 ? 256 : 512;
   const int nkb = (n + kTcBK - 1) / kTcBK;
 
   if (tid == 0) {
@@ -213,9 +216,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       }
       asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rawf + s)) : "memory");
-      if (lane == 0) {
+      if (lane == 0) {  // rows [c_lo, c_lo + nw) of the block's hi and lo parts (8-row groups of 256 B)
+        const unsigned char *blk = Bg + (size_t)kb * 2 * bfull + (size_t)c_lo * 32;
         mbar_expect_tx(rawf + s, 2 * b_bytes);
-        bulk_load(raw + 3 * a_bytes, Bg + (size_t)kb * 2 * b_bytes, 2 * b_bytes, rawf + s);
+        bulk_load(raw + 3 * a_bytes, blk, b_bytes, rawf + s);
+        bulk_load(raw + 3 * a_bytes + b_bytes, blk + bfull, b_bytes, rawf + s);
       }
       kb_last = kb;
     }
@@ -263,8 +268,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const uint32_t sa = smem_u32(ops + (size_t)s * stage_bytes);
       const uint32_t ah = sa + a_bytes, al = ah + a_bytes;
-      for (int h0 = 0; h0 < npad; h0 += 256) {
-        const int nh = min(256, npad - h0);
+      for (int h0 = 0; h0 < nw; h0 += 256) {  // N of at most 256 per MMA
+        const int nh = min(256, nw - h0);
         const uint32_t bh = sa + 3 * a_bytes + (h0 >> 3) * 256, bl = bh + b_bytes;
         const uint32_t idesc = tf32_idesc(nh), d = tbase + (uint32_t)h0;
         const uint64_t dah = kmajor_desc(ah, 128, 256), dal = kmajor_desc(al, 128, 256);
@@ -296,32 +301,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (ok && MODE == 1) {  // lane = m: for each column j the warp writes 32 consecutive floats
     const int m = warp * 32 + lane;
     const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < npad; c0 += 32) {
+    for (int c0 = 0; c0 < nw; c0 += 32) {
       uint32_t v[32];
       tmem_ld32(taddr + (uint32_t)c0, v);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (m < mvalid) {
-        float *o = out + base + (long long)c0 * geo.ldk + m;
+        float *o = out + base + (long long)(c_lo + c0) * geo.ldk + m;
 #pragma unroll
         for (int j = 0; j < 32; j++)
-          if (c0 + j < n) __stcs(o + (long long)j * geo.ldk, __uint_as_float(v[j]));
+          if (c_lo + c0 + j < n) __stcs(o + (long long)j * geo.ldk, __uint_as_float(v[j]));
       }
     }
   }
   if (ok && MODE == 0) {
     const long long row = m0 + warp * 32 + lane;
     const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
-    // 32 accumulator columns per load (npad is a multiple of 16: the last
-    // load may read 16 columns past npad, inside the allocation)
-    for (int c0 = 0; c0 < npad; c0 += 32) {
+    // 32 accumulator columns per load (nw is a multiple of 16: the last
+    // load may read 16 columns past nw, inside the allocation)
+    for (int c0 = 0; c0 < nw; c0 += 32) {
       uint32_t v[32];
       tmem_ld32(taddr + (uint32_t)c0, v);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
-        float *o = out + row * n + c0;
+        float *o = out + row * n + c_lo + c0;
 #pragma unroll
         for (int j = 0; j < 32; j += 4)
-          if (c0 + j + 4 <= n)
+          if (c_lo + c0 + j + 4 <= n)
             __stcs(reinterpret_cast<float4 *>(o + j), make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
                                                                   __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])));
       }
@@ -362,13 +367,13 @@ __global__ void tf32_arrange_k(const float *__restrict__ D, unsigned char *Bg, i
 }
 }  // namespace
 
-// stages: lines up to 256 points keep a CTA within half the shared memory
-// (two CTAs of at most 256 accumulator columns share an SM), longer lines
-// take the whole of it; at most kTcMaxS stages
+// stages: lines of up to 256 points keep a CTA within half the shared memory
+// (two CTAs of at most 256 accumulator columns share an SM; 2-4 stages);
+// longer lines take one CTA per SM with a 512-column accumulator (up to 6)
 static int tc_stages(int npad) {
   const size_t stage = 3 * (size_t)kTcM * kTcBK * 4 + 2 * (size_t)npad * kTcBK * 4;
-  const size_t budget = (npad <= 256 ? 116 * 1024 : 227 * 1024) - 1024;
-  return (int)std::min<size_t>(npad <= 256 ? 4 : kTcMaxS, budget / stage);
+  if (npad <= 256) return (int)std::min<size_t>(4, (113 * 1024 - 2048) / stage);  // two CTAs (1 KB reserved each)
+  return (int)std::min<size_t>(6, (227 * 1024 - 1024) / stage);                  // one CTA, 512 columns
 }
 
 size_t r2r_tc_smem(int n) {
@@ -428,7 +433,8 @@ void launch_r2r_tc(int axis, const float *in, float *out, const unsigned char *B
   const size_t sm = r2r_tc_smem(n);
   const int S = tc_stages(npad), mode = axis == 2 ? 0 : 1;
 #define RTM_TC_LAUNCH(MODE, SS) \
-  if (mode == MODE && S == SS) r2r_tc_k<MODE, SS><<<(unsigned)tiles, kTcThreads, sm, st>>>(in, out, Bg, n, npad, geo, err);
+  if (mode == MODE && S == SS)                                                                               \
+    r2r_tc_k<MODE, SS><<<(unsigned)tiles, kTcThreads, sm, st>>>(in, out, Bg, n, npad, geo, err);
   RTM_TC_ALL(RTM_TC_LAUNCH)
 #undef RTM_TC_LAUNCH
 }
