@@ -8,6 +8,7 @@
 //   spread_coeffs    Util::CompactOrmsbySpreadCoeff (bgprtm/Util.cpp:317-397)
 //                    with Receiver's taper_kernel (bgprtm/Receiver.cpp:291-303)
 //   r2r_line_matrix  FdEngine_r2r's derivative (bgprtm/FdEngine_r2r.cpp:4-102)
+//   r2c_line_matrix  FdEngine_r2c's derivative as a circulant (bgprtm/FdEngine_r2c.cpp:200-240)
 //                    as one matrix per axis and pass
 #include <algorithm>
 #include <cmath>
@@ -159,6 +160,32 @@ void pml_profile(int w, double d, double dt, double vmax, double eps, double sca
 //             B = DCT-III (REDFT01) B[t][0] = 1, B[t][j] = 2 cos(pi j (t + 1/2) / n)
 // with k_i = -(i + 1) dk and dk = pi / (d n) / 2 / n in float (constructor
 // :11-13, assignW :66-70).  D = B S F in FP64, rounded once.
+// FdEngine_r2c::fftderiv1_r2c (bgprtm/FdEngine_r2c.cpp:200-240) as the n x n
+// matrix it applies to a line: a real-to-complex FFT, bin j times i k_j
+// (k_j = -j dk, dk = 2 pi / (d n) / n in float, assignW :52-56; the DC bin and
+// an even line's Nyquist bin give 0; an odd line's last bin carries isign),
+// and the unnormalised complex-to-real FFT.  For a real line that is the
+// circulant D[t][u] = c[(t - u) mod n] with
+//   c[m] = -2 sum_{j=1..J} s_j k_j sin(2 pi j m / n),
+// J the last bin below Nyquist, s_j = isign for an odd line's last bin and 1
+// otherwise; FP64, rounded once.
+void r2c_line_matrix(int n, float d, int isign, std::vector<float> &D) {
+  const float dk = (float)(2.0f * M_PI / (double)(d * (float)n) * (double)(1.0f / float(n)));
+  const int J = n % 2 == 0 ? n / 2 - 1 : (n - 1) / 2;
+  std::vector<double> c(n, 0.0);
+  for (int m = 0; m < n; m++) {
+    double v = 0.0;
+    for (int j = 1; j <= J; j++) {
+      const double kj = (double)((float)(-j) * dk), sj = (n % 2 == 1 && j == n / 2) ? (double)isign : 1.0;
+      v += sj * kj * std::sin(2.0 * M_PI * (double)(((long long)j * m) % n) / n);
+    }
+    c[m] = -2.0 * v;
+  }
+  D.assign((size_t)n * n, 0.f);
+  for (int t = 0; t < n; t++)
+    for (int u = 0; u < n; u++) D[(size_t)t * n + u] = (float)c[(t - u + n) % n];
+}
+
 void r2r_line_matrix(int n, float d, int isign, std::vector<float> &D) {
   const float dk = (float)(M_PI / (double)(d * (float)n) * 0.5 * (double)(1.0f / float(n)));
   std::vector<double> SF((size_t)n * n, 0.0);  // S F: row i = the multiplied bin i

@@ -14,6 +14,7 @@ void pml_profile(int w, double d, double dt, double vmax, double eps, double sca
 // FFTWR2R first derivative of one axis as a row-major n x n line matrix
 // (out_t = sum_u D[t][u] x_u), isign +1 (cosine in, sine out) or -1
 void r2r_line_matrix(int n, float d, int isign, std::vector<float> &D);
+void r2c_line_matrix(int n, float d, int isign, std::vector<float> &D);
 // Util::CompactOrmsbySpreadCoeff + edge taper; returns the first grid index
 int spread_coeffs(int n, float x, float k1, float k2, int *nlimit, int dipole, int ntaper, float *coeff);
 }  // namespace rtm

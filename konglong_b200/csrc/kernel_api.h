@@ -327,7 +327,11 @@ int launch_fft_filter(FftPlans *p, int axis, int kind, float high, const float *
 struct FftPlans;
 // cuFFT plans of the three axes (y skipped when ny == 1) bound to stream st,
 // the wavenumber tables and the spectrum / transpose scratch
-int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st);
+// tensor_cores: the derivatives as circulant line matrices by the split-TF32
+// tcgen05 kernel where it applies (nz % 4 == 0, lines of at most 512 points);
+// err: device flag its bounded waits raise
+int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st,
+                     bool tensor_cores = false, int *err = nullptr);
 void fft_plans_destroy(FftPlans *p);
 // raw derivative of `in` along axis (0 x, 1 y, 2 z) into `out` (no PML);
 // isign +1 / -1 as FdEngine_r2c::fftderiv1_r2c's (the sign of bin n/2 for odd n)

@@ -130,6 +130,11 @@ struct FftAxis {
 
 struct FftPlans {
   FftAxis ax[3];
+  // the same derivatives as circulant line matrices on the tensor cores
+  // (kernels_r2r_tc.cu), per axis and isign, where that kernel applies
+  unsigned char *Bg[3][2] = {};
+  int tc[3] = {};
+  int *err = nullptr;
   int nx = 0, ny = 0, nz = 0;
   float2 *spec = nullptr;  // half spectrum of the largest axis set
   float *tr = nullptr;     // x lines made contiguous ([ny][nz][nx])
@@ -146,6 +151,9 @@ static std::vector<float> r2c_wavenumbers(int n, float d) {
 
 void fft_plans_destroy(FftPlans *p) {
   if (!p) return;
+  for (auto &a : p->Bg)
+    for (unsigned char *b : a)
+      if (b) cudaFree(b);
   for (FftAxis &a : p->ax) {
     if (a.made & 1) cufftDestroy(a.fwd);
     if (a.made & 2) cufftDestroy(a.inv);
@@ -156,10 +164,11 @@ void fft_plans_destroy(FftPlans *p) {
   delete p;
 }
 
-int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st) {
+int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy, float dz, cudaStream_t st,
+                     bool tensor_cores, int *err) {
   *out = nullptr;
   FftPlans *p = new FftPlans();
-  p->nx = nx, p->ny = ny, p->nz = nz;
+  p->nx = nx, p->ny = ny, p->nz = nz, p->err = err;
   const long long nxz = (long long)nx * nz;
   const int nn[3] = {nx, ny, nz};
   const float dd[3] = {dx, dy, dz};
@@ -214,6 +223,33 @@ int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy,
     fft_plans_destroy(p);
     return RTM_ERR_NOMEM;
   }
+  if (tensor_cores && r2r_tc_init() == 0) {
+    std::vector<float> D;
+    float *dD = nullptr;
+    for (int a = 0; a < 3; a++) {
+      if (nn[a] < 2 || !r2r_tc_supported(a, nx, ny, nz)) continue;
+      for (int s = 0; s < 2; s++) {
+        r2c_line_matrix(nn[a], dd[a], s == 0 ? 1 : -1, D);
+        if (cudaMalloc(&p->Bg[a][s], r2r_tc_bytes(nn[a])) != cudaSuccess ||
+            cudaMalloc(&dD, D.size() * 4) != cudaSuccess ||
+            cudaMemcpy(dD, D.data(), D.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+          cudaGetLastError();
+          if (dD) cudaFree(dD);
+          fft_plans_destroy(p);
+          return RTM_ERR_NOMEM;
+        }
+        launch_tf32_arrange(dD, p->Bg[a][s], nn[a], st);
+        const cudaError_t e = cudaStreamSynchronize(st);
+        cudaFree(dD), dD = nullptr;
+        if (e != cudaSuccess) {
+          fft_plans_destroy(p);
+          return RTM_ERR_CUDA;
+        }
+      }
+      p->tc[a] = 1;
+    }
+  }
+  cudaGetLastError();
   *out = p;
   return RTM_OK;
 }
@@ -222,6 +258,10 @@ int launch_fft_deriv(FftPlans *p, int axis, int isign, const float *in, float *o
   const FftAxis &f = p->ax[axis];
   if ((f.made & 3) != 3) return RTM_ERR_ARG;
   const int nx = p->nx, ny = p->ny, nz = p->nz;
+  if (p->tc[axis]) {  // the circulant line matrix on the tensor cores (split TF32)
+    launch_r2r_tc(axis, in, out, p->Bg[axis][isign == 1 ? 0 : 1], nx, ny, nz, p->err, st);
+    return cudaGetLastError() == cudaSuccess ? RTM_OK : RTM_ERR_CUDA;
+  }
   const float *src = in;
   float *dst = out;
   if (axis == 0) {  // [ny][nx][nz] -> [ny][nz][nx]

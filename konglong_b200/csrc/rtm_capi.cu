@@ -1550,7 +1550,8 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
       c->engine == RTM_ENGINE_SINCOS) {
     if ((rc = h->alloc(h->scr, h->n)) || (rc = h->alloc(h->scr2, h->n))) return fail(rc);
     if ((c->engine == RTM_ENGINE_R2C || c->engine == RTM_ENGINE_FFTV) &&
-        (rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st))) {
+        (rc = fft_plans_create(&h->fft, d->nx, d->ny, d->nz, d->dx, d->dy, d->dz, h->st, c->kernel_variant != 1,
+                               h->dflag))) {
       h->err = "cuFFT plan set-up failed";
       return fail(rc);
     }

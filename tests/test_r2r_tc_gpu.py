@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from konglong_b200.propagator import Propagator
-from konglong_b200.spec import ENGINE_R2R, FIELD_W1, ISO, TTI, VTI
+from konglong_b200.spec import ENGINE_FFTV, ENGINE_R2C, ENGINE_R2R, FIELD_W1, ISO, TTI, VTI
 from oracle import pyoracle as O
 from tests.conftest import rel_l2
 from tests.golden_inputs import case_inputs
@@ -56,3 +56,20 @@ def test_tensor_core_x_y_lines(shape):
         out[variant] = _steps(Propagator(spec), m, w0, w1, 2)
     assert np.abs(out[1]).max() > 0
     assert rel_l2(out[0], out[1]) < 2e-6, rel_l2(out[0], out[1])
+
+
+@pytest.mark.parametrize("engine", [ENGINE_R2C, ENGINE_FFTV])
+@pytest.mark.parametrize("shape", [(20, 24, 28), (21, 25, 36), (36, 20, 300)])
+def test_tensor_core_spectral_circulants(engine, shape):
+    """FFTWR2C / FFTV: each axis derivative as its circulant line matrix on the
+    tensor cores (kernel_variant 0) against cuFFT transforms with the bin
+    product (kernel_variant 1); odd lines carry the pass's isign on their last
+    bin (FdEngine_r2c::fftderiv1_r2c)."""
+    c = dict(engine=engine, model=VTI, shape=shape, pml=6, seed=78)
+    spec, m, w0, w1 = case_inputs(c)
+    out = {}
+    for variant in (0, 1):
+        spec.kernel_variant = variant
+        out[variant] = _steps(Propagator(spec), m, w0, w1, 2)
+    assert np.abs(out[1]).max() > 0
+    assert rel_l2(out[0], out[1]) < 3e-6, rel_l2(out[0], out[1])
