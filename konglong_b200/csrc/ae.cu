@@ -737,7 +737,8 @@ int rtm_ae_create(rtm_ae **out) {
   rtm_ae *a = new rtm_ae();
   cudaGetDevice(&a->device);
   const size_t b = (size_t)rtm::kNParams * 4;
-  if (cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking) || cudaMalloc(&a->p, b) || cudaMalloc(&a->g, b) ||
+  // a blocking stream: ordered after the parameter uploads (pageable cudaMemcpy)
+  if (cudaStreamCreate(&a->st) || cudaMalloc(&a->p, b) || cudaMalloc(&a->g, b) ||
       cudaMalloc(&a->m, b) || cudaMalloc(&a->v, b) || cudaMalloc(&a->loss, 4) || cudaMemset(a->p, 0, b) ||
       cudaMemset(a->m, 0, b) || cudaMemset(a->v, 0, b)) {
     cudaGetLastError();

@@ -210,7 +210,7 @@ int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy,
     }
     const std::vector<float> k = r2c_wavenumbers(n, dd[a]);
     if (cudaMalloc(&f.k, k.size() * 4) != cudaSuccess ||
-        cudaMemcpy(f.k, k.data(), k.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpyAsync(f.k, k.data(), k.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
       cudaGetLastError();
       fft_plans_destroy(p);
       return RTM_ERR_NOMEM;
@@ -232,7 +232,7 @@ int fft_plans_create(FftPlans **out, int nx, int ny, int nz, float dx, float dy,
         r2c_line_matrix(nn[a], dd[a], s == 0 ? 1 : -1, D);
         if (cudaMalloc(&p->Bg[a][s], r2r_tc_bytes(nn[a])) != cudaSuccess ||
             cudaMalloc(&dD, D.size() * 4) != cudaSuccess ||
-            cudaMemcpy(dD, D.data(), D.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaMemcpyAsync(dD, D.data(), D.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
           cudaGetLastError();
           if (dD) cudaFree(dD);
           fft_plans_destroy(p);
@@ -335,7 +335,7 @@ int r2r_plans_create(R2rPlans **out, int nx, int ny, int nz, float dx, float dy,
     for (int s = 0; s < 2; s++) {
       r2r_line_matrix(nn[a], dd[a], s == 0 ? 1 : -1, D);
       if (cudaMalloc(&p->D[a][s], D.size() * 4) != cudaSuccess ||
-          cudaMemcpy(p->D[a][s], D.data(), D.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+          cudaMemcpyAsync(p->D[a][s], D.data(), D.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
         cudaGetLastError();
         r2r_plans_destroy(p);
         return RTM_ERR_NOMEM;

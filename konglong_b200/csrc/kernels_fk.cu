@@ -195,7 +195,7 @@ extern "C" int rtm_fk_spread(const rtm_fk_args *a, int nr, const float *xy, cons
     if (code != RTM_OK) cudaGetLastError();
     return code;
   };
-  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return done(RTM_ERR_CUDA);
+  if (cudaStreamCreate(&st) != cudaSuccess) return done(RTM_ERR_CUDA);  // blocking: after the legacy-stream uploads
   if (cudaMalloc(&g, ncol * ntfft * 4) != cudaSuccess || cudaMalloc(&spec, ncol * nw * sizeof(float2)) != cudaSuccess)
     return done(RTM_ERR_NOMEM);
   if (fk_plan(&inv, ny, nx, ntfft, CUFFT_C2R) != CUFFT_SUCCESS) return done(RTM_ERR_CUDA);

@@ -1525,8 +1525,11 @@ int rtm_create(const rtm_dims *d, const rtm_config *c, rtm_handle **out) {
     cudaGetLastError();
     return fail(RTM_ERR_CUDA);
   }
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+  // a blocking stream: its work waits for earlier legacy-stream work, so the
+  // set-up uploads below (pageable cudaMemcpy, whose DMA may still be running
+  // when the call returns) land before any kernel of the engine reads them
+  if (cudaStreamCreate(&h->st) != cudaSuccess || cudaEventCreate(&h->ev0) != cudaSuccess ||
+      cudaEventCreate(&h->ev1) != cudaSuccess) {
     h->err = "stream/event creation failed";
     cudaGetLastError();
     return fail(RTM_ERR_CUDA);
@@ -2467,7 +2470,7 @@ int rtm_batch_create(rtm_handle *const *shots, int nshots, rtm_batch **out) {
   }
   b->device = shots[0]->device, b->pml3d = shots[0]->c.pml3d, b->model = shots[0]->c.model_type;
   cudaSetDevice(b->device);
-  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) || cudaEventCreate(&b->ev0) ||
+  if (cudaStreamCreate(&b->st) || cudaEventCreate(&b->ev0) ||  // blocking: ordered after the set-up uploads
       cudaEventCreate(&b->ev1)) {
     cudaGetLastError();
     rtm_batch_destroy(b);
