@@ -50,6 +50,7 @@ namespace {
 constexpr int kTcM = 128;   // lines per CTA (MMA M)
 constexpr int kTcBK = 8;    // K per stage (one MMA k-step)
 constexpr int kTcCh = kTcBK / 4;  // 16-byte chunks per row of a stage
+static_assert(kTcM / 4 == 32, "an x / y tile's 4-m chunks map one to one onto a warp's lanes");
 constexpr int kTcThreads = 128;
 
 __device__ __forceinline__ uint32_t tf32_round(float x) {
@@ -106,13 +107,13 @@ __device__ __forceinline__ uint32_t kblock_off(int r, int q, int rows) {
 
 }  // namespace
 
-// geometry of one launch: MODE 0 `lines` lines along K; MODE 1 tiles of 128
-// consecutive m in groups (x lines: one group per y plane of nz m; y lines:
-// one group of nx nz m), k stepping by ldk
+// geometry of one launch: MODE 0 `lines` lines along K; MODE 1 `total_m`
+// values of m, element (m, k) at (m / group_m) group_stride + k ldk +
+// m % group_m (x lines: groups = y planes of nz m; y lines: one group of nx nz
+// m); group_m % 4 == 0, so a 16-byte run of 4 m never crosses a group
 struct TcGeom {
   long long lines;
-  long long ldk, group_stride, group_m;
-  long long tiles_per_group;
+  long long ldk, group_stride, group_m, total_m;
 };
 
 // 16-byte asynchronous copy, zero-filled when src_bytes is 0
@@ -155,16 +156,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t stage_bytes = 3 * a_bytes + 2 * b_bytes;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // MODE 0: lines m0 .. m0 + 127 of length n, element (m, k) at in[m n + k];
-  // MODE 1: element (m, k) at in[base + k ldk + m], m < mvalid
-  long long m0 = 0, base = 0, M = 0;
-  int mvalid = 0;
-  if (MODE == 0) {
-    m0 = (long long)blockIdx.x * kTcM, M = geo.lines;
-  } else {
-    const long long g = blockIdx.x / geo.tiles_per_group, mt = blockIdx.x % geo.tiles_per_group;
-    base = g * geo.group_stride + mt * kTcM;
-    mvalid = (int)min((long long)kTcM, geo.group_m - mt * kTcM);
-  }
+  // MODE 1: m0 .. m0 + 127 of total_m, element (m, k) at mn_off(m) + k ldk
+  const long long m0 = (long long)blockIdx.x * kTcM;
+  const long long M = MODE == 0 ? geo.lines : geo.total_m;
+  auto mn_off = [&](long long m) { return (m / geo.group_m) * geo.group_stride + m % geo.group_m; };
+  // MODE 1 producer: lane = the tile's 4-m chunk (kTcM / 4 == 32), located once
+  const bool lane_m_ok = MODE == 1 && m0 + 4 * lane < M;
+  const long long lane_off = lane_m_ok ? mn_off(m0 + 4 * lane) : 0;
   const uint32_t ncols = nw <= 32 ? 32 : nw <= 64 ? 64 : nw <= 128 ? 128 : nw <= 256 ? 256 : 512;
   const int nkb = (n + kTcBK - 1) / kTcBK;
 
@@ -209,10 +207,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           cp_async16(raw + kblock_off(r, q, kTcM), v ? in + (m0 + r) * n + k : in, v ? 16u : 0u);
         }
       } else {  // raw chunk (m group g, k row kr) at g * 128 + kr * 16: 4 consecutive m of one k
-        for (int idx = lane; idx < kTcBK * (kTcM / 4); idx += 32) {
-          const int kr = idx / (kTcM / 4), g = idx % (kTcM / 4), k = k0 + kr;
-          const bool v = k < n && 4 * g < mvalid;
-          cp_async16(raw + g * 128 + kr * 16, v ? in + base + (long long)k * geo.ldk + 4 * g : in, v ? 16u : 0u);
+        for (int kr = 0; kr < kTcBK; kr++) {  // one k row per copy
+          const int k = k0 + kr;
+          const bool v = k < n && lane_m_ok;
+          cp_async16(raw + lane * 128 + kr * 16, v ? in + lane_off + (long long)k * geo.ldk : in, v ? 16u : 0u);
         }
       }
       asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(rawf + s)) : "memory");
@@ -299,14 +297,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   if (ok && MODE == 1) {  // lane = m: for each column j the warp writes 32 consecutive floats
-    const int m = warp * 32 + lane;
+    const long long m = m0 + warp * 32 + lane;
+    const long long mo = m < M ? mn_off(m) : 0;
     const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
     for (int c0 = 0; c0 < nw; c0 += 32) {
       uint32_t v[32];
       tmem_ld32(taddr + (uint32_t)c0, v);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (m < mvalid) {
-        float *o = out + base + (long long)(c_lo + c0) * geo.ldk + m;
+      if (m < M) {
+        float *o = out + mo + (long long)(c_lo + c0) * geo.ldk;
 #pragma unroll
         for (int j = 0; j < 32; j++)
           if (c_lo + c0 + j < n) __stcs(o + (long long)j * geo.ldk, __uint_as_float(v[j]));
@@ -424,11 +423,11 @@ void launch_r2r_tc(int axis, const float *in, float *out, const unsigned char *B
     geo.lines = (long long)nx * ny;
     tiles = (geo.lines + kTcM - 1) / kTcM;
   } else if (axis == 1) {
-    geo.ldk = nxz, geo.group_stride = 0, geo.group_m = nxz, geo.tiles_per_group = (nxz + kTcM - 1) / kTcM;
-    tiles = geo.tiles_per_group;
-  } else {
-    geo.ldk = nz, geo.group_stride = nxz, geo.group_m = nz, geo.tiles_per_group = (nz + kTcM - 1) / kTcM;
-    tiles = geo.tiles_per_group * ny;
+    geo.ldk = nxz, geo.group_stride = 0, geo.group_m = nxz, geo.total_m = nxz;
+    tiles = (geo.total_m + kTcM - 1) / kTcM;
+  } else {  // x lines: m over (y, z) pairs, so no tile is cut short at a y plane's end
+    geo.ldk = nz, geo.group_stride = nxz, geo.group_m = nz, geo.total_m = (long long)ny * nz;
+    tiles = (geo.total_m + kTcM - 1) / kTcM;
   }
   const size_t sm = r2r_tc_smem(n);
   const int S = tc_stages(npad), mode = axis == 2 ? 0 : 1;
