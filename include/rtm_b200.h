@@ -120,9 +120,11 @@ typedef struct rtm_config {
                          for VTI / TTI, the state is FP32; the autotuner picks among all FD8
                          kernels; compact FD: line solves and pointwise epilogues with TMA x / y
                          tiles when nz % 4 == 0, else register-streamed x / y lines; the
-                         autotuner may pick any compact-FD form; FFTWR2R / SINCOS: line
-                         operators on the tensor cores, split TF32), 1: one cell per thread /
-                         plain staged tiles (FFTWR2R / SINCOS: FP32 cuBLAS line products),
+                         autotuner may pick any compact-FD form; FFTWR2R / SINCOS / FFTWR2C /
+                         FFTV: line operators on the tensor cores, split TF32, where nz % 4 == 0
+                         and lines have at most 512 points), 1: one cell per thread / plain
+                         staged tiles (FFTWR2R / SINCOS: FP32 cuBLAS line products; FFTWR2C /
+                         FFTV: cuFFT transforms),
                          2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline, 3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z
                          cells per thread with register prefetch, 5: compact FD with
                          register-streamed x / y lines, 6: compact FD segment-parallel (line
