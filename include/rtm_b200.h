@@ -125,8 +125,9 @@ typedef struct rtm_config {
                          and lines have at most 512 points), 1: one cell per thread / plain
                          staged tiles (FFTWR2R / SINCOS: FP32 cuBLAS line products; FFTWR2C /
                          FFTV: cuFFT transforms),
-                         2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline, 3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z
-                         cells per thread with register prefetch, 5: compact FD with
+                         2: compact-FD x / y TMA tiles, ISO FD8 one-cell TMA plane pipeline,
+                         3: FD8 4 z cells per thread with TMA rings, 4: ISO FD8 4 z cells per
+                         thread with register prefetch, 5: compact FD with
                          register-streamed x / y lines, 6: compact FD segment-parallel (line
                          solves with the PML, scaling and update fused into them) with plain tile
                          loads, 7: as 3 with the visco-acoustic update loading its Q memory
