@@ -132,12 +132,12 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                : "memory");
 }
 
-// out[l][j] = sum_k D[j][k] in[l][k] for the 128 lines of this CTA.  Bg holds
-// D's TF32 parts pre-arranged per K block exactly as a stage's B region (hi
-// then lo, canonical layout, rows n .. npad-1 and columns past n zero), so a
-// stage's B arrives by one bulk copy.  A arrives raw by 16-byte asynchronous
-// copies S - 1 blocks ahead and is split into hi / lo in shared memory.
-// Stage s: raw A | A hi | A lo | B hi | B lo.
+// D_acc[m][j] = sum_k A[m][k] D[j][k] for the 128 m of this CTA (MODE 0: z
+// lines, MODE 1: x / y columns).  Bg holds D's TF32 parts pre-arranged per K
+// block exactly as a stage's B region (hi then lo, canonical layout, rows
+// n .. npad-1 and columns past n zero), so a stage's B arrives by bulk copies;
+// A arrives raw by 16-byte asynchronous copies and is split into hi / lo in
+// shared memory.  Stage s: raw A | A hi | A lo | B hi | B lo; S stages.
 template <int MODE, int S>
 __global__ void __launch_bounds__(kTcThreads, 1)
     r2r_tc_k(const float *__restrict__ in, float *__restrict__ out, const unsigned char *__restrict__ Bg, int n, int npad,
