@@ -40,6 +40,8 @@
  *       (bgprtm/ImagingCorrelator.cpp:180-194, bgprtm/ImagingCondition.cpp:180-226)
  *   Propagator::modelling / migration time loops -> rtm_modelling / rtm_migration
  *       (bgprtm/Propagator.cpp:1054-1155, 1157-1260)
+ *   PhaseCorrection::applyForward / applyBackward -> rtm_phase_correct
+ *       (bgprtm/PhaseCorrection.cpp:117-235)
  */
 #ifndef RTM_B200_H
 #define RTM_B200_H
@@ -226,6 +228,45 @@ typedef struct rtm_fk_args {
 } rtm_fk_args;
 /* xy [nr][2]: fractional grid indices (x, y); traces [nr][nt]; out [ny][nx][nt] */
 int rtm_fk_spread(const rtm_fk_args *a, int nr, const float *xy, const float *traces, float *out);
+
+/* Time-dispersion / phase correction of traces (PhaseCorrection,
+ * bgprtm/PhaseCorrection.h:11-25, bgprtm/PhaseCorrection.cpp:14-235): the
+ * constructor's arguments and the global parameters it reads, then
+ * applyForward (apply 1) or applyBackward (apply 2) on ntr traces of nt
+ * samples.  The correction table exp(i phs(iw, it)) * factor(iw) of init()
+ * (:62-115) is built on the host in the reference's float order; the table
+ * transforms (fft_dft's time sum, dft_fft's frequency sum) run as one tiled
+ * FP32 product kernel, the plain transforms on cuFFT.  libfftv (fft_r2c_fd,
+ * fft_c2r_bd, padfftv) is absent from the reference tree; its conventions
+ * are inferred from these call sites: forward unnormalised with exp(+i w t),
+ * the Nyquist bin packed into bin 0's imaginary part (cleared by the
+ * reference), backward the unnormalised Hermitian sum with exp(-i w t);
+ * ntfft is the caller's (even, >= nt).
+ * Output: apply 1 writes [ntr][nt]; apply 2 writes [ntr][nt_dft] (nt_dft =
+ * nt_out when resampling, else nt).  scaler (apply 2) multiplies the first
+ * nt_out samples of each output trace when nt_out > 0 (:138-139; every
+ * reference call passes one trace).  Refused (RTM_ERR_ARG): apply 1 on a
+ * direction other than FWD (:117), resampling with apply 1 or on a dft_fft
+ * path (:182), the no-op (no tdsp, w_pow 0, phase 0) with resampling (:130),
+ * fft_dft without the table when ntfft < nt_out (the reference leaves the
+ * output's tail unwritten, :185-186).  Host in, host out, on the current
+ * device. */
+typedef struct rtm_phase_args {
+  int nt;                   /* samples per input trace */
+  float dt, Dt, t0, fmax;   /* sample interval, propagation dt (0: no dispersion term), start time, max frequency */
+  int direction;            /* PhaseCorrection::DIRECTION: 0 NONE, 1 FWD, 2 BWD */
+  float w_pow, phase_deg;   /* (i w)^w_pow magnitude factor, constant phase rotation (degrees) */
+  int do_tdsp;              /* 0: no table (tdsp_correction forced to 0) */
+  int nt_out;               /* resampling: output samples (> 0 with dt_out > 0), else -1 */
+  float dt_out, t0_out;     /* resampling: output interval and start time */
+  int ntfft;                /* time FFT length (libfftv::padfftv stand-in), even, >= nt */
+  int tdsp_correction;      /* global tdsp_correction (reference default 2) */
+  int skip_tdsp_correction; /* global skip_tdsp_correction bits (1 FWD, 2 BWD) */
+  float tdsp_acos_ratio;    /* global tdsp_acos_ratio (0: sin form, 1: acos form) */
+  int skip_jacobian;        /* global tdsp_skip_jacobian */
+  int transform;            /* 0: by direction; 1: tdsp_force_fftdft; 2: tdsp_force_dftfft */
+} rtm_phase_args;
+int rtm_phase_correct(const rtm_phase_args *a, int apply, int ntr, const float *in, float *out, float scaler);
 
 /* The FFTWR2R first derivative along one axis of n points with spacing d as
  * the row-major n x n matrix D the engine applies to every line (out_t =

@@ -24,7 +24,7 @@ STATUS_CODE = {v: k for k, v in STATUS.items()}
 # every entry point of include/rtm_b200.h
 EXPORTS = ["rtm_config_default", "rtm_create", "rtm_destroy", "rtm_last_error", "rtm_set_q_coeffs",
            "rtm_set_model", "rtm_reset", "rtm_kernel", "rtm_update2nd", "rtm_swap",
-           "rtm_spread_coeffs", "rtm_r2r_line_matrix", "rtm_fk_spread", "rtm_set_injection", "rtm_set_extraction", "rtm_inject",
+           "rtm_spread_coeffs", "rtm_r2r_line_matrix", "rtm_fk_spread", "rtm_phase_correct", "rtm_set_injection", "rtm_set_extraction", "rtm_inject",
            "rtm_extract", "rtm_get_traces", "rtm_snapshot_setup", "rtm_snapshot_store",
            "rtm_snapshot_load", "rtm_image_setup", "rtm_image_accumulate", "rtm_modelling",
            "rtm_migration", "rtm_get", "rtm_put", "rtm_c16_compress", "rtm_c16_uncompress",
@@ -87,6 +87,7 @@ def lib():
     L.rtm_spread_coeffs.argtypes = [i, f, f, f, C.POINTER(i), i, i, _f32p, C.POINTER(i)]
     L.rtm_r2r_line_matrix.argtypes = [i, f, i, _f32p]
     L.rtm_fk_spread.argtypes = [vp, i, _f32p, _f32p, _f32p]
+    L.rtm_phase_correct.argtypes = [vp, i, i, _f32p, _f32p, f]
     L.rtm_set_injection.argtypes = [vp, i, i, i, i, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, i, f]
     L.rtm_set_extraction.argtypes = [vp, i, i, i, i, _i32p, _i32p, _f32p, _f32p, _f32p, i]
     L.rtm_inject.argtypes = [vp, i]

@@ -438,6 +438,63 @@ def fk_spread(nx, ny, nt, ntfft, dt, dx, dy, xy, traces, vsurf, z, trueamp=1, de
     return out
 
 
+class PhaseArgs(C.Structure):
+    """rtm_phase_args (include/rtm_b200.h)."""
+    _fields_ = [("nt", C.c_int), ("dt", C.c_float), ("Dt", C.c_float), ("t0", C.c_float), ("fmax", C.c_float),
+                ("direction", C.c_int), ("w_pow", C.c_float), ("phase_deg", C.c_float), ("do_tdsp", C.c_int),
+                ("nt_out", C.c_int), ("dt_out", C.c_float), ("t0_out", C.c_float), ("ntfft", C.c_int),
+                ("tdsp_correction", C.c_int), ("skip_tdsp_correction", C.c_int), ("tdsp_acos_ratio", C.c_float),
+                ("skip_jacobian", C.c_int), ("transform", C.c_int)]
+
+
+def pad_fft_length(n):
+    """The smallest even length >= n with no prime factor above 7 (stands in
+    for libfftv::padfftv, which is absent from the reference tree)."""
+    m = max(2, int(n) + (int(n) & 1))
+    while True:
+        r = m
+        for p in (2, 3, 5, 7):
+            while r % p == 0:
+                r //= p
+        if r == 1:
+            return m
+        m += 2
+
+
+class PhaseCorrection:
+    """PhaseCorrection (bgprtm/PhaseCorrection.h:11-25) on the GPU: the
+    constructor's arguments, the global parameters it reads as keywords
+    (tpad_ratio, tdsp_correction, skip_tdsp_correction, tdsp_acos_ratio,
+    tdsp_skip_jacobian, tdsp_force_fftdft / tdsp_force_dftfft as transform 1 / 2),
+    and applyForward / applyBackward on [ntr][nt] traces through
+    rtm_phase_correct.  Results are returned (the reference works in place)."""
+    NONE, FWD, BWD = 0, 1, 2
+
+    def __init__(self, nt, dt, Dt, t0, fmax, direction, w_pow=0.0, phase_deg=0.0, do_tdsp=1, ntOut=-1, dtOut=-1.0,
+                 t0Out=0.0, *, ntfft=None, tpad_ratio=0.5, tdsp_correction=2, skip_tdsp_correction=0,
+                 tdsp_acos_ratio=0.0, skip_jacobian=False, transform=0):
+        if ntfft is None:
+            ntfft = pad_fft_length(int(np.rint(np.float32(nt) * np.float32(1 + tpad_ratio))))
+        self.args = PhaseArgs(nt, dt, Dt, t0, fmax, direction, w_pow, phase_deg, int(do_tdsp), ntOut, dtOut, t0Out,
+                              ntfft, tdsp_correction, skip_tdsp_correction, tdsp_acos_ratio, int(bool(skip_jacobian)),
+                              transform)
+        self.nt = nt
+        self.nt_dft = ntOut if (dtOut > 0 and ntOut > 0) else nt
+
+    def _run(self, apply, trace, ntr, nout, scaler=1.0):
+        tr = np.ascontiguousarray(trace, np.float32).reshape(ntr, self.nt)
+        out = np.zeros((ntr, nout), np.float32)
+        _lib.check(_lib.lib().rtm_phase_correct(C.byref(self.args), apply, ntr, tr.ravel(), out.ravel(),
+                                                float(scaler)), "rtm_phase_correct")
+        return out
+
+    def applyForward(self, trace, ntr):
+        return self._run(1, trace, ntr, self.nt)
+
+    def applyBackward(self, trace, ntr, scaler=1.0):
+        return self._run(2, trace, ntr, self.nt_dft, scaler)
+
+
 def c16_compress(a, nx, ny, nz):
     out = np.zeros((nx * nz + 2) * ny, np.uint16)
     _lib.check(_lib.lib().rtm_c16_compress(_arr(a), out, nx, ny, nz), "rtm_c16_compress")
