@@ -10,7 +10,7 @@ dispersion forms, the tdsp_correction 1 routes, the plain-transform routes
 (no table) with w_pow and a phase rotation, and the no-op.  Sizes: one trace,
 ragged counts around the 64-trace tiles, odd nt and nt_out.  Tolerance: the
 table and the products are FP32 on both sides of the reference's own sums
-(thousands of terms), so the relative L2 error is held to 2e-5."""
+(thousands of terms); measured worst relative L2 1.2e-6, held to 5e-6."""
 import numpy as np
 import pytest
 
@@ -78,13 +78,13 @@ ROUTES = {
 def test_routes_match_the_oracle(route, ntr, nt):
     kw, apply = ROUTES[route]
     got, want = _check(kw, apply, ntr, nt, DT, seed=ntr + nt)
-    assert rel_l2(got, want) < 2e-5, (route, rel_l2(got, want))
+    assert rel_l2(got, want) < 5e-6, (route, rel_l2(got, want))
 
 
 def test_scaler_on_the_first_nt_out_samples():
     kw = dict(pos=(DTP, 0.0, 60.0, BWD, 0.0, 0.0, 1, 301, 0.006))
     got, want = _check(kw, 2, 5, 500, DT, seed=7, scaler=1.0 / 12.5)
-    assert rel_l2(got, want) < 2e-5
+    assert rel_l2(got, want) < 5e-6
     unscaled, _ = _check(kw, 2, 5, 500, DT, seed=7)
     np.testing.assert_allclose(got, unscaled / 12.5, rtol=1e-6, atol=1e-7 * np.abs(unscaled).max())
 
@@ -110,4 +110,4 @@ def test_large_batch_and_long_traces():
     p = P.Plan(3000, DT, DTP, 0.0, 60.0, BWD, ntfft=pc.args.ntfft)
     idx = np.arange(0, 2000, 97)
     want = P.apply_backward(p, x[idx])
-    assert rel_l2(got[idx], want) < 2e-5, rel_l2(got[idx], want)
+    assert rel_l2(got[idx], want) < 5e-6, rel_l2(got[idx], want)
