@@ -137,8 +137,9 @@ typedef struct rtm_config {
                          segment-parallel with TMA tile loads where the tensor maps can be made,
                          9: as 0 with each compact-FD z line solve carrying the interior cells of
                          the pointwise epilogue that follows it (the PML cells stay separate
-                         launches) (the 4-cell and segment-parallel variants fall back when they
-                         do not apply) */
+                         launches), 10: as 0 with the compact-FD x / y line solves by the
+                         pipelined persistent TMA kernel (the 4-cell and segment-parallel
+                         variants fall back when they do not apply) */
   int use_rho;        /* density model (KernelCPU::setModel's rho, bgprtm/KernelCPU.cpp:76-78):
                          the gradient is divided by rho (KernelCPU::divideRho) and the divergence
                          accumulates vel * rho (bgprtm/FdEngine_fd.cpp:411, 437, 463); ISO then takes
