@@ -2,7 +2,8 @@
 // PhaseCorrection (bgprtm/PhaseCorrection.cpp:14-235).
 //   init (:62-115): the table T[iw][it] = exp(i phs(iw, it)) * factor(iw) for
 //     the band iw < nw1 (up to fmax) and it < nt_dft, built on the host in
-//     float with the reference's operation order and types; on the device as
+//     float with the reference's operation order and types (row blocks on
+//     host threads); on the device as
 //     rows 2 iw (real parts) and 2 iw + 1 (imaginary parts) of one matrix.
 //   fft_dft (:141-190): zero-padded forward transform (cuFFT R2C, conjugated:
 //     libfftv's forward carries exp(+i w t)), Nyquist cleared, the band's bins
@@ -24,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "rtm_b200.h"
@@ -189,24 +191,46 @@ void pc_plan(const rtm_phase_args &a, PcPlan &p) {
   p.nw1 = std::min(p.nw, (int)nearbyintf((float)(2.0f * kPcPi * a.fmax / dw)) + 1);
   const int nw1 = p.nw1, nt_dft = p.nt_dft;
   const float ratio = a.tdsp_acos_ratio;
-  if (p.tdsp) p.table.assign((size_t)2 * nw1 * nt_dft, 0.f);
-  for (int iw = 0; p.tdsp && iw < nw1; iw++) {
-    const double x = (double)iw * dw * a.Dt;
-    const float factor = jacobian ? 2.0f * cosf((float)(x / 2)) : 2.0f;
-    const float dsp = (a.Dt == 0 || skip) ? 0.f : (float)((ratio * dsp_acos(x) + (1 - ratio) * dsp_sin(x)) * dt_dft / a.Dt);
-    float *tr = &p.table[(size_t)2 * iw * nt_dft], *ti = tr + nt_dft;
-    for (int it = 0; it < nt_dft; it++) {
-      float phs;
-      if (a.dt == dt_dft) {
-        const float lin = (it - it0) * dsp;
-        phs = (float)(lin - (double)(((long)(it - it_shift) * iw) % a.ntfft) * dw * dt_dft + t_shift_frac * iw * dw);
-      } else {
-        phs = (it - it0) * dsp - (float)dw * dt_dft * it * iw + (float)dw * t_shift * iw;
-        phs = round_down_angle(phs);
+  // rows iw0 .. iw1 - 1 of the table; rows are independent, so the row
+  // blocks run on host threads and the table is the same bit for bit
+  auto rows = [&](int iw0, int iw1) {
+    for (int iw = iw0; iw < iw1; iw++) {
+      const double x = (double)iw * dw * a.Dt;
+      const float factor = jacobian ? 2.0f * cosf((float)(x / 2)) : 2.0f;
+      const float dsp =
+          (a.Dt == 0 || skip) ? 0.f : (float)((ratio * dsp_acos(x) + (1 - ratio) * dsp_sin(x)) * dt_dft / a.Dt);
+      float *tr = &p.table[(size_t)2 * iw * nt_dft], *ti = tr + nt_dft;
+      for (int it = 0; it < nt_dft; it++) {
+        float phs;
+        if (a.dt == dt_dft) {
+          const float lin = (it - it0) * dsp;
+          phs = (float)(lin - (double)(((long)(it - it_shift) * iw) % a.ntfft) * dw * dt_dft + t_shift_frac * iw * dw);
+        } else {
+          phs = (it - it0) * dsp - (float)dw * dt_dft * it * iw + (float)dw * t_shift * iw;
+          phs = round_down_angle(phs);
+        }
+        tr[it] = cosf(phs) * factor;
+        ti[it] = sinf(phs) * factor;
       }
-      tr[it] = cosf(phs) * factor;
-      ti[it] = sinf(phs) * factor;
     }
+  };
+  if (p.tdsp) {
+    p.table.assign((size_t)2 * nw1 * nt_dft, 0.f);
+    const long long work = (long long)nw1 * nt_dft;
+    const int nth = (int)std::min<long long>({(long long)std::max(1u, std::thread::hardware_concurrency()), 16LL,
+                                              work / (1LL << 16) + 1, (long long)nw1});
+    std::vector<std::thread> th;
+    int handed = 0;  // rows given to threads
+    try {
+      for (int t = 0; t < nth - 1; t++) {
+        const int r1 = (int)((long long)nw1 * (t + 1) / nth);
+        th.emplace_back(rows, handed, r1);
+        handed = r1;
+      }
+    } catch (...) {  // no more threads: this one takes the rest
+    }
+    rows(handed, nw1);
+    for (auto &t : th) t.join();
   }
   // the band's spectral multipliers of fft_dft / dft_fft (:158-163, :210-214)
   const float dwf = (float)(2.0f * M_PI / (a.ntfft * a.dt)), scaler = 1.0f / a.ntfft;
